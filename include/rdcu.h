@@ -1,0 +1,182 @@
+/*
+ * rdcu.h -- C ABI of librdcu, a B200 (sm_100a) FP64 solver for dictionary
+ * reaction-diffusion equations
+ *
+ *     du_i/dt = sum_j Sigma_ij Theta_j,   Theta_j = prod_k Y_k^eta_jk,
+ *
+ * where Y = (u_i, d_a u_i, d_a d_b u_i) on a periodic uniform grid in 1-3 dimensions.
+ *
+ * Two methods, as in the reference rdcu:
+ *   RDCU_METHOD_DP45  explicit Dormand-Prince 4(5) with pseudospectral derivatives;
+ *   RDCU_METHOD_BDF   implicit variable-order NDF/BDF with 2nd-order finite differences.
+ *
+ * The reference has no library boundary: its CLI (rdcu.cu main) calls file-static
+ * steppers through function-pointer callbacks (dp45.h:7-11, bdf.h:9-13).  This ABI
+ * replaces that stepper <-> problem callback boundary with one opaque, re-entrant
+ * handle that owns its CUDA stream and device buffers.  Every entry point returns an
+ * int status: RDCU_OK (0) or a negative RDCU_ERR_* code; rdcu_last_error() gives the
+ * message.  Plain pointers and sizes only; no CUDA or C++ types in the signatures.
+ *
+ * Memory conventions: "device" pointers are CUDA device (or managed) addresses on the
+ * handle's device; entry points that accept "host or device" detect the kind.
+ * A state vector y has n*N doubles, field-major, each field a C-order grid with the
+ * last axis fastest (N = Ns[0]*...*Ns[ndim-1]).
+ */
+#ifndef RDCU_H
+#define RDCU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RDCU_OK 0
+#define RDCU_ERR_INVALID -1     /* bad argument or specification */
+#define RDCU_ERR_CUDA -2        /* a CUDA runtime call failed */
+#define RDCU_ERR_UNSUPPORTED -3 /* size or option outside what the library implements */
+#define RDCU_ERR_TIMEOUT -4     /* a bounded device loop gave up */
+#define RDCU_ERR_NOMEM -5       /* device or host allocation failed */
+#define RDCU_ERR_NUMERIC -6     /* linear solve or iteration failed to converge */
+#define RDCU_ERR_STATE -7       /* call out of order (e.g. eval before any step) */
+#define RDCU_ERR_CALLBACK -8    /* the output callback returned non-zero */
+
+#define RDCU_METHOD_DP45 0
+#define RDCU_METHOD_BDF 1
+
+typedef struct rdcu_handle rdcu_t;
+
+/* Problem specification.  Mirrors the reference's option values (rdcu.cu:603-607,
+ * 612-731) and its coupling-term table (rdcu.cu:606, 654-660, 822-837): term i has
+ * coefficient C[i] and the integer list c[i][0..nprods[i]-1] = field, then
+ * (Y index, power) pairs, Y index k = Yind*n + field with Yind 0 (u), 1..ndim (d_a u),
+ * ndim+1+a*ndim+b (d_a d_b u).  A list of odd length reads the missing last power as 0,
+ * as the reference's calloc'ed buffer does. */
+typedef struct rdcu_spec {
+  int n;                 /* number of fields (-n) */
+  int ndim;              /* 1..3 (number of -N values) */
+  int Ns[3];             /* grid points per axis (-N) */
+  double Ls[3];          /* domain length per axis (-L) */
+  int nterms;            /* number of coupling terms */
+  const double *C;       /* [nterms] coefficients */
+  const int *nprods;     /* [nterms] length of each integer list */
+  const int *const *c;   /* [nterms] integer lists (field, Yidx, pow, Yidx, pow, ...) */
+  int method;            /* RDCU_METHOD_DP45 or RDCU_METHOD_BDF (-S) */
+  int fixed;             /* fixed time step (-F) */
+  double rtol, atol;     /* -r, -a */
+  int device;            /* CUDA device ordinal (-g) */
+} rdcu_spec;
+
+/* Sizes and resources of a handle. */
+typedef struct rdcu_info {
+  long long state_len;   /* n*N */
+  long long Y_len;       /* n*(1+ndim+ndim^2)*N complex values written by rdcu_rhs's Y */
+  long long nnz_max;     /* capacity needed for rdcu_jac's cols/vals */
+  int n_channels;        /* inverse spectral channels of the fused RHS (DP45) */
+  int order;             /* current BDF order (0 for DP45) */
+  void *stream;          /* the handle's cudaStream_t */
+  long long device_bytes;/* device memory held by the handle */
+} rdcu_info;
+
+/* ---- lifecycle -------------------------------------------------------------------
+ * Replaces dp45_init (dp45.h:8) / bdf_init (bdf.h:10) together with the problem set-up
+ * in rdcu.cu main (plans rdcu.cu:899-900, device buffers rdcu.cu:1065-1088, stencils
+ * init_dY rdcu.cu:1147).  Allocates all device memory once. */
+int rdcu_create(rdcu_t **out, const rdcu_spec *spec);
+/* Replaces dp45_destroy (dp45.h:10) / bdf_destroy (bdf.h:12) and main's cleanup. */
+int rdcu_destroy(rdcu_t *h);
+
+/* State (t, h, y) and, for BDF, the order and backward differences D_1..D_order as
+ * fs.dat stores them (rdcu.cu:944-990).  y and D may be host or device pointers;
+ * D may be NULL when order == 0.  Replaces the initial-value copy of
+ * dp45_init/bdf_init (dp45.cu:207, bdf.cu:449). */
+int rdcu_set_state(rdcu_t *h, double t, double hstep, const double *y, int order,
+                   const double *D);
+/* Reads the state back; y (n*N) and D (order*n*N) may be host or device pointers or
+ * NULL.  This is what fs.dat holds (rdcu.cu:320-339). */
+int rdcu_get_state(rdcu_t *h, double *t, double *hstep, int *order, double *y, double *D);
+
+int rdcu_get_info(rdcu_t *h, rdcu_info *info);
+
+/* ---- problem evaluations ---------------------------------------------------------
+ * f = dydt(t, y) (rdcu.cu:167-184).  y, f: host or device pointers (n*N).  If Y is not NULL
+ * it receives every Y block as complex128 pairs, n*(1+ndim+ndim^2)*N of them, the
+ * layout of Y.dat (rdcu.cu:287-291): for DP45 the full complex inverse transform of
+ * each block (real and imaginary parts, makeY rdcu.cu:151-164); for BDF the real
+ * finite-difference blocks with zero imaginary parts (rdcu.cu:122-149). */
+int rdcu_rhs(rdcu_t *h, double t, const double *y, double *f, double *Y);
+
+/* CSR Jacobian of the finite-difference RHS at y (rdcu.cu:186-250): rows (n*N+1),
+ * cols/vals (capacity rdcu_info.nnz_max) and *nnz; host or device pointers.
+ * Column order and explicit zeros follow the csrgeam2 accumulation of the reference.
+ * For DP45 handles the reference has no stencils; the result is nnz = 0 with all-zero
+ * row pointers, which is what the reference's -D4 dump of a non-stiff run holds. */
+int rdcu_jac(rdcu_t *h, double t, const double *y, int *nnz, int *rows, int *cols,
+             double *vals);
+
+/* ---- stepping --------------------------------------------------------------------
+ * One step attempt from the current state: dp45_step (dp45.h:7, dp45.cu:87-147) or
+ * bdf_step (bdf.h:9, bdf.cu:135-323).  On return *t and *hstep are the updated time
+ * and step size and *accepted is 1 (accepted) or 0 (rejected).  The incoming *t and
+ * *hstep must equal the handle's state (they are the reference's in/out pointers). */
+int rdcu_step(rdcu_t *h, double *t, double *hstep, double hmin, double hmax, int *accepted);
+
+/* Dense output at t_eval within the last accepted step: dp45_eval (dp45.cu:149-152)
+ * or bdf_eval (bdf.cu:325-328).  y_eval: host or device pointer (n*N). */
+int rdcu_eval(rdcu_t *h, double t_eval, double *y_eval);
+
+/* ---- whole integration -----------------------------------------------------------
+ * Events delivered by rdcu_solve, in the order the reference's step_eval
+ * (rdcu.cu:252-341) acts on them. */
+#define RDCU_EV_ATTEMPT 0    /* after every attempt: t, h, accepted (steps.dat) */
+#define RDCU_EV_EVAL 1       /* one per output time passed: t_eval, y = dense output */
+#define RDCU_EV_CHECKPOINT 2 /* after the evals of one step: t, h, y = D (fs.dat) */
+
+typedef struct rdcu_event {
+  int kind;
+  int accepted;      /* ATTEMPT */
+  int steps;         /* accepted steps so far */
+  int eval_index;    /* EVAL: index into t_eval */
+  int order;         /* BDF order after the step (0 for DP45) */
+  double t, h;       /* time and step size after the attempt */
+  double t_eval;     /* EVAL */
+  const double *y;   /* EVAL: device pointer to y(t_eval) (n*N);
+                        CHECKPOINT: device pointer to the state y (n*N), followed for
+                        BDF by D_1..D_order (each n*N) */
+} rdcu_event;
+
+typedef int (*rdcu_out_cb)(void *user, const rdcu_event *ev);
+
+/* Integrates while t < t1 and h > hmin: dp45_run (dp45.h:9, dp45.cu:154-169) or
+ * bdf_run (bdf.h:11, bdf.cu:330-389), with the output logic of step_eval: after each
+ * accepted step, one EVAL per t_eval[i] <= t not yet output, then a CHECKPOINT if any
+ * EVAL was delivered.  Steps run on the device without host round trips between
+ * output times.  cb may be NULL.  t_eval: host array of n_eval increasing times. */
+int rdcu_solve(rdcu_t *h, double t1, double hmin, double hmax, const double *t_eval,
+               int n_eval, rdcu_out_cb cb, void *user);
+
+/* Runs exactly n_attempts step attempts from the current state with the controller on
+ * the device and no host round trip between them (the loop body of dp45_run,
+ * dp45.cu:159-168, without outputs); the stepping-only workload of the benchmark.
+ * *accepted receives how many were accepted.  DP45 handles only. */
+int rdcu_advance(rdcu_t *h, int n_attempts, double hmin, double hmax, long long *accepted);
+
+/* Accepted steps and attempts counted by the last rdcu_solve. */
+int rdcu_get_counters(rdcu_t *h, long long *accepted, long long *attempts);
+
+/* Uniform random initial condition of the reference CLI (rdcu.cu:898,991-1001):
+ * srand(seed); y[N*i+j] = A0 + A/2*(2.0/RAND_MAX*rand()-1), field loop outer, with the
+ * C library's own rand().  y: host array of n*N doubles.  No handle needed. */
+int rdcu_random_ic(double *y, int n, long long N, double A, double A0, int seed);
+
+/* Synchronous copy of `bytes` bytes between any host/device pointers on the handle's
+ * device (the reference's cudaMemcpy calls around step_eval, rdcu.cu:277-320). */
+int rdcu_memcpy(rdcu_t *h, void *dst, const void *src, unsigned long long bytes);
+
+/* ---- errors ----------------------------------------------------------------------- */
+const char *rdcu_error_string(int code);
+/* Last error message of the handle (or of the last failed rdcu_create when h is NULL). */
+const char *rdcu_last_error(rdcu_t *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RDCU_H */

@@ -1,0 +1,25 @@
+"""CPU restatement of the reference rdcu solver -- TEST INFRASTRUCTURE ONLY.
+
+This package is the parity oracle for the CUDA library in ``rdcu_b200``.  It restates,
+in numpy/scipy, what the reference's CUDA C++ does on the hot path:
+
+* ``problem``  -- coupling-term parsing, Y-index table, glibc ``rand()`` initial
+  conditions and the binary file formats (reference ``rdcu.cu``).
+* ``spectral`` -- the pseudospectral Y blocks and the dictionary RHS
+  (reference ``rdcu.cu:78-106,117-184``).
+* ``fd``       -- finite-difference stencils, FD Y blocks and the CSR Jacobian
+  (reference ``rdcu.cu:108-149,186-250,385-596``).
+* ``dp45``     -- the Dormand-Prince 4(5) stepper (reference ``dp45.cu``).
+* ``bdf``      -- the variable-order NDF/BDF stepper (reference ``bdf.cu``), with a
+  scipy sparse LU in place of cuDSS.
+* ``run``      -- an emulation of the reference ``main``/``step_eval`` that writes the
+  same output files (reference ``rdcu.cu:252-341,599-1273``).
+
+Parity pinning: the oracle is checked against fixtures produced by the reference's
+own nvcc build (``oracle/build_ref.sh``) under ``tests/golden``; see the generating
+script there.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py`` (its ``cpu_baseline``
+leg and its reference arm) may import this package, and only as the checker or the
+timed CPU baseline -- never as a product code path.
+"""

@@ -1,0 +1,24 @@
+#!/usr/bin/env bash
+# Builds the reference rdcu from its own sources, unmodified, for sm_100a:
+#   nvcc -arch=sm_100a -O3 rdcu.cu dp45.cu bdf.cu -lcufft -lcublas -lcusparse
+# with the link-only cuDSS stand-in of oracle/cudss_stub (cuDSS is not installed in
+# this image; the reference's DP45 path never calls it).  Output: oracle/_ref/rdcu_ref.
+# Test infrastructure: the binary produces golden fixtures and is the reference arm of
+# bench.py; librdcu never links or calls it.
+set -euo pipefail
+HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+REF="${RDCU_REFERENCE_DIR:-/root/reference}"
+OUT="$HERE/_ref"
+NVCC="${NVCC:-/usr/local/cuda/bin/nvcc}"
+if [ ! -f "$REF/rdcu.cu" ]; then
+  echo "reference sources not found at $REF" >&2
+  exit 2
+fi
+mkdir -p "$OUT"
+if [ -x "$OUT/rdcu_ref" ] && [ "$OUT/rdcu_ref" -nt "$REF/rdcu.cu" ] && [ "$OUT/rdcu_ref" -nt "$HERE/cudss_stub/cudss_stub.c" ]; then
+  exit 0
+fi
+"$NVCC" -arch=sm_100a -O3 -w -I"$HERE/cudss_stub" \
+  "$REF/rdcu.cu" "$REF/dp45.cu" "$REF/bdf.cu" "$HERE/cudss_stub/cudss_stub.c" \
+  -lcufft -lcublas -lcusparse -Xlinker -rpath=/usr/local/cuda/lib64 -o "$OUT/rdcu_ref"
+echo "built $OUT/rdcu_ref"

@@ -1,0 +1,275 @@
+"""rdcu_b200 -- B200-native FP64 dictionary reaction-diffusion solver.
+
+Python binding of the C ABI in ``include/rdcu.h`` (``librdcu.so``, built in-tree by
+``rdcu_b200.build``).  The reference drives its solver through the ``rdcu`` command
+line (its Python post-processing runs ``./rdcu`` with ``os.system``,
+reference makelines.py:260-268); the same CLI is built here as ``rdcu_b200/bin/rdcu``.
+This module exposes the library itself to Python: problem handles, RHS and Jacobian
+evaluation, stepping, dense output and whole integrations with an output callback.
+
+Device memory is passed as raw CUDA pointers (for example ``torch.Tensor.data_ptr()``
+of a float64 CUDA tensor).  There is no CPU fallback: loading fails loudly when the
+library is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Callable, List, Optional, Sequence
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "librdcu.so")
+CLI_PATH = os.path.join(HERE, "bin", "rdcu")
+
+RDCU_OK = 0
+RDCU_ERR_INVALID = -1
+RDCU_ERR_CUDA = -2
+RDCU_ERR_UNSUPPORTED = -3
+RDCU_ERR_TIMEOUT = -4
+RDCU_ERR_NOMEM = -5
+RDCU_ERR_NUMERIC = -6
+RDCU_ERR_STATE = -7
+RDCU_ERR_CALLBACK = -8
+
+METHOD_DP45 = 0
+METHOD_BDF = 1
+
+EV_ATTEMPT = 0
+EV_EVAL = 1
+EV_CHECKPOINT = 2
+
+# exported entry points of include/rdcu.h
+EXPORTS = [
+    "rdcu_create", "rdcu_destroy", "rdcu_set_state", "rdcu_get_state", "rdcu_get_info",
+    "rdcu_rhs", "rdcu_jac", "rdcu_step", "rdcu_eval", "rdcu_solve", "rdcu_get_counters",
+    "rdcu_memcpy", "rdcu_advance", "rdcu_random_ic", "rdcu_error_string", "rdcu_last_error",
+]
+
+
+class RdcuError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__("rdcu error %d: %s" % (code, msg))
+        self.code = code
+
+
+class rdcu_spec(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_int), ("ndim", ctypes.c_int), ("Ns", ctypes.c_int * 3),
+        ("Ls", ctypes.c_double * 3), ("nterms", ctypes.c_int),
+        ("C", ctypes.POINTER(ctypes.c_double)), ("nprods", ctypes.POINTER(ctypes.c_int)),
+        ("c", ctypes.POINTER(ctypes.POINTER(ctypes.c_int))), ("method", ctypes.c_int),
+        ("fixed", ctypes.c_int), ("rtol", ctypes.c_double), ("atol", ctypes.c_double),
+        ("device", ctypes.c_int),
+    ]
+
+
+class rdcu_info(ctypes.Structure):
+    _fields_ = [
+        ("state_len", ctypes.c_longlong), ("Y_len", ctypes.c_longlong),
+        ("nnz_max", ctypes.c_longlong), ("n_channels", ctypes.c_int), ("order", ctypes.c_int),
+        ("stream", ctypes.c_void_p), ("device_bytes", ctypes.c_longlong),
+    ]
+
+
+class rdcu_event(ctypes.Structure):
+    _fields_ = [
+        ("kind", ctypes.c_int), ("accepted", ctypes.c_int), ("steps", ctypes.c_int),
+        ("eval_index", ctypes.c_int), ("order", ctypes.c_int), ("t", ctypes.c_double),
+        ("h", ctypes.c_double), ("t_eval", ctypes.c_double), ("y", ctypes.c_void_p),
+    ]
+
+
+OUT_CB = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(rdcu_event))
+
+_lib = None
+
+
+def load_library(path: Optional[str] = None) -> ctypes.CDLL:
+    """Loads librdcu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError("librdcu.so not found at %s; run `python -m rdcu_b200.build`" % p)
+    lib = ctypes.CDLL(p)
+    vp, i, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    pd, pi = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)
+    lib.rdcu_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(rdcu_spec)]
+    lib.rdcu_destroy.argtypes = [vp]
+    lib.rdcu_set_state.argtypes = [vp, d, d, vp, i, vp]
+    lib.rdcu_get_state.argtypes = [vp, pd, pd, pi, vp, vp]
+    lib.rdcu_get_info.argtypes = [vp, ctypes.POINTER(rdcu_info)]
+    lib.rdcu_rhs.argtypes = [vp, d, vp, vp, vp]
+    lib.rdcu_jac.argtypes = [vp, d, vp, pi, vp, vp, vp]
+    lib.rdcu_step.argtypes = [vp, pd, pd, d, d, pi]
+    lib.rdcu_eval.argtypes = [vp, d, vp]
+    lib.rdcu_solve.argtypes = [vp, d, d, d, pd, i, OUT_CB, vp]
+    lib.rdcu_get_counters.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]
+    lib.rdcu_memcpy.argtypes = [vp, vp, vp, ctypes.c_ulonglong]
+    lib.rdcu_advance.argtypes = [vp, i, d, d, ctypes.POINTER(ctypes.c_longlong)]
+    lib.rdcu_random_ic.argtypes = [pd, i, ctypes.c_longlong, d, d, i]
+    lib.rdcu_error_string.argtypes = [i]
+    lib.rdcu_error_string.restype = ctypes.c_char_p
+    lib.rdcu_last_error.argtypes = [vp]
+    lib.rdcu_last_error.restype = ctypes.c_char_p
+    for name in EXPORTS:
+        if name not in ("rdcu_error_string", "rdcu_last_error"):
+            getattr(lib, name).restype = ctypes.c_int
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def parse_terms(lines: Sequence[str]):
+    """(C, ints) per coupling term from reference-format strings ``C,field,k,p,...``.
+    The CLI (and the oracle) restate the reference's exact parser; this helper accepts
+    well-formed terms only."""
+    out = []
+    for s in lines:
+        toks = [t for t in s.split(",") if t != ""]
+        out.append((float(toks[0]), [int(t) for t in toks[1:]]))
+    return out
+
+
+def random_ic(n: int, N: int, A: float, A0: float, seed: int):
+    """The reference CLI's glibc-rand() initial condition (rdcu.cu:991-1001), as numpy."""
+    import numpy as np
+
+    lib = load_library()
+    y = np.empty(n * N, np.float64)
+    rc = lib.rdcu_random_ic(y.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n, N, A, A0, seed)
+    if rc != RDCU_OK:
+        raise RdcuError(rc, lib.rdcu_last_error(None).decode())
+    return y
+
+
+class Solver:
+    """One problem handle (``rdcu_t``)."""
+
+    def __init__(self, n: int, Ns: Sequence[int], Ls: Sequence[float], terms, method: int = METHOD_DP45,
+                 rtol: float = 1e-8, atol: float = 1e-8, fixed: bool = False, device: int = 0):
+        self.lib = load_library()
+        ndim = len(Ns)
+        self.n, self.Ns, self.Ls = n, tuple(Ns), tuple(Ls)
+        terms = [(float(C), list(ints)) for C, ints in terms]
+        self._C = (ctypes.c_double * max(1, len(terms)))(*[t[0] for t in terms])
+        self._np = (ctypes.c_int * max(1, len(terms)))(*[len(t[1]) for t in terms])
+        self._lists = [(ctypes.c_int * max(1, len(t[1])))(*t[1]) for t in terms]
+        self._c = (ctypes.POINTER(ctypes.c_int) * max(1, len(terms)))(
+            *[ctypes.cast(l, ctypes.POINTER(ctypes.c_int)) for l in self._lists])
+        spec = rdcu_spec()
+        spec.n = n
+        spec.ndim = ndim
+        for a in range(3):
+            spec.Ns[a] = Ns[a] if a < ndim else 1
+            spec.Ls[a] = Ls[a] if a < ndim else 1.0
+        spec.nterms = len(terms)
+        spec.C = ctypes.cast(self._C, ctypes.POINTER(ctypes.c_double))
+        spec.nprods = ctypes.cast(self._np, ctypes.POINTER(ctypes.c_int))
+        spec.c = ctypes.cast(self._c, ctypes.POINTER(ctypes.POINTER(ctypes.c_int)))
+        spec.method = method
+        spec.fixed = 1 if fixed else 0
+        spec.rtol = rtol
+        spec.atol = atol
+        spec.device = device
+        h = ctypes.c_void_p()
+        rc = self.lib.rdcu_create(ctypes.byref(h), ctypes.byref(spec))
+        if rc != RDCU_OK:
+            raise RdcuError(rc, self.lib.rdcu_last_error(None).decode())
+        self.h = h
+        self.method = method
+
+    def _check(self, rc):
+        if rc != RDCU_OK:
+            raise RdcuError(rc, self.lib.rdcu_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.rdcu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> rdcu_info:
+        inf = rdcu_info()
+        self._check(self.lib.rdcu_get_info(self.h, ctypes.byref(inf)))
+        return inf
+
+    @property
+    def stream(self) -> int:
+        return self.info().stream
+
+    def set_state(self, t: float, h: float, y_ptr: int, order: int = 0, D_ptr: int = 0):
+        self._check(self.lib.rdcu_set_state(self.h, t, h, ctypes.c_void_p(y_ptr), order,
+                                            ctypes.c_void_p(D_ptr) if D_ptr else None))
+
+    def get_state(self, y_ptr: int = 0, D_ptr: int = 0):
+        t, h, o = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        self._check(self.lib.rdcu_get_state(self.h, ctypes.byref(t), ctypes.byref(h), ctypes.byref(o),
+                                            ctypes.c_void_p(y_ptr) if y_ptr else None,
+                                            ctypes.c_void_p(D_ptr) if D_ptr else None))
+        return t.value, h.value, o.value
+
+    def rhs(self, y_ptr: int, f_ptr: int, Y_ptr: int = 0, t: float = 0.0):
+        self._check(self.lib.rdcu_rhs(self.h, t, ctypes.c_void_p(y_ptr), ctypes.c_void_p(f_ptr),
+                                      ctypes.c_void_p(Y_ptr) if Y_ptr else None))
+
+    def jac(self, y_ptr: int, rows_ptr: int, cols_ptr: int, vals_ptr: int, t: float = 0.0) -> int:
+        nnz = ctypes.c_int()
+        self._check(self.lib.rdcu_jac(self.h, t, ctypes.c_void_p(y_ptr), ctypes.byref(nnz),
+                                      ctypes.c_void_p(rows_ptr), ctypes.c_void_p(cols_ptr),
+                                      ctypes.c_void_p(vals_ptr)))
+        return nnz.value
+
+    def step(self, t: float, h: float, hmin: float = 0.0, hmax: float = float("inf")):
+        tt, hh, acc = ctypes.c_double(t), ctypes.c_double(h), ctypes.c_int()
+        self._check(self.lib.rdcu_step(self.h, ctypes.byref(tt), ctypes.byref(hh), hmin, hmax,
+                                       ctypes.byref(acc)))
+        return bool(acc.value), tt.value, hh.value
+
+    def eval(self, t_eval: float, y_ptr: int):
+        self._check(self.lib.rdcu_eval(self.h, t_eval, ctypes.c_void_p(y_ptr)))
+
+    def solve(self, t1: float, t_eval: Sequence[float] = (), hmin: float = 0.0, hmax: float = float("inf"),
+              callback: Optional[Callable[[rdcu_event], int]] = None):
+        te = (ctypes.c_double * max(1, len(t_eval)))(*t_eval)
+
+        def _cb(user, evp):
+            try:
+                return int(callback(evp.contents) or 0) if callback else 0
+            except Exception:  # an exception in Python aborts the solve
+                import traceback
+                traceback.print_exc()
+                return 1
+
+        cb = OUT_CB(_cb)
+        self._check(self.lib.rdcu_solve(self.h, t1, hmin, hmax, ctypes.cast(te, ctypes.POINTER(ctypes.c_double)),
+                                        len(t_eval), cb, None))
+
+    def memcpy(self, dst: int, src: int, nbytes: int):
+        """Synchronous copy between host/device addresses."""
+        self._check(self.lib.rdcu_memcpy(self.h, ctypes.c_void_p(dst), ctypes.c_void_p(src), nbytes))
+
+    def copy_to_numpy(self, src: int, count: int):
+        """float64 array of `count` values copied from a device address."""
+        import numpy as np
+
+        out = np.empty(count, np.float64)
+        self.memcpy(out.ctypes.data, src, count * 8)
+        return out
+
+    def advance(self, n_attempts: int, hmin: float = 0.0, hmax: float = float("inf")) -> int:
+        """Runs n attempts on the device; returns how many were accepted."""
+        acc = ctypes.c_longlong()
+        self._check(self.lib.rdcu_advance(self.h, n_attempts, hmin, hmax, ctypes.byref(acc)))
+        return acc.value
+
+    def counters(self):
+        a, b = ctypes.c_longlong(), ctypes.c_longlong()
+        self._check(self.lib.rdcu_get_counters(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value

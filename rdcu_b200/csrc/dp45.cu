@@ -1,0 +1,484 @@
+// Dormand-Prince 4(5) with the step controller on the device.
+//
+// One attempt = six fused RHS stages (spectral.cu; the stage combination is fused into
+// the forward pass and the error estimate into the stage-7 inverse pass) and one
+// single-CTA controller kernel.  The controller restates dp45_step's accept/reject
+// logic (dp45.cu:109-146) on the device, rotates the state and slope buffers (the
+// reference's y<-ytemp, ylast<-y and FSAL k1<-k7 copies, dp45.cu:128-129,165-167)
+// by swapping slot indices, logs h after every attempt (steps.dat, rdcu.cu:257-259)
+// and stops the device loop at the first accepted step that passes an output time,
+// so the host only wakes up at output times.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "dp45.h"
+
+namespace rdcu {
+
+// dense-output coefficients (dp45.cu:15-21), row j = k_{j+1}, column p = x^(p+1)
+__constant__ double c_p[7][4] = {
+    {1.0, -8048581381.0 / 2820520608, 8663915743.0 / 2820520608, -12715105075.0 / 11282082432},
+    {0, 0, 0, 0},
+    {0, 131558114200.0 / 32700410799, -68118460800.0 / 10900136933, 87487479700.0 / 32700410799},
+    {0, -1754552775.0 / 470086768, 14199869525.0 / 1410260304, -10690763975.0 / 1880347072},
+    {0, 127303824393.0 / 49829197408, -318862633887.0 / 49829197408, 701980252875.0 / 199316789632},
+    {0, -282668133.0 / 205662961, 2019193451.0 / 616988883, -1453857185.0 / 822651844},
+    {0, 40617522.0 / 29380423, -110615467.0 / 29380423, 69997945.0 / 29380423}};
+
+namespace {
+
+constexpr int kCtlThreads = 256;
+
+__global__ void k_dp45_arm(DP45Ctl* c, int check, double t1, double hmin, double hmax, int eval_i,
+                           int n_eval, int max_attempts) {
+  c->check_t1 = check;
+  c->t1 = t1;
+  c->hmin = hmin;
+  c->hmax = hmax;
+  c->eval_i = eval_i;
+  c->n_eval = n_eval;
+  c->max_attempts = max_attempts;
+  c->attempts_this_launch = 0;
+  c->log_count = 0;
+  c->stop_reason = kStopNone;
+  c->running = check ? ((c->t < t1 && c->h > hmin) ? 1 : 0) : 1;
+  if (!c->running) c->stop_reason = kStopDone;
+}
+
+__global__ void __launch_bounds__(kCtlThreads) k_dp45_ctl(DP45Ctl* c, const double* part, double* log_h,
+                                                          double* log_t, int* log_acc, double nN,
+                                                          const double* t_eval) {
+  if (!c->running) return;
+  __shared__ double red[kCtlThreads];
+  const int tid = threadIdx.x;
+  double s = 0.0;
+  if (!c->fixed)
+    for (int i = tid; i < c->nparts; i += kCtlThreads) s += part[i];
+  red[tid] = s;
+  __syncthreads();
+  for (int w = kCtlThreads / 2; w > 0; w >>= 1) {
+    if (tid < w) red[tid] += red[tid + w];
+    __syncthreads();
+  }
+  if (tid != 0) return;
+  double t = c->t, h = c->h;
+  int acc;
+  if (c->fixed) {
+    acc = 1;
+    c->t_last = t;
+    t = t + h;
+  } else {
+    // dp45.cu:117-146: RMS norm of the scaled error, factor 0.9 err^-1/5 (0.2 if NaN)
+    double norm = sqrt(red[0]);
+    norm /= pow(nN, 0.5);
+    c->err_norm = norm;
+    double factor = 0.9 * pow(norm, -0.2);
+    if (isnan(factor)) factor = 0.2;
+    if (norm < 1) {
+      acc = 1;
+      c->t_last = t;
+      t = t + h;
+      if (factor > 10) factor = 10;
+      h *= factor;
+      if (h > c->hmax) h = c->hmax;
+    } else {
+      acc = 0;
+      if (factor < 1) {
+        if (factor < 0.2) factor = 0.2;
+        h *= factor;
+      }
+    }
+  }
+  if (acc) {
+    const int y_old = c->y_slot, yn = c->yn_slot, yl = c->yl_slot;
+    c->yl_slot = y_old;
+    c->y_slot = yn;
+    c->yn_slot = yl;
+    c->last_k1_buf = c->k1_buf;
+    c->last_k7_buf = c->k7_buf;
+    const int k1 = c->k1_buf;
+    c->k1_buf = c->k7_buf;
+    c->k7_buf = k1;
+    c->n_accepted++;
+  }
+  c->t = t;
+  c->h = h;
+  c->accepted = acc;
+  c->n_attempts++;
+  c->attempts_this_launch++;
+  if (c->log_count < c->log_cap) {
+    log_h[c->log_count] = h;
+    log_t[c->log_count] = t;
+    log_acc[c->log_count] = acc;
+  }
+  c->log_count++;
+  if (!c->check_t1) {
+    c->running = 0;
+    return;
+  }
+  int reason = kStopNone;
+  if (acc && c->eval_i < c->n_eval && t >= t_eval[c->eval_i]) reason = kStopOutput;
+  else if (!(t < c->t1 && h > c->hmin)) reason = kStopDone;
+  else if (c->log_count >= c->log_cap) reason = kStopLog;
+  else if (c->attempts_this_launch >= c->max_attempts) reason = kStopChunk;
+  if (reason != kStopNone) {
+    c->running = 0;
+    c->stop_reason = reason;
+  }
+}
+
+// interpolate kernel (dp45.cu:70-76) over the last accepted step
+__global__ void k_dp45_interp(DP45Bufs b, const DP45Ctl* c, double t_eval, double* out, long long nN) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nN) return;
+  const double* yl = b.ybuf[c->yl_slot];
+  const double* k[7];
+  k[0] = b.kbuf[c->last_k1_buf];
+  for (int j = 1; j < 6; ++j) k[j] = b.kbuf[j];
+  k[6] = b.kbuf[c->last_k7_buf];
+  const double h = c->t - c->t_last, h2 = t_eval - c->t_last;
+  const double x = h2 / h;
+  double S[4];
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+    double acc = c_p[0][p] * k[0][i];
+#pragma unroll
+    for (int j = 1; j < 7; ++j) acc += c_p[j][p] * k[j][i];
+    S[p] = acc;
+  }
+  out[i] = yl[i] + h * (x * S[0] + x * x * S[1] + x * x * x * S[2] + x * x * x * x * S[3]);
+}
+
+}  // namespace
+
+#define RDCU_TRY(x)                   \
+  do {                                \
+    cudaError_t _e = (x);             \
+    if (_e != cudaSuccess) return _e; \
+  } while (0)
+
+bool DP45Engine::init(SpectralPlan* sp, double atol, double rtol, int fixed, cudaStream_t st,
+                      std::string* msg) {
+  release();
+  sp_ = sp;
+  st_ = st;
+  nN_ = (long long)sp->n * sp->N;
+  atol_ = atol;
+  rtol_ = rtol;
+  fixed_ = fixed;
+  const size_t sb = (size_t)nN_ * sizeof(double);
+  auto fail = [&](const char* what) {
+    *msg = std::string("out of device memory (") + what + ")";
+    return false;
+  };
+  for (int i = 0; i < 3; ++i) {
+    if (cudaMalloc((void**)&bufs.ybuf[i], sb) != cudaSuccess) return fail("state buffers");
+    device_bytes += sb;
+  }
+  for (int i = 0; i < 7; ++i) {
+    if (cudaMalloc((void**)&bufs.kbuf[i], sb) != cudaSuccess) return fail("stage buffers");
+    device_bytes += sb;
+  }
+  if (cudaMalloc((void**)&y_eval, sb) != cudaSuccess) return fail("dense output");
+  device_bytes += sb;
+  const int np = std::max(1, sp->nparts_max);
+  if (cudaMalloc((void**)&err_part_, np * sizeof(double)) != cudaSuccess) return fail("error partials");
+  if (cudaMalloc((void**)&d_ctl_, sizeof(DP45Ctl)) != cudaSuccess) return fail("controller");
+  if (cudaMalloc((void**)&log_h_, log_cap_ * sizeof(double)) != cudaSuccess) return fail("log");
+  if (cudaMalloc((void**)&log_acc_, log_cap_ * sizeof(int)) != cudaSuccess) return fail("log");
+  if (cudaMalloc((void**)&log_t_, log_cap_ * sizeof(double)) != cudaSuccess) return fail("log");
+  if (cudaMallocHost((void**)&h_log_t_, log_cap_ * sizeof(double)) != cudaSuccess) return fail("pinned");
+  if (cudaMallocHost((void**)&h_ctl_pinned_, sizeof(DP45Ctl)) != cudaSuccess) return fail("pinned");
+  if (cudaMallocHost((void**)&h_log_h_, log_cap_ * sizeof(double)) != cudaSuccess) return fail("pinned");
+  if (cudaMallocHost((void**)&h_log_acc_, log_cap_ * sizeof(int)) != cudaSuccess) return fail("pinned");
+  teval_cap_ = 1;
+  if (cudaMalloc((void**)&d_teval_, sizeof(double)) != cudaSuccess) return fail("t_eval");
+  DP45Ctl c{};
+  c.atol = atol;
+  c.rtol = rtol;
+  c.fixed = fixed;
+  c.y_slot = 0;
+  c.yn_slot = 1;
+  c.yl_slot = 2;
+  c.k1_buf = 0;
+  c.k7_buf = 6;
+  c.last_k1_buf = 0;
+  c.last_k7_buf = 6;
+  c.log_cap = log_cap_;
+  c.nparts = sp->nparts_max;
+  c.hmax = INFINITY;
+  host_ctl = c;
+  if (cudaMemcpy(d_ctl_, &c, sizeof(c), cudaMemcpyHostToDevice) != cudaSuccess) return fail("controller");
+  return true;
+}
+
+void DP45Engine::release() {
+  if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+  if (graph_) cudaGraphDestroy(graph_);
+  graph_exec_ = nullptr;
+  graph_ = nullptr;
+  for (auto& p : bufs.ybuf) {
+    if (p) cudaFree(p);
+    p = nullptr;
+  }
+  for (auto& p : bufs.kbuf) {
+    if (p) cudaFree(p);
+    p = nullptr;
+  }
+  void* d[] = {y_eval, err_part_, d_ctl_, log_h_, log_acc_, log_t_, d_teval_};
+  for (void* p : d)
+    if (p) cudaFree(p);
+  void* hp[] = {h_ctl_pinned_, h_log_h_, h_log_acc_, h_log_t_};
+  for (void* p : hp)
+    if (p) cudaFreeHost(p);
+  y_eval = nullptr;
+  err_part_ = nullptr;
+  d_ctl_ = nullptr;
+  log_h_ = nullptr;
+  log_acc_ = nullptr;
+  log_t_ = nullptr;
+  h_log_t_ = nullptr;
+  d_teval_ = nullptr;
+  h_ctl_pinned_ = nullptr;
+  h_log_h_ = nullptr;
+  h_log_acc_ = nullptr;
+  device_bytes = 0;
+}
+
+cudaError_t DP45Engine::sync_ctl() {
+  RDCU_TRY(cudaMemcpyAsync(h_ctl_pinned_, d_ctl_, sizeof(DP45Ctl), cudaMemcpyDeviceToHost, st_));
+  RDCU_TRY(cudaStreamSynchronize(st_));
+  host_ctl = *h_ctl_pinned_;
+  return cudaSuccess;
+}
+
+cudaError_t DP45Engine::set_state(double t, double h, const double* y) {
+  RDCU_TRY(cudaStreamSynchronize(st_));
+  DP45Ctl c = host_ctl;
+  RDCU_TRY(sync_ctl());
+  c = host_ctl;
+  c.t = t;
+  c.h = h;
+  c.t_last = t;
+  c.y_slot = 0;
+  c.yn_slot = 1;
+  c.yl_slot = 2;
+  c.k1_buf = 0;
+  c.k7_buf = 6;
+  c.last_k1_buf = 0;
+  c.last_k7_buf = 6;
+  c.running = 0;
+  c.accepted = 0;
+  *h_ctl_pinned_ = c;
+  RDCU_TRY(cudaMemcpyAsync(d_ctl_, h_ctl_pinned_, sizeof(DP45Ctl), cudaMemcpyHostToDevice, st_));
+  if (y) RDCU_TRY(cudaMemcpyAsync(bufs.ybuf[0], y, (size_t)nN_ * sizeof(double), cudaMemcpyDefault, st_));
+  RDCU_TRY(cudaStreamSynchronize(st_));
+  host_ctl = c;
+  k1_valid_ = false;
+  have_step_ = false;
+  return cudaSuccess;
+}
+
+cudaError_t DP45Engine::get_state(double* t, double* h, double* y_dst, cudaMemcpyKind) {
+  RDCU_TRY(sync_ctl());
+  if (t) *t = host_ctl.t;
+  if (h) *h = host_ctl.h;
+  if (y_dst)
+    RDCU_TRY(cudaMemcpyAsync(y_dst, bufs.ybuf[host_ctl.y_slot], (size_t)nN_ * sizeof(double),
+                             cudaMemcpyDefault, st_));
+  return cudaStreamSynchronize(st_);
+}
+
+cudaError_t DP45Engine::arm(int check, double t1, double hmin, double hmax, int eval_i, int n_eval,
+                            int max_attempts) {
+  k_dp45_arm<<<1, 1, 0, st_>>>(d_ctl_, check, t1, hmin, hmax, eval_i, n_eval, max_attempts);
+  return cudaGetLastError();
+}
+
+cudaError_t DP45Engine::launch_k1() {
+  RhsIO io{};
+  io.mode = 1;
+  io.stage = 1;
+  io.bufs = bufs;
+  io.ctl = d_ctl_;
+  return sp_->run(io, st_);
+}
+
+cudaError_t DP45Engine::launch_attempt() {
+  for (int s = 2; s <= 7; ++s) {
+    RhsIO io{};
+    io.mode = 1;
+    io.stage = s;
+    io.bufs = bufs;
+    io.ctl = d_ctl_;
+    io.err_part = (s == 7 && !fixed_) ? err_part_ : nullptr;
+    RDCU_TRY(sp_->run(io, st_));
+  }
+  k_dp45_ctl<<<1, kCtlThreads, 0, st_>>>(d_ctl_, err_part_, log_h_, log_t_, log_acc_, (double)nN_,
+                                         d_teval_);
+  return cudaGetLastError();
+}
+
+cudaError_t DP45Engine::ensure_graph() {
+  if (graph_exec_ || !use_graph) return cudaSuccess;
+  cudaStream_t cap = st_;
+  RDCU_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = launch_attempt();
+  cudaGraph_t g = nullptr;
+  cudaError_t e2 = cudaStreamEndCapture(cap, &g);
+  if (e != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return e;
+  }
+  RDCU_TRY(e2);
+  graph_ = g;
+  RDCU_TRY(cudaGraphInstantiate(&graph_exec_, graph_, 0));
+  return cudaSuccess;
+}
+
+cudaError_t DP45Engine::step(double* t, double* h, double hmin, double hmax, int* accepted) {
+  RDCU_TRY(sync_ctl());
+  DP45Ctl c = host_ctl;
+  c.t = *t;
+  c.h = *h;
+  *h_ctl_pinned_ = c;
+  RDCU_TRY(cudaMemcpyAsync(d_ctl_, h_ctl_pinned_, sizeof(DP45Ctl), cudaMemcpyHostToDevice, st_));
+  RDCU_TRY(arm(0, INFINITY, hmin, hmax, 0, 0, 1));
+  if (!k1_valid_) {
+    RDCU_TRY(launch_k1());
+    k1_valid_ = true;
+  }
+  RDCU_TRY(launch_attempt());
+  RDCU_TRY(sync_ctl());
+  *t = host_ctl.t;
+  *h = host_ctl.h;
+  *accepted = host_ctl.accepted;
+  if (host_ctl.accepted) have_step_ = true;
+  return cudaSuccess;
+}
+
+cudaError_t DP45Engine::advance(int n, double hmin, double hmax, long long* accepted) {
+  RDCU_TRY(sync_ctl());
+  const long long acc0 = host_ctl.n_accepted;
+  // loop mode without outputs: the controller stops after n attempts (or at h <= hmin)
+  RDCU_TRY(arm(1, INFINITY, hmin, hmax, 0, 0, std::max(1, n)));
+  if (!k1_valid_) {
+    RDCU_TRY(launch_k1());
+    k1_valid_ = true;
+  }
+  RDCU_TRY(ensure_graph());
+  for (int k = 0; k < n; ++k) {
+    if (graph_exec_)
+      RDCU_TRY(cudaGraphLaunch(graph_exec_, st_));
+    else
+      RDCU_TRY(launch_attempt());
+  }
+  RDCU_TRY(sync_ctl());
+  *accepted = host_ctl.n_accepted - acc0;
+  if (host_ctl.accepted) have_step_ = true;
+  return cudaSuccess;
+}
+
+cudaError_t DP45Engine::eval(double t_eval, double* out) {
+  const unsigned blocks = (unsigned)((nN_ + 255) / 256);
+  k_dp45_interp<<<blocks, 256, 0, st_>>>(bufs, d_ctl_, t_eval, out, nN_);
+  RDCU_TRY(cudaGetLastError());
+  return cudaStreamSynchronize(st_);
+}
+
+cudaError_t DP45Engine::solve(double t1, double hmin, double hmax, const std::vector<double>& t_eval,
+                              const std::function<int(double, double, int, long long)>& on_attempt,
+                              const std::function<int(int, const double*)>& on_eval,
+                              const std::function<int(double, double, long long)>& on_checkpoint,
+                              int* cb_status) {
+  *cb_status = 0;
+  const int n_eval = (int)t_eval.size();
+  if (n_eval > teval_cap_) {
+    // the captured attempt graph holds the t_eval pointer: rebuild it
+    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+    if (graph_) cudaGraphDestroy(graph_);
+    graph_exec_ = nullptr;
+    graph_ = nullptr;
+    cudaFree(d_teval_);
+    d_teval_ = nullptr;
+    RDCU_TRY(cudaMalloc((void**)&d_teval_, (size_t)n_eval * sizeof(double)));
+    teval_cap_ = n_eval;
+  }
+  if (n_eval)
+    RDCU_TRY(cudaMemcpyAsync(d_teval_, t_eval.data(), (size_t)n_eval * sizeof(double),
+                             cudaMemcpyHostToDevice, st_));
+  RDCU_TRY(sync_ctl());
+  // dp45_run: FSAL k1 = f(y) before the loop (dp45.cu:157)
+  int eval_i = 0;
+  solve_attempts = 0;
+  solve_accepted = 0;
+  long long steps = 0;
+  RDCU_TRY(arm(1, t1, hmin, hmax, eval_i, n_eval, 1));
+  RDCU_TRY(launch_k1());
+  k1_valid_ = true;
+  RDCU_TRY(ensure_graph());
+  RDCU_TRY(sync_ctl());
+  int guard = 0;
+  while (host_ctl.t < t1 && host_ctl.h > hmin) {
+    // attempts until the next output time, estimated from the current h
+    const double t_next = eval_i < n_eval ? std::min(t_eval[eval_i], t1) : t1;
+    double est = (t_next - host_ctl.t) / host_ctl.h;
+    int K = (est > 0 && est < 1e6) ? (int)est + 2 : 64;
+    K = std::max(1, std::min(K, 256));
+    RDCU_TRY(arm(1, t1, hmin, hmax, eval_i, n_eval, K));
+    for (int k = 0; k < K; ++k) {
+      if (graph_exec_)
+        RDCU_TRY(cudaGraphLaunch(graph_exec_, st_));
+      else
+        RDCU_TRY(launch_attempt());
+    }
+    RDCU_TRY(sync_ctl());
+    const int nlog = std::min(host_ctl.log_count, host_ctl.log_cap);
+    if (nlog > 0) {
+      RDCU_TRY(cudaMemcpyAsync(h_log_h_, log_h_, nlog * sizeof(double), cudaMemcpyDeviceToHost, st_));
+      RDCU_TRY(cudaMemcpyAsync(h_log_acc_, log_acc_, nlog * sizeof(int), cudaMemcpyDeviceToHost, st_));
+      RDCU_TRY(cudaMemcpyAsync(h_log_t_, log_t_, nlog * sizeof(double), cudaMemcpyDeviceToHost, st_));
+      RDCU_TRY(cudaStreamSynchronize(st_));
+    }
+    for (int i = 0; i < nlog; ++i) {
+      if (h_log_acc_[i]) ++steps;
+      ++solve_attempts;
+      if (on_attempt) {
+        const int rc = on_attempt(h_log_t_[i], h_log_h_[i], h_log_acc_[i], steps);
+        if (rc) {
+          *cb_status = rc;
+          return cudaSuccess;
+        }
+      }
+    }
+    solve_accepted = steps;
+    if (host_ctl.stop_reason == kStopOutput) {
+      have_step_ = true;
+      bool any = false;
+      while (eval_i < n_eval && host_ctl.t >= t_eval[eval_i]) {
+        RDCU_TRY(eval(t_eval[eval_i], y_eval));
+        if (on_eval) {
+          const int rc = on_eval(eval_i, y_eval);
+          if (rc) {
+            *cb_status = rc;
+            return cudaSuccess;
+          }
+        }
+        ++eval_i;
+        any = true;
+      }
+      if (any && on_checkpoint) {
+        const int rc = on_checkpoint(host_ctl.t, host_ctl.h, steps);
+        if (rc) {
+          *cb_status = rc;
+          return cudaSuccess;
+        }
+      }
+    }
+    if (++guard > 100000000) return cudaErrorUnknown;
+  }
+  return cudaSuccess;
+}
+
+}  // namespace rdcu

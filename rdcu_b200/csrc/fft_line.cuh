@@ -1,0 +1,195 @@
+// Shared-memory FP64 Stockham FFT over a batch of complex lines (device code).
+//
+// Method: the Stockham autosort formulation (Van Loan, "Computational Frameworks for
+// the Fast Fourier Transform", SIAM 1992, ch. 1.7) with mixed radices 2, 3, 4, 5, 7, 8,
+// 11, 13.  Stage s with radix R and span Ns (product of earlier radices) maps butterfly
+// j of a line of length L (m = L/R butterflies) as
+//     in:  x[j + r*m] * w^(r * (j mod Ns) * L/(Ns*R)),   r < R
+//     out: y[(j/Ns)*Ns*R + (j mod Ns) + r*Ns]  = R-point DFT of the inputs,
+// which leaves the result in natural order.  Twiddles w^t = exp(-2 pi i t/L) come from
+// a table in shared memory.  Each stage stages its butterflies in registers, so one
+// buffer suffices (two barriers per stage).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "internal.h"
+
+namespace rdcu {
+
+__device__ __forceinline__ double2 c_mul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 c_add(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 c_sub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+// multiply by -i (forward) or +i (inverse)
+template <bool INV>
+__device__ __forceinline__ double2 c_rot(double2 a) {
+  return INV ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
+}
+
+template <bool INV>
+__device__ __forceinline__ double2 tw_get(const double2* tw, int t) {
+  double2 w = tw[t];
+  if (INV) w.y = -w.y;
+  return w;
+}
+
+// In-register R-point DFT of v (forward: exp(-2 pi i rk/R); inverse: conjugate).
+template <int R, bool INV>
+struct Dft {
+  __device__ __forceinline__ static void run(double2 (&v)[R], const double2* tw, int L) {
+    // generic small prime: O(R^2) with the line's twiddle table (R divides L)
+    double2 out[R];
+    const int step = L / R;
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      double2 acc = v[0];
+#pragma unroll
+      for (int r = 1; r < R; ++r) acc = c_add(acc, c_mul(v[r], tw_get<INV>(tw, ((r * k) % R) * step)));
+      out[k] = acc;
+    }
+#pragma unroll
+    for (int k = 0; k < R; ++k) v[k] = out[k];
+  }
+};
+
+template <bool INV>
+struct Dft<2, INV> {
+  __device__ __forceinline__ static void run(double2 (&v)[2], const double2*, int) {
+    double2 a = v[0], b = v[1];
+    v[0] = c_add(a, b);
+    v[1] = c_sub(a, b);
+  }
+};
+
+template <bool INV>
+struct Dft<4, INV> {
+  __device__ __forceinline__ static void run(double2 (&v)[4], const double2*, int) {
+    double2 t0 = c_add(v[0], v[2]), t1 = c_sub(v[0], v[2]);
+    double2 t2 = c_add(v[1], v[3]), t3 = c_rot<INV>(c_sub(v[1], v[3]));
+    v[0] = c_add(t0, t2);
+    v[2] = c_sub(t0, t2);
+    v[1] = c_add(t1, t3);
+    v[3] = c_sub(t1, t3);
+  }
+};
+
+template <bool INV>
+struct Dft<8, INV> {
+  __device__ __forceinline__ static void run(double2 (&v)[8], const double2*, int) {
+    // X[k] = E[k] + W^k O[k], X[k+4] = E[k] - W^k O[k]; E, O = 4-point DFTs of the
+    // even and odd inputs; W = exp(-+ 2 pi i / 8).
+    double2 e[4] = {v[0], v[2], v[4], v[6]};
+    double2 o[4] = {v[1], v[3], v[5], v[7]};
+    Dft<4, INV>::run(e, nullptr, 0);
+    Dft<4, INV>::run(o, nullptr, 0);
+    const double s = 0.70710678118654752440;  // sqrt(1/2)
+    // W^1 = s(1 -+ i), W^2 = -+ i, W^3 = s(-1 -+ i)
+    double2 w1o = INV ? make_double2(s * (o[1].x - o[1].y), s * (o[1].x + o[1].y))
+                      : make_double2(s * (o[1].x + o[1].y), s * (o[1].y - o[1].x));
+    double2 w2o = c_rot<INV>(o[2]);
+    double2 w3o = INV ? make_double2(-s * (o[3].x + o[3].y), s * (o[3].x - o[3].y))
+                      : make_double2(s * (o[3].y - o[3].x), -s * (o[3].x + o[3].y));
+    v[0] = c_add(e[0], o[0]);
+    v[4] = c_sub(e[0], o[0]);
+    v[1] = c_add(e[1], w1o);
+    v[5] = c_sub(e[1], w1o);
+    v[2] = c_add(e[2], w2o);
+    v[6] = c_sub(e[2], w2o);
+    v[3] = c_add(e[3], w3o);
+    v[7] = c_sub(e[3], w3o);
+  }
+};
+
+// Complex values a thread holds per stage (register budget of the staging), and the
+// largest block of an FFT pass (kMaxBlock x 128 registers fills the register file).
+constexpr int kStageElems = 8;
+constexpr int kMaxBlock = 512;
+
+// One Stockham stage over nlines lines (stride LS) held in shared memory `buf`.
+// Requires blockDim.x * QMAX >= nlines*L/R; the caller sizes the block for that.
+template <int R, bool INV>
+__device__ __forceinline__ void stockham_stage(double2* buf, int LS, int nlines, int L, int Ns,
+                                               const double2* tw) {
+  constexpr int QMAX = (R >= kStageElems) ? 1 : (kStageElems / R);
+  const int m = L / R;
+  const int nb = nlines * m;
+  const int T = blockDim.x;
+  const int tstride = L / (Ns * R);
+  double2 v[QMAX][R];
+  int dst[QMAX];
+#pragma unroll
+  for (int q = 0; q < QMAX; ++q) {
+    const int g = threadIdx.x + q * T;
+    dst[q] = -1;
+    if (g < nb) {
+      const int line = g / m;
+      const int j = g - line * m;
+      const double2* src = buf + line * LS;
+      const int kk = j % Ns;
+      const int tstep = kk * tstride;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        double2 x = src[j + r * m];
+        if (r > 0 && tstep != 0) x = c_mul(x, tw_get<INV>(tw, r * tstep));
+        v[q][r] = x;
+      }
+      Dft<R, INV>::run(v[q], tw, L);
+      dst[q] = line * LS + (j / Ns) * Ns * R + kk;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < QMAX; ++q) {
+    if (dst[q] >= 0) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) buf[dst[q] + r * Ns] = v[q][r];
+    }
+  }
+  __syncthreads();
+}
+
+// Radix sets a kernel is compiled for: power-of-two lengths use radices 8, 4, 2 only
+// (no register spills); any other supported length uses the general set.
+constexpr int kRadixPow2 = 0;
+constexpr int kRadixAll = 1;
+
+inline bool plan_is_pow2(const LinePlan& p) {
+  for (int s = 0; s < p.nstages; ++s)
+    if (p.radix[s] != 2 && p.radix[s] != 4 && p.radix[s] != 8) return false;
+  return true;
+}
+
+// Full transform of nlines lines.  All threads of the block must call it; the data
+// must be visible (a barrier before the call).  Returns after a barrier.
+template <int RS, bool INV>
+__device__ void fft_lines(double2* buf, int LS, int nlines, const LinePlan& p, const double2* tw) {
+  int Ns = 1;
+  for (int s = 0; s < p.nstages; ++s) {
+    const int R = p.radix[s];
+    if (RS == kRadixPow2) {
+      if (R == 8)
+        stockham_stage<8, INV>(buf, LS, nlines, p.L, Ns, tw);
+      else if (R == 4)
+        stockham_stage<4, INV>(buf, LS, nlines, p.L, Ns, tw);
+      else
+        stockham_stage<2, INV>(buf, LS, nlines, p.L, Ns, tw);
+    } else {
+      switch (R) {
+        case 2: stockham_stage<2, INV>(buf, LS, nlines, p.L, Ns, tw); break;
+        case 3: stockham_stage<3, INV>(buf, LS, nlines, p.L, Ns, tw); break;
+        case 4: stockham_stage<4, INV>(buf, LS, nlines, p.L, Ns, tw); break;
+        case 5: stockham_stage<5, INV>(buf, LS, nlines, p.L, Ns, tw); break;
+        case 7: stockham_stage<7, INV>(buf, LS, nlines, p.L, Ns, tw); break;
+        case 8: stockham_stage<8, INV>(buf, LS, nlines, p.L, Ns, tw); break;
+        case 11: stockham_stage<11, INV>(buf, LS, nlines, p.L, Ns, tw); break;
+        case 13: stockham_stage<13, INV>(buf, LS, nlines, p.L, Ns, tw); break;
+        default: break;  // plans only contain the radices above
+      }
+    }
+    Ns *= R;
+  }
+}
+
+
+}  // namespace rdcu

@@ -1,0 +1,105 @@
+// Internal types of librdcu (not part of the C ABI).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/rdcu.h"
+
+namespace rdcu {
+
+// ----------------------------------------------------------------------------- FFT plans
+constexpr int kMaxStages = 16;
+constexpr int kMaxLine = 4096;  // longest complex line one CTA transforms in shared memory
+
+// Mixed-radix Stockham plan for one complex line length.
+struct LinePlan {
+  int L;
+  int nstages;
+  int radix[kMaxStages];
+};
+
+bool make_line_plan(int L, LinePlan* p);
+// exp(-2 pi i t / L) for t < L, rounded from long double.
+void make_twiddles(int L, std::vector<double2>& tw);
+
+// ----------------------------------------------------------------------------- spectra
+// One entry of an inverse-transform channel: coef * Mpart(k) * U_src(k), where
+// Mpart is the real-part (part 0) or imaginary-part (part 1) multiplier of the
+// derivative operator on axes ax0 (and ax1) -- see spectral.cu.
+struct ChanEntry {
+  int src;   // source field
+  int nax;   // 0: identity, 1: d_ax0, 2: d_ax0 d_ax1
+  int ax0, ax1;
+  int part;  // 0: Re of the reference's complex Y block, 1: Im
+  int pad;
+  double coef;
+};
+
+struct ChanTable {
+  int nch;
+  const int* off;         // [nch+1] entry ranges
+  const ChanEntry* ent;
+  const double* kv;       // wavenumbers, axis a at kv + kv_off[a]
+  int kv_off[3];
+  int Ns[3];
+  int ndim;
+};
+
+// Dictionary terms left after folding the linear derivative terms into channels.
+struct DictTerm {
+  int field;
+  int nf;   // factors
+  int off;  // first factor
+  int pad;
+  double C;
+};
+struct DictFactor {
+  int q;    // quantity: < n physical field, else channel q-n
+  int eta;  // integer power (never 0: zero powers are dropped, pow(x,0) == 1)
+};
+struct DictTable {
+  int n;
+  int nterms;
+  const DictTerm* terms;      // grouped by field, reference order kept within a field
+  const DictFactor* fac;
+  const int* field_begin;     // [n+1]
+  const int* fold;            // [n] channel holding the folded linear part, -1 if none
+};
+
+// ----------------------------------------------------------------------------- DP45
+enum StopReason { kStopNone = 0, kStopDone = 1, kStopOutput = 2, kStopLog = 3, kStopChunk = 4 };
+
+// Device-resident DP45 controller state.  Kernels of one attempt read the buffer
+// slots from here, so a step sequence can run (and be captured in a CUDA graph)
+// without host round trips.
+struct DP45Ctl {
+  double t, h, hmin, hmax, t1;
+  double t_last;        // start of the last accepted step
+  double err_norm;      // last RMS error norm
+  double atol, rtol;
+  long long n_attempts, n_accepted;
+  int running;          // kernels of an attempt return at once when 0
+  int stop_reason;
+  int accepted;         // last attempt accepted
+  int fixed;
+  int check_t1;         // solve mode: stop at t >= t1 or h <= hmin
+  int y_slot, yn_slot, yl_slot;    // which ybuf is y, the stage state / y_new, y_last
+  int k1_buf, k7_buf;              // kbuf index of logical k1 and k7 (FSAL swap)
+  int last_k1_buf, last_k7_buf;    // mapping of the last accepted step (dense output)
+  int log_count, log_cap;
+  int eval_i, n_eval;
+  int max_attempts;     // per launch sequence
+  int attempts_this_launch;
+  int nparts;           // error partial sums written by the stage-7 epilogue
+  int pad;
+};
+
+struct DP45Bufs {
+  double* ybuf[3];
+  double* kbuf[7];
+};
+
+}  // namespace rdcu

@@ -1,0 +1,1059 @@
+// Fused pseudospectral RHS: f = sum_terms C prod_k Y_k^eta with Y from spectral
+// derivatives (reference rdcu.cu:78-106,117-184), as 3-5 shared-memory passes.
+//
+// Passes (d = ndim, last axis x contiguous, M = N_x, Mh = M/2+1):
+//   fwd_x : DP45 stage combination (y + h sum a_j k_j) fused with the real-to-complex
+//           FFT along x; two real rows per complex line, separated after the FFT.
+//   c2c   : complex FFT along a strided middle axis (3D only), in place.
+//   mid   : FFT along axis 0, the derivative multipliers that build each inverse
+//           channel, and the inverse FFT along axis 0 -- one kernel.
+//   c2c   : inverse along the middle axis (3D).
+//   inv_x : complex-to-real along x (two channels per complex line), then the
+//           dictionary at every grid point, written as the stage slope k_s; the
+//           stage-7 launch also forms the DP45 error estimate's partial sums.
+//
+// Channels.  Terms with a single derivative factor of power one are linear with
+// constant coefficients; per output field they are summed in spectral space into one
+// channel L_i (one inverse transform instead of one per derivative block).  Every
+// other derivative Y_k a term needs gets its own channel.  Physical fields come from
+// the stage state itself.
+//
+// Multipliers.  The reference keeps Re(IFFT(M_k FFT(u))) of a full complex transform,
+// with the wavenumber map k(na) = na*2pi/L for na < N/2 else (na-N)*2pi/L, the Nyquist
+// bin included (rdcu.cu:89-98).  With a real input, Re(IFFT(M U)) = IFFT(Mr U) where
+// Mr(k) = (M(k) + conj(M(-k)))/2 is Hermitian, so a real-to-complex transform with Mr
+// reproduces it exactly (zeroing first derivatives at their own Nyquist bin, and mixed
+// derivatives where exactly one index is at Nyquist).  The imaginary part of the
+// reference's block is IFFT(Mi U) with Mi(k) = (M(k) - conj(M(-k)))/(2i); Y.dat output
+// uses both.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "fft_line.cuh"
+#include "spectral.h"
+
+namespace rdcu {
+
+// Stage-combination coefficients a_{s,j} (dp45.cu:6-11; row s = stage 2..7) and
+// error coefficients e_j (dp45.cu:13).
+__constant__ double c_a[8][6] = {
+    {0, 0, 0, 0, 0, 0},
+    {0, 0, 0, 0, 0, 0},
+    {1.0 / 5, 0, 0, 0, 0, 0},
+    {3.0 / 40, 9.0 / 40, 0, 0, 0, 0},
+    {44.0 / 45, -56.0 / 15, 32.0 / 9, 0, 0, 0},
+    {19372.0 / 6561, -25360.0 / 2187, 64448.0 / 6561, -212.0 / 729, 0, 0},
+    {9017.0 / 3168, -355.0 / 33, 46732.0 / 5247, 49.0 / 176, -5103.0 / 18656, 0},
+    {35.0 / 384, 0, 500.0 / 1113, 125.0 / 192, -2187.0 / 6784, 11.0 / 84}};
+__constant__ double c_e[7] = {-71.0 / 57600, 0, 71.0 / 16695, -71.0 / 1920,
+                              17253.0 / 339200, -22.0 / 525, 1.0 / 40};
+
+namespace {
+
+struct Resolved {
+  const double* y = nullptr;   // stage input state
+  double* ytemp = nullptr;     // stage state written by fwd_x (nullptr: not written)
+  const double* u = nullptr;   // physical fields read by inv_x
+  double* f = nullptr;         // slope written by inv_x
+  const double* k[7] = {};
+  double h = 0, atol = 0, rtol = 0;
+  int stage = 0;
+};
+
+__device__ __forceinline__ Resolved resolve(const RhsIO& io) {
+  Resolved r;
+  if (io.mode == 0) {
+    r.y = io.y;
+    r.u = io.y;
+    r.f = io.f;
+    return r;
+  }
+  const DP45Ctl* c = io.ctl;
+  r.stage = io.stage;
+  r.h = c->h;
+  r.atol = c->atol;
+  r.rtol = c->rtol;
+  r.y = io.bufs.ybuf[c->y_slot];
+  r.k[0] = io.bufs.kbuf[c->k1_buf];
+  for (int j = 1; j < 6; ++j) r.k[j] = io.bufs.kbuf[j];
+  r.k[6] = io.bufs.kbuf[c->k7_buf];
+  if (io.stage <= 1) {
+    r.u = r.y;
+    r.f = io.bufs.kbuf[c->k1_buf];
+  } else {
+    r.ytemp = io.bufs.ybuf[c->yn_slot];
+    r.u = r.ytemp;
+    r.f = (io.stage == 7) ? io.bufs.kbuf[c->k7_buf] : io.bufs.kbuf[io.stage - 1];
+  }
+  return r;
+}
+
+// Stage state of DP45 stage s at element i, in the reference kernels' arithmetic order
+// (dp45.cu:34-69): stage 2 is y + h*a*k1, later stages y + h*(sum_j a_j k_j).  b_2 = 0
+// (dp45.cu:11), so stage 7 does not read k2.
+__device__ __forceinline__ double stage_value(int s, long long i, const Resolved& r) {
+  const double yi = r.y[i];
+  if (s == 2) return yi + r.h * c_a[2][0] * r.k[0][i];
+  double acc = c_a[s][0] * r.k[0][i];
+  if (s != 7) acc += c_a[s][1] * r.k[1][i];
+  for (int j = 2; j < s - 1; ++j) acc += c_a[s][j] * r.k[j][i];
+  return yi + r.h * acc;
+}
+
+__device__ __forceinline__ double ipow(double x, int e) {
+  if (e == 0) return 1.0;  // pow(x, 0) == 1 for every x
+  const int a = e < 0 ? -e : e;
+  double r = x;
+  for (int j = 1; j < a; ++j) r *= x;
+  return e < 0 ? 1.0 / r : r;
+}
+
+// Multiplier of one channel entry applied to u at the multi-index nidx.
+__device__ __forceinline__ double2 apply_entry(const ChanEntry& e, const int* nidx, const ChanTable& ct,
+                                               double2 u) {
+  double ap = 1.0, am = 1.0;
+  if (e.nax >= 1) {
+    const int a = e.ax0, na = nidx[a], nm = na == 0 ? 0 : ct.Ns[a] - na;
+    ap *= ct.kv[ct.kv_off[a] + na];
+    am *= ct.kv[ct.kv_off[a] + nm];
+  }
+  if (e.nax >= 2) {
+    const int a = e.ax1, na = nidx[a], nm = na == 0 ? 0 : ct.Ns[a] - na;
+    ap *= ct.kv[ct.kv_off[a] + na];
+    am *= ct.kv[ct.kv_off[a] + nm];
+  }
+  // M(k) = i^p alpha(k); Mr = i^p (alpha(k) + (-1)^p alpha(-k))/2,
+  // Mi = i^(p-1) (alpha(k) - (-1)^p alpha(-k))/2
+  const double sgn = (e.nax & 1) ? -1.0 : 1.0;
+  double beta;
+  int q;
+  if (e.part == 0) {
+    q = e.nax;
+    beta = 0.5 * (ap + sgn * am);
+  } else {
+    q = e.nax + 3;
+    beta = 0.5 * (ap - sgn * am);
+  }
+  beta *= e.coef;
+  const double2 r = make_double2(beta * u.x, beta * u.y);
+  switch (q & 3) {
+    case 0: return r;
+    case 1: return make_double2(-r.y, r.x);
+    case 2: return make_double2(-r.x, -r.y);
+    default: return make_double2(r.y, -r.x);
+  }
+}
+
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double red[32];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    for (int w = 0; w < nw; ++w) s += red[w];
+  }
+  return s;
+}
+
+// ------------------------------------------------------------------------- kernels
+struct FwdXArgs {
+  int M, Mh, nrows, P, do_fft, tw_smem;
+  LinePlan plan;
+  const double2* tw;
+  double2* S;
+  RhsIO io;
+};
+
+template <int RS>
+__global__ void __launch_bounds__(kMaxBlock, 1) k_fwd_x(FwdXArgs a) {
+  extern __shared__ double2 sm[];
+  if (a.io.mode == 1 && !a.io.ctl->running) return;
+  const Resolved r = resolve(a.io);
+  const int M = a.M, T = blockDim.x, tid = threadIdx.x;
+  const double2* tw = a.tw;
+  double2* buf = sm;
+  if (a.do_fft && a.tw_smem) {
+    double2* tws = sm;
+    for (int t = tid; t < M; t += T) tws[t] = a.tw[t];
+    tw = tws;
+    buf = sm + M;
+  }
+  const long long row0 = 2LL * blockIdx.x * a.P;
+  const int nel = a.P * 2 * M;
+  const int s = r.stage;
+  for (int e = tid; e < nel; e += T) {
+    const int pl = e / (2 * M);
+    const int w = e - pl * 2 * M;
+    const int half = w / M;
+    const int x = w - half * M;
+    const long long g = row0 + 2 * pl + half;
+    double v = 0.0;
+    if (g < a.nrows) {
+      const long long i = g * M + x;
+      v = (s >= 2) ? stage_value(s, i, r) : r.y[i];
+      if (r.ytemp) r.ytemp[i] = v;
+    }
+    if (a.do_fft) reinterpret_cast<double*>(buf)[2 * (pl * M + x) + half] = v;
+  }
+  if (!a.do_fft) return;
+  __syncthreads();
+  fft_lines<RS, false>(buf, M, a.P, a.plan, tw);
+  const int Mh = a.Mh;
+  const int nout = a.P * 2 * Mh;
+  for (int e = tid; e < nout; e += T) {
+    const int pl = e / (2 * Mh);
+    const int w = e - pl * 2 * Mh;
+    const int half = w / Mh;
+    const int kx = w - half * Mh;
+    const long long g = row0 + 2 * pl + half;
+    if (g >= a.nrows) continue;
+    const double2 z = buf[pl * M + kx];
+    const double2 zm = buf[pl * M + (kx == 0 ? 0 : M - kx)];
+    double2 o;
+    if (half == 0)
+      o = make_double2(0.5 * (z.x + zm.x), 0.5 * (z.y - zm.y));
+    else
+      o = make_double2(0.5 * (z.y + zm.y), -0.5 * (z.x - zm.x));
+    a.S[g * Mh + kx] = o;
+  }
+}
+
+struct C2CArgs {
+  int La, I, TW;
+  LinePlan plan;
+  const double2* tw;
+  double2* S;
+  RhsIO io;
+};
+
+template <int RS, bool INV>
+__global__ void __launch_bounds__(kMaxBlock, 1) k_c2c(C2CArgs a) {
+  extern __shared__ double2 sm[];
+  if (a.io.mode == 1 && !a.io.ctl->running) return;
+  const int La = a.La, TW = a.TW, LS = La + 1, T = blockDim.x, tid = threadIdx.x;
+  double2* tw = sm;
+  double2* buf = sm + La;
+  for (int t = tid; t < La; t += T) tw[t] = a.tw[t];
+  const long long i0 = (long long)blockIdx.x * TW;
+  double2* base = a.S + (long long)blockIdx.y * La * a.I;
+  const int nel = La * TW;
+  for (int e = tid; e < nel; e += T) {
+    const int c = e % TW, z = e / TW;
+    const long long ii = i0 + c;
+    buf[c * LS + z] = ii < a.I ? base[(long long)z * a.I + ii] : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  fft_lines<RS, INV>(buf, LS, TW, a.plan, tw);
+  for (int e = tid; e < nel; e += T) {
+    const int c = e % TW, z = e / TW;
+    const long long ii = i0 + c;
+    if (ii < a.I) base[(long long)z * a.I + ii] = buf[c * LS + z];
+  }
+}
+
+struct MidArgs {
+  int L0, I, TW, nsrc, G, GB, ch0;
+  int ndim, D1, Mh;
+  LinePlan plan;
+  const double2* tw;
+  const double2* Sf;
+  double2* Sc;
+  ChanTable chan;
+  RhsIO io;
+};
+
+template <int RS>
+__global__ void __launch_bounds__(kMaxBlock, 1) k_mid(MidArgs a) {
+  extern __shared__ double2 sm[];
+  if (a.io.mode == 1 && !a.io.ctl->running) return;
+  const int L0 = a.L0, TW = a.TW, LS = L0 + 1, T = blockDim.x, tid = threadIdx.x;
+  double2* tw = sm;
+  double2* fb = sm + L0;
+  double2* cb = fb + a.nsrc * TW * LS;
+  for (int t = tid; t < L0; t += T) tw[t] = a.tw[t];
+  const long long i0 = (long long)blockIdx.x * TW;
+  const int nload = a.nsrc * L0 * TW;
+  for (int e = tid; e < nload; e += T) {
+    const int c = e % TW;
+    const int z = (e / TW) % L0;
+    const int f = e / (TW * L0);
+    const long long ii = i0 + c;
+    fb[(f * TW + c) * LS + z] =
+        ii < a.I ? a.Sf[((long long)f * L0 + z) * a.I + ii] : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  fft_lines<RS, false>(fb, LS, a.nsrc * TW, a.plan, tw);
+  for (int g0 = 0; g0 < a.G; g0 += a.GB) {
+    const int gc = min(a.GB, a.G - g0);
+    const int ncomp = gc * L0 * TW;
+    for (int e = tid; e < ncomp; e += T) {
+      const int c = e % TW;
+      const int z = (e / TW) % L0;
+      const int ch = e / (TW * L0);
+      const long long ii = i0 + c;
+      double2 acc = make_double2(0.0, 0.0);
+      if (ii < a.I) {
+        int nidx[3];
+        nidx[0] = z;
+        if (a.ndim == 3) {
+          nidx[1] = (int)(ii / a.Mh);
+          nidx[2] = (int)(ii - (long long)nidx[1] * a.Mh);
+        } else {
+          nidx[1] = (int)ii;
+        }
+        const int gch = a.ch0 + g0 + ch;
+        for (int q = a.chan.off[gch]; q < a.chan.off[gch + 1]; ++q) {
+          const ChanEntry en = a.chan.ent[q];
+          const double2 u = fb[(en.src * TW + c) * LS + z];
+          const double2 v = apply_entry(en, nidx, a.chan, u);
+          acc.x += v.x;
+          acc.y += v.y;
+        }
+      }
+      cb[(ch * TW + c) * LS + z] = acc;
+    }
+    __syncthreads();
+    fft_lines<RS, true>(cb, LS, gc * TW, a.plan, tw);
+    for (int e = tid; e < ncomp; e += T) {
+      const int c = e % TW;
+      const int z = (e / TW) % L0;
+      const int ch = e / (TW * L0);
+      const long long ii = i0 + c;
+      if (ii < a.I) a.Sc[((long long)(g0 + ch) * L0 + z) * a.I + ii] = cb[(ch * TW + c) * LS + z];
+    }
+    __syncthreads();
+  }
+}
+
+struct Mult1DArgs {
+  int Mh, nch, ch0;
+  const double2* Sf;
+  double2* Sc;
+  ChanTable chan;
+  RhsIO io;
+};
+
+__global__ void k_mult1d(Mult1DArgs a) {
+  if (a.io.mode == 1 && !a.io.ctl->running) return;
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (long long)a.nch * a.Mh) return;
+  const int ch = (int)(e / a.Mh), kx = (int)(e - (long long)ch * a.Mh);
+  int nidx[3] = {kx, 0, 0};
+  double2 acc = make_double2(0.0, 0.0);
+  const int gch = a.ch0 + ch;
+  for (int q = a.chan.off[gch]; q < a.chan.off[gch + 1]; ++q) {
+    const ChanEntry en = a.chan.ent[q];
+    const double2 v = apply_entry(en, nidx, a.chan, a.Sf[(long long)en.src * a.Mh + kx]);
+    acc.x += v.x;
+    acc.y += v.y;
+  }
+  a.Sc[(long long)ch * a.Mh + kx] = acc;
+}
+
+struct InvXArgs {
+  int M, Mh, R, P, n, nch_run, npairs, do_fft, tw_smem;
+  long long N;
+  LinePlan plan;
+  const double2* tw;
+  const double2* Sc;
+  DictTable dict;
+  RhsIO io;
+  double* Yout;       // Y mode: channel c -> complex block ydst[c]>>1, part ydst[c]&1
+  const int* ydst;
+};
+
+template <int RS>
+__global__ void __launch_bounds__(kMaxBlock, 1) k_inv_x(InvXArgs a) {
+  extern __shared__ double2 sm[];
+  if (a.io.mode == 1 && !a.io.ctl->running) return;
+  const Resolved r = resolve(a.io);
+  const int M = a.M, Mh = a.Mh, T = blockDim.x, tid = threadIdx.x;
+  const int P = a.P, np = a.npairs, n = a.n;
+  const double2* tw = a.tw;
+  double2* lines = sm;
+  if (a.do_fft && a.tw_smem) {
+    double2* tws = sm;
+    for (int t = tid; t < M; t += T) tws[t] = a.tw[t];
+    tw = tws;
+    lines = sm + M;
+  }
+  double* phys = reinterpret_cast<double*>(lines + (a.do_fft ? P * np * M : 0));
+  const long long r0 = (long long)blockIdx.x * P;
+  if (a.do_fft) {
+    const int nel = P * np * M;
+    for (int e = tid; e < nel; e += T) {
+      const int pr = e / (np * M);
+      const int w = e - pr * np * M;
+      const int cp = w / M;
+      const int kx = w - cp * M;
+      const long long row = r0 + pr;
+      double2 z = make_double2(0.0, 0.0);
+      if (row < a.R) {
+        const int c0 = 2 * cp, c1 = c0 + 1;
+        const bool cj = kx >= Mh;
+        const int kk = cj ? M - kx : kx;
+        double2 A = a.Sc[((long long)c0 * a.R + row) * Mh + kk];
+        double2 B = c1 < a.nch_run ? a.Sc[((long long)c1 * a.R + row) * Mh + kk] : make_double2(0.0, 0.0);
+        if (kx == 0 || 2 * kx == M) {
+          A.y = 0.0;
+          B.y = 0.0;
+        }
+        if (cj) {
+          A.y = -A.y;
+          B.y = -B.y;
+        }
+        z = make_double2(A.x - B.y, A.y + B.x);
+      }
+      lines[(pr * np + cp) * M + kx] = z;
+    }
+  }
+  if (!a.Yout) {
+    const int nph = P * n * M;
+    for (int e = tid; e < nph; e += T) {
+      const int pr = e / (n * M);
+      const int w = e - pr * n * M;
+      const int fi = w / M;
+      const int x = w - fi * M;
+      const long long row = r0 + pr;
+      phys[(pr * n + fi) * M + x] = row < a.R ? r.u[((long long)fi * a.R + row) * M + x] : 0.0;
+    }
+  }
+  __syncthreads();
+  if (a.do_fft) fft_lines<RS, true>(lines, M, P * np, a.plan, tw);
+
+  if (a.Yout) {
+    const int nel = P * a.nch_run * M;
+    for (int e = tid; e < nel; e += T) {
+      const int pr = e / (a.nch_run * M);
+      const int w = e - pr * a.nch_run * M;
+      const int c = w / M;
+      const int x = w - c * M;
+      const long long row = r0 + pr;
+      if (row >= a.R) continue;
+      const double2 z = lines[(pr * np + (c >> 1)) * M + x];
+      const int d = a.ydst[c];
+      a.Yout[(((long long)(d >> 1)) * a.N + row * M + x) * 2 + (d & 1)] = (c & 1) ? z.y : z.x;
+    }
+    return;
+  }
+
+  const DictTable& D = a.dict;
+  // stage-7 epilogue of adaptive steps only (fixed steps pass no partials buffer)
+  const bool err = (a.io.mode == 1 && r.stage == 7 && a.io.err_part != nullptr);
+  double err2 = 0.0;
+  const int npts = P * M;
+  for (int e = tid; e < npts; e += T) {
+    const int pr = e / M;
+    const int x = e - pr * M;
+    const long long row = r0 + pr;
+    if (row >= a.R) continue;
+    const double* ph = phys + (long long)pr * n * M + x;
+    const double2* ln = lines + (long long)pr * np * M + x;
+    for (int i = 0; i < n; ++i) {
+      double acc = 0.0;
+      const int fc = D.fold[i];
+      if (fc >= 0) {
+        const double2 z = ln[(fc >> 1) * M];
+        acc = (fc & 1) ? z.y : z.x;
+      }
+      for (int t = D.field_begin[i]; t < D.field_begin[i + 1]; ++t) {
+        const DictTerm tm = D.terms[t];
+        double prod = 1.0;
+        for (int q = 0; q < tm.nf; ++q) {
+          const DictFactor fc2 = D.fac[tm.off + q];
+          double v;
+          if (fc2.q < n) {
+            v = ph[fc2.q * M];
+          } else {
+            const int c = fc2.q - n;
+            const double2 z = ln[(c >> 1) * M];
+            v = (c & 1) ? z.y : z.x;
+          }
+          prod *= ipow(v, fc2.eta);
+        }
+        acc += tm.C * prod;
+      }
+      const long long gi = ((long long)i * a.R + row) * M + x;
+      r.f[gi] = acc;
+      if (err) {
+        // error kernel of dp45.cu:79-84 (e_2 = 0 drops k2)
+        const double ynew = ph[i * M];
+        const double yold = r.y[gi];
+        const double es = c_e[0] * r.k[0][gi] + c_e[2] * r.k[2][gi] + c_e[3] * r.k[3][gi] +
+                          c_e[4] * r.k[4][gi] + c_e[5] * r.k[5][gi] + c_e[6] * acc;
+        const double ev = r.h * es / (r.atol + r.rtol * fmax(fabs(yold), fabs(ynew)));
+        err2 += ev * ev;
+      }
+    }
+  }
+  if (err) {
+    const double s = block_sum(err2);
+    if (tid == 0) a.io.err_part[blockIdx.x] = s;
+  }
+}
+
+inline int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+// at most kMaxElems complex values per FFT pass CTA: kMaxBlock threads x kStageElems
+constexpr int kMaxElems = kMaxBlock * kStageElems;
+
+int block_for(const LinePlan& p, int elems);
+int stage_threads(const LinePlan& p, int elems) {
+  // each thread stages at most QMAX*R values per stage (see stockham_stage)
+  int worst = kStageElems;
+  for (int s = 0; s < p.nstages; ++s) {
+    const int R = p.radix[s];
+    const int per = (R >= kStageElems) ? R : (kStageElems / R) * R;
+    worst = std::min(worst, per);
+  }
+  return (elems + worst - 1) / worst;
+}
+
+constexpr size_t kSmemBudget = 200 * 1024;
+constexpr int kTargetCtas = 2 * 148;
+
+}  // namespace
+
+#define RDCU_TRY(x)                        \
+  do {                                     \
+    cudaError_t _e = (x);                  \
+    if (_e != cudaSuccess) return _e;      \
+  } while (0)
+
+// Geometry of the inverse x pass for nch_run channels (with or without the
+// physical-field staging): rows per CTA, grid, block and dynamic shared memory.
+static void inv_geometry(int M, int R, int n, int nch_run, bool yout, const LinePlan& plan, PassCfg* c,
+                         int* tw_smem) {
+  const bool spectral = nch_run > 0;
+  const int np = (nch_run + 1) / 2;
+  const int npm = std::max(1, np);
+  int P = std::max(1, std::min(std::max(1, kMaxElems / 2 / (M * npm)), R / kTargetCtas));
+  auto bytes = [&](int p, bool tws) {
+    return (size_t)((spectral && tws ? M : 0) + (spectral ? p * np * M : 0)) * 16 + (yout ? 0 : (size_t)p * n * M * 8);
+  };
+  while (P > 1 && bytes(P, true) > kSmemBudget) P /= 2;
+  const bool tws = bytes(P, true) <= kSmemBudget;
+  c->per_cta = P;
+  c->grid = (R + P - 1) / P;
+  c->block = std::min(kMaxBlock, std::max(128, round_up(stage_threads(plan, P * npm * M), 32)));
+  c->smem = bytes(P, tws);
+  *tw_smem = tws ? 1 : 0;
+}
+
+// ----------------------------------------------------------------------------- plan
+ChanTable SpectralPlan::chan_table(const int* off, const ChanEntry* ent, int nchan) const {
+  ChanTable t{};
+  t.nch = nchan;
+  t.off = off;
+  t.ent = ent;
+  t.kv = kv_;
+  for (int a = 0; a < 3; ++a) {
+    t.kv_off[a] = kv_off_[a];
+    t.Ns[a] = Ns[a];
+  }
+  t.ndim = ndim;
+  return t;
+}
+
+DictTable SpectralPlan::dict_table() const {
+  DictTable d{};
+  d.n = n;
+  d.nterms = nterms_dict_;
+  d.terms = d_terms_;
+  d.fac = d_fac_;
+  d.field_begin = d_field_begin_;
+  d.fold = d_fold_;
+  return d;
+}
+
+template <typename T>
+static cudaError_t upload(T** dst, const std::vector<T>& v, size_t* bytes) {
+  const size_t b = std::max<size_t>(1, v.size()) * sizeof(T);
+  cudaError_t e = cudaMalloc((void**)dst, b);
+  if (e != cudaSuccess) return e;
+  *bytes += b;
+  if (!v.empty()) e = cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+  return e;
+}
+
+static ChanEntry entry_for(int k, int n, int ndim, int part, double coef) {
+  ChanEntry e{};
+  e.src = k % n;
+  const int Yind = k / n;
+  e.part = part;
+  e.coef = coef;
+  if (Yind == 0) {
+    e.nax = 0;
+  } else if (Yind <= ndim) {
+    e.nax = 1;
+    e.ax0 = Yind - 1;
+  } else {
+    const int t = Yind - ndim - 1;
+    e.nax = 2;
+    e.ax0 = t / ndim;
+    e.ax1 = t % ndim;
+  }
+  return e;
+}
+
+bool SpectralPlan::init(int n_, int ndim_, const int* Ns_, const double* Ls_,
+                        const std::vector<HostTerm>& terms, std::string* msg) {
+  release();
+  n = n_;
+  ndim = ndim_;
+  N = 1;
+  for (int a = 0; a < 3; ++a) {
+    Ns[a] = a < ndim ? Ns_[a] : 1;
+    Ls[a] = a < ndim ? Ls_[a] : 1.0;
+  }
+  for (int a = 0; a < ndim; ++a) N *= Ns[a];
+  M = Ns[ndim - 1];
+  Mh = M / 2 + 1;
+  R = (int)(N / M);
+  const int nY = 1 + ndim + ndim * ndim;
+  if (!make_line_plan(M, &plan_x_)) {
+    *msg = "grid size " + std::to_string(M) + " along the last axis is not supported (radices 2,3,5,7,11,13; at most 8192)";
+    return false;
+  }
+  for (int a = 0; a + 1 < ndim; ++a) {
+    if (!make_line_plan(Ns[a], &plan_ax_[a])) {
+      *msg = "grid size " + std::to_string(Ns[a]) + " along axis " + std::to_string(a) + " is not supported";
+      return false;
+    }
+  }
+
+  // ---- channels and dictionary (host)
+  const double invN = 1.0 / (double)N;
+  std::vector<std::vector<ChanEntry>> fold(n);
+  std::vector<int> needY;  // Y indices (>= n) needed physically
+  struct TermOut { int field; double C; std::vector<std::pair<int, int>> fac; };
+  std::vector<TermOut> kept;
+  for (const auto& t : terms) {
+    const int field = t.ints.empty() ? 0 : t.ints[0];
+    if (field < 0 || field >= n) {
+      *msg = "coupling term field " + std::to_string(field) + " out of range";
+      return false;
+    }
+    std::vector<std::pair<int, int>> fac;
+    const int np = (int)t.ints.size();
+    for (int j = 1; j < np; j += 2) {
+      const int k = t.ints[j];
+      const int p = (j + 1 < np) ? t.ints[j + 1] : 0;
+      if (k < 0 || k >= nY * n) {
+        *msg = "coupling term Y index " + std::to_string(k) + " out of range";
+        return false;
+      }
+      if (p != 0) fac.push_back({k, p});  // pow(x, 0) == 1 for every x
+    }
+    if (fac.size() == 1 && fac[0].second == 1 && fac[0].first >= n) {
+      fold[field].push_back(entry_for(fac[0].first, n, ndim, 0, t.C * invN));
+      continue;
+    }
+    for (auto& f : fac)
+      if (f.first >= n && std::find(needY.begin(), needY.end(), f.first) == needY.end()) needY.push_back(f.first);
+    kept.push_back({field, t.C, fac});
+  }
+  std::sort(needY.begin(), needY.end());
+  std::vector<int> ch_off{0};
+  std::vector<ChanEntry> ch_ent;
+  std::vector<int> fold_ch(n, -1);
+  nch = 0;
+  for (int i = 0; i < n; ++i) {
+    if (fold[i].empty()) continue;
+    fold_ch[i] = nch++;
+    for (auto& e : fold[i]) ch_ent.push_back(e);
+    ch_off.push_back((int)ch_ent.size());
+  }
+  std::vector<int> ych_of(nY * n, -1);
+  for (int k : needY) {
+    ych_of[k] = nch++;
+    ch_ent.push_back(entry_for(k, n, ndim, 0, invN));
+    ch_off.push_back((int)ch_ent.size());
+  }
+  std::vector<DictTerm> dterms;
+  std::vector<DictFactor> dfac;
+  std::vector<int> field_begin(n + 1, 0);
+  for (int i = 0; i < n; ++i) {
+    field_begin[i] = (int)dterms.size();
+    for (auto& t : kept) {
+      if (t.field != i) continue;
+      DictTerm dt{};
+      dt.field = i;
+      dt.C = t.C;
+      dt.off = (int)dfac.size();
+      dt.nf = (int)t.fac.size();
+      for (auto& f : t.fac) {
+        DictFactor df{};
+        df.q = f.first < n ? f.first : n + ych_of[f.first];
+        df.eta = f.second;
+        dfac.push_back(df);
+      }
+      dterms.push_back(dt);
+    }
+  }
+  field_begin[n] = (int)dterms.size();
+  nterms_dict_ = (int)dterms.size();
+
+  // Y-mode channels: every block k, real and imaginary part
+  std::vector<int> y_off{0};
+  std::vector<ChanEntry> y_ent;
+  std::vector<int> y_dst;
+  for (int k = 0; k < nY * n; ++k)
+    for (int part = 0; part < 2; ++part) {
+      y_ent.push_back(entry_for(k, n, ndim, part, invN));
+      y_off.push_back((int)y_ent.size());
+      y_dst.push_back(k * 2 + part);
+    }
+  ych_ = (int)y_dst.size();
+
+  // wavenumbers exactly as d1 forms them (rdcu.cu:89-95)
+  const double PI = 3.14159265358979323846;
+  std::vector<double> kv;
+  for (int a = 0; a < ndim; ++a) {
+    kv_off_[a] = (int)kv.size();
+    for (int na = 0; na < Ns[a]; ++na) {
+      const int m2 = (na < Ns[a] / 2) ? na * 2 : (na - Ns[a]) * 2;
+      kv.push_back(m2 * PI / Ls[a]);
+    }
+  }
+
+  // ---- device tables
+  device_bytes = 0;
+  std::vector<double2> tw;
+  bool ok = true;
+  auto chk = [&](cudaError_t e) {
+    if (e != cudaSuccess && ok) {
+      ok = false;
+      *msg = std::string("CUDA error in spectral plan: ") + cudaGetErrorString(e);
+    }
+  };
+  make_twiddles(M, tw);
+  chk(upload(&tw_x_, tw, &device_bytes));
+  for (int a = 0; a + 1 < ndim; ++a) {
+    make_twiddles(Ns[a], tw);
+    chk(upload(&tw_ax_[a], tw, &device_bytes));
+  }
+  chk(upload(&kv_, kv, &device_bytes));
+  chk(upload(&ch_off_, ch_off, &device_bytes));
+  chk(upload(&ch_ent_, ch_ent, &device_bytes));
+  chk(upload(&d_terms_, dterms, &device_bytes));
+  chk(upload(&d_fac_, dfac, &device_bytes));
+  chk(upload(&d_field_begin_, field_begin, &device_bytes));
+  chk(upload(&d_fold_, fold_ch, &device_bytes));
+  chk(upload(&ych_off_, y_off, &device_bytes));
+  chk(upload(&ych_ent_, y_ent, &device_bytes));
+  chk(upload(&ych_dst_, y_dst, &device_bytes));
+  if (!ok) return false;
+
+  // ---- launch configurations
+  const int nrows = n * R;
+  const int pairs = (nrows + 1) / 2;
+  {
+    int P = std::max(1, std::min(std::max(1, kMaxElems / 2 / M), pairs / kTargetCtas));
+    const bool tws = (size_t)(M + P * M) * 16 <= kSmemBudget;
+    fwd_.per_cta = P;
+    fwd_.grid = (pairs + P - 1) / P;
+    fwd_.block = std::min(kMaxBlock, std::max(128, round_up(stage_threads(plan_x_, P * M), 32)));
+    fwd_.smem = (size_t)((tws ? M : 0) + P * M) * 16;
+  }
+  {
+    int tws = 0;
+    inv_geometry(M, R, n, nch, false, plan_x_, &inv_, &tws);
+  }
+  nparts_max = inv_.grid;
+  // Y-mode channel group
+  const int GY = std::min(ych_, 8);
+  sc_rows_ = std::max(nch, 1);
+  if (ndim >= 2) {
+    const int L0 = Ns[0];
+    const int I = (ndim == 3) ? Ns[1] * Mh : Mh;
+    for (int which = 0; which < 2; ++which) {
+      const int G = which == 0 ? nch : GY;
+      if (G == 0) continue;
+      int TW = std::max(1, std::min(16, I / kTargetCtas));
+      int GB = std::min(G, 4);
+      while (TW > 1 && std::max(n, GB) * TW * L0 > kMaxElems) TW /= 2;
+      while (GB > 1 && std::max(n, GB) * TW * L0 > kMaxElems) --GB;
+      if (std::max(n, GB) * TW * L0 > kMaxElems) {
+        *msg = "too many fields for one axis-0 pass (n * N0 must be <= " + std::to_string(kMaxElems) + ")";
+        return false;
+      }
+      auto smem_of = [&](int tw_, int gb) { return (size_t)(L0 + (n + gb) * tw_ * (L0 + 1)) * 16; };
+      while (TW > 1 && smem_of(TW, GB) > kSmemBudget) TW /= 2;
+      while (GB > 1 && smem_of(TW, GB) > kSmemBudget) --GB;
+      if (smem_of(TW, GB) > 227 * 1024) {
+        *msg = "grid too large for the shared-memory axis-0 pass";
+        return false;
+      }
+      PassCfg& c = mid_[which];
+      c.grid = (I + TW - 1) / TW;
+      c.block = std::min(kMaxBlock, std::max(128, round_up(stage_threads(plan_ax_[0], std::max(n, GB) * TW * L0), 32)));
+      c.smem = smem_of(TW, GB);
+      c.per_cta = TW | (GB << 16);  // columns per CTA | channel lines held at once
+    }
+    if (ndim == 3) {
+      const int La = Ns[1], I1 = Mh;
+      int TW = std::min(16, I1);
+      while (TW > 1 && ((size_t)(La + TW * (La + 1)) * 16 > kSmemBudget || TW * La > kMaxElems)) TW /= 2;
+      c2c_f_.per_cta = TW;
+      c2c_f_.grid = (I1 + TW - 1) / TW;
+      c2c_f_.block = std::min(kMaxBlock, std::max(128, round_up(stage_threads(plan_ax_[1], TW * La), 32)));
+      c2c_f_.smem = (size_t)(La + TW * (La + 1)) * 16;
+      c2c_i_ = c2c_f_;
+    }
+  }
+  mult_.block = 256;
+
+  // ---- buffers
+  const size_t srow = (size_t)R * Mh * sizeof(double2);
+  cudaError_t e = cudaMalloc((void**)&Sf_, std::max<size_t>(1, (size_t)n * srow));
+  if (e != cudaSuccess) {
+    *msg = "out of device memory (spectral buffers)";
+    return false;
+  }
+  device_bytes += (size_t)n * srow;
+  e = cudaMalloc((void**)&Sc_, (size_t)sc_rows_ * srow);
+  if (e != cudaSuccess) {
+    *msg = "out of device memory (spectral buffers)";
+    return false;
+  }
+  device_bytes += (size_t)sc_rows_ * srow;
+
+  // opt in to large dynamic shared memory
+  const int maxsm = 227 * 1024;
+  cudaFuncSetAttribute(k_fwd_x<kRadixPow2>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+  cudaFuncSetAttribute(k_fwd_x<kRadixAll>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+  cudaFuncSetAttribute(k_inv_x<kRadixPow2>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+  cudaFuncSetAttribute(k_inv_x<kRadixAll>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+  cudaFuncSetAttribute(k_mid<kRadixPow2>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+  cudaFuncSetAttribute(k_mid<kRadixAll>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+  cudaFuncSetAttribute(k_c2c<kRadixPow2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+  cudaFuncSetAttribute(k_c2c<kRadixPow2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+  cudaFuncSetAttribute(k_c2c<kRadixAll, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+  cudaFuncSetAttribute(k_c2c<kRadixAll, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+  if (fwd_.smem > (size_t)maxsm || inv_.smem > (size_t)maxsm) {
+    *msg = "grid too large for the shared-memory x pass";
+    return false;
+  }
+  built_ = true;
+  return true;
+}
+
+cudaError_t SpectralPlan::ensure_channel_capacity(int rows) {
+  if (rows <= sc_rows_) return cudaSuccess;
+  const size_t srow = (size_t)R * Mh * sizeof(double2);
+  double2* p = nullptr;
+  RDCU_TRY(cudaMalloc((void**)&p, (size_t)rows * srow));
+  cudaFree(Sc_);
+  device_bytes += (size_t)(rows - sc_rows_) * srow;
+  Sc_ = p;
+  sc_rows_ = rows;
+  return cudaSuccess;
+}
+
+void SpectralPlan::release() {
+  void* ptrs[] = {tw_x_, tw_ax_[0], tw_ax_[1], tw_ax_[2], kv_, ch_off_, ch_ent_, d_terms_, d_fac_,
+                  d_field_begin_, d_fold_, ych_off_, ych_ent_, ych_dst_, Sf_, Sc_};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  tw_x_ = nullptr;
+  for (auto& t : tw_ax_) t = nullptr;
+  kv_ = nullptr;
+  ch_off_ = nullptr;
+  ch_ent_ = nullptr;
+  d_terms_ = nullptr;
+  d_fac_ = nullptr;
+  d_field_begin_ = nullptr;
+  d_fold_ = nullptr;
+  ych_off_ = nullptr;
+  ych_ent_ = nullptr;
+  ych_dst_ = nullptr;
+  Sf_ = nullptr;
+  Sc_ = nullptr;
+  built_ = false;
+}
+
+// Runs the passes for channels [g_first, g_first+nch_run) of table ct.  When Yout is
+// set the inverse x pass writes channels to Y.dat layout instead of the dictionary.
+cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, int nch_run, int g_first,
+                                        double* Yout, const int* ydst, cudaStream_t st) {
+  const bool spectral = nch_run > 0;
+  if (spectral && ndim >= 2) {
+    const int which = Yout ? 1 : 0;
+    const PassCfg& c = mid_[which];
+    MidArgs m{};
+    m.L0 = Ns[0];
+    m.I = (ndim == 3) ? Ns[1] * Mh : Mh;
+    m.TW = c.per_cta & 0xffff;
+    m.GB = c.per_cta >> 16;
+    m.nsrc = n;
+    m.G = nch_run;
+    m.ch0 = g_first;
+    m.ndim = ndim;
+    m.D1 = Ns[1];
+    m.Mh = Mh;
+    m.plan = plan_ax_[0];
+    m.tw = tw_ax_[0];
+    m.Sf = Sf_;
+    m.Sc = Sc_;
+    m.chan = ct;
+    m.io = io;
+    if (plan_is_pow2(plan_ax_[0]))
+      k_mid<kRadixPow2><<<c.grid, c.block, c.smem, st>>>(m);
+    else
+      k_mid<kRadixAll><<<c.grid, c.block, c.smem, st>>>(m);
+    RDCU_TRY(cudaGetLastError());
+    if (ndim == 3) {
+      C2CArgs a{};
+      a.La = Ns[1];
+      a.I = Mh;
+      a.TW = c2c_i_.per_cta;
+      a.plan = plan_ax_[1];
+      a.tw = tw_ax_[1];
+      a.S = Sc_;
+      a.io = io;
+      dim3 grid(c2c_i_.grid, nch_run * Ns[0]);
+      if (plan_is_pow2(plan_ax_[1]))
+        k_c2c<kRadixPow2, true><<<grid, c2c_i_.block, c2c_i_.smem, st>>>(a);
+      else
+        k_c2c<kRadixAll, true><<<grid, c2c_i_.block, c2c_i_.smem, st>>>(a);
+      RDCU_TRY(cudaGetLastError());
+    }
+  } else if (spectral) {
+    Mult1DArgs m{};
+    m.Mh = Mh;
+    m.nch = nch_run;
+    m.ch0 = g_first;
+    m.Sf = Sf_;
+    m.Sc = Sc_;
+    m.chan = ct;
+    m.io = io;
+    const long long tot = (long long)nch_run * Mh;
+    k_mult1d<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(m);
+    RDCU_TRY(cudaGetLastError());
+  }
+  InvXArgs a{};
+  a.M = M;
+  a.Mh = Mh;
+  a.R = R;
+  a.n = n;
+  a.nch_run = nch_run;
+  a.npairs = (nch_run + 1) / 2;
+  a.do_fft = spectral ? 1 : 0;
+  a.N = N;
+  a.plan = plan_x_;
+  a.tw = tw_x_;
+  a.Sc = Sc_;
+  a.dict = dict_table();
+  a.io = io;
+  a.Yout = Yout;
+  a.ydst = ydst;
+  // geometry for this channel count (the hot path's is the one the error partials
+  // buffer was sized for)
+  PassCfg g;
+  int tws = 0;
+  inv_geometry(M, R, n, nch_run, Yout != nullptr, plan_x_, &g, &tws);
+  a.P = g.per_cta;
+  a.tw_smem = tws;
+  const int grid = g.grid, block = g.block;
+  const size_t smem = g.smem;
+  if (plan_is_pow2(plan_x_))
+    k_inv_x<kRadixPow2><<<grid, block, smem, st>>>(a);
+  else
+    k_inv_x<kRadixAll><<<grid, block, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t SpectralPlan::run(const RhsIO& io, cudaStream_t st) {
+  const bool spectral = nch > 0;
+  const bool need_fwd = spectral || (io.mode == 1 && io.stage >= 2);
+  if (need_fwd) {
+    FwdXArgs a{};
+    a.M = M;
+    a.Mh = Mh;
+    a.nrows = n * R;
+    a.P = fwd_.per_cta;
+    a.do_fft = spectral ? 1 : 0;
+    a.tw_smem = fwd_.smem >= (size_t)(M + a.P * M) * 16 ? 1 : 0;
+    a.plan = plan_x_;
+    a.tw = tw_x_;
+    a.S = Sf_;
+    a.io = io;
+    const size_t smem = spectral ? fwd_.smem : 0;
+    if (plan_is_pow2(plan_x_))
+      k_fwd_x<kRadixPow2><<<fwd_.grid, fwd_.block, smem, st>>>(a);
+    else
+      k_fwd_x<kRadixAll><<<fwd_.grid, fwd_.block, smem, st>>>(a);
+    RDCU_TRY(cudaGetLastError());
+  }
+  if (spectral && ndim == 3) {
+    C2CArgs a{};
+    a.La = Ns[1];
+    a.I = Mh;
+    a.TW = c2c_f_.per_cta;
+    a.plan = plan_ax_[1];
+    a.tw = tw_ax_[1];
+    a.S = Sf_;
+    a.io = io;
+    dim3 grid(c2c_f_.grid, n * Ns[0]);
+    if (plan_is_pow2(plan_ax_[1]))
+      k_c2c<kRadixPow2, false><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(a);
+    else
+      k_c2c<kRadixAll, false><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(a);
+    RDCU_TRY(cudaGetLastError());
+  }
+  return launch_passes(io, chan_table(ch_off_, ch_ent_, nch), nch, 0, nullptr, nullptr, st);
+}
+
+cudaError_t SpectralPlan::run_Y(const double* y, double* Yout, cudaStream_t st) {
+  const int GY = std::min(ych_, 8);
+  RDCU_TRY(ensure_channel_capacity(GY));
+  RhsIO io{};
+  io.mode = 0;
+  io.y = y;
+  FwdXArgs a{};
+  a.M = M;
+  a.Mh = Mh;
+  a.nrows = n * R;
+  a.P = fwd_.per_cta;
+  a.do_fft = 1;
+  a.tw_smem = fwd_.smem >= (size_t)(M + a.P * M) * 16 ? 1 : 0;
+  a.plan = plan_x_;
+  a.tw = tw_x_;
+  a.S = Sf_;
+  a.io = io;
+  if (plan_is_pow2(plan_x_))
+    k_fwd_x<kRadixPow2><<<fwd_.grid, fwd_.block, fwd_.smem, st>>>(a);
+  else
+    k_fwd_x<kRadixAll><<<fwd_.grid, fwd_.block, fwd_.smem, st>>>(a);
+  RDCU_TRY(cudaGetLastError());
+  if (ndim == 3) {
+    C2CArgs c{};
+    c.La = Ns[1];
+    c.I = Mh;
+    c.TW = c2c_f_.per_cta;
+    c.plan = plan_ax_[1];
+    c.tw = tw_ax_[1];
+    c.S = Sf_;
+    c.io = io;
+    dim3 grid(c2c_f_.grid, n * Ns[0]);
+    if (plan_is_pow2(plan_ax_[1]))
+      k_c2c<kRadixPow2, false><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(c);
+    else
+      k_c2c<kRadixAll, false><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(c);
+    RDCU_TRY(cudaGetLastError());
+  }
+  const ChanTable ct = chan_table(ych_off_, ych_ent_, ych_);
+  for (int g = 0; g < ych_; g += GY) {
+    const int cnt = std::min(GY, ych_ - g);
+    RDCU_TRY(launch_passes(io, ct, cnt, g, Yout, ych_dst_ + g, st));
+  }
+  return cudaSuccess;
+}
+
+}  // namespace rdcu

@@ -1,0 +1,92 @@
+// Fused pseudospectral RHS of the dictionary: plan and launchers.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+namespace rdcu {
+
+// A coupling term as the reference stores it (rdcu.cu:606,654-660): coefficient and
+// the integer list (field, Yidx, pow, Yidx, pow, ...).
+struct HostTerm {
+  double C;
+  std::vector<int> ints;
+};
+
+// Where the inputs of one RHS evaluation come from and where f goes.
+struct RhsIO {
+  int mode = 0;               // 0: plain y -> f;  1: DP45 stage (buffers resolved on device)
+  int stage = 0;              // mode 1: 1 (k1 = f(y)) or 2..7
+  const double* y = nullptr;  // mode 0 input
+  double* f = nullptr;        // mode 0 output
+  DP45Bufs bufs{};            // mode 1
+  DP45Ctl* ctl = nullptr;     // mode 1
+  double* err_part = nullptr; // mode 1, stage 7: per-CTA partial sums of err^2
+};
+
+struct PassCfg {
+  int grid = 0, block = 0;
+  size_t smem = 0;
+  int per_cta = 0;  // pairs / rows / columns per CTA
+};
+
+class SpectralPlan {
+ public:
+  // Builds the plan; returns false with msg set when the problem is unsupported.
+  bool init(int n, int ndim, const int* Ns, const double* Ls, const std::vector<HostTerm>& terms,
+            std::string* msg);
+  void release();
+  ~SpectralPlan() { release(); }
+
+  // f = RHS(y) on `stream` (mode 0) or one DP45 stage (mode 1).
+  cudaError_t run(const RhsIO& io, cudaStream_t stream);
+  // All complex Y blocks (Y.dat layout) of y, written to Yout (device).
+  cudaError_t run_Y(const double* y, double* Yout, cudaStream_t stream);
+
+  int n = 0, ndim = 0, Ns[3] = {1, 1, 1};
+  double Ls[3] = {1, 1, 1};
+  long long N = 0;  // grid points
+  int M = 0, Mh = 0, R = 0;
+  int nch = 0;                // channels of the hot RHS
+  int nparts_max = 0;         // error partials buffer size needed (stage-7 epilogue)
+  size_t device_bytes = 0;
+
+ private:
+  bool built_ = false;
+  // line plans: x axis (length M) and the strided axes (0..ndim-2)
+  LinePlan plan_x_{}, plan_ax_[3]{};
+  double2* tw_x_ = nullptr;
+  double2* tw_ax_[3] = {nullptr, nullptr, nullptr};
+  double* kv_ = nullptr;
+  int kv_off_[3] = {0, 0, 0};
+  // hot-path channels and dictionary
+  int* ch_off_ = nullptr;
+  ChanEntry* ch_ent_ = nullptr;
+  DictTerm* d_terms_ = nullptr;
+  DictFactor* d_fac_ = nullptr;
+  int* d_field_begin_ = nullptr;
+  int* d_fold_ = nullptr;
+  int nterms_dict_ = 0;
+  // Y-mode channels (every block, real and imaginary part)
+  int ych_ = 0;
+  int* ych_off_ = nullptr;
+  ChanEntry* ych_ent_ = nullptr;
+  int* ych_dst_ = nullptr;
+  // spectral buffers
+  double2* Sf_ = nullptr;  // field half spectra [n][R][Mh]
+  double2* Sc_ = nullptr;  // channel half spectra [max(nch, G)][R][Mh]
+  int sc_rows_ = 0;        // channel capacity of Sc_
+  // launch configurations
+  PassCfg fwd_, inv_, mid_[2], c2c_f_, c2c_i_, mult_;
+
+  ChanTable chan_table(const int* off, const ChanEntry* ent, int nch) const;
+  DictTable dict_table() const;
+  cudaError_t launch_passes(const RhsIO& io, const ChanTable& ct, int nch_run, int g_first,
+                            double* Yout, const int* ydst, cudaStream_t stream);
+  cudaError_t ensure_channel_capacity(int rows);
+};
+
+}  // namespace rdcu

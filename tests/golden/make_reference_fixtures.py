@@ -1,0 +1,62 @@
+"""Runs the golden cases (cases.py) through the reference's own build and stores every
+output file as a compressed .npz fixture.
+
+    python tests/golden/make_reference_fixtures.py --ref oracle/_ref/rdcu_ref --out DIR
+
+Needs a GPU (the reference is CUDA-only).  The committed fixtures in tests/golden were
+made with this script from the reference sources built by oracle/build_ref.sh.
+"""
+import argparse
+import os
+import shlex
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))))
+from tests.golden.cases import CASES, case_ic  # noqa: E402
+
+FILES = {"states": np.float64, "times": np.float64, "steps": np.float64, "f": np.float64,
+         "Y": np.complex128, "rows": np.int32, "cols": np.int32, "vals": np.float64, "fs": np.uint8}
+
+
+def run_case(ref, case, workdir):
+    fb = os.path.join(workdir, case["name"])
+    with open(fb + "coupling.dat", "w") as fh:
+        fh.write("\n".join(case["coupling"]) + "\n")
+    ic = case_ic(case)
+    if ic is not None:
+        ic.tofile(fb + "ic.dat")
+    cmd = [ref] + shlex.split(case["args"]) + [fb]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+    out = {"argv": np.array(case["args"]), "returncode": np.array(r.returncode),
+           "stdout": np.array(r.stdout)}
+    for k, dt in FILES.items():
+        p = fb + k + ".dat"
+        if os.path.exists(p):
+            out[k] = np.fromfile(p, dt)
+    if os.path.exists(fb + ".out"):
+        out["out"] = np.array(open(fb + ".out").read())
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", required=True)
+    ap.add_argument("--out", required=True)
+    ap.add_argument("--only", default=None)
+    a = ap.parse_args()
+    os.makedirs(a.out, exist_ok=True)
+    with tempfile.TemporaryDirectory() as wd:
+        for case in CASES:
+            if a.only and a.only not in case["name"]:
+                continue
+            res = run_case(a.ref, case, wd)
+            np.savez_compressed(os.path.join(a.out, case["name"] + ".npz"), **res)
+            print(case["name"], "rc", int(res["returncode"]), sorted(k for k in res if k not in ("argv", "stdout")))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,51 @@
+"""Shared helpers for the parity tests (CPU side: problem generators, comparisons)."""
+from __future__ import annotations
+
+import numpy as np
+
+from oracle.problem import Problem, Term, parse_term
+
+
+def rel_err(a, b) -> float:
+    """max|a-b| / max|b| (max-norm relative difference)."""
+    a = np.asarray(a, np.float64).ravel()
+    b = np.asarray(b, np.float64).ravel()
+    den = float(np.max(np.abs(b))) if b.size else 0.0
+    return float(np.max(np.abs(a - b))) / max(den, 1e-300) if a.size else 0.0
+
+
+def random_terms(rng, n: int, ndim: int, nterms: int, max_factors: int = 3, deriv: bool = True,
+                 allow_zero_pow: bool = True) -> list:
+    """Random dictionary: coefficients N(0,1), factors over all Y indices (or fields only),
+    powers 0..3 (power 0 allowed), constant terms included."""
+    nY = 1 + ndim + ndim * ndim
+    out = []
+    for _ in range(nterms):
+        field = int(rng.integers(0, n))
+        nf = int(rng.integers(0, max_factors + 1))
+        ints = [field]
+        for _ in range(nf):
+            k = int(rng.integers(0, nY * n)) if deriv else int(rng.integers(0, n))
+            p = int(rng.integers(0 if allow_zero_pow else 1, 4))
+            ints += [k, p]
+        out.append(Term(float(rng.normal()), ints))
+    return out
+
+
+def smooth_field(rng, prob: Problem, amp: float = 1.0, modes: int = 3) -> np.ndarray:
+    """Sum of a few random low Fourier modes per field (plus an offset)."""
+    grids = np.meshgrid(*[np.arange(N) / N for N in prob.Ns], indexing="ij")
+    out = []
+    for _ in range(prob.n):
+        u = np.full(prob.Ns, float(rng.normal()))
+        for _ in range(modes):
+            k = [int(rng.integers(-2, 3)) for _ in prob.Ns]
+            ph = float(rng.uniform(0, 2 * np.pi))
+            arg = sum(2 * np.pi * kk * g for kk, g in zip(k, grids))
+            u = u + amp * float(rng.normal()) * np.cos(arg + ph)
+        out.append(u.ravel())
+    return np.concatenate(out)
+
+
+def spec_terms(prob: Problem):
+    return [(t.C, list(t.ints)) for t in prob.terms]

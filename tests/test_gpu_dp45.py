@@ -1,0 +1,139 @@
+"""GPU parity: DP45 stepping of librdcu against the oracle's restatement of dp45.cu.
+
+* fixed steps (-F): trajectories within 1e-10 relative (max-norm);
+* adaptive steps: identical accept/reject sequence and step sizes within 1e-9 relative
+  over short horizons (the CGLE is chaotic; short horizons keep rounding differences
+  from growing);
+* dense output, FSAL and the whole-integration event stream (rdcu_solve).
+"""
+import numpy as np
+import pytest
+
+from oracle import dp45 as odp
+from oracle import spectral as osp
+from oracle.problem import Problem, cgle_terms
+from tests.helpers import rel_err, spec_terms
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(torch, prob, y0, **kw):
+    import rdcu_b200 as R
+
+    s = R.Solver(prob.n, prob.Ns, prob.Ls, spec_terms(prob), **kw)
+    yd = torch.tensor(y0, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    return s, yd
+
+
+def _oracle(prob, y0, fixed, rtol=1e-8, atol=1e-8):
+    st = odp.DP45(y0, atol, rtol, fixed, lambda t, y: osp.rhs(y, prob))
+    st.k[0] = st.dydt(0.0, st.y)
+    return st
+
+
+def test_fixed_step_trajectory(cuda):
+    rng = np.random.default_rng(11)
+    prob = Problem(2, (32, 32), (40.0, 40.0), cgle_terms(2))
+    y0 = rng.uniform(-1, 1, 2 * prob.N)
+    s, yd = _setup(cuda, prob, y0, fixed=True)
+    h = 1e-2
+    s.set_state(0.0, h, yd.data_ptr())
+    o = _oracle(prob, y0, True)
+    t = to = 0.0
+    for _ in range(20):
+        acc, t, h2 = s.step(t, h)
+        ok, to, _ = o.step(to, h, 0.0, np.inf)
+        o.k[0] = o.k[6]
+        assert acc and ok
+    out = cuda.empty_like(yd)
+    tt, hh, _ = s.get_state(out.data_ptr())
+    assert abs(tt - to) < 1e-14
+    assert rel_err(out.cpu().numpy(), o.y) < 1e-10
+
+
+@pytest.mark.parametrize("Ns,Ls,rtol", [((32, 32), (40.0, 40.0), 1e-8), ((64,), (30.0,), 1e-6),
+                                        ((8, 8, 16), (12.0, 12.0, 20.0), 1e-7)])
+def test_adaptive_sequence(cuda, Ns, Ls, rtol):
+    rng = np.random.default_rng(len(Ns))
+    prob = Problem(2, Ns, Ls, cgle_terms(len(Ns)))
+    y0 = rng.uniform(-1, 1, 2 * prob.N)
+    s, yd = _setup(cuda, prob, y0, rtol=rtol, atol=rtol)
+    h = 1e-2
+    s.set_state(0.0, h, yd.data_ptr())
+    o = _oracle(prob, y0, False, rtol, rtol)
+    t = to = 0.0
+    hg = ho = h
+    for i in range(25):
+        acc, t, hg = s.step(t, hg)
+        ok, to, ho = o.step(to, ho, 0.0, np.inf)
+        if ok:
+            o.k[0] = o.k[6]
+        assert acc == ok, i
+        assert abs(hg - ho) <= 1e-9 * abs(ho), (i, hg, ho)
+        assert abs(t - to) <= 1e-12 * max(1.0, abs(to))
+    out = cuda.empty_like(yd)
+    s.get_state(out.data_ptr())
+    assert rel_err(out.cpu().numpy(), o.y) < 1e-9
+
+
+def test_dense_output(cuda):
+    rng = np.random.default_rng(21)
+    prob = Problem(2, (16, 16), (20.0, 20.0), cgle_terms(2))
+    y0 = rng.uniform(-1, 1, 2 * prob.N)
+    s, yd = _setup(cuda, prob, y0)
+    s.set_state(0.0, 0.05, yd.data_ptr())
+    o = _oracle(prob, y0, False)
+    acc, t, h = s.step(0.0, 0.05)
+    ok, to, ho = o.step(0.0, 0.05, 0.0, np.inf)
+    assert acc and ok
+    ye = cuda.empty_like(yd)
+    for frac in (0.0, 0.3, 0.77, 1.0):
+        te = t - (t - 0.0) * (1 - frac)
+        s.eval(te, ye.data_ptr())
+        assert rel_err(ye.cpu().numpy(), o.eval(to, te)) < 1e-10
+
+
+def test_solve_events_match_oracle_run(cuda):
+    """rdcu_solve's event stream against the reference driver loop (dp45_run + step_eval)."""
+    rng = np.random.default_rng(31)
+    prob = Problem(2, (16, 16), (20.0, 20.0), cgle_terms(2))
+    y0 = rng.uniform(-1, 1, 2 * prob.N)
+    s, yd = _setup(cuda, prob, y0, rtol=1e-6, atol=1e-6)
+    s.set_state(0.0, 0.01, yd.data_ptr())
+    t_eval = [0.1, 0.2, 0.3]
+    ev = {"h": [], "acc": [], "evals": [], "ckpt": []}
+
+    def cb(e):
+        if e.kind == 0:
+            ev["h"].append(e.h)
+            ev["acc"].append(e.accepted)
+        elif e.kind == 1:
+            ev["evals"].append((e.t_eval, s.copy_to_numpy(e.y, 2 * prob.N)))
+        else:
+            ev["ckpt"].append((e.t, e.h))
+        return 0
+
+    s.solve(0.3, t_eval, callback=cb)
+    o = odp.DP45(y0, 1e-6, 1e-6, False, lambda t, y: osp.rhs(y, prob))
+    oh, oacc, oev = [], [], []
+    ei = [0]
+
+    def se(t, h, y, ok):
+        oh.append(h)
+        oacc.append(ok)
+        if ok:
+            while ei[0] < len(t_eval) and t >= t_eval[ei[0]]:
+                oev.append((t_eval[ei[0]], o.eval(t, t_eval[ei[0]])))
+                ei[0] += 1
+
+    o.run(0.0, 0.01, 0.0, np.inf, 0.3, se)
+    assert ev["acc"] == [int(a) for a in oacc]
+    assert np.max(np.abs(np.array(ev["h"]) - np.array(oh)) / np.abs(oh)) < 1e-9
+    assert len(ev["evals"]) == len(oev) == 3
+    for (te, yg), (teo, yo) in zip(ev["evals"], oev):
+        assert te == teo
+        assert rel_err(yg, yo) < 1e-9
+    assert len(ev["ckpt"]) == 3
+    acc, att = s.counters()
+    assert acc == sum(oacc) and att == len(oacc)

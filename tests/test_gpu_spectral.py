@@ -1,0 +1,112 @@
+"""GPU parity: the fused pseudospectral RHS and Y blocks of librdcu against the oracle.
+
+Tolerance: 1e-12 relative in max-norm (the RHS criterion of the reference port's
+acceptance), on white-noise and smooth inputs, even and odd grids, 1-3 dimensions,
+random dictionaries with mixed derivatives, power-0 factors and constant terms.
+"""
+import numpy as np
+import pytest
+
+from oracle import spectral as osp
+from oracle.problem import Problem, cgle_terms, parse_term
+from tests.helpers import rel_err, random_terms, smooth_field, spec_terms
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+
+
+def _solver(prob, **kw):
+    import rdcu_b200 as R
+
+    return R.Solver(prob.n, prob.Ns, prob.Ls, spec_terms(prob), **kw)
+
+
+def gpu_rhs(torch, prob, y, want_Y=False):
+    s = _solver(prob)
+    yd = torch.tensor(y, dtype=torch.float64, device="cuda")
+    fd = torch.full_like(yd, float("nan"))
+    Yd = torch.full((prob.nY * prob.n * prob.N * 2,), float("nan"), dtype=torch.float64, device="cuda") \
+        if want_Y else None
+    torch.cuda.synchronize()
+    s.rhs(yd.data_ptr(), fd.data_ptr(), Yd.data_ptr() if want_Y else 0)
+    f = fd.cpu().numpy()
+    Y = Yd.cpu().numpy().view(np.complex128).reshape(prob.nY * prob.n, prob.N) if want_Y else None
+    s.close()
+    return f, Y
+
+
+@pytest.mark.parametrize("Ns,Ls", [((16, 16), (20.0, 20.0)), ((32, 16), (100.0, 50.0)),
+                                   ((64, 64), (100.0, 100.0))])
+def test_cgle_2d_white_noise(cuda, Ns, Ls):
+    rng = np.random.default_rng(1)
+    prob = Problem(2, Ns, Ls, cgle_terms(2))
+    y = rng.uniform(-1, 1, 2 * prob.N)
+    f, _ = gpu_rhs(cuda, prob, y)
+    fo = osp.rhs(y, prob)
+    assert rel_err(f, fo) < TOL
+
+
+@pytest.mark.parametrize("Ns", [(8,), (7,), (6,), (12,), (8, 6), (5, 7), (6, 5), (4, 4, 6), (6, 4, 5), (8, 8, 8),
+                                (3, 5, 4), (16, 12, 10)])
+def test_random_dictionary_shapes(cuda, Ns):
+    rng = np.random.default_rng(sum(Ns) * 7 + len(Ns))
+    ndim = len(Ns)
+    n = 2
+    Ls = tuple(float(rng.uniform(1, 10)) for _ in Ns)
+    prob = Problem(n, Ns, Ls, random_terms(rng, n, ndim, 12))
+    y = rng.uniform(-1, 1, n * prob.N)
+    f, Y = gpu_rhs(cuda, prob, y, want_Y=True)
+    fo, Yo = osp.rhs(y, prob, return_Y=True)
+    assert rel_err(f, fo) < TOL
+    # every block, real and imaginary parts (Y.dat)
+    for k in range(prob.nY * n):
+        scale = max(np.max(np.abs(Yo[k])), 1e-300)
+        assert np.max(np.abs(Y[k] - Yo[k])) / scale < TOL, k
+
+
+def test_cgle_3d(cuda):
+    rng = np.random.default_rng(3)
+    prob = Problem(2, (16, 8, 12), (30.0, 20.0, 25.0), cgle_terms(3))
+    y = rng.uniform(-1, 1, 2 * prob.N)
+    f, _ = gpu_rhs(cuda, prob, y)
+    assert rel_err(f, osp.rhs(y, prob)) < TOL
+
+
+def test_three_fields_mixed(cuda):
+    rng = np.random.default_rng(5)
+    n, Ns = 3, (12, 10)
+    terms = random_terms(rng, n, 2, 20, max_factors=4)
+    terms.append(parse_term("0.7,2"))      # constant term
+    terms.append(parse_term("1.5,1,4"))    # odd-length list: power read as 0
+    prob = Problem(n, Ns, (7.0, 9.0), terms)
+    y = smooth_field(rng, prob)
+    f, _ = gpu_rhs(cuda, prob, y)
+    assert rel_err(f, osp.rhs(y, prob)) < TOL
+
+
+def test_negative_powers(cuda):
+    rng = np.random.default_rng(9)
+    prob = Problem(2, (16, 8), (5.0, 3.0), [parse_term(s) for s in
+                                            ["1.0,0,0,-1", "0.5,1,1,-2,0,1", "1.0,0,6,1", "-0.3,1,2,1,0,-1"]])
+    y = rng.uniform(1.0, 2.0, 2 * prob.N)
+    f, _ = gpu_rhs(cuda, prob, y)
+    assert rel_err(f, osp.rhs(y, prob)) < TOL
+
+
+@pytest.mark.parametrize("Ns", [(128, 128), (256, 256), (32, 32, 32)])
+def test_plane_wave_laplacian_large(cuda, Ns):
+    """Size-independent check at full sizes: a plane wave is an eigenfunction of the
+    spectral Laplacian (exact up to rounding), so f = -|k|^2 u."""
+    ndim = len(Ns)
+    Ls = tuple(100.0 for _ in Ns)
+    n = 1
+    # u_aa indices: n + ndim*n + (a*ndim+a)*n
+    terms = [parse_term("1.0,0,%d,1" % (1 + ndim + a * ndim + a)) for a in range(ndim)]
+    prob = Problem(n, Ns, Ls, terms)
+    grids = np.meshgrid(*[np.arange(N) * (L / N) for N, L in zip(Ns, Ls)], indexing="ij")
+    ks = [2 * np.pi / L * m for L, m in zip(Ls, [3, 5, 2][:ndim])]
+    u = np.cos(sum(k * g for k, g in zip(ks, grids)) + 0.3)
+    f, _ = gpu_rhs(cuda, prob, u.ravel())
+    expect = -sum(k * k for k in ks) * u.ravel()
+    assert rel_err(f, expect) < 1e-11
