@@ -1,0 +1,382 @@
+"""Benchmark: grid-pt.steps/s of DP45 pseudospectral integration on one B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--workload NAME]
+
+Workload (default "cgle3d_256"): 3D complex Ginzburg-Landau as two FP64 fields on a
+256^3 periodic grid, L = 200^3, the 22-term coupling of the reference's 3D example
+(b = 2, c = 0.8), uniform random [-1, 1] initial condition from glibc rand() with seed 2,
+adaptive DP45 at rtol = atol = 1e-8, first step dt/100 with dt = 20 (the reference CLI
+run ``-n 2 -N 256,256,256 -L 200,200,200 -A 2 -s 2 -t T -d T``).  Synthetic data: there
+is no dataset; the IC is the reference's own generator.
+
+A bench step is TAU units of simulation time of that trajectory.  W warm-up steps
+integrate [0, W*TAU] untimed (the white-noise transient), then K steps [W*TAU,
+(W+K)*TAU] are timed; the metric counts accepted DP45 steps (rejected attempts are
+overhead), value = grid points x accepted steps / seconds.  Inputs are far larger than
+the 126 MB L2 (every stage moves ~0.27 GB arrays), so no L2 flush is needed.
+
+* ``value``: device-resident integration (rdcu_solve, controller on the device), timed
+  with CUDA events on the library's stream.
+* ``e2e``: the same window through the public C ABI with host buffers: rdcu_set_state
+  from a pinned host array, rdcu_solve with one output at the window's end copied to the
+  host, rdcu_get_state to the host; wall clock around the calls.
+* ``roofline``: the dominant pass kernel of one fused RHS stage (rdcu_profile_passes),
+  achieved = bytes the pass must move per launch / its CUDA-event time.
+* ``cpu_baseline``: the oracle's numpy/scipy restatement (scipy.fft, all host cores) on
+  one DP45 attempt of the same workload from the warm state.
+* ``--impl reference``: the reference's own nvcc sm_100a build (cuFFT/cuBLAS; the
+  reference has no CPU path) run twice, to W*TAU and to (W+K)*TAU; value = grid points
+  x (difference of accepted steps) / (difference of runtimes), so set-up and file output
+  cancel.
+
+Multi-GPU (torchrun, N > 1): replicas.  The problem does not shard; every rank
+integrates its own copy, timing is the max over ranks, value is the sum of all ranks'
+grid-pt.steps over that time ("scaling": "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import shlex
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "grid-pt·steps/s"
+TAU = 0.05  # simulation time per bench step
+
+WORKLOADS = {
+    "cgle3d_256": dict(Ns=(256, 256, 256), Ls=(200.0, 200.0, 200.0), seed=2, dt=20.0),
+    "cgle3d_128": dict(Ns=(128, 128, 128), Ls=(200.0, 200.0, 200.0), seed=2, dt=20.0),
+    "cgle2d_256": dict(Ns=(256, 256), Ls=(100.0, 100.0), seed=1, dt=1.0),
+    "cgle2d_128": dict(Ns=(128, 128), Ls=(100.0, 100.0), seed=1, dt=1.0),
+}
+
+
+def cgle_lines(ndim):
+    from oracle.problem import cgle_coupling_lines  # the coupling text the reference notebook writes
+
+    return cgle_coupling_lines(ndim)
+
+
+def parse_terms(lines):
+    out = []
+    for s in lines:
+        toks = [t for t in s.split(",") if t]
+        out.append((float(toks[0]), [int(t) for t in toks[1:]]))
+    return out
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            p = [x.strip() for x in l.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------- our arm
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    import rdcu_b200 as R
+
+    wl = WORKLOADS[args.workload]
+    Ns, Ls = wl["Ns"], wl["Ls"]
+    N = int(np.prod(Ns))
+    nN = 2 * N
+    torch.cuda.set_device(local_rank)
+    terms = parse_terms(cgle_lines(len(Ns)))
+    s = R.Solver(2, Ns, Ls, terms, rtol=1e-8, atol=1e-8, device=local_rank)
+    y0 = R.random_ic(2, N, 2.0, 0.0, wl["seed"])
+    h0 = wl["dt"] / 100
+    T_A, T_B = args.warmup * TAU, (args.warmup + args.steps) * TAU
+    s.set_state(0.0, h0, y0.ctypes.data)
+    # warm-up: integrate the transient [0, T_A] (device loop)
+    s.solve(T_A, [])
+    yA = np.empty(nN)
+    tA, hA, _ = s.get_state(yA.ctypes.data)
+    stream = torch.cuda.ExternalStream(s.stream, device=local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    # timed: [T_A, T_B] on the device
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        e0.record(stream)
+        s.solve(T_B, [])
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    acc, att = s.counters()
+    tB, hB, _ = s.get_state()
+    if dist:
+        dist.barrier()
+        t = torch.tensor([ms, float(acc) * N], dtype=torch.float64, device="cuda")
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = t.clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        ms_max, work = float(mx[0]), float(sm[1])
+    else:
+        ms_max, work = ms, float(acc) * N
+    value = work / (ms_max / 1e3)
+
+    # per-pass roofline of one fused RHS stage (device, CUDA events)
+    passes = s.profile_passes(reps=10)
+    peak, peak_kind = load_peaks()
+    top = max(passes, key=lambda p: p[1])
+    achieved = top[2] / (top[1] / 1e3) / 1e9
+    total_ms = sum(p[1] for p in passes)
+    # whole-step view: algorithmic bytes of one DP45 step (1040 N bytes for the 3D CGLE:
+    # 41 state-sized arrays + one spectral round trip per field per direction, 6 stages)
+    b_step = (1040.0 if len(Ns) == 3 else 656.0) * N
+    step_ms = ms / max(1, att)
+
+    # e2e through the public API with host buffers, same window from the saved state
+    s2 = s  # set_state resets the handle
+    pin = torch.empty(nN, dtype=torch.float64).pin_memory()
+    pin.numpy()[:] = yA
+    out_pin = torch.empty(nN, dtype=torch.float64).pin_memory()
+    last = torch.empty(nN, dtype=torch.float64).pin_memory()
+    if dist:
+        dist.barrier()
+
+    def cb(ev):
+        if ev.kind == R.EV_EVAL:
+            s2.memcpy(out_pin.data_ptr(), ev.y, nN * 8)
+        return 0
+
+    w0 = time.perf_counter()
+    s2.set_state(tA, hA, pin.data_ptr())
+    s2.solve(T_B, [T_B], callback=cb)
+    s2.get_state(last.data_ptr())
+    e2e_s = time.perf_counter() - w0
+    acc2, att2 = s2.counters()
+    if dist:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t[0])
+        wk = torch.tensor([float(acc2) * N], dtype=torch.float64, device="cuda")
+        dist.all_reduce(wk, op=dist.ReduceOp.SUM)
+        e2e_work = float(wk[0])
+    else:
+        e2e_work = float(acc2) * N
+    e2e_value = e2e_work / e2e_s
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(Ns, Ls, yA, tA, hA)
+    s.close()
+    line = {
+        "metric": METRIC, "value": value, "unit": "grid-pt·steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "grid": list(Ns), "L": list(Ls), "fields": 2,
+                   "dictionary": "CGLE b=2 c=0.8 (%d terms)" % len(terms), "method": "DP45 pseudospectral",
+                   "rtol": 1e-8, "atol": 1e-8, "ic": "glibc rand seed %d, [-1,1]" % wl["seed"],
+                   "window_sim_time": [T_A, T_B], "tau_per_step": TAU,
+                   "accepted_steps": acc, "attempts": att, "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "inputs > L2 (no flush needed)"},
+        "gpu_launches": launches_per_attempt(len(Ns)) * att * world,
+        "clocks": clk.summary(),
+        "e2e": {"value": e2e_value, "unit": "grid-pt·steps/s", "h2d_bytes_per_step": nN * 8 / args.steps,
+                "d2h_bytes_per_step": 2 * nN * 8 / args.steps, "accepted_steps": acc2, "seconds": e2e_s},
+        "roofline": {"bound": "hbm", "kernel": top[0], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_launch": top[2], "launch_ms": top[1],
+                     "passes": [{"name": p[0], "ms": p[1], "GBps": p[2] / (p[1] / 1e3) / 1e9,
+                                 "share": p[1] / total_ms} for p in passes],
+                     "step": {"algorithmic_bytes": b_step, "ms_per_attempt": step_ms,
+                              "achieved_GBps": b_step / (step_ms / 1e3) / 1e9,
+                              "frac": b_step / (step_ms / 1e3) / 1e9 / peak}},
+    }
+    if cpu:
+        line["cpu_baseline"] = cpu
+    return line
+
+
+def launches_per_attempt(ndim):
+    per_stage = {1: 3, 2: 3, 3: 5}[ndim]
+    return 6 * per_stage + 1
+
+
+def cpu_baseline(Ns, Ls, y, t, h):
+    """One DP45 attempt of the same workload on the host cores (oracle port)."""
+    from oracle import cpu_port
+
+    ncores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    acc = cpu_port.dp45_attempts(Ns, Ls, y, h, attempts=1, workers=ncores)
+    sec = time.perf_counter() - t0
+    N = int(np.prod(Ns))
+    return {"value": N * max(acc, 1) / sec, "unit": "grid-pt·steps/s", "cores": ncores, "kind": "port",
+            "sample": "1 DP45 attempt (6 RHS) of the %s CGLE from the state at the window start, "
+                      "numpy + scipy.fft with %d workers; %.1f s" % ("x".join(map(str, Ns)), ncores, sec)}
+
+
+# ----------------------------------------------------------------------------- reference arm
+def reference_binary():
+    p = os.path.join(ROOT, "oracle", "_ref", "rdcu_ref")
+    if os.path.exists(p):
+        return p, None
+    if os.path.exists("/root/reference/rdcu.cu"):
+        r = subprocess.run(["bash", os.path.join(ROOT, "oracle", "build_ref.sh")], capture_output=True, text=True)
+        if r.returncode == 0 and os.path.exists(p):
+            return p, None
+        return None, "reference build failed: " + r.stderr.strip().splitlines()[-1] if r.stderr else "build failed"
+    return None, "reference binary oracle/_ref/rdcu_ref not built and reference sources absent"
+
+
+def run_reference(args):
+    exe, why = reference_binary()
+    if exe is None:
+        return {"impl": "reference", "unavailable": why}
+    wl = WORKLOADS[args.workload]
+    Ns, Ls = wl["Ns"], wl["Ls"]
+    N = int(np.prod(Ns))
+    T_A, T_B = args.warmup * TAU, (args.warmup + args.steps) * TAU
+
+    def one(T):
+        with tempfile.TemporaryDirectory() as wd:
+            fb = os.path.join(wd, "bench")
+            open(fb + "coupling.dat", "w").write("\n".join(cgle_lines(len(Ns))) + "\n")
+            # -D1 (the reference writes times.dat unconditionally at outputs); one output
+            # at T; -d sets dt = 20 for the first step dt/100, the output time is T
+            cmd = [exe, "-n", "2", "-N", ",".join(map(str, Ns)), "-L", ",".join("%g" % l for l in Ls),
+                   "-A", "2", "-s", str(wl["seed"]), "-t", repr(T), "-d", "%r,%r" % (T, wl["dt"] / 100), "-D1", fb]
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=3600)
+            out = open(fb + ".out").read()
+            steps = int(re.search(r"steps: (\d+)", out).group(1))
+            runtime = float(re.search(r"runtime: ([0-9.]+)", out).group(1))
+            return steps, runtime, r.returncode, " ".join(shlex.quote(c) for c in cmd)
+
+    sA, rA, cA, cmdA = one(T_A)
+    sB, rB, cB, cmdB = one(T_B)
+    if cA != 0 or cB != 0:
+        return {"impl": "reference", "unavailable": "reference run failed (rc %d/%d)" % (cA, cB)}
+    value = N * (sB - sA) / (rB - rA)
+    sample = ("reference nvcc sm_100a build (cuFFT/cuBLAS), runs to t=%g (%d steps, %.2f s) and t=%g "
+              "(%d steps, %.2f s); difference = the window" % (T_A, sA, rA, T_B, sB, rB))
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "grid-pt·steps/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": (rB - rA) * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "grid": list(Ns), "L": list(Ls), "window_sim_time": [T_A, T_B],
+                   "accepted_steps": sB - sA, "command": cmdB},
+        "cpu_baseline": {"value": value, "unit": "grid-pt·steps/s", "cores": 1, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "grid-pt·steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference has no CPU implementation of the path; its own GPU build is the reference arm",
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=4)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="cgle3d_256", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        print(json.dumps(run_reference(args)), flush=True)
+        return 0
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    line = run_ours(args, rank, world, local_rank)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -159,6 +159,19 @@ int rdcu_solve(rdcu_t *h, double t1, double hmin, double hmax, const double *t_e
  * *accepted receives how many were accepted.  DP45 handles only. */
 int rdcu_advance(rdcu_t *h, int n_attempts, double hmin, double hmax, long long *accepted);
 
+/* Per-kernel timing of one fused RHS stage for roofline reporting: each pass kernel of
+ * DP45 stage 4 (forward x transform with the stage combination, strided transforms,
+ * axis-0 pass with the derivative multipliers, inverse x transform with the dictionary)
+ * is launched `reps` times between CUDA events on the handle's stream.  Fills up to
+ * max_passes entries with the pass name, its average time in ms and the bytes the pass
+ * must read and write per launch.  Leaves y and k1 untouched.  DP45 handles only. */
+typedef struct rdcu_pass_timing {
+  const char *name;
+  double ms;
+  double bytes;
+} rdcu_pass_timing;
+int rdcu_profile_passes(rdcu_t *h, int reps, rdcu_pass_timing *out, int max_passes, int *npass);
+
 /* Accepted steps and attempts counted by the last rdcu_solve. */
 int rdcu_get_counters(rdcu_t *h, long long *accepted, long long *attempts);
 

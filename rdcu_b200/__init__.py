@@ -42,7 +42,8 @@ EV_CHECKPOINT = 2
 EXPORTS = [
     "rdcu_create", "rdcu_destroy", "rdcu_set_state", "rdcu_get_state", "rdcu_get_info",
     "rdcu_rhs", "rdcu_jac", "rdcu_step", "rdcu_eval", "rdcu_solve", "rdcu_get_counters",
-    "rdcu_memcpy", "rdcu_advance", "rdcu_random_ic", "rdcu_error_string", "rdcu_last_error",
+    "rdcu_memcpy", "rdcu_advance", "rdcu_random_ic", "rdcu_profile_passes", "rdcu_error_string",
+    "rdcu_last_error",
 ]
 
 
@@ -79,6 +80,10 @@ class rdcu_event(ctypes.Structure):
     ]
 
 
+class rdcu_pass_timing(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char_p), ("ms", ctypes.c_double), ("bytes", ctypes.c_double)]
+
+
 OUT_CB = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(rdcu_event))
 
 _lib = None
@@ -109,6 +114,7 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
     lib.rdcu_memcpy.argtypes = [vp, vp, vp, ctypes.c_ulonglong]
     lib.rdcu_advance.argtypes = [vp, i, d, d, ctypes.POINTER(ctypes.c_longlong)]
     lib.rdcu_random_ic.argtypes = [pd, i, ctypes.c_longlong, d, d, i]
+    lib.rdcu_profile_passes.argtypes = [vp, i, ctypes.POINTER(rdcu_pass_timing), i, pi]
     lib.rdcu_error_string.argtypes = [i]
     lib.rdcu_error_string.restype = ctypes.c_char_p
     lib.rdcu_last_error.argtypes = [vp]
@@ -268,6 +274,13 @@ class Solver:
         acc = ctypes.c_longlong()
         self._check(self.lib.rdcu_advance(self.h, n_attempts, hmin, hmax, ctypes.byref(acc)))
         return acc.value
+
+    def profile_passes(self, reps: int = 20):
+        """[(name, ms per launch, bytes per launch)] for each pass of one fused RHS stage."""
+        arr = (rdcu_pass_timing * 16)()
+        npass = ctypes.c_int()
+        self._check(self.lib.rdcu_profile_passes(self.h, reps, arr, 16, ctypes.byref(npass)))
+        return [(arr[i].name.decode(), arr[i].ms, arr[i].bytes) for i in range(npass.value)]
 
     def counters(self):
         a, b = ctypes.c_longlong(), ctypes.c_longlong()

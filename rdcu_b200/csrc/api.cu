@@ -444,6 +444,22 @@ int rdcu_random_ic(double* y, int n, long long N, double A, double A0, int seed)
   return RDCU_OK;
 }
 
+int rdcu_profile_passes(rdcu_t* h, int reps, rdcu_pass_timing* out, int max_passes, int* npass) {
+  if (!h || !out || !npass || reps < 1) return set_err(h, RDCU_ERR_INVALID, "bad argument");
+  if (!h->dp) return set_err(h, RDCU_ERR_UNSUPPORTED, "pass profiling is implemented for DP45 handles");
+  if (int rc = activate(h)) return rc;
+  std::vector<SpectralPlan::PassTime> pt;
+  CHECK_CUDA(h, h->dp->profile(reps, &pt), "rdcu_profile_passes");
+  const int m = std::min((int)pt.size(), max_passes);
+  for (int i = 0; i < m; ++i) {
+    out[i].name = pt[i].name;
+    out[i].ms = pt[i].ms;
+    out[i].bytes = pt[i].bytes;
+  }
+  *npass = m;
+  return RDCU_OK;
+}
+
 int rdcu_get_counters(rdcu_t* h, long long* accepted, long long* attempts) {
   if (!h) return set_err(h, RDCU_ERR_INVALID, "null argument");
   if (accepted) *accepted = h->last_accepted;

@@ -1,26 +1,358 @@
-// Variable-order NDF/BDF integrator on the finite-difference RHS (in progress).
+// Variable-order NDF/BDF integrator (ode15s style) on the finite-difference RHS.
+//
+// The step logic restates bdf_step (reference bdf.cu:135-323) on the host, with every
+// vector operation a kernel here: predictor and error scale (step0/errscale,
+// bdf.cu:85-101), Newton right-hand side (rhs, bdf.cu:104-113), scaled RMS norms
+// (scale_err + cublasDnrm2, bdf.cu:127-132,166,238), the difference updates after an
+// accepted step (bdf.cu:262-271), the step-size rescaling of the differences (updateD,
+// bdf.cu:72-83, with makeRU bdf.cu:35-69) and dense output (interpolate,
+// bdf.cu:115-125).
+//
+// Linear solves.  The reference factorises A = I + alpha*J with cuDSS (LU, refactorised
+// whenever h or the order changes) and solves once per Newton iteration.  cuDSS is not
+// available here; A dd = b is solved by restarted GMRES with right preconditioning,
+// A applied as dd + alpha*(J dd) on the CSR Jacobian the FD kernels assemble.  The
+// preconditioner is the exact inverse of I + alpha*J_lin, J_lin the constant-
+// coefficient linear part of the dictionary (diffusion and linear reaction terms):
+// the reference's stencils are circulant, so the FFT diagonalises J_lin and each
+// Fourier mode is an n x n solve (spectral.cu k_mid_solve).  GMRES runs to a relative
+// residual of 1e-12, far below the Newton tolerance, so Newton and step decisions are
+// those of an exact solve.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "bdf.h"
+#include "spectral.h"
 
 namespace rdcu {
+namespace {
 
-struct BDFEngine::Impl {};
+// bdf.cu:8-9
+const double kKappa[6] = {0.0, -0.1850, -1.0 / 9, -0.0823, -0.0415, 0.0};
+const double kGamma[6] = {0.0, 1.0, 1.0 + 1.0 / 2, 1.0 + 1.0 / 2 + 1.0 / 3, 1.0 + 1.0 / 2 + 1.0 / 3 + 1.0 / 4,
+                          1.0 + 1.0 / 2 + 1.0 / 3 + 1.0 / 4 + 1.0 / 5};
+constexpr int kNwit = 4;  // bdf.cu:23
 
-bool BDFEngine::init(FDProblem* fd, double, double, int, cudaStream_t st, std::string* msg) {
+struct Small {
+  double v[36];
+};
+
+constexpr int kRedBlocks = 296;
+constexpr int kRedThreads = 256;
+
+__device__ __forceinline__ double block_reduce(double v) {
+  __shared__ double red[kRedThreads / 32];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < kRedThreads / 32; ++w) s += red[w];
+  __syncthreads();
+  return s;
+}
+
+// step0 + errscale (bdf.cu:93-101, 85-90)
+__global__ void k_predict(const double* D, long long nN, int order, double atl, double rtl, double* ytemp,
+                          double* yscale) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nN) return;
+  double y = D[i];
+  for (int j = 1; j <= order; ++j) y += D[nN * j + i];
+  ytemp[i] = y;
+  if (yscale) yscale[i] = atl + rtl * fabs(y);
+}
+
+__global__ void k_errscale(const double* y, long long nN, double atl, double rtl, double* yscale) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nN) yscale[i] = atl + rtl * fabs(y[i]);
+}
+
+// rhs kernel (bdf.cu:104-113): b = h/alpha f - sum_j D_j gamma_j/alpha - d
+__global__ void k_newton_rhs(double* b, const double* f, const double* d, const double* D, long long nN, int order,
+                             double h, double alpha, Small gam) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nN) return;
+  double v = h / alpha * f[i];
+  for (int j = 1; j <= order; ++j) v -= D[nN * j + i] * gam.v[j] / alpha;
+  v -= d[i];
+  b[i] = v;
+}
+
+// partial sums of (x/yscale)^2 (scale_err + Dnrm2)
+__global__ void k_wsq(const double* x, const double* yscale, long long nN, double* part) {
+  double s = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nN; i += (long long)gridDim.x * blockDim.x) {
+    const double v = x[i] / yscale[i];
+    s += v * v;
+  }
+  s = block_reduce(s);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// dots of w with V[0..nvec) (row blockIdx.y) and, in row nvec, w . w
+__global__ void k_dots(const double* V, int nvec, const double* w, long long nN, double* part) {
+  const int row = blockIdx.y;
+  const double* a = row < nvec ? V + (long long)row * nN : w;
+  double s = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nN; i += (long long)gridDim.x * blockDim.x)
+    s += a[i] * w[i];
+  s = block_reduce(s);
+  if (threadIdx.x == 0) part[(long long)row * gridDim.x + blockIdx.x] = s;
+}
+
+__global__ void k_sum_rows(const double* part, int nrow, int ncol, double* out) {
+  const int r = blockIdx.x;
+  if (r >= nrow) return;
+  double s = 0.0;
+  for (int c = threadIdx.x; c < ncol; c += blockDim.x) s += part[(long long)r * ncol + c];
+  s = block_reduce(s);
+  if (threadIdx.x == 0) out[r] = s;
+}
+
+// w -= sum_i h_i V_i   (h on the device)
+__global__ void k_vsub(const double* V, int nvec, const double* h, double* w, long long nN) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nN) return;
+  double acc = w[i];
+  for (int k = 0; k < nvec; ++k) acc -= h[k] * V[(long long)k * nN + i];
+  w[i] = acc;
+}
+
+// u = sum_i y_i V_i
+__global__ void k_vcomb(const double* V, int nvec, const double* y, double* u, long long nN) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nN) return;
+  double acc = 0.0;
+  for (int k = 0; k < nvec; ++k) acc += y[k] * V[(long long)k * nN + i];
+  u[i] = acc;
+}
+
+__global__ void k_scale(const double* x, double s, double* y, long long nN) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nN) y[i] = s * x[i];
+}
+
+__global__ void k_axpy(double a, const double* x, double* y, long long nN) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nN) y[i] += a * x[i];
+}
+
+// y = x + alpha * (J x): the action of A = I + alpha J (csrgeam2 of bdf.cu:153)
+__global__ void k_apply_A(const int* rows, const int* cols, const double* vals, double alpha, const double* x,
+                          double* y, long long nN) {
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nN) return;
+  double acc = 0.0;
+  for (int p = rows[r]; p < rows[r + 1]; ++p) acc += vals[p] * x[cols[p]];
+  y[r] = x[r] + alpha * acc;
+}
+
+// r = b - A x
+__global__ void k_residual(const int* rows, const int* cols, const double* vals, double alpha, const double* x,
+                           const double* b, double* r, long long nN) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nN) return;
+  double acc = 0.0;
+  for (int p = rows[i]; p < rows[i + 1]; ++p) acc += vals[p] * x[cols[p]];
+  r[i] = b[i] - (x[i] + alpha * acc);
+}
+
+// ytemp += dd; d += dd (the two Daxpy of bdf.cu:187-188)
+__global__ void k_newton_update(const double* dd, double* ytemp, double* d, long long nN) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nN) return;
+  ytemp[i] += dd[i];
+  d[i] += dd[i];
+}
+
+// updateD (bdf.cu:72-83) in place: Dnew[k] = sum_j RU[(order+1)*j+k] D[j]
+__global__ void k_updateD(double* D, long long nN, int order, Small RU) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nN) return;
+  double dj[6];
+  for (int j = 0; j <= order; ++j) dj[j] = D[nN * j + i];
+  for (int k = 0; k <= order; ++k) {
+    double val = 0;
+    for (int j = 0; j <= order; ++j) val += RU.v[(order + 1) * j + k] * dj[j];
+    D[nN * k + i] = val;
+  }
+}
+
+// accepted step (bdf.cu:262-271): D0 = ytemp; D[k+2] = d - D[k+1]; D[k+1] = d;
+// D[i] += D[i+1] for i = k..1
+__global__ void k_accept(double* D, const double* d, const double* ytemp, long long nN, int order) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nN) return;
+  double Dv[8];
+  for (int j = 0; j <= order + 1; ++j) Dv[j] = D[nN * j + i];
+  const double di = d[i];
+  Dv[0] = ytemp[i];
+  Dv[order + 2] = di - Dv[order + 1];
+  Dv[order + 1] = di;
+  for (int j = order; j >= 1; --j) Dv[j] = Dv[j] + Dv[j + 1];
+  for (int j = 0; j <= order + 2; ++j) D[nN * j + i] = Dv[j];
+}
+
+// interpolate (bdf.cu:115-125) with the factors computed on the host in the same order
+__global__ void k_interp(const double* D, long long nN, int order, Small fac, double* y) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nN) return;
+  double v = D[i];
+  for (int j = 1; j <= order; ++j) v += D[nN * j + i] * fac.v[j];
+  y[i] = v;
+}
+
+// makeRU (bdf.cu:35-69)
+void make_RU(int order, double factor, double* RU) {
+  double R[36], U[36];
+  double prod;
+  for (int i = 0; i <= order; i++)
+    for (int j = 0; j <= order; j++) {
+      prod = 1.0 / std::max(i, 1);
+      for (int k = 0; k < i; k++) prod *= (k - factor * j) / std::max(k, 1);
+      R[(order + 1) * i + j] = prod;
+    }
+  for (int i = 0; i <= order; i++)
+    for (int j = 0; j <= order; j++) {
+      prod = 1.0 / std::max(i, 1);
+      for (int k = 0; k < i; k++) prod *= (k - j) * 1.0 / std::max(k, 1);
+      U[(order + 1) * i + j] = prod;
+    }
+  for (int i = 0; i <= order; i++)
+    for (int j = 0; j <= order; j++) {
+      RU[(order + 1) * i + j] = 0;
+      for (int k = 0; k <= order; k++) RU[(order + 1) * i + j] += R[(order + 1) * i + k] * U[(order + 1) * k + j];
+    }
+}
+
+}  // namespace
+
+#define RDCU_TRY(x)                   \
+  do {                                \
+    cudaError_t _e = (x);             \
+    if (_e != cudaSuccess) return _e; \
+  } while (0)
+
+struct BDFEngine::Impl {
+  SpectralPlan prec;
+  bool have_prec = false;
+  long long nN = 0;
+  int blocks = 0;
+  double *ytemp = nullptr, *yscale = nullptr, *f = nullptr, *d = nullptr, *dd = nullptr, *b = nullptr;
+  double *y_eval = nullptr, *w = nullptr, *z = nullptr, *xacc = nullptr, *r = nullptr;
+  double* V = nullptr;
+  int m = 40;
+  double* part = nullptr;   // [(m+2)][kRedBlocks]
+  double* dots = nullptr;   // [m+2] device
+  double* hdots = nullptr;  // pinned
+  double* hvec = nullptr;   // device coefficients for k_vsub / k_vcomb
+  double* hvec_host = nullptr;  // pinned
+  int refactor = 1, rejac = 1;
+  double nconststeps = 0;
+  double ntol = 0;
+  double alpha = 0;  // alpha of the current "factorisation" (bdf.cu:152)
+  double atl = 0, rtl = 0;
+  int fixed = 0;
+  bool jac_ready = false;
+  bool started = false;  // bdf_run set-up done for the current state
+  double lin_tol = 1e-12;
+  int lin_max_iters = 400;
+};
+
+static std::vector<LinEntry> linear_part(const FDProblem& fd) {
+  std::vector<LinEntry> out;
+  const int n = fd.n, ndim = fd.ndim;
+  for (const auto& t : fd.terms) {
+    const int field = t.ints.empty() ? 0 : t.ints[0];
+    int cnt = 0, k = -1, p = 0;
+    const int np = (int)t.ints.size();
+    for (int j = 1; j < np; j += 2) {
+      const int pw = j + 1 < np ? t.ints[j + 1] : 0;
+      if (pw != 0) {
+        ++cnt;
+        k = t.ints[j];
+        p = pw;
+      }
+    }
+    if (cnt != 1 || p != 1) continue;
+    LinEntry e{};
+    e.row = field;
+    e.src = k % n;
+    const int yind = k / n;
+    if (yind == 0) {
+      e.nax = 0;
+    } else if (yind <= ndim) {
+      e.nax = 1;
+      e.ax0 = yind - 1;
+    } else {
+      const int q = yind - ndim - 1;
+      e.nax = 2;
+      e.ax0 = q / ndim;
+      e.ax1 = q % ndim;
+    }
+    e.coef = t.C;
+    out.push_back(e);
+  }
+  return out;
+}
+
+bool BDFEngine::init(FDProblem* fd, double atol, double rtol, int fixed, cudaStream_t st, std::string* msg) {
+  release();
   fd_ = fd;
   st_ = st;
-  const size_t b = (size_t)fd->nN * 8 * sizeof(double);
-  if (cudaMalloc((void**)&D_, b) != cudaSuccess) {
-    *msg = "out of device memory (BDF differences)";
+  impl_ = new Impl;
+  Impl& I = *impl_;
+  I.nN = fd->nN;
+  I.atl = atol;
+  I.rtl = rtol;
+  I.fixed = fixed;
+  // ntol (bdf.cu:395-401)
+  I.ntol = 0.03;
+  if (std::pow(rtol, 0.5) < 0.03) I.ntol = std::pow(rtol, 0.5);
+  if (10 * std::pow(2, -52) / rtol > I.ntol) I.ntol = 10 * std::pow(2, -52) / (rtol + std::pow(2, -52));
+  I.blocks = (int)((I.nN + 255) / 256);
+  const size_t sb = (size_t)I.nN * sizeof(double);
+  auto fail = [&](const char* what) {
+    *msg = std::string("out of device memory (") + what + ")";
     return false;
+  };
+  if (cudaMalloc((void**)&D_, sb * 8) != cudaSuccess) return fail("BDF differences");
+  double** vecs[] = {&I.ytemp, &I.yscale, &I.f, &I.d, &I.dd, &I.b, &I.y_eval, &I.w, &I.z, &I.xacc, &I.r};
+  for (double** p : vecs)
+    if (cudaMalloc((void**)p, sb) != cudaSuccess) return fail("BDF vectors");
+  if (cudaMalloc((void**)&I.V, sb * (I.m + 1)) != cudaSuccess) return fail("GMRES basis");
+  if (cudaMalloc((void**)&I.part, sizeof(double) * (I.m + 2) * kRedBlocks) != cudaSuccess) return fail("reductions");
+  if (cudaMalloc((void**)&I.dots, sizeof(double) * (I.m + 2)) != cudaSuccess) return fail("reductions");
+  if (cudaMalloc((void**)&I.hvec, sizeof(double) * (I.m + 2)) != cudaSuccess) return fail("reductions");
+  if (cudaMallocHost((void**)&I.hdots, sizeof(double) * (I.m + 2)) != cudaSuccess) return fail("pinned");
+  if (cudaMallocHost((void**)&I.hvec_host, sizeof(double) * (I.m + 2)) != cudaSuccess) return fail("pinned");
+  device_bytes = sb * (8 + 11 + I.m + 1) + fd->device_bytes;
+  std::vector<LinEntry> lin = linear_part(*fd);
+  if (!lin.empty() && fd->n <= kMaxPrecFields) {
+    std::string pm;
+    if (I.prec.init_precond(fd->n, fd->ndim, fd->Ns, fd->Ls, lin, &pm)) {
+      I.have_prec = true;
+      device_bytes += I.prec.device_bytes;
+    }
   }
-  device_bytes = b;
   return true;
 }
 
 void BDFEngine::release() {
+  if (impl_) {
+    Impl& I = *impl_;
+    double* vecs[] = {I.ytemp, I.yscale, I.f, I.d, I.dd, I.b, I.y_eval, I.w, I.z, I.xacc, I.r, I.V, I.part, I.dots, I.hvec};
+    for (double* p : vecs)
+      if (p) cudaFree(p);
+    if (I.hdots) cudaFreeHost(I.hdots);
+    if (I.hvec_host) cudaFreeHost(I.hvec_host);
+    delete impl_;
+    impl_ = nullptr;
+  }
   if (D_) cudaFree(D_);
   D_ = nullptr;
 }
@@ -30,10 +362,15 @@ cudaError_t BDFEngine::set_state(double t, double h, const double* y, int order,
   h_ = h;
   order_ = order;
   const size_t sb = (size_t)fd_->nN * sizeof(double);
-  cudaError_t e = cudaMemcpyAsync(D_, y, sb, cudaMemcpyDefault, st_);
-  if (e == cudaSuccess && order > 0 && D) e = cudaMemcpyAsync(D_ + fd_->nN, D, sb * order, cudaMemcpyDefault, st_);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
-  return e;
+  RDCU_TRY(cudaMemcpyAsync(D_, y, sb, cudaMemcpyDefault, st_));
+  if (order > 0 && D) RDCU_TRY(cudaMemcpyAsync(D_ + fd_->nN, D, sb * order, cudaMemcpyDefault, st_));
+  RDCU_TRY(cudaStreamSynchronize(st_));
+  impl_->refactor = 1;
+  impl_->rejac = 1;
+  impl_->nconststeps = 0;
+  impl_->started = false;
+  impl_->jac_ready = false;
+  return cudaSuccess;
 }
 
 cudaError_t BDFEngine::get_state(double* t, double* h, int* order, double* y, double* D) {
@@ -41,29 +378,360 @@ cudaError_t BDFEngine::get_state(double* t, double* h, int* order, double* y, do
   if (h) *h = h_;
   if (order) *order = order_;
   const size_t sb = (size_t)fd_->nN * sizeof(double);
-  cudaError_t e = cudaSuccess;
-  if (y) e = cudaMemcpyAsync(y, D_, sb, cudaMemcpyDefault, st_);
-  if (e == cudaSuccess && D && order_ > 0) e = cudaMemcpyAsync(D, D_ + fd_->nN, sb * order_, cudaMemcpyDefault, st_);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
-  return e;
+  if (y) RDCU_TRY(cudaMemcpyAsync(y, D_, sb, cudaMemcpyDefault, st_));
+  if (D && order_ > 0) RDCU_TRY(cudaMemcpyAsync(D, D_ + fd_->nN, sb * order_, cudaMemcpyDefault, st_));
+  return cudaStreamSynchronize(st_);
 }
 
-cudaError_t BDFEngine::step(double*, double*, double, double, int*, int* status) {
-  *status = RDCU_ERR_UNSUPPORTED;
-  last_msg = "BDF stepping not built";
+// ---------------------------------------------------------------- helpers (host)
+namespace {
+
+cudaError_t wnorm(BDFEngine::Impl& I, const double* x, cudaStream_t st, double* out) {
+  k_wsq<<<kRedBlocks, kRedThreads, 0, st>>>(x, I.yscale, I.nN, I.part);
+  k_sum_rows<<<1, kRedThreads, 0, st>>>(I.part, 1, kRedBlocks, I.dots);
+  RDCU_TRY(cudaMemcpyAsync(I.hdots, I.dots, sizeof(double), cudaMemcpyDeviceToHost, st));
+  RDCU_TRY(cudaStreamSynchronize(st));
+  *out = std::sqrt(I.hdots[0]);
+  return cudaGetLastError();
+}
+
+// dots[0..nvec) = V^T w, dots[nvec] = w.w  (host copy in I.hdots)
+cudaError_t vdots(BDFEngine::Impl& I, int nvec, const double* w, cudaStream_t st) {
+  dim3 grid(kRedBlocks, nvec + 1);
+  k_dots<<<grid, kRedThreads, 0, st>>>(I.V, nvec, w, I.nN, I.part);
+  k_sum_rows<<<nvec + 1, kRedThreads, 0, st>>>(I.part, nvec + 1, kRedBlocks, I.dots);
+  RDCU_TRY(cudaMemcpyAsync(I.hdots, I.dots, sizeof(double) * (nvec + 1), cudaMemcpyDeviceToHost, st));
+  RDCU_TRY(cudaStreamSynchronize(st));
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+// Solves (I + alpha J) x = b; x in I.dd.  Returns the number of GMRES iterations.
+static cudaError_t gmres(BDFEngine::Impl& I, const FDProblem& fd, double alpha, const double* b, double* x,
+                         cudaStream_t st, int* iters) {
+  const long long nN = I.nN;
+  const int nb = I.blocks;
+  const int m = I.m;
+  *iters = 0;
+  RDCU_TRY(vdots(I, 0, b, st));
+  const double beta0 = std::sqrt(I.hdots[0]);
+  RDCU_TRY(cudaMemsetAsync(x, 0, sizeof(double) * nN, st));
+  if (!(beta0 > 0)) return cudaStreamSynchronize(st);
+  const double tol = I.lin_tol * beta0;
+  std::vector<double> H((m + 1) * m), cs(m), sn(m), g(m + 1), y(m);
+  const double* r = b;
+  double beta = beta0;
+  int total = 0;
+  for (int restart = 0; restart < 50 && total < I.lin_max_iters; ++restart) {
+    if (restart > 0) {
+      k_residual<<<nb, 256, 0, st>>>(fd.rows_, fd.cols_, fd.vals_, alpha, x, b, I.r, nN);
+      RDCU_TRY(vdots(I, 0, I.r, st));
+      beta = std::sqrt(I.hdots[0]);
+      if (!(beta > tol)) break;
+      r = I.r;
+    }
+    k_scale<<<nb, 256, 0, st>>>(r, 1.0 / beta, I.V, nN);
+    std::fill(g.begin(), g.end(), 0.0);
+    g[0] = beta;
+    int jdone = 0;
+    bool conv = false;
+    for (int j = 0; j < m; ++j) {
+      const double* vj = I.V + (long long)j * nN;
+      const double* zin = vj;
+      if (I.have_prec) {
+        RDCU_TRY(I.prec.precond(vj, I.z, alpha, st));
+        zin = I.z;
+      }
+      k_apply_A<<<nb, 256, 0, st>>>(fd.rows_, fd.cols_, fd.vals_, alpha, zin, I.w, nN);
+      // classical Gram-Schmidt, twice
+      double hcol[64];
+      for (int pass = 0; pass < 2; ++pass) {
+        RDCU_TRY(vdots(I, j + 1, I.w, st));
+        for (int k = 0; k <= j; ++k) {
+          I.hvec_host[k] = I.hdots[k];
+          hcol[k] = (pass == 0 ? 0.0 : hcol[k]) + I.hdots[k];
+        }
+        RDCU_TRY(cudaMemcpyAsync(I.hvec, I.hvec_host, sizeof(double) * (j + 1), cudaMemcpyHostToDevice, st));
+        k_vsub<<<nb, 256, 0, st>>>(I.V, j + 1, I.hvec, I.w, nN);
+      }
+      RDCU_TRY(vdots(I, 0, I.w, st));
+      const double hn = std::sqrt(I.hdots[0]);
+      ++total;
+      // Givens rotations on column j
+      for (int k = 0; k < j; ++k) {
+        const double a = cs[k] * hcol[k] + sn[k] * hcol[k + 1];
+        hcol[k + 1] = -sn[k] * hcol[k] + cs[k] * hcol[k + 1];
+        hcol[k] = a;
+      }
+      const double den = std::sqrt(hcol[j] * hcol[j] + hn * hn);
+      cs[j] = den > 0 ? hcol[j] / den : 1.0;
+      sn[j] = den > 0 ? hn / den : 0.0;
+      hcol[j] = den;
+      g[j + 1] = -sn[j] * g[j];
+      g[j] = cs[j] * g[j];
+      for (int k = 0; k <= j; ++k) H[k * m + j] = hcol[k];
+      jdone = j + 1;
+      if (std::fabs(g[j + 1]) <= tol || !(hn > 0) || total >= I.lin_max_iters) {
+        conv = std::fabs(g[j + 1]) <= tol || !(hn > 0);
+        break;
+      }
+      k_scale<<<nb, 256, 0, st>>>(I.w, 1.0 / hn, I.V + (long long)(j + 1) * nN, nN);
+    }
+    // back substitution, then x += P^-1 (V y)
+    for (int k = jdone - 1; k >= 0; --k) {
+      double acc = g[k];
+      for (int q = k + 1; q < jdone; ++q) acc -= H[k * m + q] * y[q];
+      y[k] = H[k * m + k] != 0 ? acc / H[k * m + k] : 0.0;
+    }
+    for (int k = 0; k < jdone; ++k) I.hvec_host[k] = y[k];
+    RDCU_TRY(cudaMemcpyAsync(I.hvec, I.hvec_host, sizeof(double) * jdone, cudaMemcpyHostToDevice, st));
+    k_vcomb<<<nb, 256, 0, st>>>(I.V, jdone, I.hvec, I.w, nN);
+    if (I.have_prec) {
+      RDCU_TRY(I.prec.precond(I.w, I.z, alpha, st));
+      k_axpy<<<nb, 256, 0, st>>>(1.0, I.z, x, nN);
+    } else {
+      k_axpy<<<nb, 256, 0, st>>>(1.0, I.w, x, nN);
+    }
+    RDCU_TRY(cudaGetLastError());
+    if (conv) break;
+  }
+  *iters = total;
+  return cudaGetLastError();
+}
+
+// bdf_run set-up (bdf.cu:333-374): f and J at D_0; order 0 -> D_1 = h f
+static cudaError_t bdf_setup(BDFEngine::Impl& I, FDProblem& fd, double* D, int* order, double h,
+                             cudaStream_t st) {
+  RDCU_TRY(fd.rhs(D, I.f, nullptr));
+  RDCU_TRY(fd.jac_values(D));
+  I.jac_ready = true;
+  if (*order == 0) {
+    k_scale<<<I.blocks, 256, 0, st>>>(I.f, h, D + I.nN, I.nN);
+    RDCU_TRY(cudaGetLastError());
+    *order = 1;
+  }
+  I.started = true;
   return cudaSuccess;
 }
 
-cudaError_t BDFEngine::eval(double, double*) { return cudaErrorNotSupported; }
-
-cudaError_t BDFEngine::solve(double t1, double hmin, double, const std::vector<double>&,
-                             const std::function<int(double, double, int, long long)>&,
-                             const std::function<int(int, const double*)>&,
-                             const std::function<int(double, double, long long)>&, int*, int* status) {
+cudaError_t BDFEngine::step(double* t, double* h, double hmin, double hmax, int* accepted, int* status) {
   *status = RDCU_OK;
-  if (!(t_ < t1 && h_ > hmin)) return cudaSuccess;
-  *status = RDCU_ERR_UNSUPPORTED;
-  last_msg = "BDF stepping not built";
+  Impl& I = *impl_;
+  if (!I.started) {
+    RDCU_TRY(bdf_setup(I, *fd_, D_, &order_, *h, st_));
+  }
+  t_ = *t;
+  h_ = *h;
+  const long long nN = I.nN;
+  const int nb = I.blocks;
+  const double sqN = std::pow((double)nN, 0.5);
+  int order = order_;
+  int converged = 0, it = 0;
+  double dnorm = 0, dnormold = 0, rate = 0, factor = 1.0;
+  const double h0 = h_;
+  double hh = h_, tt = t_;
+  k_predict<<<nb, 256, 0, st_>>>(D_, nN, order, I.atl, I.rtl, I.ytemp, I.yscale);
+  RDCU_TRY(cudaMemsetAsync(I.d, 0, sizeof(double) * nN, st_));
+  Small gam{};
+  for (int j = 0; j < 6; ++j) gam.v[j] = kGamma[j];
+  for (it = 0; it < kNwit; it++) {
+    RDCU_TRY(fd_->rhs(I.ytemp, I.f, nullptr));
+    if (I.refactor) {
+      I.alpha = -hh / ((1 - kKappa[order]) * kGamma[order]);
+      I.refactor = 0;
+    }
+    k_newton_rhs<<<nb, 256, 0, st_>>>(I.b, I.f, I.d, D_, nN, order, hh, (1 - kKappa[order]) * kGamma[order], gam);
+    int iters = 0;
+    RDCU_TRY(gmres(I, *fd_, I.alpha, I.b, I.dd, st_, &iters));
+    lin_iters += iters;
+    ++lin_solves;
+    RDCU_TRY(wnorm(I, I.dd, st_, &dnorm));
+    dnorm /= sqN;
+    if (dnormold > 0) rate = dnorm / dnormold;
+    if (rate >= 1) break;
+    if (std::pow(rate, kNwit - it) / (1 - rate) * dnorm > I.ntol) break;
+    if (dnormold > 0 && rate / (1 - rate) * dnorm < I.ntol) {
+      converged = 1;
+      break;
+    }
+    k_newton_update<<<nb, 256, 0, st_>>>(I.dd, I.ytemp, I.d, nN);
+    dnormold = dnorm;
+  }
+  *accepted = 0;
+  if (!converged) {
+    if (I.rejac) {
+      k_predict<<<nb, 256, 0, st_>>>(D_, nN, order, I.atl, I.rtl, I.ytemp, nullptr);
+      RDCU_TRY(fd_->jac_values(I.ytemp));
+      I.refactor = 1;
+      I.rejac = 0;
+      RDCU_TRY(cudaStreamSynchronize(st_));
+      *t = tt;
+      *h = hh;
+      return cudaSuccess;
+    } else if (!I.fixed) {
+      factor = 0.5;
+      hh *= factor;
+      h_ = hh;
+      *h = hh;
+      *t = tt;
+      if (hh < hmin) return cudaStreamSynchronize(st_);
+      Small RU{};
+      make_RU(order, factor, RU.v);
+      k_updateD<<<nb, 256, 0, st_>>>(D_, nN, order, RU);
+      I.refactor = 1;
+      I.nconststeps = 0;
+      return cudaStreamSynchronize(st_);
+    }
+  }
+  if (I.fixed) {
+    RDCU_TRY(cudaMemcpyAsync(D_, I.ytemp, sizeof(double) * nN, cudaMemcpyDeviceToDevice, st_));
+    hh = h0;
+    tt = tt + hh;
+    t_ = tt;
+    h_ = hh;
+    *t = tt;
+    *h = hh;
+    *accepted = 1;
+    return cudaStreamSynchronize(st_);
+  }
+  // error test (bdf.cu:231-259)
+  const double safety = (2 * kNwit + 1) * 0.9 / (2 * kNwit + it + 1);
+  double errnorm;
+  k_errscale<<<nb, 256, 0, st_>>>(I.ytemp, nN, I.atl, I.rtl, I.yscale);
+  RDCU_TRY(wnorm(I, I.d, st_, &errnorm));
+  errnorm *= (kKappa[order] * kGamma[order] + 1.0 / (order + 1)) / sqN;
+  factor = safety * std::pow(errnorm, (-1.0 / (order + 1)));
+  if (errnorm > 1) {
+    if (factor < 0.2) factor = 0.2;
+    hh = hh * factor;
+    h_ = hh;
+    *h = hh;
+    *t = tt;
+    if (hh < hmin) return cudaStreamSynchronize(st_);
+    Small RU{};
+    make_RU(order, factor, RU.v);
+    k_updateD<<<nb, 256, 0, st_>>>(D_, nN, order, RU);
+    I.refactor = 1;
+    I.nconststeps = 0;
+    return cudaStreamSynchronize(st_);
+  }
+  // accept (bdf.cu:262-271)
+  tt = tt + hh;
+  k_accept<<<nb, 256, 0, st_>>>(D_, I.d, I.ytemp, nN, order);
+  I.rejac = 1;
+  I.nconststeps++;
+  if (I.nconststeps > order) {
+    double errm = INFINITY, errp = INFINITY, fm = 0.0, fp = 0.0;
+    if (order > 1) {
+      RDCU_TRY(wnorm(I, D_ + nN * order, st_, &errm));
+      errm *= (kKappa[order - 1] * kGamma[order - 1] + 1.0 / (order)) / sqN;
+      fm = safety * std::pow(errm, (-1.0 / (order)));
+    }
+    if (order < 5) {
+      RDCU_TRY(wnorm(I, D_ + nN * (order + 2), st_, &errp));
+      errp *= (kKappa[order + 1] * kGamma[order + 1] + 1.0 / (order + 2)) / sqN;
+      fp = safety * std::pow(errp, (-1.0 / (order + 2)));
+    }
+    int dorder = 0;
+    if (order > 1 && fm > factor && fm > fp) {
+      factor = fm;
+      dorder = -1;
+    } else if (order < 5 && fp > factor) {
+      factor = fp;
+      dorder = 1;
+    }
+    if (factor > 10) factor = 10;
+    if (hh * factor > hmax) {
+      factor = hmax / hh;
+      hh = hmax;
+    } else {
+      hh = hh * factor;
+    }
+    order += dorder;
+    Small RU{};
+    make_RU(order, factor, RU.v);
+    k_updateD<<<nb, 256, 0, st_>>>(D_, nN, order, RU);
+    I.nconststeps = 0;
+    I.refactor = 1;
+  }
+  order_ = order;
+  t_ = tt;
+  h_ = hh;
+  *t = tt;
+  *h = hh;
+  *accepted = 1;
+  return cudaStreamSynchronize(st_);
+}
+
+cudaError_t BDFEngine::eval(double t_eval, double* y_eval) {
+  Small fac{};
+  double factor = 1.0;
+  for (int j = 1; j <= order_; j++) {
+    factor *= (t_eval - t_ + j * h_) / (j * h_);
+    fac.v[j] = factor;
+  }
+  k_interp<<<impl_->blocks, 256, 0, st_>>>(D_, impl_->nN, order_, fac, y_eval);
+  RDCU_TRY(cudaGetLastError());
+  return cudaStreamSynchronize(st_);
+}
+
+cudaError_t BDFEngine::solve(double t1, double hmin, double hmax, const std::vector<double>& t_eval,
+                             const std::function<int(double, double, int, long long)>& on_attempt,
+                             const std::function<int(int, const double*)>& on_eval,
+                             const std::function<int(double, double, long long)>& on_checkpoint, int* cb_status,
+                             int* status) {
+  *cb_status = 0;
+  *status = RDCU_OK;
+  Impl& I = *impl_;
+  // bdf_run (bdf.cu:330-383): set-up, then attempt while t < t1 and h > hmin
+  RDCU_TRY(bdf_setup(I, *fd_, D_, &order_, h_, st_));
+  RDCU_TRY(cudaStreamSynchronize(st_));
+  solve_attempts = 0;
+  solve_accepted = 0;
+  long long steps = 0;
+  int eval_i = 0;
+  const int n_eval = (int)t_eval.size();
+  while (t_ < t1 && h_ > hmin) {
+    double t = t_, h = h_;
+    int acc = 0, st = 0;
+    RDCU_TRY(step(&t, &h, hmin, hmax, &acc, &st));
+    if (st) {
+      *status = st;
+      return cudaSuccess;
+    }
+    ++solve_attempts;
+    if (acc) ++steps;
+    solve_accepted = steps;
+    if (on_attempt) {
+      const int rc = on_attempt(t_, h_, acc, steps);
+      if (rc) {
+        *cb_status = rc;
+        return cudaSuccess;
+      }
+    }
+    if (!acc) continue;
+    bool any = false;
+    while (eval_i < n_eval && t_ >= t_eval[eval_i]) {
+      RDCU_TRY(eval(t_eval[eval_i], I.y_eval));
+      if (on_eval) {
+        const int rc = on_eval(eval_i, I.y_eval);
+        if (rc) {
+          *cb_status = rc;
+          return cudaSuccess;
+        }
+      }
+      ++eval_i;
+      any = true;
+    }
+    if (any && on_checkpoint) {
+      const int rc = on_checkpoint(t_, h_, steps);
+      if (rc) {
+        *cb_status = rc;
+        return cudaSuccess;
+      }
+    }
+  }
   return cudaSuccess;
 }
 

@@ -39,8 +39,9 @@ class BDFEngine {
   // linear-solver statistics
   long long lin_iters = 0, lin_solves = 0;
 
- private:
   struct Impl;
+
+ private:
   Impl* impl_ = nullptr;
   FDProblem* fd_ = nullptr;
   cudaStream_t st_ = nullptr;

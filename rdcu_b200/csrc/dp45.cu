@@ -380,6 +380,26 @@ cudaError_t DP45Engine::advance(int n, double hmin, double hmax, long long* acce
   return cudaSuccess;
 }
 
+cudaError_t DP45Engine::profile(int reps, std::vector<SpectralPlan::PassTime>* out) {
+  RDCU_TRY(sync_ctl());
+  // single-attempt arming makes the stage kernels run; the controller is not launched
+  RDCU_TRY(arm(0, INFINITY, 0.0, INFINITY, 0, 0, 1));
+  if (!k1_valid_) {
+    RDCU_TRY(launch_k1());
+    k1_valid_ = true;
+  }
+  RhsIO io{};
+  io.mode = 1;
+  io.stage = 4;
+  io.bufs = bufs;
+  io.ctl = d_ctl_;
+  RDCU_TRY(sp_->profile(io, reps, st_, out));
+  // leave the controller idle, as after a completed attempt
+  k_dp45_arm<<<1, 1, 0, st_>>>(d_ctl_, 0, INFINITY, 0.0, INFINITY, 0, 0, 1);
+  RDCU_TRY(cudaGetLastError());
+  return sync_ctl();
+}
+
 cudaError_t DP45Engine::eval(double t_eval, double* out) {
   const unsigned blocks = (unsigned)((nN_ + 255) / 256);
   k_dp45_interp<<<blocks, 256, 0, st_>>>(bufs, d_ctl_, t_eval, out, nN_);

@@ -38,6 +38,8 @@ class DP45Engine {
                     const std::function<int(double t, double h, long long steps)>& on_checkpoint,
                     int* cb_status);
 
+  // per-pass timing of stage 4 (see rdcu_profile_passes)
+  cudaError_t profile(int reps, std::vector<SpectralPlan::PassTime>* out);
   // n attempts on the device (graph launches), one sync at the end
   cudaError_t advance(int n, double hmin, double hmax, long long* accepted);
   // Launches one attempt (stages 2..7 and the controller) on the stream; no sync.

@@ -69,6 +69,28 @@ struct DictTable {
   const int* fold;            // [n] channel holding the folded linear part, -1 if none
 };
 
+// Constant-coefficient linear part of the finite-difference Jacobian, one entry per
+// linear term: row field, source field, FD operator, coefficient.  Its symbol at
+// wavenumber theta_a = 2 pi m_a / N_a is exact for the reference's stencils:
+// identity 1; d_a -> i sin(theta_a)/dx_a; d_a d_a -> (2 cos(theta_a) - 2)/dx_a^2;
+// d_a d_b -> -2 sin(theta_a) sin(theta_b)/(dx_a dx_b) (the reference's 0.5 factor).
+struct LinEntry {
+  int row, src, nax, ax0, ax1, pad;
+  double coef;
+};
+constexpr int kMaxPrecFields = 4;  // per-mode dense solve size of the preconditioner
+
+struct LinTable {
+  int n, nent, ndim;
+  const LinEntry* ent;
+  const double* sinv;  // sin(2 pi m / N_a) at sinv + off[a]
+  const double* cosv;
+  int off[3];
+  int Ns[3];
+  double dx[3];
+  double alpha;        // preconditioner of I + alpha * J_lin
+};
+
 // ----------------------------------------------------------------------------- DP45
 enum StopReason { kStopNone = 0, kStopDone = 1, kStopOutput = 2, kStopLog = 3, kStopChunk = 4 };
 

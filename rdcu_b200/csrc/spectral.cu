@@ -355,6 +355,155 @@ __global__ void k_mult1d(Mult1DArgs a) {
   a.Sc[(long long)ch * a.Mh + kx] = acc;
 }
 
+// Symbol of the constant-coefficient FD operator of one linear entry at multi-index
+// nidx (see LinEntry): returns the complex value.
+__device__ __forceinline__ double2 lin_symbol(const LinEntry& e, const int* nidx, const LinTable& t) {
+  if (e.nax == 0) return make_double2(1.0, 0.0);
+  const int a = e.ax0;
+  const double sa = t.sinv[t.off[a] + nidx[a]];
+  if (e.nax == 1) return make_double2(0.0, sa / t.dx[a]);
+  if (e.ax0 == e.ax1) {
+    const double ca = t.cosv[t.off[a] + nidx[a]];
+    return make_double2((2.0 * ca - 2.0) / (t.dx[a] * t.dx[a]), 0.0);
+  }
+  const int b = e.ax1;
+  const double sb = t.sinv[t.off[b] + nidx[b]];
+  return make_double2(-2.0 * sa * sb / (t.dx[a] * t.dx[b]), 0.0);
+}
+
+// x = (I + alpha L(k))^-1 r at one mode, n <= kMaxPrecFields, Gaussian elimination
+// with partial pivoting; a (numerically) singular mode is passed through unchanged.
+__device__ __forceinline__ void mode_solve(const LinTable& t, const int* nidx, double2* v, int n) {
+  double2 A[kMaxPrecFields][kMaxPrecFields];
+  double2 b[kMaxPrecFields];
+#pragma unroll
+  for (int i = 0; i < kMaxPrecFields; ++i) {
+#pragma unroll
+    for (int j = 0; j < kMaxPrecFields; ++j) A[i][j] = make_double2(i == j ? 1.0 : 0.0, 0.0);
+    b[i] = i < n ? v[i] : make_double2(0.0, 0.0);
+  }
+  for (int q = 0; q < t.nent; ++q) {
+    const LinEntry e = t.ent[q];
+    const double2 sy = lin_symbol(e, nidx, t);
+    const double cf = t.alpha * e.coef;
+#pragma unroll
+    for (int i = 0; i < kMaxPrecFields; ++i)
+#pragma unroll
+      for (int j = 0; j < kMaxPrecFields; ++j)
+        if (i == e.row && j == e.src) {
+          A[i][j].x += cf * sy.x;
+          A[i][j].y += cf * sy.y;
+        }
+  }
+  bool ok = true;
+#pragma unroll
+  for (int k = 0; k < kMaxPrecFields; ++k) {
+    if (k >= n) break;
+    // pivot
+    int p = k;
+    double best = A[k][k].x * A[k][k].x + A[k][k].y * A[k][k].y;
+#pragma unroll
+    for (int i = k + 1; i < kMaxPrecFields; ++i) {
+      if (i >= n) break;
+      const double m2 = A[i][k].x * A[i][k].x + A[i][k].y * A[i][k].y;
+      if (m2 > best) { best = m2; p = i; }
+    }
+    if (!(best > 1e-300)) { ok = false; break; }
+#pragma unroll
+    for (int i = 0; i < kMaxPrecFields; ++i)
+      if (i == p && p != k) {
+#pragma unroll
+        for (int j = 0; j < kMaxPrecFields; ++j) { const double2 tmp = A[k][j]; A[k][j] = A[i][j]; A[i][j] = tmp; }
+        const double2 tb = b[k]; b[k] = b[i]; b[i] = tb;
+      }
+    const double2 piv = A[k][k];
+    const double inv = 1.0 / (piv.x * piv.x + piv.y * piv.y);
+    const double2 ip = make_double2(piv.x * inv, -piv.y * inv);
+#pragma unroll
+    for (int i = k + 1; i < kMaxPrecFields; ++i) {
+      if (i >= n) break;
+      const double2 f = c_mul(A[i][k], ip);
+#pragma unroll
+      for (int j = k; j < kMaxPrecFields; ++j) A[i][j] = c_sub(A[i][j], c_mul(f, A[k][j]));
+      b[i] = c_sub(b[i], c_mul(f, b[k]));
+    }
+  }
+  if (!ok) return;
+#pragma unroll
+  for (int k = kMaxPrecFields - 1; k >= 0; --k) {
+    if (k >= n) continue;
+    double2 acc = b[k];
+#pragma unroll
+    for (int j = k + 1; j < kMaxPrecFields; ++j)
+      if (j < n) acc = c_sub(acc, c_mul(A[k][j], b[j]));
+    const double2 piv = A[k][k];
+    const double inv = 1.0 / (piv.x * piv.x + piv.y * piv.y);
+    b[k] = c_mul(acc, make_double2(piv.x * inv, -piv.y * inv));
+  }
+  for (int i = 0; i < n; ++i) v[i] = b[i];
+}
+
+struct MidSolveArgs {
+  int L0, I, TW, n, ndim, Mh;
+  LinePlan plan;
+  const double2* tw;
+  const double2* Sf;
+  double2* Sc;
+  LinTable lin;
+};
+
+template <int RS>
+__global__ void __launch_bounds__(kMaxBlock, 1) k_mid_solve(MidSolveArgs a) {
+  extern __shared__ double2 sm[];
+  const int L0 = a.L0, TW = a.TW, LS = L0 + 1, T = blockDim.x, tid = threadIdx.x, n = a.n;
+  double2* tw = sm;
+  double2* fb = sm + L0;
+  for (int t = tid; t < L0; t += T) tw[t] = a.tw[t];
+  const long long i0 = (long long)blockIdx.x * TW;
+  const int nload = n * L0 * TW;
+  for (int e = tid; e < nload; e += T) {
+    const int c = e % TW, z = (e / TW) % L0, f = e / (TW * L0);
+    const long long ii = i0 + c;
+    fb[(f * TW + c) * LS + z] = ii < a.I ? a.Sf[((long long)f * L0 + z) * a.I + ii] : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  fft_lines<RS, false>(fb, LS, n * TW, a.plan, tw);
+  for (int e = tid; e < L0 * TW; e += T) {
+    const int c = e % TW, z = e / TW;
+    const long long ii = i0 + c;
+    if (ii >= a.I) continue;
+    int nidx[3];
+    nidx[0] = z;
+    if (a.ndim == 3) {
+      nidx[1] = (int)(ii / a.Mh);
+      nidx[2] = (int)(ii - (long long)nidx[1] * a.Mh);
+    } else {
+      nidx[1] = (int)ii;
+    }
+    double2 v[kMaxPrecFields];
+    for (int f = 0; f < n; ++f) v[f] = fb[(f * TW + c) * LS + z];
+    mode_solve(a.lin, nidx, v, n);
+    for (int f = 0; f < n; ++f) fb[(f * TW + c) * LS + z] = v[f];
+  }
+  __syncthreads();
+  fft_lines<RS, true>(fb, LS, n * TW, a.plan, tw);
+  for (int e = tid; e < nload; e += T) {
+    const int c = e % TW, z = (e / TW) % L0, f = e / (TW * L0);
+    const long long ii = i0 + c;
+    if (ii < a.I) a.Sc[((long long)f * L0 + z) * a.I + ii] = fb[(f * TW + c) * LS + z];
+  }
+}
+
+__global__ void k_mult1d_solve(int Mh, int n, const double2* Sf, double2* Sc, LinTable lin) {
+  const int kx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (kx >= Mh) return;
+  int nidx[3] = {kx, 0, 0};
+  double2 v[kMaxPrecFields];
+  for (int f = 0; f < n; ++f) v[f] = Sf[(long long)f * Mh + kx];
+  mode_solve(lin, nidx, v, n);
+  for (int f = 0; f < n; ++f) Sc[(long long)f * Mh + kx] = v[f];
+}
+
 struct InvXArgs {
   int M, Mh, R, P, n, nch_run, npairs, do_fft, tw_smem;
   long long N;
@@ -365,6 +514,7 @@ struct InvXArgs {
   RhsIO io;
   double* Yout;       // Y mode: channel c -> complex block ydst[c]>>1, part ydst[c]&1
   const int* ydst;
+  int yplain;         // 1: channel c -> real array Yout[c*N + point]
 };
 
 template <int RS>
@@ -436,8 +586,13 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_inv_x(InvXArgs a) {
       const long long row = r0 + pr;
       if (row >= a.R) continue;
       const double2 z = lines[(pr * np + (c >> 1)) * M + x];
-      const int d = a.ydst[c];
-      a.Yout[(((long long)(d >> 1)) * a.N + row * M + x) * 2 + (d & 1)] = (c & 1) ? z.y : z.x;
+      const double val = (c & 1) ? z.y : z.x;
+      if (a.yplain) {
+        a.Yout[(long long)c * a.N + row * M + x] = val;
+      } else {
+        const int d = a.ydst[c];
+        a.Yout[(((long long)(d >> 1)) * a.N + row * M + x) * 2 + (d & 1)] = val;
+      }
     }
     return;
   }
@@ -524,6 +679,18 @@ constexpr int kTargetCtas = 2 * 148;
     cudaError_t _e = (x);                  \
     if (_e != cudaSuccess) return _e;      \
   } while (0)
+
+// Allows a kernel the largest dynamic shared memory the device grants next to its
+// static shared memory.
+static bool opt_in_smem(const void* func) {
+  cudaFuncAttributes fa;
+  if (cudaFuncGetAttributes(&fa, func) != cudaSuccess) return false;
+  int dev = 0, optin = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return false;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return false;
+  const int dyn = optin - (int)fa.sharedSizeBytes;
+  return cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) == cudaSuccess;
+}
 
 // Geometry of the inverse x pass for nch_run channels (with or without the
 // physical-field staging): rows per CTA, grid, block and dynamic shared memory.
@@ -824,18 +991,23 @@ bool SpectralPlan::init(int n_, int ndim_, const int* Ns_, const double* Ls_,
   }
   device_bytes += (size_t)sc_rows_ * srow;
 
-  // opt in to large dynamic shared memory
+  // opt in to large dynamic shared memory (the limit is per block, static included)
   const int maxsm = 227 * 1024;
-  cudaFuncSetAttribute(k_fwd_x<kRadixPow2>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
-  cudaFuncSetAttribute(k_fwd_x<kRadixAll>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
-  cudaFuncSetAttribute(k_inv_x<kRadixPow2>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
-  cudaFuncSetAttribute(k_inv_x<kRadixAll>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
-  cudaFuncSetAttribute(k_mid<kRadixPow2>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
-  cudaFuncSetAttribute(k_mid<kRadixAll>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
-  cudaFuncSetAttribute(k_c2c<kRadixPow2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
-  cudaFuncSetAttribute(k_c2c<kRadixPow2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
-  cudaFuncSetAttribute(k_c2c<kRadixAll, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
-  cudaFuncSetAttribute(k_c2c<kRadixAll, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+  bool optin_ok = true;
+  optin_ok &= opt_in_smem((const void*)k_fwd_x<kRadixPow2>);
+  optin_ok &= opt_in_smem((const void*)k_fwd_x<kRadixAll>);
+  optin_ok &= opt_in_smem((const void*)k_inv_x<kRadixPow2>);
+  optin_ok &= opt_in_smem((const void*)k_inv_x<kRadixAll>);
+  optin_ok &= opt_in_smem((const void*)k_mid<kRadixPow2>);
+  optin_ok &= opt_in_smem((const void*)k_mid<kRadixAll>);
+  optin_ok &= opt_in_smem((const void*)k_c2c<kRadixPow2, false>);
+  optin_ok &= opt_in_smem((const void*)k_c2c<kRadixPow2, true>);
+  optin_ok &= opt_in_smem((const void*)k_c2c<kRadixAll, false>);
+  optin_ok &= opt_in_smem((const void*)k_c2c<kRadixAll, true>);
+  if (!optin_ok) {
+    *msg = "cannot enable large shared memory for the FFT passes";
+    return false;
+  }
   if (fwd_.smem > (size_t)maxsm || inv_.smem > (size_t)maxsm) {
     *msg = "grid too large for the shared-memory x pass";
     return false;
@@ -858,7 +1030,7 @@ cudaError_t SpectralPlan::ensure_channel_capacity(int rows) {
 
 void SpectralPlan::release() {
   void* ptrs[] = {tw_x_, tw_ax_[0], tw_ax_[1], tw_ax_[2], kv_, ch_off_, ch_ent_, d_terms_, d_fac_,
-                  d_field_begin_, d_fold_, ych_off_, ych_ent_, ych_dst_, Sf_, Sc_};
+                  d_field_begin_, d_fold_, ych_off_, ych_ent_, ych_dst_, Sf_, Sc_, lin_ent_, sinv_, cosv_};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   tw_x_ = nullptr;
@@ -875,13 +1047,17 @@ void SpectralPlan::release() {
   ych_dst_ = nullptr;
   Sf_ = nullptr;
   Sc_ = nullptr;
+  lin_ent_ = nullptr;
+  sinv_ = nullptr;
+  cosv_ = nullptr;
+  nlin_ = 0;
   built_ = false;
 }
 
 // Runs the passes for channels [g_first, g_first+nch_run) of table ct.  When Yout is
 // set the inverse x pass writes channels to Y.dat layout instead of the dictionary.
 cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, int nch_run, int g_first,
-                                        double* Yout, const int* ydst, cudaStream_t st) {
+                                        double* Yout, const int* ydst, cudaStream_t st, int yplain) {
   const bool spectral = nch_run > 0;
   if (spectral && ndim >= 2) {
     const int which = Yout ? 1 : 0;
@@ -953,6 +1129,7 @@ cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, in
   a.io = io;
   a.Yout = Yout;
   a.ydst = ydst;
+  a.yplain = yplain;
   // geometry for this channel count (the hot path's is the one the error partials
   // buffer was sized for)
   PassCfg g;
@@ -1053,6 +1230,311 @@ cudaError_t SpectralPlan::run_Y(const double* y, double* Yout, cudaStream_t st) 
     const int cnt = std::min(GY, ych_ - g);
     RDCU_TRY(launch_passes(io, ct, cnt, g, Yout, ych_dst_ + g, st));
   }
+  return cudaSuccess;
+}
+
+bool SpectralPlan::init_precond(int n_, int ndim_, const int* Ns_, const double* Ls_,
+                                const std::vector<LinEntry>& lin, std::string* msg) {
+  if (n_ > kMaxPrecFields) {
+    *msg = "preconditioner supports at most " + std::to_string(kMaxPrecFields) + " fields";
+    return false;
+  }
+  if (!init(n_, ndim_, Ns_, Ls_, std::vector<HostTerm>(), msg)) return false;
+  std::vector<double> sv, cv;
+  const double PI = 3.14159265358979323846;
+  for (int a = 0; a < ndim; ++a) {
+    sc_off_[a] = (int)sv.size();
+    for (int m = 0; m < Ns[a]; ++m) {
+      const long double th = 2.0L * 3.141592653589793238462643383279502884L * m / Ns[a];
+      sv.push_back((double)sinl(th));
+      cv.push_back((double)cosl(th));
+    }
+  }
+  (void)PI;
+  nlin_ = (int)lin.size();
+  cudaError_t e = upload(&lin_ent_, lin, &device_bytes);
+  if (e == cudaSuccess) e = upload(&sinv_, sv, &device_bytes);
+  if (e == cudaSuccess) e = upload(&cosv_, cv, &device_bytes);
+  if (e == cudaSuccess) e = ensure_channel_capacity(n);
+  if (e == cudaSuccess && !ych_dst_) e = cudaErrorInvalidValue;
+  if (e != cudaSuccess) {
+    *msg = std::string("preconditioner set-up: ") + cudaGetErrorString(e);
+    return false;
+  }
+  if (ndim >= 2) {
+    const int L0 = Ns[0];
+    const int I = (ndim == 3) ? Ns[1] * Mh : Mh;
+    int TW = std::max(1, std::min(16, I / kTargetCtas));
+    auto smem_of = [&](int tw_) { return (size_t)(L0 + n * tw_ * (L0 + 1)) * 16; };
+    while (TW > 1 && (smem_of(TW) > kSmemBudget || n * TW * L0 > kMaxElems)) TW /= 2;
+    if (smem_of(TW) > 227 * 1024 || n * TW * L0 > kMaxElems) {
+      *msg = "grid too large for the preconditioner's axis-0 pass";
+      return false;
+    }
+    midsolve_.per_cta = TW;
+    midsolve_.grid = (I + TW - 1) / TW;
+    midsolve_.block = std::min(kMaxBlock, std::max(128, round_up(stage_threads(plan_ax_[0], n * TW * L0), 32)));
+    midsolve_.smem = smem_of(TW);
+    if (!opt_in_smem((const void*)k_mid_solve<kRadixPow2>) || !opt_in_smem((const void*)k_mid_solve<kRadixAll>)) {
+      *msg = "cannot enable large shared memory for the preconditioner pass";
+      return false;
+    }
+  }
+  return true;
+}
+
+cudaError_t SpectralPlan::launch_forward(const double* y, cudaStream_t st) {
+  RhsIO io{};
+  io.mode = 0;
+  io.y = y;
+  FwdXArgs a{};
+  a.M = M;
+  a.Mh = Mh;
+  a.nrows = n * R;
+  a.P = fwd_.per_cta;
+  a.do_fft = 1;
+  a.tw_smem = fwd_.smem >= (size_t)(M + a.P * M) * 16 ? 1 : 0;
+  a.plan = plan_x_;
+  a.tw = tw_x_;
+  a.S = Sf_;
+  a.io = io;
+  if (plan_is_pow2(plan_x_))
+    k_fwd_x<kRadixPow2><<<fwd_.grid, fwd_.block, fwd_.smem, st>>>(a);
+  else
+    k_fwd_x<kRadixAll><<<fwd_.grid, fwd_.block, fwd_.smem, st>>>(a);
+  RDCU_TRY(cudaGetLastError());
+  if (ndim == 3) {
+    C2CArgs c{};
+    c.La = Ns[1];
+    c.I = Mh;
+    c.TW = c2c_f_.per_cta;
+    c.plan = plan_ax_[1];
+    c.tw = tw_ax_[1];
+    c.S = Sf_;
+    c.io = io;
+    dim3 grid(c2c_f_.grid, n * Ns[0]);
+    if (plan_is_pow2(plan_ax_[1]))
+      k_c2c<kRadixPow2, false><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(c);
+    else
+      k_c2c<kRadixAll, false><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(c);
+    RDCU_TRY(cudaGetLastError());
+  }
+  return cudaSuccess;
+}
+
+cudaError_t SpectralPlan::precond(const double* r, double* z, double alpha, cudaStream_t st) {
+  RDCU_TRY(launch_forward(r, st));
+  LinTable lt{};
+  lt.n = n;
+  lt.nent = nlin_;
+  lt.ndim = ndim;
+  lt.ent = lin_ent_;
+  lt.sinv = sinv_;
+  lt.cosv = cosv_;
+  lt.alpha = alpha;
+  for (int a = 0; a < 3; ++a) {
+    lt.off[a] = sc_off_[a];
+    lt.Ns[a] = Ns[a];
+    lt.dx[a] = Ls[a] / Ns[a];
+  }
+  if (ndim >= 2) {
+    MidSolveArgs m{};
+    m.L0 = Ns[0];
+    m.I = (ndim == 3) ? Ns[1] * Mh : Mh;
+    m.TW = midsolve_.per_cta;
+    m.n = n;
+    m.ndim = ndim;
+    m.Mh = Mh;
+    m.plan = plan_ax_[0];
+    m.tw = tw_ax_[0];
+    m.Sf = Sf_;
+    m.Sc = Sc_;
+    m.lin = lt;
+    if (plan_is_pow2(plan_ax_[0]))
+      k_mid_solve<kRadixPow2><<<midsolve_.grid, midsolve_.block, midsolve_.smem, st>>>(m);
+    else
+      k_mid_solve<kRadixAll><<<midsolve_.grid, midsolve_.block, midsolve_.smem, st>>>(m);
+    RDCU_TRY(cudaGetLastError());
+    if (ndim == 3) {
+      C2CArgs a{};
+      a.La = Ns[1];
+      a.I = Mh;
+      a.TW = c2c_i_.per_cta;
+      a.plan = plan_ax_[1];
+      a.tw = tw_ax_[1];
+      a.S = Sc_;
+      a.io = RhsIO{};
+      dim3 grid(c2c_i_.grid, n * Ns[0]);
+      if (plan_is_pow2(plan_ax_[1]))
+        k_c2c<kRadixPow2, true><<<grid, c2c_i_.block, c2c_i_.smem, st>>>(a);
+      else
+        k_c2c<kRadixAll, true><<<grid, c2c_i_.block, c2c_i_.smem, st>>>(a);
+      RDCU_TRY(cudaGetLastError());
+    }
+  } else {
+    k_mult1d_solve<<<(Mh + 127) / 128, 128, 0, st>>>(Mh, n, Sf_, Sc_, lt);
+    RDCU_TRY(cudaGetLastError());
+  }
+  // inverse x pass of the n solved fields straight into z
+  InvXArgs a{};
+  a.M = M;
+  a.Mh = Mh;
+  a.R = R;
+  a.n = n;
+  a.nch_run = n;
+  a.npairs = (n + 1) / 2;
+  a.do_fft = 1;
+  a.N = N;
+  a.plan = plan_x_;
+  a.tw = tw_x_;
+  a.Sc = Sc_;
+  a.dict = dict_table();
+  a.io = RhsIO{};
+  a.Yout = z;
+  a.ydst = nullptr;
+  a.yplain = 1;
+  PassCfg g;
+  int tws = 0;
+  inv_geometry(M, R, n, n, true, plan_x_, &g, &tws);
+  a.P = g.per_cta;
+  a.tw_smem = tws;
+  if (plan_is_pow2(plan_x_))
+    k_inv_x<kRadixPow2><<<g.grid, g.block, g.smem, st>>>(a);
+  else
+    k_inv_x<kRadixAll><<<g.grid, g.block, g.smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, std::vector<PassTime>* out) {
+  out->clear();
+  cudaEvent_t e0, e1;
+  RDCU_TRY(cudaEventCreate(&e0));
+  RDCU_TRY(cudaEventCreate(&e1));
+  const double spec_row = (double)R * Mh * 16.0;  // one field's half spectrum
+  const double arr = (double)N * 8.0;             // one field's physical array
+  const int s = io.stage >= 2 ? io.stage : 1;
+  const int nk = s >= 2 ? (s == 7 ? s - 2 : s - 1) : 0;  // slopes the stage combination reads
+  auto timed = [&](const char* name, double bytes, auto&& launch) -> cudaError_t {
+    RDCU_TRY(launch());  // warm-up
+    RDCU_TRY(cudaEventRecord(e0, st));
+    for (int r = 0; r < reps; ++r) RDCU_TRY(launch());
+    RDCU_TRY(cudaEventRecord(e1, st));
+    RDCU_TRY(cudaEventSynchronize(e1));
+    float ms = 0;
+    RDCU_TRY(cudaEventElapsedTime(&ms, e0, e1));
+    out->push_back({name, ms / reps, bytes});
+    return cudaSuccess;
+  };
+  const bool spectral = nch > 0;
+  FwdXArgs fa{};
+  fa.M = M;
+  fa.Mh = Mh;
+  fa.nrows = n * R;
+  fa.P = fwd_.per_cta;
+  fa.do_fft = spectral ? 1 : 0;
+  fa.tw_smem = fwd_.smem >= (size_t)(M + fa.P * M) * 16 ? 1 : 0;
+  fa.plan = plan_x_;
+  fa.tw = tw_x_;
+  fa.S = Sf_;
+  fa.io = io;
+  RDCU_TRY(timed("fwd_x", n * ((1 + nk) * arr + (s >= 2 ? arr : 0) + spec_row), [&]() {
+    if (plan_is_pow2(plan_x_))
+      k_fwd_x<kRadixPow2><<<fwd_.grid, fwd_.block, fwd_.smem, st>>>(fa);
+    else
+      k_fwd_x<kRadixAll><<<fwd_.grid, fwd_.block, fwd_.smem, st>>>(fa);
+    return cudaGetLastError();
+  }));
+  if (spectral && ndim == 3) {
+    C2CArgs c{};
+    c.La = Ns[1];
+    c.I = Mh;
+    c.TW = c2c_f_.per_cta;
+    c.plan = plan_ax_[1];
+    c.tw = tw_ax_[1];
+    c.S = Sf_;
+    c.io = io;
+    dim3 grid(c2c_f_.grid, n * Ns[0]);
+    RDCU_TRY(timed("c2c_axis1_fwd", 2.0 * n * spec_row, [&]() {
+      if (plan_is_pow2(plan_ax_[1]))
+        k_c2c<kRadixPow2, false><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(c);
+      else
+        k_c2c<kRadixAll, false><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(c);
+      return cudaGetLastError();
+    }));
+  }
+  if (spectral && ndim >= 2) {
+    const PassCfg& c = mid_[0];
+    MidArgs m{};
+    m.L0 = Ns[0];
+    m.I = (ndim == 3) ? Ns[1] * Mh : Mh;
+    m.TW = c.per_cta & 0xffff;
+    m.GB = c.per_cta >> 16;
+    m.nsrc = n;
+    m.G = nch;
+    m.ch0 = 0;
+    m.ndim = ndim;
+    m.D1 = Ns[1];
+    m.Mh = Mh;
+    m.plan = plan_ax_[0];
+    m.tw = tw_ax_[0];
+    m.Sf = Sf_;
+    m.Sc = Sc_;
+    m.chan = chan_table(ch_off_, ch_ent_, nch);
+    m.io = io;
+    RDCU_TRY(timed("mid_axis0", (double)(n + nch) * spec_row, [&]() {
+      if (plan_is_pow2(plan_ax_[0]))
+        k_mid<kRadixPow2><<<c.grid, c.block, c.smem, st>>>(m);
+      else
+        k_mid<kRadixAll><<<c.grid, c.block, c.smem, st>>>(m);
+      return cudaGetLastError();
+    }));
+    if (ndim == 3) {
+      C2CArgs a{};
+      a.La = Ns[1];
+      a.I = Mh;
+      a.TW = c2c_i_.per_cta;
+      a.plan = plan_ax_[1];
+      a.tw = tw_ax_[1];
+      a.S = Sc_;
+      a.io = io;
+      dim3 grid(c2c_i_.grid, nch * Ns[0]);
+      RDCU_TRY(timed("c2c_axis1_inv", 2.0 * nch * spec_row, [&]() {
+        if (plan_is_pow2(plan_ax_[1]))
+          k_c2c<kRadixPow2, true><<<grid, c2c_i_.block, c2c_i_.smem, st>>>(a);
+        else
+          k_c2c<kRadixAll, true><<<grid, c2c_i_.block, c2c_i_.smem, st>>>(a);
+        return cudaGetLastError();
+      }));
+    }
+  }
+  InvXArgs a{};
+  a.M = M;
+  a.Mh = Mh;
+  a.R = R;
+  a.n = n;
+  a.nch_run = nch;
+  a.npairs = (nch + 1) / 2;
+  a.do_fft = spectral ? 1 : 0;
+  a.N = N;
+  a.plan = plan_x_;
+  a.tw = tw_x_;
+  a.Sc = Sc_;
+  a.dict = dict_table();
+  a.io = io;
+  PassCfg g;
+  int tws = 0;
+  inv_geometry(M, R, n, nch, false, plan_x_, &g, &tws);
+  a.P = g.per_cta;
+  a.tw_smem = tws;
+  RDCU_TRY(timed("inv_x_dictionary", nch * spec_row + 2.0 * n * arr, [&]() {
+    if (plan_is_pow2(plan_x_))
+      k_inv_x<kRadixPow2><<<g.grid, g.block, g.smem, st>>>(a);
+    else
+      k_inv_x<kRadixAll><<<g.grid, g.block, g.smem, st>>>(a);
+    return cudaGetLastError();
+  }));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
   return cudaSuccess;
 }
 

@@ -46,6 +46,20 @@ class SpectralPlan {
   // All complex Y blocks (Y.dat layout) of y, written to Yout (device).
   cudaError_t run_Y(const double* y, double* Yout, cudaStream_t stream);
 
+  struct PassTime {
+    const char* name;
+    double ms;
+    double bytes;
+  };
+  // Times every pass of one RHS evaluation (io) `reps` times each.
+  cudaError_t profile(const RhsIO& io, int reps, cudaStream_t stream, std::vector<PassTime>* out);
+
+  // FFT-only plan for the BDF preconditioner: z = (I + alpha*J_lin)^-1 r with J_lin
+  // the constant-coefficient linear FD operator of `lin` (solved mode by mode).
+  bool init_precond(int n, int ndim, const int* Ns, const double* Ls, const std::vector<LinEntry>& lin,
+                    std::string* msg);
+  cudaError_t precond(const double* r, double* z, double alpha, cudaStream_t stream);
+
   int n = 0, ndim = 0, Ns[3] = {1, 1, 1};
   double Ls[3] = {1, 1, 1};
   long long N = 0;  // grid points
@@ -75,6 +89,13 @@ class SpectralPlan {
   int* ych_off_ = nullptr;
   ChanEntry* ych_ent_ = nullptr;
   int* ych_dst_ = nullptr;
+  // preconditioner tables
+  LinEntry* lin_ent_ = nullptr;
+  int nlin_ = 0;
+  double* sinv_ = nullptr;
+  double* cosv_ = nullptr;
+  int sc_off_[3] = {0, 0, 0};
+  PassCfg midsolve_{};
   // spectral buffers
   double2* Sf_ = nullptr;  // field half spectra [n][R][Mh]
   double2* Sc_ = nullptr;  // channel half spectra [max(nch, G)][R][Mh]
@@ -85,7 +106,9 @@ class SpectralPlan {
   ChanTable chan_table(const int* off, const ChanEntry* ent, int nch) const;
   DictTable dict_table() const;
   cudaError_t launch_passes(const RhsIO& io, const ChanTable& ct, int nch_run, int g_first,
-                            double* Yout, const int* ydst, cudaStream_t stream);
+                            double* Yout, const int* ydst, cudaStream_t stream, int yplain = 0);
+  cudaError_t launch_forward(const double* y, cudaStream_t stream);
+  bool geometry(std::string* msg);
   cudaError_t ensure_channel_capacity(int rows);
 };
 

@@ -1,0 +1,85 @@
+"""C ABI checks that need no GPU: librdcu loads, exports every entry point that
+include/rdcu.h declares, validates specifications before touching CUDA, and its
+initial-condition generator reproduces the reference's glibc rand() stream."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import rdcu_b200 as R
+from oracle.problem import glibc_uniform_ic
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    text = open(os.path.join(ROOT, "include", "rdcu.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(rdcu_\w+)\s*\(", text)))
+
+
+def test_header_declares_the_abi():
+    names = declared_functions()
+    for must in ("rdcu_create", "rdcu_destroy", "rdcu_rhs", "rdcu_step", "rdcu_solve", "rdcu_jac", "rdcu_eval"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(R.LIB_PATH)
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+    assert sorted(R.EXPORTS) == declared_functions()
+
+
+def _spec(**kw):
+    s = R.rdcu_spec()
+    s.n = kw.get("n", 2)
+    s.ndim = kw.get("ndim", 2)
+    for a in range(3):
+        s.Ns[a] = 8
+        s.Ls[a] = 1.0
+    s.nterms = 0
+    s.method = kw.get("method", 0)
+    s.rtol = s.atol = 1e-8
+    return s
+
+
+@pytest.mark.parametrize("bad", [dict(n=0), dict(ndim=0), dict(ndim=4), dict(method=7)])
+def test_create_rejects_bad_specs(bad):
+    lib = R.load_library()
+    h = ctypes.c_void_p()
+    rc = lib.rdcu_create(ctypes.byref(h), ctypes.byref(_spec(**bad)))
+    assert rc == R.RDCU_ERR_INVALID
+    assert lib.rdcu_last_error(None)
+
+
+def test_create_rejects_out_of_range_terms():
+    with pytest.raises(R.RdcuError) as e:
+        R.Solver(2, (8, 8), (1.0, 1.0), [(1.0, [0, 14, 1])])  # 2 fields, 2D: Y indices 0..13
+    assert e.value.code == R.RDCU_ERR_INVALID
+    with pytest.raises(R.RdcuError):
+        R.Solver(2, (8, 8), (1.0, 1.0), [(1.0, [2, 0, 1])])  # field 2 of 2
+
+
+def test_error_strings():
+    lib = R.load_library()
+    assert lib.rdcu_error_string(R.RDCU_ERR_CUDA) == b"CUDA error"
+    assert lib.rdcu_error_string(0) == b"ok"
+
+
+@pytest.mark.parametrize("n,N,A,A0,seed", [(1, 7, 1e-3, 0.0, 1), (2, 50, 2.0, 0.5, 3), (3, 11, 1.0, -1.0, 12345)])
+def test_random_ic_matches_glibc_stream(n, N, A, A0, seed):
+    np.testing.assert_array_equal(R.random_ic(n, N, A, A0, seed), glibc_uniform_ic(n, N, A, A0, seed))
+
+
+def test_no_cpu_fallback_without_gpu():
+    """Without a GPU the library fails loudly (there is no CPU path)."""
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(R.RdcuError) as e:
+        R.Solver(2, (8, 8), (1.0, 1.0), [(1.0, [0, 0, 1])])
+    assert e.value.code == R.RDCU_ERR_CUDA
