@@ -34,6 +34,15 @@ __device__ __forceinline__ double2 tw_get(const double2* tw, int t) {
   return w;
 }
 
+// 16-byte asynchronous global->shared copy (zero-filled when pred is false; the source
+// address is then not read).  Completion: cp_async_wait_all() and a barrier.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool pred) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = pred ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // In-register R-point DFT of v (forward: exp(-2 pi i rk/R); inverse: conjugate).
 template <int R, bool INV>
 struct Dft {

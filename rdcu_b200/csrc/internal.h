@@ -46,6 +46,7 @@ struct ChanTable {
   int kv_off[3];
   int Ns[3];
   int ndim;
+  int kv_total;  // sum of Ns over the axes (length of kv)
 };
 
 // Dictionary terms left after folding the linear derivative terms into channels.
@@ -67,6 +68,7 @@ struct DictTable {
   const DictFactor* fac;
   const int* field_begin;     // [n+1]
   const int* fold;            // [n] channel holding the folded linear part, -1 if none
+  int nfac;                   // number of factors (fac length)
 };
 
 // Constant-coefficient linear part of the finite-difference Jacobian, one entry per

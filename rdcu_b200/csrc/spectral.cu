@@ -28,6 +28,7 @@
 // uses both.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "fft_line.cuh"
@@ -89,18 +90,9 @@ __device__ __forceinline__ Resolved resolve(const RhsIO& io) {
   return r;
 }
 
-// Stage state of DP45 stage s at element i, in the reference kernels' arithmetic order
-// (dp45.cu:34-69): stage 2 is y + h*a*k1, later stages y + h*(sum_j a_j k_j).  b_2 = 0
-// (dp45.cu:11), so stage 7 does not read k2.
-__device__ __forceinline__ double stage_value(int s, long long i, const Resolved& r) {
-  const double yi = r.y[i];
-  if (s == 2) return yi + r.h * c_a[2][0] * r.k[0][i];
-  double acc = c_a[s][0] * r.k[0][i];
-  if (s != 7) acc += c_a[s][1] * r.k[1][i];
-  for (int j = 2; j < s - 1; ++j) acc += c_a[s][j] * r.k[j][i];
-  return yi + r.h * acc;
-}
-
+// Stage states follow the reference kernels' arithmetic order (dp45.cu:34-69): stage 2
+// is y + h*a*k1, later stages y + h*(sum_j a_j k_j); b_2 = 0 (dp45.cu:11), so stage 7
+// does not read k2 (stage_value_t below).
 __device__ __forceinline__ double ipow(double x, int e) {
   if (e == 0) return 1.0;  // pow(x, 0) == 1 for every x
   const int a = e < 0 ? -e : e;
@@ -145,6 +137,42 @@ __device__ __forceinline__ double2 apply_entry(const ChanEntry& e, const int* ni
   }
 }
 
+__device__ __forceinline__ double sel3(double a0, double a1, double a2, int i) {
+  return i == 0 ? a0 : (i == 1 ? a1 : a2);
+}
+
+// apply_entry with the point's wavenumbers k(n_a), k(-n_a) already in registers
+__device__ __forceinline__ double2 apply_entry_k(const ChanEntry& e, const double* kp, const double* km,
+                                                 double2 u) {
+  double ap = 1.0, am = 1.0;
+  if (e.nax >= 1) {
+    ap *= sel3(kp[0], kp[1], kp[2], e.ax0);
+    am *= sel3(km[0], km[1], km[2], e.ax0);
+  }
+  if (e.nax >= 2) {
+    ap *= sel3(kp[0], kp[1], kp[2], e.ax1);
+    am *= sel3(km[0], km[1], km[2], e.ax1);
+  }
+  const double sgn = (e.nax & 1) ? -1.0 : 1.0;
+  double beta;
+  int q;
+  if (e.part == 0) {
+    q = e.nax;
+    beta = 0.5 * (ap + sgn * am);
+  } else {
+    q = e.nax + 3;
+    beta = 0.5 * (ap - sgn * am);
+  }
+  beta *= e.coef;
+  const double2 r = make_double2(beta * u.x, beta * u.y);
+  switch (q & 3) {
+    case 0: return r;
+    case 1: return make_double2(-r.y, r.x);
+    case 2: return make_double2(-r.x, -r.y);
+    default: return make_double2(r.y, -r.x);
+  }
+}
+
 __device__ __forceinline__ double block_sum(double v) {
   __shared__ double red[32];
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -169,6 +197,63 @@ struct FwdXArgs {
   RhsIO io;
 };
 
+// Stage state with the stage number known at compile time (slopes in registers).
+template <int S>
+__device__ __forceinline__ double stage_value_t(long long i, const Resolved& r) {
+  const double yi = r.y[i];
+  if (S <= 1) return yi;
+  if (S == 2) return yi + r.h * c_a[2][0] * r.k[0][i];
+  double acc = c_a[S][0] * r.k[0][i];
+  if (S != 7) acc += c_a[S][1] * r.k[1][i];
+#pragma unroll
+  for (int j = 2; j < S - 1; ++j) acc += c_a[S][j] * r.k[j][i];
+  return yi + r.h * acc;
+}
+
+// Loads (with the stage combination) the rows of P line pairs into the complex lines
+// of buf, real row in .x, partner row in .y; writes the stage state when asked.  Each
+// thread issues the loads of kUnroll elements before storing any of them.
+template <int S>
+__device__ __forceinline__ void fwd_load(const FwdXArgs& a, const Resolved& r, double2* buf, long long row0) {
+  constexpr int kUnroll = 4;
+  const int M = a.M, T = blockDim.x, tid = threadIdx.x;
+  const int nel = a.P * 2 * M;
+  for (int e0 = tid; e0 < nel; e0 += T * kUnroll) {
+    double v[kUnroll];
+    long long gi[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const int e = e0 + u * T;
+      gi[u] = -1;
+      v[u] = 0.0;
+      if (e < nel) {
+        const int pl = e / (2 * M);
+        const int w = e - pl * 2 * M;
+        const int half = w / M;
+        const int x = w - half * M;
+        const long long g = row0 + 2 * pl + half;
+        if (g < a.nrows) {
+          gi[u] = g * M + x;
+          v[u] = stage_value_t<S>(gi[u], r);
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const int e = e0 + u * T;
+      if (e >= nel) break;
+      if (r.ytemp && gi[u] >= 0) r.ytemp[gi[u]] = v[u];
+      if (a.do_fft) {
+        const int pl = e / (2 * M);
+        const int w = e - pl * 2 * M;
+        const int half = w / M;
+        const int x = w - half * M;
+        reinterpret_cast<double*>(buf)[2 * (pl * M + x) + half] = v[u];
+      }
+    }
+  }
+}
+
 template <int RS>
 __global__ void __launch_bounds__(kMaxBlock, 1) k_fwd_x(FwdXArgs a) {
   extern __shared__ double2 sm[];
@@ -184,21 +269,14 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_fwd_x(FwdXArgs a) {
     buf = sm + M;
   }
   const long long row0 = 2LL * blockIdx.x * a.P;
-  const int nel = a.P * 2 * M;
-  const int s = r.stage;
-  for (int e = tid; e < nel; e += T) {
-    const int pl = e / (2 * M);
-    const int w = e - pl * 2 * M;
-    const int half = w / M;
-    const int x = w - half * M;
-    const long long g = row0 + 2 * pl + half;
-    double v = 0.0;
-    if (g < a.nrows) {
-      const long long i = g * M + x;
-      v = (s >= 2) ? stage_value(s, i, r) : r.y[i];
-      if (r.ytemp) r.ytemp[i] = v;
-    }
-    if (a.do_fft) reinterpret_cast<double*>(buf)[2 * (pl * M + x) + half] = v;
+  switch (r.stage) {
+    case 2: fwd_load<2>(a, r, buf, row0); break;
+    case 3: fwd_load<3>(a, r, buf, row0); break;
+    case 4: fwd_load<4>(a, r, buf, row0); break;
+    case 5: fwd_load<5>(a, r, buf, row0); break;
+    case 6: fwd_load<6>(a, r, buf, row0); break;
+    case 7: fwd_load<7>(a, r, buf, row0); break;
+    default: fwd_load<1>(a, r, buf, row0); break;
   }
   if (!a.do_fft) return;
   __syncthreads();
@@ -245,8 +323,10 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_c2c(C2CArgs a) {
   for (int e = tid; e < nel; e += T) {
     const int c = e % TW, z = e / TW;
     const long long ii = i0 + c;
-    buf[c * LS + z] = ii < a.I ? base[(long long)z * a.I + ii] : make_double2(0.0, 0.0);
+    const bool in = ii < a.I;
+    cp_async16(&buf[c * LS + z], in ? (const void*)&base[(long long)z * a.I + ii] : (const void*)base, in);
   }
+  cp_async_wait_all();
   __syncthreads();
   fft_lines<RS, INV>(buf, LS, TW, a.plan, tw);
   for (int e = tid; e < nel; e += T) {
@@ -258,6 +338,7 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_c2c(C2CArgs a) {
 
 struct MidArgs {
   int L0, I, TW, nsrc, G, GB, ch0;
+  int ent0, nent;  // entries [ent0, ent0+nent) of the launched channels, staged in smem
   int ndim, D1, Mh;
   LinePlan plan;
   const double2* tw;
@@ -275,7 +356,14 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_mid(MidArgs a) {
   double2* tw = sm;
   double2* fb = sm + L0;
   double2* cb = fb + a.nsrc * TW * LS;
+  // channel entries, offsets (relative to ent0) and wavenumbers staged in shared memory
+  ChanEntry* se = reinterpret_cast<ChanEntry*>(cb + a.GB * TW * LS);
+  double* skv = reinterpret_cast<double*>(se + a.nent);
+  int* soff = reinterpret_cast<int*>(skv + a.chan.kv_total);
   for (int t = tid; t < L0; t += T) tw[t] = a.tw[t];
+  for (int t = tid; t < a.nent; t += T) se[t] = a.chan.ent[a.ent0 + t];
+  for (int t = tid; t < a.chan.kv_total; t += T) skv[t] = a.chan.kv[t];
+  for (int t = tid; t <= a.G; t += T) soff[t] = a.chan.off[a.ch0 + t] - a.ent0;
   const long long i0 = (long long)blockIdx.x * TW;
   const int nload = a.nsrc * L0 * TW;
   for (int e = tid; e < nload; e += T) {
@@ -283,9 +371,11 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_mid(MidArgs a) {
     const int z = (e / TW) % L0;
     const int f = e / (TW * L0);
     const long long ii = i0 + c;
-    fb[(f * TW + c) * LS + z] =
-        ii < a.I ? a.Sf[((long long)f * L0 + z) * a.I + ii] : make_double2(0.0, 0.0);
+    const bool in = ii < a.I;
+    cp_async16(&fb[(f * TW + c) * LS + z], in ? (const void*)&a.Sf[((long long)f * L0 + z) * a.I + ii] : (const void*)a.Sf,
+               in);
   }
+  cp_async_wait_all();
   __syncthreads();
   fft_lines<RS, false>(fb, LS, a.nsrc * TW, a.plan, tw);
   for (int g0 = 0; g0 < a.G; g0 += a.GB) {
@@ -298,19 +388,27 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_mid(MidArgs a) {
       const long long ii = i0 + c;
       double2 acc = make_double2(0.0, 0.0);
       if (ii < a.I) {
-        int nidx[3];
-        nidx[0] = z;
+        int nidx[3] = {z, 0, 0};
         if (a.ndim == 3) {
           nidx[1] = (int)(ii / a.Mh);
           nidx[2] = (int)(ii - (long long)nidx[1] * a.Mh);
         } else {
           nidx[1] = (int)ii;
         }
-        const int gch = a.ch0 + g0 + ch;
-        for (int q = a.chan.off[gch]; q < a.chan.off[gch + 1]; ++q) {
-          const ChanEntry en = a.chan.ent[q];
+        double kp[3] = {0.0, 0.0, 0.0}, km[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax) {
+          if (ax < a.ndim) {
+            const int na = nidx[ax], nm = na == 0 ? 0 : a.chan.Ns[ax] - na;
+            kp[ax] = skv[a.chan.kv_off[ax] + na];
+            km[ax] = skv[a.chan.kv_off[ax] + nm];
+          }
+        }
+        const int lch = g0 + ch;
+        for (int q = soff[lch]; q < soff[lch + 1]; ++q) {
+          const ChanEntry en = se[q];
           const double2 u = fb[(en.src * TW + c) * LS + z];
-          const double2 v = apply_entry(en, nidx, a.chan, u);
+          const double2 v = apply_entry_k(en, kp, km, u);
           acc.x += v.x;
           acc.y += v.y;
         }
@@ -464,8 +562,11 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_mid_solve(MidSolveArgs a) {
   for (int e = tid; e < nload; e += T) {
     const int c = e % TW, z = (e / TW) % L0, f = e / (TW * L0);
     const long long ii = i0 + c;
-    fb[(f * TW + c) * LS + z] = ii < a.I ? a.Sf[((long long)f * L0 + z) * a.I + ii] : make_double2(0.0, 0.0);
+    const bool in = ii < a.I;
+    cp_async16(&fb[(f * TW + c) * LS + z], in ? (const void*)&a.Sf[((long long)f * L0 + z) * a.I + ii] : (const void*)a.Sf,
+               in);
   }
+  cp_async_wait_all();
   __syncthreads();
   fft_lines<RS, false>(fb, LS, n * TW, a.plan, tw);
   for (int e = tid; e < L0 * TW; e += T) {
@@ -515,6 +616,7 @@ struct InvXArgs {
   double* Yout;       // Y mode: channel c -> complex block ydst[c]>>1, part ydst[c]&1
   const int* ydst;
   int yplain;         // 1: channel c -> real array Yout[c*N + point]
+  int ch_base;        // first channel row of Sc this launch reads
 };
 
 template <int RS>
@@ -534,45 +636,88 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_inv_x(InvXArgs a) {
   }
   double* phys = reinterpret_cast<double*>(lines + (a.do_fft ? P * np * M : 0));
   const long long r0 = (long long)blockIdx.x * P;
-  if (a.do_fft) {
-    const int nel = P * np * M;
-    for (int e = tid; e < nel; e += T) {
-      const int pr = e / (np * M);
-      const int w = e - pr * np * M;
-      const int cp = w / M;
-      const int kx = w - cp * M;
-      const long long row = r0 + pr;
-      double2 z = make_double2(0.0, 0.0);
-      if (row < a.R) {
-        const int c0 = 2 * cp, c1 = c0 + 1;
-        const bool cj = kx >= Mh;
-        const int kk = cj ? M - kx : kx;
-        double2 A = a.Sc[((long long)c0 * a.R + row) * Mh + kk];
-        double2 B = c1 < a.nch_run ? a.Sc[((long long)c1 * a.R + row) * Mh + kk] : make_double2(0.0, 0.0);
-        if (kx == 0 || 2 * kx == M) {
-          A.y = 0.0;
-          B.y = 0.0;
-        }
-        if (cj) {
-          A.y = -A.y;
-          B.y = -B.y;
-        }
-        z = make_double2(A.x - B.y, A.y + B.x);
-      }
-      lines[(pr * np + cp) * M + kx] = z;
-    }
+  // dictionary tables staged in shared memory (read by every point)
+  DictTerm* sterm = reinterpret_cast<DictTerm*>(phys + (long long)P * n * M);
+  DictFactor* sfac = reinterpret_cast<DictFactor*>(sterm + a.dict.nterms);
+  int* sfb = reinterpret_cast<int*>(sfac + a.dict.nfac);
+  int* sfold = sfb + n + 1;
+  if (!a.Yout) {
+    for (int t = tid; t < a.dict.nterms; t += T) sterm[t] = a.dict.terms[t];
+    for (int t = tid; t < a.dict.nfac; t += T) sfac[t] = a.dict.fac[t];
+    for (int t = tid; t <= n; t += T) sfb[t] = a.dict.field_begin[t];
+    for (int t = tid; t < n; t += T) sfold[t] = a.dict.fold[t];
   }
   if (!a.Yout) {
-    const int nph = P * n * M;
-    for (int e = tid; e < nph; e += T) {
-      const int pr = e / (n * M);
-      const int w = e - pr * n * M;
-      const int fi = w / M;
-      const int x = w - fi * M;
-      const long long row = r0 + pr;
-      phys[(pr * n + fi) * M + x] = row < a.R ? r.u[((long long)fi * a.R + row) * M + x] : 0.0;
+    // physical fields of the P rows: asynchronous copies, 16 bytes where rows allow
+    if ((M & 1) == 0) {
+      const int half = M / 2;
+      const int nph = P * n * half;
+      for (int e = tid; e < nph; e += T) {
+        const int pr = e / (n * half);
+        const int w = e - pr * n * half;
+        const int fi = w / half;
+        const int x2 = (w - fi * half) * 2;
+        const long long row = r0 + pr;
+        const bool in = row < a.R;
+        cp_async16(&phys[(pr * n + fi) * M + x2], in ? (const void*)&r.u[((long long)fi * a.R + row) * M + x2] : (const void*)r.u,
+                   in);
+      }
+    } else {
+      const int nph = P * n * M;
+      for (int e = tid; e < nph; e += T) {
+        const int pr = e / (n * M);
+        const int w = e - pr * n * M;
+        const int fi = w / M;
+        const int x = w - fi * M;
+        const long long row = r0 + pr;
+        phys[(pr * n + fi) * M + x] = row < a.R ? r.u[((long long)fi * a.R + row) * M + x] : 0.0;
+      }
     }
   }
+  if (a.do_fft) {
+    constexpr int kUnroll = 4;
+    const int nel = P * np * M;
+    for (int e0 = tid; e0 < nel; e0 += T * kUnroll) {
+      double2 A[kUnroll], B[kUnroll];
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        const int e = e0 + u * T;
+        A[u] = make_double2(0.0, 0.0);
+        B[u] = make_double2(0.0, 0.0);
+        if (e >= nel) continue;
+        const int pr = e / (np * M);
+        const int w = e - pr * np * M;
+        const int cp = w / M;
+        const int kx = w - cp * M;
+        const long long row = r0 + pr;
+        if (row >= a.R) continue;
+        const int c0 = 2 * cp, c1 = c0 + 1;
+        const int kk = kx >= Mh ? M - kx : kx;
+        A[u] = a.Sc[((long long)(a.ch_base + c0) * a.R + row) * Mh + kk];
+        if (c1 < a.nch_run) B[u] = a.Sc[((long long)(a.ch_base + c1) * a.R + row) * Mh + kk];
+      }
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        const int e = e0 + u * T;
+        if (e >= nel) break;
+        const int pr = e / (np * M);
+        const int w = e - pr * np * M;
+        const int cp = w / M;
+        const int kx = w - cp * M;
+        double2 Av = A[u], Bv = B[u];
+        if (kx == 0 || 2 * kx == M) {
+          Av.y = 0.0;
+          Bv.y = 0.0;
+        }
+        if (kx >= Mh) {
+          Av.y = -Av.y;
+          Bv.y = -Bv.y;
+        }
+        lines[(pr * np + cp) * M + kx] = make_double2(Av.x - Bv.y, Av.y + Bv.x);
+      }
+    }
+  }
+  cp_async_wait_all();
   __syncthreads();
   if (a.do_fft) fft_lines<RS, true>(lines, M, P * np, a.plan, tw);
 
@@ -611,16 +756,16 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_inv_x(InvXArgs a) {
     const double2* ln = lines + (long long)pr * np * M + x;
     for (int i = 0; i < n; ++i) {
       double acc = 0.0;
-      const int fc = D.fold[i];
+      const int fc = sfold[i];
       if (fc >= 0) {
         const double2 z = ln[(fc >> 1) * M];
         acc = (fc & 1) ? z.y : z.x;
       }
-      for (int t = D.field_begin[i]; t < D.field_begin[i + 1]; ++t) {
-        const DictTerm tm = D.terms[t];
+      for (int t = sfb[i]; t < sfb[i + 1]; ++t) {
+        const DictTerm tm = sterm[t];
         double prod = 1.0;
         for (int q = 0; q < tm.nf; ++q) {
-          const DictFactor fc2 = D.fac[tm.off + q];
+          const DictFactor fc2 = sfac[tm.off + q];
           double v;
           if (fc2.q < n) {
             v = ph[fc2.q * M];
@@ -656,6 +801,20 @@ inline int round_up(int v, int m) { return (v + m - 1) / m * m; }
 
 // at most kMaxElems complex values per FFT pass CTA: kMaxBlock threads x kStageElems
 constexpr int kMaxElems = kMaxBlock * kStageElems;
+
+// Complex values a pass CTA aims to transform: 1024 (128 threads at 128 registers, four
+// or more CTAs per SM so one CTA's loads overlap another's FFT stages).  A longer line
+// takes one line per CTA.  RDCU_CTA_ELEMS overrides it (tuning experiments).
+static int cta_elems() {
+  static int v = [] {
+    const char* e = getenv("RDCU_CTA_ELEMS");
+    int x = e ? atoi(e) : 1024;
+    if (x < 256) x = 256;
+    if (x > kMaxElems) x = kMaxElems;
+    return x;
+  }();
+  return v;
+}
 
 int block_for(const LinePlan& p, int elems);
 int stage_threads(const LinePlan& p, int elems) {
@@ -695,13 +854,14 @@ static bool opt_in_smem(const void* func) {
 // Geometry of the inverse x pass for nch_run channels (with or without the
 // physical-field staging): rows per CTA, grid, block and dynamic shared memory.
 static void inv_geometry(int M, int R, int n, int nch_run, bool yout, const LinePlan& plan, PassCfg* c,
-                         int* tw_smem) {
+                         int* tw_smem, size_t extra = 0) {
   const bool spectral = nch_run > 0;
   const int np = (nch_run + 1) / 2;
   const int npm = std::max(1, np);
-  int P = std::max(1, std::min(std::max(1, kMaxElems / 2 / (M * npm)), R / kTargetCtas));
+  int P = std::max(1, std::min(std::max(1, cta_elems() / (M * npm)), R / kTargetCtas));
   auto bytes = [&](int p, bool tws) {
-    return (size_t)((spectral && tws ? M : 0) + (spectral ? p * np * M : 0)) * 16 + (yout ? 0 : (size_t)p * n * M * 8);
+    return (size_t)((spectral && tws ? M : 0) + (spectral ? p * np * M : 0)) * 16 +
+           (yout ? 0 : (size_t)p * n * M * 8 + extra);
   };
   while (P > 1 && bytes(P, true) > kSmemBudget) P /= 2;
   const bool tws = bytes(P, true) <= kSmemBudget;
@@ -724,7 +884,14 @@ ChanTable SpectralPlan::chan_table(const int* off, const ChanEntry* ent, int nch
     t.Ns[a] = Ns[a];
   }
   t.ndim = ndim;
+  t.kv_total = kv_total_;
   return t;
+}
+
+size_t SpectralPlan::dict_smem_bytes() const {
+  const size_t b = (size_t)nterms_dict_ * sizeof(DictTerm) + (size_t)nfac_dict_ * sizeof(DictFactor) +
+                   (size_t)(2 * n + 1) * sizeof(int);
+  return (b + 15) / 16 * 16;
 }
 
 DictTable SpectralPlan::dict_table() const {
@@ -735,6 +902,7 @@ DictTable SpectralPlan::dict_table() const {
   d.fac = d_fac_;
   d.field_begin = d_field_begin_;
   d.fold = d_fold_;
+  d.nfac = nfac_dict_;
   return d;
 }
 
@@ -865,6 +1033,8 @@ bool SpectralPlan::init(int n_, int ndim_, const int* Ns_, const double* Ls_,
   }
   field_begin[n] = (int)dterms.size();
   nterms_dict_ = (int)dterms.size();
+  nfac_dict_ = (int)dfac.size();
+  h_ch_off_ = ch_off;
 
   // Y-mode channels: every block k, real and imaginary part
   std::vector<int> y_off{0};
@@ -877,6 +1047,7 @@ bool SpectralPlan::init(int n_, int ndim_, const int* Ns_, const double* Ls_,
       y_dst.push_back(k * 2 + part);
     }
   ych_ = (int)y_dst.size();
+  h_ych_off_ = y_off;
 
   // wavenumbers exactly as d1 forms them (rdcu.cu:89-95)
   const double PI = 3.14159265358979323846;
@@ -888,6 +1059,7 @@ bool SpectralPlan::init(int n_, int ndim_, const int* Ns_, const double* Ls_,
       kv.push_back(m2 * PI / Ls[a]);
     }
   }
+  kv_total_ = (int)kv.size();
 
   // ---- device tables
   device_bytes = 0;
@@ -921,16 +1093,21 @@ bool SpectralPlan::init(int n_, int ndim_, const int* Ns_, const double* Ls_,
   const int nrows = n * R;
   const int pairs = (nrows + 1) / 2;
   {
-    int P = std::max(1, std::min(std::max(1, kMaxElems / 2 / M), pairs / kTargetCtas));
+    int P = std::max(1, std::min(std::max(1, cta_elems() / M), pairs / kTargetCtas));
     const bool tws = (size_t)(M + P * M) * 16 <= kSmemBudget;
     fwd_.per_cta = P;
     fwd_.grid = (pairs + P - 1) / P;
     fwd_.block = std::min(kMaxBlock, std::max(128, round_up(stage_threads(plan_x_, P * M), 32)));
     fwd_.smem = (size_t)((tws ? M : 0) + P * M) * 16;
   }
+  if (((nch + 1) / 2) * M > kMaxElems) {
+    *msg = "the dictionary needs " + std::to_string(nch) + " inverse channels; with " + std::to_string(M) +
+           " points along the last axis at most " + std::to_string(2 * (kMaxElems / M)) + " are supported";
+    return false;
+  }
   {
     int tws = 0;
-    inv_geometry(M, R, n, nch, false, plan_x_, &inv_, &tws);
+    inv_geometry(M, R, n, nch, false, plan_x_, &inv_, &tws, dict_smem_bytes());
   }
   nparts_max = inv_.grid;
   // Y-mode channel group
@@ -944,13 +1121,16 @@ bool SpectralPlan::init(int n_, int ndim_, const int* Ns_, const double* Ls_,
       if (G == 0) continue;
       int TW = std::max(1, std::min(16, I / kTargetCtas));
       int GB = std::min(G, 4);
-      while (TW > 1 && std::max(n, GB) * TW * L0 > kMaxElems) TW /= 2;
+      while (TW > 1 && std::max(n, GB) * TW * L0 > cta_elems()) TW /= 2;
       while (GB > 1 && std::max(n, GB) * TW * L0 > kMaxElems) --GB;
       if (std::max(n, GB) * TW * L0 > kMaxElems) {
         *msg = "too many fields for one axis-0 pass (n * N0 must be <= " + std::to_string(kMaxElems) + ")";
         return false;
       }
-      auto smem_of = [&](int tw_, int gb) { return (size_t)(L0 + (n + gb) * tw_ * (L0 + 1)) * 16; };
+      // plus the staged channel entries, wavenumbers and offsets (see k_mid)
+      const int nent = which == 0 ? h_ch_off_[nch] : GY;
+      const size_t extra = (size_t)nent * sizeof(ChanEntry) + (size_t)kv_total_ * 8 + (size_t)(G + 1) * 4;
+      auto smem_of = [&](int tw_, int gb) { return (size_t)(L0 + (n + gb) * tw_ * (L0 + 1)) * 16 + extra; };
       while (TW > 1 && smem_of(TW, GB) > kSmemBudget) TW /= 2;
       while (GB > 1 && smem_of(TW, GB) > kSmemBudget) --GB;
       if (smem_of(TW, GB) > 227 * 1024) {
@@ -966,7 +1146,7 @@ bool SpectralPlan::init(int n_, int ndim_, const int* Ns_, const double* Ls_,
     if (ndim == 3) {
       const int La = Ns[1], I1 = Mh;
       int TW = std::min(16, I1);
-      while (TW > 1 && ((size_t)(La + TW * (La + 1)) * 16 > kSmemBudget || TW * La > kMaxElems)) TW /= 2;
+      while (TW > 1 && ((size_t)(La + TW * (La + 1)) * 16 > kSmemBudget || TW * La > cta_elems())) TW /= 2;
       c2c_f_.per_cta = TW;
       c2c_f_.grid = (I1 + TW - 1) / TW;
       c2c_f_.block = std::min(kMaxBlock, std::max(128, round_up(stage_threads(plan_ax_[1], TW * La), 32)));
@@ -1056,8 +1236,9 @@ void SpectralPlan::release() {
 
 // Runs the passes for channels [g_first, g_first+nch_run) of table ct.  When Yout is
 // set the inverse x pass writes channels to Y.dat layout instead of the dictionary.
-cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, int nch_run, int g_first,
-                                        double* Yout, const int* ydst, cudaStream_t st, int yplain) {
+cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, const std::vector<int>& hoff,
+                                        int nch_run, int g_first, double* Yout, const int* ydst, cudaStream_t st,
+                                        int yplain) {
   const bool spectral = nch_run > 0;
   if (spectral && ndim >= 2) {
     const int which = Yout ? 1 : 0;
@@ -1079,10 +1260,13 @@ cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, in
     m.Sc = Sc_;
     m.chan = ct;
     m.io = io;
+    m.ent0 = hoff[g_first];
+    m.nent = hoff[g_first + nch_run] - m.ent0;
+    const size_t smem = c.smem;  // includes the staged tables
     if (plan_is_pow2(plan_ax_[0]))
-      k_mid<kRadixPow2><<<c.grid, c.block, c.smem, st>>>(m);
+      k_mid<kRadixPow2><<<c.grid, c.block, smem, st>>>(m);
     else
-      k_mid<kRadixAll><<<c.grid, c.block, c.smem, st>>>(m);
+      k_mid<kRadixAll><<<c.grid, c.block, smem, st>>>(m);
     RDCU_TRY(cudaGetLastError());
     if (ndim == 3) {
       C2CArgs a{};
@@ -1113,37 +1297,42 @@ cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, in
     k_mult1d<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(m);
     RDCU_TRY(cudaGetLastError());
   }
-  InvXArgs a{};
-  a.M = M;
-  a.Mh = Mh;
-  a.R = R;
-  a.n = n;
-  a.nch_run = nch_run;
-  a.npairs = (nch_run + 1) / 2;
-  a.do_fft = spectral ? 1 : 0;
-  a.N = N;
-  a.plan = plan_x_;
-  a.tw = tw_x_;
-  a.Sc = Sc_;
-  a.dict = dict_table();
-  a.io = io;
-  a.Yout = Yout;
-  a.ydst = ydst;
-  a.yplain = yplain;
-  // geometry for this channel count (the hot path's is the one the error partials
-  // buffer was sized for)
-  PassCfg g;
-  int tws = 0;
-  inv_geometry(M, R, n, nch_run, Yout != nullptr, plan_x_, &g, &tws);
-  a.P = g.per_cta;
-  a.tw_smem = tws;
-  const int grid = g.grid, block = g.block;
-  const size_t smem = g.smem;
-  if (plan_is_pow2(plan_x_))
-    k_inv_x<kRadixPow2><<<grid, block, smem, st>>>(a);
-  else
-    k_inv_x<kRadixAll><<<grid, block, smem, st>>>(a);
-  return cudaGetLastError();
+  // inverse x pass: the dictionary needs every channel of a row in one CTA; the Y.dat
+  // output is launched one channel pair at a time
+  const int step = Yout ? 2 : std::max(1, nch_run);
+  for (int c0 = 0; c0 < std::max(1, nch_run); c0 += step) {
+    const int cnt = spectral ? std::min(step, nch_run - c0) : 0;
+    InvXArgs a{};
+    a.M = M;
+    a.Mh = Mh;
+    a.R = R;
+    a.n = n;
+    a.nch_run = cnt;
+    a.npairs = (cnt + 1) / 2;
+    a.do_fft = spectral ? 1 : 0;
+    a.N = N;
+    a.plan = plan_x_;
+    a.tw = tw_x_;
+    a.Sc = Sc_;
+    a.dict = dict_table();
+    a.io = io;
+    a.Yout = Yout;
+    a.ydst = ydst ? ydst + c0 : nullptr;
+    a.yplain = yplain;
+    a.ch_base = c0;
+    PassCfg g;
+    int tws = 0;
+    inv_geometry(M, R, n, cnt, Yout != nullptr, plan_x_, &g, &tws, Yout ? 0 : dict_smem_bytes());
+    a.P = g.per_cta;
+    a.tw_smem = tws;
+    if (plan_is_pow2(plan_x_))
+      k_inv_x<kRadixPow2><<<g.grid, g.block, g.smem, st>>>(a);
+    else
+      k_inv_x<kRadixAll><<<g.grid, g.block, g.smem, st>>>(a);
+    RDCU_TRY(cudaGetLastError());
+    if (!spectral) break;
+  }
+  return cudaSuccess;
 }
 
 cudaError_t SpectralPlan::run(const RhsIO& io, cudaStream_t st) {
@@ -1184,7 +1373,7 @@ cudaError_t SpectralPlan::run(const RhsIO& io, cudaStream_t st) {
       k_c2c<kRadixAll, false><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(a);
     RDCU_TRY(cudaGetLastError());
   }
-  return launch_passes(io, chan_table(ch_off_, ch_ent_, nch), nch, 0, nullptr, nullptr, st);
+  return launch_passes(io, chan_table(ch_off_, ch_ent_, nch), h_ch_off_, nch, 0, nullptr, nullptr, st);
 }
 
 cudaError_t SpectralPlan::run_Y(const double* y, double* Yout, cudaStream_t st) {
@@ -1228,7 +1417,7 @@ cudaError_t SpectralPlan::run_Y(const double* y, double* Yout, cudaStream_t st) 
   const ChanTable ct = chan_table(ych_off_, ych_ent_, ych_);
   for (int g = 0; g < ych_; g += GY) {
     const int cnt = std::min(GY, ych_ - g);
-    RDCU_TRY(launch_passes(io, ct, cnt, g, Yout, ych_dst_ + g, st));
+    RDCU_TRY(launch_passes(io, ct, h_ych_off_, cnt, g, Yout, ych_dst_ + g, st));
   }
   return cudaSuccess;
 }
@@ -1240,6 +1429,10 @@ bool SpectralPlan::init_precond(int n_, int ndim_, const int* Ns_, const double*
     return false;
   }
   if (!init(n_, ndim_, Ns_, Ls_, std::vector<HostTerm>(), msg)) return false;
+  if (((n + 1) / 2) * M > kMaxElems) {
+    *msg = "preconditioner: too many fields for the last-axis length";
+    return false;
+  }
   std::vector<double> sv, cv;
   const double PI = 3.14159265358979323846;
   for (int a = 0; a < ndim; ++a) {
@@ -1266,7 +1459,7 @@ bool SpectralPlan::init_precond(int n_, int ndim_, const int* Ns_, const double*
     const int I = (ndim == 3) ? Ns[1] * Mh : Mh;
     int TW = std::max(1, std::min(16, I / kTargetCtas));
     auto smem_of = [&](int tw_) { return (size_t)(L0 + n * tw_ * (L0 + 1)) * 16; };
-    while (TW > 1 && (smem_of(TW) > kSmemBudget || n * TW * L0 > kMaxElems)) TW /= 2;
+    while (TW > 1 && (smem_of(TW) > kSmemBudget || n * TW * L0 > cta_elems())) TW /= 2;
     if (smem_of(TW) > 227 * 1024 || n * TW * L0 > kMaxElems) {
       *msg = "grid too large for the preconditioner's axis-0 pass";
       return false;
@@ -1393,6 +1586,7 @@ cudaError_t SpectralPlan::precond(const double* r, double* z, double alpha, cuda
   a.Yout = z;
   a.ydst = nullptr;
   a.yplain = 1;
+  a.ch_base = 0;
   PassCfg g;
   int tws = 0;
   inv_geometry(M, R, n, n, true, plan_x_, &g, &tws);
@@ -1481,11 +1675,14 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
     m.Sc = Sc_;
     m.chan = chan_table(ch_off_, ch_ent_, nch);
     m.io = io;
+    m.ent0 = 0;
+    m.nent = h_ch_off_[nch];
+    const size_t msmem = c.smem;
     RDCU_TRY(timed("mid_axis0", (double)(n + nch) * spec_row, [&]() {
       if (plan_is_pow2(plan_ax_[0]))
-        k_mid<kRadixPow2><<<c.grid, c.block, c.smem, st>>>(m);
+        k_mid<kRadixPow2><<<c.grid, c.block, msmem, st>>>(m);
       else
-        k_mid<kRadixAll><<<c.grid, c.block, c.smem, st>>>(m);
+        k_mid<kRadixAll><<<c.grid, c.block, msmem, st>>>(m);
       return cudaGetLastError();
     }));
     if (ndim == 3) {
@@ -1523,7 +1720,7 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
   a.io = io;
   PassCfg g;
   int tws = 0;
-  inv_geometry(M, R, n, nch, false, plan_x_, &g, &tws);
+  inv_geometry(M, R, n, nch, false, plan_x_, &g, &tws, dict_smem_bytes());
   a.P = g.per_cta;
   a.tw_smem = tws;
   RDCU_TRY(timed("inv_x_dictionary", nch * spec_row + 2.0 * n * arr, [&]() {

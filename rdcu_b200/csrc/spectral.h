@@ -84,6 +84,9 @@ class SpectralPlan {
   int* d_field_begin_ = nullptr;
   int* d_fold_ = nullptr;
   int nterms_dict_ = 0;
+  int nfac_dict_ = 0;
+  int kv_total_ = 0;
+  std::vector<int> h_ch_off_, h_ych_off_;  // host copies of the channel offsets
   // Y-mode channels (every block, real and imaginary part)
   int ych_ = 0;
   int* ych_off_ = nullptr;
@@ -105,8 +108,9 @@ class SpectralPlan {
 
   ChanTable chan_table(const int* off, const ChanEntry* ent, int nch) const;
   DictTable dict_table() const;
-  cudaError_t launch_passes(const RhsIO& io, const ChanTable& ct, int nch_run, int g_first,
-                            double* Yout, const int* ydst, cudaStream_t stream, int yplain = 0);
+  cudaError_t launch_passes(const RhsIO& io, const ChanTable& ct, const std::vector<int>& hoff, int nch_run,
+                            int g_first, double* Yout, const int* ydst, cudaStream_t stream, int yplain = 0);
+  size_t dict_smem_bytes() const;
   cudaError_t launch_forward(const double* y, cudaStream_t stream);
   bool geometry(std::string* msg);
   cudaError_t ensure_channel_capacity(int rows);

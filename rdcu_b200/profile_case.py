@@ -1,0 +1,55 @@
+"""Runs a few DP45 attempts of a CGLE problem and times every pass kernel of one fused
+RHS stage (rdcu_profile_passes); prints one JSON line.  Intended as a small, fixed
+workload for profilers such as Nsight Compute:
+
+    python -m rdcu_b200.profile_case 256,256,128 [--attempts 3] [--reps 2]
+"""
+import argparse
+import json
+
+import numpy as np
+
+from . import Solver, random_ic
+
+
+def cgle_terms(ndim, b=2.0, c=0.8):
+    n = 2
+
+    def dd(i, j):
+        return n + ndim * n + (j * ndim + j) * n + i
+
+    lines = ["1.0,0,0,1"] + ["1.0,0,%d,1" % dd(0, j) for j in range(ndim)]
+    lines += ["-%f,0,%d,1" % (b, dd(1, j)) for j in range(ndim)]
+    lines += ["-1.0,0,0,3", "-1.0,0,0,1,1,2", "1.0,1,1,1"]
+    lines += ["1.0,1,%d,1" % dd(1, j) for j in range(ndim)]
+    lines += ["%f,1,%d,1" % (b, dd(0, j)) for j in range(ndim)]
+    lines += ["-1.0,1,0,2,1,1", "-1.0,1,1,3", "%f,1,0,3" % c, "%f,1,0,1,1,2" % c, "-%f,0,0,2,1,1" % c,
+              "-%f,0,1,3" % c]
+    out = []
+    for s in lines:
+        t = s.split(",")
+        out.append((float(t[0]), [int(x) for x in t[1:]]))
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("grid", help="comma-separated grid sizes, e.g. 256,256,128")
+    ap.add_argument("--length", type=float, default=200.0)
+    ap.add_argument("--attempts", type=int, default=3)
+    ap.add_argument("--reps", type=int, default=2)
+    a = ap.parse_args()
+    Ns = tuple(int(x) for x in a.grid.split(","))
+    s = Solver(2, Ns, (a.length,) * len(Ns), cgle_terms(len(Ns)))
+    N = int(np.prod(Ns))
+    y = random_ic(2, N, 2.0, 0.0, 2)
+    s.set_state(0.0, 1e-3, y.ctypes.data)
+    acc = s.advance(a.attempts)
+    passes = s.profile_passes(reps=a.reps)
+    print(json.dumps({"grid": Ns, "accepted": acc, "passes": [
+        {"name": p[0], "ms": p[1], "bytes": p[2], "GBps": p[2] / (p[1] / 1e3) / 1e9} for p in passes]}))
+    s.close()
+
+
+if __name__ == "__main__":
+    main()
