@@ -184,6 +184,31 @@ int rdcu_random_ic(double *y, int n, long long N, double A, double A0, int seed)
  * device (the reference's cudaMemcpy calls around step_eval, rdcu.cu:277-320). */
 int rdcu_memcpy(rdcu_t *h, void *dst, const void *src, unsigned long long bytes);
 
+/* ---- allocation-free RHS ----------------------------------------------------------
+ * No counterpart in the reference: an addition for callers that cannot allocate device
+ * memory.  Examples: code that runs under a device-memory budget owned by another
+ * framework (a caching allocator that already holds the GPU's memory, so a raw
+ * cudaMalloc fails or fragments it), and real-time loops that cannot afford the device-
+ * wide synchronisation cudaMalloc/cudaFree may imply.
+ *
+ * f = dydt(t, y) of a pseudospectral (RDCU_METHOD_DP45) problem, like rdcu_rhs, with
+ * no handle and no allocation: no cudaMalloc, cudaFree or allocating library call.
+ * Its working memory (FFT tables, dictionary tables, spectra) lives in one file-scope
+ * __device__ array of RDCU_NOALLOC_SCRATCH_BYTES (64 MiB) that every GPU which loads
+ * librdcu holds until the process exits.  Problems that need more scratch than that
+ * (about n_fields * N * 16 bytes for the spectra plus a few KB of tables; a 2-field
+ * grid of up to ~1M points fits) are rejected with RDCU_ERR_UNSUPPORTED.
+ *   - y and f are device pointers of n*N doubles; spec->device selects the GPU.
+ *   - The work is queued on `stream` (a cudaStream_t; NULL for the default stream) and
+ *     the call returns after that stream has finished it.
+ *   - The first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress); make that first call before any stream capture.
+ *   - All calls share the one array, which keeps the last call's contents (each call
+ *     overwrites everything it reads).  Calls that overlap on the GPU race with each
+ *     other: issue them on one stream, or otherwise one at a time. */
+#define RDCU_NOALLOC_SCRATCH_BYTES (64ull << 20)
+int rdcu_rhs_noalloc(const rdcu_spec *spec, const double *y, double *f, void *stream);
+
 /* ---- errors ----------------------------------------------------------------------- */
 const char *rdcu_error_string(int code);
 /* Last error message of the handle (or of the last failed rdcu_create when h is NULL). */

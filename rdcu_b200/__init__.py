@@ -42,8 +42,8 @@ EV_CHECKPOINT = 2
 EXPORTS = [
     "rdcu_create", "rdcu_destroy", "rdcu_set_state", "rdcu_get_state", "rdcu_get_info",
     "rdcu_rhs", "rdcu_jac", "rdcu_step", "rdcu_eval", "rdcu_solve", "rdcu_get_counters",
-    "rdcu_memcpy", "rdcu_advance", "rdcu_random_ic", "rdcu_profile_passes", "rdcu_error_string",
-    "rdcu_last_error",
+    "rdcu_memcpy", "rdcu_advance", "rdcu_random_ic", "rdcu_profile_passes", "rdcu_rhs_noalloc",
+    "rdcu_error_string", "rdcu_last_error",
 ]
 
 
@@ -115,6 +115,7 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
     lib.rdcu_advance.argtypes = [vp, i, d, d, ctypes.POINTER(ctypes.c_longlong)]
     lib.rdcu_random_ic.argtypes = [pd, i, ctypes.c_longlong, d, d, i]
     lib.rdcu_profile_passes.argtypes = [vp, i, ctypes.POINTER(rdcu_pass_timing), i, pi]
+    lib.rdcu_rhs_noalloc.argtypes = [ctypes.POINTER(rdcu_spec), vp, vp, vp]
     lib.rdcu_error_string.argtypes = [i]
     lib.rdcu_error_string.restype = ctypes.c_char_p
     lib.rdcu_last_error.argtypes = [vp]
@@ -148,6 +149,40 @@ def random_ic(n: int, N: int, A: float, A0: float, seed: int):
     if rc != RDCU_OK:
         raise RdcuError(rc, lib.rdcu_last_error(None).decode())
     return y
+
+
+NOALLOC_SCRATCH_BYTES = 64 << 20
+
+
+def rhs_noalloc(n: int, Ns: Sequence[int], Ls: Sequence[float], terms, y_ptr: int, f_ptr: int,
+                stream: int = 0, device: int = 0) -> None:
+    """f = RHS(y) of a pseudospectral problem through rdcu_rhs_noalloc, the entry point
+    that allocates no device memory (for callers that cannot allocate: its scratch is a
+    fixed 64 MiB device array inside the library).  y_ptr, f_ptr: device addresses of
+    n*N doubles; stream: a cudaStream_t handle or 0."""
+    lib = load_library()
+    terms = [(float(C), list(ints)) for C, ints in terms]
+    Cs = (ctypes.c_double * max(1, len(terms)))(*[t[0] for t in terms])
+    nps = (ctypes.c_int * max(1, len(terms)))(*[len(t[1]) for t in terms])
+    lists = [(ctypes.c_int * max(1, len(t[1])))(*t[1]) for t in terms]
+    cps = (ctypes.POINTER(ctypes.c_int) * max(1, len(terms)))(
+        *[ctypes.cast(l, ctypes.POINTER(ctypes.c_int)) for l in lists])
+    spec = rdcu_spec()
+    spec.n = n
+    spec.ndim = len(Ns)
+    for a in range(3):
+        spec.Ns[a] = Ns[a] if a < len(Ns) else 1
+        spec.Ls[a] = Ls[a] if a < len(Ns) else 1.0
+    spec.nterms = len(terms)
+    spec.C = ctypes.cast(Cs, ctypes.POINTER(ctypes.c_double))
+    spec.nprods = ctypes.cast(nps, ctypes.POINTER(ctypes.c_int))
+    spec.c = ctypes.cast(cps, ctypes.POINTER(ctypes.POINTER(ctypes.c_int)))
+    spec.method = METHOD_DP45
+    spec.device = device
+    rc = lib.rdcu_rhs_noalloc(ctypes.byref(spec), ctypes.c_void_p(y_ptr), ctypes.c_void_p(f_ptr),
+                              ctypes.c_void_p(stream) if stream else None)
+    if rc != RDCU_OK:
+        raise RdcuError(rc, lib.rdcu_last_error(None).decode())
 
 
 class Solver:

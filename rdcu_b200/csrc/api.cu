@@ -72,6 +72,10 @@ static int set_err(rdcu_t* h, int code, const std::string& msg) {
   return code;
 }
 
+namespace rdcu {
+void set_thread_error(const std::string& msg) { g_create_error = msg; }
+}  // namespace rdcu
+
 static int cuda_err(rdcu_t* h, cudaError_t e, const char* where) {
   return set_err(h, RDCU_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
 }

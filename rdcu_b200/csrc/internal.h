@@ -126,4 +126,7 @@ struct DP45Bufs {
   double* kbuf[7];
 };
 
+// Sets the message rdcu_last_error(NULL) returns on this thread (api.cu).
+void set_thread_error(const std::string& msg);
+
 }  // namespace rdcu

@@ -916,6 +916,36 @@ static cudaError_t upload(T** dst, const std::vector<T>& v, size_t* bytes) {
   return e;
 }
 
+// Device memory of the plan: cudaMalloc, or the next 256-byte-aligned piece of the arena.
+template <typename T>
+cudaError_t SpectralPlan::dev_alloc(T** p, size_t bytes) {
+  if (!arena_) return cudaMalloc((void**)p, bytes);
+  const size_t off = (arena_->used + 255) / 256 * 256;
+  if (off + bytes > arena_->size) return cudaErrorMemoryAllocation;
+  *p = reinterpret_cast<T*>(arena_->base + off);
+  arena_->used = off + bytes;
+  return cudaSuccess;
+}
+
+template <typename T>
+cudaError_t SpectralPlan::upload_vec(T** dst, const std::vector<T>& v) {
+  if (!arena_) return upload(dst, v, &device_bytes);
+  const size_t b = std::max<size_t>(1, v.size()) * sizeof(T);
+  cudaError_t e = dev_alloc(dst, b);
+  if (e != cudaSuccess) return e;
+  if (!v.empty())
+    e = cudaMemcpyAsync(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, arena_->stream);
+  return e;
+}
+
+bool SpectralPlan::init_in_arena(int n_, int ndim_, const int* Ns_, const double* Ls_,
+                                 const std::vector<HostTerm>& terms, PlanArena* arena, std::string* msg) {
+  release();
+  arena_ = arena;
+  const bool ok = init(n_, ndim_, Ns_, Ls_, terms, msg);
+  return ok;
+}
+
 static ChanEntry entry_for(int k, int n, int ndim, int part, double coef) {
   ChanEntry e{};
   e.src = k % n;
@@ -1072,21 +1102,21 @@ bool SpectralPlan::init(int n_, int ndim_, const int* Ns_, const double* Ls_,
     }
   };
   make_twiddles(M, tw);
-  chk(upload(&tw_x_, tw, &device_bytes));
+  chk(upload_vec(&tw_x_, tw));
   for (int a = 0; a + 1 < ndim; ++a) {
     make_twiddles(Ns[a], tw);
-    chk(upload(&tw_ax_[a], tw, &device_bytes));
+    chk(upload_vec(&tw_ax_[a], tw));
   }
-  chk(upload(&kv_, kv, &device_bytes));
-  chk(upload(&ch_off_, ch_off, &device_bytes));
-  chk(upload(&ch_ent_, ch_ent, &device_bytes));
-  chk(upload(&d_terms_, dterms, &device_bytes));
-  chk(upload(&d_fac_, dfac, &device_bytes));
-  chk(upload(&d_field_begin_, field_begin, &device_bytes));
-  chk(upload(&d_fold_, fold_ch, &device_bytes));
-  chk(upload(&ych_off_, y_off, &device_bytes));
-  chk(upload(&ych_ent_, y_ent, &device_bytes));
-  chk(upload(&ych_dst_, y_dst, &device_bytes));
+  chk(upload_vec(&kv_, kv));
+  chk(upload_vec(&ch_off_, ch_off));
+  chk(upload_vec(&ch_ent_, ch_ent));
+  chk(upload_vec(&d_terms_, dterms));
+  chk(upload_vec(&d_fac_, dfac));
+  chk(upload_vec(&d_field_begin_, field_begin));
+  chk(upload_vec(&d_fold_, fold_ch));
+  chk(upload_vec(&ych_off_, y_off));
+  chk(upload_vec(&ych_ent_, y_ent));
+  chk(upload_vec(&ych_dst_, y_dst));
   if (!ok) return false;
 
   // ---- launch configurations
@@ -1158,13 +1188,13 @@ bool SpectralPlan::init(int n_, int ndim_, const int* Ns_, const double* Ls_,
 
   // ---- buffers
   const size_t srow = (size_t)R * Mh * sizeof(double2);
-  cudaError_t e = cudaMalloc((void**)&Sf_, std::max<size_t>(1, (size_t)n * srow));
+  cudaError_t e = dev_alloc(&Sf_, std::max<size_t>(1, (size_t)n * srow));
   if (e != cudaSuccess) {
     *msg = "out of device memory (spectral buffers)";
     return false;
   }
   device_bytes += (size_t)n * srow;
-  e = cudaMalloc((void**)&Sc_, (size_t)sc_rows_ * srow);
+  e = dev_alloc(&Sc_, (size_t)sc_rows_ * srow);
   if (e != cudaSuccess) {
     *msg = "out of device memory (spectral buffers)";
     return false;
@@ -1211,8 +1241,9 @@ cudaError_t SpectralPlan::ensure_channel_capacity(int rows) {
 void SpectralPlan::release() {
   void* ptrs[] = {tw_x_, tw_ax_[0], tw_ax_[1], tw_ax_[2], kv_, ch_off_, ch_ent_, d_terms_, d_fac_,
                   d_field_begin_, d_fold_, ych_off_, ych_ent_, ych_dst_, Sf_, Sc_, lin_ent_, sinv_, cosv_};
-  for (void* p : ptrs)
-    if (p) cudaFree(p);
+  if (!arena_)  // arena memory belongs to the caller
+    for (void* p : ptrs)
+      if (p) cudaFree(p);
   tw_x_ = nullptr;
   for (auto& t : tw_ax_) t = nullptr;
   kv_ = nullptr;

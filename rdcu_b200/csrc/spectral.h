@@ -33,11 +33,22 @@ struct PassCfg {
   int per_cta = 0;  // pairs / rows / columns per CTA
 };
 
+// Caller-provided device memory for a plan (bump allocation, never freed by the plan).
+struct PlanArena {
+  char* base = nullptr;
+  size_t size = 0;
+  size_t used = 0;
+  cudaStream_t stream = nullptr;  // table uploads are ordered on this stream
+};
+
 class SpectralPlan {
  public:
   // Builds the plan; returns false with msg set when the problem is unsupported.
   bool init(int n, int ndim, const int* Ns, const double* Ls, const std::vector<HostTerm>& terms,
             std::string* msg);
+  // Same plan with every device buffer carved from `arena` instead of cudaMalloc.
+  bool init_in_arena(int n, int ndim, const int* Ns, const double* Ls, const std::vector<HostTerm>& terms,
+                     PlanArena* arena, std::string* msg);
   void release();
   ~SpectralPlan() { release(); }
 
@@ -103,6 +114,11 @@ class SpectralPlan {
   double2* Sf_ = nullptr;  // field half spectra [n][R][Mh]
   double2* Sc_ = nullptr;  // channel half spectra [max(nch, G)][R][Mh]
   int sc_rows_ = 0;        // channel capacity of Sc_
+  PlanArena* arena_ = nullptr;
+  template <typename T>
+  cudaError_t dev_alloc(T** p, size_t bytes);
+  template <typename T>
+  cudaError_t upload_vec(T** dst, const std::vector<T>& v);
   // launch configurations
   PassCfg fwd_, inv_, mid_[2], c2c_f_, c2c_i_, mult_;
 
