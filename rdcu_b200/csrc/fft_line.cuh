@@ -117,14 +117,18 @@ constexpr int kMaxBlock = 512;
 
 // One Stockham stage over nlines lines (stride LS) held in shared memory `buf`.
 // Requires blockDim.x * QMAX >= nlines*L/R; the caller sizes the block for that.
-template <int R, bool INV>
-__device__ __forceinline__ void stockham_stage(double2* buf, int LS, int nlines, int L, int Ns,
-                                               const double2* tw) {
+// POW2: L and Ns are powers of two (index arithmetic by shifts); otherwise the
+// plan's precomputed invariant divisors are used.
+template <int R, bool INV, bool POW2>
+__device__ __forceinline__ void stockham_stage(double2* buf, int LS, int nlines, int L, int Ns, FastDiv dm,
+                                               FastDiv dns, const double2* tw) {
   constexpr int QMAX = (R >= kStageElems) ? 1 : (kStageElems / R);
   const int m = L / R;
   const int nb = nlines * m;
   const int T = blockDim.x;
   const int tstride = L / (Ns * R);
+  const int lm = POW2 ? __ffs(m) - 1 : 0;
+  const int lns = POW2 ? __ffs(Ns) - 1 : 0;
   double2 v[QMAX][R];
   int dst[QMAX];
 #pragma unroll
@@ -132,10 +136,11 @@ __device__ __forceinline__ void stockham_stage(double2* buf, int LS, int nlines,
     const int g = threadIdx.x + q * T;
     dst[q] = -1;
     if (g < nb) {
-      const int line = g / m;
+      const int line = POW2 ? (g >> lm) : fdiv(g, dm);
       const int j = g - line * m;
+      const int jd = POW2 ? (j >> lns) : fdiv(j, dns);
+      const int kk = j - jd * Ns;
       const double2* src = buf + line * LS;
-      const int kk = j % Ns;
       const int tstep = kk * tstride;
 #pragma unroll
       for (int r = 0; r < R; ++r) {
@@ -144,7 +149,7 @@ __device__ __forceinline__ void stockham_stage(double2* buf, int LS, int nlines,
         v[q][r] = x;
       }
       Dft<R, INV>::run(v[q], tw, L);
-      dst[q] = line * LS + (j / Ns) * Ns * R + kk;
+      dst[q] = line * LS + jd * Ns * R + kk;
     }
   }
   __syncthreads();
@@ -176,29 +181,29 @@ __device__ void fft_lines(double2* buf, int LS, int nlines, const LinePlan& p, c
   int Ns = 1;
   for (int s = 0; s < p.nstages; ++s) {
     const int R = p.radix[s];
+    const FastDiv dm = p.div_m[s], dns = p.div_ns[s];
     if (RS == kRadixPow2) {
       if (R == 8)
-        stockham_stage<8, INV>(buf, LS, nlines, p.L, Ns, tw);
+        stockham_stage<8, INV, true>(buf, LS, nlines, p.L, Ns, dm, dns, tw);
       else if (R == 4)
-        stockham_stage<4, INV>(buf, LS, nlines, p.L, Ns, tw);
+        stockham_stage<4, INV, true>(buf, LS, nlines, p.L, Ns, dm, dns, tw);
       else
-        stockham_stage<2, INV>(buf, LS, nlines, p.L, Ns, tw);
+        stockham_stage<2, INV, true>(buf, LS, nlines, p.L, Ns, dm, dns, tw);
     } else {
       switch (R) {
-        case 2: stockham_stage<2, INV>(buf, LS, nlines, p.L, Ns, tw); break;
-        case 3: stockham_stage<3, INV>(buf, LS, nlines, p.L, Ns, tw); break;
-        case 4: stockham_stage<4, INV>(buf, LS, nlines, p.L, Ns, tw); break;
-        case 5: stockham_stage<5, INV>(buf, LS, nlines, p.L, Ns, tw); break;
-        case 7: stockham_stage<7, INV>(buf, LS, nlines, p.L, Ns, tw); break;
-        case 8: stockham_stage<8, INV>(buf, LS, nlines, p.L, Ns, tw); break;
-        case 11: stockham_stage<11, INV>(buf, LS, nlines, p.L, Ns, tw); break;
-        case 13: stockham_stage<13, INV>(buf, LS, nlines, p.L, Ns, tw); break;
+        case 2: stockham_stage<2, INV, false>(buf, LS, nlines, p.L, Ns, dm, dns, tw); break;
+        case 3: stockham_stage<3, INV, false>(buf, LS, nlines, p.L, Ns, dm, dns, tw); break;
+        case 4: stockham_stage<4, INV, false>(buf, LS, nlines, p.L, Ns, dm, dns, tw); break;
+        case 5: stockham_stage<5, INV, false>(buf, LS, nlines, p.L, Ns, dm, dns, tw); break;
+        case 7: stockham_stage<7, INV, false>(buf, LS, nlines, p.L, Ns, dm, dns, tw); break;
+        case 8: stockham_stage<8, INV, false>(buf, LS, nlines, p.L, Ns, dm, dns, tw); break;
+        case 11: stockham_stage<11, INV, false>(buf, LS, nlines, p.L, Ns, dm, dns, tw); break;
+        case 13: stockham_stage<13, INV, false>(buf, LS, nlines, p.L, Ns, dm, dns, tw); break;
         default: break;  // plans only contain the radices above
       }
     }
     Ns *= R;
   }
 }
-
 
 }  // namespace rdcu

@@ -19,7 +19,14 @@ bool make_line_plan(int L, LinePlan* p) {
       rem /= r;
     }
   }
-  return rem == 1;
+  if (rem != 1) return false;
+  int Ns = 1;
+  for (int st = 0; st < p->nstages; ++st) {
+    p->div_m[st] = make_fastdiv((unsigned)(L / p->radix[st]));
+    p->div_ns[st] = make_fastdiv((unsigned)Ns);
+    Ns *= p->radix[st];
+  }
+  return true;
 }
 
 void make_twiddles(int L, std::vector<double2>& tw) {

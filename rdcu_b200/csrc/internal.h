@@ -14,11 +14,36 @@ namespace rdcu {
 constexpr int kMaxStages = 16;
 constexpr int kMaxLine = 4096;  // longest complex line one CTA transforms in shared memory
 
+// Division of 0 <= n < 2^31 by an invariant d >= 1 with a multiply and a shift
+// (Granlund & Montgomery, "Division by invariant integers using multiplication",
+// PLDI 1994): s = ceil(log2 d), m = ceil(2^(31+s) / d) < 2^32, q = (n*m) >> (31+s).
+// Exact because the rounding error of m is below d and n*error < 2^(31+s).
+struct FastDiv {
+  unsigned m;
+  int s;
+};
+inline FastDiv make_fastdiv(unsigned d) {
+  int s = 0;
+  while ((1ull << s) < d) ++s;
+  const unsigned long long num = 1ull << (31 + s);
+  FastDiv f;
+  f.m = (unsigned)((num + d - 1) / d);
+  f.s = s;
+  return f;
+}
+#ifdef __CUDACC__
+__device__ __forceinline__ int fdiv(int n, FastDiv f) {
+  return (int)(((unsigned long long)(unsigned)n * f.m) >> (31 + f.s));
+}
+#endif
+
 // Mixed-radix Stockham plan for one complex line length.
 struct LinePlan {
   int L;
   int nstages;
   int radix[kMaxStages];
+  FastDiv div_m[kMaxStages];   // L / radix[s] (butterflies per line at stage s)
+  FastDiv div_ns[kMaxStages];  // span Ns before stage s
 };
 
 bool make_line_plan(int L, LinePlan* p);

@@ -83,7 +83,7 @@ __device__ __forceinline__ Resolved resolve(const RhsIO& io) {
     r.u = r.y;
     r.f = io.bufs.kbuf[c->k1_buf];
   } else {
-    r.ytemp = io.bufs.ybuf[c->yn_slot];
+    r.ytemp = io.ytemp_out ? io.ytemp_out : io.bufs.ybuf[c->yn_slot];
     r.u = r.ytemp;
     r.f = (io.stage == 7) ? io.bufs.kbuf[c->k7_buf] : io.bufs.kbuf[io.stage - 1];
   }
@@ -94,7 +94,16 @@ __device__ __forceinline__ Resolved resolve(const RhsIO& io) {
 // is y + h*a*k1, later stages y + h*(sum_j a_j k_j); b_2 = 0 (dp45.cu:11), so stage 7
 // does not read k2 (stage_value_t below).
 __device__ __forceinline__ double ipow(double x, int e) {
-  if (e == 0) return 1.0;  // pow(x, 0) == 1 for every x
+  // straight-line products for the small powers dictionaries use (e is warp-uniform)
+  switch (e) {
+    case 1: return x;
+    case 2: return x * x;
+    case 3: return x * x * x;
+    case 0: return 1.0;  // pow(x, 0) == 1 for every x
+    case -1: return 1.0 / x;
+    case -2: return 1.0 / (x * x);
+    default: break;
+  }
   const int a = e < 0 ? -e : e;
   double r = x;
   for (int j = 1; j < a; ++j) r *= x;
@@ -191,6 +200,7 @@ __device__ __forceinline__ double block_sum(double v) {
 // ------------------------------------------------------------------------- kernels
 struct FwdXArgs {
   int M, Mh, nrows, P, do_fft, tw_smem;
+  FastDiv d2M, dM, d2Mh, dMh;  // invariant divisors (prep)
   LinePlan plan;
   const double2* tw;
   double2* S;
@@ -227,9 +237,9 @@ __device__ __forceinline__ void fwd_load(const FwdXArgs& a, const Resolved& r, d
       gi[u] = -1;
       v[u] = 0.0;
       if (e < nel) {
-        const int pl = e / (2 * M);
+        const int pl = fdiv(e, a.d2M);
         const int w = e - pl * 2 * M;
-        const int half = w / M;
+        const int half = fdiv(w, a.dM);
         const int x = w - half * M;
         const long long g = row0 + 2 * pl + half;
         if (g < a.nrows) {
@@ -244,9 +254,9 @@ __device__ __forceinline__ void fwd_load(const FwdXArgs& a, const Resolved& r, d
       if (e >= nel) break;
       if (r.ytemp && gi[u] >= 0) r.ytemp[gi[u]] = v[u];
       if (a.do_fft) {
-        const int pl = e / (2 * M);
+        const int pl = fdiv(e, a.d2M);
         const int w = e - pl * 2 * M;
-        const int half = w / M;
+        const int half = fdiv(w, a.dM);
         const int x = w - half * M;
         reinterpret_cast<double*>(buf)[2 * (pl * M + x) + half] = v[u];
       }
@@ -284,9 +294,9 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_fwd_x(FwdXArgs a) {
   const int Mh = a.Mh;
   const int nout = a.P * 2 * Mh;
   for (int e = tid; e < nout; e += T) {
-    const int pl = e / (2 * Mh);
+    const int pl = fdiv(e, a.d2Mh);
     const int w = e - pl * 2 * Mh;
-    const int half = w / Mh;
+    const int half = fdiv(w, a.dMh);
     const int kx = w - half * Mh;
     const long long g = row0 + 2 * pl + half;
     if (g >= a.nrows) continue;
@@ -303,6 +313,7 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_fwd_x(FwdXArgs a) {
 
 struct C2CArgs {
   int La, I, TW;
+  FastDiv dTW;
   LinePlan plan;
   const double2* tw;
   double2* S;
@@ -321,7 +332,7 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_c2c(C2CArgs a) {
   double2* base = a.S + (long long)blockIdx.y * La * a.I;
   const int nel = La * TW;
   for (int e = tid; e < nel; e += T) {
-    const int c = e % TW, z = e / TW;
+    const int z = fdiv(e, a.dTW), c = e - z * TW;
     const long long ii = i0 + c;
     const bool in = ii < a.I;
     cp_async16(&buf[c * LS + z], in ? (const void*)&base[(long long)z * a.I + ii] : (const void*)base, in);
@@ -330,7 +341,7 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_c2c(C2CArgs a) {
   __syncthreads();
   fft_lines<RS, INV>(buf, LS, TW, a.plan, tw);
   for (int e = tid; e < nel; e += T) {
-    const int c = e % TW, z = e / TW;
+    const int z = fdiv(e, a.dTW), c = e - z * TW;
     const long long ii = i0 + c;
     if (ii < a.I) base[(long long)z * a.I + ii] = buf[c * LS + z];
   }
@@ -338,6 +349,8 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_c2c(C2CArgs a) {
 
 struct MidArgs {
   int L0, I, TW, nsrc, G, GB, ch0;
+  int sorted;      // entries sorted by operator, .pad = local channel (all G <= 4 channels at once)
+  FastDiv dTW, dL0, dMh;
   int ent0, nent;  // entries [ent0, ent0+nent) of the launched channels, staged in smem
   int ndim, D1, Mh;
   LinePlan plan;
@@ -367,9 +380,8 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_mid(MidArgs a) {
   const long long i0 = (long long)blockIdx.x * TW;
   const int nload = a.nsrc * L0 * TW;
   for (int e = tid; e < nload; e += T) {
-    const int c = e % TW;
-    const int z = (e / TW) % L0;
-    const int f = e / (TW * L0);
+    const int q0 = fdiv(e, a.dTW), c = e - q0 * TW;
+    const int f = fdiv(q0, a.dL0), z = q0 - f * L0;
     const long long ii = i0 + c;
     const bool in = ii < a.I;
     cp_async16(&fb[(f * TW + c) * LS + z], in ? (const void*)&a.Sf[((long long)f * L0 + z) * a.I + ii] : (const void*)a.Sf,
@@ -378,20 +390,101 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_mid(MidArgs a) {
   cp_async_wait_all();
   __syncthreads();
   fft_lines<RS, false>(fb, LS, a.nsrc * TW, a.plan, tw);
+  if (a.sorted) {
+    // every channel at once: each distinct operator's multiplier once per point
+    const int npts = L0 * TW;
+    for (int e = tid; e < npts; e += T) {
+      const int z = fdiv(e, a.dTW), c = e - z * TW;
+      const long long ii = i0 + c;
+      double2 acc[4] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0), make_double2(0.0, 0.0),
+                        make_double2(0.0, 0.0)};
+      if (ii < a.I) {
+        int nidx[3] = {z, 0, 0};
+        if (a.ndim == 3) {
+          nidx[1] = fdiv((int)ii, a.dMh);
+          nidx[2] = (int)ii - nidx[1] * a.Mh;
+        } else {
+          nidx[1] = (int)ii;
+        }
+        double kp[3] = {0.0, 0.0, 0.0}, km[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax) {
+          if (ax < a.ndim) {
+            const int na = nidx[ax], nm = na == 0 ? 0 : a.chan.Ns[ax] - na;
+            kp[ax] = skv[a.chan.kv_off[ax] + na];
+            km[ax] = skv[a.chan.kv_off[ax] + nm];
+          }
+        }
+        int last = -1, q = 0;
+        double beta = 0.0;
+        for (int qi = 0; qi < a.nent; ++qi) {
+          const ChanEntry en = se[qi];
+          const int key = en.nax | (en.ax0 << 2) | (en.ax1 << 4) | (en.part << 6);
+          if (key != last) {
+            last = key;
+            double ap = 1.0, am = 1.0;
+            if (en.nax >= 1) {
+              ap *= sel3(kp[0], kp[1], kp[2], en.ax0);
+              am *= sel3(km[0], km[1], km[2], en.ax0);
+            }
+            if (en.nax >= 2) {
+              ap *= sel3(kp[0], kp[1], kp[2], en.ax1);
+              am *= sel3(km[0], km[1], km[2], en.ax1);
+            }
+            const double sgn = (en.nax & 1) ? -1.0 : 1.0;
+            if (en.part == 0) {
+              q = en.nax;
+              beta = 0.5 * (ap + sgn * am);
+            } else {
+              q = en.nax + 3;
+              beta = 0.5 * (ap - sgn * am);
+            }
+          }
+          const double2 u = fb[(en.src * TW + c) * LS + z];
+          const double bc = beta * en.coef;
+          double2 v = make_double2(bc * u.x, bc * u.y);
+          switch (q & 3) {
+            case 1: v = make_double2(-v.y, v.x); break;
+            case 2: v = make_double2(-v.x, -v.y); break;
+            case 3: v = make_double2(v.y, -v.x); break;
+            default: break;
+          }
+#pragma unroll
+          for (int c4 = 0; c4 < 4; ++c4)
+            if (c4 == en.pad) {
+              acc[c4].x += v.x;
+              acc[c4].y += v.y;
+            }
+        }
+      }
+#pragma unroll
+      for (int c4 = 0; c4 < 4; ++c4)
+        if (c4 < a.G) cb[(c4 * TW + c) * LS + z] = acc[c4];
+    }
+    __syncthreads();
+    fft_lines<RS, true>(cb, LS, a.G * TW, a.plan, tw);
+    const int ncomp = a.G * L0 * TW;
+    for (int e = tid; e < ncomp; e += T) {
+      const int q0 = fdiv(e, a.dTW), c = e - q0 * TW;
+      const int ch = fdiv(q0, a.dL0), z = q0 - ch * L0;
+      const long long ii = i0 + c;
+      if (ii < a.I) a.Sc[((long long)ch * L0 + z) * a.I + ii] = cb[(ch * TW + c) * LS + z];
+    }
+    return;
+  }
   for (int g0 = 0; g0 < a.G; g0 += a.GB) {
     const int gc = min(a.GB, a.G - g0);
     const int ncomp = gc * L0 * TW;
     for (int e = tid; e < ncomp; e += T) {
-      const int c = e % TW;
-      const int z = (e / TW) % L0;
-      const int ch = e / (TW * L0);
+      const int q0 = fdiv(e, a.dTW), c = e - q0 * TW;
+      const int ch = fdiv(q0, a.dL0), z = q0 - ch * L0;
       const long long ii = i0 + c;
       double2 acc = make_double2(0.0, 0.0);
       if (ii < a.I) {
         int nidx[3] = {z, 0, 0};
         if (a.ndim == 3) {
-          nidx[1] = (int)(ii / a.Mh);
-          nidx[2] = (int)(ii - (long long)nidx[1] * a.Mh);
+          nidx[1] = fdiv((int)ii, a.dMh);
+          nidx[2] = (int)ii - nidx[1] * a.Mh;
         } else {
           nidx[1] = (int)ii;
         }
@@ -418,9 +511,8 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_mid(MidArgs a) {
     __syncthreads();
     fft_lines<RS, true>(cb, LS, gc * TW, a.plan, tw);
     for (int e = tid; e < ncomp; e += T) {
-      const int c = e % TW;
-      const int z = (e / TW) % L0;
-      const int ch = e / (TW * L0);
+      const int q0 = fdiv(e, a.dTW), c = e - q0 * TW;
+      const int ch = fdiv(q0, a.dL0), z = q0 - ch * L0;
       const long long ii = i0 + c;
       if (ii < a.I) a.Sc[((long long)(g0 + ch) * L0 + z) * a.I + ii] = cb[(ch * TW + c) * LS + z];
     }
@@ -543,6 +635,7 @@ __device__ __forceinline__ void mode_solve(const LinTable& t, const int* nidx, d
 
 struct MidSolveArgs {
   int L0, I, TW, n, ndim, Mh;
+  FastDiv dTW, dL0, dMh;
   LinePlan plan;
   const double2* tw;
   const double2* Sf;
@@ -560,7 +653,8 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_mid_solve(MidSolveArgs a) {
   const long long i0 = (long long)blockIdx.x * TW;
   const int nload = n * L0 * TW;
   for (int e = tid; e < nload; e += T) {
-    const int c = e % TW, z = (e / TW) % L0, f = e / (TW * L0);
+    const int q0 = fdiv(e, a.dTW), c = e - q0 * TW;
+    const int f = fdiv(q0, a.dL0), z = q0 - f * L0;
     const long long ii = i0 + c;
     const bool in = ii < a.I;
     cp_async16(&fb[(f * TW + c) * LS + z], in ? (const void*)&a.Sf[((long long)f * L0 + z) * a.I + ii] : (const void*)a.Sf,
@@ -570,14 +664,14 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_mid_solve(MidSolveArgs a) {
   __syncthreads();
   fft_lines<RS, false>(fb, LS, n * TW, a.plan, tw);
   for (int e = tid; e < L0 * TW; e += T) {
-    const int c = e % TW, z = e / TW;
+    const int z = fdiv(e, a.dTW), c = e - z * TW;
     const long long ii = i0 + c;
     if (ii >= a.I) continue;
     int nidx[3];
     nidx[0] = z;
     if (a.ndim == 3) {
-      nidx[1] = (int)(ii / a.Mh);
-      nidx[2] = (int)(ii - (long long)nidx[1] * a.Mh);
+      nidx[1] = fdiv((int)ii, a.dMh);
+      nidx[2] = (int)ii - nidx[1] * a.Mh;
     } else {
       nidx[1] = (int)ii;
     }
@@ -589,7 +683,8 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_mid_solve(MidSolveArgs a) {
   __syncthreads();
   fft_lines<RS, true>(fb, LS, n * TW, a.plan, tw);
   for (int e = tid; e < nload; e += T) {
-    const int c = e % TW, z = (e / TW) % L0, f = e / (TW * L0);
+    const int q0 = fdiv(e, a.dTW), c = e - q0 * TW;
+    const int f = fdiv(q0, a.dL0), z = q0 - f * L0;
     const long long ii = i0 + c;
     if (ii < a.I) a.Sc[((long long)f * L0 + z) * a.I + ii] = fb[(f * TW + c) * LS + z];
   }
@@ -607,6 +702,7 @@ __global__ void k_mult1d_solve(int Mh, int n, const double2* Sf, double2* Sc, Li
 
 struct InvXArgs {
   int M, Mh, R, P, n, nch_run, npairs, do_fft, tw_smem;
+  FastDiv dM, dnpM, dnhalf, dhalf, dnM, dncM;
   long long N;
   LinePlan plan;
   const double2* tw;
@@ -653,9 +749,9 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_inv_x(InvXArgs a) {
       const int half = M / 2;
       const int nph = P * n * half;
       for (int e = tid; e < nph; e += T) {
-        const int pr = e / (n * half);
+        const int pr = fdiv(e, a.dnhalf);
         const int w = e - pr * n * half;
-        const int fi = w / half;
+        const int fi = fdiv(w, a.dhalf);
         const int x2 = (w - fi * half) * 2;
         const long long row = r0 + pr;
         const bool in = row < a.R;
@@ -665,9 +761,9 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_inv_x(InvXArgs a) {
     } else {
       const int nph = P * n * M;
       for (int e = tid; e < nph; e += T) {
-        const int pr = e / (n * M);
+        const int pr = fdiv(e, a.dnM);
         const int w = e - pr * n * M;
-        const int fi = w / M;
+        const int fi = fdiv(w, a.dM);
         const int x = w - fi * M;
         const long long row = r0 + pr;
         phys[(pr * n + fi) * M + x] = row < a.R ? r.u[((long long)fi * a.R + row) * M + x] : 0.0;
@@ -685,9 +781,9 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_inv_x(InvXArgs a) {
         A[u] = make_double2(0.0, 0.0);
         B[u] = make_double2(0.0, 0.0);
         if (e >= nel) continue;
-        const int pr = e / (np * M);
+        const int pr = fdiv(e, a.dnpM);
         const int w = e - pr * np * M;
-        const int cp = w / M;
+        const int cp = fdiv(w, a.dM);
         const int kx = w - cp * M;
         const long long row = r0 + pr;
         if (row >= a.R) continue;
@@ -700,9 +796,9 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_inv_x(InvXArgs a) {
       for (int u = 0; u < kUnroll; ++u) {
         const int e = e0 + u * T;
         if (e >= nel) break;
-        const int pr = e / (np * M);
+        const int pr = fdiv(e, a.dnpM);
         const int w = e - pr * np * M;
-        const int cp = w / M;
+        const int cp = fdiv(w, a.dM);
         const int kx = w - cp * M;
         double2 Av = A[u], Bv = B[u];
         if (kx == 0 || 2 * kx == M) {
@@ -724,9 +820,9 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_inv_x(InvXArgs a) {
   if (a.Yout) {
     const int nel = P * a.nch_run * M;
     for (int e = tid; e < nel; e += T) {
-      const int pr = e / (a.nch_run * M);
+      const int pr = fdiv(e, a.dncM);
       const int w = e - pr * a.nch_run * M;
-      const int c = w / M;
+      const int c = fdiv(w, a.dM);
       const int x = w - c * M;
       const long long row = r0 + pr;
       if (row >= a.R) continue;
@@ -748,7 +844,7 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_inv_x(InvXArgs a) {
   double err2 = 0.0;
   const int npts = P * M;
   for (int e = tid; e < npts; e += T) {
-    const int pr = e / M;
+    const int pr = fdiv(e, a.dM);
     const int x = e - pr * M;
     const long long row = r0 + pr;
     if (row >= a.R) continue;
@@ -798,6 +894,34 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_inv_x(InvXArgs a) {
 }
 
 inline int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+// Invariant divisors of each pass's index arithmetic, filled before every launch.
+void prep(FwdXArgs& a) {
+  a.d2M = make_fastdiv(2 * a.M);
+  a.dM = make_fastdiv(a.M);
+  a.d2Mh = make_fastdiv(2 * a.Mh);
+  a.dMh = make_fastdiv(a.Mh);
+}
+void prep(C2CArgs& a) { a.dTW = make_fastdiv(a.TW); }
+void prep(MidArgs& a) {
+  a.dTW = make_fastdiv(a.TW);
+  a.dL0 = make_fastdiv(a.L0);
+  a.dMh = make_fastdiv(a.Mh > 0 ? a.Mh : 1);
+}
+void prep(MidSolveArgs& a) {
+  a.dTW = make_fastdiv(a.TW);
+  a.dL0 = make_fastdiv(a.L0);
+  a.dMh = make_fastdiv(a.Mh > 0 ? a.Mh : 1);
+}
+void prep(InvXArgs& a) {
+  const int half = a.M / 2;
+  a.dM = make_fastdiv(a.M);
+  a.dnpM = make_fastdiv(std::max(1, a.npairs) * a.M);
+  a.dnhalf = make_fastdiv(std::max(1, a.n * half));
+  a.dhalf = make_fastdiv(std::max(1, half));
+  a.dnM = make_fastdiv(a.n * a.M);
+  a.dncM = make_fastdiv(std::max(1, a.nch_run) * a.M);
+}
 
 // at most kMaxElems complex values per FFT pass CTA: kMaxBlock threads x kStageElems
 constexpr int kMaxElems = kMaxBlock * kStageElems;
@@ -916,6 +1040,24 @@ static cudaError_t upload(T** dst, const std::vector<T>& v, size_t* bytes) {
   return e;
 }
 
+// Channel entries in operator order with the local channel index in .pad (the k_mid
+// fast path computes each distinct multiplier once per point).
+static std::vector<ChanEntry> sorted_entries(const std::vector<ChanEntry>& ent, const std::vector<int>& off, int nch) {
+  std::vector<ChanEntry> srt;
+  for (int c = 0; c < nch; ++c)
+    for (int q = off[c]; q < off[c + 1]; ++q) {
+      ChanEntry e = ent[q];
+      e.pad = c;
+      srt.push_back(e);
+    }
+  std::stable_sort(srt.begin(), srt.end(), [](const ChanEntry& x, const ChanEntry& y) {
+    const int kx = x.nax | (x.ax0 << 2) | (x.ax1 << 4) | (x.part << 6);
+    const int ky = y.nax | (y.ax0 << 2) | (y.ax1 << 4) | (y.part << 6);
+    return kx < ky;
+  });
+  return srt;
+}
+
 // Device memory of the plan: cudaMalloc, or the next 256-byte-aligned piece of the arena.
 template <typename T>
 cudaError_t SpectralPlan::dev_alloc(T** p, size_t bytes) {
@@ -998,7 +1140,10 @@ bool SpectralPlan::init(int n_, int ndim_, const int* Ns_, const double* Ls_,
   std::vector<int> needY;  // Y indices (>= n) needed physically
   struct TermOut { int field; double C; std::vector<std::pair<int, int>> fac; };
   std::vector<TermOut> kept;
-  for (const auto& t : terms) {
+  std::vector<std::vector<int>> fold_term(n);  // term index of each fold entry
+  std::vector<int> kept_term;                   // term index of each kept term
+  for (size_t ti = 0; ti < terms.size(); ++ti) {
+    const auto& t = terms[ti];
     const int field = t.ints.empty() ? 0 : t.ints[0];
     if (field < 0 || field >= n) {
       *msg = "coupling term field " + std::to_string(field) + " out of range";
@@ -1017,36 +1162,61 @@ bool SpectralPlan::init(int n_, int ndim_, const int* Ns_, const double* Ls_,
     }
     if (fac.size() == 1 && fac[0].second == 1 && fac[0].first >= n) {
       fold[field].push_back(entry_for(fac[0].first, n, ndim, 0, t.C * invN));
+      fold_term[field].push_back((int)ti);
       continue;
     }
     for (auto& f : fac)
       if (f.first >= n && std::find(needY.begin(), needY.end(), f.first) == needY.end()) needY.push_back(f.first);
     kept.push_back({field, t.C, fac});
+    kept_term.push_back((int)ti);
   }
   std::sort(needY.begin(), needY.end());
   std::vector<int> ch_off{0};
   std::vector<ChanEntry> ch_ent;
   std::vector<int> fold_ch(n, -1);
   nch = 0;
-  for (int i = 0; i < n; ++i) {
-    if (fold[i].empty()) continue;
-    fold_ch[i] = nch++;
-    for (auto& e : fold[i]) ch_ent.push_back(e);
-    ch_off.push_back((int)ch_ent.size());
-  }
+  h_ent_term_.clear();
   std::vector<int> ych_of(nY * n, -1);
-  for (int k : needY) {
-    ych_of[k] = nch++;
-    ch_ent.push_back(entry_for(k, n, ndim, 0, invN));
-    ch_off.push_back((int)ch_ent.size());
+  if (explicit_channels_) {
+    // a linear operator given channel by channel (adjoint passes): no dictionary
+    for (auto& chn : *explicit_channels_) {
+      for (ChanEntry e : chn) {
+        e.coef *= invN;
+        ch_ent.push_back(e);
+        h_ent_term_.push_back(-1);
+      }
+      ch_off.push_back((int)ch_ent.size());
+      ++nch;
+    }
+    kept.clear();
+    kept_term.clear();
+  } else {
+    for (int i = 0; i < n; ++i) {
+      if (fold[i].empty()) continue;
+      fold_ch[i] = nch++;
+      for (size_t q = 0; q < fold[i].size(); ++q) {
+        ch_ent.push_back(fold[i][q]);
+        h_ent_term_.push_back(fold_term[i][q]);
+      }
+      ch_off.push_back((int)ch_ent.size());
+    }
+    for (int k : needY) {
+      ych_of[k] = nch++;
+      ch_ent.push_back(entry_for(k, n, ndim, 0, invN));
+      h_ent_term_.push_back(-1);
+      ch_off.push_back((int)ch_ent.size());
+    }
   }
   std::vector<DictTerm> dterms;
   std::vector<DictFactor> dfac;
   std::vector<int> field_begin(n + 1, 0);
+  h_dict_term_.clear();
   for (int i = 0; i < n; ++i) {
     field_begin[i] = (int)dterms.size();
-    for (auto& t : kept) {
+    for (size_t kt = 0; kt < kept.size(); ++kt) {
+      auto& t = kept[kt];
       if (t.field != i) continue;
+      h_dict_term_.push_back(kept_term[kt]);
       DictTerm dt{};
       dt.field = i;
       dt.C = t.C;
@@ -1065,6 +1235,9 @@ bool SpectralPlan::init(int n_, int ndim_, const int* Ns_, const double* Ls_,
   nterms_dict_ = (int)dterms.size();
   nfac_dict_ = (int)dfac.size();
   h_ch_off_ = ch_off;
+  h_ch_ent_ = ch_ent;
+  h_dterms_ = dterms;
+  inv_n_ = invN;
 
   // Y-mode channels: every block k, real and imaginary part
   std::vector<int> y_off{0};
@@ -1110,6 +1283,8 @@ bool SpectralPlan::init(int n_, int ndim_, const int* Ns_, const double* Ls_,
   chk(upload_vec(&kv_, kv));
   chk(upload_vec(&ch_off_, ch_off));
   chk(upload_vec(&ch_ent_, ch_ent));
+  // operator-sorted copy of the hot entries with the local channel in .pad
+  if (nch >= 1 && nch <= 4) chk(upload_vec(&ch_sorted_, sorted_entries(ch_ent, ch_off, nch)));
   chk(upload_vec(&d_terms_, dterms));
   chk(upload_vec(&d_fac_, dfac));
   chk(upload_vec(&d_field_begin_, field_begin));
@@ -1239,6 +1414,8 @@ cudaError_t SpectralPlan::ensure_channel_capacity(int rows) {
 }
 
 void SpectralPlan::release() {
+  if (ch_sorted_ && !arena_) cudaFree(ch_sorted_);
+  ch_sorted_ = nullptr;
   void* ptrs[] = {tw_x_, tw_ax_[0], tw_ax_[1], tw_ax_[2], kv_, ch_off_, ch_ent_, d_terms_, d_fac_,
                   d_field_begin_, d_fold_, ych_off_, ych_ent_, ych_dst_, Sf_, Sc_, lin_ent_, sinv_, cosv_};
   if (!arena_)  // arena memory belongs to the caller
@@ -1272,7 +1449,7 @@ cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, co
                                         int yplain) {
   const bool spectral = nch_run > 0;
   if (spectral && ndim >= 2) {
-    const int which = Yout ? 1 : 0;
+    const int which = (ct.ent == ch_ent_) ? 0 : 1;  // hot table or the Y-block table
     const PassCfg& c = mid_[which];
     MidArgs m{};
     m.L0 = Ns[0];
@@ -1293,7 +1470,12 @@ cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, co
     m.io = io;
     m.ent0 = hoff[g_first];
     m.nent = hoff[g_first + nch_run] - m.ent0;
+    if (ct.ent == ch_ent_ && ch_sorted_ && nch_run <= m.GB && g_first == 0) {
+      m.sorted = 1;
+      m.chan.ent = ch_sorted_;  // staged into shared memory in operator order
+    }
     const size_t smem = c.smem;  // includes the staged tables
+    prep(m);
     if (plan_is_pow2(plan_ax_[0]))
       k_mid<kRadixPow2><<<c.grid, c.block, smem, st>>>(m);
     else
@@ -1309,6 +1491,7 @@ cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, co
       a.S = Sc_;
       a.io = io;
       dim3 grid(c2c_i_.grid, nch_run * Ns[0]);
+      prep(a);
       if (plan_is_pow2(plan_ax_[1]))
         k_c2c<kRadixPow2, true><<<grid, c2c_i_.block, c2c_i_.smem, st>>>(a);
       else
@@ -1347,7 +1530,7 @@ cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, co
     a.Sc = Sc_;
     a.dict = dict_table();
     a.io = io;
-    a.Yout = Yout;
+    a.Yout = (Yout && yplain) ? Yout + (long long)c0 * N : Yout;
     a.ydst = ydst ? ydst + c0 : nullptr;
     a.yplain = yplain;
     a.ch_base = c0;
@@ -1356,6 +1539,7 @@ cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, co
     inv_geometry(M, R, n, cnt, Yout != nullptr, plan_x_, &g, &tws, Yout ? 0 : dict_smem_bytes());
     a.P = g.per_cta;
     a.tw_smem = tws;
+    prep(a);
     if (plan_is_pow2(plan_x_))
       k_inv_x<kRadixPow2><<<g.grid, g.block, g.smem, st>>>(a);
     else
@@ -1382,6 +1566,7 @@ cudaError_t SpectralPlan::run(const RhsIO& io, cudaStream_t st) {
     a.S = Sf_;
     a.io = io;
     const size_t smem = spectral ? fwd_.smem : 0;
+    prep(a);
     if (plan_is_pow2(plan_x_))
       k_fwd_x<kRadixPow2><<<fwd_.grid, fwd_.block, smem, st>>>(a);
     else
@@ -1398,6 +1583,7 @@ cudaError_t SpectralPlan::run(const RhsIO& io, cudaStream_t st) {
     a.S = Sf_;
     a.io = io;
     dim3 grid(c2c_f_.grid, n * Ns[0]);
+    prep(a);
     if (plan_is_pow2(plan_ax_[1]))
       k_c2c<kRadixPow2, false><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(a);
     else
@@ -1424,6 +1610,7 @@ cudaError_t SpectralPlan::run_Y(const double* y, double* Yout, cudaStream_t st) 
   a.tw = tw_x_;
   a.S = Sf_;
   a.io = io;
+  prep(a);
   if (plan_is_pow2(plan_x_))
     k_fwd_x<kRadixPow2><<<fwd_.grid, fwd_.block, fwd_.smem, st>>>(a);
   else
@@ -1439,6 +1626,7 @@ cudaError_t SpectralPlan::run_Y(const double* y, double* Yout, cudaStream_t st) 
     c.S = Sf_;
     c.io = io;
     dim3 grid(c2c_f_.grid, n * Ns[0]);
+    prep(c);
     if (plan_is_pow2(plan_ax_[1]))
       k_c2c<kRadixPow2, false><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(c);
     else
@@ -1522,6 +1710,7 @@ cudaError_t SpectralPlan::launch_forward(const double* y, cudaStream_t st) {
   a.tw = tw_x_;
   a.S = Sf_;
   a.io = io;
+  prep(a);
   if (plan_is_pow2(plan_x_))
     k_fwd_x<kRadixPow2><<<fwd_.grid, fwd_.block, fwd_.smem, st>>>(a);
   else
@@ -1537,6 +1726,7 @@ cudaError_t SpectralPlan::launch_forward(const double* y, cudaStream_t st) {
     c.S = Sf_;
     c.io = io;
     dim3 grid(c2c_f_.grid, n * Ns[0]);
+    prep(c);
     if (plan_is_pow2(plan_ax_[1]))
       k_c2c<kRadixPow2, false><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(c);
     else
@@ -1574,6 +1764,7 @@ cudaError_t SpectralPlan::precond(const double* r, double* z, double alpha, cuda
     m.Sf = Sf_;
     m.Sc = Sc_;
     m.lin = lt;
+    prep(m);
     if (plan_is_pow2(plan_ax_[0]))
       k_mid_solve<kRadixPow2><<<midsolve_.grid, midsolve_.block, midsolve_.smem, st>>>(m);
     else
@@ -1589,6 +1780,7 @@ cudaError_t SpectralPlan::precond(const double* r, double* z, double alpha, cuda
       a.S = Sc_;
       a.io = RhsIO{};
       dim3 grid(c2c_i_.grid, n * Ns[0]);
+      prep(a);
       if (plan_is_pow2(plan_ax_[1]))
         k_c2c<kRadixPow2, true><<<grid, c2c_i_.block, c2c_i_.smem, st>>>(a);
       else
@@ -1623,6 +1815,7 @@ cudaError_t SpectralPlan::precond(const double* r, double* z, double alpha, cuda
   inv_geometry(M, R, n, n, true, plan_x_, &g, &tws);
   a.P = g.per_cta;
   a.tw_smem = tws;
+  prep(a);
   if (plan_is_pow2(plan_x_))
     k_inv_x<kRadixPow2><<<g.grid, g.block, g.smem, st>>>(a);
   else
@@ -1663,6 +1856,7 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
   fa.S = Sf_;
   fa.io = io;
   RDCU_TRY(timed("fwd_x", n * ((1 + nk) * arr + (s >= 2 ? arr : 0) + spec_row), [&]() {
+    prep(fa);
     if (plan_is_pow2(plan_x_))
       k_fwd_x<kRadixPow2><<<fwd_.grid, fwd_.block, fwd_.smem, st>>>(fa);
     else
@@ -1680,6 +1874,7 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
     c.io = io;
     dim3 grid(c2c_f_.grid, n * Ns[0]);
     RDCU_TRY(timed("c2c_axis1_fwd", 2.0 * n * spec_row, [&]() {
+      prep(c);
       if (plan_is_pow2(plan_ax_[1]))
         k_c2c<kRadixPow2, false><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(c);
       else
@@ -1708,8 +1903,13 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
     m.io = io;
     m.ent0 = 0;
     m.nent = h_ch_off_[nch];
+    if (ch_sorted_ && nch <= m.GB) {
+      m.sorted = 1;
+      m.chan.ent = ch_sorted_;
+    }
     const size_t msmem = c.smem;
     RDCU_TRY(timed("mid_axis0", (double)(n + nch) * spec_row, [&]() {
+      prep(m);
       if (plan_is_pow2(plan_ax_[0]))
         k_mid<kRadixPow2><<<c.grid, c.block, msmem, st>>>(m);
       else
@@ -1727,6 +1927,7 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
       a.io = io;
       dim3 grid(c2c_i_.grid, nch * Ns[0]);
       RDCU_TRY(timed("c2c_axis1_inv", 2.0 * nch * spec_row, [&]() {
+        prep(a);
         if (plan_is_pow2(plan_ax_[1]))
           k_c2c<kRadixPow2, true><<<grid, c2c_i_.block, c2c_i_.smem, st>>>(a);
         else
@@ -1755,6 +1956,7 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
   a.P = g.per_cta;
   a.tw_smem = tws;
   RDCU_TRY(timed("inv_x_dictionary", nch * spec_row + 2.0 * n * arr, [&]() {
+    prep(a);
     if (plan_is_pow2(plan_x_))
       k_inv_x<kRadixPow2><<<g.grid, g.block, g.smem, st>>>(a);
     else
@@ -1764,6 +1966,39 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return cudaSuccess;
+}
+
+bool SpectralPlan::init_linear(int n_in, int ndim_, const int* Ns_, const double* Ls_,
+                               const std::vector<std::vector<ChanEntry>>& channels, std::string* msg) {
+  explicit_channels_ = &channels;
+  const bool ok = init(n_in, ndim_, Ns_, Ls_, std::vector<HostTerm>(), msg);
+  explicit_channels_ = nullptr;
+  return ok;
+}
+
+cudaError_t SpectralPlan::set_coefficients(const std::vector<double>& C) {
+  std::vector<ChanEntry> ent = h_ch_ent_;
+  for (size_t q = 0; q < ent.size(); ++q)
+    if (h_ent_term_[q] >= 0) ent[q].coef = C[h_ent_term_[q]] * inv_n_;
+  std::vector<DictTerm> dt = h_dterms_;
+  for (size_t q = 0; q < dt.size(); ++q) dt[q].C = C[h_dict_term_[q]];
+  if (!ent.empty()) RDCU_TRY(cudaMemcpy(ch_ent_, ent.data(), ent.size() * sizeof(ChanEntry), cudaMemcpyHostToDevice));
+  if (ch_sorted_ && nch >= 1 && nch <= 4) {
+    const std::vector<ChanEntry> srt = sorted_entries(ent, h_ch_off_, nch);
+    RDCU_TRY(cudaMemcpy(ch_sorted_, srt.data(), srt.size() * sizeof(ChanEntry), cudaMemcpyHostToDevice));
+  }
+  if (!dt.empty()) RDCU_TRY(cudaMemcpy(d_terms_, dt.data(), dt.size() * sizeof(DictTerm), cudaMemcpyHostToDevice));
+  h_ch_ent_ = ent;
+  h_dterms_ = dt;
+  return cudaSuccess;
+}
+
+cudaError_t SpectralPlan::run_linear(const double* in, double* out, cudaStream_t st) {
+  RDCU_TRY(launch_forward(in, st));
+  RhsIO io{};
+  io.mode = 0;
+  io.y = in;
+  return launch_passes(io, chan_table(ch_off_, ch_ent_, nch), h_ch_off_, nch, 0, out, nullptr, st, 1);
 }
 
 }  // namespace rdcu

@@ -25,6 +25,7 @@ struct RhsIO {
   DP45Bufs bufs{};            // mode 1
   DP45Ctl* ctl = nullptr;     // mode 1
   double* err_part = nullptr; // mode 1, stage 7: per-CTA partial sums of err^2
+  double* ytemp_out = nullptr;// mode 1, stages >= 2: write the stage state here instead of its slot
 };
 
 struct PassCfg {
@@ -46,6 +47,14 @@ class SpectralPlan {
   // Builds the plan; returns false with msg set when the problem is unsupported.
   bool init(int n, int ndim, const int* Ns, const double* Ls, const std::vector<HostTerm>& terms,
             std::string* msg);
+  // A linear operator instead of a dictionary: output channel c = sum over its entries
+  // of coef * multiplier(op) applied to input field src (coefficients unscaled).
+  bool init_linear(int n_in, int ndim, const int* Ns, const double* Ls,
+                   const std::vector<std::vector<ChanEntry>>& channels, std::string* msg);
+  // out[c*N + point] = channel c of the linear operator applied to in (n_in fields).
+  cudaError_t run_linear(const double* in, double* out, cudaStream_t stream);
+  // New coefficients C[term] for the dictionary (same structure as at init).
+  cudaError_t set_coefficients(const std::vector<double>& C);
   // Same plan with every device buffer carved from `arena` instead of cudaMalloc.
   bool init_in_arena(int n, int ndim, const int* Ns, const double* Ls, const std::vector<HostTerm>& terms,
                      PlanArena* arena, std::string* msg);
@@ -90,6 +99,7 @@ class SpectralPlan {
   // hot-path channels and dictionary
   int* ch_off_ = nullptr;
   ChanEntry* ch_ent_ = nullptr;
+  ChanEntry* ch_sorted_ = nullptr;  // hot entries in operator order (mid pass fast path)
   DictTerm* d_terms_ = nullptr;
   DictFactor* d_fac_ = nullptr;
   int* d_field_begin_ = nullptr;
@@ -115,6 +125,12 @@ class SpectralPlan {
   double2* Sc_ = nullptr;  // channel half spectra [max(nch, G)][R][Mh]
   int sc_rows_ = 0;        // channel capacity of Sc_
   PlanArena* arena_ = nullptr;
+  const std::vector<std::vector<ChanEntry>>* explicit_channels_ = nullptr;
+  std::vector<ChanEntry> h_ch_ent_;
+  std::vector<int> h_ent_term_;   // term index of each hot entry (-1: not a term coefficient)
+  std::vector<DictTerm> h_dterms_;
+  std::vector<int> h_dict_term_;  // term index of each dictionary term
+  double inv_n_ = 1.0;
   template <typename T>
   cudaError_t dev_alloc(T** p, size_t bytes);
   template <typename T>
