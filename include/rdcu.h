@@ -184,6 +184,35 @@ int rdcu_random_ic(double *y, int n, long long N, double A, double A0, int seed)
  * device (the reference's cudaMemcpy calls around step_eval, rdcu.cu:277-320). */
 int rdcu_memcpy(rdcu_t *h, void *dst, const void *src, unsigned long long bytes);
 
+/* ---- coefficients and the discrete adjoint ----------------------------------------
+ * No counterpart in the reference (its coefficients are fixed when FILEBASEcoupling.dat
+ * is read, rdcu.cu:606-662, and it has no gradients).
+ *
+ * rdcu_set_coefficients: replaces the coefficient of every coupling term (C[nterms], in
+ * the order of rdcu_spec.c) without rebuilding the plan.  Pseudospectral handles only;
+ * call rdcu_set_state afterwards (the cached slope k1 of the old coefficients is
+ * dropped). */
+int rdcu_set_coefficients(rdcu_t *h, const double *C);
+
+/* rdcu_adjoint_forward: the DP45 map y0 -> yT over the step sizes hs[0..nsteps) (host
+ * array; one value repeated for fixed steps, or an accepted-step sequence recorded from
+ * an adaptive run), as fixed steps (no error control).  Keeps the state every K steps
+ * on the device for rdcu_adjoint_backward.  y0 and yT (may be NULL) are host or device
+ * arrays of n*N doubles.  The handle's state afterwards is yT at t = sum(hs).  Needs a
+ * pseudospectral handle created with fixed = 1.  Device memory: one state per
+ * checkpoint plus 6*K states of stage storage and about 10 states of work space.
+ *
+ * rdcu_adjoint_backward: the discrete adjoint of the last rdcu_adjoint_forward: given
+ * lambdaT = dL/dyT (host or device), writes dL/dy0 to grad_y0 (host or device, n*N;
+ * may be NULL) and dL/dC_t for every coupling term to grad_C (host, nterms; may be
+ * NULL).  Stage states are recomputed segment by segment from the checkpoints.  The
+ * result is the exact derivative of the discrete map (Dormand-Prince tableau of
+ * dp45.cu:6-11), up to rounding.  It can be called again with another lambdaT; the
+ * handle's state (t, h, y) afterwards is unspecified: set it before stepping again. */
+int rdcu_adjoint_forward(rdcu_t *h, const double *y0, const double *hs, int nsteps, int K,
+                         double *yT);
+int rdcu_adjoint_backward(rdcu_t *h, const double *lambdaT, double *grad_y0, double *grad_C);
+
 /* ---- allocation-free RHS ----------------------------------------------------------
  * No counterpart in the reference: an addition for callers that cannot allocate device
  * memory.  Examples: code that runs under a device-memory budget owned by another

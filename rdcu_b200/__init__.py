@@ -43,6 +43,7 @@ EXPORTS = [
     "rdcu_create", "rdcu_destroy", "rdcu_set_state", "rdcu_get_state", "rdcu_get_info",
     "rdcu_rhs", "rdcu_jac", "rdcu_step", "rdcu_eval", "rdcu_solve", "rdcu_get_counters",
     "rdcu_memcpy", "rdcu_advance", "rdcu_random_ic", "rdcu_profile_passes", "rdcu_rhs_noalloc",
+    "rdcu_set_coefficients", "rdcu_adjoint_forward", "rdcu_adjoint_backward",
     "rdcu_error_string", "rdcu_last_error",
 ]
 
@@ -116,6 +117,9 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
     lib.rdcu_random_ic.argtypes = [pd, i, ctypes.c_longlong, d, d, i]
     lib.rdcu_profile_passes.argtypes = [vp, i, ctypes.POINTER(rdcu_pass_timing), i, pi]
     lib.rdcu_rhs_noalloc.argtypes = [ctypes.POINTER(rdcu_spec), vp, vp, vp]
+    lib.rdcu_set_coefficients.argtypes = [vp, pd]
+    lib.rdcu_adjoint_forward.argtypes = [vp, vp, pd, i, i, vp]
+    lib.rdcu_adjoint_backward.argtypes = [vp, vp, vp, pd]
     lib.rdcu_error_string.argtypes = [i]
     lib.rdcu_error_string.restype = ctypes.c_char_p
     lib.rdcu_last_error.argtypes = [vp]
@@ -321,3 +325,30 @@ class Solver:
         a, b = ctypes.c_longlong(), ctypes.c_longlong()
         self._check(self.lib.rdcu_get_counters(self.h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
+
+    @property
+    def nterms(self) -> int:
+        return len(self._lists)
+
+    def set_coefficients(self, C: Sequence[float]):
+        """New coefficient for every coupling term (same dictionary structure)."""
+        if len(C) != self.nterms:
+            raise ValueError("expected %d coefficients" % self.nterms)
+        arr = (ctypes.c_double * max(1, len(C)))(*[float(c) for c in C])
+        self._check(self.lib.rdcu_set_coefficients(self.h, arr))
+        for k, c in enumerate(C):
+            self._C[k] = float(c)
+
+    def adjoint_forward(self, y0_ptr: int, hs: Sequence[float], K: int = 50, yT_ptr: int = 0):
+        """DP45 over the step sizes hs from y0 (fixed steps), checkpointing every K steps."""
+        arr = (ctypes.c_double * max(1, len(hs)))(*[float(h) for h in hs])
+        self._check(self.lib.rdcu_adjoint_forward(self.h, ctypes.c_void_p(y0_ptr), arr, len(hs), int(K),
+                                                  ctypes.c_void_p(yT_ptr) if yT_ptr else None))
+
+    def adjoint_backward(self, lamT_ptr: int, grad_y0_ptr: int = 0):
+        """dL/dy0 (written to grad_y0_ptr) and dL/dC (returned, one per term) of the last
+        adjoint_forward, given dL/dyT at lamT_ptr."""
+        g = (ctypes.c_double * max(1, self.nterms))()
+        self._check(self.lib.rdcu_adjoint_backward(self.h, ctypes.c_void_p(lamT_ptr),
+                                                   ctypes.c_void_p(grad_y0_ptr) if grad_y0_ptr else None, g))
+        return [g[k] for k in range(self.nterms)]

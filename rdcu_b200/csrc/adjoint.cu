@@ -1,0 +1,546 @@
+// Discrete adjoint of fixed-step DP45 on the pseudospectral dictionary RHS.
+//
+// Step map (fixed h, dp45.cu:34-69 with the b row of dp45.cu:11):
+//   Y_i = y_n + h sum_{j<i} a_ij k_j,  k_i = f(Y_i; C),  y_{n+1} = y_n + h sum_i b_i k_i.
+// Reverse sweep for lambda = dL/dy_{n+1}, stages i = 6..1 (stage 7 only feeds the error
+// estimate and FSAL, so it is absent from the fixed-step map):
+//   kbar_i = h b_i lambda + h sum_{l>i} a_li Ybar_l,   Ybar_i = J_f(Y_i)^T kbar_i,
+//   Cbar  += (df/dC)(Y_i)^T kbar_i,                    dL/dy_n = lambda + sum_i Ybar_i.
+// The VJP of f = sum_t C_t prod_q Q_q^eta (Q: fields and spectral derivative blocks)
+// splits into
+//   * a pointwise kernel over the monomials: d/dQ_q of every term (product rule over its
+//     factors) times the cotangent, and the C-gradients <w_field, term> (reductions);
+//   * the transposed spectral operators: a derivative block Q_k = M_k u_src contributes
+//     M_k^T Qbar_k to ubar_src.  For the real operators here M^T has the symbol
+//     conj(M(k)) = (-1)^order M(k), so the same FFT passes apply it with the entry
+//     coefficients multiplied by (-1)^order.  Linear single-derivative terms C_t M_t u_s
+//     are handled in the transposed pass only: ubar_s += C_t M_t^T w_field and
+//     dL/dC_t = <M_t^T w_field, u_s>.
+// Checkpoints: the state every K steps; each segment is recomputed from its
+// checkpoint with the fused forward stages, keeping the stage states Y_1..Y_6.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "adjoint.h"
+
+namespace rdcu {
+namespace {
+
+// dp45.cu:6-11 (a_{l,i} for l = 2..6, and b)
+const double kA[8][6] = {
+    {0, 0, 0, 0, 0, 0},
+    {0, 0, 0, 0, 0, 0},
+    {1.0 / 5, 0, 0, 0, 0, 0},
+    {3.0 / 40, 9.0 / 40, 0, 0, 0, 0},
+    {44.0 / 45, -56.0 / 15, 32.0 / 9, 0, 0, 0},
+    {19372.0 / 6561, -25360.0 / 2187, 64448.0 / 6561, -212.0 / 729, 0, 0},
+    {9017.0 / 3168, -355.0 / 33, 46732.0 / 5247, 49.0 / 176, -5103.0 / 18656, 0},
+    {35.0 / 384, 0, 500.0 / 1113, 125.0 / 192, -2187.0 / 6784, 11.0 / 84}};
+
+constexpr int kBlocks = 296;
+constexpr int kThreads = 256;
+constexpr int kMaxQ = 16;      // fields + derivative quantities in one term evaluation
+constexpr int kMaxTerms = 64;  // terms with per-thread gradient accumulators
+
+struct AdjTerm {
+  int field, nf, off, orig;
+  double C;
+};
+struct AdjFactor {
+  int q, eta;  // q < n: field q; else derivative quantity q - n
+};
+struct AdjFold {
+  int src, g, orig, field;
+  double C;
+};
+struct AdjQ {
+  int src, g;
+};
+
+__device__ __forceinline__ double pw(double x, int e) {
+  switch (e) {
+    case 0: return 1.0;
+    case 1: return x;
+    case 2: return x * x;
+    case 3: return x * x * x;
+    default: break;
+  }
+  const int a = e < 0 ? -e : e;
+  double r = 1.0;
+  for (int i = 0; i < a; ++i) r *= x;
+  return e < 0 ? 1.0 / r : r;
+}
+
+__device__ __forceinline__ double block_reduce(double v) {
+  __shared__ double red[kThreads / 32];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < kThreads / 32; ++w) s += red[w];
+  __syncthreads();
+  return s;
+}
+
+struct PointwiseArgs {
+  int n, nq, nkept;
+  long long N;
+  const AdjTerm* terms;
+  const AdjFactor* fac;
+  const double* u;   // stage state (n fields)
+  const double* Q;   // derivative quantities (nq)
+  const double* w;   // cotangent kbar (n fields)
+  double* ubar;      // n fields
+  double* Qbar;      // nq fields
+  double* part;      // [orig term][kBlocks]
+};
+
+// Monomial VJP: ubar_f = sum_t w_field(t) dP_t/du_f, Qbar_q likewise, partial sums of
+// dL/dC_t = sum_x w_field(t) P_t / C_t.
+__global__ void __launch_bounds__(kThreads) k_adj_pointwise(PointwiseArgs a) {
+  double gacc[kMaxTerms];
+  for (int t = 0; t < a.nkept; ++t) gacc[t] = 0.0;
+  const int nqt = a.n + a.nq;
+  for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < a.N;
+       x += (long long)gridDim.x * blockDim.x) {
+    double q[kMaxQ], qb[kMaxQ];
+    for (int i = 0; i < nqt; ++i) {
+      q[i] = i < a.n ? a.u[(long long)i * a.N + x] : a.Q[(long long)(i - a.n) * a.N + x];
+      qb[i] = 0.0;
+    }
+    for (int t = 0; t < a.nkept; ++t) {
+      const AdjTerm tm = a.terms[t];
+      const double w = a.w[(long long)tm.field * a.N + x];
+      double P = 1.0;
+      for (int j = 0; j < tm.nf; ++j) {
+        const AdjFactor f = a.fac[tm.off + j];
+        P *= pw(q[f.q], f.eta);
+      }
+      gacc[t] += w * P;
+      for (int j = 0; j < tm.nf; ++j) {
+        // product rule: eta_j Q_j^(eta_j - 1) * prod of the other factors
+        double d = tm.C;
+        for (int l = 0; l < tm.nf; ++l) {
+          const AdjFactor f = a.fac[tm.off + l];
+          d *= (l == j) ? f.eta * pw(q[f.q], f.eta - 1) : pw(q[f.q], f.eta);
+        }
+        qb[a.fac[tm.off + j].q] += w * d;
+      }
+    }
+    for (int i = 0; i < a.n; ++i) a.ubar[(long long)i * a.N + x] = qb[i];
+    for (int i = 0; i < a.nq; ++i) a.Qbar[(long long)i * a.N + x] = qb[a.n + i];
+  }
+  for (int t = 0; t < a.nkept; ++t) {
+    const double s = block_reduce(gacc[t]);
+    if (threadIdx.x == 0) a.part[(long long)a.terms[t].orig * gridDim.x + blockIdx.x] = s;
+  }
+}
+
+struct CombineArgs {
+  int n, nfold, nq;
+  long long N;
+  const AdjFold* folds;
+  const AdjQ* qs;
+  const double* ubar;
+  const double* G;   // transposed-operator outputs (ng channels)
+  const double* u;   // stage state
+  double* Yb;        // out: n fields
+  double* part;
+};
+
+__global__ void __launch_bounds__(kThreads) k_adj_combine(CombineArgs a) {
+  double gacc[kMaxTerms];
+  for (int t = 0; t < a.nfold; ++t) gacc[t] = 0.0;
+  for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < a.N;
+       x += (long long)gridDim.x * blockDim.x) {
+    for (int s = 0; s < a.n; ++s) {
+      double v = a.ubar[(long long)s * a.N + x];
+      for (int t = 0; t < a.nfold; ++t)
+        if (a.folds[t].src == s) v += a.folds[t].C * a.G[(long long)a.folds[t].g * a.N + x];
+      for (int q = 0; q < a.nq; ++q)
+        if (a.qs[q].src == s) v += a.G[(long long)a.qs[q].g * a.N + x];
+      a.Yb[(long long)s * a.N + x] = v;
+    }
+    for (int t = 0; t < a.nfold; ++t)
+      gacc[t] += a.G[(long long)a.folds[t].g * a.N + x] * a.u[(long long)a.folds[t].src * a.N + x];
+  }
+  for (int t = 0; t < a.nfold; ++t) {
+    const double s = block_reduce(gacc[t]);
+    if (threadIdx.x == 0) a.part[(long long)a.folds[t].orig * gridDim.x + blockIdx.x] = s;
+  }
+}
+
+__global__ void k_adj_reduce(const double* part, int nterms, double* gC) {
+  const int t = blockIdx.x;
+  if (t >= nterms) return;
+  double s = 0.0;
+  for (int b = threadIdx.x; b < kBlocks; b += blockDim.x) s += part[(long long)t * kBlocks + b];
+  s = block_reduce(s);
+  if (threadIdx.x == 0) gC[t] += s;
+}
+
+struct Coef7 {
+  double c[7];
+};
+
+// kbar = h (b_i lambda + sum_{l > i} a_li Ybar_l), Ybar_l at Yb + (l-1)*nN
+__global__ void k_adj_kbar(double* out, const double* lam, const double* Yb, long long nN, double hb,
+                           Coef7 ha, int i) {
+  const long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= nN) return;
+  double v = hb * lam[x];
+  for (int l = i + 1; l <= 6; ++l) v += ha.c[l] * Yb[(long long)(l - 1) * nN + x];
+  out[x] = v;
+}
+
+__global__ void k_adj_lambda(double* lam, const double* Yb, long long nN) {
+  const long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= nN) return;
+  double v = lam[x];
+  for (int i = 0; i < 6; ++i) v += Yb[(long long)i * nN + x];
+  lam[x] = v;
+}
+
+ChanEntry op_entry(int k, int n, int ndim, int src_index, double coef) {
+  ChanEntry e{};
+  const int Yind = k / n;
+  e.src = src_index;
+  e.part = 0;
+  e.coef = coef;
+  if (Yind == 0) {
+    e.nax = 0;
+  } else if (Yind <= ndim) {
+    e.nax = 1;
+    e.ax0 = Yind - 1;
+  } else {
+    const int t = Yind - ndim - 1;
+    e.nax = 2;
+    e.ax0 = t / ndim;
+    e.ax1 = t % ndim;
+  }
+  return e;
+}
+
+}  // namespace
+
+struct AdjointEngine::Tables {
+  AdjTerm* terms = nullptr;
+  AdjFactor* fac = nullptr;
+  AdjFold* folds = nullptr;
+  AdjQ* qs = nullptr;
+  int nkept = 0, nfac = 0, nfold = 0, nq = 0;
+  std::vector<AdjTerm> h_terms;
+  std::vector<AdjFold> h_folds;
+};
+
+#define RDCU_TRY(x)                   \
+  do {                                \
+    cudaError_t _e = (x);             \
+    if (_e != cudaSuccess) return _e; \
+  } while (0)
+
+template <typename T>
+static cudaError_t up(T** d, const std::vector<T>& v) {
+  RDCU_TRY(cudaMalloc((void**)d, std::max<size_t>(1, v.size()) * sizeof(T)));
+  if (!v.empty()) RDCU_TRY(cudaMemcpy(*d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return cudaSuccess;
+}
+
+bool AdjointEngine::init(SpectralPlan* fwd, DP45Engine* dp, const std::vector<HostTerm>& terms, int n, int ndim,
+                         const int* Ns, const double* Ls, cudaStream_t st, std::string* msg) {
+  release();
+  fwd_ = fwd;
+  dp_ = dp;
+  st_ = st;
+  n_ = n;
+  terms_ = terms;
+  nterms = (int)terms.size();
+  N_ = 1;
+  for (int a = 0; a < ndim; ++a) N_ *= Ns[a];
+  nN_ = N_ * n;
+  tab_ = new Tables;
+  Tables& T = *tab_;
+  // classify the terms exactly as the forward plan does
+  std::vector<int> qk;  // derivative Y indices needed pointwise (nonlinear factors)
+  struct Kept {
+    int field, orig;
+    double C;
+    std::vector<std::pair<int, int>> fac;
+  };
+  std::vector<Kept> kept;
+  struct Fold {
+    int field, src, k, orig;
+    double C;
+  };
+  std::vector<Fold> folds;
+  for (int ti = 0; ti < nterms; ++ti) {
+    const auto& t = terms[ti];
+    const int field = t.ints.empty() ? 0 : t.ints[0];
+    std::vector<std::pair<int, int>> fac;
+    const int np = (int)t.ints.size();
+    for (int j = 1; j < np; j += 2) {
+      const int p = (j + 1 < np) ? t.ints[j + 1] : 0;
+      if (p != 0) fac.push_back({t.ints[j], p});
+    }
+    if (fac.size() == 1 && fac[0].second == 1 && fac[0].first >= n) {
+      folds.push_back({field, fac[0].first % n, fac[0].first, ti, t.C});
+      continue;
+    }
+    for (auto& f : fac)
+      if (f.first >= n && std::find(qk.begin(), qk.end(), f.first) == qk.end()) qk.push_back(f.first);
+    kept.push_back({field, ti, t.C, fac});
+  }
+  std::sort(qk.begin(), qk.end());
+  nq_ = (int)qk.size();
+  if ((int)kept.size() > kMaxTerms || (int)folds.size() > kMaxTerms || n + nq_ > kMaxQ) {
+    *msg = "dictionary too large for the adjoint kernels";
+    return false;
+  }
+  // distinct (operator, cotangent field) pairs of the folded terms
+  std::vector<std::pair<int, int>> pairs;  // (Yind, field)
+  std::vector<int> fold_g(folds.size());
+  for (size_t i = 0; i < folds.size(); ++i) {
+    const std::pair<int, int> key{folds[i].k / n, folds[i].field};
+    auto it = std::find(pairs.begin(), pairs.end(), key);
+    fold_g[i] = (int)(it - pairs.begin());
+    if (it == pairs.end()) pairs.push_back(key);
+  }
+  nfold_pairs_ = (int)pairs.size();
+  ng_ = nfold_pairs_ + nq_;
+  // transposed operators: inputs [kbar (n), Qbar (nq)], outputs G (ng)
+  std::vector<std::vector<ChanEntry>> tch;
+  for (auto& pr : pairs) {
+    const int k = pr.first * n;  // Y index of the operator (field 0), source = cotangent field pr.second
+    ChanEntry e = op_entry(k, n, ndim, pr.second, 1.0);
+    if (e.nax & 1) e.coef = -1.0;  // transpose of an odd-order derivative
+    tch.push_back({e});
+  }
+  for (int q = 0; q < nq_; ++q) {
+    ChanEntry e = op_entry(qk[q], n, ndim, n + q, 1.0);
+    if (e.nax & 1) e.coef = -1.0;
+    tch.push_back({e});
+  }
+  if (ng_ > 0 && !planT_.init_linear(n + nq_, ndim, Ns, Ls, tch, msg)) return false;
+  if (nq_ > 0) {
+    std::vector<std::vector<ChanEntry>> qch;
+    for (int q = 0; q < nq_; ++q) qch.push_back({op_entry(qk[q], n, ndim, qk[q] % n, 1.0)});
+    if (!planQ_.init_linear(n, ndim, Ns, Ls, qch, msg)) return false;
+    have_q_ = true;
+  }
+  // device tables
+  std::vector<AdjFactor> fac;
+  for (auto& k : kept) {
+    AdjTerm t{};
+    t.field = k.field;
+    t.orig = k.orig;
+    t.C = k.C;
+    t.off = (int)fac.size();
+    t.nf = (int)k.fac.size();
+    for (auto& f : k.fac) {
+      AdjFactor af{};
+      af.q = f.first < n ? f.first : n + (int)(std::find(qk.begin(), qk.end(), f.first) - qk.begin());
+      af.eta = f.second;
+      fac.push_back(af);
+    }
+    T.h_terms.push_back(t);
+  }
+  for (size_t i = 0; i < folds.size(); ++i) {
+    AdjFold f{};
+    f.src = folds[i].src;
+    f.g = fold_g[i];
+    f.orig = folds[i].orig;
+    f.field = folds[i].field;
+    f.C = folds[i].C;
+    T.h_folds.push_back(f);
+  }
+  std::vector<AdjQ> qs;
+  for (int q = 0; q < nq_; ++q) qs.push_back({qk[q] % n, nfold_pairs_ + q});
+  T.nkept = (int)T.h_terms.size();
+  T.nfac = (int)fac.size();
+  T.nfold = (int)T.h_folds.size();
+  T.nq = nq_;
+  const size_t sb = (size_t)nN_ * sizeof(double);
+  auto fail = [&](const char* w) {
+    *msg = std::string("adjoint set-up: ") + w;
+    return false;
+  };
+  if (up(&T.terms, T.h_terms) != cudaSuccess || up(&T.fac, fac) != cudaSuccess ||
+      up(&T.folds, T.h_folds) != cudaSuccess || up(&T.qs, qs) != cudaSuccess)
+    return fail("tables");
+  if (cudaMalloc((void**)&lam_, sb) != cudaSuccess) return fail("out of device memory");
+  if (cudaMalloc((void**)&Yb_, sb * 6) != cudaSuccess) return fail("out of device memory");
+  if (cudaMalloc((void**)&tin_, (size_t)N_ * (n + nq_) * sizeof(double)) != cudaSuccess)
+    return fail("out of device memory");
+  if (cudaMalloc((void**)&tout_, (size_t)N_ * std::max(1, ng_) * sizeof(double)) != cudaSuccess)
+    return fail("out of device memory");
+  if (cudaMalloc((void**)&qv_, (size_t)N_ * std::max(1, nq_) * sizeof(double)) != cudaSuccess)
+    return fail("out of device memory");
+  if (cudaMalloc((void**)&ubar_, sb) != cudaSuccess) return fail("out of device memory");
+  if (cudaMalloc((void**)&part_, sizeof(double) * std::max(1, nterms) * kBlocks) != cudaSuccess)
+    return fail("out of device memory");
+  if (cudaMalloc((void**)&gC_, sizeof(double) * std::max(1, nterms)) != cudaSuccess) return fail("out of device memory");
+  device_bytes = sb * 8 + (size_t)N_ * (n + 2 * nq_ + ng_) * sizeof(double);
+  return true;
+}
+
+void AdjointEngine::release() {
+  for (double* p : ckpt_)
+    if (p) cudaFree(p);
+  ckpt_.clear();
+  double* bufs[] = {store_, lam_, Yb_, tin_, tout_, qv_, ubar_, part_, gC_};
+  for (double* p : bufs)
+    if (p) cudaFree(p);
+  store_ = lam_ = Yb_ = tin_ = tout_ = qv_ = ubar_ = part_ = gC_ = nullptr;
+  store_steps_ = 0;
+  if (tab_) {
+    void* t[] = {tab_->terms, tab_->fac, tab_->folds, tab_->qs};
+    for (void* p : t)
+      if (p) cudaFree(p);
+    delete tab_;
+    tab_ = nullptr;
+  }
+}
+
+cudaError_t AdjointEngine::set_coefficients(const std::vector<double>& C) {
+  Tables& T = *tab_;
+  for (auto& t : T.h_terms) t.C = C[t.orig];
+  for (auto& f : T.h_folds) f.C = C[f.orig];
+  if (!T.h_terms.empty())
+    RDCU_TRY(cudaMemcpy(T.terms, T.h_terms.data(), T.h_terms.size() * sizeof(AdjTerm), cudaMemcpyHostToDevice));
+  if (!T.h_folds.empty())
+    RDCU_TRY(cudaMemcpy(T.folds, T.h_folds.data(), T.h_folds.size() * sizeof(AdjFold), cudaMemcpyHostToDevice));
+  return cudaSuccess;
+}
+
+cudaError_t AdjointEngine::forward(const double* y0, const double* hs, int nsteps, int K, double* yT) {
+  nsteps_ = std::max(0, nsteps);
+  hs_.assign(hs, hs + nsteps_);
+  uniform_h_ = true;
+  for (int j = 1; j < nsteps_; ++j) uniform_h_ = uniform_h_ && hs_[j] == hs_[0];
+  K_ = std::max(1, K);
+  const int nseg = std::max(1, (nsteps_ + K_ - 1) / K_);
+  const size_t sb = (size_t)nN_ * sizeof(double);
+  for (double* p : ckpt_)
+    if (p) cudaFree(p);
+  ckpt_.assign(nseg, nullptr);
+  for (auto& p : ckpt_) RDCU_TRY(cudaMalloc((void**)&p, sb));
+  RDCU_TRY(dp_->set_state(0.0, nsteps_ ? hs_[0] : 0.0, y0));
+  for (int seg = 0; seg < nseg; ++seg) {
+    RDCU_TRY(dp_->copy_current_y(ckpt_[seg]));
+    const int j0 = seg * K_, steps = std::min(K_, nsteps_ - j0);
+    if (steps <= 0) break;
+    if (uniform_h_) {
+      long long acc = 0;
+      RDCU_TRY(dp_->advance(steps, 0.0, INFINITY, &acc));
+    } else {
+      RDCU_TRY(dp_->arm(1, INFINITY, 0.0, INFINITY, 0, 0, steps));
+      if (seg == 0) RDCU_TRY(dp_->launch_k1());
+      for (int j = 0; j < steps; ++j) {
+        RDCU_TRY(dp_->set_h_async(hs_[j0 + j]));
+        RDCU_TRY(dp_->launch_attempt());
+      }
+    }
+  }
+  if (yT) RDCU_TRY(dp_->get_state(nullptr, nullptr, yT, cudaMemcpyDefault));
+  return cudaStreamSynchronize(st_);
+}
+
+cudaError_t AdjointEngine::recompute_segment(int seg, int steps) {
+  const size_t sb = (size_t)nN_ * sizeof(double);
+  if (store_steps_ < steps) {
+    if (store_) cudaFree(store_);
+    store_ = nullptr;
+    store_steps_ = 0;
+    RDCU_TRY(cudaMalloc((void**)&store_, sb * 6 * (size_t)steps));
+    store_steps_ = steps;
+  }
+  const int j0 = seg * K_;
+  RDCU_TRY(dp_->set_state(0.0, hs_[j0], ckpt_[seg]));
+  RDCU_TRY(dp_->arm(1, INFINITY, 0.0, INFINITY, 0, 0, steps));
+  RDCU_TRY(dp_->launch_k1());
+  for (int j = 0; j < steps; ++j) {
+    double* base = store_ + (size_t)j * 6 * nN_;
+    RDCU_TRY(dp_->copy_current_y(base));  // Y_1 = y_j
+    double* outs[8] = {};
+    for (int s = 2; s <= 6; ++s) outs[s] = base + (size_t)(s - 1) * nN_;
+    if (!uniform_h_) RDCU_TRY(dp_->set_h_async(hs_[j0 + j]));
+    RDCU_TRY(dp_->launch_attempt_capture(outs));
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t AdjointEngine::vjp(const double* Y, double* Yb) {
+  Tables& T = *tab_;
+  const int blocks = kBlocks;
+  if (have_q_) RDCU_TRY(planQ_.run_linear(Y, qv_, st_));
+  PointwiseArgs pa{};
+  pa.n = n_;
+  pa.nq = nq_;
+  pa.nkept = T.nkept;
+  pa.N = N_;
+  pa.terms = T.terms;
+  pa.fac = T.fac;
+  pa.u = Y;
+  pa.Q = qv_;
+  pa.w = tin_;
+  pa.ubar = ubar_;
+  pa.Qbar = tin_ + (size_t)n_ * N_;
+  pa.part = part_;
+  k_adj_pointwise<<<blocks, kThreads, 0, st_>>>(pa);
+  RDCU_TRY(cudaGetLastError());
+  if (ng_ > 0) RDCU_TRY(planT_.run_linear(tin_, tout_, st_));
+  CombineArgs ca{};
+  ca.n = n_;
+  ca.nfold = T.nfold;
+  ca.nq = nq_;
+  ca.N = N_;
+  ca.folds = T.folds;
+  ca.qs = T.qs;
+  ca.ubar = ubar_;
+  ca.G = tout_;
+  ca.u = Y;
+  ca.Yb = Yb;
+  ca.part = part_;
+  k_adj_combine<<<blocks, kThreads, 0, st_>>>(ca);
+  RDCU_TRY(cudaGetLastError());
+  k_adj_reduce<<<std::max(1, nterms), kThreads, 0, st_>>>(part_, nterms, gC_);
+  return cudaGetLastError();
+}
+
+cudaError_t AdjointEngine::backward(const double* lambdaT, double* grad_y0, double* grad_C) {
+  if (ckpt_.empty()) return cudaErrorInvalidValue;  // no forward run recorded
+  const size_t sb = (size_t)nN_ * sizeof(double);
+  RDCU_TRY(cudaMemcpyAsync(lam_, lambdaT, sb, cudaMemcpyDefault, st_));
+  RDCU_TRY(cudaMemsetAsync(gC_, 0, sizeof(double) * std::max(1, nterms), st_));
+  const int nseg = (nsteps_ + K_ - 1) / K_;
+  const unsigned gb = (unsigned)((nN_ + 255) / 256);
+  for (int seg = nseg - 1; seg >= 0; --seg) {
+    const int steps = std::min(K_, nsteps_ - seg * K_);
+    RDCU_TRY(recompute_segment(seg, steps));
+    for (int j = steps - 1; j >= 0; --j) {
+      const double* Ystore = store_ + (size_t)j * 6 * nN_;
+      const double h = hs_[seg * K_ + j];
+      for (int i = 6; i >= 1; --i) {
+        Coef7 ha{};
+        for (int l = i + 1; l <= 6; ++l) ha.c[l] = h * kA[l][i - 1];
+        k_adj_kbar<<<gb, 256, 0, st_>>>(tin_, lam_, Yb_, nN_, h * kA[7][i - 1], ha, i);
+        RDCU_TRY(cudaGetLastError());
+        RDCU_TRY(vjp(Ystore + (size_t)(i - 1) * nN_, Yb_ + (size_t)(i - 1) * nN_));
+      }
+      k_adj_lambda<<<gb, 256, 0, st_>>>(lam_, Yb_, nN_);
+      RDCU_TRY(cudaGetLastError());
+    }
+  }
+  if (grad_y0) RDCU_TRY(cudaMemcpyAsync(grad_y0, lam_, sb, cudaMemcpyDefault, st_));
+  std::vector<double> g(std::max(1, nterms));
+  RDCU_TRY(cudaMemcpyAsync(g.data(), gC_, sizeof(double) * std::max(1, nterms), cudaMemcpyDeviceToHost, st_));
+  RDCU_TRY(cudaStreamSynchronize(st_));
+  if (grad_C)
+    for (int t = 0; t < nterms; ++t) grad_C[t] = g[t];
+  return cudaSuccess;
+}
+
+}  // namespace rdcu

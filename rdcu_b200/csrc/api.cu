@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "../../include/rdcu.h"
+#include "adjoint.h"
 #include "bdf.h"
 #include "dp45.h"
 #include "fd.h"
@@ -29,6 +30,7 @@ struct rdcu_handle {
   // DP45 (pseudospectral)
   std::unique_ptr<SpectralPlan> sp;
   std::unique_ptr<DP45Engine> dp;
+  std::unique_ptr<AdjointEngine> adj;  // created by the first rdcu_adjoint_forward
   // BDF (finite differences)
   std::unique_ptr<FDProblem> fd;
   std::unique_ptr<BDFEngine> bdf;
@@ -188,6 +190,7 @@ int rdcu_destroy(rdcu_t* h) {
   if (!h) return RDCU_OK;
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
+  h->adj.reset();
   h->dp.reset();
   h->sp.reset();
   h->bdf.reset();
@@ -468,6 +471,49 @@ int rdcu_get_counters(rdcu_t* h, long long* accepted, long long* attempts) {
   if (!h) return set_err(h, RDCU_ERR_INVALID, "null argument");
   if (accepted) *accepted = h->last_accepted;
   if (attempts) *attempts = h->last_attempts;
+  return RDCU_OK;
+}
+
+int rdcu_set_coefficients(rdcu_t* h, const double* C) {
+  if (!h || (!C && !h->terms.empty())) return set_err(h, RDCU_ERR_INVALID, "null argument");
+  if (!h->sp) return set_err(h, RDCU_ERR_UNSUPPORTED, "coefficients can be replaced on pseudospectral handles");
+  if (int rc = activate(h)) return rc;
+  std::vector<double> c(C, C + h->terms.size());
+  for (size_t i = 0; i < c.size(); ++i) {
+    if (!std::isfinite(c[i])) return set_err(h, RDCU_ERR_INVALID, "coefficients must be finite");
+    h->terms[i].C = c[i];
+  }
+  CHECK_CUDA(h, cudaStreamSynchronize(h->stream), "rdcu_set_coefficients");
+  CHECK_CUDA(h, h->sp->set_coefficients(c), "rdcu_set_coefficients");
+  if (h->adj) CHECK_CUDA(h, h->adj->set_coefficients(c), "rdcu_set_coefficients");
+  h->dp->invalidate_k1();
+  return RDCU_OK;
+}
+
+int rdcu_adjoint_forward(rdcu_t* h, const double* y0, const double* hs, int nsteps, int K, double* yT) {
+  if (!h || !y0 || (!hs && nsteps > 0) || nsteps < 0 || K < 1) return set_err(h, RDCU_ERR_INVALID, "bad argument");
+  if (!h->sp) return set_err(h, RDCU_ERR_UNSUPPORTED, "the adjoint is implemented for pseudospectral DP45 handles");
+  if (!h->spec.fixed) return set_err(h, RDCU_ERR_STATE, "the adjoint needs a handle created with fixed = 1");
+  for (int j = 0; j < nsteps; ++j)
+    if (!(hs[j] > 0) || !std::isfinite(hs[j])) return set_err(h, RDCU_ERR_INVALID, "step sizes must be positive and finite");
+  if (int rc = activate(h)) return rc;
+  if (!h->adj) {
+    std::string msg;
+    std::unique_ptr<AdjointEngine> a(new AdjointEngine);
+    if (!a->init(h->sp.get(), h->dp.get(), h->terms, h->spec.n, h->spec.ndim, h->spec.Ns, h->spec.Ls, h->stream,
+                 &msg))
+      return set_err(h, msg.find("memory") != std::string::npos ? RDCU_ERR_NOMEM : RDCU_ERR_UNSUPPORTED, msg);
+    h->adj = std::move(a);
+  }
+  CHECK_CUDA(h, h->adj->forward(y0, hs, nsteps, K, yT), "rdcu_adjoint_forward");
+  return RDCU_OK;
+}
+
+int rdcu_adjoint_backward(rdcu_t* h, const double* lambdaT, double* grad_y0, double* grad_C) {
+  if (!h || !lambdaT) return set_err(h, RDCU_ERR_INVALID, "null argument");
+  if (!h->adj || !h->adj->recorded()) return set_err(h, RDCU_ERR_STATE, "rdcu_adjoint_forward has not run");
+  if (int rc = activate(h)) return rc;
+  CHECK_CUDA(h, h->adj->backward(lambdaT, grad_y0, grad_C), "rdcu_adjoint_backward");
   return RDCU_OK;
 }
 

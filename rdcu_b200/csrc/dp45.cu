@@ -150,6 +150,14 @@ __global__ void k_dp45_interp(DP45Bufs b, const DP45Ctl* c, double t_eval, doubl
   out[i] = yl[i] + h * (x * S[0] + x * x * S[1] + x * x * x * S[2] + x * x * x * x * S[3]);
 }
 
+__global__ void k_dp45_copy_y(DP45Bufs b, const DP45Ctl* c, double* dst, long long nN) {
+  const double* y = b.ybuf[c->y_slot];
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nN; i += (long long)gridDim.x * blockDim.x)
+    dst[i] = y[i];
+}
+
+__global__ void k_dp45_set_h(DP45Ctl* c, double h) { c->h = h; }
+
 }  // namespace
 
 #define RDCU_TRY(x)                   \
@@ -305,7 +313,20 @@ cudaError_t DP45Engine::launch_k1() {
   return sp_->run(io, st_);
 }
 
-cudaError_t DP45Engine::launch_attempt() {
+cudaError_t DP45Engine::launch_attempt() { return launch_attempt_capture(nullptr); }
+
+cudaError_t DP45Engine::copy_current_y(double* dst) {
+  const unsigned blocks = (unsigned)std::min<long long>(1184, (nN_ + 255) / 256);
+  k_dp45_copy_y<<<blocks, 256, 0, st_>>>(bufs, d_ctl_, dst, nN_);
+  return cudaGetLastError();
+}
+
+cudaError_t DP45Engine::set_h_async(double h) {
+  k_dp45_set_h<<<1, 1, 0, st_>>>(d_ctl_, h);
+  return cudaGetLastError();
+}
+
+cudaError_t DP45Engine::launch_attempt_capture(double* const* ytemp_out) {
   for (int s = 2; s <= 7; ++s) {
     RhsIO io{};
     io.mode = 1;
@@ -313,6 +334,7 @@ cudaError_t DP45Engine::launch_attempt() {
     io.bufs = bufs;
     io.ctl = d_ctl_;
     io.err_part = (s == 7 && !fixed_) ? err_part_ : nullptr;
+    if (ytemp_out && s <= 6) io.ytemp_out = ytemp_out[s];
     RDCU_TRY(sp_->run(io, st_));
   }
   k_dp45_ctl<<<1, kCtlThreads, 0, st_>>>(d_ctl_, err_part_, log_h_, log_t_, log_acc_, (double)nN_,

@@ -44,9 +44,21 @@ class DP45Engine {
   cudaError_t advance(int n, double hmin, double hmax, long long* accepted);
   // Launches one attempt (stages 2..7 and the controller) on the stream; no sync.
   cudaError_t launch_attempt();
+  // launch_attempt with the stage states of stages 2..6 written to ytemp_out[2..6]
+  // (entries may be null) instead of the scratch state slot
+  cudaError_t launch_attempt_capture(double* const* ytemp_out);
   cudaError_t launch_k1();
+  // device copy of the current state y (slot chosen on the device); no sync
+  cudaError_t copy_current_y(double* dst);
+  // sets the step size of the next attempt on the device; no sync
+  cudaError_t set_h_async(double h);
   cudaError_t arm(int check, double t1, double hmin, double hmax, int eval_i, int n_eval,
                   int max_attempts);
+  // the cached slope k1 = f(y) is stale (new coefficients): recompute it before the next attempt
+  void invalidate_k1() {
+    k1_valid_ = false;
+    have_step_ = false;
+  }
   cudaError_t sync_ctl();  // copies the controller state to host_ctl (synchronises)
 
   DP45Ctl host_ctl{};
