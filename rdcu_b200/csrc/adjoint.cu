@@ -42,6 +42,7 @@ constexpr int kBlocks = 296;
 constexpr int kThreads = 256;
 constexpr int kMaxQ = 16;      // fields + derivative quantities in one term evaluation
 constexpr int kMaxTerms = 64;  // terms with per-thread gradient accumulators
+constexpr int kMaxGraphSteps = 512;  // longer segments are launched directly (graph size)
 
 struct AdjTerm {
   int field, nf, off, orig;
@@ -85,123 +86,182 @@ __device__ __forceinline__ double block_reduce(double v) {
   return s;
 }
 
-struct PointwiseArgs {
-  int n, nq, nkept;
-  long long N;
-  const AdjTerm* terms;
-  const AdjFactor* fac;
-  const double* u;   // stage state (n fields)
-  const double* Q;   // derivative quantities (nq)
-  const double* w;   // cotangent kbar (n fields)
-  double* ubar;      // n fields
-  double* Qbar;      // nq fields
-  double* part;      // [orig term][kBlocks]
+struct Coef7 {
+  double c[7];
 };
 
-// Monomial VJP: ubar_f = sum_t w_field(t) dP_t/du_f, Qbar_q likewise, partial sums of
-// dL/dC_t = sum_x w_field(t) P_t / C_t.
+struct PointwiseArgs {
+  int n, nq, nkept, nfac, stage;
+  long long N, nN;
+  const AdjTerm* terms;
+  const AdjFactor* fac;
+  const double* u;   // stage state Y_i (n fields)
+  const double* Q;   // derivative quantities of Y_i (nq)
+  const double* lam; // adjoint state after the step
+  const double* Yb;  // stage adjoints, block l-1 for stage l
+  double hb;         // h b_i
+  Coef7 ha;          // ha.c[l] = h a_{l,i}
+  double* w;         // out: kbar_i (n fields), input of the transposed operators
+  double* ubar;      // out: pointwise field adjoint (n)
+  double* Qbar;      // out: derivative-quantity adjoint (nq)
+  double* part;      // [term][kBlocks] partial sums of dL/dC, accumulated
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Shared memory of k_adj_pointwise: per-thread slices [i][thread] of the quantities q,
+// their adjoints qb and kbar (indexed by the dictionary's runtime factor lists, so they
+// live in shared rather than local memory), then per-warp gradient sums [term][warp].
+size_t pointwise_smem(int n, int nq, int nkept, int nfac) {
+  return ((size_t)(2 * (n + nq) + n) * kThreads + (size_t)nkept * (kThreads / 32)) * sizeof(double) +
+         (size_t)nkept * sizeof(AdjTerm) + (size_t)nfac * sizeof(AdjFactor);
+}
+
+// kbar_i = h b_i lambda + h sum_{l > i} a_li Ybar_l (computed per point, stored for the
+// transposed operators), then the monomial VJP: ubar_f = sum_t kbar_field(t) dP_t/du_f,
+// Qbar_q likewise, and per-block partial sums of dL/dC_t = sum_x kbar_field(t) P_t
+// (warp sums, then warps in a fixed order: deterministic).
 __global__ void __launch_bounds__(kThreads) k_adj_pointwise(PointwiseArgs a) {
-  double gacc[kMaxTerms];
-  for (int t = 0; t < a.nkept; ++t) gacc[t] = 0.0;
+  extern __shared__ double psm[];
+  constexpr int T = kThreads, NW = kThreads / 32;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nqt = a.n + a.nq;
-  for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < a.N;
-       x += (long long)gridDim.x * blockDim.x) {
-    double q[kMaxQ], qb[kMaxQ];
-    for (int i = 0; i < nqt; ++i) {
-      q[i] = i < a.n ? a.u[(long long)i * a.N + x] : a.Q[(long long)(i - a.n) * a.N + x];
-      qb[i] = 0.0;
+  double* sq = psm;
+  double* sqb = sq + nqt * T;
+  double* swk = sqb + nqt * T;
+  double* sg = swk + a.n * T;
+  AdjTerm* sterm = reinterpret_cast<AdjTerm*>(sg + a.nkept * NW);
+  AdjFactor* sfac = reinterpret_cast<AdjFactor*>(sterm + a.nkept);
+  for (int i = tid; i < a.nkept * NW; i += T) sg[i] = 0.0;
+  // the tables are read in every term iteration: stage them next to the slices
+  for (int i = tid; i < a.nkept; i += T) sterm[i] = a.terms[i];
+  for (int i = tid; i < a.nfac; i += T) sfac[i] = a.fac[i];
+  __syncthreads();
+  for (long long base = (long long)blockIdx.x * T; base < a.N; base += (long long)gridDim.x * T) {
+    const long long x = base + tid;
+    const bool live = x < a.N;
+    if (live) {
+      for (int f = 0; f < a.n; ++f) {
+        const long long o = (long long)f * a.N + x;
+        double v = a.hb * a.lam[o];
+        for (int l = a.stage + 1; l <= 6; ++l) v += a.ha.c[l] * a.Yb[(long long)(l - 1) * a.nN + o];
+        a.w[o] = v;
+        swk[f * T + tid] = v;
+      }
+      for (int i = 0; i < nqt; ++i) {
+        sq[i * T + tid] = i < a.n ? a.u[(long long)i * a.N + x] : a.Q[(long long)(i - a.n) * a.N + x];
+        sqb[i * T + tid] = 0.0;
+      }
     }
     for (int t = 0; t < a.nkept; ++t) {
-      const AdjTerm tm = a.terms[t];
-      const double w = a.w[(long long)tm.field * a.N + x];
-      double P = 1.0;
-      for (int j = 0; j < tm.nf; ++j) {
-        const AdjFactor f = a.fac[tm.off + j];
-        P *= pw(q[f.q], f.eta);
-      }
-      gacc[t] += w * P;
-      for (int j = 0; j < tm.nf; ++j) {
-        // product rule: eta_j Q_j^(eta_j - 1) * prod of the other factors
-        double d = tm.C;
-        for (int l = 0; l < tm.nf; ++l) {
-          const AdjFactor f = a.fac[tm.off + l];
-          d *= (l == j) ? f.eta * pw(q[f.q], f.eta - 1) : pw(q[f.q], f.eta);
+      double g = 0.0;
+      if (live) {
+        const AdjTerm tm = sterm[t];
+        const double w = swk[tm.field * T + tid];
+        double P = 1.0;
+        for (int j = 0; j < tm.nf; ++j) {
+          const AdjFactor f = sfac[tm.off + j];
+          P *= pw(sq[f.q * T + tid], f.eta);
         }
-        qb[a.fac[tm.off + j].q] += w * d;
+        g = w * P;
+        for (int j = 0; j < tm.nf; ++j) {
+          // product rule: eta_j Q_j^(eta_j - 1) * prod of the other factors
+          double d = tm.C;
+          for (int l = 0; l < tm.nf; ++l) {
+            const AdjFactor f = sfac[tm.off + l];
+            const double qv = sq[f.q * T + tid];
+            d *= (l == j) ? f.eta * pw(qv, f.eta - 1) : pw(qv, f.eta);
+          }
+          sqb[sfac[tm.off + j].q * T + tid] += w * d;
+        }
       }
+      g = warp_sum(g);
+      if (lane == 0) sg[t * NW + warp] += g;
     }
-    for (int i = 0; i < a.n; ++i) a.ubar[(long long)i * a.N + x] = qb[i];
-    for (int i = 0; i < a.nq; ++i) a.Qbar[(long long)i * a.N + x] = qb[a.n + i];
+    if (live) {
+      for (int i = 0; i < a.n; ++i) a.ubar[(long long)i * a.N + x] = sqb[i * T + tid];
+      for (int i = 0; i < a.nq; ++i) a.Qbar[(long long)i * a.N + x] = sqb[(a.n + i) * T + tid];
+    }
   }
-  for (int t = 0; t < a.nkept; ++t) {
-    const double s = block_reduce(gacc[t]);
-    if (threadIdx.x == 0) a.part[(long long)a.terms[t].orig * gridDim.x + blockIdx.x] = s;
+  __syncthreads();
+  for (int t = tid; t < a.nkept; t += T) {
+    double s = 0.0;
+    for (int w = 0; w < NW; ++w) s += sg[t * NW + w];
+    a.part[(long long)sterm[t].orig * gridDim.x + blockIdx.x] += s;
   }
 }
 
 struct CombineArgs {
-  int n, nfold, nq;
-  long long N;
+  int n, nfold, nq, final_stage;
+  long long N, nN;
   const AdjFold* folds;
   const AdjQ* qs;
   const double* ubar;
   const double* G;   // transposed-operator outputs (ng channels)
   const double* u;   // stage state
-  double* Yb;        // out: n fields
+  double* Yb;        // out: Ybar_i (n fields); stage 1: not stored
+  double* lam;       // stage 1: lambda += sum_i Ybar_i
   double* part;
 };
 
+// Ybar_i = ubar + sum_folded C_t M_t^T kbar_field(t) + sum_q M_q^T Qbar_q; partial sums of
+// dL/dC_t = <M_t^T kbar_field(t), u_src(t)> for the folded terms.  At stage 1 the step
+// ends: lambda_n = lambda_{n+1} + sum_{i=1..6} Ybar_i.
 __global__ void __launch_bounds__(kThreads) k_adj_combine(CombineArgs a) {
-  double gacc[kMaxTerms];
-  for (int t = 0; t < a.nfold; ++t) gacc[t] = 0.0;
-  for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < a.N;
-       x += (long long)gridDim.x * blockDim.x) {
-    for (int s = 0; s < a.n; ++s) {
-      double v = a.ubar[(long long)s * a.N + x];
-      for (int t = 0; t < a.nfold; ++t)
-        if (a.folds[t].src == s) v += a.folds[t].C * a.G[(long long)a.folds[t].g * a.N + x];
-      for (int q = 0; q < a.nq; ++q)
-        if (a.qs[q].src == s) v += a.G[(long long)a.qs[q].g * a.N + x];
-      a.Yb[(long long)s * a.N + x] = v;
+  constexpr int T = kThreads, NW = kThreads / 32;
+  __shared__ double sg[kMaxTerms * NW];
+  __shared__ AdjFold sfold[kMaxTerms];
+  __shared__ AdjQ sqs[kMaxQ];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int i = tid; i < a.nfold * NW; i += T) sg[i] = 0.0;
+  for (int i = tid; i < a.nfold; i += T) sfold[i] = a.folds[i];
+  for (int i = tid; i < a.nq; i += T) sqs[i] = a.qs[i];
+  __syncthreads();
+  for (long long base = (long long)blockIdx.x * T; base < a.N; base += (long long)gridDim.x * T) {
+    const long long x = base + tid;
+    const bool live = x < a.N;
+    if (live) {
+      for (int s = 0; s < a.n; ++s) {
+        const long long o = (long long)s * a.N + x;
+        double v = a.ubar[o];
+        for (int t = 0; t < a.nfold; ++t)
+          if (sfold[t].src == s) v += sfold[t].C * a.G[(long long)sfold[t].g * a.N + x];
+        for (int q = 0; q < a.nq; ++q)
+          if (sqs[q].src == s) v += a.G[(long long)sqs[q].g * a.N + x];
+        if (a.final_stage) {
+          double l = a.lam[o] + v;
+          for (int i = 2; i <= 6; ++i) l += a.Yb[(long long)(i - 1) * a.nN + o];
+          a.lam[o] = l;
+        } else {
+          a.Yb[o] = v;
+        }
+      }
     }
-    for (int t = 0; t < a.nfold; ++t)
-      gacc[t] += a.G[(long long)a.folds[t].g * a.N + x] * a.u[(long long)a.folds[t].src * a.N + x];
+    for (int t = 0; t < a.nfold; ++t) {
+      double g = live ? a.G[(long long)sfold[t].g * a.N + x] * a.u[(long long)sfold[t].src * a.N + x] : 0.0;
+      g = warp_sum(g);
+      if (lane == 0) sg[t * NW + warp] += g;
+    }
   }
-  for (int t = 0; t < a.nfold; ++t) {
-    const double s = block_reduce(gacc[t]);
-    if (threadIdx.x == 0) a.part[(long long)a.folds[t].orig * gridDim.x + blockIdx.x] = s;
+  __syncthreads();
+  for (int t = tid; t < a.nfold; t += T) {
+    double s = 0.0;
+    for (int w = 0; w < NW; ++w) s += sg[t * NW + w];
+    a.part[(long long)sfold[t].orig * gridDim.x + blockIdx.x] += s;
   }
 }
 
+// dL/dC_t = sum over the blocks' accumulated partials (fixed order: deterministic)
 __global__ void k_adj_reduce(const double* part, int nterms, double* gC) {
   const int t = blockIdx.x;
   if (t >= nterms) return;
   double s = 0.0;
   for (int b = threadIdx.x; b < kBlocks; b += blockDim.x) s += part[(long long)t * kBlocks + b];
   s = block_reduce(s);
-  if (threadIdx.x == 0) gC[t] += s;
-}
-
-struct Coef7 {
-  double c[7];
-};
-
-// kbar = h (b_i lambda + sum_{l > i} a_li Ybar_l), Ybar_l at Yb + (l-1)*nN
-__global__ void k_adj_kbar(double* out, const double* lam, const double* Yb, long long nN, double hb,
-                           Coef7 ha, int i) {
-  const long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (x >= nN) return;
-  double v = hb * lam[x];
-  for (int l = i + 1; l <= 6; ++l) v += ha.c[l] * Yb[(long long)(l - 1) * nN + x];
-  out[x] = v;
-}
-
-__global__ void k_adj_lambda(double* lam, const double* Yb, long long nN) {
-  const long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (x >= nN) return;
-  double v = lam[x];
-  for (int i = 0; i < 6; ++i) v += Yb[(long long)i * nN + x];
-  lam[x] = v;
+  if (threadIdx.x == 0) gC[t] = s;
 }
 
 ChanEntry op_entry(int k, int n, int ndim, int src_index, double coef) {
@@ -362,6 +422,12 @@ bool AdjointEngine::init(SpectralPlan* fwd, DP45Engine* dp, const std::vector<Ho
   T.nfac = (int)fac.size();
   T.nfold = (int)T.h_folds.size();
   T.nq = nq_;
+  pw_smem_ = pointwise_smem(n, nq_, T.nkept, T.nfac);
+  if (pw_smem_ > 48 * 1024 &&
+      cudaFuncSetAttribute(k_adj_pointwise, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pw_smem_) != cudaSuccess) {
+    *msg = "adjoint set-up: dictionary too large for the pointwise kernel's shared memory";
+    return false;
+  }
   const size_t sb = (size_t)nN_ * sizeof(double);
   auto fail = [&](const char* w) {
     *msg = std::string("adjoint set-up: ") + w;
@@ -387,8 +453,10 @@ bool AdjointEngine::init(SpectralPlan* fwd, DP45Engine* dp, const std::vector<Ho
 }
 
 void AdjointEngine::release() {
-  for (double* p : ckpt_)
+  drop_graphs();
+  for (double* p : ckpt_pool_)
     if (p) cudaFree(p);
+  ckpt_pool_.clear();
   ckpt_.clear();
   double* bufs[] = {store_, lam_, Yb_, tin_, tout_, qv_, ubar_, part_, gC_};
   for (double* p : bufs)
@@ -423,10 +491,14 @@ cudaError_t AdjointEngine::forward(const double* y0, const double* hs, int nstep
   K_ = std::max(1, K);
   const int nseg = std::max(1, (nsteps_ + K_ - 1) / K_);
   const size_t sb = (size_t)nN_ * sizeof(double);
-  for (double* p : ckpt_)
-    if (p) cudaFree(p);
-  ckpt_.assign(nseg, nullptr);
-  for (auto& p : ckpt_) RDCU_TRY(cudaMalloc((void**)&p, sb));
+  // checkpoint buffers are kept across calls and only added to
+  ckpt_.clear();
+  while ((int)ckpt_pool_.size() < nseg) {
+    double* p = nullptr;
+    RDCU_TRY(cudaMalloc((void**)&p, sb));
+    ckpt_pool_.push_back(p);
+  }
+  ckpt_.assign(ckpt_pool_.begin(), ckpt_pool_.begin() + nseg);
   RDCU_TRY(dp_->set_state(0.0, nsteps_ ? hs_[0] : 0.0, y0));
   for (int seg = 0; seg < nseg; ++seg) {
     RDCU_TRY(dp_->copy_current_y(ckpt_[seg]));
@@ -436,9 +508,10 @@ cudaError_t AdjointEngine::forward(const double* y0, const double* hs, int nstep
       long long acc = 0;
       RDCU_TRY(dp_->advance(steps, 0.0, INFINITY, &acc));
     } else {
-      RDCU_TRY(dp_->arm(1, INFINITY, 0.0, INFINITY, 0, 0, steps));
-      if (seg == 0) RDCU_TRY(dp_->launch_k1());
+      const int cap = dp_->log_cap();  // a full attempt log stops the controller: re-arm
       for (int j = 0; j < steps; ++j) {
+        if (j % cap == 0) RDCU_TRY(dp_->arm(1, INFINITY, 0.0, INFINITY, 0, 0, std::min(cap, steps - j)));
+        if (seg == 0 && j == 0) RDCU_TRY(dp_->launch_k1());
         RDCU_TRY(dp_->set_h_async(hs_[j0 + j]));
         RDCU_TRY(dp_->launch_attempt());
       }
@@ -448,92 +521,143 @@ cudaError_t AdjointEngine::forward(const double* y0, const double* hs, int nstep
   return cudaStreamSynchronize(st_);
 }
 
-cudaError_t AdjointEngine::recompute_segment(int seg, int steps) {
-  const size_t sb = (size_t)nN_ * sizeof(double);
-  if (store_steps_ < steps) {
-    if (store_) cudaFree(store_);
-    store_ = nullptr;
-    store_steps_ = 0;
-    RDCU_TRY(cudaMalloc((void**)&store_, sb * 6 * (size_t)steps));
-    store_steps_ = steps;
+cudaError_t AdjointEngine::ensure_store(int steps) {
+  if (store_steps_ >= steps) return cudaSuccess;
+  drop_graphs();  // the graphs hold store_ addresses
+  if (store_) cudaFree(store_);
+  store_ = nullptr;
+  store_steps_ = 0;
+  RDCU_TRY(cudaMalloc((void**)&store_, (size_t)nN_ * sizeof(double) * 6 * (size_t)steps));
+  store_steps_ = steps;
+  return cudaSuccess;
+}
+
+void AdjointEngine::drop_graphs() {
+  for (auto& g : graphs_) {
+    if (g.rec) cudaGraphExecDestroy(g.rec);
+    if (g.rev) cudaGraphExecDestroy(g.rev);
   }
-  const int j0 = seg * K_;
-  RDCU_TRY(dp_->set_state(0.0, hs_[j0], ckpt_[seg]));
-  RDCU_TRY(dp_->arm(1, INFINITY, 0.0, INFINITY, 0, 0, steps));
-  RDCU_TRY(dp_->launch_k1());
+  graphs_.clear();
+}
+
+// Recomputes `steps` steps from the state in bufs.ybuf[0] (queued; capturable), storing
+// the stage states Y_1..Y_6 of step j at store_ + 6 j nN.
+cudaError_t AdjointEngine::launch_recompute(int j0, int steps) {
+  const int cap = dp_->log_cap();
+  RDCU_TRY(dp_->reset_async(0.0, hs_[j0]));
   for (int j = 0; j < steps; ++j) {
+    if (j % cap == 0) RDCU_TRY(dp_->arm(1, INFINITY, 0.0, INFINITY, 0, 0, std::min(cap, steps - j)));
+    if (j == 0) RDCU_TRY(dp_->launch_k1());
     double* base = store_ + (size_t)j * 6 * nN_;
     RDCU_TRY(dp_->copy_current_y(base));  // Y_1 = y_j
     double* outs[8] = {};
-    for (int s = 2; s <= 6; ++s) outs[s] = base + (size_t)(s - 1) * nN_;
+    for (int st = 2; st <= 6; ++st) outs[st] = base + (size_t)(st - 1) * nN_;
     if (!uniform_h_) RDCU_TRY(dp_->set_h_async(hs_[j0 + j]));
     RDCU_TRY(dp_->launch_attempt_capture(outs));
   }
-  return cudaGetLastError();
+  return cudaSuccess;
 }
 
-cudaError_t AdjointEngine::vjp(const double* Y, double* Yb) {
+// Reverse sweep over `steps` recomputed steps (queued; capturable).
+cudaError_t AdjointEngine::launch_reverse(int j0, int steps) {
+  for (int j = steps - 1; j >= 0; --j) {
+    const double* Ystore = store_ + (size_t)j * 6 * nN_;
+    const double h = hs_[j0 + j];
+    for (int i = 6; i >= 1; --i) RDCU_TRY(vjp(Ystore + (size_t)(i - 1) * nN_, i, h));
+  }
+  return cudaSuccess;
+}
+
+cudaError_t AdjointEngine::vjp(const double* Y, int stage, double h) {
   Tables& T = *tab_;
-  const int blocks = kBlocks;
   if (have_q_) RDCU_TRY(planQ_.run_linear(Y, qv_, st_));
   PointwiseArgs pa{};
   pa.n = n_;
   pa.nq = nq_;
   pa.nkept = T.nkept;
+  pa.nfac = T.nfac;
+  pa.stage = stage;
   pa.N = N_;
+  pa.nN = nN_;
   pa.terms = T.terms;
   pa.fac = T.fac;
   pa.u = Y;
   pa.Q = qv_;
+  pa.lam = lam_;
+  pa.Yb = Yb_;
+  pa.hb = h * kA[7][stage - 1];
+  for (int l = stage + 1; l <= 6; ++l) pa.ha.c[l] = h * kA[l][stage - 1];
   pa.w = tin_;
   pa.ubar = ubar_;
   pa.Qbar = tin_ + (size_t)n_ * N_;
   pa.part = part_;
-  k_adj_pointwise<<<blocks, kThreads, 0, st_>>>(pa);
+  k_adj_pointwise<<<kBlocks, kThreads, pw_smem_, st_>>>(pa);
   RDCU_TRY(cudaGetLastError());
   if (ng_ > 0) RDCU_TRY(planT_.run_linear(tin_, tout_, st_));
   CombineArgs ca{};
   ca.n = n_;
   ca.nfold = T.nfold;
   ca.nq = nq_;
+  ca.final_stage = stage == 1;
   ca.N = N_;
+  ca.nN = nN_;
   ca.folds = T.folds;
   ca.qs = T.qs;
   ca.ubar = ubar_;
   ca.G = tout_;
   ca.u = Y;
-  ca.Yb = Yb;
+  ca.Yb = Yb_ + (size_t)(stage - 1) * nN_;
+  ca.lam = lam_;
   ca.part = part_;
-  k_adj_combine<<<blocks, kThreads, 0, st_>>>(ca);
-  RDCU_TRY(cudaGetLastError());
-  k_adj_reduce<<<std::max(1, nterms), kThreads, 0, st_>>>(part_, nterms, gC_);
+  k_adj_combine<<<kBlocks, kThreads, 0, st_>>>(ca);
   return cudaGetLastError();
+}
+
+template <typename F>
+static cudaError_t capture(cudaStream_t st, cudaGraphExec_t* out, F&& body) {
+  RDCU_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = body();
+  cudaGraph_t g = nullptr;
+  cudaError_t e2 = cudaStreamEndCapture(st, &g);
+  if (e == cudaSuccess) e = e2;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(out, g, 0);
+  if (g) cudaGraphDestroy(g);
+  return e;
 }
 
 cudaError_t AdjointEngine::backward(const double* lambdaT, double* grad_y0, double* grad_C) {
   if (ckpt_.empty()) return cudaErrorInvalidValue;  // no forward run recorded
   const size_t sb = (size_t)nN_ * sizeof(double);
   RDCU_TRY(cudaMemcpyAsync(lam_, lambdaT, sb, cudaMemcpyDefault, st_));
-  RDCU_TRY(cudaMemsetAsync(gC_, 0, sizeof(double) * std::max(1, nterms), st_));
+  RDCU_TRY(cudaMemsetAsync(part_, 0, sizeof(double) * std::max(1, nterms) * kBlocks, st_));
   const int nseg = (nsteps_ + K_ - 1) / K_;
-  const unsigned gb = (unsigned)((nN_ + 255) / 256);
+  if (nseg > 0) RDCU_TRY(ensure_store(std::min(K_, nsteps_)));
   for (int seg = nseg - 1; seg >= 0; --seg) {
-    const int steps = std::min(K_, nsteps_ - seg * K_);
-    RDCU_TRY(recompute_segment(seg, steps));
-    for (int j = steps - 1; j >= 0; --j) {
-      const double* Ystore = store_ + (size_t)j * 6 * nN_;
-      const double h = hs_[seg * K_ + j];
-      for (int i = 6; i >= 1; --i) {
-        Coef7 ha{};
-        for (int l = i + 1; l <= 6; ++l) ha.c[l] = h * kA[l][i - 1];
-        k_adj_kbar<<<gb, 256, 0, st_>>>(tin_, lam_, Yb_, nN_, h * kA[7][i - 1], ha, i);
-        RDCU_TRY(cudaGetLastError());
-        RDCU_TRY(vjp(Ystore + (size_t)(i - 1) * nN_, Yb_ + (size_t)(i - 1) * nN_));
+    const int j0 = seg * K_, steps = std::min(K_, nsteps_ - j0);
+    RDCU_TRY(cudaMemcpyAsync(dp_->bufs.ybuf[0], ckpt_[seg], sb, cudaMemcpyDeviceToDevice, st_));
+    if (uniform_h_ && use_graphs && steps <= kMaxGraphSteps) {
+      // segments of equal length and step size replay the same two graphs
+      SegGraphs* g = nullptr;
+      for (auto& e : graphs_)
+        if (e.steps == steps && e.h == hs_[j0]) g = &e;
+      if (!g) {
+        SegGraphs e{};
+        e.steps = steps;
+        e.h = hs_[j0];
+        RDCU_TRY(capture(st_, &e.rec, [&] { return launch_recompute(j0, steps); }));
+        RDCU_TRY(capture(st_, &e.rev, [&] { return launch_reverse(j0, steps); }));
+        graphs_.push_back(e);
+        g = &graphs_.back();
       }
-      k_adj_lambda<<<gb, 256, 0, st_>>>(lam_, Yb_, nN_);
-      RDCU_TRY(cudaGetLastError());
+      RDCU_TRY(cudaGraphLaunch(g->rec, st_));
+      RDCU_TRY(cudaGraphLaunch(g->rev, st_));
+    } else {
+      RDCU_TRY(launch_recompute(j0, steps));
+      RDCU_TRY(launch_reverse(j0, steps));
     }
   }
+  k_adj_reduce<<<std::max(1, nterms), kThreads, 0, st_>>>(part_, nterms, gC_);
+  RDCU_TRY(cudaGetLastError());
   if (grad_y0) RDCU_TRY(cudaMemcpyAsync(grad_y0, lam_, sb, cudaMemcpyDefault, st_));
   std::vector<double> g(std::max(1, nterms));
   RDCU_TRY(cudaMemcpyAsync(g.data(), gC_, sizeof(double) * std::max(1, nterms), cudaMemcpyDeviceToHost, st_));

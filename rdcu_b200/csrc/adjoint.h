@@ -30,6 +30,7 @@ class AdjointEngine {
 
   size_t device_bytes = 0;
   int nterms = 0;
+  bool use_graphs = true;  // replay full segments as CUDA graphs (uniform step size)
 
  private:
   SpectralPlan* fwd_ = nullptr;
@@ -41,7 +42,8 @@ class AdjointEngine {
   std::vector<double> hs_;
   bool uniform_h_ = true;
   int nsteps_ = 0, K_ = 0;
-  std::vector<double*> ckpt_;       // state at steps 0, K, 2K, ...
+  std::vector<double*> ckpt_;       // state at steps 0, K, 2K, ... of the last forward run
+  std::vector<double*> ckpt_pool_;  // every checkpoint buffer allocated so far
   // segment store: stage states Y_1..Y_6 of up to K steps
   double* store_ = nullptr;
   int store_steps_ = 0;
@@ -58,12 +60,22 @@ class AdjointEngine {
   SpectralPlan planQ_, planT_;
   bool have_q_ = false;
   int nq_ = 0, ng_ = 0, nfold_pairs_ = 0;
+  size_t pw_smem_ = 0;  // dynamic shared memory of the pointwise kernel
   // tables (device)
   struct Tables;
   Tables* tab_ = nullptr;
   std::vector<HostTerm> terms_;
-  cudaError_t vjp(const double* Y, double* Yb);
-  cudaError_t recompute_segment(int seg, int steps);
+  struct SegGraphs {
+    int steps;
+    double h;
+    cudaGraphExec_t rec, rev;
+  };
+  std::vector<SegGraphs> graphs_;
+  cudaError_t vjp(const double* Y, int stage, double h);
+  cudaError_t ensure_store(int steps);
+  void drop_graphs();
+  cudaError_t launch_recompute(int j0, int steps);
+  cudaError_t launch_reverse(int j0, int steps);
 };
 
 }  // namespace rdcu

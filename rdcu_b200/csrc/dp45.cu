@@ -158,6 +158,22 @@ __global__ void k_dp45_copy_y(DP45Bufs b, const DP45Ctl* c, double* dst, long lo
 
 __global__ void k_dp45_set_h(DP45Ctl* c, double h) { c->h = h; }
 
+// state slots back to their initial assignment at (t, h); y is then in ybuf[0]
+__global__ void k_dp45_reset(DP45Ctl* c, double t, double h) {
+  c->t = t;
+  c->h = h;
+  c->t_last = t;
+  c->y_slot = 0;
+  c->yn_slot = 1;
+  c->yl_slot = 2;
+  c->k1_buf = 0;
+  c->k7_buf = 6;
+  c->last_k1_buf = 0;
+  c->last_k7_buf = 6;
+  c->running = 0;
+  c->accepted = 0;
+}
+
 }  // namespace
 
 #define RDCU_TRY(x)                   \
@@ -321,6 +337,13 @@ cudaError_t DP45Engine::copy_current_y(double* dst) {
   return cudaGetLastError();
 }
 
+cudaError_t DP45Engine::reset_async(double t, double h) {
+  k_dp45_reset<<<1, 1, 0, st_>>>(d_ctl_, t, h);
+  k1_valid_ = false;
+  have_step_ = false;
+  return cudaGetLastError();
+}
+
 cudaError_t DP45Engine::set_h_async(double h) {
   k_dp45_set_h<<<1, 1, 0, st_>>>(d_ctl_, h);
   return cudaGetLastError();
@@ -383,19 +406,25 @@ cudaError_t DP45Engine::step(double* t, double* h, double hmin, double hmax, int
 cudaError_t DP45Engine::advance(int n, double hmin, double hmax, long long* accepted) {
   RDCU_TRY(sync_ctl());
   const long long acc0 = host_ctl.n_accepted;
-  // loop mode without outputs: the controller stops after n attempts (or at h <= hmin)
-  RDCU_TRY(arm(1, INFINITY, hmin, hmax, 0, 0, std::max(1, n)));
-  if (!k1_valid_) {
-    RDCU_TRY(launch_k1());
-    k1_valid_ = true;
-  }
-  RDCU_TRY(ensure_graph());
-  for (int k = 0; k < n; ++k) {
-    if (graph_exec_)
-      RDCU_TRY(cudaGraphLaunch(graph_exec_, st_));
-    else
-      RDCU_TRY(launch_attempt());
-  }
+  // loop mode without outputs: the controller stops after n attempts (or at h <= hmin);
+  // it is re-armed every log_cap_ attempts, since a full attempt log also stops it
+  int done = 0;
+  do {
+    const int chunk = std::min(n - done, log_cap_);
+    RDCU_TRY(arm(1, INFINITY, hmin, hmax, 0, 0, std::max(1, chunk)));
+    if (!k1_valid_) {
+      RDCU_TRY(launch_k1());
+      k1_valid_ = true;
+    }
+    RDCU_TRY(ensure_graph());
+    for (int k = 0; k < chunk; ++k) {
+      if (graph_exec_)
+        RDCU_TRY(cudaGraphLaunch(graph_exec_, st_));
+      else
+        RDCU_TRY(launch_attempt());
+    }
+    done += chunk;
+  } while (done < n);
   RDCU_TRY(sync_ctl());
   *accepted = host_ctl.n_accepted - acc0;
   if (host_ctl.accepted) have_step_ = true;

@@ -52,6 +52,10 @@ class DP45Engine {
   cudaError_t copy_current_y(double* dst);
   // sets the step size of the next attempt on the device; no sync
   cudaError_t set_h_async(double h);
+  // (t, h) and the slot assignment of set_state, queued on the stream (no sync, no
+  // copy: the caller fills bufs.ybuf[0]); stream-capturable
+  cudaError_t reset_async(double t, double h);
+  int log_cap() const { return log_cap_; }
   cudaError_t arm(int check, double t1, double hmin, double hmax, int eval_i, int n_eval,
                   int max_attempts);
   // the cached slope k1 = f(y) is stale (new coefficients): recompute it before the next attempt

@@ -229,3 +229,19 @@ def test_error_paths(cuda):
     assert e.value.code == R.RDCU_ERR_UNSUPPORTED
     for x in (a, s, b):
         x.close()
+
+
+def test_long_segments_and_step_sequences(cuda):
+    """Segments longer than the controller's attempt log (4096) and a non-uniform step
+    sequence (direct launches): K = nsteps and K = 1000 agree bitwise."""
+    rng = np.random.default_rng(17)
+    prob = Problem(2, (8, 8), (10.0, 10.0), cgle_terms(2))
+    y0 = smooth_field(rng, prob, amp=0.5)
+    hs = [1e-4 * (1.0 + 0.1 * (j % 3)) for j in range(4200)]
+    w = rng.normal(size=y0.size)
+    s = _solver(prob)
+    a = _grads(cuda, s, y0, hs, 4200, w)
+    b = _grads(cuda, s, y0, hs, 1000, w)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+    s.close()

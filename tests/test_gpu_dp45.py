@@ -145,3 +145,16 @@ def test_solve_events_match_oracle_run(cuda):
     assert len(ev["ckpt"]) == 3
     acc, att = s.counters()
     assert acc == sum(oacc) and att == len(oacc)
+
+
+def test_advance_beyond_the_attempt_log(cuda):
+    """rdcu_advance re-arms the device controller past its 4096-entry attempt log."""
+    rng = np.random.default_rng(21)
+    prob = Problem(2, (16, 16), (20.0, 20.0), cgle_terms(2))
+    y0 = smooth_field(rng, prob, amp=0.5)
+    s, yd = _setup(cuda, prob, y0, fixed=True)
+    s.set_state(0.0, 1e-4, yd.data_ptr())
+    assert s.advance(5000) == 5000
+    t, h, _ = s.get_state()
+    assert abs(t - 0.5) < 1e-12 and h == 1e-4
+    s.close()
