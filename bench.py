@@ -64,6 +64,8 @@ WORKLOADS = {
     "cgle3d_128": dict(Ns=(128, 128, 128), Ls=(200.0, 200.0, 200.0), seed=2, h0=1e-3),
     "cgle2d_256": dict(Ns=(256, 256), Ls=(100.0, 100.0), seed=1, h0=1e-3),
     "cgle2d_128": dict(Ns=(128, 128), Ls=(100.0, 100.0), seed=1, h0=1e-3),
+    # discrete adjoint: gradient of a terminal mismatch over 5000 fixed steps (see run_adjoint)
+    "adjoint_cgle2d_256": dict(Ns=(256, 256), Ls=(200.0, 200.0), seed=1, h=1e-3, T=5.0, K=50),
 }
 
 
@@ -269,6 +271,112 @@ def run_ours(args, rank, world, local_rank):
     return line
 
 
+def run_adjoint(args):
+    """Gradient workload: 2D CGLE 256^2, L = 200, fixed h = 1e-3 to T = 5 (5000 steps),
+    checkpoints every 50 steps.  Loss = mean squared mismatch at T against a target the
+    method generates from coefficients scaled by 1 + 0.05 N(0,1) (numpy seed 7); gradients
+    with respect to all 18 coefficients and the 2 x 256^2 initial state.  value = grid
+    points x steps / (forward with checkpoints + backward) seconds; cost_ratio = that time
+    over a plain forward run (rdcu_advance) of the same steps; fd_check = central
+    differences with eps = 1e-6 along 8 random unit coefficient directions."""
+    import torch
+
+    import rdcu_b200 as R
+
+    wl = WORKLOADS[args.workload]
+    Ns, Ls = wl["Ns"], wl["Ls"]
+    N = int(np.prod(Ns))
+    nN = 2 * N
+    nsteps = int(round(wl["T"] / wl["h"]))
+    hs = [wl["h"]] * nsteps
+    terms = parse_terms(cgle_lines(2))
+    C = np.array([c for c, _ in terms])
+    s = R.Solver(2, Ns, Ls, terms, fixed=True)
+    stream = torch.cuda.ExternalStream(s.stream)
+    y0 = torch.tensor(R.random_ic(2, N, 2.0, 0.0, wl["seed"]), dtype=torch.float64, device="cuda")
+    rng = np.random.default_rng(7)
+    Cp = C * (1.0 + 0.05 * rng.normal(size=C.size))
+    target = torch.empty_like(y0)
+    yT = torch.empty_like(y0)
+    g = torch.empty_like(y0)
+    torch.cuda.synchronize()
+    s.set_coefficients(list(Cp))
+    s.adjoint_forward(y0.data_ptr(), hs, wl["K"], target.data_ptr())
+    s.set_coefficients(list(C))
+
+    def loss(out):
+        return float(((out - target) ** 2).mean())
+
+    # warm-up (graph capture of the segment sweeps happens here)
+    s.adjoint_forward(y0.data_ptr(), hs[:2 * wl["K"]], wl["K"], yT.data_ptr())
+    lam = (2.0 / nN) * (yT - target)
+    s.adjoint_backward(lam.data_ptr(), g.data_ptr())
+    torch.cuda.synchronize()
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return r, e0.elapsed_time(e1) / 1e3
+
+    with ClockSampler(0) as clk:
+        s.set_state(0.0, wl["h"], y0.data_ptr())
+        _, t_plain = timed(lambda: s.advance(nsteps))
+        _, t_fwd = timed(lambda: s.adjoint_forward(y0.data_ptr(), hs, wl["K"], yT.data_ptr()))
+        L0 = loss(yT)
+        lam = (2.0 / nN) * (yT - target)
+        torch.cuda.synchronize()
+        gC, t_bwd = timed(lambda: s.adjoint_backward(lam.data_ptr(), g.data_ptr()))
+    gC = np.array(gC)
+    # e2e: host arrays through the C ABI (the library stages them)
+    y0_h = torch.empty(nN, dtype=torch.float64).pin_memory()
+    y0_h.copy_(y0.cpu())
+    yT_h = torch.empty(nN, dtype=torch.float64).pin_memory()
+    g_h = torch.empty(nN, dtype=torch.float64).pin_memory()
+    tgt_h = target.cpu().numpy()
+    w0 = time.perf_counter()
+    s.adjoint_forward(y0_h.data_ptr(), hs, wl["K"], yT_h.data_ptr())
+    lam_h = torch.from_numpy((2.0 / nN) * (yT_h.numpy() - tgt_h)).pin_memory()
+    s.adjoint_backward(lam_h.data_ptr(), g_h.data_ptr())
+    e2e_s = time.perf_counter() - w0
+    # central differences along random unit coefficient directions
+    fd = []
+    for _ in range(8):
+        d = rng.normal(size=C.size)
+        d /= np.linalg.norm(d)
+        eps = 1e-6
+        vals = []
+        for sgn in (1, -1):
+            s.set_coefficients(list(C + sgn * eps * d))
+            s.adjoint_forward(y0.data_ptr(), hs, nsteps, yT.data_ptr())
+            vals.append(loss(yT))
+        fdv = (vals[0] - vals[1]) / (2 * eps)
+        adj = float(np.dot(gC, d))
+        fd.append({"fd": fdv, "adjoint": adj, "rel_err": abs(fdv - adj) / max(abs(fdv), 1e-300)})
+    s.set_coefficients(list(C))
+    s.close()
+    work = float(N) * nsteps
+    t_grad = t_fwd + t_bwd
+    return {
+        "metric": "grid-pt·steps/s (gradient: forward with checkpoints + adjoint)", "value": work / t_grad,
+        "unit": "grid-pt·steps/s", "n_gpus": 1, "steps": nsteps, "warmup": 1, "ms_per_step": t_grad * 1e3 / nsteps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "grid": list(Ns), "L": list(Ls), "h": wl["h"], "T": wl["T"],
+                   "checkpoint_every": wl["K"], "terms": len(terms), "loss": "mean squared mismatch vs target "
+                   "from coefficients x (1 + 0.05 N(0,1)), seed 7", "ic": "glibc rand seed %d" % wl["seed"],
+                   "l2": "state 1 MB: L2-resident (latency-bound regime)"},
+        "cost_ratio": t_grad / t_plain, "seconds": {"plain_forward": t_plain, "forward_checkpointed": t_fwd,
+                                                    "backward": t_bwd},
+        "loss": L0, "fd_check": {"eps": 1e-6, "directions": 8, "max_rel_err": max(f["rel_err"] for f in fd),
+                                 "cases": fd},
+        "clocks": clk.summary(),
+        "e2e": {"value": work / e2e_s, "unit": "grid-pt·steps/s", "h2d_bytes_per_step": 2 * nN * 8 / nsteps,
+                "d2h_bytes_per_step": 2 * nN * 8 / nsteps, "seconds": e2e_s},
+    }
+
+
 def launches_per_attempt(ndim):
     per_stage = {1: 3, 2: 3, 3: 5}[ndim]
     return 6 * per_stage + 1
@@ -302,6 +410,8 @@ def reference_binary():
 
 
 def run_reference(args):
+    if args.workload.startswith("adjoint"):
+        return {"impl": "reference", "unavailable": "the reference computes no gradients (no adjoint to time)"}
     exe, why = reference_binary()
     if exe is None:
         return {"impl": "reference", "unavailable": why}
@@ -371,7 +481,10 @@ def main():
 
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    line = run_ours(args, rank, world, local_rank)
+    if args.workload.startswith("adjoint"):
+        line = run_adjoint(args) if rank == 0 else None
+    else:
+        line = run_ours(args, rank, world, local_rank)
     if world > 1:
         import torch.distributed as dist
 

@@ -213,6 +213,37 @@ int rdcu_adjoint_forward(rdcu_t *h, const double *y0, const double *hs, int nste
                          double *yT);
 int rdcu_adjoint_backward(rdcu_t *h, const double *lambdaT, double *grad_y0, double *grad_C);
 
+/* ---- ensembles ---------------------------------------------------------------------
+ * No counterpart in the reference (one problem per process).  Many independent 2D
+ * pseudospectral DP45 problems -- each with its own grid, lengths, coupling terms and
+ * tolerances -- stepped together: every FFT pass of a stage is one persistent launch over
+ * all members' tiles, each member keeps its own adaptive step control on the device,
+ * and one ensemble attempt is replayed as a CUDA graph.  A member's trajectory is
+ * bitwise the one a single handle with the same spec produces (same accepted and
+ * rejected steps, same states).
+ *
+ * rdcu_ensemble_create: specs[0..count) as for rdcu_create, with method DP45, ndim 2 and
+ *   fixed 0; every spec names the same device.
+ * rdcu_ensemble_set_state / get_state: (t, h, y) of member i (y host or device).
+ * rdcu_ensemble_solve: every member from its state until its first accepted step at or
+ *   past t1 (the end condition of rdcu_solve without outputs); synchronous.
+ * rdcu_ensemble_counters: accepted steps and attempts of member i since its set_state.
+ * rdcu_ensemble_tune: times one batched RHS stage for a few tile sizes (complex values
+ *   per CTA) and keeps the fastest; *tile_elems receives it.  States are kept.
+ * rdcu_ensemble_info: member count, the stream (cudaStream_t) and device bytes. */
+typedef struct rdcu_ensemble rdcu_ensemble_t;
+int rdcu_ensemble_create(rdcu_ensemble_t **out, const rdcu_spec *specs, int count);
+int rdcu_ensemble_destroy(rdcu_ensemble_t *e);
+int rdcu_ensemble_set_state(rdcu_ensemble_t *e, int i, double t, double hstep, const double *y);
+int rdcu_ensemble_get_state(rdcu_ensemble_t *e, int i, double *t, double *hstep, double *y);
+int rdcu_ensemble_solve(rdcu_ensemble_t *e, double t1, double hmin, double hmax);
+int rdcu_ensemble_counters(rdcu_ensemble_t *e, int i, long long *accepted, long long *attempts);
+int rdcu_ensemble_tune(rdcu_ensemble_t *e, int *tile_elems);
+int rdcu_ensemble_info(rdcu_ensemble_t *e, int *count, void **stream, long long *device_bytes);
+/* Last error message of the ensemble (or of the last failed rdcu_ensemble_create when
+ * e is NULL). */
+const char *rdcu_ensemble_last_error(rdcu_ensemble_t *e);
+
 /* ---- allocation-free RHS ----------------------------------------------------------
  * No counterpart in the reference: an addition for callers that cannot allocate device
  * memory.  Examples: code that runs under a device-memory budget owned by another

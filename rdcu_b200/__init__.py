@@ -44,7 +44,9 @@ EXPORTS = [
     "rdcu_rhs", "rdcu_jac", "rdcu_step", "rdcu_eval", "rdcu_solve", "rdcu_get_counters",
     "rdcu_memcpy", "rdcu_advance", "rdcu_random_ic", "rdcu_profile_passes", "rdcu_rhs_noalloc",
     "rdcu_set_coefficients", "rdcu_adjoint_forward", "rdcu_adjoint_backward",
-    "rdcu_error_string", "rdcu_last_error",
+    "rdcu_ensemble_create", "rdcu_ensemble_destroy", "rdcu_ensemble_set_state", "rdcu_ensemble_get_state",
+    "rdcu_ensemble_solve", "rdcu_ensemble_counters", "rdcu_ensemble_tune", "rdcu_ensemble_info",
+    "rdcu_ensemble_last_error", "rdcu_error_string", "rdcu_last_error",
 ]
 
 
@@ -120,12 +122,23 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
     lib.rdcu_set_coefficients.argtypes = [vp, pd]
     lib.rdcu_adjoint_forward.argtypes = [vp, vp, pd, i, i, vp]
     lib.rdcu_adjoint_backward.argtypes = [vp, vp, vp, pd]
+    ll = ctypes.c_longlong
+    lib.rdcu_ensemble_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(rdcu_spec), i]
+    lib.rdcu_ensemble_destroy.argtypes = [vp]
+    lib.rdcu_ensemble_set_state.argtypes = [vp, i, d, d, vp]
+    lib.rdcu_ensemble_get_state.argtypes = [vp, i, pd, pd, vp]
+    lib.rdcu_ensemble_solve.argtypes = [vp, d, d, d]
+    lib.rdcu_ensemble_counters.argtypes = [vp, i, ctypes.POINTER(ll), ctypes.POINTER(ll)]
+    lib.rdcu_ensemble_tune.argtypes = [vp, pi]
+    lib.rdcu_ensemble_info.argtypes = [vp, pi, ctypes.POINTER(vp), ctypes.POINTER(ll)]
+    lib.rdcu_ensemble_last_error.argtypes = [vp]
+    lib.rdcu_ensemble_last_error.restype = ctypes.c_char_p
     lib.rdcu_error_string.argtypes = [i]
     lib.rdcu_error_string.restype = ctypes.c_char_p
     lib.rdcu_last_error.argtypes = [vp]
     lib.rdcu_last_error.restype = ctypes.c_char_p
     for name in EXPORTS:
-        if name not in ("rdcu_error_string", "rdcu_last_error"):
+        if name not in ("rdcu_error_string", "rdcu_last_error", "rdcu_ensemble_last_error"):
             getattr(lib, name).restype = ctypes.c_int
     if path is None:
         _lib = lib
@@ -352,3 +365,104 @@ class Solver:
         self._check(self.lib.rdcu_adjoint_backward(self.h, ctypes.c_void_p(lamT_ptr),
                                                    ctypes.c_void_p(grad_y0_ptr) if grad_y0_ptr else None, g))
         return [g[k] for k in range(self.nterms)]
+
+
+class _SpecHolder:
+    """An rdcu_spec with the term arrays it points to kept alive."""
+
+    def __init__(self, n, Ns, Ls, terms, method=METHOD_DP45, rtol=1e-8, atol=1e-8, fixed=False, device=0):
+        ndim = len(Ns)
+        terms = [(float(C), list(ints)) for C, ints in terms]
+        self._C = (ctypes.c_double * max(1, len(terms)))(*[t[0] for t in terms])
+        self._np = (ctypes.c_int * max(1, len(terms)))(*[len(t[1]) for t in terms])
+        self._lists = [(ctypes.c_int * max(1, len(t[1])))(*t[1]) for t in terms]
+        self._c = (ctypes.POINTER(ctypes.c_int) * max(1, len(terms)))(
+            *[ctypes.cast(l, ctypes.POINTER(ctypes.c_int)) for l in self._lists])
+        sp = rdcu_spec()
+        sp.n = n
+        sp.ndim = ndim
+        for a in range(3):
+            sp.Ns[a] = Ns[a] if a < ndim else 1
+            sp.Ls[a] = Ls[a] if a < ndim else 1.0
+        sp.nterms = len(terms)
+        sp.C = ctypes.cast(self._C, ctypes.POINTER(ctypes.c_double))
+        sp.nprods = ctypes.cast(self._np, ctypes.POINTER(ctypes.c_int))
+        sp.c = ctypes.cast(self._c, ctypes.POINTER(ctypes.POINTER(ctypes.c_int)))
+        sp.method = method
+        sp.fixed = 1 if fixed else 0
+        sp.rtol = rtol
+        sp.atol = atol
+        sp.device = device
+        self.spec = sp
+
+
+class Ensemble:
+    """Many 2D DP45 problems stepped together (``rdcu_ensemble_t``).
+
+    ``members`` is a list of dicts with keys n, Ns, Ls, terms and optionally rtol, atol.
+    """
+
+    def __init__(self, members, device: int = 0):
+        self.lib = load_library()
+        holders = [_SpecHolder(m["n"], m["Ns"], m["Ls"], m["terms"], rtol=m.get("rtol", 1e-8),
+                               atol=m.get("atol", 1e-8), device=device) for m in members]
+        arr = (rdcu_spec * len(holders))(*[h.spec for h in holders])
+        e = ctypes.c_void_p()
+        rc = self.lib.rdcu_ensemble_create(ctypes.byref(e), arr, len(holders))
+        if rc != RDCU_OK:
+            raise RdcuError(rc, self.lib.rdcu_ensemble_last_error(None).decode())
+        self.e = e
+        self.sizes = [m["n"] * m["Ns"][0] * m["Ns"][1] for m in members]
+
+    def _check(self, rc):
+        if rc != RDCU_OK:
+            raise RdcuError(rc, self.lib.rdcu_ensemble_last_error(self.e).decode())
+
+    def close(self):
+        if getattr(self, "e", None):
+            self.lib.rdcu_ensemble_destroy(self.e)
+            self.e = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self):
+        return len(self.sizes)
+
+    def set_state(self, i: int, t: float, h: float, y_ptr: int):
+        self._check(self.lib.rdcu_ensemble_set_state(self.e, i, t, h, ctypes.c_void_p(y_ptr)))
+
+    def get_state(self, i: int, y_ptr: int = 0):
+        t, h = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.rdcu_ensemble_get_state(self.e, i, ctypes.byref(t), ctypes.byref(h),
+                                                     ctypes.c_void_p(y_ptr) if y_ptr else None))
+        return t.value, h.value
+
+    def solve(self, t1: float, hmin: float = 0.0, hmax: float = float("inf")):
+        self._check(self.lib.rdcu_ensemble_solve(self.e, t1, hmin, hmax))
+
+    def counters(self, i: int):
+        a, b = ctypes.c_longlong(), ctypes.c_longlong()
+        self._check(self.lib.rdcu_ensemble_counters(self.e, i, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def tune(self) -> int:
+        v = ctypes.c_int()
+        self._check(self.lib.rdcu_ensemble_tune(self.e, ctypes.byref(v)))
+        return v.value
+
+    @property
+    def stream(self) -> int:
+        c, st, b = ctypes.c_int(), ctypes.c_void_p(), ctypes.c_longlong()
+        self._check(self.lib.rdcu_ensemble_info(self.e, ctypes.byref(c), ctypes.byref(st), ctypes.byref(b)))
+        return st.value
+
+    @property
+    def device_bytes(self) -> int:
+        c, st, b = ctypes.c_int(), ctypes.c_void_p(), ctypes.c_longlong()
+        self._check(self.lib.rdcu_ensemble_info(self.e, ctypes.byref(c), ctypes.byref(st), ctypes.byref(b)))
+        return b.value
+

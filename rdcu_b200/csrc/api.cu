@@ -14,6 +14,7 @@
 #include "adjoint.h"
 #include "bdf.h"
 #include "dp45.h"
+#include "ensemble.h"
 #include "fd.h"
 #include "spectral.h"
 
@@ -516,5 +517,153 @@ int rdcu_adjoint_backward(rdcu_t* h, const double* lambdaT, double* grad_y0, dou
   CHECK_CUDA(h, h->adj->backward(lambdaT, grad_y0, grad_C), "rdcu_adjoint_backward");
   return RDCU_OK;
 }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------- ensembles
+struct rdcu_ensemble {
+  EnsembleEngine eng;
+  cudaStream_t stream = nullptr;
+  int device = 0;
+  std::string err;
+};
+
+static thread_local std::string g_ens_create_error;
+
+static int ens_err(rdcu_ensemble_t* e, int code, const std::string& msg) {
+  if (e)
+    e->err = msg;
+  else
+    g_ens_create_error = msg;
+  return code;
+}
+
+#define ENS_CUDA(e, x, where)                                                                            \
+  do {                                                                                                   \
+    cudaError_t _c = (x);                                                                                \
+    if (_c != cudaSuccess) return ens_err(e, RDCU_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(_c)); \
+  } while (0)
+
+extern "C" {
+
+int rdcu_ensemble_create(rdcu_ensemble_t** out, const rdcu_spec* specs, int count) {
+  if (!out || !specs || count < 1) return ens_err(nullptr, RDCU_ERR_INVALID, "bad argument");
+  *out = nullptr;
+  std::vector<EnsembleProblem> probs(count);
+  const int dev = specs[0].device;
+  for (int i = 0; i < count; ++i) {
+    const rdcu_spec& s = specs[i];
+    const std::string who = "member " + std::to_string(i) + ": ";
+    if (s.method != RDCU_METHOD_DP45 || s.ndim != 2 || s.fixed)
+      return ens_err(nullptr, RDCU_ERR_UNSUPPORTED, who + "ensembles take adaptive 2D DP45 problems");
+    if (s.device != dev) return ens_err(nullptr, RDCU_ERR_INVALID, who + "all members must use one device");
+    if (s.n < 1 || s.Ns[0] < 1 || s.Ns[1] < 1 || !(s.Ls[0] != 0) || !(s.Ls[1] != 0))
+      return ens_err(nullptr, RDCU_ERR_INVALID, who + "bad n, grid or lengths");
+    if (s.nterms < 0 || (s.nterms > 0 && (!s.C || !s.nprods || !s.c)))
+      return ens_err(nullptr, RDCU_ERR_INVALID, who + "bad coupling-term arrays");
+    EnsembleProblem& p = probs[i];
+    p.n = s.n;
+    p.Ns[0] = s.Ns[0];
+    p.Ns[1] = s.Ns[1];
+    p.Ls[0] = s.Ls[0];
+    p.Ls[1] = s.Ls[1];
+    const int nY = 1 + 2 + 4;
+    for (int k = 0; k < s.nterms; ++k) {
+      HostTerm t;
+      t.C = s.C[k];
+      const int np = s.nprods[k];
+      if (np < 0 || (np > 0 && !s.c[k])) return ens_err(nullptr, RDCU_ERR_INVALID, who + "bad coupling term list");
+      t.ints.assign(s.c[k], s.c[k] + np);
+      const int field = np > 0 ? t.ints[0] : 0;
+      if (field < 0 || field >= s.n) return ens_err(nullptr, RDCU_ERR_INVALID, who + "field out of range");
+      for (int j = 1; j < np; j += 2)
+        if (t.ints[j] < 0 || t.ints[j] >= nY * s.n) return ens_err(nullptr, RDCU_ERR_INVALID, who + "Y index out of range");
+      p.terms.push_back(std::move(t));
+    }
+  }
+  std::unique_ptr<rdcu_ensemble> e(new rdcu_ensemble);
+  e->device = dev;
+  cudaError_t c = cudaSetDevice(dev);
+  if (c != cudaSuccess) return ens_err(nullptr, RDCU_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(c));
+  c = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+  if (c != cudaSuccess) return ens_err(nullptr, RDCU_ERR_CUDA, std::string("stream: ") + cudaGetErrorString(c));
+  std::string msg;
+  // per-member tolerances: the controllers hold them; the engine takes the first pair
+  // and the loop below overrides each member's
+  if (!e->eng.init(probs, specs[0].rtol, specs[0].atol, e->stream, &msg)) {
+    e->eng.release();
+    cudaStreamDestroy(e->stream);
+    return ens_err(nullptr, msg.find("memory") != std::string::npos ? RDCU_ERR_NOMEM : RDCU_ERR_UNSUPPORTED, msg);
+  }
+  for (int i = 0; i < count; ++i) {
+    c = e->eng.set_tolerances(i, specs[i].rtol, specs[i].atol);
+    if (c != cudaSuccess) {
+      e->eng.release();
+      cudaStreamDestroy(e->stream);
+      return ens_err(nullptr, RDCU_ERR_CUDA, std::string("ensemble tolerances: ") + cudaGetErrorString(c));
+    }
+  }
+  *out = e.release();
+  return RDCU_OK;
+}
+
+int rdcu_ensemble_destroy(rdcu_ensemble_t* e) {
+  if (!e) return RDCU_OK;
+  cudaSetDevice(e->device);
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  e->eng.release();
+  if (e->stream) cudaStreamDestroy(e->stream);
+  delete e;
+  return RDCU_OK;
+}
+
+int rdcu_ensemble_set_state(rdcu_ensemble_t* e, int i, double t, double hstep, const double* y) {
+  if (!e || !y) return ens_err(e, RDCU_ERR_INVALID, "null argument");
+  if (i < 0 || i >= e->eng.size()) return ens_err(e, RDCU_ERR_INVALID, "member index out of range");
+  ENS_CUDA(e, cudaSetDevice(e->device), "cudaSetDevice");
+  ENS_CUDA(e, e->eng.set_state(i, t, hstep, y), "rdcu_ensemble_set_state");
+  return RDCU_OK;
+}
+
+int rdcu_ensemble_get_state(rdcu_ensemble_t* e, int i, double* t, double* hstep, double* y) {
+  if (!e) return ens_err(e, RDCU_ERR_INVALID, "null argument");
+  if (i < 0 || i >= e->eng.size()) return ens_err(e, RDCU_ERR_INVALID, "member index out of range");
+  ENS_CUDA(e, cudaSetDevice(e->device), "cudaSetDevice");
+  ENS_CUDA(e, e->eng.get_state(i, t, hstep, y), "rdcu_ensemble_get_state");
+  return RDCU_OK;
+}
+
+int rdcu_ensemble_solve(rdcu_ensemble_t* e, double t1, double hmin, double hmax) {
+  if (!e) return ens_err(e, RDCU_ERR_INVALID, "null argument");
+  ENS_CUDA(e, cudaSetDevice(e->device), "cudaSetDevice");
+  ENS_CUDA(e, e->eng.solve(t1, hmin, hmax), "rdcu_ensemble_solve");
+  return RDCU_OK;
+}
+
+int rdcu_ensemble_counters(rdcu_ensemble_t* e, int i, long long* accepted, long long* attempts) {
+  if (!e) return ens_err(e, RDCU_ERR_INVALID, "null argument");
+  if (i < 0 || i >= e->eng.size()) return ens_err(e, RDCU_ERR_INVALID, "member index out of range");
+  ENS_CUDA(e, cudaSetDevice(e->device), "cudaSetDevice");
+  ENS_CUDA(e, e->eng.counters(i, accepted, attempts), "rdcu_ensemble_counters");
+  return RDCU_OK;
+}
+
+int rdcu_ensemble_tune(rdcu_ensemble_t* e, int* tile_elems) {
+  if (!e) return ens_err(e, RDCU_ERR_INVALID, "null argument");
+  ENS_CUDA(e, cudaSetDevice(e->device), "cudaSetDevice");
+  ENS_CUDA(e, e->eng.tune(nullptr), "rdcu_ensemble_tune");
+  if (tile_elems) *tile_elems = e->eng.tile_elems;
+  return RDCU_OK;
+}
+
+int rdcu_ensemble_info(rdcu_ensemble_t* e, int* count, void** stream, long long* device_bytes) {
+  if (!e) return ens_err(e, RDCU_ERR_INVALID, "null argument");
+  if (count) *count = e->eng.size();
+  if (stream) *stream = (void*)e->stream;
+  if (device_bytes) *device_bytes = (long long)e->eng.device_bytes;
+  return RDCU_OK;
+}
+
+const char* rdcu_ensemble_last_error(rdcu_ensemble_t* e) { return e ? e->err.c_str() : g_ens_create_error.c_str(); }
 
 }  // extern "C"

@@ -30,6 +30,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <type_traits>
 
 #include "fft_line.cuh"
 #include "spectral.h"
@@ -182,21 +183,6 @@ __device__ __forceinline__ double2 apply_entry_k(const ChanEntry& e, const doubl
   }
 }
 
-__device__ __forceinline__ double block_sum(double v) {
-  __shared__ double red[32];
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  __syncthreads();
-  if (lane == 0) red[wid] = v;
-  __syncthreads();
-  double s = 0.0;
-  if (threadIdx.x == 0) {
-    const int nw = (blockDim.x + 31) >> 5;
-    for (int w = 0; w < nw; ++w) s += red[w];
-  }
-  return s;
-}
-
 // ------------------------------------------------------------------------- kernels
 struct FwdXArgs {
   int M, Mh, nrows, P, do_fft, tw_smem;
@@ -264,8 +250,9 @@ __device__ __forceinline__ void fwd_load(const FwdXArgs& a, const Resolved& r, d
   }
 }
 
+// bx: the CTA's index within this plan's grid (blockIdx.x, or a work item of a batch)
 template <int RS>
-__global__ void __launch_bounds__(kMaxBlock, 1) k_fwd_x(FwdXArgs a) {
+__device__ __forceinline__ void fwd_x_body(const FwdXArgs& a, int bx) {
   extern __shared__ double2 sm[];
   if (a.io.mode == 1 && !a.io.ctl->running) return;
   const Resolved r = resolve(a.io);
@@ -278,7 +265,7 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_fwd_x(FwdXArgs a) {
     tw = tws;
     buf = sm + M;
   }
-  const long long row0 = 2LL * blockIdx.x * a.P;
+  const long long row0 = 2LL * bx * a.P;
   switch (r.stage) {
     case 2: fwd_load<2>(a, r, buf, row0); break;
     case 3: fwd_load<3>(a, r, buf, row0); break;
@@ -309,6 +296,11 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_fwd_x(FwdXArgs a) {
       o = make_double2(0.5 * (z.y + zm.y), -0.5 * (z.x - zm.x));
     a.S[g * Mh + kx] = o;
   }
+}
+
+template <int RS>
+__global__ void __launch_bounds__(kMaxBlock, 1) k_fwd_x(FwdXArgs a) {
+  fwd_x_body<RS>(a, blockIdx.x);
 }
 
 struct C2CArgs {
@@ -362,7 +354,7 @@ struct MidArgs {
 };
 
 template <int RS>
-__global__ void __launch_bounds__(kMaxBlock, 1) k_mid(MidArgs a) {
+__device__ __forceinline__ void mid_body(const MidArgs& a, int bx) {
   extern __shared__ double2 sm[];
   if (a.io.mode == 1 && !a.io.ctl->running) return;
   const int L0 = a.L0, TW = a.TW, LS = L0 + 1, T = blockDim.x, tid = threadIdx.x;
@@ -377,7 +369,7 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_mid(MidArgs a) {
   for (int t = tid; t < a.nent; t += T) se[t] = a.chan.ent[a.ent0 + t];
   for (int t = tid; t < a.chan.kv_total; t += T) skv[t] = a.chan.kv[t];
   for (int t = tid; t <= a.G; t += T) soff[t] = a.chan.off[a.ch0 + t] - a.ent0;
-  const long long i0 = (long long)blockIdx.x * TW;
+  const long long i0 = (long long)bx * TW;
   const int nload = a.nsrc * L0 * TW;
   for (int e = tid; e < nload; e += T) {
     const int q0 = fdiv(e, a.dTW), c = e - q0 * TW;
@@ -518,6 +510,11 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_mid(MidArgs a) {
     }
     __syncthreads();
   }
+}
+
+template <int RS>
+__global__ void __launch_bounds__(kMaxBlock, 1) k_mid(MidArgs a) {
+  mid_body<RS>(a, blockIdx.x);
 }
 
 struct Mult1DArgs {
@@ -716,7 +713,7 @@ struct InvXArgs {
 };
 
 template <int RS>
-__global__ void __launch_bounds__(kMaxBlock, 1) k_inv_x(InvXArgs a) {
+__device__ __forceinline__ void inv_x_body(const InvXArgs& a, int bx) {
   extern __shared__ double2 sm[];
   if (a.io.mode == 1 && !a.io.ctl->running) return;
   const Resolved r = resolve(a.io);
@@ -731,9 +728,11 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_inv_x(InvXArgs a) {
     lines = sm + M;
   }
   double* phys = reinterpret_cast<double*>(lines + (a.do_fft ? P * np * M : 0));
-  const long long r0 = (long long)blockIdx.x * P;
+  const long long r0 = (long long)bx * P;
+  // per-point squared error of stage 7 (summed over the fields), then the tables
+  double* serr = phys + (long long)P * n * M;
   // dictionary tables staged in shared memory (read by every point)
-  DictTerm* sterm = reinterpret_cast<DictTerm*>(phys + (long long)P * n * M);
+  DictTerm* sterm = reinterpret_cast<DictTerm*>(serr + (long long)P * M);
   DictFactor* sfac = reinterpret_cast<DictFactor*>(sterm + a.dict.nterms);
   int* sfb = reinterpret_cast<int*>(sfac + a.dict.nfac);
   int* sfold = sfb + n + 1;
@@ -841,13 +840,13 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_inv_x(InvXArgs a) {
   const DictTable& D = a.dict;
   // stage-7 epilogue of adaptive steps only (fixed steps pass no partials buffer)
   const bool err = (a.io.mode == 1 && r.stage == 7 && a.io.err_part != nullptr);
-  double err2 = 0.0;
   const int npts = P * M;
   for (int e = tid; e < npts; e += T) {
     const int pr = fdiv(e, a.dM);
     const int x = e - pr * M;
     const long long row = r0 + pr;
     if (row >= a.R) continue;
+    double err2 = 0.0;
     const double* ph = phys + (long long)pr * n * M + x;
     const double2* ln = lines + (long long)pr * np * M + x;
     for (int i = 0; i < n; ++i) {
@@ -886,10 +885,75 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_inv_x(InvXArgs a) {
         err2 += ev * ev;
       }
     }
+    if (err) serr[e] = err2;
   }
   if (err) {
-    const double s = block_sum(err2);
-    if (tid == 0) a.io.err_part[blockIdx.x] = s;
+    // one partial sum per grid row, in an order fixed by the row alone (x = lane,
+    // lane + 32, ..., then a butterfly over the lanes): the error norm does not depend
+    // on how rows are tiled into CTAs or on the block size
+    __syncthreads();
+    const int lane = tid & 31, nw = T >> 5;
+    for (int pr = tid >> 5; pr < P; pr += nw) {
+      const long long row = r0 + pr;
+      if (row >= a.R) break;
+      double v = 0.0;
+      for (int x = lane; x < M; x += 32) v += serr[pr * M + x];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) a.io.err_part[row] = v;
+    }
+  }
+}
+
+template <int RS>
+__global__ void __launch_bounds__(kMaxBlock, 1) k_inv_x(InvXArgs a) {
+  inv_x_body<RS>(a, blockIdx.x);
+}
+
+// ---- batched passes: persistent CTAs over (problem, tile) work items
+template <typename A>
+__device__ __forceinline__ void load_args(A* dst, const A* src) {
+  static_assert(sizeof(A) % 8 == 0, "argument blocks are copied as 8-byte words");
+  const unsigned long long* s = reinterpret_cast<const unsigned long long*>(src);
+  unsigned long long* d = reinterpret_cast<unsigned long long*>(dst);
+  for (int w = threadIdx.x; w < (int)(sizeof(A) / 8); w += blockDim.x) d[w] = s[w];
+}
+
+template <int RS>
+__global__ void __launch_bounds__(kMaxBlock, 1)
+    k_fwd_x_batch(const FwdXArgs* __restrict__ args, const int2* __restrict__ items, int nitems) {
+  __shared__ __align__(16) FwdXArgs sa;
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int2 w = items[it];
+    load_args(&sa, args + w.x);
+    __syncthreads();
+    fwd_x_body<RS>(sa, w.y);
+    __syncthreads();
+  }
+}
+
+template <int RS>
+__global__ void __launch_bounds__(kMaxBlock, 1)
+    k_mid_batch(const MidArgs* __restrict__ args, const int2* __restrict__ items, int nitems) {
+  __shared__ __align__(16) MidArgs sa;
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int2 w = items[it];
+    load_args(&sa, args + w.x);
+    __syncthreads();
+    mid_body<RS>(sa, w.y);
+    __syncthreads();
+  }
+}
+
+template <int RS>
+__global__ void __launch_bounds__(kMaxBlock, 1)
+    k_inv_x_batch(const InvXArgs* __restrict__ args, const int2* __restrict__ items, int nitems) {
+  __shared__ __align__(16) InvXArgs sa;
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int2 w = items[it];
+    load_args(&sa, args + w.x);
+    __syncthreads();
+    inv_x_body<RS>(sa, w.y);
+    __syncthreads();
   }
 }
 
@@ -978,14 +1042,16 @@ static bool opt_in_smem(const void* func) {
 // Geometry of the inverse x pass for nch_run channels (with or without the
 // physical-field staging): rows per CTA, grid, block and dynamic shared memory.
 static void inv_geometry(int M, int R, int n, int nch_run, bool yout, const LinePlan& plan, PassCfg* c,
-                         int* tw_smem, size_t extra = 0) {
+                         int* tw_smem, size_t extra = 0, int batch_elems = 0) {
   const bool spectral = nch_run > 0;
   const int np = (nch_run + 1) / 2;
   const int npm = std::max(1, np);
-  int P = std::max(1, std::min(std::max(1, cta_elems() / (M * npm)), R / kTargetCtas));
+  // a single problem spreads its rows over the GPU; a batch member only sizes its tiles
+  int P = batch_elems > 0 ? std::max(1, std::min(batch_elems / (M * npm), R))
+                          : std::max(1, std::min(std::max(1, cta_elems() / (M * npm)), R / kTargetCtas));
   auto bytes = [&](int p, bool tws) {
     return (size_t)((spectral && tws ? M : 0) + (spectral ? p * np * M : 0)) * 16 +
-           (yout ? 0 : (size_t)p * n * M * 8 + extra);
+           (yout ? 0 : (size_t)p * (n + 1) * M * 8 + extra);
   };
   while (P > 1 && bytes(P, true) > kSmemBudget) P /= 2;
   const bool tws = bytes(P, true) <= kSmemBudget;
@@ -1314,7 +1380,7 @@ bool SpectralPlan::init(int n_, int ndim_, const int* Ns_, const double* Ls_,
     int tws = 0;
     inv_geometry(M, R, n, nch, false, plan_x_, &inv_, &tws, dict_smem_bytes());
   }
-  nparts_max = inv_.grid;
+  nparts_max = R;  // stage-7 error partials: one per grid row
   // Y-mode channel group
   const int GY = std::min(ych_, 8);
   sc_rows_ = std::max(nch, 1);
@@ -1999,6 +2065,218 @@ cudaError_t SpectralPlan::run_linear(const double* in, double* out, cudaStream_t
   io.mode = 0;
   io.y = in;
   return launch_passes(io, chan_table(ch_off_, ch_ent_, nch), h_ch_off_, nch, 0, out, nullptr, st, 1);
+}
+
+// ----------------------------------------------------------------------------- batch
+struct SpectralBatch::Impl {
+  int nm = 0;
+  bool pow2 = true;
+  FwdXArgs* fwd[8] = {};
+  MidArgs* mid[8] = {};
+  InvXArgs* inv[8] = {};
+  int2* items[3] = {};
+  int nitems[3] = {0, 0, 0};
+  int grid[3] = {0, 0, 0}, block[3] = {0, 0, 0};
+  size_t smem[3] = {0, 0, 0};
+};
+
+void SpectralBatch::release() {
+  if (!impl_) return;
+  for (int s = 0; s < 8; ++s) {
+    if (impl_->fwd[s]) cudaFree(impl_->fwd[s]);
+    if (impl_->mid[s]) cudaFree(impl_->mid[s]);
+    if (impl_->inv[s]) cudaFree(impl_->inv[s]);
+  }
+  for (auto* p : impl_->items)
+    if (p) cudaFree(p);
+  delete impl_;
+  impl_ = nullptr;
+  device_bytes = 0;
+}
+
+bool SpectralBatch::init(const std::vector<BatchMember>& members, int elems_, std::string* msg) {
+  release();
+  impl_ = new Impl;
+  Impl& B = *impl_;
+  B.nm = (int)members.size();
+  elems = std::max(128, std::min(elems_, kMaxElems));
+  if (B.nm == 0) {
+    *msg = "empty batch";
+    return false;
+  }
+  std::vector<std::vector<FwdXArgs>> hf(8);
+  std::vector<std::vector<MidArgs>> hmid(8);
+  std::vector<std::vector<InvXArgs>> hi(8);
+  std::vector<int2> it[3];
+  for (int m = 0; m < B.nm; ++m) {
+    const SpectralPlan& p = *members[m].plan;
+    if (p.ndim != 2) {
+      *msg = "batched problems must be two-dimensional";
+      return false;
+    }
+    B.pow2 = B.pow2 && plan_is_pow2(p.plan_x_) && plan_is_pow2(p.plan_ax_[0]);
+    const int M = p.M, Mh = p.Mh, R = p.R, n = p.n, nch = p.nch;
+    const bool spectral = nch > 0;
+    // fwd_x tiles: P line pairs per item
+    const int pairs = (n * R + 1) / 2;
+    const int Pf = std::max(1, std::min(elems / M, pairs));
+    const bool ftws = (size_t)(M + Pf * M) * 16 <= kSmemBudget;
+    const int gf = (pairs + Pf - 1) / Pf;
+    B.block[0] = std::max(B.block[0], std::min(kMaxBlock, std::max(128, round_up(stage_threads(p.plan_x_, Pf * M), 32))));
+    B.smem[0] = std::max(B.smem[0], spectral ? (size_t)((ftws ? M : 0) + Pf * M) * 16 : 0);
+    for (int j = 0; j < gf; ++j) it[0].push_back(make_int2(m, j));
+    // mid tiles: TW columns per item, every channel at once when the plan does so
+    const int L0 = p.Ns[0], I = Mh;
+    const int GBp = p.mid_[0].per_cta >> 16;
+    const bool sorted = p.ch_sorted_ && nch <= GBp;
+    int GB = sorted ? nch : std::min(std::max(nch, 1), 4);
+    int TW = std::max(1, std::min(elems / (std::max(n, GB) * L0), I));
+    const size_t extra = (size_t)p.h_ch_off_[nch] * sizeof(ChanEntry) + (size_t)p.kv_total_ * 8 + (size_t)(nch + 1) * 4;
+    auto smem_of = [&](int tw_, int gb) { return (size_t)(L0 + (n + gb) * tw_ * (L0 + 1)) * 16 + extra; };
+    while (TW > 1 && (smem_of(TW, GB) > kSmemBudget || std::max(n, GB) * TW * L0 > kMaxElems)) TW /= 2;
+    while (!sorted && GB > 1 && (smem_of(TW, GB) > kSmemBudget || std::max(n, GB) * TW * L0 > kMaxElems)) --GB;
+    if (spectral && (smem_of(TW, GB) > 227 * 1024 || std::max(n, GB) * TW * L0 > kMaxElems)) {
+      *msg = "batch member too large for the shared-memory axis-0 pass";
+      return false;
+    }
+    const int gm = (I + TW - 1) / TW;
+    if (spectral) {
+      B.block[1] = std::max(B.block[1], std::min(kMaxBlock, std::max(128, round_up(stage_threads(p.plan_ax_[0], std::max(n, GB) * TW * L0), 32))));
+      B.smem[1] = std::max(B.smem[1], smem_of(TW, GB));
+      for (int j = 0; j < gm; ++j) it[1].push_back(make_int2(m, j));
+    }
+    // inv_x tiles
+    PassCfg gi;
+    int itws = 0;
+    inv_geometry(M, R, n, nch, false, p.plan_x_, &gi, &itws, p.dict_smem_bytes(), elems);
+    B.block[2] = std::max(B.block[2], gi.block);
+    B.smem[2] = std::max(B.smem[2], gi.smem);
+    for (int j = 0; j < gi.grid; ++j) it[2].push_back(make_int2(m, j));
+    for (int st = 1; st <= 7; ++st) {
+      RhsIO io{};
+      io.mode = 1;
+      io.stage = st;
+      io.bufs = members[m].bufs;
+      io.ctl = members[m].ctl;
+      io.err_part = st == 7 ? members[m].err_part : nullptr;
+      FwdXArgs a{};
+      a.M = M;
+      a.Mh = Mh;
+      a.nrows = n * R;
+      a.P = Pf;
+      a.do_fft = spectral ? 1 : 0;
+      a.tw_smem = ftws ? 1 : 0;
+      a.plan = p.plan_x_;
+      a.tw = p.tw_x_;
+      a.S = p.Sf_;
+      a.io = io;
+      prep(a);
+      hf[st].push_back(a);
+      MidArgs md{};
+      md.L0 = L0;
+      md.I = I;
+      md.TW = TW;
+      md.GB = GB;
+      md.nsrc = n;
+      md.G = nch;
+      md.ch0 = 0;
+      md.ndim = 2;
+      md.D1 = p.Ns[1];
+      md.Mh = Mh;
+      md.plan = p.plan_ax_[0];
+      md.tw = p.tw_ax_[0];
+      md.Sf = p.Sf_;
+      md.Sc = p.Sc_;
+      md.chan = p.chan_table(p.ch_off_, p.ch_ent_, nch);
+      md.io = io;
+      md.ent0 = 0;
+      md.nent = p.h_ch_off_[nch];
+      if (sorted) {
+        md.sorted = 1;
+        md.chan.ent = p.ch_sorted_;
+      }
+      prep(md);
+      hmid[st].push_back(md);
+      InvXArgs v{};
+      v.M = M;
+      v.Mh = Mh;
+      v.R = R;
+      v.n = n;
+      v.nch_run = nch;
+      v.npairs = (nch + 1) / 2;
+      v.do_fft = spectral ? 1 : 0;
+      v.N = p.N;
+      v.plan = p.plan_x_;
+      v.tw = p.tw_x_;
+      v.Sc = p.Sc_;
+      v.dict = p.dict_table();
+      v.io = io;
+      v.P = gi.per_cta;
+      v.tw_smem = itws;
+      prep(v);
+      hi[st].push_back(v);
+    }
+  }
+  auto put = [&](auto** dst, const auto& v) -> bool {
+    using T = typename std::remove_reference<decltype(v[0])>::type;
+    const size_t b = std::max<size_t>(1, v.size()) * sizeof(T);
+    if (cudaMalloc((void**)dst, b) != cudaSuccess) return false;
+    device_bytes += b;
+    return v.empty() || cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice) == cudaSuccess;
+  };
+  bool ok = true;
+  for (int st = 1; st <= 7; ++st) ok = ok && put(&B.fwd[st], hf[st]) && put(&B.mid[st], hmid[st]) && put(&B.inv[st], hi[st]);
+  for (int k = 0; k < 3; ++k) {
+    ok = ok && put(&B.items[k], it[k]);
+    B.nitems[k] = nitems[k] = (int)it[k].size();
+  }
+  if (!ok) {
+    *msg = "out of device memory (batch tables)";
+    return false;
+  }
+  // persistent grids: as many CTAs as stay resident
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const void* kern[3] = {B.pow2 ? (const void*)k_fwd_x_batch<kRadixPow2> : (const void*)k_fwd_x_batch<kRadixAll>,
+                         B.pow2 ? (const void*)k_mid_batch<kRadixPow2> : (const void*)k_mid_batch<kRadixAll>,
+                         B.pow2 ? (const void*)k_inv_x_batch<kRadixPow2> : (const void*)k_inv_x_batch<kRadixAll>};
+  for (int k = 0; k < 3; ++k) {
+    if (!opt_in_smem(kern[k])) {
+      *msg = "cannot enable large shared memory for the batched passes";
+      return false;
+    }
+    B.block[k] = std::max(B.block[k], 128);
+    int per_sm = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern[k], B.block[k], B.smem[k]) != cudaSuccess || per_sm < 1) {
+      *msg = "batched pass does not fit on an SM";
+      return false;
+    }
+    B.grid[k] = std::max(1, std::min(B.nitems[k], per_sm * nsm));
+  }
+  return true;
+}
+
+cudaError_t SpectralBatch::launch_stage(int stage, cudaStream_t st) {
+  Impl& B = *impl_;
+  if (stage < 1 || stage > 7) return cudaErrorInvalidValue;
+  if (B.pow2)
+    k_fwd_x_batch<kRadixPow2><<<B.grid[0], B.block[0], B.smem[0], st>>>(B.fwd[stage], B.items[0], B.nitems[0]);
+  else
+    k_fwd_x_batch<kRadixAll><<<B.grid[0], B.block[0], B.smem[0], st>>>(B.fwd[stage], B.items[0], B.nitems[0]);
+  RDCU_TRY(cudaGetLastError());
+  if (B.nitems[1] > 0) {
+    if (B.pow2)
+      k_mid_batch<kRadixPow2><<<B.grid[1], B.block[1], B.smem[1], st>>>(B.mid[stage], B.items[1], B.nitems[1]);
+    else
+      k_mid_batch<kRadixAll><<<B.grid[1], B.block[1], B.smem[1], st>>>(B.mid[stage], B.items[1], B.nitems[1]);
+    RDCU_TRY(cudaGetLastError());
+  }
+  if (B.pow2)
+    k_inv_x_batch<kRadixPow2><<<B.grid[2], B.block[2], B.smem[2], st>>>(B.inv[stage], B.items[2], B.nitems[2]);
+  else
+    k_inv_x_batch<kRadixAll><<<B.grid[2], B.block[2], B.smem[2], st>>>(B.inv[stage], B.items[2], B.nitems[2]);
+  return cudaGetLastError();
 }
 
 }  // namespace rdcu

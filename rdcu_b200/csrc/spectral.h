@@ -42,7 +42,11 @@ struct PlanArena {
   cudaStream_t stream = nullptr;  // table uploads are ordered on this stream
 };
 
+class SpectralBatch;
+
 class SpectralPlan {
+  friend class SpectralBatch;
+
  public:
   // Builds the plan; returns false with msg set when the problem is unsupported.
   bool init(int n, int ndim, const int* Ns, const double* Ls, const std::vector<HostTerm>& terms,
@@ -146,6 +150,36 @@ class SpectralPlan {
   cudaError_t launch_forward(const double* y, cudaStream_t stream);
   bool geometry(std::string* msg);
   cudaError_t ensure_channel_capacity(int rows);
+};
+
+// One problem of a batch: a 2D plan and its DP45 state.
+struct BatchMember {
+  SpectralPlan* plan = nullptr;
+  DP45Bufs bufs{};
+  DP45Ctl* ctl = nullptr;
+  double* err_part = nullptr;  // one partial per grid row (stage 7)
+};
+
+// DP45 stages of many 2D problems of different sizes and coefficients: every pass is one
+// persistent launch over a list of (problem, tile) work items; each item runs the CTA
+// body of the single-problem kernel with that problem's arguments.  Nothing a pass
+// computes depends on the tiling (the error partials are per grid row), so results are
+// bitwise those of each problem's own plan while the tiles are chosen for the batch.
+class SpectralBatch {
+ public:
+  // elems: target complex values per CTA of the x passes and of the axis-0 pass
+  bool init(const std::vector<BatchMember>& members, int elems, std::string* msg);
+  void release();
+  ~SpectralBatch() { release(); }
+  // stage 1 (k1 = f(y)) .. 7 of every running member, 3 launches
+  cudaError_t launch_stage(int stage, cudaStream_t stream);
+  size_t device_bytes = 0;
+  int elems = 0;
+  int nitems[3] = {0, 0, 0};  // work items of the fwd_x, mid and inv_x passes
+
+ private:
+  struct Impl;
+  Impl* impl_ = nullptr;
 };
 
 }  // namespace rdcu
