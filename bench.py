@@ -64,13 +64,15 @@ WORKLOADS = {
     "cgle3d_128": dict(Ns=(128, 128, 128), Ls=(200.0, 200.0, 200.0), seed=2, h0=1e-3),
     "cgle2d_256": dict(Ns=(256, 256), Ls=(100.0, 100.0), seed=1, h0=1e-3),
     "cgle2d_128": dict(Ns=(128, 128), Ls=(100.0, 100.0), seed=1, h0=1e-3),
+    # 512 independent 2D CGLE problems of uneven size, stepped as one ensemble (see run_ensemble)
+    "ensemble_cgle2d_512": dict(members=512, sizes=(64, 96, 128, 192, 256), seed=3, h0=1e-3, tau=0.1),
     # discrete adjoint: gradient of a terminal mismatch over 5000 fixed steps (see run_adjoint)
     "adjoint_cgle2d_256": dict(Ns=(256, 256), Ls=(200.0, 200.0), seed=1, h=1e-3, T=5.0, K=50),
 }
 
 
 def cgle_lines(ndim):
-    from oracle.problem import cgle_coupling_lines  # the coupling text the reference notebook writes
+    from rdcu_b200.problems import cgle_coupling_lines  # the coupling text the reference notebook writes
 
     return cgle_coupling_lines(ndim)
 
@@ -377,6 +379,132 @@ def run_adjoint(args):
     }
 
 
+def ensemble_members(wl):
+    """Members of the ensemble workload: grid N x N with N drawn uniformly from the sizes,
+    L = 0.78 N, CGLE b ~ U[0.5, 3], c ~ U[-2, 0] (numpy seed wl["seed"]); initial states
+    uniform [-1, 1] from glibc rand() with seeds 0..members-1 (the reference's IC
+    generator)."""
+    rng = np.random.default_rng(wl["seed"])
+    m = wl["members"]
+    Ns = rng.choice(wl["sizes"], size=m)
+    bs = rng.uniform(0.5, 3.0, size=m)
+    cs = rng.uniform(-2.0, 0.0, size=m)
+    mem = []
+    for N, b, c in zip(Ns, bs, cs):
+        N = int(N)
+        lines = cgle_lines_bc(b, c)
+        mem.append(dict(n=2, Ns=(N, N), Ls=(0.78 * N, 0.78 * N), terms=parse_terms(lines), rtol=1e-8, atol=1e-8))
+    return mem
+
+
+def cgle_lines_bc(b, c):
+    from rdcu_b200.problems import cgle_coupling_lines
+
+    return cgle_coupling_lines(2, b, c)
+
+
+def run_ensemble(args):
+    """Ensemble workload: 512 2D CGLE members of uneven size, adaptive DP45 at rtol = atol
+    = 1e-8.  Warm-up [0, W tau] untimed, timed window [W tau, (W+K) tau] (tau = 0.1);
+    value = sum over members of grid points x accepted steps / device seconds.  The
+    instance-by-instance baseline runs a stratified sample of members (two per grid size)
+    one after another through single handles over the same window and checks each
+    member's accepted/attempt counts against the ensemble's; its rate is reported as
+    baseline_sequential and the ratio as speedup_vs_sequential."""
+    import torch
+
+    import rdcu_b200 as R
+
+    wl = WORKLOADS[args.workload]
+    mem = ensemble_members(wl)
+    m = len(mem)
+    tau = wl["tau"]
+    T_A, T_B = args.warmup * tau, (args.warmup + args.steps) * tau
+    npts = np.array([x["Ns"][0] * x["Ns"][1] for x in mem], dtype=np.float64)
+    ics = [R.random_ic(2, int(N), 2.0, 0.0, i) for i, N in enumerate(npts)]
+    ens = R.Ensemble(mem)
+    for i in range(m):
+        ens.set_state(i, 0.0, wl["h0"], ics[i].ctypes.data)
+    tile = ens.tune()
+    ens.solve(T_A)  # warm-up: the white-noise transient
+    states = []
+    for i in range(m):
+        y = np.empty(2 * int(npts[i]))
+        t, h = ens.get_state(i, y.ctypes.data)
+        states.append((t, h, y))
+        ens.set_state(i, t, h, y.ctypes.data)  # counters from the window start
+    stream = torch.cuda.ExternalStream(ens.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    with ClockSampler(0) as clk:
+        e0.record(stream)
+        ens.solve(T_B)
+        e1.record(stream)
+        e1.synchronize()
+    sec = e0.elapsed_time(e1) / 1e3
+    cnt = np.array([ens.counters(i) for i in range(m)], dtype=np.float64)
+    work = float(np.sum(cnt[:, 0] * npts))
+    # e2e: host states in, host states out, through the public API (same window)
+    w0 = time.perf_counter()
+    for i in range(m):
+        ens.set_state(i, states[i][0], states[i][1], states[i][2].ctypes.data)
+    ens.solve(T_B)
+    outs = [np.empty(2 * int(N)) for N in npts]
+    for i in range(m):
+        ens.get_state(i, outs[i].ctypes.data)
+    e2e_s = time.perf_counter() - w0
+    # instance-by-instance baseline on a stratified sample
+    sample = []
+    for N in wl["sizes"]:
+        sample += [i for i in range(m) if mem[i]["Ns"][0] == N][:2]
+    seq_s, seq_work = 0.0, 0.0
+    for i in sample:
+        s = R.Solver(2, mem[i]["Ns"], mem[i]["Ls"], mem[i]["terms"], rtol=1e-8, atol=1e-8)
+        s.set_state(states[i][0], states[i][1], states[i][2].ctypes.data)
+        torch.cuda.synchronize()
+        st = torch.cuda.ExternalStream(s.stream)
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(st)
+        s.solve(T_B, [])
+        a1.record(st)
+        a1.synchronize()
+        acc, att = s.counters()
+        if (acc, att) != (int(cnt[i, 0]), int(cnt[i, 1])):
+            raise RuntimeError("member %d: single handle took %d/%d steps, ensemble %d/%d" %
+                               (i, acc, att, cnt[i, 0], cnt[i, 1]))
+        seq_s += a0.elapsed_time(a1) / 1e3
+        seq_work += acc * npts[i]
+        s.close()
+    seq_rate = seq_work / seq_s
+    bytes_attempt = 41.0 * 8 * 2 * float(np.sum(npts))  # 41 state-sized arrays per DP45 attempt
+    peak, peak_kind = load_peaks()
+    attempts_batched = cnt[:, 1].max()
+    achieved = bytes_attempt * attempts_batched / sec / 1e9
+    ens.close()
+    return {
+        "metric": METRIC, "value": work / sec, "unit": "grid-pt·steps/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": sec * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "members": m, "sizes": list(wl["sizes"]), "L": "0.78 N",
+                   "coefficients": "b ~ U[0.5,3], c ~ U[-2,0] (numpy seed %d)" % wl["seed"],
+                   "ic": "glibc rand seeds 0..%d, [-1,1]" % (m - 1), "rtol": 1e-8, "atol": 1e-8,
+                   "window_sim_time": [T_A, T_B], "tau_per_step": tau, "tile_elems": tile,
+                   "accepted_steps": int(cnt[:, 0].sum()), "attempts": int(cnt[:, 1].sum()),
+                   "l2": "states 216 MB per array > L2 (no flush needed)"},
+        "baseline_sequential": {"value": seq_rate, "unit": "grid-pt·steps/s", "sample_members": sample,
+                                "seconds": seq_s, "note": "single handles one after another, same window"},
+        "speedup_vs_sequential": (work / sec) / seq_rate,
+        "gpu_launches": int(attempts_batched) * 19,
+        "clocks": clk.summary(),
+        "e2e": {"value": work / e2e_s, "unit": "grid-pt·steps/s",
+                "h2d_bytes_per_step": 16.0 * float(np.sum(npts)) / args.steps,
+                "d2h_bytes_per_step": 32.0 * float(np.sum(npts)) / args.steps, "seconds": e2e_s},
+        "roofline": {"bound": "hbm", "kernel": "batched DP45 attempt (all passes)", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_attempt": bytes_attempt, "batched_attempts": int(attempts_batched)},
+    }
+
+
 def launches_per_attempt(ndim):
     per_stage = {1: 3, 2: 3, 3: 5}[ndim]
     return 6 * per_stage + 1
@@ -412,6 +540,10 @@ def reference_binary():
 def run_reference(args):
     if args.workload.startswith("adjoint"):
         return {"impl": "reference", "unavailable": "the reference computes no gradients (no adjoint to time)"}
+    if args.workload.startswith("ensemble"):
+        return {"impl": "reference", "unavailable": "the reference has no ensemble; its one-problem-per-process "
+                "rate is the cgle2d workloads' reference arm, and the instance-by-instance baseline of this "
+                "workload is reported by our arm"}
     exe, why = reference_binary()
     if exe is None:
         return {"impl": "reference", "unavailable": why}
@@ -483,6 +615,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     if args.workload.startswith("adjoint"):
         line = run_adjoint(args) if rank == 0 else None
+    elif args.workload.startswith("ensemble"):
+        line = run_ensemble(args) if rank == 0 else None
     else:
         line = run_ours(args, rank, world, local_rank)
     if world > 1:

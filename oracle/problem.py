@@ -241,15 +241,15 @@ def cgle_coupling_lines(ndim: int, b: float = 2.0, c: float = 0.8) -> List[str]:
     def dd(i, j):
         return n + ndim * n + (j * ndim + j) * n + i
 
-    fmt = lambda v: ("%f" % v)
+    fmt = lambda v: ("%f" % v)  # signed: "-%s" % fmt(-2.0) would read "--2.0", which atof takes as 0
     lines = ["1.0,0,0,1"]
     lines += ["1.0,0,%d,1" % dd(0, j) for j in range(ndim)]
-    lines += ["-%s,0,%d,1" % (fmt(b), dd(1, j)) for j in range(ndim)]
+    lines += ["%s,0,%d,1" % (fmt(-b), dd(1, j)) for j in range(ndim)]
     lines += ["-1.0,0,0,3", "-1.0,0,0,1,1,2", "1.0,1,1,1"]
     lines += ["1.0,1,%d,1" % dd(1, j) for j in range(ndim)]
     lines += ["%s,1,%d,1" % (fmt(b), dd(0, j)) for j in range(ndim)]
     lines += ["-1.0,1,0,2,1,1", "-1.0,1,1,3", "%s,1,0,3" % fmt(c), "%s,1,0,1,1,2" % fmt(c),
-              "-%s,0,0,2,1,1" % fmt(c), "-%s,0,1,3" % fmt(c)]
+              "%s,0,0,2,1,1" % fmt(-c), "%s,0,1,3" % fmt(-c)]
     return lines
 
 

@@ -83,3 +83,16 @@ def test_no_cpu_fallback_without_gpu():
     with pytest.raises(R.RdcuError) as e:
         R.Solver(2, (8, 8), (1.0, 1.0), [(1.0, [0, 0, 1])])
     assert e.value.code == R.RDCU_ERR_CUDA
+
+
+def test_problem_coupling_lists_match_the_oracle():
+    """The package's coupling lists (workload definitions) and the oracle's agree."""
+    from oracle import problem as op
+    from rdcu_b200 import problems as pp
+
+    for ndim in (1, 2, 3):
+        for b, c in ((2.0, 0.8), (0.7, -1.3), (-1.5, 0.0)):
+            assert pp.cgle_coupling_lines(ndim, b, c) == op.cgle_coupling_lines(ndim, b, c)
+            parsed = [op.parse_term(s) for s in pp.cgle_coupling_lines(ndim, b, c)]
+            assert any(abs(t.C - c) < 1e-6 for t in parsed) and any(abs(t.C + b) < 1e-6 for t in parsed)
+    assert pp.brusselator_coupling_lines() == op.brusselator_coupling_lines()
