@@ -163,6 +163,15 @@ __device__ __forceinline__ void stockham_stage(double2* buf, int LS, int nlines,
   __syncthreads();
 }
 
+// A stage of the runtime-planned transform as a called function: the plan's stage loop
+// then holds one stage's registers at a time (inlined, the union of every radix's
+// registers exceeds the budget and spills).
+template <int R, bool INV, bool POW2>
+__device__ __noinline__ void stockham_stage_call(double2* buf, int LS, int nlines, int L, int Ns, FastDiv dm,
+                                                 FastDiv dns, const double2* tw) {
+  stockham_stage<R, INV, POW2>(buf, LS, nlines, L, Ns, dm, dns, tw);
+}
+
 // Radix sets a kernel is compiled for: power-of-two lengths use radices 8, 4, 2 only
 // (no register spills); any other supported length uses the general set.
 constexpr int kRadixPow2 = 0;
@@ -184,25 +193,39 @@ __device__ void fft_lines(double2* buf, int LS, int nlines, const LinePlan& p, c
     const FastDiv dm = p.div_m[s], dns = p.div_ns[s];
     if (RS == kRadixPow2) {
       if (R == 8)
-        stockham_stage<8, INV, true>(buf, LS, nlines, p.L, Ns, dm, dns, tw);
+        stockham_stage_call<8, INV, true>(buf, LS, nlines, p.L, Ns, dm, dns, tw);
       else if (R == 4)
-        stockham_stage<4, INV, true>(buf, LS, nlines, p.L, Ns, dm, dns, tw);
+        stockham_stage_call<4, INV, true>(buf, LS, nlines, p.L, Ns, dm, dns, tw);
       else
-        stockham_stage<2, INV, true>(buf, LS, nlines, p.L, Ns, dm, dns, tw);
+        stockham_stage_call<2, INV, true>(buf, LS, nlines, p.L, Ns, dm, dns, tw);
     } else {
       switch (R) {
-        case 2: stockham_stage<2, INV, false>(buf, LS, nlines, p.L, Ns, dm, dns, tw); break;
-        case 3: stockham_stage<3, INV, false>(buf, LS, nlines, p.L, Ns, dm, dns, tw); break;
-        case 4: stockham_stage<4, INV, false>(buf, LS, nlines, p.L, Ns, dm, dns, tw); break;
-        case 5: stockham_stage<5, INV, false>(buf, LS, nlines, p.L, Ns, dm, dns, tw); break;
-        case 7: stockham_stage<7, INV, false>(buf, LS, nlines, p.L, Ns, dm, dns, tw); break;
-        case 8: stockham_stage<8, INV, false>(buf, LS, nlines, p.L, Ns, dm, dns, tw); break;
-        case 11: stockham_stage<11, INV, false>(buf, LS, nlines, p.L, Ns, dm, dns, tw); break;
-        case 13: stockham_stage<13, INV, false>(buf, LS, nlines, p.L, Ns, dm, dns, tw); break;
+        case 2: stockham_stage_call<2, INV, false>(buf, LS, nlines, p.L, Ns, dm, dns, tw); break;
+        case 3: stockham_stage_call<3, INV, false>(buf, LS, nlines, p.L, Ns, dm, dns, tw); break;
+        case 4: stockham_stage_call<4, INV, false>(buf, LS, nlines, p.L, Ns, dm, dns, tw); break;
+        case 5: stockham_stage_call<5, INV, false>(buf, LS, nlines, p.L, Ns, dm, dns, tw); break;
+        case 7: stockham_stage_call<7, INV, false>(buf, LS, nlines, p.L, Ns, dm, dns, tw); break;
+        case 8: stockham_stage_call<8, INV, false>(buf, LS, nlines, p.L, Ns, dm, dns, tw); break;
+        case 11: stockham_stage_call<11, INV, false>(buf, LS, nlines, p.L, Ns, dm, dns, tw); break;
+        case 13: stockham_stage_call<13, INV, false>(buf, LS, nlines, p.L, Ns, dm, dns, tw); break;
         default: break;  // plans only contain the radices above
       }
     }
     Ns *= R;
+  }
+}
+
+// The same transform for a power-of-two length L known at compile time: the stage
+// sequence of make_line_plan (radix 8 while 8 divides what is left, then 4 or 2) with
+// every length, span and stride a constant.  Bitwise equal to fft_lines on that plan.
+template <int L, bool INV, int NS = 1>
+__device__ __forceinline__ void fft_pow2_t(double2* buf, int LS, int nlines, const double2* tw) {
+  if constexpr (NS < L) {
+    constexpr int REM = L / NS;
+    constexpr int R = (REM % 8 == 0) ? 8 : REM;  // REM is 8^a times 1, 2 or 4
+    static_assert(R == 2 || R == 4 || R == 8, "power-of-two lengths only");
+    stockham_stage<R, INV, true>(buf, LS, nlines, L, NS, FastDiv{}, FastDiv{}, tw);
+    fft_pow2_t<L, INV, NS * R>(buf, LS, nlines, tw);
   }
 }
 

@@ -193,6 +193,25 @@ struct FwdXArgs {
   RhsIO io;
 };
 
+// Division by an invariant divisor: the compile-time constant D when D > 0, else the
+// precomputed FastDiv f.
+template <int D>
+__device__ __forceinline__ int fdivc(int n, FastDiv f) {
+  if constexpr (D > 0)
+    return (int)((unsigned)n / (unsigned)D);
+  else
+    return fdiv(n, f);
+}
+
+// Line FFTs of a pass: compile-time power-of-two length LX, or the plan's stages (LX = 0).
+template <int RS, int LX, bool INV>
+__device__ __forceinline__ void fft_lines_x(double2* buf, int LS, int nlines, const LinePlan& p, const double2* tw) {
+  if constexpr (LX > 0)
+    fft_pow2_t<LX, INV>(buf, LS, nlines, tw);
+  else
+    fft_lines<RS, INV>(buf, LS, nlines, p, tw);
+}
+
 // Stage state with the stage number known at compile time (slopes in registers).
 template <int S>
 __device__ __forceinline__ double stage_value_t(long long i, const Resolved& r) {
@@ -209,10 +228,10 @@ __device__ __forceinline__ double stage_value_t(long long i, const Resolved& r) 
 // Loads (with the stage combination) the rows of P line pairs into the complex lines
 // of buf, real row in .x, partner row in .y; writes the stage state when asked.  Each
 // thread issues the loads of kUnroll elements before storing any of them.
-template <int S>
+template <int S, int LX>
 __device__ __forceinline__ void fwd_load(const FwdXArgs& a, const Resolved& r, double2* buf, long long row0) {
   constexpr int kUnroll = 4;
-  const int M = a.M, T = blockDim.x, tid = threadIdx.x;
+  const int M = LX ? LX : a.M, T = blockDim.x, tid = threadIdx.x;
   const int nel = a.P * 2 * M;
   for (int e0 = tid; e0 < nel; e0 += T * kUnroll) {
     double v[kUnroll];
@@ -223,9 +242,9 @@ __device__ __forceinline__ void fwd_load(const FwdXArgs& a, const Resolved& r, d
       gi[u] = -1;
       v[u] = 0.0;
       if (e < nel) {
-        const int pl = fdiv(e, a.d2M);
+        const int pl = fdivc<2 * LX>(e, a.d2M);
         const int w = e - pl * 2 * M;
-        const int half = fdiv(w, a.dM);
+        const int half = fdivc<LX>(w, a.dM);
         const int x = w - half * M;
         const long long g = row0 + 2 * pl + half;
         if (g < a.nrows) {
@@ -240,9 +259,9 @@ __device__ __forceinline__ void fwd_load(const FwdXArgs& a, const Resolved& r, d
       if (e >= nel) break;
       if (r.ytemp && gi[u] >= 0) r.ytemp[gi[u]] = v[u];
       if (a.do_fft) {
-        const int pl = fdiv(e, a.d2M);
+        const int pl = fdivc<2 * LX>(e, a.d2M);
         const int w = e - pl * 2 * M;
-        const int half = fdiv(w, a.dM);
+        const int half = fdivc<LX>(w, a.dM);
         const int x = w - half * M;
         reinterpret_cast<double*>(buf)[2 * (pl * M + x) + half] = v[u];
       }
@@ -251,12 +270,12 @@ __device__ __forceinline__ void fwd_load(const FwdXArgs& a, const Resolved& r, d
 }
 
 // bx: the CTA's index within this plan's grid (blockIdx.x, or a work item of a batch)
-template <int RS>
+template <int RS, int LX>
 __device__ __forceinline__ void fwd_x_body(const FwdXArgs& a, int bx) {
   extern __shared__ double2 sm[];
   if (a.io.mode == 1 && !a.io.ctl->running) return;
   const Resolved r = resolve(a.io);
-  const int M = a.M, T = blockDim.x, tid = threadIdx.x;
+  const int M = LX ? LX : a.M, T = blockDim.x, tid = threadIdx.x;
   const double2* tw = a.tw;
   double2* buf = sm;
   if (a.do_fft && a.tw_smem) {
@@ -267,23 +286,23 @@ __device__ __forceinline__ void fwd_x_body(const FwdXArgs& a, int bx) {
   }
   const long long row0 = 2LL * bx * a.P;
   switch (r.stage) {
-    case 2: fwd_load<2>(a, r, buf, row0); break;
-    case 3: fwd_load<3>(a, r, buf, row0); break;
-    case 4: fwd_load<4>(a, r, buf, row0); break;
-    case 5: fwd_load<5>(a, r, buf, row0); break;
-    case 6: fwd_load<6>(a, r, buf, row0); break;
-    case 7: fwd_load<7>(a, r, buf, row0); break;
-    default: fwd_load<1>(a, r, buf, row0); break;
+    case 2: fwd_load<2, LX>(a, r, buf, row0); break;
+    case 3: fwd_load<3, LX>(a, r, buf, row0); break;
+    case 4: fwd_load<4, LX>(a, r, buf, row0); break;
+    case 5: fwd_load<5, LX>(a, r, buf, row0); break;
+    case 6: fwd_load<6, LX>(a, r, buf, row0); break;
+    case 7: fwd_load<7, LX>(a, r, buf, row0); break;
+    default: fwd_load<1, LX>(a, r, buf, row0); break;
   }
   if (!a.do_fft) return;
   __syncthreads();
-  fft_lines<RS, false>(buf, M, a.P, a.plan, tw);
-  const int Mh = a.Mh;
+  fft_lines_x<RS, LX, false>(buf, M, a.P, a.plan, tw);
+  const int Mh = LX ? LX / 2 + 1 : a.Mh;
   const int nout = a.P * 2 * Mh;
   for (int e = tid; e < nout; e += T) {
-    const int pl = fdiv(e, a.d2Mh);
+    const int pl = fdivc<LX ? 2 * (LX / 2 + 1) : 0>(e, a.d2Mh);
     const int w = e - pl * 2 * Mh;
-    const int half = fdiv(w, a.dMh);
+    const int half = fdivc<LX ? LX / 2 + 1 : 0>(w, a.dMh);
     const int kx = w - half * Mh;
     const long long g = row0 + 2 * pl + half;
     if (g >= a.nrows) continue;
@@ -298,9 +317,9 @@ __device__ __forceinline__ void fwd_x_body(const FwdXArgs& a, int bx) {
   }
 }
 
-template <int RS>
+template <int RS, int LX>
 __global__ void __launch_bounds__(kMaxBlock, 1) k_fwd_x(FwdXArgs a) {
-  fwd_x_body<RS>(a, blockIdx.x);
+  fwd_x_body<RS, LX>(a, blockIdx.x);
 }
 
 struct C2CArgs {
@@ -312,11 +331,11 @@ struct C2CArgs {
   RhsIO io;
 };
 
-template <int RS, bool INV>
+template <int RS, bool INV, int LX>
 __global__ void __launch_bounds__(kMaxBlock, 1) k_c2c(C2CArgs a) {
   extern __shared__ double2 sm[];
   if (a.io.mode == 1 && !a.io.ctl->running) return;
-  const int La = a.La, TW = a.TW, LS = La + 1, T = blockDim.x, tid = threadIdx.x;
+  const int La = LX ? LX : a.La, TW = a.TW, LS = La + 1, T = blockDim.x, tid = threadIdx.x;
   double2* tw = sm;
   double2* buf = sm + La;
   for (int t = tid; t < La; t += T) tw[t] = a.tw[t];
@@ -331,7 +350,7 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_c2c(C2CArgs a) {
   }
   cp_async_wait_all();
   __syncthreads();
-  fft_lines<RS, INV>(buf, LS, TW, a.plan, tw);
+  fft_lines_x<RS, LX, INV>(buf, LS, TW, a.plan, tw);
   for (int e = tid; e < nel; e += T) {
     const int z = fdiv(e, a.dTW), c = e - z * TW;
     const long long ii = i0 + c;
@@ -353,11 +372,11 @@ struct MidArgs {
   RhsIO io;
 };
 
-template <int RS>
+template <int RS, int LX>
 __device__ __forceinline__ void mid_body(const MidArgs& a, int bx) {
   extern __shared__ double2 sm[];
   if (a.io.mode == 1 && !a.io.ctl->running) return;
-  const int L0 = a.L0, TW = a.TW, LS = L0 + 1, T = blockDim.x, tid = threadIdx.x;
+  const int L0 = LX ? LX : a.L0, TW = a.TW, LS = L0 + 1, T = blockDim.x, tid = threadIdx.x;
   double2* tw = sm;
   double2* fb = sm + L0;
   double2* cb = fb + a.nsrc * TW * LS;
@@ -373,7 +392,7 @@ __device__ __forceinline__ void mid_body(const MidArgs& a, int bx) {
   const int nload = a.nsrc * L0 * TW;
   for (int e = tid; e < nload; e += T) {
     const int q0 = fdiv(e, a.dTW), c = e - q0 * TW;
-    const int f = fdiv(q0, a.dL0), z = q0 - f * L0;
+    const int f = fdivc<LX>(q0, a.dL0), z = q0 - f * L0;
     const long long ii = i0 + c;
     const bool in = ii < a.I;
     cp_async16(&fb[(f * TW + c) * LS + z], in ? (const void*)&a.Sf[((long long)f * L0 + z) * a.I + ii] : (const void*)a.Sf,
@@ -381,7 +400,7 @@ __device__ __forceinline__ void mid_body(const MidArgs& a, int bx) {
   }
   cp_async_wait_all();
   __syncthreads();
-  fft_lines<RS, false>(fb, LS, a.nsrc * TW, a.plan, tw);
+  fft_lines_x<RS, LX, false>(fb, LS, a.nsrc * TW, a.plan, tw);
   if (a.sorted) {
     // every channel at once: each distinct operator's multiplier once per point
     const int npts = L0 * TW;
@@ -454,11 +473,11 @@ __device__ __forceinline__ void mid_body(const MidArgs& a, int bx) {
         if (c4 < a.G) cb[(c4 * TW + c) * LS + z] = acc[c4];
     }
     __syncthreads();
-    fft_lines<RS, true>(cb, LS, a.G * TW, a.plan, tw);
+    fft_lines_x<RS, LX, true>(cb, LS, a.G * TW, a.plan, tw);
     const int ncomp = a.G * L0 * TW;
     for (int e = tid; e < ncomp; e += T) {
       const int q0 = fdiv(e, a.dTW), c = e - q0 * TW;
-      const int ch = fdiv(q0, a.dL0), z = q0 - ch * L0;
+      const int ch = fdivc<LX>(q0, a.dL0), z = q0 - ch * L0;
       const long long ii = i0 + c;
       if (ii < a.I) a.Sc[((long long)ch * L0 + z) * a.I + ii] = cb[(ch * TW + c) * LS + z];
     }
@@ -469,7 +488,7 @@ __device__ __forceinline__ void mid_body(const MidArgs& a, int bx) {
     const int ncomp = gc * L0 * TW;
     for (int e = tid; e < ncomp; e += T) {
       const int q0 = fdiv(e, a.dTW), c = e - q0 * TW;
-      const int ch = fdiv(q0, a.dL0), z = q0 - ch * L0;
+      const int ch = fdivc<LX>(q0, a.dL0), z = q0 - ch * L0;
       const long long ii = i0 + c;
       double2 acc = make_double2(0.0, 0.0);
       if (ii < a.I) {
@@ -501,10 +520,10 @@ __device__ __forceinline__ void mid_body(const MidArgs& a, int bx) {
       cb[(ch * TW + c) * LS + z] = acc;
     }
     __syncthreads();
-    fft_lines<RS, true>(cb, LS, gc * TW, a.plan, tw);
+    fft_lines_x<RS, LX, true>(cb, LS, gc * TW, a.plan, tw);
     for (int e = tid; e < ncomp; e += T) {
       const int q0 = fdiv(e, a.dTW), c = e - q0 * TW;
-      const int ch = fdiv(q0, a.dL0), z = q0 - ch * L0;
+      const int ch = fdivc<LX>(q0, a.dL0), z = q0 - ch * L0;
       const long long ii = i0 + c;
       if (ii < a.I) a.Sc[((long long)(g0 + ch) * L0 + z) * a.I + ii] = cb[(ch * TW + c) * LS + z];
     }
@@ -512,9 +531,9 @@ __device__ __forceinline__ void mid_body(const MidArgs& a, int bx) {
   }
 }
 
-template <int RS>
+template <int RS, int LX>
 __global__ void __launch_bounds__(kMaxBlock, 1) k_mid(MidArgs a) {
-  mid_body<RS>(a, blockIdx.x);
+  mid_body<RS, LX>(a, blockIdx.x);
 }
 
 struct Mult1DArgs {
@@ -712,12 +731,12 @@ struct InvXArgs {
   int ch_base;        // first channel row of Sc this launch reads
 };
 
-template <int RS>
+template <int RS, int LX>
 __device__ __forceinline__ void inv_x_body(const InvXArgs& a, int bx) {
   extern __shared__ double2 sm[];
   if (a.io.mode == 1 && !a.io.ctl->running) return;
   const Resolved r = resolve(a.io);
-  const int M = a.M, Mh = a.Mh, T = blockDim.x, tid = threadIdx.x;
+  const int M = LX ? LX : a.M, Mh = LX ? LX / 2 + 1 : a.Mh, T = blockDim.x, tid = threadIdx.x;
   const int P = a.P, np = a.npairs, n = a.n;
   const double2* tw = a.tw;
   double2* lines = sm;
@@ -750,7 +769,7 @@ __device__ __forceinline__ void inv_x_body(const InvXArgs& a, int bx) {
       for (int e = tid; e < nph; e += T) {
         const int pr = fdiv(e, a.dnhalf);
         const int w = e - pr * n * half;
-        const int fi = fdiv(w, a.dhalf);
+        const int fi = fdivc<LX / 2>(w, a.dhalf);
         const int x2 = (w - fi * half) * 2;
         const long long row = r0 + pr;
         const bool in = row < a.R;
@@ -762,7 +781,7 @@ __device__ __forceinline__ void inv_x_body(const InvXArgs& a, int bx) {
       for (int e = tid; e < nph; e += T) {
         const int pr = fdiv(e, a.dnM);
         const int w = e - pr * n * M;
-        const int fi = fdiv(w, a.dM);
+        const int fi = fdivc<LX>(w, a.dM);
         const int x = w - fi * M;
         const long long row = r0 + pr;
         phys[(pr * n + fi) * M + x] = row < a.R ? r.u[((long long)fi * a.R + row) * M + x] : 0.0;
@@ -782,7 +801,7 @@ __device__ __forceinline__ void inv_x_body(const InvXArgs& a, int bx) {
         if (e >= nel) continue;
         const int pr = fdiv(e, a.dnpM);
         const int w = e - pr * np * M;
-        const int cp = fdiv(w, a.dM);
+        const int cp = fdivc<LX>(w, a.dM);
         const int kx = w - cp * M;
         const long long row = r0 + pr;
         if (row >= a.R) continue;
@@ -797,7 +816,7 @@ __device__ __forceinline__ void inv_x_body(const InvXArgs& a, int bx) {
         if (e >= nel) break;
         const int pr = fdiv(e, a.dnpM);
         const int w = e - pr * np * M;
-        const int cp = fdiv(w, a.dM);
+        const int cp = fdivc<LX>(w, a.dM);
         const int kx = w - cp * M;
         double2 Av = A[u], Bv = B[u];
         if (kx == 0 || 2 * kx == M) {
@@ -814,14 +833,14 @@ __device__ __forceinline__ void inv_x_body(const InvXArgs& a, int bx) {
   }
   cp_async_wait_all();
   __syncthreads();
-  if (a.do_fft) fft_lines<RS, true>(lines, M, P * np, a.plan, tw);
+  if (a.do_fft) fft_lines_x<RS, LX, true>(lines, M, P * np, a.plan, tw);
 
   if (a.Yout) {
     const int nel = P * a.nch_run * M;
     for (int e = tid; e < nel; e += T) {
       const int pr = fdiv(e, a.dncM);
       const int w = e - pr * a.nch_run * M;
-      const int c = fdiv(w, a.dM);
+      const int c = fdivc<LX>(w, a.dM);
       const int x = w - c * M;
       const long long row = r0 + pr;
       if (row >= a.R) continue;
@@ -842,7 +861,7 @@ __device__ __forceinline__ void inv_x_body(const InvXArgs& a, int bx) {
   const bool err = (a.io.mode == 1 && r.stage == 7 && a.io.err_part != nullptr);
   const int npts = P * M;
   for (int e = tid; e < npts; e += T) {
-    const int pr = fdiv(e, a.dM);
+    const int pr = fdivc<LX>(e, a.dM);
     const int x = e - pr * M;
     const long long row = r0 + pr;
     if (row >= a.R) continue;
@@ -904,9 +923,9 @@ __device__ __forceinline__ void inv_x_body(const InvXArgs& a, int bx) {
   }
 }
 
-template <int RS>
+template <int RS, int LX>
 __global__ void __launch_bounds__(kMaxBlock, 1) k_inv_x(InvXArgs a) {
-  inv_x_body<RS>(a, blockIdx.x);
+  inv_x_body<RS, LX>(a, blockIdx.x);
 }
 
 // ---- batched passes: persistent CTAs over (problem, tile) work items
@@ -926,7 +945,7 @@ __global__ void __launch_bounds__(kMaxBlock, 1)
     const int2 w = items[it];
     load_args(&sa, args + w.x);
     __syncthreads();
-    fwd_x_body<RS>(sa, w.y);
+    fwd_x_body<RS, 0>(sa, w.y);
     __syncthreads();
   }
 }
@@ -939,7 +958,7 @@ __global__ void __launch_bounds__(kMaxBlock, 1)
     const int2 w = items[it];
     load_args(&sa, args + w.x);
     __syncthreads();
-    mid_body<RS>(sa, w.y);
+    mid_body<RS, 0>(sa, w.y);
     __syncthreads();
   }
 }
@@ -952,7 +971,7 @@ __global__ void __launch_bounds__(kMaxBlock, 1)
     const int2 w = items[it];
     load_args(&sa, args + w.x);
     __syncthreads();
-    inv_x_body<RS>(sa, w.y);
+    inv_x_body<RS, 0>(sa, w.y);
     __syncthreads();
   }
 }
@@ -1060,6 +1079,25 @@ static void inv_geometry(int M, int R, int n, int nch_run, bool yout, const Line
   c->block = std::min(kMaxBlock, std::max(128, round_up(stage_threads(plan, P * npm * M), 32)));
   c->smem = bytes(P, tws);
   *tw_smem = tws ? 1 : 0;
+}
+
+// Calls f(radix set, line length) with compile-time values for the plan's lengths:
+// power-of-two lines of 64..512 points get kernels specialised to their length, other
+// power-of-two lines the shift-indexed kernels, every other length the general ones.
+template <typename F>
+static void by_length(const LinePlan& p, F&& f) {
+  using RP = std::integral_constant<int, kRadixPow2>;
+  if (!plan_is_pow2(p)) {
+    f(std::integral_constant<int, kRadixAll>{}, std::integral_constant<int, 0>{});
+    return;
+  }
+  switch (p.L) {
+    case 64: f(RP{}, std::integral_constant<int, 64>{}); return;
+    case 128: f(RP{}, std::integral_constant<int, 128>{}); return;
+    case 256: f(RP{}, std::integral_constant<int, 256>{}); return;
+    case 512: f(RP{}, std::integral_constant<int, 512>{}); return;
+    default: f(RP{}, std::integral_constant<int, 0>{}); return;
+  }
 }
 
 // ----------------------------------------------------------------------------- plan
@@ -1445,16 +1483,18 @@ bool SpectralPlan::init(int n_, int ndim_, const int* Ns_, const double* Ls_,
   // opt in to large dynamic shared memory (the limit is per block, static included)
   const int maxsm = 227 * 1024;
   bool optin_ok = true;
-  optin_ok &= opt_in_smem((const void*)k_fwd_x<kRadixPow2>);
-  optin_ok &= opt_in_smem((const void*)k_fwd_x<kRadixAll>);
-  optin_ok &= opt_in_smem((const void*)k_inv_x<kRadixPow2>);
-  optin_ok &= opt_in_smem((const void*)k_inv_x<kRadixAll>);
-  optin_ok &= opt_in_smem((const void*)k_mid<kRadixPow2>);
-  optin_ok &= opt_in_smem((const void*)k_mid<kRadixAll>);
-  optin_ok &= opt_in_smem((const void*)k_c2c<kRadixPow2, false>);
-  optin_ok &= opt_in_smem((const void*)k_c2c<kRadixPow2, true>);
-  optin_ok &= opt_in_smem((const void*)k_c2c<kRadixAll, false>);
-  optin_ok &= opt_in_smem((const void*)k_c2c<kRadixAll, true>);
+  auto optin_all = [&](const LinePlan& pl) {
+    by_length(pl, [&](auto rs, auto lx) {
+      constexpr int RS = decltype(rs)::value, LX = decltype(lx)::value;
+      optin_ok &= opt_in_smem((const void*)k_fwd_x<RS, LX>);
+      optin_ok &= opt_in_smem((const void*)k_inv_x<RS, LX>);
+      optin_ok &= opt_in_smem((const void*)k_mid<RS, LX>);
+      optin_ok &= opt_in_smem((const void*)k_c2c<RS, false, LX>);
+      optin_ok &= opt_in_smem((const void*)k_c2c<RS, true, LX>);
+    });
+  };
+  optin_all(plan_x_);
+  for (int ax = 0; ax + 1 < ndim; ++ax) optin_all(plan_ax_[ax]);
   if (!optin_ok) {
     *msg = "cannot enable large shared memory for the FFT passes";
     return false;
@@ -1542,10 +1582,7 @@ cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, co
     }
     const size_t smem = c.smem;  // includes the staged tables
     prep(m);
-    if (plan_is_pow2(plan_ax_[0]))
-      k_mid<kRadixPow2><<<c.grid, c.block, smem, st>>>(m);
-    else
-      k_mid<kRadixAll><<<c.grid, c.block, smem, st>>>(m);
+    by_length(plan_ax_[0], [&](auto rs, auto lx) { k_mid<decltype(rs)::value, decltype(lx)::value><<<c.grid, c.block, smem, st>>>(m); });
     RDCU_TRY(cudaGetLastError());
     if (ndim == 3) {
       C2CArgs a{};
@@ -1558,10 +1595,7 @@ cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, co
       a.io = io;
       dim3 grid(c2c_i_.grid, nch_run * Ns[0]);
       prep(a);
-      if (plan_is_pow2(plan_ax_[1]))
-        k_c2c<kRadixPow2, true><<<grid, c2c_i_.block, c2c_i_.smem, st>>>(a);
-      else
-        k_c2c<kRadixAll, true><<<grid, c2c_i_.block, c2c_i_.smem, st>>>(a);
+      by_length(plan_ax_[1], [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, true, decltype(lx)::value><<<grid, c2c_i_.block, c2c_i_.smem, st>>>(a); });
       RDCU_TRY(cudaGetLastError());
     }
   } else if (spectral) {
@@ -1606,10 +1640,7 @@ cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, co
     a.P = g.per_cta;
     a.tw_smem = tws;
     prep(a);
-    if (plan_is_pow2(plan_x_))
-      k_inv_x<kRadixPow2><<<g.grid, g.block, g.smem, st>>>(a);
-    else
-      k_inv_x<kRadixAll><<<g.grid, g.block, g.smem, st>>>(a);
+    by_length(plan_x_, [&](auto rs, auto lx) { k_inv_x<decltype(rs)::value, decltype(lx)::value><<<g.grid, g.block, g.smem, st>>>(a); });
     RDCU_TRY(cudaGetLastError());
     if (!spectral) break;
   }
@@ -1633,10 +1664,7 @@ cudaError_t SpectralPlan::run(const RhsIO& io, cudaStream_t st) {
     a.io = io;
     const size_t smem = spectral ? fwd_.smem : 0;
     prep(a);
-    if (plan_is_pow2(plan_x_))
-      k_fwd_x<kRadixPow2><<<fwd_.grid, fwd_.block, smem, st>>>(a);
-    else
-      k_fwd_x<kRadixAll><<<fwd_.grid, fwd_.block, smem, st>>>(a);
+    by_length(plan_x_, [&](auto rs, auto lx) { k_fwd_x<decltype(rs)::value, decltype(lx)::value><<<fwd_.grid, fwd_.block, smem, st>>>(a); });
     RDCU_TRY(cudaGetLastError());
   }
   if (spectral && ndim == 3) {
@@ -1650,10 +1678,7 @@ cudaError_t SpectralPlan::run(const RhsIO& io, cudaStream_t st) {
     a.io = io;
     dim3 grid(c2c_f_.grid, n * Ns[0]);
     prep(a);
-    if (plan_is_pow2(plan_ax_[1]))
-      k_c2c<kRadixPow2, false><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(a);
-    else
-      k_c2c<kRadixAll, false><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(a);
+    by_length(plan_ax_[1], [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, false, decltype(lx)::value><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(a); });
     RDCU_TRY(cudaGetLastError());
   }
   return launch_passes(io, chan_table(ch_off_, ch_ent_, nch), h_ch_off_, nch, 0, nullptr, nullptr, st);
@@ -1677,10 +1702,7 @@ cudaError_t SpectralPlan::run_Y(const double* y, double* Yout, cudaStream_t st) 
   a.S = Sf_;
   a.io = io;
   prep(a);
-  if (plan_is_pow2(plan_x_))
-    k_fwd_x<kRadixPow2><<<fwd_.grid, fwd_.block, fwd_.smem, st>>>(a);
-  else
-    k_fwd_x<kRadixAll><<<fwd_.grid, fwd_.block, fwd_.smem, st>>>(a);
+  by_length(plan_x_, [&](auto rs, auto lx) { k_fwd_x<decltype(rs)::value, decltype(lx)::value><<<fwd_.grid, fwd_.block, fwd_.smem, st>>>(a); });
   RDCU_TRY(cudaGetLastError());
   if (ndim == 3) {
     C2CArgs c{};
@@ -1693,10 +1715,7 @@ cudaError_t SpectralPlan::run_Y(const double* y, double* Yout, cudaStream_t st) 
     c.io = io;
     dim3 grid(c2c_f_.grid, n * Ns[0]);
     prep(c);
-    if (plan_is_pow2(plan_ax_[1]))
-      k_c2c<kRadixPow2, false><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(c);
-    else
-      k_c2c<kRadixAll, false><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(c);
+    by_length(plan_ax_[1], [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, false, decltype(lx)::value><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(c); });
     RDCU_TRY(cudaGetLastError());
   }
   const ChanTable ct = chan_table(ych_off_, ych_ent_, ych_);
@@ -1777,10 +1796,7 @@ cudaError_t SpectralPlan::launch_forward(const double* y, cudaStream_t st) {
   a.S = Sf_;
   a.io = io;
   prep(a);
-  if (plan_is_pow2(plan_x_))
-    k_fwd_x<kRadixPow2><<<fwd_.grid, fwd_.block, fwd_.smem, st>>>(a);
-  else
-    k_fwd_x<kRadixAll><<<fwd_.grid, fwd_.block, fwd_.smem, st>>>(a);
+  by_length(plan_x_, [&](auto rs, auto lx) { k_fwd_x<decltype(rs)::value, decltype(lx)::value><<<fwd_.grid, fwd_.block, fwd_.smem, st>>>(a); });
   RDCU_TRY(cudaGetLastError());
   if (ndim == 3) {
     C2CArgs c{};
@@ -1793,10 +1809,7 @@ cudaError_t SpectralPlan::launch_forward(const double* y, cudaStream_t st) {
     c.io = io;
     dim3 grid(c2c_f_.grid, n * Ns[0]);
     prep(c);
-    if (plan_is_pow2(plan_ax_[1]))
-      k_c2c<kRadixPow2, false><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(c);
-    else
-      k_c2c<kRadixAll, false><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(c);
+    by_length(plan_ax_[1], [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, false, decltype(lx)::value><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(c); });
     RDCU_TRY(cudaGetLastError());
   }
   return cudaSuccess;
@@ -1847,10 +1860,7 @@ cudaError_t SpectralPlan::precond(const double* r, double* z, double alpha, cuda
       a.io = RhsIO{};
       dim3 grid(c2c_i_.grid, n * Ns[0]);
       prep(a);
-      if (plan_is_pow2(plan_ax_[1]))
-        k_c2c<kRadixPow2, true><<<grid, c2c_i_.block, c2c_i_.smem, st>>>(a);
-      else
-        k_c2c<kRadixAll, true><<<grid, c2c_i_.block, c2c_i_.smem, st>>>(a);
+      by_length(plan_ax_[1], [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, true, decltype(lx)::value><<<grid, c2c_i_.block, c2c_i_.smem, st>>>(a); });
       RDCU_TRY(cudaGetLastError());
     }
   } else {
@@ -1882,10 +1892,7 @@ cudaError_t SpectralPlan::precond(const double* r, double* z, double alpha, cuda
   a.P = g.per_cta;
   a.tw_smem = tws;
   prep(a);
-  if (plan_is_pow2(plan_x_))
-    k_inv_x<kRadixPow2><<<g.grid, g.block, g.smem, st>>>(a);
-  else
-    k_inv_x<kRadixAll><<<g.grid, g.block, g.smem, st>>>(a);
+  by_length(plan_x_, [&](auto rs, auto lx) { k_inv_x<decltype(rs)::value, decltype(lx)::value><<<g.grid, g.block, g.smem, st>>>(a); });
   return cudaGetLastError();
 }
 
@@ -1923,10 +1930,7 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
   fa.io = io;
   RDCU_TRY(timed("fwd_x", n * ((1 + nk) * arr + (s >= 2 ? arr : 0) + spec_row), [&]() {
     prep(fa);
-    if (plan_is_pow2(plan_x_))
-      k_fwd_x<kRadixPow2><<<fwd_.grid, fwd_.block, fwd_.smem, st>>>(fa);
-    else
-      k_fwd_x<kRadixAll><<<fwd_.grid, fwd_.block, fwd_.smem, st>>>(fa);
+    by_length(plan_x_, [&](auto rs, auto lx) { k_fwd_x<decltype(rs)::value, decltype(lx)::value><<<fwd_.grid, fwd_.block, fwd_.smem, st>>>(fa); });
     return cudaGetLastError();
   }));
   if (spectral && ndim == 3) {
@@ -1941,10 +1945,7 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
     dim3 grid(c2c_f_.grid, n * Ns[0]);
     RDCU_TRY(timed("c2c_axis1_fwd", 2.0 * n * spec_row, [&]() {
       prep(c);
-      if (plan_is_pow2(plan_ax_[1]))
-        k_c2c<kRadixPow2, false><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(c);
-      else
-        k_c2c<kRadixAll, false><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(c);
+      by_length(plan_ax_[1], [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, false, decltype(lx)::value><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(c); });
       return cudaGetLastError();
     }));
   }
@@ -1976,10 +1977,7 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
     const size_t msmem = c.smem;
     RDCU_TRY(timed("mid_axis0", (double)(n + nch) * spec_row, [&]() {
       prep(m);
-      if (plan_is_pow2(plan_ax_[0]))
-        k_mid<kRadixPow2><<<c.grid, c.block, msmem, st>>>(m);
-      else
-        k_mid<kRadixAll><<<c.grid, c.block, msmem, st>>>(m);
+      by_length(plan_ax_[0], [&](auto rs, auto lx) { k_mid<decltype(rs)::value, decltype(lx)::value><<<c.grid, c.block, msmem, st>>>(m); });
       return cudaGetLastError();
     }));
     if (ndim == 3) {
@@ -1994,10 +1992,7 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
       dim3 grid(c2c_i_.grid, nch * Ns[0]);
       RDCU_TRY(timed("c2c_axis1_inv", 2.0 * nch * spec_row, [&]() {
         prep(a);
-        if (plan_is_pow2(plan_ax_[1]))
-          k_c2c<kRadixPow2, true><<<grid, c2c_i_.block, c2c_i_.smem, st>>>(a);
-        else
-          k_c2c<kRadixAll, true><<<grid, c2c_i_.block, c2c_i_.smem, st>>>(a);
+        by_length(plan_ax_[1], [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, true, decltype(lx)::value><<<grid, c2c_i_.block, c2c_i_.smem, st>>>(a); });
         return cudaGetLastError();
       }));
     }
@@ -2023,10 +2018,7 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
   a.tw_smem = tws;
   RDCU_TRY(timed("inv_x_dictionary", nch * spec_row + 2.0 * n * arr, [&]() {
     prep(a);
-    if (plan_is_pow2(plan_x_))
-      k_inv_x<kRadixPow2><<<g.grid, g.block, g.smem, st>>>(a);
-    else
-      k_inv_x<kRadixAll><<<g.grid, g.block, g.smem, st>>>(a);
+    by_length(plan_x_, [&](auto rs, auto lx) { k_inv_x<decltype(rs)::value, decltype(lx)::value><<<g.grid, g.block, g.smem, st>>>(a); });
     return cudaGetLastError();
   }));
   cudaEventDestroy(e0);
