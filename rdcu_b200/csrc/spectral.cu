@@ -402,7 +402,32 @@ __device__ __forceinline__ void mid_body(const MidArgs& a, int bx) {
   __syncthreads();
   fft_lines_x<RS, LX, false>(fb, LS, a.nsrc * TW, a.plan, tw);
   if (a.sorted) {
-    // every channel at once: each distinct operator's multiplier once per point
+    // Every channel at once in dense form.  The operator-sorted entries become groups of
+    // one operator each with a coefficient matrix A[g][channel][source] (built once per
+    // CTA); per point, each group's multiplier beta_g is formed once and
+    //   channel c += i^q_g beta_g sum_s A[g][c][s] u_s.
+    int* sng = soff + a.G + 1;
+    ChanEntry* sgrp = reinterpret_cast<ChanEntry*>(reinterpret_cast<char*>(sm) +
+                                                   ((reinterpret_cast<char*>(sng + 1) - reinterpret_cast<char*>(sm) + 15) / 16 * 16));
+    double* sA = reinterpret_cast<double*>(sgrp + a.nent);
+    __syncthreads();  // staged entries visible
+    if (tid == 0) {
+      int g = -1, last = -1;
+      for (int qi = 0; qi < a.nent; ++qi) {
+        const ChanEntry en = se[qi];
+        const int key = en.nax | (en.ax0 << 2) | (en.ax1 << 4) | (en.part << 6);
+        if (key != last) {
+          last = key;
+          ++g;
+          sgrp[g] = en;
+          for (int k = 0; k < 16; ++k) sA[g * 16 + k] = 0.0;
+        }
+        sA[g * 16 + en.pad * 4 + en.src] += en.coef;
+      }
+      *sng = g + 1;
+    }
+    __syncthreads();
+    const int ngrp = *sng;
     const int npts = L0 * TW;
     for (int e = tid; e < npts; e += T) {
       const int z = fdiv(e, a.dTW), c = e - z * TW;
@@ -426,46 +451,52 @@ __device__ __forceinline__ void mid_body(const MidArgs& a, int bx) {
             km[ax] = skv[a.chan.kv_off[ax] + nm];
           }
         }
-        int last = -1, q = 0;
-        double beta = 0.0;
-        for (int qi = 0; qi < a.nent; ++qi) {
-          const ChanEntry en = se[qi];
-          const int key = en.nax | (en.ax0 << 2) | (en.ax1 << 4) | (en.part << 6);
-          if (key != last) {
-            last = key;
-            double ap = 1.0, am = 1.0;
-            if (en.nax >= 1) {
-              ap *= sel3(kp[0], kp[1], kp[2], en.ax0);
-              am *= sel3(km[0], km[1], km[2], en.ax0);
-            }
-            if (en.nax >= 2) {
-              ap *= sel3(kp[0], kp[1], kp[2], en.ax1);
-              am *= sel3(km[0], km[1], km[2], en.ax1);
-            }
-            const double sgn = (en.nax & 1) ? -1.0 : 1.0;
-            if (en.part == 0) {
-              q = en.nax;
-              beta = 0.5 * (ap + sgn * am);
-            } else {
-              q = en.nax + 3;
-              beta = 0.5 * (ap - sgn * am);
-            }
-          }
-          const double2 u = fb[(en.src * TW + c) * LS + z];
-          const double bc = beta * en.coef;
-          double2 v = make_double2(bc * u.x, bc * u.y);
-          switch (q & 3) {
-            case 1: v = make_double2(-v.y, v.x); break;
-            case 2: v = make_double2(-v.x, -v.y); break;
-            case 3: v = make_double2(v.y, -v.x); break;
-            default: break;
-          }
+        double2 u[4];
 #pragma unroll
-          for (int c4 = 0; c4 < 4; ++c4)
-            if (c4 == en.pad) {
-              acc[c4].x += v.x;
-              acc[c4].y += v.y;
+        for (int s4 = 0; s4 < 4; ++s4) u[s4] = s4 < a.nsrc ? fb[(s4 * TW + c) * LS + z] : make_double2(0.0, 0.0);
+        for (int g = 0; g < ngrp; ++g) {
+          const ChanEntry en = sgrp[g];
+          double ap = 1.0, am = 1.0;
+          if (en.nax >= 1) {
+            ap *= sel3(kp[0], kp[1], kp[2], en.ax0);
+            am *= sel3(km[0], km[1], km[2], en.ax0);
+          }
+          if (en.nax >= 2) {
+            ap *= sel3(kp[0], kp[1], kp[2], en.ax1);
+            am *= sel3(km[0], km[1], km[2], en.ax1);
+          }
+          const double sgn = (en.nax & 1) ? -1.0 : 1.0;
+          int q;
+          double beta;
+          if (en.part == 0) {
+            q = en.nax;
+            beta = 0.5 * (ap + sgn * am);
+          } else {
+            q = en.nax + 3;
+            beta = 0.5 * (ap - sgn * am);
+          }
+          const double* Ag = sA + g * 16;
+#pragma unroll
+          for (int c4 = 0; c4 < 4; ++c4) {
+            if (c4 >= a.G) break;
+            double2 sum = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int s4 = 0; s4 < 4; ++s4) {
+              if (s4 >= a.nsrc) break;
+              const double w = Ag[c4 * 4 + s4];
+              sum.x += w * u[s4].x;
+              sum.y += w * u[s4].y;
             }
+            double2 v = make_double2(beta * sum.x, beta * sum.y);
+            switch (q & 3) {
+              case 1: v = make_double2(-v.y, v.x); break;
+              case 2: v = make_double2(-v.x, -v.y); break;
+              case 3: v = make_double2(v.y, -v.x); break;
+              default: break;
+            }
+            acc[c4].x += v.x;
+            acc[c4].y += v.y;
+          }
         }
       }
 #pragma unroll
@@ -860,51 +891,82 @@ __device__ __forceinline__ void inv_x_body(const InvXArgs& a, int bx) {
   // stage-7 epilogue of adaptive steps only (fixed steps pass no partials buffer)
   const bool err = (a.io.mode == 1 && r.stage == 7 && a.io.err_part != nullptr);
   const int npts = P * M;
-  for (int e = tid; e < npts; e += T) {
-    const int pr = fdivc<LX>(e, a.dM);
-    const int x = e - pr * M;
-    const long long row = r0 + pr;
-    if (row >= a.R) continue;
-    double err2 = 0.0;
-    const double* ph = phys + (long long)pr * n * M + x;
-    const double2* ln = lines + (long long)pr * np * M + x;
+  // Each thread evaluates the dictionary at PPT points at once, so that the term and
+  // factor tables (warp-uniform shared-memory reads, loop control, the power switch) are
+  // read once per PPT points.  Points past the tile read a valid address and store nothing.
+  constexpr int PPT = 4;
+  for (int e0 = tid; e0 < npts; e0 += T * PPT) {
+    int phoff[PPT], lnoff[PPT];
+    long long gbase[PPT];
+    bool live[PPT];
+    double err2[PPT];
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) {
+      const int e = e0 + k * T;
+      const int pr = fdivc<LX>(e, a.dM);
+      const int x = e - pr * M;
+      const long long row = r0 + pr;
+      live[k] = e < npts && row < a.R;
+      phoff[k] = live[k] ? pr * n * M + x : 0;
+      lnoff[k] = live[k] ? pr * np * M + x : 0;
+      gbase[k] = live[k] ? row * M + x : 0;
+      err2[k] = 0.0;
+    }
     for (int i = 0; i < n; ++i) {
-      double acc = 0.0;
+      double acc[PPT];
       const int fc = sfold[i];
-      if (fc >= 0) {
-        const double2 z = ln[(fc >> 1) * M];
-        acc = (fc & 1) ? z.y : z.x;
+#pragma unroll
+      for (int k = 0; k < PPT; ++k) {
+        acc[k] = 0.0;
+        if (fc >= 0) {
+          const double2 z = lines[lnoff[k] + (fc >> 1) * M];
+          acc[k] = (fc & 1) ? z.y : z.x;
+        }
       }
       for (int t = sfb[i]; t < sfb[i + 1]; ++t) {
         const DictTerm tm = sterm[t];
-        double prod = 1.0;
+        double prod[PPT];
+#pragma unroll
+        for (int k = 0; k < PPT; ++k) prod[k] = 1.0;
         for (int q = 0; q < tm.nf; ++q) {
           const DictFactor fc2 = sfac[tm.off + q];
-          double v;
           if (fc2.q < n) {
-            v = ph[fc2.q * M];
+#pragma unroll
+            for (int k = 0; k < PPT; ++k) prod[k] *= ipow(phys[phoff[k] + fc2.q * M], fc2.eta);
           } else {
             const int c = fc2.q - n;
-            const double2 z = ln[(c >> 1) * M];
-            v = (c & 1) ? z.y : z.x;
+            const int co = (c >> 1) * M;
+#pragma unroll
+            for (int k = 0; k < PPT; ++k) {
+              const double2 z = lines[lnoff[k] + co];
+              prod[k] *= ipow((c & 1) ? z.y : z.x, fc2.eta);
+            }
           }
-          prod *= ipow(v, fc2.eta);
         }
-        acc += tm.C * prod;
+#pragma unroll
+        for (int k = 0; k < PPT; ++k) acc[k] += tm.C * prod[k];
       }
-      const long long gi = ((long long)i * a.R + row) * M + x;
-      r.f[gi] = acc;
-      if (err) {
-        // error kernel of dp45.cu:79-84 (e_2 = 0 drops k2)
-        const double ynew = ph[i * M];
-        const double yold = r.y[gi];
-        const double es = c_e[0] * r.k[0][gi] + c_e[2] * r.k[2][gi] + c_e[3] * r.k[3][gi] +
-                          c_e[4] * r.k[4][gi] + c_e[5] * r.k[5][gi] + c_e[6] * acc;
-        const double ev = r.h * es / (r.atol + r.rtol * fmax(fabs(yold), fabs(ynew)));
-        err2 += ev * ev;
+#pragma unroll
+      for (int k = 0; k < PPT; ++k) {
+        if (!live[k]) continue;
+        const long long gi = (long long)i * a.R * M + gbase[k];
+        r.f[gi] = acc[k];
+        if (err) {
+          // error kernel of dp45.cu:79-84 (e_2 = 0 drops k2)
+          const double ynew = phys[phoff[k] + i * M];
+          const double yold = r.y[gi];
+          const double es = c_e[0] * r.k[0][gi] + c_e[2] * r.k[2][gi] + c_e[3] * r.k[3][gi] +
+                            c_e[4] * r.k[4][gi] + c_e[5] * r.k[5][gi] + c_e[6] * acc[k];
+          const double ev = r.h * es / (r.atol + r.rtol * fmax(fabs(yold), fabs(ynew)));
+          err2[k] += ev * ev;
+        }
       }
     }
-    if (err) serr[e] = err2;
+    if (err) {
+#pragma unroll
+      for (int k = 0; k < PPT; ++k)
+        if (live[k]) serr[e0 + k * T] = err2[k];
+    }
   }
   if (err) {
     // one partial sum per grid row, in an order fixed by the row alone (x = lane,
@@ -1068,6 +1130,7 @@ static void inv_geometry(int M, int R, int n, int nch_run, bool yout, const Line
   // a single problem spreads its rows over the GPU; a batch member only sizes its tiles
   int P = batch_elems > 0 ? std::max(1, std::min(batch_elems / (M * npm), R))
                           : std::max(1, std::min(std::max(1, cta_elems() / (M * npm)), R / kTargetCtas));
+  auto block_of = [&](int p) { return std::min(kMaxBlock, std::max(128, round_up(stage_threads(plan, p * npm * M), 32))); };
   auto bytes = [&](int p, bool tws) {
     return (size_t)((spectral && tws ? M : 0) + (spectral ? p * np * M : 0)) * 16 +
            (yout ? 0 : (size_t)p * (n + 1) * M * 8 + extra);
@@ -1076,7 +1139,7 @@ static void inv_geometry(int M, int R, int n, int nch_run, bool yout, const Line
   const bool tws = bytes(P, true) <= kSmemBudget;
   c->per_cta = P;
   c->grid = (R + P - 1) / P;
-  c->block = std::min(kMaxBlock, std::max(128, round_up(stage_threads(plan, P * npm * M), 32)));
+  c->block = block_of(P);
   c->smem = bytes(P, tws);
   *tw_smem = tws ? 1 : 0;
 }
@@ -1388,7 +1451,7 @@ bool SpectralPlan::init(int n_, int ndim_, const int* Ns_, const double* Ls_,
   chk(upload_vec(&ch_off_, ch_off));
   chk(upload_vec(&ch_ent_, ch_ent));
   // operator-sorted copy of the hot entries with the local channel in .pad
-  if (nch >= 1 && nch <= 4) chk(upload_vec(&ch_sorted_, sorted_entries(ch_ent, ch_off, nch)));
+  if (nch >= 1 && nch <= 4 && n <= 4) chk(upload_vec(&ch_sorted_, sorted_entries(ch_ent, ch_off, nch)));
   chk(upload_vec(&d_terms_, dterms));
   chk(upload_vec(&d_fac_, dfac));
   chk(upload_vec(&d_field_begin_, field_begin));
@@ -1438,7 +1501,9 @@ bool SpectralPlan::init(int n_, int ndim_, const int* Ns_, const double* Ls_,
       }
       // plus the staged channel entries, wavenumbers and offsets (see k_mid)
       const int nent = which == 0 ? h_ch_off_[nch] : GY;
-      const size_t extra = (size_t)nent * sizeof(ChanEntry) + (size_t)kv_total_ * 8 + (size_t)(G + 1) * 4;
+      // (+ the dense operator groups of the all-channel path, see k_mid)
+      const size_t extra = (size_t)nent * sizeof(ChanEntry) + (size_t)kv_total_ * 8 + (size_t)(G + 2) * 4 + 16 +
+                           (size_t)nent * (sizeof(ChanEntry) + 16 * 8);
       auto smem_of = [&](int tw_, int gb) { return (size_t)(L0 + (n + gb) * tw_ * (L0 + 1)) * 16 + extra; };
       while (TW > 1 && smem_of(TW, GB) > kSmemBudget) TW /= 2;
       while (GB > 1 && smem_of(TW, GB) > kSmemBudget) --GB;
@@ -2123,7 +2188,8 @@ bool SpectralBatch::init(const std::vector<BatchMember>& members, int elems_, st
     const bool sorted = p.ch_sorted_ && nch <= GBp;
     int GB = sorted ? nch : std::min(std::max(nch, 1), 4);
     int TW = std::max(1, std::min(elems / (std::max(n, GB) * L0), I));
-    const size_t extra = (size_t)p.h_ch_off_[nch] * sizeof(ChanEntry) + (size_t)p.kv_total_ * 8 + (size_t)(nch + 1) * 4;
+    const size_t extra = (size_t)p.h_ch_off_[nch] * sizeof(ChanEntry) + (size_t)p.kv_total_ * 8 + (size_t)(nch + 2) * 4 +
+                         16 + (size_t)p.h_ch_off_[nch] * (sizeof(ChanEntry) + 16 * 8);
     auto smem_of = [&](int tw_, int gb) { return (size_t)(L0 + (n + gb) * tw_ * (L0 + 1)) * 16 + extra; };
     while (TW > 1 && (smem_of(TW, GB) > kSmemBudget || std::max(n, GB) * TW * L0 > kMaxElems)) TW /= 2;
     while (!sorted && GB > 1 && (smem_of(TW, GB) > kSmemBudget || std::max(n, GB) * TW * L0 > kMaxElems)) --GB;
@@ -2141,8 +2207,8 @@ bool SpectralBatch::init(const std::vector<BatchMember>& members, int elems_, st
     PassCfg gi;
     int itws = 0;
     inv_geometry(M, R, n, nch, false, p.plan_x_, &gi, &itws, p.dict_smem_bytes(), elems);
-    B.block[2] = std::max(B.block[2], gi.block);
     B.smem[2] = std::max(B.smem[2], gi.smem);
+    B.block[2] = std::max(B.block[2], gi.block);
     for (int j = 0; j < gi.grid; ++j) it[2].push_back(make_int2(m, j));
     for (int st = 1; st <= 7; ++st) {
       RhsIO io{};
