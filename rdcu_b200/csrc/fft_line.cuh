@@ -115,11 +115,19 @@ struct Dft<8, INV> {
 constexpr int kStageElems = 8;
 constexpr int kMaxBlock = 512;
 
+// Position of line element i under the swizzle of a radix-8 first stage: the low three
+// bits are XORed with the 8-element block index, so the eight consecutive outputs of a
+// butterfly land in eight different bank groups across a quarter warp.
+__device__ __forceinline__ int swz8(int i) { return i ^ ((i >> 3) & 7); }
+
 // One Stockham stage over nlines lines (stride LS) held in shared memory `buf`.
 // Requires blockDim.x * QMAX >= nlines*L/R; the caller sizes the block for that.
 // POW2: L and Ns are powers of two (index arithmetic by shifts); otherwise the
 // plan's precomputed invariant divisors are used.
-template <int R, bool INV, bool POW2>
+// SWZ: bit 0 writes the outputs at swz8 positions (a first stage, Ns = 1, R = 8: its
+// stride-8 stores otherwise put a quarter warp on one bank group); bit 1 reads the
+// inputs from swz8 positions (the stage after it).  Values are unchanged.
+template <int R, bool INV, bool POW2, int SWZ = 0>
 __device__ __forceinline__ void stockham_stage(double2* buf, int LS, int nlines, int L, int Ns, FastDiv dm,
                                                FastDiv dns, const double2* tw) {
   constexpr int QMAX = (R >= kStageElems) ? 1 : (kStageElems / R);
@@ -130,11 +138,12 @@ __device__ __forceinline__ void stockham_stage(double2* buf, int LS, int nlines,
   const int lm = POW2 ? __ffs(m) - 1 : 0;
   const int lns = POW2 ? __ffs(Ns) - 1 : 0;
   double2 v[QMAX][R];
-  int dst[QMAX];
+  int dst[QMAX], dbase[QMAX];
 #pragma unroll
   for (int q = 0; q < QMAX; ++q) {
     const int g = threadIdx.x + q * T;
     dst[q] = -1;
+    dbase[q] = 0;
     if (g < nb) {
       const int line = POW2 ? (g >> lm) : fdiv(g, dm);
       const int j = g - line * m;
@@ -144,12 +153,13 @@ __device__ __forceinline__ void stockham_stage(double2* buf, int LS, int nlines,
       const int tstep = kk * tstride;
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        double2 x = src[j + r * m];
+        double2 x = src[(SWZ & 2) ? swz8(j + r * m) : j + r * m];
         if (r > 0 && tstep != 0) x = c_mul(x, tw_get<INV>(tw, r * tstep));
         v[q][r] = x;
       }
       Dft<R, INV>::run(v[q], tw, L);
-      dst[q] = line * LS + jd * Ns * R + kk;
+      dbase[q] = line * LS;
+      dst[q] = jd * Ns * R + kk;
     }
   }
   __syncthreads();
@@ -157,7 +167,7 @@ __device__ __forceinline__ void stockham_stage(double2* buf, int LS, int nlines,
   for (int q = 0; q < QMAX; ++q) {
     if (dst[q] >= 0) {
 #pragma unroll
-      for (int r = 0; r < R; ++r) buf[dst[q] + r * Ns] = v[q][r];
+      for (int r = 0; r < R; ++r) buf[dbase[q] + ((SWZ & 1) ? swz8(dst[q] + r * Ns) : dst[q] + r * Ns)] = v[q][r];
     }
   }
   __syncthreads();
@@ -224,7 +234,9 @@ __device__ __forceinline__ void fft_pow2_t(double2* buf, int LS, int nlines, con
     constexpr int REM = L / NS;
     constexpr int R = (REM % 8 == 0) ? 8 : REM;  // REM is 8^a times 1, 2 or 4
     static_assert(R == 2 || R == 4 || R == 8, "power-of-two lengths only");
-    stockham_stage<R, INV, true>(buf, LS, nlines, L, NS, FastDiv{}, FastDiv{}, tw);
+    // a radix-8 first stage writes swizzled when a second stage reads it back
+    constexpr int SWZ = (NS == 1 && R == 8 && L > 8) ? 1 : (NS == 8 ? 2 : 0);
+    stockham_stage<R, INV, true, SWZ>(buf, LS, nlines, L, NS, FastDiv{}, FastDiv{}, tw);
     fft_pow2_t<L, INV, NS * R>(buf, LS, nlines, tw);
   }
 }
