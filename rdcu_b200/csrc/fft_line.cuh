@@ -126,10 +126,12 @@ __device__ __forceinline__ int swz8(int i) { return i ^ ((i >> 3) & 7); }
 // plan's precomputed invariant divisors are used.
 // SWZ: bit 0 writes the outputs at swz8 positions (a first stage, Ns = 1, R = 8: its
 // stride-8 stores otherwise put a quarter warp on one bank group); bit 1 reads the
-// inputs from swz8 positions (the stage after it).  Values are unchanged.
+// inputs from swz8 positions (the stage after it).  twz: the twiddle table is stored at
+// swz8 positions (the span-8 stage reads twiddles r*kk*L/64 for kk = 0..7, which
+// otherwise share a bank group).  Values are unchanged.
 template <int R, bool INV, bool POW2, int SWZ = 0>
 __device__ __forceinline__ void stockham_stage(double2* buf, int LS, int nlines, int L, int Ns, FastDiv dm,
-                                               FastDiv dns, const double2* tw) {
+                                               FastDiv dns, const double2* tw, bool twz = false) {
   constexpr int QMAX = (R >= kStageElems) ? 1 : (kStageElems / R);
   const int m = L / R;
   const int nb = nlines * m;
@@ -154,7 +156,7 @@ __device__ __forceinline__ void stockham_stage(double2* buf, int LS, int nlines,
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         double2 x = src[(SWZ & 2) ? swz8(j + r * m) : j + r * m];
-        if (r > 0 && tstep != 0) x = c_mul(x, tw_get<INV>(tw, r * tstep));
+        if (r > 0 && tstep != 0) x = c_mul(x, tw_get<INV>(tw, twz ? swz8(r * tstep) : r * tstep));
         v[q][r] = x;
       }
       Dft<R, INV>::run(v[q], tw, L);
@@ -229,15 +231,15 @@ __device__ void fft_lines(double2* buf, int LS, int nlines, const LinePlan& p, c
 // sequence of make_line_plan (radix 8 while 8 divides what is left, then 4 or 2) with
 // every length, span and stride a constant.  Bitwise equal to fft_lines on that plan.
 template <int L, bool INV, int NS = 1>
-__device__ __forceinline__ void fft_pow2_t(double2* buf, int LS, int nlines, const double2* tw) {
+__device__ __forceinline__ void fft_pow2_t(double2* buf, int LS, int nlines, const double2* tw, bool twz) {
   if constexpr (NS < L) {
     constexpr int REM = L / NS;
     constexpr int R = (REM % 8 == 0) ? 8 : REM;  // REM is 8^a times 1, 2 or 4
     static_assert(R == 2 || R == 4 || R == 8, "power-of-two lengths only");
     // a radix-8 first stage writes swizzled when a second stage reads it back
     constexpr int SWZ = (NS == 1 && R == 8 && L > 8) ? 1 : (NS == 8 ? 2 : 0);
-    stockham_stage<R, INV, true, SWZ>(buf, LS, nlines, L, NS, FastDiv{}, FastDiv{}, tw);
-    fft_pow2_t<L, INV, NS * R>(buf, LS, nlines, tw);
+    stockham_stage<R, INV, true, SWZ>(buf, LS, nlines, L, NS, FastDiv{}, FastDiv{}, tw, twz);
+    fft_pow2_t<L, INV, NS * R>(buf, LS, nlines, tw, twz);
   }
 }
 

@@ -204,12 +204,22 @@ __device__ __forceinline__ int fdivc(int n, FastDiv f) {
 }
 
 // Line FFTs of a pass: compile-time power-of-two length LX, or the plan's stages (LX = 0).
+// twz: the twiddle table is in shared memory at swz8 positions (stage_twiddles).
 template <int RS, int LX, bool INV>
-__device__ __forceinline__ void fft_lines_x(double2* buf, int LS, int nlines, const LinePlan& p, const double2* tw) {
+__device__ __forceinline__ void fft_lines_x(double2* buf, int LS, int nlines, const LinePlan& p, const double2* tw,
+                                            bool twz) {
   if constexpr (LX > 0)
-    fft_pow2_t<LX, INV>(buf, LS, nlines, tw);
+    fft_pow2_t<LX, INV>(buf, LS, nlines, tw, twz);
   else
     fft_lines<RS, INV>(buf, LS, nlines, p, tw);
+}
+
+// Copies the L-point twiddle table into shared memory; kernels specialised to a
+// power-of-two length store it swizzled (see fft_pow2_t).  Returns whether it did.
+template <int LX>
+__device__ __forceinline__ bool stage_twiddles(double2* dst, const double2* src, int L) {
+  for (int t = threadIdx.x; t < L; t += blockDim.x) dst[LX > 0 ? swz8(t) : t] = src[t];
+  return LX > 0;
 }
 
 // Stage state with the stage number known at compile time (slopes in registers).
@@ -278,10 +288,10 @@ __device__ __forceinline__ void fwd_x_body(const FwdXArgs& a, int bx) {
   const int M = LX ? LX : a.M, T = blockDim.x, tid = threadIdx.x;
   const double2* tw = a.tw;
   double2* buf = sm;
+  bool twz = false;
   if (a.do_fft && a.tw_smem) {
-    double2* tws = sm;
-    for (int t = tid; t < M; t += T) tws[t] = a.tw[t];
-    tw = tws;
+    twz = stage_twiddles<LX>(sm, a.tw, M);
+    tw = sm;
     buf = sm + M;
   }
   const long long row0 = 2LL * bx * a.P;
@@ -296,7 +306,7 @@ __device__ __forceinline__ void fwd_x_body(const FwdXArgs& a, int bx) {
   }
   if (!a.do_fft) return;
   __syncthreads();
-  fft_lines_x<RS, LX, false>(buf, M, a.P, a.plan, tw);
+  fft_lines_x<RS, LX, false>(buf, M, a.P, a.plan, tw, twz);
   const int Mh = LX ? LX / 2 + 1 : a.Mh;
   const int nout = a.P * 2 * Mh;
   for (int e = tid; e < nout; e += T) {
@@ -338,7 +348,7 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_c2c(C2CArgs a) {
   const int La = LX ? LX : a.La, TW = a.TW, LS = La + 1, T = blockDim.x, tid = threadIdx.x;
   double2* tw = sm;
   double2* buf = sm + La;
-  for (int t = tid; t < La; t += T) tw[t] = a.tw[t];
+  const bool twz = stage_twiddles<LX>(tw, a.tw, La);
   const long long i0 = (long long)blockIdx.x * TW;
   double2* base = a.S + (long long)blockIdx.y * La * a.I;
   const int nel = La * TW;
@@ -350,7 +360,7 @@ __global__ void __launch_bounds__(kMaxBlock, 1) k_c2c(C2CArgs a) {
   }
   cp_async_wait_all();
   __syncthreads();
-  fft_lines_x<RS, LX, INV>(buf, LS, TW, a.plan, tw);
+  fft_lines_x<RS, LX, INV>(buf, LS, TW, a.plan, tw, twz);
   for (int e = tid; e < nel; e += T) {
     const int z = fdiv(e, a.dTW), c = e - z * TW;
     const long long ii = i0 + c;
@@ -384,7 +394,7 @@ __device__ __forceinline__ void mid_body(const MidArgs& a, int bx) {
   ChanEntry* se = reinterpret_cast<ChanEntry*>(cb + a.GB * TW * LS);
   double* skv = reinterpret_cast<double*>(se + a.nent);
   int* soff = reinterpret_cast<int*>(skv + a.chan.kv_total);
-  for (int t = tid; t < L0; t += T) tw[t] = a.tw[t];
+  const bool twz = stage_twiddles<LX>(tw, a.tw, L0);
   for (int t = tid; t < a.nent; t += T) se[t] = a.chan.ent[a.ent0 + t];
   for (int t = tid; t < a.chan.kv_total; t += T) skv[t] = a.chan.kv[t];
   for (int t = tid; t <= a.G; t += T) soff[t] = a.chan.off[a.ch0 + t] - a.ent0;
@@ -400,7 +410,7 @@ __device__ __forceinline__ void mid_body(const MidArgs& a, int bx) {
   }
   cp_async_wait_all();
   __syncthreads();
-  fft_lines_x<RS, LX, false>(fb, LS, a.nsrc * TW, a.plan, tw);
+  fft_lines_x<RS, LX, false>(fb, LS, a.nsrc * TW, a.plan, tw, twz);
   if (a.sorted) {
     // Every channel at once in dense form.  The operator-sorted entries become groups of
     // one operator each with a coefficient matrix A[g][channel][source] (built once per
@@ -504,7 +514,7 @@ __device__ __forceinline__ void mid_body(const MidArgs& a, int bx) {
         if (c4 < a.G) cb[(c4 * TW + c) * LS + z] = acc[c4];
     }
     __syncthreads();
-    fft_lines_x<RS, LX, true>(cb, LS, a.G * TW, a.plan, tw);
+    fft_lines_x<RS, LX, true>(cb, LS, a.G * TW, a.plan, tw, twz);
     const int ncomp = a.G * L0 * TW;
     for (int e = tid; e < ncomp; e += T) {
       const int q0 = fdiv(e, a.dTW), c = e - q0 * TW;
@@ -551,7 +561,7 @@ __device__ __forceinline__ void mid_body(const MidArgs& a, int bx) {
       cb[(ch * TW + c) * LS + z] = acc;
     }
     __syncthreads();
-    fft_lines_x<RS, LX, true>(cb, LS, gc * TW, a.plan, tw);
+    fft_lines_x<RS, LX, true>(cb, LS, gc * TW, a.plan, tw, twz);
     for (int e = tid; e < ncomp; e += T) {
       const int q0 = fdiv(e, a.dTW), c = e - q0 * TW;
       const int ch = fdivc<LX>(q0, a.dL0), z = q0 - ch * L0;
@@ -771,10 +781,10 @@ __device__ __forceinline__ void inv_x_body(const InvXArgs& a, int bx) {
   const int P = a.P, np = a.npairs, n = a.n;
   const double2* tw = a.tw;
   double2* lines = sm;
+  bool twz = false;
   if (a.do_fft && a.tw_smem) {
-    double2* tws = sm;
-    for (int t = tid; t < M; t += T) tws[t] = a.tw[t];
-    tw = tws;
+    twz = stage_twiddles<LX>(sm, a.tw, M);
+    tw = sm;
     lines = sm + M;
   }
   double* phys = reinterpret_cast<double*>(lines + (a.do_fft ? P * np * M : 0));
@@ -864,7 +874,7 @@ __device__ __forceinline__ void inv_x_body(const InvXArgs& a, int bx) {
   }
   cp_async_wait_all();
   __syncthreads();
-  if (a.do_fft) fft_lines_x<RS, LX, true>(lines, M, P * np, a.plan, tw);
+  if (a.do_fft) fft_lines_x<RS, LX, true>(lines, M, P * np, a.plan, tw, twz);
 
   if (a.Yout) {
     const int nel = P * a.nch_run * M;
