@@ -193,6 +193,11 @@ struct FwdXArgs {
   RhsIO io;
 };
 
+// Largest block of the length-specialised kernels (the axis-0 pass is compiled for three
+// resident 256-thread CTAs per SM, at most 85 registers per thread, to hide shared-memory
+// and FP64 latency); a launch that needs more threads takes the general kernels.
+constexpr int kSpecBlock = 256;
+
 // Division by an invariant divisor: the compile-time constant D when D > 0, else the
 // precomputed FastDiv f.
 template <int D>
@@ -328,7 +333,7 @@ __device__ __forceinline__ void fwd_x_body(const FwdXArgs& a, int bx) {
 }
 
 template <int RS, int LX>
-__global__ void __launch_bounds__(kMaxBlock, 1) k_fwd_x(FwdXArgs a) {
+__global__ void __launch_bounds__(LX > 0 ? kSpecBlock : kMaxBlock, LX > 0 ? 2 : 1) k_fwd_x(FwdXArgs a) {
   fwd_x_body<RS, LX>(a, blockIdx.x);
 }
 
@@ -342,7 +347,7 @@ struct C2CArgs {
 };
 
 template <int RS, bool INV, int LX>
-__global__ void __launch_bounds__(kMaxBlock, 1) k_c2c(C2CArgs a) {
+__global__ void __launch_bounds__(LX > 0 ? kSpecBlock : kMaxBlock, LX > 0 ? 2 : 1) k_c2c(C2CArgs a) {
   extern __shared__ double2 sm[];
   if (a.io.mode == 1 && !a.io.ctl->running) return;
   const int La = LX ? LX : a.La, TW = a.TW, LS = La + 1, T = blockDim.x, tid = threadIdx.x;
@@ -389,9 +394,12 @@ __device__ __forceinline__ void mid_body(const MidArgs& a, int bx) {
   const int L0 = LX ? LX : a.L0, TW = a.TW, LS = L0 + 1, T = blockDim.x, tid = threadIdx.x;
   double2* tw = sm;
   double2* fb = sm + L0;
-  double2* cb = fb + a.nsrc * TW * LS;
+  // the all-channel path writes each point's channels over its own sources (every point
+  // belongs to one thread), so its channel lines reuse the source lines
+  const bool inplace = a.sorted && a.G <= a.nsrc;
+  double2* cb = inplace ? fb : fb + a.nsrc * TW * LS;
   // channel entries, offsets (relative to ent0) and wavenumbers staged in shared memory
-  ChanEntry* se = reinterpret_cast<ChanEntry*>(cb + a.GB * TW * LS);
+  ChanEntry* se = reinterpret_cast<ChanEntry*>(inplace ? fb + a.nsrc * TW * LS : cb + a.GB * TW * LS);
   double* skv = reinterpret_cast<double*>(se + a.nent);
   int* soff = reinterpret_cast<int*>(skv + a.chan.kv_total);
   const bool twz = stage_twiddles<LX>(tw, a.tw, L0);
@@ -573,7 +581,7 @@ __device__ __forceinline__ void mid_body(const MidArgs& a, int bx) {
 }
 
 template <int RS, int LX>
-__global__ void __launch_bounds__(kMaxBlock, 1) k_mid(MidArgs a) {
+__global__ void __launch_bounds__(LX > 0 ? kSpecBlock : kMaxBlock, LX > 0 ? 3 : 1) k_mid(MidArgs a) {
   mid_body<RS, LX>(a, blockIdx.x);
 }
 
@@ -996,7 +1004,7 @@ __device__ __forceinline__ void inv_x_body(const InvXArgs& a, int bx) {
 }
 
 template <int RS, int LX>
-__global__ void __launch_bounds__(kMaxBlock, 1) k_inv_x(InvXArgs a) {
+__global__ void __launch_bounds__(LX > 0 ? kSpecBlock : kMaxBlock, LX > 0 ? 2 : 1) k_inv_x(InvXArgs a) {
   inv_x_body<RS, LX>(a, blockIdx.x);
 }
 
@@ -1158,13 +1166,13 @@ static void inv_geometry(int M, int R, int n, int nch_run, bool yout, const Line
 // power-of-two lines of 64..512 points get kernels specialised to their length, other
 // power-of-two lines the shift-indexed kernels, every other length the general ones.
 template <typename F>
-static void by_length(const LinePlan& p, F&& f) {
+static void by_length(const LinePlan& p, int block, F&& f) {
   using RP = std::integral_constant<int, kRadixPow2>;
   if (!plan_is_pow2(p)) {
     f(std::integral_constant<int, kRadixAll>{}, std::integral_constant<int, 0>{});
     return;
   }
-  switch (p.L) {
+  switch (block <= kSpecBlock ? p.L : 0) {
     case 64: f(RP{}, std::integral_constant<int, 64>{}); return;
     case 128: f(RP{}, std::integral_constant<int, 128>{}); return;
     case 256: f(RP{}, std::integral_constant<int, 256>{}); return;
@@ -1525,6 +1533,8 @@ bool SpectralPlan::init(int n_, int ndim_, const int* Ns_, const double* Ls_,
       c.grid = (I + TW - 1) / TW;
       c.block = std::min(kMaxBlock, std::max(128, round_up(stage_threads(plan_ax_[0], std::max(n, GB) * TW * L0), 32)));
       c.smem = smem_of(TW, GB);
+      if (which == 0 && ch_sorted_ && nch <= GB && nch <= n)  // in-place channel lines (k_mid)
+        c.smem = (size_t)(L0 + n * TW * (L0 + 1)) * 16 + extra;
       c.per_cta = TW | (GB << 16);  // columns per CTA | channel lines held at once
     }
     if (ndim == 3) {
@@ -1559,14 +1569,17 @@ bool SpectralPlan::init(int n_, int ndim_, const int* Ns_, const double* Ls_,
   const int maxsm = 227 * 1024;
   bool optin_ok = true;
   auto optin_all = [&](const LinePlan& pl) {
-    by_length(pl, [&](auto rs, auto lx) {
-      constexpr int RS = decltype(rs)::value, LX = decltype(lx)::value;
-      optin_ok &= opt_in_smem((const void*)k_fwd_x<RS, LX>);
-      optin_ok &= opt_in_smem((const void*)k_inv_x<RS, LX>);
-      optin_ok &= opt_in_smem((const void*)k_mid<RS, LX>);
-      optin_ok &= opt_in_smem((const void*)k_c2c<RS, false, LX>);
-      optin_ok &= opt_in_smem((const void*)k_c2c<RS, true, LX>);
-    });
+    // the length-specialised kernels and the general ones larger blocks take
+    for (int blk : {kSpecBlock, kMaxBlock}) {
+      by_length(pl, blk, [&](auto rs, auto lx) {
+        constexpr int RS = decltype(rs)::value, LX = decltype(lx)::value;
+        optin_ok &= opt_in_smem((const void*)k_fwd_x<RS, LX>);
+        optin_ok &= opt_in_smem((const void*)k_inv_x<RS, LX>);
+        optin_ok &= opt_in_smem((const void*)k_mid<RS, LX>);
+        optin_ok &= opt_in_smem((const void*)k_c2c<RS, false, LX>);
+        optin_ok &= opt_in_smem((const void*)k_c2c<RS, true, LX>);
+      });
+    }
   };
   optin_all(plan_x_);
   for (int ax = 0; ax + 1 < ndim; ++ax) optin_all(plan_ax_[ax]);
@@ -1657,7 +1670,7 @@ cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, co
     }
     const size_t smem = c.smem;  // includes the staged tables
     prep(m);
-    by_length(plan_ax_[0], [&](auto rs, auto lx) { k_mid<decltype(rs)::value, decltype(lx)::value><<<c.grid, c.block, smem, st>>>(m); });
+    by_length(plan_ax_[0], c.block, [&](auto rs, auto lx) { k_mid<decltype(rs)::value, decltype(lx)::value><<<c.grid, c.block, smem, st>>>(m); });
     RDCU_TRY(cudaGetLastError());
     if (ndim == 3) {
       C2CArgs a{};
@@ -1670,7 +1683,7 @@ cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, co
       a.io = io;
       dim3 grid(c2c_i_.grid, nch_run * Ns[0]);
       prep(a);
-      by_length(plan_ax_[1], [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, true, decltype(lx)::value><<<grid, c2c_i_.block, c2c_i_.smem, st>>>(a); });
+      by_length(plan_ax_[1], c2c_i_.block, [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, true, decltype(lx)::value><<<grid, c2c_i_.block, c2c_i_.smem, st>>>(a); });
       RDCU_TRY(cudaGetLastError());
     }
   } else if (spectral) {
@@ -1715,7 +1728,7 @@ cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, co
     a.P = g.per_cta;
     a.tw_smem = tws;
     prep(a);
-    by_length(plan_x_, [&](auto rs, auto lx) { k_inv_x<decltype(rs)::value, decltype(lx)::value><<<g.grid, g.block, g.smem, st>>>(a); });
+    by_length(plan_x_, g.block, [&](auto rs, auto lx) { k_inv_x<decltype(rs)::value, decltype(lx)::value><<<g.grid, g.block, g.smem, st>>>(a); });
     RDCU_TRY(cudaGetLastError());
     if (!spectral) break;
   }
@@ -1739,7 +1752,7 @@ cudaError_t SpectralPlan::run(const RhsIO& io, cudaStream_t st) {
     a.io = io;
     const size_t smem = spectral ? fwd_.smem : 0;
     prep(a);
-    by_length(plan_x_, [&](auto rs, auto lx) { k_fwd_x<decltype(rs)::value, decltype(lx)::value><<<fwd_.grid, fwd_.block, smem, st>>>(a); });
+    by_length(plan_x_, fwd_.block, [&](auto rs, auto lx) { k_fwd_x<decltype(rs)::value, decltype(lx)::value><<<fwd_.grid, fwd_.block, smem, st>>>(a); });
     RDCU_TRY(cudaGetLastError());
   }
   if (spectral && ndim == 3) {
@@ -1753,7 +1766,7 @@ cudaError_t SpectralPlan::run(const RhsIO& io, cudaStream_t st) {
     a.io = io;
     dim3 grid(c2c_f_.grid, n * Ns[0]);
     prep(a);
-    by_length(plan_ax_[1], [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, false, decltype(lx)::value><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(a); });
+    by_length(plan_ax_[1], c2c_f_.block, [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, false, decltype(lx)::value><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(a); });
     RDCU_TRY(cudaGetLastError());
   }
   return launch_passes(io, chan_table(ch_off_, ch_ent_, nch), h_ch_off_, nch, 0, nullptr, nullptr, st);
@@ -1777,7 +1790,7 @@ cudaError_t SpectralPlan::run_Y(const double* y, double* Yout, cudaStream_t st) 
   a.S = Sf_;
   a.io = io;
   prep(a);
-  by_length(plan_x_, [&](auto rs, auto lx) { k_fwd_x<decltype(rs)::value, decltype(lx)::value><<<fwd_.grid, fwd_.block, fwd_.smem, st>>>(a); });
+  by_length(plan_x_, fwd_.block, [&](auto rs, auto lx) { k_fwd_x<decltype(rs)::value, decltype(lx)::value><<<fwd_.grid, fwd_.block, fwd_.smem, st>>>(a); });
   RDCU_TRY(cudaGetLastError());
   if (ndim == 3) {
     C2CArgs c{};
@@ -1790,7 +1803,7 @@ cudaError_t SpectralPlan::run_Y(const double* y, double* Yout, cudaStream_t st) 
     c.io = io;
     dim3 grid(c2c_f_.grid, n * Ns[0]);
     prep(c);
-    by_length(plan_ax_[1], [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, false, decltype(lx)::value><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(c); });
+    by_length(plan_ax_[1], c2c_f_.block, [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, false, decltype(lx)::value><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(c); });
     RDCU_TRY(cudaGetLastError());
   }
   const ChanTable ct = chan_table(ych_off_, ych_ent_, ych_);
@@ -1871,7 +1884,7 @@ cudaError_t SpectralPlan::launch_forward(const double* y, cudaStream_t st) {
   a.S = Sf_;
   a.io = io;
   prep(a);
-  by_length(plan_x_, [&](auto rs, auto lx) { k_fwd_x<decltype(rs)::value, decltype(lx)::value><<<fwd_.grid, fwd_.block, fwd_.smem, st>>>(a); });
+  by_length(plan_x_, fwd_.block, [&](auto rs, auto lx) { k_fwd_x<decltype(rs)::value, decltype(lx)::value><<<fwd_.grid, fwd_.block, fwd_.smem, st>>>(a); });
   RDCU_TRY(cudaGetLastError());
   if (ndim == 3) {
     C2CArgs c{};
@@ -1884,7 +1897,7 @@ cudaError_t SpectralPlan::launch_forward(const double* y, cudaStream_t st) {
     c.io = io;
     dim3 grid(c2c_f_.grid, n * Ns[0]);
     prep(c);
-    by_length(plan_ax_[1], [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, false, decltype(lx)::value><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(c); });
+    by_length(plan_ax_[1], c2c_f_.block, [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, false, decltype(lx)::value><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(c); });
     RDCU_TRY(cudaGetLastError());
   }
   return cudaSuccess;
@@ -1935,7 +1948,7 @@ cudaError_t SpectralPlan::precond(const double* r, double* z, double alpha, cuda
       a.io = RhsIO{};
       dim3 grid(c2c_i_.grid, n * Ns[0]);
       prep(a);
-      by_length(plan_ax_[1], [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, true, decltype(lx)::value><<<grid, c2c_i_.block, c2c_i_.smem, st>>>(a); });
+      by_length(plan_ax_[1], c2c_i_.block, [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, true, decltype(lx)::value><<<grid, c2c_i_.block, c2c_i_.smem, st>>>(a); });
       RDCU_TRY(cudaGetLastError());
     }
   } else {
@@ -1967,7 +1980,7 @@ cudaError_t SpectralPlan::precond(const double* r, double* z, double alpha, cuda
   a.P = g.per_cta;
   a.tw_smem = tws;
   prep(a);
-  by_length(plan_x_, [&](auto rs, auto lx) { k_inv_x<decltype(rs)::value, decltype(lx)::value><<<g.grid, g.block, g.smem, st>>>(a); });
+  by_length(plan_x_, g.block, [&](auto rs, auto lx) { k_inv_x<decltype(rs)::value, decltype(lx)::value><<<g.grid, g.block, g.smem, st>>>(a); });
   return cudaGetLastError();
 }
 
@@ -2005,7 +2018,7 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
   fa.io = io;
   RDCU_TRY(timed("fwd_x", n * ((1 + nk) * arr + (s >= 2 ? arr : 0) + spec_row), [&]() {
     prep(fa);
-    by_length(plan_x_, [&](auto rs, auto lx) { k_fwd_x<decltype(rs)::value, decltype(lx)::value><<<fwd_.grid, fwd_.block, fwd_.smem, st>>>(fa); });
+    by_length(plan_x_, fwd_.block, [&](auto rs, auto lx) { k_fwd_x<decltype(rs)::value, decltype(lx)::value><<<fwd_.grid, fwd_.block, fwd_.smem, st>>>(fa); });
     return cudaGetLastError();
   }));
   if (spectral && ndim == 3) {
@@ -2020,7 +2033,7 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
     dim3 grid(c2c_f_.grid, n * Ns[0]);
     RDCU_TRY(timed("c2c_axis1_fwd", 2.0 * n * spec_row, [&]() {
       prep(c);
-      by_length(plan_ax_[1], [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, false, decltype(lx)::value><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(c); });
+      by_length(plan_ax_[1], c2c_f_.block, [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, false, decltype(lx)::value><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(c); });
       return cudaGetLastError();
     }));
   }
@@ -2052,7 +2065,7 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
     const size_t msmem = c.smem;
     RDCU_TRY(timed("mid_axis0", (double)(n + nch) * spec_row, [&]() {
       prep(m);
-      by_length(plan_ax_[0], [&](auto rs, auto lx) { k_mid<decltype(rs)::value, decltype(lx)::value><<<c.grid, c.block, msmem, st>>>(m); });
+      by_length(plan_ax_[0], c.block, [&](auto rs, auto lx) { k_mid<decltype(rs)::value, decltype(lx)::value><<<c.grid, c.block, msmem, st>>>(m); });
       return cudaGetLastError();
     }));
     if (ndim == 3) {
@@ -2067,7 +2080,7 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
       dim3 grid(c2c_i_.grid, nch * Ns[0]);
       RDCU_TRY(timed("c2c_axis1_inv", 2.0 * nch * spec_row, [&]() {
         prep(a);
-        by_length(plan_ax_[1], [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, true, decltype(lx)::value><<<grid, c2c_i_.block, c2c_i_.smem, st>>>(a); });
+        by_length(plan_ax_[1], c2c_i_.block, [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, true, decltype(lx)::value><<<grid, c2c_i_.block, c2c_i_.smem, st>>>(a); });
         return cudaGetLastError();
       }));
     }
@@ -2093,7 +2106,7 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
   a.tw_smem = tws;
   RDCU_TRY(timed("inv_x_dictionary", nch * spec_row + 2.0 * n * arr, [&]() {
     prep(a);
-    by_length(plan_x_, [&](auto rs, auto lx) { k_inv_x<decltype(rs)::value, decltype(lx)::value><<<g.grid, g.block, g.smem, st>>>(a); });
+    by_length(plan_x_, g.block, [&](auto rs, auto lx) { k_inv_x<decltype(rs)::value, decltype(lx)::value><<<g.grid, g.block, g.smem, st>>>(a); });
     return cudaGetLastError();
   }));
   cudaEventDestroy(e0);
@@ -2210,7 +2223,7 @@ bool SpectralBatch::init(const std::vector<BatchMember>& members, int elems_, st
     const int gm = (I + TW - 1) / TW;
     if (spectral) {
       B.block[1] = std::max(B.block[1], std::min(kMaxBlock, std::max(128, round_up(stage_threads(p.plan_ax_[0], std::max(n, GB) * TW * L0), 32))));
-      B.smem[1] = std::max(B.smem[1], smem_of(TW, GB));
+      B.smem[1] = std::max(B.smem[1], sorted && nch <= n ? (size_t)(L0 + n * TW * (L0 + 1)) * 16 + extra : smem_of(TW, GB));
       for (int j = 0; j < gm; ++j) it[1].push_back(make_int2(m, j));
     }
     // inv_x tiles
