@@ -797,10 +797,8 @@ __device__ __forceinline__ void inv_x_body(const InvXArgs& a, int bx) {
   }
   double* phys = reinterpret_cast<double*>(lines + (a.do_fft ? P * np * M : 0));
   const long long r0 = (long long)bx * P;
-  // per-point squared error of stage 7 (summed over the fields), then the tables
-  double* serr = phys + (long long)P * n * M;
   // dictionary tables staged in shared memory (read by every point)
-  DictTerm* sterm = reinterpret_cast<DictTerm*>(serr + (long long)P * M);
+  DictTerm* sterm = reinterpret_cast<DictTerm*>(phys + (long long)P * n * M);
   DictFactor* sfac = reinterpret_cast<DictFactor*>(sterm + a.dict.nterms);
   int* sfb = reinterpret_cast<int*>(sfac + a.dict.nfac);
   int* sfold = sfb + n + 1;
@@ -981,9 +979,11 @@ __device__ __forceinline__ void inv_x_body(const InvXArgs& a, int bx) {
       }
     }
     if (err) {
+      // a point's squared error replaces its own first field in the staging buffer (no
+      // other thread reads that point)
 #pragma unroll
       for (int k = 0; k < PPT; ++k)
-        if (live[k]) serr[e0 + k * T] = err2[k];
+        if (live[k]) phys[phoff[k]] = err2[k];
     }
   }
   if (err) {
@@ -996,7 +996,7 @@ __device__ __forceinline__ void inv_x_body(const InvXArgs& a, int bx) {
       const long long row = r0 + pr;
       if (row >= a.R) break;
       double v = 0.0;
-      for (int x = lane; x < M; x += 32) v += serr[pr * M + x];
+      for (int x = lane; x < M; x += 32) v += phys[pr * n * M + x];
       for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
       if (lane == 0) a.io.err_part[row] = v;
     }
@@ -1004,7 +1004,7 @@ __device__ __forceinline__ void inv_x_body(const InvXArgs& a, int bx) {
 }
 
 template <int RS, int LX>
-__global__ void __launch_bounds__(LX > 0 ? kSpecBlock : kMaxBlock, LX > 0 ? 2 : 1) k_inv_x(InvXArgs a) {
+__global__ void __launch_bounds__(LX > 0 ? kSpecBlock : kMaxBlock, LX > 0 ? 3 : 1) k_inv_x(InvXArgs a) {
   inv_x_body<RS, LX>(a, blockIdx.x);
 }
 
@@ -1151,7 +1151,7 @@ static void inv_geometry(int M, int R, int n, int nch_run, bool yout, const Line
   auto block_of = [&](int p) { return std::min(kMaxBlock, std::max(128, round_up(stage_threads(plan, p * npm * M), 32))); };
   auto bytes = [&](int p, bool tws) {
     return (size_t)((spectral && tws ? M : 0) + (spectral ? p * np * M : 0)) * 16 +
-           (yout ? 0 : (size_t)p * (n + 1) * M * 8 + extra);
+           (yout ? 0 : (size_t)p * n * M * 8 + extra);
   };
   while (P > 1 && bytes(P, true) > kSmemBudget) P /= 2;
   const bool tws = bytes(P, true) <= kSmemBudget;
