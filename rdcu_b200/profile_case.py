@@ -10,23 +10,12 @@ import json
 import numpy as np
 
 from . import Solver, random_ic
+from .problems import cgle_coupling_lines
 
 
 def cgle_terms(ndim, b=2.0, c=0.8):
-    n = 2
-
-    def dd(i, j):
-        return n + ndim * n + (j * ndim + j) * n + i
-
-    lines = ["1.0,0,0,1"] + ["1.0,0,%d,1" % dd(0, j) for j in range(ndim)]
-    lines += ["-%f,0,%d,1" % (b, dd(1, j)) for j in range(ndim)]
-    lines += ["-1.0,0,0,3", "-1.0,0,0,1,1,2", "1.0,1,1,1"]
-    lines += ["1.0,1,%d,1" % dd(1, j) for j in range(ndim)]
-    lines += ["%f,1,%d,1" % (b, dd(0, j)) for j in range(ndim)]
-    lines += ["-1.0,1,0,2,1,1", "-1.0,1,1,3", "%f,1,0,3" % c, "%f,1,0,1,1,2" % c, "-%f,0,0,2,1,1" % c,
-              "-%f,0,1,3" % c]
     out = []
-    for s in lines:
+    for s in cgle_coupling_lines(ndim, b, c):
         t = s.split(",")
         out.append((float(t[0]), [int(x) for x in t[1:]]))
     return out
