@@ -198,6 +198,11 @@ struct FwdXArgs {
 // and FP64 latency); a launch that needs more threads takes the general kernels.
 constexpr int kSpecBlock = 256;
 
+// Line stride (in double2) of the column tiles of the strided-axis passes: TW columns of
+// one row are consecutive threads, so line c starts at c * LS; LS = L + 8/TW (at least
+// L + 1) makes c * LS + z hit distinct 16-byte bank groups across a quarter warp.
+__host__ __device__ __forceinline__ int tile_stride(int L, int TW) { return L + (TW >= 8 ? 1 : 8 / TW); }
+
 // Division by an invariant divisor: the compile-time constant D when D > 0, else the
 // precomputed FastDiv f.
 template <int D>
@@ -350,7 +355,7 @@ template <int RS, bool INV, int LX>
 __global__ void __launch_bounds__(LX > 0 ? kSpecBlock : kMaxBlock, LX > 0 ? 2 : 1) k_c2c(C2CArgs a) {
   extern __shared__ double2 sm[];
   if (a.io.mode == 1 && !a.io.ctl->running) return;
-  const int La = LX ? LX : a.La, TW = a.TW, LS = La + 1, T = blockDim.x, tid = threadIdx.x;
+  const int La = LX ? LX : a.La, TW = a.TW, LS = tile_stride(La, TW), T = blockDim.x, tid = threadIdx.x;
   double2* tw = sm;
   double2* buf = sm + La;
   const bool twz = stage_twiddles<LX>(tw, a.tw, La);
@@ -391,7 +396,7 @@ template <int RS, int LX>
 __device__ __forceinline__ void mid_body(const MidArgs& a, int bx) {
   extern __shared__ double2 sm[];
   if (a.io.mode == 1 && !a.io.ctl->running) return;
-  const int L0 = LX ? LX : a.L0, TW = a.TW, LS = L0 + 1, T = blockDim.x, tid = threadIdx.x;
+  const int L0 = LX ? LX : a.L0, TW = a.TW, LS = tile_stride(L0, TW), T = blockDim.x, tid = threadIdx.x;
   double2* tw = sm;
   double2* fb = sm + L0;
   // the all-channel path writes each point's channels over its own sources (every point
@@ -1522,7 +1527,7 @@ bool SpectralPlan::init(int n_, int ndim_, const int* Ns_, const double* Ls_,
       // (+ the dense operator groups of the all-channel path, see k_mid)
       const size_t extra = (size_t)nent * sizeof(ChanEntry) + (size_t)kv_total_ * 8 + (size_t)(G + 2) * 4 + 16 +
                            (size_t)nent * (sizeof(ChanEntry) + 16 * 8);
-      auto smem_of = [&](int tw_, int gb) { return (size_t)(L0 + (n + gb) * tw_ * (L0 + 1)) * 16 + extra; };
+      auto smem_of = [&](int tw_, int gb) { return (size_t)(L0 + (n + gb) * tw_ * tile_stride(L0, tw_)) * 16 + extra; };
       while (TW > 1 && smem_of(TW, GB) > kSmemBudget) TW /= 2;
       while (GB > 1 && smem_of(TW, GB) > kSmemBudget) --GB;
       if (smem_of(TW, GB) > 227 * 1024) {
@@ -1534,17 +1539,17 @@ bool SpectralPlan::init(int n_, int ndim_, const int* Ns_, const double* Ls_,
       c.block = std::min(kMaxBlock, std::max(128, round_up(stage_threads(plan_ax_[0], std::max(n, GB) * TW * L0), 32)));
       c.smem = smem_of(TW, GB);
       if (which == 0 && ch_sorted_ && nch <= GB && nch <= n)  // in-place channel lines (k_mid)
-        c.smem = (size_t)(L0 + n * TW * (L0 + 1)) * 16 + extra;
+        c.smem = (size_t)(L0 + n * TW * tile_stride(L0, TW)) * 16 + extra;
       c.per_cta = TW | (GB << 16);  // columns per CTA | channel lines held at once
     }
     if (ndim == 3) {
       const int La = Ns[1], I1 = Mh;
       int TW = std::min(16, I1);
-      while (TW > 1 && ((size_t)(La + TW * (La + 1)) * 16 > kSmemBudget || TW * La > cta_elems())) TW /= 2;
+      while (TW > 1 && ((size_t)(La + TW * tile_stride(La, TW)) * 16 > kSmemBudget || TW * La > cta_elems())) TW /= 2;
       c2c_f_.per_cta = TW;
       c2c_f_.grid = (I1 + TW - 1) / TW;
       c2c_f_.block = std::min(kMaxBlock, std::max(128, round_up(stage_threads(plan_ax_[1], TW * La), 32)));
-      c2c_f_.smem = (size_t)(La + TW * (La + 1)) * 16;
+      c2c_f_.smem = (size_t)(La + TW * tile_stride(La, TW)) * 16;
       c2c_i_ = c2c_f_;
     }
   }
@@ -2213,7 +2218,7 @@ bool SpectralBatch::init(const std::vector<BatchMember>& members, int elems_, st
     int TW = std::max(1, std::min(elems / (std::max(n, GB) * L0), I));
     const size_t extra = (size_t)p.h_ch_off_[nch] * sizeof(ChanEntry) + (size_t)p.kv_total_ * 8 + (size_t)(nch + 2) * 4 +
                          16 + (size_t)p.h_ch_off_[nch] * (sizeof(ChanEntry) + 16 * 8);
-    auto smem_of = [&](int tw_, int gb) { return (size_t)(L0 + (n + gb) * tw_ * (L0 + 1)) * 16 + extra; };
+    auto smem_of = [&](int tw_, int gb) { return (size_t)(L0 + (n + gb) * tw_ * tile_stride(L0, tw_)) * 16 + extra; };
     while (TW > 1 && (smem_of(TW, GB) > kSmemBudget || std::max(n, GB) * TW * L0 > kMaxElems)) TW /= 2;
     while (!sorted && GB > 1 && (smem_of(TW, GB) > kSmemBudget || std::max(n, GB) * TW * L0 > kMaxElems)) --GB;
     if (spectral && (smem_of(TW, GB) > 227 * 1024 || std::max(n, GB) * TW * L0 > kMaxElems)) {
@@ -2223,7 +2228,8 @@ bool SpectralBatch::init(const std::vector<BatchMember>& members, int elems_, st
     const int gm = (I + TW - 1) / TW;
     if (spectral) {
       B.block[1] = std::max(B.block[1], std::min(kMaxBlock, std::max(128, round_up(stage_threads(p.plan_ax_[0], std::max(n, GB) * TW * L0), 32))));
-      B.smem[1] = std::max(B.smem[1], sorted && nch <= n ? (size_t)(L0 + n * TW * (L0 + 1)) * 16 + extra : smem_of(TW, GB));
+      B.smem[1] = std::max(B.smem[1], sorted && nch <= n ? (size_t)(L0 + n * TW * tile_stride(L0, TW)) * 16 + extra
+                                                         : smem_of(TW, GB));
       for (int j = 0; j < gm; ++j) it[1].push_back(make_int2(m, j));
     }
     // inv_x tiles
