@@ -94,6 +94,42 @@ struct DictTable {
   const int* field_begin;     // [n+1]
   const int* fold;            // [n] channel holding the folded linear part, -1 if none
   int nfac;                   // number of factors (fac length)
+  // Dense form when every term is a product of fields of total degree <= 3 in poly_nf
+  // (= n <= 3) fields: f_i = fold_i + sum_m poly[i * poly_count + m] * monomial_m (Mono
+  // order); poly_nf = 0 otherwise.
+  const double* poly;
+  int poly_nf, poly_count;
+};
+
+// Monomials of total degree <= 3 in NF variables, in a fixed order: monomial 0 is 1 and
+// monomial m > 0 is monomial parent(m) times variable var(m).
+template <int NF>
+struct Mono;
+template <>
+struct Mono<1> {
+  static constexpr int count = 4;
+  __host__ __device__ static constexpr int parent(int m) { return m - 1; }
+  __host__ __device__ static constexpr int var(int) { return 0; }
+};
+template <>
+struct Mono<2> {
+  static constexpr int count = 10;  // 1 u v uu uv vv uuu uuv uvv vvv
+  __host__ __device__ static constexpr int parent(int m) {
+    return m == 1 || m == 2 ? 0 : m == 3 || m == 4 ? 1 : m == 5 ? 2 : m == 6 || m == 7 ? 3 : m == 8 ? 4 : 5;
+  }
+  __host__ __device__ static constexpr int var(int m) { return m == 1 || m == 3 || m == 6 ? 0 : 1; }
+};
+template <>
+struct Mono<3> {
+  static constexpr int count = 20;
+  __host__ __device__ static constexpr int parent(int m) {
+    constexpr int p[20] = {-1, 0, 0, 0, 1, 1, 1, 2, 2, 3, 4, 4, 4, 5, 5, 6, 7, 7, 8, 9};
+    return p[m];
+  }
+  __host__ __device__ static constexpr int var(int m) {
+    constexpr int v[20] = {-1, 0, 1, 2, 0, 1, 2, 1, 2, 2, 0, 1, 2, 1, 2, 2, 1, 2, 2, 2};
+    return v[m];
+  }
 };
 
 // Constant-coefficient linear part of the finite-difference Jacobian, one entry per

@@ -27,6 +27,7 @@
 // reference's block is IFFT(Mi U) with Mi(k) = (M(k) - conj(M(-k)))/(2i); Y.dat output
 // uses both.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -803,11 +804,14 @@ __device__ __forceinline__ void inv_x_body(const InvXArgs& a, int bx) {
   double* phys = reinterpret_cast<double*>(lines + (a.do_fft ? P * np * M : 0));
   const long long r0 = (long long)bx * P;
   // dictionary tables staged in shared memory (read by every point)
-  DictTerm* sterm = reinterpret_cast<DictTerm*>(phys + (long long)P * n * M);
+  double* spoly = phys + (long long)P * n * M;
+  const int npoly = a.dict.poly_nf ? n * a.dict.poly_count : 0;
+  DictTerm* sterm = reinterpret_cast<DictTerm*>(spoly + npoly);
   DictFactor* sfac = reinterpret_cast<DictFactor*>(sterm + a.dict.nterms);
   int* sfb = reinterpret_cast<int*>(sfac + a.dict.nfac);
   int* sfold = sfb + n + 1;
   if (!a.Yout) {
+    for (int t = tid; t < npoly; t += T) spoly[t] = a.dict.poly[t];
     for (int t = tid; t < a.dict.nterms; t += T) sterm[t] = a.dict.terms[t];
     for (int t = tid; t < a.dict.nfac; t += T) sfac[t] = a.dict.fac[t];
     for (int t = tid; t <= n; t += T) sfb[t] = a.dict.field_begin[t];
@@ -912,84 +916,116 @@ __device__ __forceinline__ void inv_x_body(const InvXArgs& a, int bx) {
   // stage-7 epilogue of adaptive steps only (fixed steps pass no partials buffer)
   const bool err = (a.io.mode == 1 && r.stage == 7 && a.io.err_part != nullptr);
   const int npts = P * M;
-  // Each thread evaluates the dictionary at PPT points at once, so that the term and
-  // factor tables (warp-uniform shared-memory reads, loop control, the power switch) are
-  // read once per PPT points.  Points past the tile read a valid address and store nothing.
-  constexpr int PPT = 4;
-  for (int e0 = tid; e0 < npts; e0 += T * PPT) {
-    int phoff[PPT], lnoff[PPT];
-    long long gbase[PPT];
-    bool live[PPT];
-    double err2[PPT];
-#pragma unroll
-    for (int k = 0; k < PPT; ++k) {
-      const int e = e0 + k * T;
-      const int pr = fdivc<LX>(e, a.dM);
-      const int x = e - pr * M;
-      const long long row = r0 + pr;
-      live[k] = e < npts && row < a.R;
-      phoff[k] = live[k] ? pr * n * M + x : 0;
-      lnoff[k] = live[k] ? pr * np * M + x : 0;
-      gbase[k] = live[k] ? row * M + x : 0;
-      err2[k] = 0.0;
-    }
-    for (int i = 0; i < n; ++i) {
-      double acc[PPT];
-      const int fc = sfold[i];
+  // Each thread evaluates the dictionary at PPT points at once, so that the tables
+  // (warp-uniform shared-memory reads, loop control, the power switch) are read once per
+  // PPT points.  Points past the tile read a valid address and store nothing.  NF > 0: the
+  // dense polynomial form (all monomials of the NF fields once per point, then one
+  // multiply-add per monomial and field); NF = 0: the term list.
+  auto points = [&](auto ppt, auto nf) {
+    constexpr int PPT = decltype(ppt)::value, NF = decltype(nf)::value;
+    for (int e0 = tid; e0 < npts; e0 += T * PPT) {
+      int phoff[PPT], lnoff[PPT];
+      long long gbase[PPT];
+      bool live[PPT];
+      double err2[PPT];
 #pragma unroll
       for (int k = 0; k < PPT; ++k) {
-        acc[k] = 0.0;
-        if (fc >= 0) {
-          const double2 z = lines[lnoff[k] + (fc >> 1) * M];
-          acc[k] = (fc & 1) ? z.y : z.x;
+        const int e = e0 + k * T;
+        const int pr = fdivc<LX>(e, a.dM);
+        const int x = e - pr * M;
+        const long long row = r0 + pr;
+        live[k] = e < npts && row < a.R;
+        phoff[k] = live[k] ? pr * n * M + x : 0;
+        lnoff[k] = live[k] ? pr * np * M + x : 0;
+        gbase[k] = live[k] ? row * M + x : 0;
+        err2[k] = 0.0;
+      }
+      double mono[PPT][NF > 0 ? Mono<(NF > 0 ? NF : 1)>::count : 1];
+      if constexpr (NF > 0) {
+        using MN = Mono<NF>;
+#pragma unroll
+        for (int k = 0; k < PPT; ++k) {
+          mono[k][0] = 1.0;
+#pragma unroll
+          for (int m = 1; m < MN::count; ++m) mono[k][m] = mono[k][MN::parent(m)] * phys[phoff[k] + MN::var(m) * M];
         }
       }
-      for (int t = sfb[i]; t < sfb[i + 1]; ++t) {
-        const DictTerm tm = sterm[t];
-        double prod[PPT];
+      for (int i = 0; i < n; ++i) {
+        double acc[PPT];
+        const int fc = sfold[i];
 #pragma unroll
-        for (int k = 0; k < PPT; ++k) prod[k] = 1.0;
-        for (int q = 0; q < tm.nf; ++q) {
-          const DictFactor fc2 = sfac[tm.off + q];
-          if (fc2.q < n) {
+        for (int k = 0; k < PPT; ++k) {
+          acc[k] = 0.0;
+          if (fc >= 0) {
+            const double2 z = lines[lnoff[k] + (fc >> 1) * M];
+            acc[k] = (fc & 1) ? z.y : z.x;
+          }
+        }
+        if constexpr (NF > 0) {
+          const double* ci = spoly + i * Mono<NF>::count;
 #pragma unroll
-            for (int k = 0; k < PPT; ++k) prod[k] *= ipow(phys[phoff[k] + fc2.q * M], fc2.eta);
-          } else {
-            const int c = fc2.q - n;
-            const int co = (c >> 1) * M;
+          for (int m = 0; m < Mono<NF>::count; ++m) {
+            const double c = ci[m];
 #pragma unroll
-            for (int k = 0; k < PPT; ++k) {
-              const double2 z = lines[lnoff[k] + co];
-              prod[k] *= ipow((c & 1) ? z.y : z.x, fc2.eta);
+            for (int k = 0; k < PPT; ++k) acc[k] += c * mono[k][m];
+          }
+        } else {
+          for (int t = sfb[i]; t < sfb[i + 1]; ++t) {
+            const DictTerm tm = sterm[t];
+            double prod[PPT];
+#pragma unroll
+            for (int k = 0; k < PPT; ++k) prod[k] = 1.0;
+            for (int q = 0; q < tm.nf; ++q) {
+              const DictFactor fc2 = sfac[tm.off + q];
+              if (fc2.q < n) {
+#pragma unroll
+                for (int k = 0; k < PPT; ++k) prod[k] *= ipow(phys[phoff[k] + fc2.q * M], fc2.eta);
+              } else {
+                const int c = fc2.q - n;
+                const int co = (c >> 1) * M;
+#pragma unroll
+                for (int k = 0; k < PPT; ++k) {
+                  const double2 z = lines[lnoff[k] + co];
+                  prod[k] *= ipow((c & 1) ? z.y : z.x, fc2.eta);
+                }
+              }
             }
+#pragma unroll
+            for (int k = 0; k < PPT; ++k) acc[k] += tm.C * prod[k];
           }
         }
 #pragma unroll
-        for (int k = 0; k < PPT; ++k) acc[k] += tm.C * prod[k];
-      }
-#pragma unroll
-      for (int k = 0; k < PPT; ++k) {
-        if (!live[k]) continue;
-        const long long gi = (long long)i * a.R * M + gbase[k];
-        r.f[gi] = acc[k];
-        if (err) {
-          // error kernel of dp45.cu:79-84 (e_2 = 0 drops k2)
-          const double ynew = phys[phoff[k] + i * M];
-          const double yold = r.y[gi];
-          const double es = c_e[0] * r.k[0][gi] + c_e[2] * r.k[2][gi] + c_e[3] * r.k[3][gi] +
-                            c_e[4] * r.k[4][gi] + c_e[5] * r.k[5][gi] + c_e[6] * acc[k];
-          const double ev = r.h * es / (r.atol + r.rtol * fmax(fabs(yold), fabs(ynew)));
-          err2[k] += ev * ev;
+        for (int k = 0; k < PPT; ++k) {
+          if (!live[k]) continue;
+          const long long gi = (long long)i * a.R * M + gbase[k];
+          r.f[gi] = acc[k];
+          if (err) {
+            // error kernel of dp45.cu:79-84 (e_2 = 0 drops k2)
+            const double ynew = phys[phoff[k] + i * M];
+            const double yold = r.y[gi];
+            const double es = c_e[0] * r.k[0][gi] + c_e[2] * r.k[2][gi] + c_e[3] * r.k[3][gi] +
+                              c_e[4] * r.k[4][gi] + c_e[5] * r.k[5][gi] + c_e[6] * acc[k];
+            const double ev = r.h * es / (r.atol + r.rtol * fmax(fabs(yold), fabs(ynew)));
+            err2[k] += ev * ev;
+          }
         }
       }
-    }
-    if (err) {
-      // a point's squared error replaces its own first field in the staging buffer (no
-      // other thread reads that point)
+      if (err) {
+        // a point's squared error replaces its own first field in the staging buffer (no
+        // other thread reads that point)
 #pragma unroll
-      for (int k = 0; k < PPT; ++k)
-        if (live[k]) phys[phoff[k]] = err2[k];
+        for (int k = 0; k < PPT; ++k)
+          if (live[k]) phys[phoff[k]] = err2[k];
+      }
     }
+  };
+  using I1 = std::integral_constant<int, 1>;
+  using I2 = std::integral_constant<int, 2>;
+  switch (a.dict.poly_nf) {
+    case 1: points(I2{}, I1{}); break;
+    case 2: points(I2{}, I2{}); break;
+    case 3: points(I1{}, std::integral_constant<int, 3>{}); break;
+    default: points(std::integral_constant<int, 4>{}, std::integral_constant<int, 0>{}); break;
   }
   if (err) {
     // one partial sum per grid row, in an order fixed by the row alone (x = lane,
@@ -1203,9 +1239,32 @@ ChanTable SpectralPlan::chan_table(const int* off, const ChanEntry* ent, int nch
 }
 
 size_t SpectralPlan::dict_smem_bytes() const {
-  const size_t b = (size_t)nterms_dict_ * sizeof(DictTerm) + (size_t)nfac_dict_ * sizeof(DictFactor) +
-                   (size_t)(2 * n + 1) * sizeof(int);
+  const size_t b = (size_t)(poly_nf_ ? n * poly_count_ : 0) * sizeof(double) + (size_t)nterms_dict_ * sizeof(DictTerm) +
+                   (size_t)nfac_dict_ * sizeof(DictFactor) + (size_t)(2 * n + 1) * sizeof(int);
   return (b + 15) / 16 * 16;
+}
+
+std::vector<double> SpectralPlan::poly_table() const {
+  std::vector<double> A((size_t)n * poly_count_, 0.0);
+  for (size_t t = 0; t < h_dterms_.size(); ++t) A[(size_t)h_dterms_[t].field * poly_count_ + h_poly_mono_[t]] += h_dterms_[t].C;
+  return A;
+}
+
+// Exponent vectors (up to 3 variables) of the Mono<nf> monomials.
+static std::vector<std::array<int, 3>> mono_exponents(int nf) {
+  std::vector<std::array<int, 3>> ex;
+  auto build = [&](auto mn) {
+    using MN = decltype(mn);
+    ex.assign(MN::count, {0, 0, 0});
+    for (int m = 1; m < MN::count; ++m) {
+      ex[m] = ex[MN::parent(m)];
+      ex[m][MN::var(m)] += 1;
+    }
+  };
+  if (nf == 1) build(Mono<1>{});
+  if (nf == 2) build(Mono<2>{});
+  if (nf == 3) build(Mono<3>{});
+  return ex;
 }
 
 DictTable SpectralPlan::dict_table() const {
@@ -1217,6 +1276,9 @@ DictTable SpectralPlan::dict_table() const {
   d.field_begin = d_field_begin_;
   d.fold = d_fold_;
   d.nfac = nfac_dict_;
+  d.poly = d_poly_;
+  d.poly_nf = poly_nf_;
+  d.poly_count = poly_count_;
   return d;
 }
 
@@ -1427,6 +1489,39 @@ bool SpectralPlan::init(int n_, int ndim_, const int* Ns_, const double* Ls_,
   h_ch_off_ = ch_off;
   h_ch_ent_ = ch_ent;
   h_dterms_ = dterms;
+  // dense polynomial form: every term a product of fields (no derivative quantity), total
+  // degree <= 3, at most 3 fields
+  poly_nf_ = 0;
+  poly_count_ = 0;
+  h_poly_mono_.clear();
+  if (n <= 3 && !dterms.empty()) {
+    const auto ex = mono_exponents(n);
+    bool dense = true;
+    std::vector<int> mono(dterms.size(), -1);
+    for (size_t t = 0; t < dterms.size() && dense; ++t) {
+      std::array<int, 3> e{0, 0, 0};
+      for (int f = 0; f < dterms[t].nf; ++f) {
+        const DictFactor& fc = dfac[dterms[t].off + f];
+        if (fc.q >= n || fc.eta <= 0) {
+          dense = false;
+          break;
+        }
+        e[fc.q] += fc.eta;
+      }
+      if (!dense || e[0] + e[1] + e[2] > 3) {
+        dense = false;
+        break;
+      }
+      for (size_t m = 0; m < ex.size(); ++m)
+        if (ex[m] == e) mono[t] = (int)m;
+      dense = mono[t] >= 0;
+    }
+    if (dense) {
+      poly_nf_ = n;
+      poly_count_ = (int)ex.size();
+      h_poly_mono_ = mono;
+    }
+  }
   inv_n_ = invN;
 
   // Y-mode channels: every block k, real and imaginary part
@@ -1477,6 +1572,7 @@ bool SpectralPlan::init(int n_, int ndim_, const int* Ns_, const double* Ls_,
   if (nch >= 1 && nch <= 4 && n <= 4) chk(upload_vec(&ch_sorted_, sorted_entries(ch_ent, ch_off, nch)));
   chk(upload_vec(&d_terms_, dterms));
   chk(upload_vec(&d_fac_, dfac));
+  if (poly_nf_) chk(upload_vec(&d_poly_, poly_table()));
   chk(upload_vec(&d_field_begin_, field_begin));
   chk(upload_vec(&d_fold_, fold_ch));
   chk(upload_vec(&ych_off_, y_off));
@@ -1615,7 +1711,7 @@ cudaError_t SpectralPlan::ensure_channel_capacity(int rows) {
 void SpectralPlan::release() {
   if (ch_sorted_ && !arena_) cudaFree(ch_sorted_);
   ch_sorted_ = nullptr;
-  void* ptrs[] = {tw_x_, tw_ax_[0], tw_ax_[1], tw_ax_[2], kv_, ch_off_, ch_ent_, d_terms_, d_fac_,
+  void* ptrs[] = {tw_x_, tw_ax_[0], tw_ax_[1], tw_ax_[2], kv_, ch_off_, ch_ent_, d_terms_, d_fac_, d_poly_,
                   d_field_begin_, d_fold_, ych_off_, ych_ent_, ych_dst_, Sf_, Sc_, lin_ent_, sinv_, cosv_};
   if (!arena_)  // arena memory belongs to the caller
     for (void* p : ptrs)
@@ -1627,6 +1723,7 @@ void SpectralPlan::release() {
   ch_ent_ = nullptr;
   d_terms_ = nullptr;
   d_fac_ = nullptr;
+  d_poly_ = nullptr;
   d_field_begin_ = nullptr;
   d_fold_ = nullptr;
   ych_off_ = nullptr;
@@ -2141,6 +2238,10 @@ cudaError_t SpectralPlan::set_coefficients(const std::vector<double>& C) {
   if (!dt.empty()) RDCU_TRY(cudaMemcpy(d_terms_, dt.data(), dt.size() * sizeof(DictTerm), cudaMemcpyHostToDevice));
   h_ch_ent_ = ent;
   h_dterms_ = dt;
+  if (poly_nf_) {
+    const std::vector<double> A = poly_table();
+    RDCU_TRY(cudaMemcpy(d_poly_, A.data(), A.size() * sizeof(double), cudaMemcpyHostToDevice));
+  }
   return cudaSuccess;
 }
 

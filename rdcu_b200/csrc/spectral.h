@@ -108,6 +108,9 @@ class SpectralPlan {
   DictFactor* d_fac_ = nullptr;
   int* d_field_begin_ = nullptr;
   int* d_fold_ = nullptr;
+  double* d_poly_ = nullptr;        // dense polynomial form of the dictionary (DictTable.poly)
+  int poly_nf_ = 0, poly_count_ = 0;
+  std::vector<int> h_poly_mono_;    // monomial of each dictionary term (dense form)
   int nterms_dict_ = 0;
   int nfac_dict_ = 0;
   int kv_total_ = 0;
@@ -150,6 +153,7 @@ class SpectralPlan {
   cudaError_t launch_forward(const double* y, cudaStream_t stream);
   bool geometry(std::string* msg);
   cudaError_t ensure_channel_capacity(int rows);
+  std::vector<double> poly_table() const;  // dense coefficients from h_dterms_
 };
 
 // One problem of a batch: a 2D plan and its DP45 state.
