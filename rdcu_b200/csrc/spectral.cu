@@ -1058,6 +1058,36 @@ __device__ __forceinline__ void load_args(A* dst, const A* src) {
   for (int w = threadIdx.x; w < (int)(sizeof(A) / 8); w += blockDim.x) d[w] = s[w];
 }
 
+// Runs f(radix set, length) for a work item: the body specialised to the member's line
+// length L when it is a power of two of 64..512 (the switch is uniform across the CTA),
+// the general body otherwise.
+template <int RS, typename F>
+__device__ __forceinline__ void by_member_length(int L, F&& f) {
+  using RP = std::integral_constant<int, kRadixPow2>;
+  switch (L) {
+    case 64: f(RP{}, std::integral_constant<int, 64>{}); break;
+    case 128: f(RP{}, std::integral_constant<int, 128>{}); break;
+    case 256: f(RP{}, std::integral_constant<int, 256>{}); break;
+    case 512: f(RP{}, std::integral_constant<int, 512>{}); break;
+    default: f(std::integral_constant<int, RS>{}, std::integral_constant<int, 0>{}); break;
+  }
+}
+
+// Work-item bodies as called functions: each length variant keeps its own register
+// allocation (inlined into one kernel, the union of the variants spills).
+template <int RS, int LX>
+__device__ __noinline__ void fwd_x_item(const FwdXArgs& a, int bx) {
+  fwd_x_body<RS, LX>(a, bx);
+}
+template <int RS, int LX>
+__device__ __noinline__ void mid_item(const MidArgs& a, int bx) {
+  mid_body<RS, LX>(a, bx);
+}
+template <int RS, int LX>
+__device__ __noinline__ void inv_x_item(const InvXArgs& a, int bx) {
+  inv_x_body<RS, LX>(a, bx);
+}
+
 template <int RS>
 __global__ void __launch_bounds__(kMaxBlock, 1)
     k_fwd_x_batch(const FwdXArgs* __restrict__ args, const int2* __restrict__ items, int nitems) {
@@ -1066,7 +1096,7 @@ __global__ void __launch_bounds__(kMaxBlock, 1)
     const int2 w = items[it];
     load_args(&sa, args + w.x);
     __syncthreads();
-    fwd_x_body<RS, 0>(sa, w.y);
+    by_member_length<RS>(sa.M, [&](auto rs, auto lx) { fwd_x_item<decltype(rs)::value, decltype(lx)::value>(sa, w.y); });
     __syncthreads();
   }
 }
@@ -1079,7 +1109,7 @@ __global__ void __launch_bounds__(kMaxBlock, 1)
     const int2 w = items[it];
     load_args(&sa, args + w.x);
     __syncthreads();
-    mid_body<RS, 0>(sa, w.y);
+    by_member_length<RS>(sa.L0, [&](auto rs, auto lx) { mid_item<decltype(rs)::value, decltype(lx)::value>(sa, w.y); });
     __syncthreads();
   }
 }
@@ -1092,7 +1122,7 @@ __global__ void __launch_bounds__(kMaxBlock, 1)
     const int2 w = items[it];
     load_args(&sa, args + w.x);
     __syncthreads();
-    inv_x_body<RS, 0>(sa, w.y);
+    by_member_length<RS>(sa.M, [&](auto rs, auto lx) { inv_x_item<decltype(rs)::value, decltype(lx)::value>(sa, w.y); });
     __syncthreads();
   }
 }
