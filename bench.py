@@ -148,6 +148,15 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------------------- our arm
+# DRAM bytes (read + write) per launch of each pass of DP45 stage 4 on the 3D CGLE, from
+# one ncu capture (`ncu --set full ... python -m rdcu_b200.profile_case 256,256,128`,
+# 8.39 M grid points); traffic grows with the grid points, so the full-size workload's
+# figure is this one scaled by its points.
+NCU_POINTS = 256 * 256 * 128
+NCU_TRAFFIC_3D = {"fwd_x": 772.5e6, "c2c_axis1_fwd": 218.7e6, "mid_axis0": 234.5e6, "c2c_axis1_inv": 218.7e6,
+                  "inv_x_dictionary": 374.7e6}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
 
@@ -260,7 +269,10 @@ def run_ours(args, rank, world, local_rank):
         "e2e": {"value": e2e_value, "unit": "grid-pt·steps/s", "h2d_bytes_per_step": nN * 8 / args.steps,
                 "d2h_bytes_per_step": 2 * nN * 8 / args.steps, "accepted_steps": acc2, "seconds": e2e_s},
         "roofline": {"bound": "hbm", "kernel": top[0], "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": (NCU_TRAFFIC_3D[top[0]] * N / NCU_POINTS) if len(Ns) == 3 else None,
+                     "traffic_note": "ncu DRAM bytes of the 256x256x128 capture scaled by grid points"
+                                     if len(Ns) == 3 else "no capture for 1D/2D",
                      "algorithmic_bytes_per_launch": top[2], "launch_ms": top[1],
                      "passes": [{"name": p[0], "ms": p[1], "GBps": p[2] / (p[1] / 1e3) / 1e9,
                                  "share": p[1] / total_ms} for p in passes],
