@@ -290,6 +290,80 @@ __device__ __forceinline__ void fwd_load(const FwdXArgs& a, const Resolved& r, d
   }
 }
 
+// stage_value_t for the two consecutive points i, i+1 (i even) with 16-byte loads; the
+// same arithmetic per component.
+template <int S>
+__device__ __forceinline__ double2 stage_value_t2(long long i, const Resolved& r) {
+  const double2 yi = *reinterpret_cast<const double2*>(r.y + i);
+  if (S <= 1) return yi;
+  if (S == 2) {
+    const double2 k0 = *reinterpret_cast<const double2*>(r.k[0] + i);
+    return make_double2(yi.x + r.h * c_a[2][0] * k0.x, yi.y + r.h * c_a[2][0] * k0.y);
+  }
+  const double2 k0 = *reinterpret_cast<const double2*>(r.k[0] + i);
+  double ax = c_a[S][0] * k0.x, ay = c_a[S][0] * k0.y;
+  if (S != 7) {
+    const double2 k1 = *reinterpret_cast<const double2*>(r.k[1] + i);
+    ax += c_a[S][1] * k1.x;
+    ay += c_a[S][1] * k1.y;
+  }
+#pragma unroll
+  for (int j = 2; j < S - 1; ++j) {
+    const double2 kj = *reinterpret_cast<const double2*>(r.k[j] + i);
+    ax += c_a[S][j] * kj.x;
+    ay += c_a[S][j] * kj.y;
+  }
+  return make_double2(yi.x + r.h * ax, yi.y + r.h * ay);
+}
+
+// fwd_load for a compile-time power-of-two row length: each thread moves pairs of
+// consecutive points (16-byte loads and stores of the state arrays).
+template <int S, int LX>
+__device__ __forceinline__ void fwd_load2(const FwdXArgs& a, const Resolved& r, double2* buf, long long row0) {
+  static_assert(LX % 2 == 0, "even compile-time row length");
+  if constexpr (LX > 0) {
+  constexpr int kUnroll = 4, H = LX / 2;
+  const int T = blockDim.x, tid = threadIdx.x;
+  const int npair = a.P * LX;  // P line pairs of two rows, LX/2 point pairs per row
+  for (int e0 = tid; e0 < npair; e0 += T * kUnroll) {
+    double2 v[kUnroll];
+    long long gi[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const int e = e0 + u * T;
+      gi[u] = -1;
+      v[u] = make_double2(0.0, 0.0);
+      if (e < npair) {
+        const int pl = (unsigned)e / LX;
+        const int w = e - pl * LX;
+        const int half = (unsigned)w / H;
+        const int x = (w - half * H) * 2;
+        const long long g = row0 + 2 * pl + half;
+        if (g < a.nrows) {
+          gi[u] = g * LX + x;
+          v[u] = stage_value_t2<S>(gi[u], r);
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const int e = e0 + u * T;
+      if (e >= npair) break;
+      if (r.ytemp && gi[u] >= 0) *reinterpret_cast<double2*>(r.ytemp + gi[u]) = v[u];
+      if (a.do_fft) {
+        const int pl = (unsigned)e / LX;
+        const int w = e - pl * LX;
+        const int half = (unsigned)w / H;
+        const int x = (w - half * H) * 2;
+        double* b = reinterpret_cast<double*>(buf) + 2 * (pl * LX + x) + half;
+        b[0] = v[u].x;
+        b[2] = v[u].y;
+      }
+    }
+  }
+  }
+}
+
 // bx: the CTA's index within this plan's grid (blockIdx.x, or a work item of a batch)
 template <int RS, int LX>
 __device__ __forceinline__ void fwd_x_body(const FwdXArgs& a, int bx) {
@@ -306,14 +380,29 @@ __device__ __forceinline__ void fwd_x_body(const FwdXArgs& a, int bx) {
     buf = sm + M;
   }
   const long long row0 = 2LL * bx * a.P;
-  switch (r.stage) {
-    case 2: fwd_load<2, LX>(a, r, buf, row0); break;
-    case 3: fwd_load<3, LX>(a, r, buf, row0); break;
-    case 4: fwd_load<4, LX>(a, r, buf, row0); break;
-    case 5: fwd_load<5, LX>(a, r, buf, row0); break;
-    case 6: fwd_load<6, LX>(a, r, buf, row0); break;
-    case 7: fwd_load<7, LX>(a, r, buf, row0); break;
-    default: fwd_load<1, LX>(a, r, buf, row0); break;
+  // 16-byte state loads need 16-byte aligned arrays (a caller's y may be offset)
+  unsigned long long align = reinterpret_cast<unsigned long long>(r.y) | reinterpret_cast<unsigned long long>(r.ytemp);
+  for (int j = 0; j < 7; ++j) align |= reinterpret_cast<unsigned long long>(r.k[j]);
+  if (LX > 0 && (align & 15) == 0) {
+    switch (r.stage) {
+      case 2: fwd_load2<2, LX>(a, r, buf, row0); break;
+      case 3: fwd_load2<3, LX>(a, r, buf, row0); break;
+      case 4: fwd_load2<4, LX>(a, r, buf, row0); break;
+      case 5: fwd_load2<5, LX>(a, r, buf, row0); break;
+      case 6: fwd_load2<6, LX>(a, r, buf, row0); break;
+      case 7: fwd_load2<7, LX>(a, r, buf, row0); break;
+      default: fwd_load2<1, LX>(a, r, buf, row0); break;
+    }
+  } else {
+    switch (r.stage) {
+      case 2: fwd_load<2, LX>(a, r, buf, row0); break;
+      case 3: fwd_load<3, LX>(a, r, buf, row0); break;
+      case 4: fwd_load<4, LX>(a, r, buf, row0); break;
+      case 5: fwd_load<5, LX>(a, r, buf, row0); break;
+      case 6: fwd_load<6, LX>(a, r, buf, row0); break;
+      case 7: fwd_load<7, LX>(a, r, buf, row0); break;
+      default: fwd_load<1, LX>(a, r, buf, row0); break;
+    }
   }
   if (!a.do_fft) return;
   __syncthreads();
