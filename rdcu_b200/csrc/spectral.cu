@@ -907,8 +907,9 @@ __device__ __forceinline__ void inv_x_body(const InvXArgs& a, int bx) {
     for (int t = tid; t < n; t += T) sfold[t] = a.dict.fold[t];
   }
   if (!a.Yout) {
-    // physical fields of the P rows: asynchronous copies, 16 bytes where rows allow
-    if ((M & 1) == 0) {
+    // physical fields of the P rows: asynchronous 16-byte copies where rows and the
+    // array's alignment allow (a caller's y may be only 8-byte aligned)
+    if ((M & 1) == 0 && (reinterpret_cast<unsigned long long>(r.u) & 15) == 0) {
       const int half = M / 2;
       const int nph = P * n * half;
       for (int e = tid; e < nph; e += T) {

@@ -110,3 +110,55 @@ def test_plane_wave_laplacian_large(cuda, Ns):
     f, _ = gpu_rhs(cuda, prob, u.ravel())
     expect = -sum(k * k for k in ks) * u.ravel()
     assert rel_err(f, expect) < 1e-11
+
+
+def test_misaligned_device_input(cuda):
+    """A caller's state array that is only 8-byte aligned (an offset view) takes the
+    scalar load path of the length-specialised kernels: same values as an aligned one."""
+    import rdcu_b200 as R
+
+    rng = np.random.default_rng(31)
+    prob = Problem(2, (64, 128), (80.0, 160.0), cgle_terms(2))
+    y = rng.uniform(-1, 1, 2 * prob.N)
+    s = R.Solver(prob.n, prob.Ns, prob.Ls, spec_terms(prob))
+    big = cuda.zeros(2 * prob.N + 1, dtype=cuda.float64, device="cuda")
+    big[1:] = cuda.tensor(y, dtype=cuda.float64, device="cuda")
+    ya = cuda.tensor(y, dtype=cuda.float64, device="cuda")
+    assert big[1:].data_ptr() % 16 == 8
+    f1, f2 = cuda.empty_like(ya), cuda.empty_like(ya)
+    cuda.cuda.synchronize()
+    s.rhs(big[1:].data_ptr(), f1.data_ptr())
+    s.rhs(ya.data_ptr(), f2.data_ptr())
+    assert cuda.equal(f1, f2)
+    assert rel_err(f1.cpu().numpy(), osp.rhs(y, prob)) < TOL
+    s.close()
+
+
+@pytest.mark.parametrize("Ns", [(64, 512), (512, 64), (128, 256), (64, 128, 256), (256, 64, 64)])
+def test_length_specialised_kernels(cuda, Ns):
+    """Line lengths 64..512 run kernels compiled for their length (every pass)."""
+    rng = np.random.default_rng(sum(Ns))
+    prob = Problem(2, Ns, tuple(0.78 * N for N in Ns), cgle_terms(len(Ns)))
+    y = rng.uniform(-1, 1, 2 * prob.N)
+    f, _ = gpu_rhs(cuda, prob, y)
+    assert rel_err(f, osp.rhs(y, prob)) < TOL
+
+
+@pytest.mark.parametrize("case", ["dense3", "degree4", "derivative_product"])
+def test_dictionary_forms(cuda, case):
+    """Dense polynomial form (3 fields, degree <= 3) and the term list (degree 4; a
+    product with a derivative block) against the oracle."""
+    rng = np.random.default_rng(7)
+    if case == "dense3":
+        lines = ["0.5,0", "1.0,0,0,1,1,1,2,1", "-0.7,1,1,3", "0.3,2,0,2,2,1", "1.1,2,1,1", "0.2,0,3,1",
+                 "-0.4,1,2,1"]
+        prob = Problem(3, (32, 24), (20.0, 15.0), [parse_term(l) for l in lines])
+    elif case == "degree4":
+        lines = ["1.0,0,0,4", "-0.5,1,0,2,1,2", "0.25,0,1,1", "0.3,1,6,1"]
+        prob = Problem(2, (64, 32), (30.0, 20.0), [parse_term(l) for l in lines])
+    else:
+        lines = ["1.0,0,0,1,2,1", "-0.5,1,1,2,5,1", "0.25,0,6,1", "0.3,1,13,1"]
+        prob = Problem(2, (64, 32), (30.0, 20.0), [parse_term(l) for l in lines])
+    y = rng.uniform(-1, 1, prob.n * prob.N)
+    f, _ = gpu_rhs(cuda, prob, y)
+    assert rel_err(f, osp.rhs(y, prob)) < TOL
