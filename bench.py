@@ -66,6 +66,8 @@ WORKLOADS = {
     "cgle2d_128": dict(Ns=(128, 128), Ls=(100.0, 100.0), seed=1, h0=1e-3),
     # 512 independent 2D CGLE problems of uneven size, stepped as one ensemble (see run_ensemble)
     "ensemble_cgle2d_512": dict(members=512, sizes=(64, 96, 128, 192, 256), seed=3, h0=1e-3, tau=0.1),
+    # stiff path: 2D Brusselator, 5-point finite differences, variable-order BDF (see run_bdf)
+    "bdf_brusselator_256": dict(Ns=(256, 256), Ls=(64.0, 64.0), seed=3, h0=1e-3, tau=1.0),
     # discrete adjoint: gradient of a terminal mismatch over 5000 fixed steps (see run_adjoint)
     "adjoint_cgle2d_256": dict(Ns=(256, 256), Ls=(200.0, 200.0), seed=1, h=1e-3, T=5.0, K=50),
 }
@@ -391,6 +393,66 @@ def run_adjoint(args):
     }
 
 
+def run_bdf(args):
+    """Stiff workload: 2D Brusselator u_t = 1 - 4u + u^2 v + lap u, v_t = 3u - u^2 v + 8 lap v
+    on 256^2, L = 64, periodic 5-point finite differences, variable-order BDF at rtol = atol
+    = 1e-6; initial state (1, 3) + U[-0.1, 0.1] from glibc rand() seed 3.  Warm-up
+    [0, W tau], timed [W tau, (W+K) tau] (tau = 1); value = grid points x accepted steps /
+    device seconds.  The linear solves are FFT-preconditioned GMRES (the reference's
+    cuDSS is not available)."""
+    import torch
+
+    import rdcu_b200 as R
+    from rdcu_b200.problems import brusselator_coupling_lines
+
+    wl = WORKLOADS[args.workload]
+    Ns, Ls = wl["Ns"], wl["Ls"]
+    N = int(np.prod(Ns))
+    nN = 2 * N
+    terms = parse_terms(brusselator_coupling_lines())
+    s = R.Solver(2, Ns, Ls, terms, method=R.METHOD_BDF, rtol=1e-6, atol=1e-6)
+    y0 = R.random_ic(2, N, 0.2, 0.0, wl["seed"])
+    y0[:N] += 1.0
+    y0[N:] += 3.0
+    T_A, T_B = args.warmup * wl["tau"], (args.warmup + args.steps) * wl["tau"]
+    s.set_state(0.0, wl["h0"], y0.ctypes.data)
+    s.solve(T_A, [])
+    yA = np.empty(nN)
+    D = np.empty(nN * 8)
+    tA, hA, oA = s.get_state(yA.ctypes.data, D.ctypes.data)
+    stream = torch.cuda.ExternalStream(s.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    with ClockSampler(0) as clk:
+        e0.record(stream)
+        s.solve(T_B, [])
+        e1.record(stream)
+        e1.synchronize()
+    sec = e0.elapsed_time(e1) / 1e3
+    acc, att = s.counters()
+    # e2e: the same window from host arrays through the C ABI, final state to the host
+    w0 = time.perf_counter()
+    s.set_state(tA, hA, yA.ctypes.data, oA, D.ctypes.data)
+    s.solve(T_B, [])
+    out = np.empty(nN)
+    s.get_state(out.ctypes.data)
+    e2e_s = time.perf_counter() - w0
+    acc2, _ = s.counters()
+    s.close()
+    return {
+        "metric": METRIC, "value": N * acc / sec, "unit": "grid-pt·steps/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": sec * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "grid": list(Ns), "L": list(Ls), "method": "BDF (NDF orders 1-5), FD",
+                   "rtol": 1e-6, "atol": 1e-6, "window_sim_time": [T_A, T_B], "accepted_steps": acc,
+                   "attempts": att, "linear_solver": "GMRES(40), FFT preconditioner",
+                   "l2": "state 1 MB: L2-resident (latency-bound regime)"},
+        "clocks": clk.summary(),
+        "e2e": {"value": N * acc2 / e2e_s, "unit": "grid-pt·steps/s", "h2d_bytes_per_step": 9 * nN * 8 / args.steps,
+                "d2h_bytes_per_step": nN * 8 / args.steps, "seconds": e2e_s},
+    }
+
+
 def ensemble_members(wl):
     """Members of the ensemble workload: grid N x N with N drawn uniformly from the sizes,
     L = 0.78 N, CGLE b ~ U[0.5, 3], c ~ U[-2, 0] (numpy seed wl["seed"]); initial states
@@ -552,6 +614,9 @@ def reference_binary():
 def run_reference(args):
     if args.workload.startswith("adjoint"):
         return {"impl": "reference", "unavailable": "the reference computes no gradients (no adjoint to time)"}
+    if args.workload.startswith("bdf"):
+        return {"impl": "reference", "unavailable": "the reference's BDF path needs cuDSS, which is not installed "
+                "in this image (no cudss.h or libcudss)"}
     if args.workload.startswith("ensemble"):
         return {"impl": "reference", "unavailable": "the reference has no ensemble; its one-problem-per-process "
                 "rate is the cgle2d workloads' reference arm, and the instance-by-instance baseline of this "
@@ -629,6 +694,8 @@ def main():
         line = run_adjoint(args) if rank == 0 else None
     elif args.workload.startswith("ensemble"):
         line = run_ensemble(args) if rank == 0 else None
+    elif args.workload.startswith("bdf"):
+        line = run_bdf(args) if rank == 0 else None
     else:
         line = run_ours(args, rank, world, local_rank)
     if world > 1:
