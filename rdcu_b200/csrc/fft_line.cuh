@@ -243,4 +243,25 @@ __device__ __forceinline__ void fft_pow2_t(double2* buf, int LS, int nlines, con
   }
 }
 
+// Radix of the next stage when `rem` points of the line remain to be factored, in
+// make_line_plan's order (all 8s, then 4s, 2s, 3s, 5s, 7s, 11s, 13s).
+__host__ __device__ constexpr int plan_radix(int rem) {
+  return rem % 8 == 0 ? 8 : rem % 4 == 0 ? 4 : rem % 2 == 0 ? 2 : rem % 3 == 0 ? 3 : rem % 5 == 0 ? 5
+         : rem % 7 == 0 ? 7 : rem % 11 == 0 ? 11 : 13;
+}
+
+// The transform for any supported length L known at compile time (the plan's stage
+// sequence, constant spans and divisors; bitwise equal to fft_lines on that plan).  A
+// radix-8 first stage writes swizzled for the stage after it; twiddles are read plainly.
+template <int L, bool INV, int NS = 1>
+__device__ __forceinline__ void fft_fixed_t(double2* buf, int LS, int nlines, const double2* tw) {
+  if constexpr (NS < L) {
+    constexpr int R = plan_radix(L / NS);
+    constexpr int R0 = plan_radix(L);
+    constexpr int SWZ = (NS == 1 && R == 8 && L > 8) ? 1 : (NS == 8 && R0 == 8 ? 2 : 0);
+    stockham_stage<R, INV, false, SWZ>(buf, LS, nlines, L, NS, make_fastdiv_c(L / R), make_fastdiv_c(NS), tw);
+    fft_fixed_t<L, INV, NS * R>(buf, LS, nlines, tw);
+  }
+}
+
 }  // namespace rdcu

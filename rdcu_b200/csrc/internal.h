@@ -31,6 +31,13 @@ inline FastDiv make_fastdiv(unsigned d) {
   f.s = s;
   return f;
 }
+// make_fastdiv for a divisor known at compile time
+__host__ __device__ constexpr FastDiv make_fastdiv_c(unsigned d) {
+  int s = 0;
+  while ((1ull << s) < d) ++s;
+  const unsigned long long num = 1ull << (31 + s);
+  return FastDiv{(unsigned)((num + d - 1) / d), s};
+}
 #ifdef __CUDACC__
 __device__ __forceinline__ int fdiv(int n, FastDiv f) {
   return (int)(((unsigned long long)(unsigned)n * f.m) >> (31 + f.s));

@@ -219,8 +219,10 @@ __device__ __forceinline__ int fdivc(int n, FastDiv f) {
 template <int RS, int LX, bool INV>
 __device__ __forceinline__ void fft_lines_x(double2* buf, int LS, int nlines, const LinePlan& p, const double2* tw,
                                             bool twz) {
-  if constexpr (LX > 0)
+  if constexpr (LX > 0 && (LX & (LX - 1)) == 0)
     fft_pow2_t<LX, INV>(buf, LS, nlines, tw, twz);
+  else if constexpr (LX > 0)
+    fft_fixed_t<LX, INV>(buf, LS, nlines, tw);
   else
     fft_lines<RS, INV>(buf, LS, nlines, p, tw);
 }
@@ -229,8 +231,9 @@ __device__ __forceinline__ void fft_lines_x(double2* buf, int LS, int nlines, co
 // power-of-two length store it swizzled (see fft_pow2_t).  Returns whether it did.
 template <int LX>
 __device__ __forceinline__ bool stage_twiddles(double2* dst, const double2* src, int L) {
-  for (int t = threadIdx.x; t < L; t += blockDim.x) dst[LX > 0 ? swz8(t) : t] = src[t];
-  return LX > 0;
+  constexpr bool swz = LX > 0 && (LX & (LX - 1)) == 0;
+  for (int t = threadIdx.x; t < L; t += blockDim.x) dst[swz ? swz8(t) : t] = src[t];
+  return swz;
 }
 
 // Stage state with the stage number known at compile time (slopes in registers).
@@ -1149,8 +1152,8 @@ __device__ __forceinline__ void load_args(A* dst, const A* src) {
 }
 
 // Runs f(radix set, length) for a work item: the body specialised to the member's line
-// length L when it is a power of two of 64..512 (the switch is uniform across the CTA),
-// the general body otherwise.
+// length L when it is one of the specialised lengths (the switch is uniform across the
+// CTA), the general body otherwise.
 template <int RS, typename F>
 __device__ __forceinline__ void by_member_length(int L, F&& f) {
   using RP = std::integral_constant<int, kRadixPow2>;
@@ -1159,6 +1162,8 @@ __device__ __forceinline__ void by_member_length(int L, F&& f) {
     case 128: f(RP{}, std::integral_constant<int, 128>{}); break;
     case 256: f(RP{}, std::integral_constant<int, 256>{}); break;
     case 512: f(RP{}, std::integral_constant<int, 512>{}); break;
+    case 96: f(std::integral_constant<int, kRadixAll>{}, std::integral_constant<int, 96>{}); break;
+    case 192: f(std::integral_constant<int, kRadixAll>{}, std::integral_constant<int, 192>{}); break;
     default: f(std::integral_constant<int, RS>{}, std::integral_constant<int, 0>{}); break;
   }
 }
@@ -1324,22 +1329,26 @@ static void inv_geometry(int M, int R, int n, int nch_run, bool yout, const Line
 }
 
 // Calls f(radix set, line length) with compile-time values for the plan's lengths:
-// power-of-two lines of 64..512 points get kernels specialised to their length, other
-// power-of-two lines the shift-indexed kernels, every other length the general ones.
+// lines of 64..512 points (powers of two, and 96 and 192) get kernels specialised to
+// their length, other power-of-two lines the shift-indexed kernels, every other length
+// the general ones.
 template <typename F>
 static void by_length(const LinePlan& p, int block, F&& f) {
   using RP = std::integral_constant<int, kRadixPow2>;
-  if (!plan_is_pow2(p)) {
-    f(std::integral_constant<int, kRadixAll>{}, std::integral_constant<int, 0>{});
-    return;
-  }
+  using RA = std::integral_constant<int, kRadixAll>;
   switch (block <= kSpecBlock ? p.L : 0) {
     case 64: f(RP{}, std::integral_constant<int, 64>{}); return;
     case 128: f(RP{}, std::integral_constant<int, 128>{}); return;
     case 256: f(RP{}, std::integral_constant<int, 256>{}); return;
     case 512: f(RP{}, std::integral_constant<int, 512>{}); return;
-    default: f(RP{}, std::integral_constant<int, 0>{}); return;
+    case 96: f(RA{}, std::integral_constant<int, 96>{}); return;
+    case 192: f(RA{}, std::integral_constant<int, 192>{}); return;
+    default: break;
   }
+  if (plan_is_pow2(p))
+    f(RP{}, std::integral_constant<int, 0>{});
+  else
+    f(RA{}, std::integral_constant<int, 0>{});
 }
 
 // ----------------------------------------------------------------------------- plan

@@ -21,7 +21,8 @@ def _cgle(b, c):
 def _members(rng):
     out = []
     for k, (Ns, b, c) in enumerate([((16, 16), 2.0, 0.8), ((24, 20), 1.0, -0.5), ((32, 32), 2.5, -1.5),
-                                    ((20, 15), 0.7, 0.3), ((64, 48), 1.5, -1.0), ((48, 64), 3.0, -2.0)]):
+                                    ((20, 15), 0.7, 0.3), ((64, 48), 1.5, -1.0), ((48, 64), 3.0, -2.0),
+                                    ((96, 192), 1.2, -0.6)]):
         out.append(dict(n=2, Ns=Ns, Ls=(0.78 * Ns[0], 0.78 * Ns[1]), terms=_cgle(b, c),
                         rtol=1e-8 if k % 2 else 1e-9, atol=1e-8 if k % 2 else 1e-9))
     # products of derivative blocks (n = 2, Y index = block * 2 + field: u0_x = 2,
@@ -75,7 +76,7 @@ def test_members_match_single_handles_bitwise(cuda):
     rng = np.random.default_rng(1)
     members = _members(rng)
     ys = _ics(members, 2)
-    t0s = [0.0, 0.0, 0.1, 0.0, 0.05, 0.0, 0.0]
+    t0s = [0.0, 0.0, 0.1, 0.0, 0.05, 0.0, 0.0, 0.0]
     ens = R.Ensemble(members)
     got = _run_ensemble(cuda, ens, members, ys, t0s, 1e-3, 2.0)
     for i, m in enumerate(members):

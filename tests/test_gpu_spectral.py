@@ -134,9 +134,10 @@ def test_misaligned_device_input(cuda):
     s.close()
 
 
-@pytest.mark.parametrize("Ns", [(64, 512), (512, 64), (128, 256), (64, 128, 256), (256, 64, 64)])
+@pytest.mark.parametrize("Ns", [(64, 512), (512, 64), (128, 256), (64, 128, 256), (256, 64, 64), (96, 192), (192, 96),
+                                (96, 64, 192)])
 def test_length_specialised_kernels(cuda, Ns):
-    """Line lengths 64..512 run kernels compiled for their length (every pass)."""
+    """Line lengths 64..512 (powers of two, 96, 192) run kernels compiled for their length."""
     rng = np.random.default_rng(sum(Ns))
     prob = Problem(2, Ns, tuple(0.78 * N for N in Ns), cgle_terms(len(Ns)))
     y = rng.uniform(-1, 1, 2 * prob.N)
