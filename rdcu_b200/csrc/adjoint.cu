@@ -90,6 +90,19 @@ struct Coef7 {
   double c[7];
 };
 
+struct CombineArgs {
+  int n, nfold, nq, final_stage;
+  long long N, nN;
+  const AdjFold* folds;
+  const AdjQ* qs;
+  const double* ubar;
+  const double* G;   // transposed-operator outputs (ng channels)
+  const double* u;   // stage state
+  double* Yb;        // out: Ybar_i (n fields); stage 1: not stored
+  double* lam;       // stage 1: lambda += sum_i Ybar_i
+  double* part;
+};
+
 struct PointwiseArgs {
   int n, nq, nkept, nfac, stage;
   long long N, nN;
@@ -112,7 +125,7 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// Shared memory of k_adj_pointwise: per-thread slices [i][thread] of the quantities q,
+// Shared memory of k_adj_stage: per-thread slices [i][thread] of the quantities q,
 // their adjoints qb and kbar (indexed by the dictionary's runtime factor lists, so they
 // live in shared rather than local memory), then per-warp gradient sums [term][warp].
 size_t pointwise_smem(int n, int nq, int nkept, int nfac) {
@@ -120,13 +133,23 @@ size_t pointwise_smem(int n, int nq, int nkept, int nfac) {
          (size_t)nkept * sizeof(AdjTerm) + (size_t)nfac * sizeof(AdjFactor);
 }
 
-// kbar_i = h b_i lambda + h sum_{l > i} a_li Ybar_l (computed per point, stored for the
-// transposed operators), then the monomial VJP: ubar_f = sum_t kbar_field(t) dP_t/du_f,
-// Qbar_q likewise, and per-block partial sums of dL/dC_t = sum_x kbar_field(t) P_t
-// (warp sums, then warps in a fixed order: deterministic).
-__global__ void __launch_bounds__(kThreads) k_adj_pointwise(PointwiseArgs a) {
+// One kernel per stage of the reverse sweep, at every point:
+//  (1) when do_cb: the end of the previous stage's adjoint (the "combine"):
+//      Ybar_i = ubar + sum_folded C_t M_t^T kbar_field(t) + sum_q M_q^T Qbar_q, with partial
+//      sums of dL/dC_t = <M_t^T kbar_field(t), u_src(t)> for the folded terms; at stage 1
+//      the step ends: lambda_n = lambda_{n+1} + sum_{i=1..6} Ybar_i;
+//  (2) when do_pw: this stage's start (the "pointwise" part): kbar_i = h b_i lambda +
+//      h sum_{l > i} a_li Ybar_l (stored for the transposed operators), then the monomial
+//      VJP ubar_f = sum_t kbar_field(t) dP_t/du_f, Qbar_q likewise, and per-block partial
+//      sums of dL/dC_t = sum_x kbar_field(t) P_t.
+// (2) reads the Ybar and lambda that (1) just wrote at the same point (same thread).
+// Partial sums: warp sums, then warps in a fixed order (deterministic).
+__global__ void __launch_bounds__(kThreads) k_adj_stage(PointwiseArgs a, CombineArgs cb, int do_pw, int do_cb) {
   extern __shared__ double psm[];
   constexpr int T = kThreads, NW = kThreads / 32;
+  __shared__ double sgc[kMaxTerms * NW];
+  __shared__ AdjFold sfold[kMaxTerms];
+  __shared__ AdjQ sqs[kMaxQ];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nqt = a.n + a.nq;
   double* sq = psm;
@@ -136,13 +159,41 @@ __global__ void __launch_bounds__(kThreads) k_adj_pointwise(PointwiseArgs a) {
   AdjTerm* sterm = reinterpret_cast<AdjTerm*>(sg + a.nkept * NW);
   AdjFactor* sfac = reinterpret_cast<AdjFactor*>(sterm + a.nkept);
   for (int i = tid; i < a.nkept * NW; i += T) sg[i] = 0.0;
+  for (int i = tid; i < cb.nfold * NW; i += T) sgc[i] = 0.0;
   // the tables are read in every term iteration: stage them next to the slices
   for (int i = tid; i < a.nkept; i += T) sterm[i] = a.terms[i];
   for (int i = tid; i < a.nfac; i += T) sfac[i] = a.fac[i];
+  for (int i = tid; i < cb.nfold; i += T) sfold[i] = cb.folds[i];
+  for (int i = tid; i < cb.nq; i += T) sqs[i] = cb.qs[i];
   __syncthreads();
   for (long long base = (long long)blockIdx.x * T; base < a.N; base += (long long)gridDim.x * T) {
     const long long x = base + tid;
     const bool live = x < a.N;
+    if (do_cb) {
+      if (live) {
+        for (int s = 0; s < cb.n; ++s) {
+          const long long o = (long long)s * cb.N + x;
+          double v = cb.ubar[o];
+          for (int t = 0; t < cb.nfold; ++t)
+            if (sfold[t].src == s) v += sfold[t].C * cb.G[(long long)sfold[t].g * cb.N + x];
+          for (int q = 0; q < cb.nq; ++q)
+            if (sqs[q].src == s) v += cb.G[(long long)sqs[q].g * cb.N + x];
+          if (cb.final_stage) {
+            double l = cb.lam[o] + v;
+            for (int i = 2; i <= 6; ++i) l += cb.Yb[(long long)(i - 1) * cb.nN + o];
+            cb.lam[o] = l;
+          } else {
+            cb.Yb[o] = v;
+          }
+        }
+      }
+      for (int t = 0; t < cb.nfold; ++t) {
+        double g = live ? cb.G[(long long)sfold[t].g * cb.N + x] * cb.u[(long long)sfold[t].src * cb.N + x] : 0.0;
+        g = warp_sum(g);
+        if (lane == 0) sgc[t * NW + warp] += g;
+      }
+    }
+    if (!do_pw) continue;
     if (live) {
       for (int f = 0; f < a.n; ++f) {
         const long long o = (long long)f * a.N + x;
@@ -187,70 +238,19 @@ __global__ void __launch_bounds__(kThreads) k_adj_pointwise(PointwiseArgs a) {
     }
   }
   __syncthreads();
-  for (int t = tid; t < a.nkept; t += T) {
-    double s = 0.0;
-    for (int w = 0; w < NW; ++w) s += sg[t * NW + w];
-    a.part[(long long)sterm[t].orig * gridDim.x + blockIdx.x] += s;
-  }
-}
-
-struct CombineArgs {
-  int n, nfold, nq, final_stage;
-  long long N, nN;
-  const AdjFold* folds;
-  const AdjQ* qs;
-  const double* ubar;
-  const double* G;   // transposed-operator outputs (ng channels)
-  const double* u;   // stage state
-  double* Yb;        // out: Ybar_i (n fields); stage 1: not stored
-  double* lam;       // stage 1: lambda += sum_i Ybar_i
-  double* part;
-};
-
-// Ybar_i = ubar + sum_folded C_t M_t^T kbar_field(t) + sum_q M_q^T Qbar_q; partial sums of
-// dL/dC_t = <M_t^T kbar_field(t), u_src(t)> for the folded terms.  At stage 1 the step
-// ends: lambda_n = lambda_{n+1} + sum_{i=1..6} Ybar_i.
-__global__ void __launch_bounds__(kThreads) k_adj_combine(CombineArgs a) {
-  constexpr int T = kThreads, NW = kThreads / 32;
-  __shared__ double sg[kMaxTerms * NW];
-  __shared__ AdjFold sfold[kMaxTerms];
-  __shared__ AdjQ sqs[kMaxQ];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int i = tid; i < a.nfold * NW; i += T) sg[i] = 0.0;
-  for (int i = tid; i < a.nfold; i += T) sfold[i] = a.folds[i];
-  for (int i = tid; i < a.nq; i += T) sqs[i] = a.qs[i];
-  __syncthreads();
-  for (long long base = (long long)blockIdx.x * T; base < a.N; base += (long long)gridDim.x * T) {
-    const long long x = base + tid;
-    const bool live = x < a.N;
-    if (live) {
-      for (int s = 0; s < a.n; ++s) {
-        const long long o = (long long)s * a.N + x;
-        double v = a.ubar[o];
-        for (int t = 0; t < a.nfold; ++t)
-          if (sfold[t].src == s) v += sfold[t].C * a.G[(long long)sfold[t].g * a.N + x];
-        for (int q = 0; q < a.nq; ++q)
-          if (sqs[q].src == s) v += a.G[(long long)sqs[q].g * a.N + x];
-        if (a.final_stage) {
-          double l = a.lam[o] + v;
-          for (int i = 2; i <= 6; ++i) l += a.Yb[(long long)(i - 1) * a.nN + o];
-          a.lam[o] = l;
-        } else {
-          a.Yb[o] = v;
-        }
-      }
-    }
-    for (int t = 0; t < a.nfold; ++t) {
-      double g = live ? a.G[(long long)sfold[t].g * a.N + x] * a.u[(long long)sfold[t].src * a.N + x] : 0.0;
-      g = warp_sum(g);
-      if (lane == 0) sg[t * NW + warp] += g;
+  if (do_pw) {
+    for (int t = tid; t < a.nkept; t += T) {
+      double s = 0.0;
+      for (int w = 0; w < NW; ++w) s += sg[t * NW + w];
+      a.part[(long long)sterm[t].orig * gridDim.x + blockIdx.x] += s;
     }
   }
-  __syncthreads();
-  for (int t = tid; t < a.nfold; t += T) {
-    double s = 0.0;
-    for (int w = 0; w < NW; ++w) s += sg[t * NW + w];
-    a.part[(long long)sfold[t].orig * gridDim.x + blockIdx.x] += s;
+  if (do_cb) {
+    for (int t = tid; t < cb.nfold; t += T) {
+      double s = 0.0;
+      for (int w = 0; w < NW; ++w) s += sgc[t * NW + w];
+      cb.part[(long long)sfold[t].orig * gridDim.x + blockIdx.x] += s;
+    }
   }
 }
 
@@ -424,7 +424,7 @@ bool AdjointEngine::init(SpectralPlan* fwd, DP45Engine* dp, const std::vector<Ho
   T.nq = nq_;
   pw_smem_ = pointwise_smem(n, nq_, T.nkept, T.nfac);
   if (pw_smem_ > 48 * 1024 &&
-      cudaFuncSetAttribute(k_adj_pointwise, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pw_smem_) != cudaSuccess) {
+      cudaFuncSetAttribute(k_adj_stage, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pw_smem_) != cudaSuccess) {
     *msg = "adjoint set-up: dictionary too large for the pointwise kernel's shared memory";
     return false;
   }
@@ -558,19 +558,32 @@ cudaError_t AdjointEngine::launch_recompute(int j0, int steps) {
   return cudaSuccess;
 }
 
-// Reverse sweep over `steps` recomputed steps (queued; capturable).
+// Reverse sweep over `steps` recomputed steps (queued; capturable).  Each stage's
+// combine runs in the kernel of the next stage's pointwise part; the last one alone.
 cudaError_t AdjointEngine::launch_reverse(int j0, int steps) {
+  bool pending = false;
+  const double* Yprev = nullptr;
+  int sprev = 0;
   for (int j = steps - 1; j >= 0; --j) {
     const double* Ystore = store_ + (size_t)j * 6 * nN_;
     const double h = hs_[j0 + j];
-    for (int i = 6; i >= 1; --i) RDCU_TRY(vjp(Ystore + (size_t)(i - 1) * nN_, i, h));
+    for (int i = 6; i >= 1; --i) {
+      const double* Y = Ystore + (size_t)(i - 1) * nN_;
+      RDCU_TRY(stage_kernels(Y, i, h, pending ? Yprev : nullptr, sprev));
+      pending = true;
+      Yprev = Y;
+      sprev = i;
+    }
   }
+  if (pending) RDCU_TRY(stage_kernels(nullptr, 0, 0.0, Yprev, sprev));
   return cudaSuccess;
 }
 
-cudaError_t AdjointEngine::vjp(const double* Y, int stage, double h) {
+// Launches the combine of stage sprev at state Yprev (if Yprev) fused with the pointwise
+// part of stage `stage` at state Y (if Y), then stage's transposed operators.
+cudaError_t AdjointEngine::stage_kernels(const double* Y, int stage, double h, const double* Yprev, int sprev) {
   Tables& T = *tab_;
-  if (have_q_) RDCU_TRY(planQ_.run_linear(Y, qv_, st_));
+  if (Y && have_q_) RDCU_TRY(planQ_.run_linear(Y, qv_, st_));
   PointwiseArgs pa{};
   pa.n = n_;
   pa.nq = nq_;
@@ -585,32 +598,32 @@ cudaError_t AdjointEngine::vjp(const double* Y, int stage, double h) {
   pa.Q = qv_;
   pa.lam = lam_;
   pa.Yb = Yb_;
-  pa.hb = h * kA[7][stage - 1];
-  for (int l = stage + 1; l <= 6; ++l) pa.ha.c[l] = h * kA[l][stage - 1];
+  pa.hb = Y ? h * kA[7][stage - 1] : 0.0;
+  if (Y)
+    for (int l = stage + 1; l <= 6; ++l) pa.ha.c[l] = h * kA[l][stage - 1];
   pa.w = tin_;
   pa.ubar = ubar_;
   pa.Qbar = tin_ + (size_t)n_ * N_;
   pa.part = part_;
-  k_adj_pointwise<<<kBlocks, kThreads, pw_smem_, st_>>>(pa);
-  RDCU_TRY(cudaGetLastError());
-  if (ng_ > 0) RDCU_TRY(planT_.run_linear(tin_, tout_, st_));
   CombineArgs ca{};
   ca.n = n_;
-  ca.nfold = T.nfold;
-  ca.nq = nq_;
-  ca.final_stage = stage == 1;
+  ca.nfold = Yprev ? T.nfold : 0;
+  ca.nq = Yprev ? nq_ : 0;
+  ca.final_stage = sprev == 1;
   ca.N = N_;
   ca.nN = nN_;
   ca.folds = T.folds;
   ca.qs = T.qs;
   ca.ubar = ubar_;
   ca.G = tout_;
-  ca.u = Y;
-  ca.Yb = Yb_ + (size_t)(stage - 1) * nN_;
+  ca.u = Yprev;
+  ca.Yb = Yb_ + (size_t)(sprev > 0 ? sprev - 1 : 0) * nN_;
   ca.lam = lam_;
   ca.part = part_;
-  k_adj_combine<<<kBlocks, kThreads, 0, st_>>>(ca);
-  return cudaGetLastError();
+  k_adj_stage<<<kBlocks, kThreads, pw_smem_, st_>>>(pa, ca, Y ? 1 : 0, Yprev ? 1 : 0);
+  RDCU_TRY(cudaGetLastError());
+  if (Y && ng_ > 0) RDCU_TRY(planT_.run_linear(tin_, tout_, st_));
+  return cudaSuccess;
 }
 
 template <typename F>

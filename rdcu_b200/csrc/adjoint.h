@@ -71,7 +71,7 @@ class AdjointEngine {
     cudaGraphExec_t rec, rev;
   };
   std::vector<SegGraphs> graphs_;
-  cudaError_t vjp(const double* Y, int stage, double h);
+  cudaError_t stage_kernels(const double* Y, int stage, double h, const double* Yprev, int sprev);
   cudaError_t ensure_store(int steps);
   void drop_graphs();
   cudaError_t launch_recompute(int j0, int steps);
