@@ -159,6 +159,19 @@ NCU_TRAFFIC_3D = {"fwd_x": 772.5e6, "c2c_axis1_fwd": 218.7e6, "mid_axis0": 234.5
                   "inv_x_dictionary": 374.7e6}
 
 
+def combine_ranks(seconds, work, device):
+    """Whole-job figures of N replicas: the slowest rank's time and the sum of all ranks'
+    work (every rank calls this; one all-reduce each)."""
+    import torch
+    import torch.distributed as dist
+
+    mx = torch.tensor([seconds], dtype=torch.float64, device=device)
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    sm = torch.tensor([work], dtype=torch.float64, device=device)
+    dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+    return float(mx[0]), float(sm[0])
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
 
@@ -200,12 +213,7 @@ def run_ours(args, rank, world, local_rank):
     tB, hB, _ = s.get_state()
     if dist:
         dist.barrier()
-        t = torch.tensor([ms, float(acc) * N], dtype=torch.float64, device="cuda")
-        mx = t.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        sm = t.clone()
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        ms_max, work = float(mx[0]), float(sm[1])
+        ms_max, work = combine_ranks(ms, float(acc) * N, "cuda")
     else:
         ms_max, work = ms, float(acc) * N
     value = work / (ms_max / 1e3)
@@ -242,12 +250,7 @@ def run_ours(args, rank, world, local_rank):
     e2e_s = time.perf_counter() - w0
     acc2, att2 = s2.counters()
     if dist:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t[0])
-        wk = torch.tensor([float(acc2) * N], dtype=torch.float64, device="cuda")
-        dist.all_reduce(wk, op=dist.ReduceOp.SUM)
-        e2e_work = float(wk[0])
+        e2e_s, e2e_work = combine_ranks(e2e_s, float(acc2) * N, "cuda")
     else:
         e2e_work = float(acc2) * N
     e2e_value = e2e_work / e2e_s
@@ -477,26 +480,31 @@ def cgle_lines_bc(b, c):
     return cgle_coupling_lines(2, b, c)
 
 
-def run_ensemble(args):
+def run_ensemble(args, rank=0, world=1, local_rank=0):
     """Ensemble workload: 512 2D CGLE members of uneven size, adaptive DP45 at rtol = atol
     = 1e-8.  Warm-up [0, W tau] untimed, timed window [W tau, (W+K) tau] (tau = 0.1);
     value = sum over members of grid points x accepted steps / device seconds.  The
     instance-by-instance baseline runs a stratified sample of members (two per grid size)
     one after another through single handles over the same window and checks each
     member's accepted/attempt counts against the ensemble's; its rate is reported as
-    baseline_sequential and the ratio as speedup_vs_sequential."""
+    baseline_sequential and the ratio as speedup_vs_sequential.  On N GPUs the members are
+    dealt round-robin to the ranks (independent problems: no exchange); value = all
+    members' work / the slowest rank's time (strong scaling of the fixed ensemble)."""
     import torch
 
     import rdcu_b200 as R
 
     wl = WORKLOADS[args.workload]
-    mem = ensemble_members(wl)
+    torch.cuda.set_device(local_rank)
+    every = ensemble_members(wl)
+    mine = [i for i in range(len(every)) if i % world == rank]
+    mem = [every[i] for i in mine]
     m = len(mem)
     tau = wl["tau"]
     T_A, T_B = args.warmup * tau, (args.warmup + args.steps) * tau
     npts = np.array([x["Ns"][0] * x["Ns"][1] for x in mem], dtype=np.float64)
-    ics = [R.random_ic(2, int(N), 2.0, 0.0, i) for i, N in enumerate(npts)]
-    ens = R.Ensemble(mem)
+    ics = [R.random_ic(2, int(N), 2.0, 0.0, mine[i]) for i, N in enumerate(npts)]
+    ens = R.Ensemble(mem, device=local_rank)
     for i in range(m):
         ens.set_state(i, 0.0, wl["h0"], ics[i].ctypes.data)
     tile = ens.tune()
@@ -509,8 +517,12 @@ def run_ensemble(args):
         ens.set_state(i, t, h, y.ctypes.data)  # counters from the window start
     stream = torch.cuda.ExternalStream(ens.stream)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
     torch.cuda.synchronize()
-    with ClockSampler(0) as clk:
+    with ClockSampler(local_rank) as clk:
         e0.record(stream)
         ens.solve(T_B)
         e1.record(stream)
@@ -518,6 +530,9 @@ def run_ensemble(args):
     sec = e0.elapsed_time(e1) / 1e3
     cnt = np.array([ens.counters(i) for i in range(m)], dtype=np.float64)
     work = float(np.sum(cnt[:, 0] * npts))
+    my_work = work
+    if world > 1:
+        sec, work = combine_ranks(sec, work, "cuda")
     # e2e: host states in, host states out, through the public API (same window)
     w0 = time.perf_counter()
     for i in range(m):
@@ -527,7 +542,10 @@ def run_ensemble(args):
     for i in range(m):
         ens.get_state(i, outs[i].ctypes.data)
     e2e_s = time.perf_counter() - w0
-    # instance-by-instance baseline on a stratified sample
+    e2e_work = my_work
+    if world > 1:
+        e2e_s, e2e_work = combine_ranks(e2e_s, my_work, "cuda")
+    # instance-by-instance baseline on a stratified sample (of this rank's members)
     sample = []
     for N in wl["sizes"]:
         sample += [i for i in range(m) if mem[i]["Ns"][0] == N][:2]
@@ -556,10 +574,13 @@ def run_ensemble(args):
     achieved = bytes_attempt * attempts_batched / sec / 1e9
     ens.close()
     return {
-        "metric": METRIC, "value": work / sec, "unit": "grid-pt·steps/s", "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": sec * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "metric": METRIC, "value": work / sec, "unit": "grid-pt·steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": sec * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "strong" if world > 1 else "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "members": m, "sizes": list(wl["sizes"]), "L": "0.78 N",
+        "config": {"workload": args.workload, "members": len(every), "members_per_rank": m,
+                   "parallelism": "members dealt to %d ranks" % world if world > 1 else "single",
+                   "sizes": list(wl["sizes"]), "L": "0.78 N",
                    "coefficients": "b ~ U[0.5,3], c ~ U[-2,0] (numpy seed %d)" % wl["seed"],
                    "ic": "glibc rand seeds 0..%d, [-1,1]" % (m - 1), "rtol": 1e-8, "atol": 1e-8,
                    "window_sim_time": [T_A, T_B], "tau_per_step": tau, "tile_elems": tile,
@@ -570,7 +591,7 @@ def run_ensemble(args):
         "speedup_vs_sequential": (work / sec) / seq_rate,
         "gpu_launches": int(attempts_batched) * 19,
         "clocks": clk.summary(),
-        "e2e": {"value": work / e2e_s, "unit": "grid-pt·steps/s",
+        "e2e": {"value": e2e_work / e2e_s, "unit": "grid-pt·steps/s",
                 "h2d_bytes_per_step": 16.0 * float(np.sum(npts)) / args.steps,
                 "d2h_bytes_per_step": 32.0 * float(np.sum(npts)) / args.steps, "seconds": e2e_s},
         "roofline": {"bound": "hbm", "kernel": "batched DP45 attempt (all passes)", "achieved": achieved,
@@ -693,7 +714,7 @@ def main():
     if args.workload.startswith("adjoint"):
         line = run_adjoint(args) if rank == 0 else None
     elif args.workload.startswith("ensemble"):
-        line = run_ensemble(args) if rank == 0 else None
+        line = run_ensemble(args, rank, world, local_rank)
     elif args.workload.startswith("bdf"):
         line = run_bdf(args) if rank == 0 else None
     else:
