@@ -326,9 +326,10 @@ bool BDFEngine::init(FDProblem* fd, double atol, double rtol, int fixed, cudaStr
     if (cudaMalloc((void**)p, sb) != cudaSuccess) return fail("BDF vectors");
   if (cudaMalloc((void**)&I.V, sb * (I.m + 1)) != cudaSuccess) return fail("GMRES basis");
   if (cudaMalloc((void**)&I.part, sizeof(double) * (I.m + 2) * kRedBlocks) != cudaSuccess) return fail("reductions");
-  if (cudaMalloc((void**)&I.dots, sizeof(double) * (I.m + 2)) != cudaSuccess) return fail("reductions");
+  // three rows of m+2: the two Gram-Schmidt passes and the new vector's norm
+  if (cudaMalloc((void**)&I.dots, sizeof(double) * 3 * (I.m + 2)) != cudaSuccess) return fail("reductions");
   if (cudaMalloc((void**)&I.hvec, sizeof(double) * (I.m + 2)) != cudaSuccess) return fail("reductions");
-  if (cudaMallocHost((void**)&I.hdots, sizeof(double) * (I.m + 2)) != cudaSuccess) return fail("pinned");
+  if (cudaMallocHost((void**)&I.hdots, sizeof(double) * 3 * (I.m + 2)) != cudaSuccess) return fail("pinned");
   if (cudaMallocHost((void**)&I.hvec_host, sizeof(double) * (I.m + 2)) != cudaSuccess) return fail("pinned");
   device_bytes = sb * (8 + 11 + I.m + 1) + fd->device_bytes;
   std::vector<LinEntry> lin = linear_part(*fd);
@@ -405,6 +406,14 @@ cudaError_t vdots(BDFEngine::Impl& I, int nvec, const double* w, cudaStream_t st
   return cudaGetLastError();
 }
 
+// vdots without the host copy: out[0..nvec) = V^T w, out[nvec] = w.w on the device
+cudaError_t vdots_dev(BDFEngine::Impl& I, int nvec, const double* w, cudaStream_t st, double* out) {
+  dim3 grid(kRedBlocks, nvec + 1);
+  k_dots<<<grid, kRedThreads, 0, st>>>(I.V, nvec, w, I.nN, I.part);
+  k_sum_rows<<<nvec + 1, kRedThreads, 0, st>>>(I.part, nvec + 1, kRedBlocks, out);
+  return cudaGetLastError();
+}
+
 }  // namespace
 
 // Solves (I + alpha J) x = b; x in I.dd.  Returns the number of GMRES iterations.
@@ -444,19 +453,19 @@ static cudaError_t gmres(BDFEngine::Impl& I, const FDProblem& fd, double alpha, 
         zin = I.z;
       }
       k_apply_A<<<nb, 256, 0, st>>>(fd.rows_, fd.cols_, fd.vals_, alpha, zin, I.w, nN);
-      // classical Gram-Schmidt, twice
+      // classical Gram-Schmidt, twice, with the projections applied on the device; one
+      // host round trip per iteration brings back both passes' coefficients and the norm
       double hcol[64];
+      const int row = m + 2;
       for (int pass = 0; pass < 2; ++pass) {
-        RDCU_TRY(vdots(I, j + 1, I.w, st));
-        for (int k = 0; k <= j; ++k) {
-          I.hvec_host[k] = I.hdots[k];
-          hcol[k] = (pass == 0 ? 0.0 : hcol[k]) + I.hdots[k];
-        }
-        RDCU_TRY(cudaMemcpyAsync(I.hvec, I.hvec_host, sizeof(double) * (j + 1), cudaMemcpyHostToDevice, st));
-        k_vsub<<<nb, 256, 0, st>>>(I.V, j + 1, I.hvec, I.w, nN);
+        RDCU_TRY(vdots_dev(I, j + 1, I.w, st, I.dots + pass * row));
+        k_vsub<<<nb, 256, 0, st>>>(I.V, j + 1, I.dots + pass * row, I.w, nN);
       }
-      RDCU_TRY(vdots(I, 0, I.w, st));
-      const double hn = std::sqrt(I.hdots[0]);
+      RDCU_TRY(vdots_dev(I, 0, I.w, st, I.dots + 2 * row));
+      RDCU_TRY(cudaMemcpyAsync(I.hdots, I.dots, sizeof(double) * 3 * row, cudaMemcpyDeviceToHost, st));
+      RDCU_TRY(cudaStreamSynchronize(st));
+      for (int k = 0; k <= j; ++k) hcol[k] = (0.0 + I.hdots[k]) + I.hdots[row + k];
+      const double hn = std::sqrt(I.hdots[2 * row]);
       ++total;
       // Givens rotations on column j
       for (int k = 0; k < j; ++k) {
