@@ -49,3 +49,27 @@ def smooth_field(rng, prob: Problem, amp: float = 1.0, modes: int = 3) -> np.nda
 
 def spec_terms(prob: Problem):
     return [(t.C, list(t.ints)) for t in prob.terms]
+
+
+def defect_state(Ns, seed: int, frame: int = 0, nterms: int = 3, noise: float = 0.1, drift: float = 1.0):
+    """A 2-field state (u block, v block) whose phase carries vortex lines: each term adds
+    atan2(sin(2 pi (x_b - q)/N_b), sin(2 pi (x_a - p)/N_a)) -- four periodic lines along the
+    third axis, wobbling along it and drifting with the frame index -- plus phase noise.
+    Same seed, later frame: the same lines moved on."""
+    rng = np.random.default_rng(seed)
+    Ns = tuple(int(n) for n in Ns)
+    g = np.meshgrid(*[np.arange(n, dtype=np.float64) for n in Ns], indexing="ij")
+    th = np.zeros(Ns)
+    for _ in range(nterms):
+        ax = int(rng.integers(3))
+        a, b = [x for x in range(3) if x != ax]
+        p0, q0 = rng.uniform(0, Ns[a]), rng.uniform(0, Ns[b])
+        vp, vq = rng.normal(size=2) * drift
+        amp, ph = rng.uniform(0, 2.5), rng.uniform(0, 2 * np.pi)
+        s = 2 * np.pi * g[ax] / Ns[ax] + ph
+        p = p0 + vp * frame + amp * np.sin(s)
+        q = q0 + vq * frame + amp * np.cos(s)
+        th += np.arctan2(np.sin(2 * np.pi * (g[b] - q) / Ns[b]), np.sin(2 * np.pi * (g[a] - p) / Ns[a]))
+    th += noise * np.random.default_rng([seed, frame]).normal(size=Ns)
+    r = 1.0 + 0.2 * np.random.default_rng([seed, frame, 1]).uniform(size=Ns)
+    return np.concatenate([(r * np.cos(th)).ravel(), (r * np.sin(th)).ravel()])
