@@ -269,6 +269,57 @@ const char *rdcu_ensemble_last_error(rdcu_ensemble_t *e);
 #define RDCU_NOALLOC_SCRATCH_BYTES (64ull << 20)
 int rdcu_rhs_noalloc(const rdcu_spec *spec, const double *y, double *f, void *stream);
 
+/* ---- defect lines -----------------------------------------------------------------
+ * The reference's post-processing of 3D CGLE states (makelines.py) on the GPU: the
+ * phase theta = atan2(v, u) + pi of a 2-field state, the winding of every grid
+ * plaquette (wloop, makelines.py:19-24), the "line cubes" on either side of each
+ * winding plaquette, their periodic face-neighbour graph and its connected components
+ * (findlines, makelines.py:26-57), and the minimum periodic L1 distance between the
+ * components of two frames (correlate, makelines.py:112-144).  The reference's Python
+ * functions are the interface these entry points replace; its graph is built by an
+ * all-pairs distance test and numbered by networkx, here by a grid lookup and a
+ * union-find on the device.  3D grids only, every axis >= 2, at most 2^29 points.
+ *
+ * rdcu_lines_create: workspace for one grid (Ns, Ls as the reference's --Ns/--Ls) on
+ *   `device`; the handle owns a stream and keeps the results of its last frame.
+ * rdcu_lines_find: one frame.  src (host or device) is the state -- u block then v block,
+ *   2*N doubles, C order, as one frame of states.dat (makelines.py:60-65) -- when kind is
+ *   RDCU_LINES_STATE, or the phase field theta (N doubles) when RDCU_LINES_PHASE.
+ *   Outputs the number of line cubes, edges and components.  Components are numbered
+ *   by their smallest cube (networkx's connected_components order).
+ * rdcu_lines_edges: xyz[n_edges][2][3] (host or device) -- edge (u, v), u < v, of every
+ *   component as cube coordinates c scaled (c * L) / (N - 1), components in order, each
+ *   component's edges in ascending (u, v) order -- and comp_offsets[n_components + 1]
+ *   into them.  Either pointer may be NULL.
+ * rdcu_lines_cubes: the cube indices (C order) grouped by component, ascending within
+ *   each, and comp_offsets[n_components + 1].  Either pointer may be NULL.
+ * rdcu_lines_correlate: diffs[n_cur][n_prev] (int64, host or device) between the last
+ *   frames of two handles on the same grid: the minimum over cubes a of component i of
+ *   `prev` and b of component j of `cur` of sum_axis |((a - b + N/2) mod N) - N/2|, with
+ *   the cube coordinates recovered from the scaled edge coordinates as the reference
+ *   does (rounded for prev, truncated toward zero for cur).
+ * rdcu_lines_correlate_sets: the same matrix for explicit cube sets (C-order indices
+ *   grouped by component, offsets n + 1 starting at 0, host or device), on l's grid.
+ * rdcu_lines_info: the handle's stream (cudaStream_t), device bytes and the number of
+ *   kernels it has launched. */
+#define RDCU_LINES_STATE 0
+#define RDCU_LINES_PHASE 1
+typedef struct rdcu_lines rdcu_lines_t;
+int rdcu_lines_create(rdcu_lines_t **out, const int Ns[3], const double Ls[3], int device);
+int rdcu_lines_destroy(rdcu_lines_t *l);
+int rdcu_lines_find(rdcu_lines_t *l, const double *src, int kind, long long *n_cubes, long long *n_edges,
+                    long long *n_components);
+int rdcu_lines_edges(rdcu_lines_t *l, double *xyz, long long *comp_offsets);
+int rdcu_lines_cubes(rdcu_lines_t *l, long long *cubes, long long *comp_offsets);
+int rdcu_lines_correlate(rdcu_lines_t *prev, rdcu_lines_t *cur, long long *diffs);
+int rdcu_lines_correlate_sets(rdcu_lines_t *l, const long long *prev_cubes, const long long *prev_offsets,
+                              long long n_prev, const long long *cur_cubes, const long long *cur_offsets,
+                              long long n_cur, long long *diffs);
+int rdcu_lines_info(rdcu_lines_t *l, void **stream, long long *device_bytes, long long *launches);
+/* Last error message of the handle (or of the last failed rdcu_lines_create when l is
+ * NULL). */
+const char *rdcu_lines_last_error(rdcu_lines_t *l);
+
 /* ---- errors ----------------------------------------------------------------------- */
 const char *rdcu_error_string(int code);
 /* Last error message of the handle (or of the last failed rdcu_create when h is NULL). */

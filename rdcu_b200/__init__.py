@@ -46,8 +46,11 @@ EXPORTS = [
     "rdcu_set_coefficients", "rdcu_adjoint_forward", "rdcu_adjoint_backward",
     "rdcu_ensemble_create", "rdcu_ensemble_destroy", "rdcu_ensemble_set_state", "rdcu_ensemble_get_state",
     "rdcu_ensemble_solve", "rdcu_ensemble_counters", "rdcu_ensemble_tune", "rdcu_ensemble_info",
-    "rdcu_ensemble_last_error", "rdcu_error_string", "rdcu_last_error",
+    "rdcu_ensemble_last_error", "rdcu_lines_create", "rdcu_lines_destroy", "rdcu_lines_find", "rdcu_lines_edges",
+    "rdcu_lines_cubes", "rdcu_lines_correlate", "rdcu_lines_correlate_sets", "rdcu_lines_info",
+    "rdcu_lines_last_error", "rdcu_error_string", "rdcu_last_error",
 ]
+_STRING_RESULTS = ("rdcu_error_string", "rdcu_last_error", "rdcu_ensemble_last_error", "rdcu_lines_last_error")
 
 
 class RdcuError(RuntimeError):
@@ -133,12 +136,23 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
     lib.rdcu_ensemble_info.argtypes = [vp, pi, ctypes.POINTER(vp), ctypes.POINTER(ll)]
     lib.rdcu_ensemble_last_error.argtypes = [vp]
     lib.rdcu_ensemble_last_error.restype = ctypes.c_char_p
+    pll = ctypes.POINTER(ll)
+    lib.rdcu_lines_create.argtypes = [ctypes.POINTER(vp), pi, pd, i]
+    lib.rdcu_lines_destroy.argtypes = [vp]
+    lib.rdcu_lines_find.argtypes = [vp, vp, i, pll, pll, pll]
+    lib.rdcu_lines_edges.argtypes = [vp, vp, vp]
+    lib.rdcu_lines_cubes.argtypes = [vp, vp, vp]
+    lib.rdcu_lines_correlate.argtypes = [vp, vp, vp]
+    lib.rdcu_lines_correlate_sets.argtypes = [vp, vp, vp, ll, vp, vp, ll, vp]
+    lib.rdcu_lines_info.argtypes = [vp, ctypes.POINTER(vp), pll, pll]
+    lib.rdcu_lines_last_error.argtypes = [vp]
+    lib.rdcu_lines_last_error.restype = ctypes.c_char_p
     lib.rdcu_error_string.argtypes = [i]
     lib.rdcu_error_string.restype = ctypes.c_char_p
     lib.rdcu_last_error.argtypes = [vp]
     lib.rdcu_last_error.restype = ctypes.c_char_p
     for name in EXPORTS:
-        if name not in ("rdcu_error_string", "rdcu_last_error", "rdcu_ensemble_last_error"):
+        if name not in _STRING_RESULTS:
             getattr(lib, name).restype = ctypes.c_int
     if path is None:
         _lib = lib
