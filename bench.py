@@ -70,6 +70,9 @@ WORKLOADS = {
     "bdf_brusselator_256": dict(Ns=(256, 256), Ls=(64.0, 64.0), seed=3, h0=1e-3, tau=1.0),
     # discrete adjoint: gradient of a terminal mismatch over 5000 fixed steps (see run_adjoint)
     "adjoint_cgle2d_256": dict(Ns=(256, 256), Ls=(200.0, 200.0), seed=1, h=1e-3, T=5.0, K=50),
+    # defect lines of 3D CGLE frames at the line tracker's default grid (see run_lines)
+    "lines_cgle3d_128": dict(Ns=(128, 128, 128), Ls=(50.0, 50.0, 50.0), seed=7, terms=8, noise=0.1, drift=0.7,
+                             frames_per_step=16, ring=48),
 }
 
 
@@ -106,6 +109,7 @@ class ClockSampler:
         self.dev = device_index
         self.proc = None
         self.lines = []
+        self.skip = 0
 
     def __enter__(self):
         try:
@@ -114,6 +118,11 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # the first sample can take a while to appear: start timing once it has
+            t0 = time.perf_counter()
+            while not self.lines and time.perf_counter() - t0 < 3.0 and self.proc.poll() is None:
+                time.sleep(0.02)
+            self.skip = len(self.lines)  # taken before the timed region
         except OSError:
             self.proc = None
         return self
@@ -133,7 +142,8 @@ class ClockSampler:
     def summary(self):
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in self.lines:
+        during = self.lines[self.skip:] or self.lines  # a short region may see no sample of its own
+        for l in during:
             p = [x.strip() for x in l.split(",")]
             if len(p) < 9:
                 continue
@@ -600,6 +610,191 @@ def run_ensemble(args, rank=0, world=1, local_rank=0):
     }
 
 
+def line_frames(wl, count, device):
+    """Synthetic 3D CGLE-like frames with vortex lines (no dataset exists): the phase is a
+    sum of wl["terms"] terms atan2(sin(2 pi (x_b - q)/N_b), sin(2 pi (x_a - p)/N_a)) --
+    four periodic lines along the third axis each, wobbling along it and drifting
+    wl["drift"] cells per frame -- plus Gaussian phase noise; amplitude 1 + U[0, 0.2].
+    Returns a (count, 2*N) float64 tensor on `device` (u block, v block per frame)."""
+    import torch
+
+    Ns = wl["Ns"]
+    rng = np.random.default_rng(wl["seed"])
+    g = torch.meshgrid(*[torch.arange(n, dtype=torch.float64, device=device) for n in Ns], indexing="ij")
+    terms = []
+    for _ in range(wl["terms"]):
+        ax = int(rng.integers(3))
+        a, b = [x for x in range(3) if x != ax]
+        terms.append((ax, a, b, rng.uniform(0, Ns[a]), rng.uniform(0, Ns[b]), *(rng.normal(size=2) * wl["drift"]),
+                      rng.uniform(0, 2.5), rng.uniform(0, 2 * np.pi)))
+    gen = torch.Generator(device=device)
+    gen.manual_seed(wl["seed"])
+    n = int(np.prod(Ns))
+    out = torch.empty((count, 2 * n), dtype=torch.float64, device=device)
+    for k in range(count):
+        th = torch.zeros(Ns, dtype=torch.float64, device=device)
+        for ax, a, b, p0, q0, vp, vq, amp, ph in terms:
+            s_ = 2 * np.pi * g[ax] / Ns[ax] + ph
+            p = p0 + vp * k + amp * torch.sin(s_)
+            q = q0 + vq * k + amp * torch.cos(s_)
+            th += torch.atan2(torch.sin(2 * np.pi * (g[b] - q) / Ns[b]), torch.sin(2 * np.pi * (g[a] - p) / Ns[a]))
+        th += wl["noise"] * torch.randn(Ns, dtype=torch.float64, device=device, generator=gen)
+        r = 1.0 + 0.2 * torch.rand(Ns, dtype=torch.float64, device=device, generator=gen)
+        out[k, :n] = (r * torch.cos(th)).reshape(-1)
+        out[k, n:] = (r * torch.sin(th)).reshape(-1)
+    return out
+
+
+def lines_cpu_sample(wl, frames_host, count):
+    """The oracle (numpy/scipy, one thread) on `count` frames: phase, lines, correlate
+    with the previous frame.  Returns seconds per frame."""
+    from oracle import lines as ol
+
+    Ns, Ls = wl["Ns"], wl["Ls"]
+    prev = ol.findlines(ol.phase(frames_host[0], Ns), Ns, Ls)
+    t0 = time.perf_counter()
+    for k in range(1, count + 1):
+        cur = ol.findlines(ol.phase(frames_host[k], Ns), Ns, Ls)
+        ol.correlate(prev, cur, Ns, Ls)
+        prev = cur
+    return (time.perf_counter() - t0) / count
+
+
+def run_lines(args, rank=0, world=1, local_rank=0):
+    """Defect-line workload (the reference's makelines.py per-frame work): for each frame
+    of a sequence of 128^3 2-field states, the phase, plaquette windings, line cubes,
+    their components and edge lists (findlines), and the distance matrix to the previous
+    frame's components (correlate).  A bench step is wl["frames_per_step"] frames, taken
+    in turn from a ring of wl["ring"] distinct frames (1.6 GB, beyond L2); value =
+    frames/s.  ``value`` runs on frames resident in HBM (edge lists stay on the device,
+    the small distance matrix comes back); ``e2e`` starts from pinned host frames and
+    brings every frame's edge list and distance matrix to the host through the public
+    API.  On N GPUs each rank processes its own frame sequence (independent frames: no
+    exchange)."""
+    import torch
+
+    from rdcu_b200.lines import STATE, Lines
+
+    wl = WORKLOADS[args.workload]
+    torch.cuda.set_device(local_rank)
+    Ns, Ls = wl["Ns"], wl["Ls"]
+    N = int(np.prod(Ns))
+    W, K, F, R = args.warmup, args.steps, wl["frames_per_step"], wl["ring"]
+    frames = line_frames(dict(wl, seed=wl["seed"] + rank), R, "cuda")
+    hs = [Lines(Ns, Ls, local_rank), Lines(Ns, Ls, local_rank)]
+
+    def step(k, src):
+        cur, prev = hs[k % 2], hs[(k - 1) % 2]
+        cur.find(src[k % R], STATE)
+        return cur.correlate(prev)
+
+    hs[0].find(frames[0], STATE)
+    for k in range(1, W * F + 1):
+        step(k, frames)
+    k0, k1 = W * F + 1, (W + K) * F + 1
+    launches0 = sum(h.info()[2] for h in hs)
+    streams = [torch.cuda.ExternalStream(h.stream) for h in hs]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    comps, cubes = [], []
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        e0.record(streams[k0 % 2])
+        for k in range(k0, k1):
+            d = step(k, frames)
+            comps.append(d.shape[0])
+            cubes.append(hs[k % 2].counts[0])
+        e1.record(streams[(k1 - 1) % 2])
+        e1.synchronize()
+    sec = e0.elapsed_time(e1) / 1e3
+    launches = sum(h.info()[2] for h in hs) - launches0
+    # one find alone, CUDA events on its stream
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    f0.record(streams[0])
+    for r in range(8):
+        hs[0].find(frames[r], STATE)
+    f1.record(streams[0])
+    f1.synchronize()
+    find_s = f0.elapsed_time(f1) / 1e3 / 8
+    work = float(K * F)
+    if world > 1:
+        sec, work = combine_ranks(sec, work, "cuda")
+    # e2e: pinned host frames in, edge lists and distance matrices out
+    host = frames.cpu().pin_memory()
+    torch.cuda.synchronize()
+    hs[(k0 - 1) % 2].find(host[(k0 - 1) % R], STATE)
+    w0 = time.perf_counter()
+    out_bytes = 0
+    for k in range(k0, k1):
+        d = step(k, host)
+        xyz, off = hs[k % 2].edges()
+        out_bytes += xyz.nbytes + off.nbytes + d.nbytes
+    e2e_s = time.perf_counter() - w0
+    e2e_work = float(K * F)
+    if world > 1:
+        e2e_s, e2e_work = combine_ranks(e2e_s, e2e_work, "cuda")
+    peak, peak_kind = load_peaks()
+    find_bytes = 40.0 * N  # state 16 B read; phase 8 B written, 8 B read; face, mark, node map 8 B
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        per = lines_cpu_sample(wl, host.numpy(), 2)
+        cpu = {"value": 1.0 / per, "unit": "frames/s", "cores": 1, "kind": "port",
+               "sample": "oracle/lines.py (numpy/scipy, one thread) on 2 frames: phase, lines, correlate"}
+    for h in hs:
+        h.close()
+    return {
+        "metric": "frames/s", "value": work / sec, "unit": "frames/s", "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": sec * 1e3 / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "grid": list(Ns), "L": list(Ls), "frames_per_step": F,
+                   "frames": "synthetic vortex-line states, %d terms (4 lines each), phase noise %g, drift %g "
+                             "cells/frame, seed %d, ring of %d" % (wl["terms"], wl["noise"], wl["drift"],
+                                                                  wl["seed"], R),
+                   "mean_line_cubes": float(np.mean(cubes)), "mean_components": float(np.mean(comps)),
+                   "parallelism": "independent frame sequences per rank" if world > 1 else "single",
+                   "l2": "ring of %d distinct 33.5 MB frames (1.6 GB > L2), no flush needed" % R},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+        "e2e": {"value": e2e_work / e2e_s, "unit": "frames/s", "h2d_bytes_per_step": 16.0 * N * F,
+                "d2h_bytes_per_step": out_bytes / K, "seconds": e2e_s},
+        "roofline": {"bound": "hbm", "kernel": "rdcu_lines_find (grid passes + graph passes)",
+                     "achieved": find_bytes / find_s / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": find_bytes / find_s / 1e9 / peak, "peak_kind": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_launch": find_bytes, "find_ms": find_s * 1e3},
+        "cpu_baseline": cpu,
+    }
+
+
+def run_lines_reference(args):
+    """Reference arm of the defect-line workload: the reference's line tracker is Python
+    (makelines.py, numpy + torch + networkx) that is not on the GPU box, so its CPU
+    restatement oracle/lines.py times a bounded sample of the same frames (phase, lines,
+    correlate per frame, one thread)."""
+    import torch
+
+    wl = WORKLOADS[args.workload]
+    n = 4
+    frames = line_frames(wl, n + 1, "cuda" if torch.cuda.is_available() else "cpu").cpu().numpy()
+    per = lines_cpu_sample(wl, frames, n)
+    value = 1.0 / per
+    return {
+        "impl": "reference", "metric": "frames/s", "value": value, "unit": "frames/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1e3 * wl["frames_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "grid": list(wl["Ns"]), "L": list(wl["Ls"])},
+        "cpu_baseline": {"value": value, "unit": "frames/s", "cores": 1, "kind": "port",
+                         "sample": "oracle/lines.py on %d frames of the workload (phase, findlines, correlate each)"
+                                   % n},
+        "e2e": {"value": value, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference's makelines.py cannot run on the box; the oracle builds the neighbour graph from "
+                "the grid, faster than the reference's all-pairs test, so this arm overstates the reference",
+    }
+
+
 def launches_per_attempt(ndim):
     per_stage = {1: 3, 2: 3, 3: 5}[ndim]
     return 6 * per_stage + 1
@@ -642,6 +837,8 @@ def run_reference(args):
         return {"impl": "reference", "unavailable": "the reference has no ensemble; its one-problem-per-process "
                 "rate is the cgle2d workloads' reference arm, and the instance-by-instance baseline of this "
                 "workload is reported by our arm"}
+    if args.workload.startswith("lines"):
+        return run_lines_reference(args)
     exe, why = reference_binary()
     if exe is None:
         return {"impl": "reference", "unavailable": why}
@@ -717,6 +914,8 @@ def main():
         line = run_ensemble(args, rank, world, local_rank)
     elif args.workload.startswith("bdf"):
         line = run_bdf(args) if rank == 0 else None
+    elif args.workload.startswith("lines"):
+        line = run_lines(args, rank, world, local_rank)
     else:
         line = run_ours(args, rank, world, local_rank)
     if world > 1:
