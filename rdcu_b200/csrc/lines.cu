@@ -73,8 +73,15 @@ __device__ __forceinline__ double wrap_pi(double x) {
 
 // Nonzero winding of the plaquette t0 -> t1 -> t2 -> t3 (makelines.py:19-24): the four
 // wrapped differences summed in that order, over 2 pi, rounded half to even.
+// Shortcut with the same answer: when every difference d is below 3 in magnitude, d + pi
+// lies in (0.14, 6.15), no branch of wrap_pi adds or subtracts 2 pi, and each wrapped
+// difference is d to within two roundings of pi-sized values (~1e-15); the exact
+// differences sum to zero, so the rounded ones, and s, stay within ~1e-14 of zero and
+// rint(s / 2 pi) is 0.  A NaN fails the comparisons and takes the full path.
 __device__ __forceinline__ bool winds(double t0, double t1, double t2, double t3) {
-  const double s = wrap_pi(t1 - t0) + wrap_pi(t2 - t1) + wrap_pi(t3 - t2) + wrap_pi(t0 - t3);
+  const double d0 = t1 - t0, d1 = t2 - t1, d2 = t3 - t2, d3 = t0 - t3;
+  if (fabs(d0) < 3.0 && fabs(d1) < 3.0 && fabs(d2) < 3.0 && fabs(d3) < 3.0) return false;
+  const double s = wrap_pi(d0) + wrap_pi(d1) + wrap_pi(d2) + wrap_pi(d3);
   return rint(s / kTwoPi) != 0.0;
 }
 
