@@ -528,14 +528,12 @@ __global__ void k_fill(int* a, long long n, int v) {
 }
 
 __device__ __forceinline__ int axis_dist(int a, int b, int N) {
-  // |((a - b + N/2) mod N) - N/2| with a floored modulus (makelines.py:133-134)
-  const int h = N >> 1;
-  int t = a - b + h;
-  if (t < 0)
-    t += N;
-  else if (t >= N)
-    t -= N;
-  return abs(t - h);
+  // |((a - b + N/2) mod N) - N/2| with a floored modulus (makelines.py:133-134).  For
+  // a, b in [0, N) that is the minimum image min(|a - b|, N - |a - b|): the modulus maps
+  // a - b into [-N/2, N - N/2), where |t| is the shorter way round (both equal N/2 when
+  // |a - b| = N/2).
+  const int d = abs(a - b);
+  return min(d, N - d);
 }
 
 // diffs[j][i] = min over cubes a of component i (frame A) and b of component j (frame B)
