@@ -70,6 +70,12 @@ WORKLOADS = {
     "bdf_brusselator_256": dict(Ns=(256, 256), Ls=(64.0, 64.0), seed=3, h0=1e-3, tau=1.0),
     # discrete adjoint: gradient of a terminal mismatch over 5000 fixed steps (see run_adjoint)
     "adjoint_cgle2d_256": dict(Ns=(256, 256), Ls=(200.0, 200.0), seed=1, h=1e-3, T=5.0, K=50),
+    # whole CLI runs with outputs, same flags for both CLIs (see run_cli): C1 as given, and
+    # C2's output-every-time-unit run shortened to T = 4 (5 frames of 268 MB)
+    "cli_c1_cgle2d_128": dict(cli="-n 2 -N 128,128 -L 100,100 -A 2 -s 1 -t 100 -d 1 -r 1e-8 -a 1e-8 -D1",
+                              Ns=(128, 128), outputs=101),
+    "cli_c2_cgle3d_256_d1": dict(cli="-n 2 -N 256,256,256 -L 200,200,200 -A 2 -s 2 -t 4 -D1", Ns=(256, 256, 256),
+                                 outputs=5),
     # defect lines of 3D CGLE frames at the line tracker's default grid (see run_lines)
     "lines_cgle3d_128": dict(Ns=(128, 128, 128), Ls=(50.0, 50.0, 50.0), seed=7, terms=8, noise=0.1, drift=0.7,
                              frames_per_step=16, ring=48),
@@ -769,6 +775,79 @@ def run_lines(args, rank=0, world=1, local_rank=0):
     }
 
 
+def cli_run(exe, wl):
+    """One CLI run of the workload's command line in a scratch directory (coupling file:
+    the reference notebook's CGLE).  Returns the integration-only rate from the .out
+    progress lines (N x difference of the cumulative steps / difference of the elapsed
+    seconds between the first and last output), the run's own totals and wall time."""
+    Ns = wl["Ns"]
+    N = int(np.prod(Ns))
+    with tempfile.TemporaryDirectory() as wd:
+        fb = os.path.join(wd, "cli")
+        open(fb + "coupling.dat", "w").write("\n".join(cgle_lines(len(Ns))) + "\n")
+        cmd = [exe] + shlex.split(wl["cli"]) + [fb]
+        w0 = time.perf_counter()
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=3600)
+        wall = time.perf_counter() - w0
+        out = open(fb + ".out").read() if os.path.exists(fb + ".out") else ""
+        states = os.path.getsize(fb + "states.dat") if os.path.exists(fb + "states.dat") else 0
+    prog = []
+    for line in out.splitlines():
+        f = line.split("\t")
+        if len(f) >= 5 and re.fullmatch(r"[0-9.]+", f[0]):
+            prog.append((float(f[1]), int(f[4])))
+    m = re.search(r"steps: (\d+)", out)
+    rt = re.search(r"runtime: ([0-9.]+)", out)
+    if r.returncode != 0 or len(prog) < 2 or not m:
+        return None, "rc %d, %d progress lines: %s" % (r.returncode, len(prog), (r.stderr or r.stdout)[-200:])
+    (e0, s0), (e1, s1) = prog[0], prog[-1]
+    return {"value": N * (s1 - s0) / (e1 - e0), "steps": int(m.group(1)), "window_steps": s1 - s0,
+            "window_s": e1 - e0, "runtime_s": float(rt.group(1)) if rt else None, "wall_s": wall,
+            "outputs": len(prog), "states_bytes": states, "command": " ".join(shlex.quote(c) for c in cmd)}, None
+
+
+def run_cli(args, impl):
+    """CLI workloads: the same command line through this package's rdcu CLI (ours) or the
+    reference's own build (reference arm), outputs included; value from the .out
+    progress lines, as for the reference (the integration between the first and the
+    last output, set-up excluded, output writes included)."""
+    wl = WORKLOADS[args.workload]
+    if impl == "reference":
+        exe, why = reference_binary()
+        if exe is None:
+            return {"impl": "reference", "unavailable": why}
+    else:
+        from rdcu_b200 import CLI_PATH
+
+        exe = CLI_PATH
+    with ClockSampler(0) as clk:
+        res, err = cli_run(exe, wl)
+    if res is None:
+        line = {"metric": METRIC, "unavailable": "CLI run failed: " + err}
+        if impl == "reference":
+            line["impl"] = "reference"
+        return line
+    line = {
+        "metric": METRIC, "value": res["value"], "unit": "grid-pt·steps/s", "n_gpus": 1,
+        "steps": res["outputs"] - 1, "warmup": 0, "ms_per_step": res["window_s"] * 1e3 / max(1, res["outputs"] - 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "command": res["command"], "accepted_steps": res["steps"],
+                   "window_steps": res["window_steps"], "outputs": res["outputs"],
+                   "states_bytes": res["states_bytes"], "runtime_s": res["runtime_s"], "wall_s": res["wall_s"],
+                   "step": "one output interval of the run (dt = 1)"},
+        "e2e": {"value": res["value"], "unit": "grid-pt·steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": res["states_bytes"] / max(1, res["outputs"]),
+                "note": "CLI process: outputs written to states.dat inside the window"},
+        "gpu_launches": None,
+        "clocks": clk.summary(),
+    }
+    if impl == "reference":
+        line["impl"] = "reference"
+        line["cpu_baseline"] = {"value": res["value"], "unit": "grid-pt·steps/s", "cores": 1, "kind": "reference",
+                                "sample": "the reference's own CLI build on the same command line"}
+    return line
+
+
 def run_lines_reference(args):
     """Reference arm of the defect-line workload: the reference's line tracker is Python
     (makelines.py, numpy + torch + networkx) that is not on the GPU box, so its CPU
@@ -839,6 +918,8 @@ def run_reference(args):
                 "workload is reported by our arm"}
     if args.workload.startswith("lines"):
         return run_lines_reference(args)
+    if args.workload.startswith("cli"):
+        return run_cli(args, "reference")
     exe, why = reference_binary()
     if exe is None:
         return {"impl": "reference", "unavailable": why}
@@ -916,6 +997,8 @@ def main():
         line = run_bdf(args) if rank == 0 else None
     elif args.workload.startswith("lines"):
         line = run_lines(args, rank, world, local_rank)
+    elif args.workload.startswith("cli"):
+        line = run_cli(args, "ours") if rank == 0 else None
     else:
         line = run_ours(args, rank, world, local_rank)
     if world > 1:

@@ -62,7 +62,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
             raise RuntimeError("link failed:\n%s\n%s" % (r.stdout, r.stderr))
     cli_src = os.path.join(HERE, "cli", "rdcu_main.cpp")
     if os.path.exists(cli_src) and (force or _newer(CLI, [cli_src, LIB, os.path.join(ROOT, "include", "rdcu.h")])):
-        cmd = ["g++", "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), cli_src, "-o", CLI,
+        cmd = ["g++", "-O2", "-std=c++17", "-pthread", "-I" + os.path.join(ROOT, "include"), cli_src, "-o", CLI,
                "-L" + LIB_DIR, "-lrdcu", "-Wl,-rpath,$ORIGIN/../lib"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:

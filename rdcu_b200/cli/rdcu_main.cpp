@@ -15,10 +15,16 @@
 #include <unistd.h>
 
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
+#include <functional>
+#include <memory>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "rdcu.h"
@@ -77,6 +83,76 @@ double elapsed_since(const timeval& start) {
   return end.tv_sec - start.tv_sec + 1e-6 * (end.tv_usec - start.tv_usec);
 }
 
+// Output files written behind the integration: one background thread runs the writes in
+// the order they were issued, from host copies of the state taken when the library
+// delivers them, so the GPU keeps stepping while states.dat, times.dat and fs.dat are
+// written.  Host buffers are recycled (at most kBuffers in flight; a new output waits for
+// a free one), and drain() waits for every write -- the contents and order of each file
+// are those of synchronous writes.
+class Writer {
+ public:
+  static constexpr int kBuffers = 3;
+  Writer() {
+    for (int i = 0; i < kBuffers; ++i) free_.push_back(std::make_unique<std::vector<double>>());
+    th_ = std::thread([this] { run(); });
+  }
+  ~Writer() {
+    drain();
+    {
+      std::lock_guard<std::mutex> g(m_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    th_.join();
+  }
+  // a buffer for the next output (waits while all are queued for writing)
+  std::unique_ptr<std::vector<double>> acquire() {
+    std::unique_lock<std::mutex> g(m_);
+    cv_.wait(g, [this] { return !free_.empty(); });
+    auto b = std::move(free_.back());
+    free_.pop_back();
+    return b;
+  }
+  // runs task(buffer) on the writer thread, then recycles the buffer
+  void submit(std::unique_ptr<std::vector<double>> b, std::function<void(const std::vector<double>&)> task) {
+    {
+      std::lock_guard<std::mutex> g(m_);
+      q_.emplace_back(std::move(b), std::move(task));
+    }
+    cv_.notify_all();
+  }
+  void drain() {
+    std::unique_lock<std::mutex> g(m_);
+    cv_.wait(g, [this] { return q_.empty() && !busy_; });
+  }
+
+ private:
+  using Job = std::pair<std::unique_ptr<std::vector<double>>, std::function<void(const std::vector<double>&)>>;
+  std::mutex m_;
+  std::condition_variable cv_;
+  std::deque<Job> q_;
+  std::vector<std::unique_ptr<std::vector<double>>> free_;
+  bool stop_ = false, busy_ = false;
+  std::thread th_;
+
+  void run() {
+    std::unique_lock<std::mutex> g(m_);
+    for (;;) {
+      cv_.wait(g, [this] { return stop_ || !q_.empty(); });
+      if (q_.empty()) return;
+      Job j = std::move(q_.front());
+      q_.pop_front();
+      busy_ = true;
+      g.unlock();
+      j.second(*j.first);
+      g.lock();
+      free_.push_back(std::move(j.first));
+      busy_ = false;
+      cv_.notify_all();
+    }
+  }
+};
+
 struct Ctx {
   rdcu_t* h = nullptr;
   int n = 1, ndim = 1, dense = 1, stiff = 0, verbose = 0;
@@ -91,6 +167,7 @@ struct Ctx {
   std::vector<int> rowsloc, colsloc;
   long long nnz_max = 0;
   int failed = 0;
+  Writer* writer = nullptr;
 };
 
 int check(Ctx& c, int rc, const char* what) {
@@ -141,18 +218,23 @@ int on_event(void* user, const rdcu_event* ev) {
   }
   if (ev->kind == RDCU_EV_EVAL) {
     if (c.dense >= 1) {
-      if (check(c, rdcu_memcpy(c.h, c.yloc.data(), ev->y, (unsigned long long)c.nN * sizeof(double)), "copy"))
+      auto b = c.writer->acquire();
+      b->resize((size_t)c.nN);
+      if (check(c, rdcu_memcpy(c.h, b->data(), ev->y, (unsigned long long)c.nN * sizeof(double)), "copy")) {
+        c.writer->submit(std::move(b), [](const std::vector<double>&) {});
         return 1;
-      fwrite(c.yloc.data(), sizeof(double), c.nN, c.outstates);
-      fflush(c.outstates);
+      }
+      const double te = ev->t_eval;
+      FILE *fst = c.outstates, *ftm = c.outtimes;
+      c.writer->submit(std::move(b), [fst, ftm, te](const std::vector<double>& y) {
+        fwrite(y.data(), sizeof(double), y.size(), fst);
+        fflush(fst);
+        fwrite(&te, sizeof(double), 1, ftm);
+        fflush(ftm);
+      });
     }
     if (write_derived(c, ev->y, ev->t_eval)) return 1;
     if (c.dense >= 4 && write_jac(c, ev->y, ev->t_eval)) return 1;
-    const double te = ev->t_eval;
-    if (c.dense >= 1) {
-      fwrite(&te, sizeof(double), 1, c.outtimes);
-      fflush(c.outtimes);
-    }
     return 0;
   }
   // checkpoint: progress line and fs.dat
@@ -167,24 +249,29 @@ int on_event(void* user, const rdcu_event* ev) {
   fprintf(c.out, "%.3f\t%1.3e\t%1.3e\t%f\t%i\t\n", frac, el, eta, h, c.steps);
   fflush(c.out);
   const std::string file = c.filebase + "fs.dat";
-  FILE* fs = fopen(file.c_str(), "wb");
-  if (!fs) return 0;
   const int order = ev->order;
   const long long nblk = c.stiff ? 1 + order : 1;
-  std::vector<double> buf((size_t)(c.nN * nblk));
-  if (check(c, rdcu_memcpy(c.h, buf.data(), ev->y, (unsigned long long)(c.nN * nblk) * sizeof(double)), "copy")) {
-    fclose(fs);
+  auto b = c.writer->acquire();
+  b->resize((size_t)(c.nN * nblk));
+  if (check(c, rdcu_memcpy(c.h, b->data(), ev->y, (unsigned long long)(c.nN * nblk) * sizeof(double)), "copy")) {
+    c.writer->submit(std::move(b), [](const std::vector<double>&) {});
     return 1;
   }
-  fwrite(buf.data(), sizeof(double), c.nN, fs);
-  fwrite(&t, sizeof(double), 1, fs);
-  fwrite(&h, sizeof(double), 1, fs);
-  if (c.stiff) {
-    fwrite(&order, sizeof(int), 1, fs);
-    for (int i = 1; i <= order; i++) fwrite(buf.data() + (size_t)c.nN * i, sizeof(double), c.nN, fs);
-  }
-  fflush(fs);
-  fclose(fs);
+  const long long nN = c.nN;
+  const int stiff = c.stiff;
+  c.writer->submit(std::move(b), [file, nN, t, h, stiff, order](const std::vector<double>& buf) {
+    FILE* fs = fopen(file.c_str(), "wb");
+    if (!fs) return;
+    fwrite(buf.data(), sizeof(double), nN, fs);
+    fwrite(&t, sizeof(double), 1, fs);
+    fwrite(&h, sizeof(double), 1, fs);
+    if (stiff) {
+      fwrite(&order, sizeof(int), 1, fs);
+      for (int i = 1; i <= order; i++) fwrite(buf.data() + (size_t)nN * i, sizeof(double), nN, fs);
+    }
+    fflush(fs);
+    fclose(fs);
+  });
   return 0;
 }
 
@@ -555,8 +642,14 @@ int main(int argc, char* argv[]) {
     if (dense >= 4 && stiff && write_jac(c, c.yloc.data(), t)) return EXIT_FAILURE;
   }
 
-  rc = rdcu_solve(c.h, t1, hmin, hmax, t_eval.data(), (int)t_eval.size(), on_event, &c);
-  if (rc != RDCU_OK && rc != RDCU_ERR_CALLBACK) check(c, rc, "solve");
+  {
+    Writer writer;
+    c.writer = &writer;
+    rc = rdcu_solve(c.h, t1, hmin, hmax, t_eval.data(), (int)t_eval.size(), on_event, &c);
+    if (rc != RDCU_OK && rc != RDCU_ERR_CALLBACK) check(c, rc, "solve");
+    writer.drain();
+    c.writer = nullptr;
+  }
 
   const double runtime = elapsed_since(c.start);
   printf("\nruntime: %f\n", runtime);
