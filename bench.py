@@ -171,6 +171,10 @@ class ClockSampler:
 # 8.39 M grid points); traffic grows with the grid points, so the full-size workload's
 # figure is this one scaled by its points.
 NCU_POINTS = 256 * 256 * 128
+# DRAM bytes per launch of the defect-line grid passes on the 128^3 workload frames, from
+# one ncu capture (`ncu --set full -k regex:"k_(faces|hook|corr)" ... bench.py --workload
+# lines_cgle3d_128 --steps 1 --warmup 3`): k_faces reads the 16.8 MB phase field once.
+NCU_TRAFFIC_LINES = {"faces": 16.8e6}
 NCU_TRAFFIC_3D = {"fwd_x": 772.5e6, "c2c_axis1_fwd": 218.7e6, "mid_axis0": 234.5e6, "c2c_axis1_inv": 218.7e6,
                   "inv_x_dictionary": 374.7e6}
 
@@ -717,7 +721,7 @@ def run_lines(args, rank=0, world=1, local_rank=0):
         e1.synchronize()
     sec = e0.elapsed_time(e1) / 1e3
     launches = sum(h.info()[2] for h in hs) - launches0
-    # one find alone, CUDA events on its stream
+    # one find alone, CUDA events on its stream, and its passes (rdcu_lines_profile)
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     f0.record(streams[0])
@@ -726,6 +730,8 @@ def run_lines(args, rank=0, world=1, local_rank=0):
     f1.record(streams[0])
     f1.synchronize()
     find_s = f0.elapsed_time(f1) / 1e3 / 8
+    passes = hs[0].profile(frames[W + 1], STATE, reps=10)
+    top = max(passes, key=lambda p: p[1])
     work = float(K * F)
     if world > 1:
         sec, work = combine_ranks(sec, work, "cuda")
@@ -767,10 +773,14 @@ def run_lines(args, rank=0, world=1, local_rank=0):
         "clocks": clk.summary(),
         "e2e": {"value": e2e_work / e2e_s, "unit": "frames/s", "h2d_bytes_per_step": 16.0 * N * F,
                 "d2h_bytes_per_step": out_bytes / K, "seconds": e2e_s},
-        "roofline": {"bound": "hbm", "kernel": "rdcu_lines_find (grid passes + graph passes)",
-                     "achieved": find_bytes / find_s / 1e9, "peak": peak, "unit": "GB/s",
-                     "frac": find_bytes / find_s / 1e9 / peak, "peak_kind": peak_kind, "traffic": None,
-                     "algorithmic_bytes_per_launch": find_bytes, "find_ms": find_s * 1e3},
+        "roofline": {"bound": "hbm", "kernel": "rdcu_lines_find pass '%s'" % top[0],
+                     "achieved": top[2] / (top[1] / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": top[2] / (top[1] / 1e3) / 1e9 / peak, "peak_kind": peak_kind,
+                     "traffic": NCU_TRAFFIC_LINES.get(top[0]), "algorithmic_bytes_per_launch": top[2],
+                     "launch_ms": top[1], "find_ms": find_s * 1e3,
+                     "find_achieved_GBps": find_bytes / find_s / 1e9,
+                     "passes": [{"name": a, "ms": b, "bytes": c, "GBps": c / (b / 1e3) / 1e9 if b > 0 else None,
+                                 "share": b / sum(p[1] for p in passes)} for a, b, c in passes]},
         "cpu_baseline": cpu,
     }
 

@@ -287,6 +287,8 @@ int rdcu_rhs_noalloc(const rdcu_spec *spec, const double *y, double *f, void *st
  *   RDCU_LINES_STATE, or the phase field theta (N doubles) when RDCU_LINES_PHASE.
  *   Outputs the number of line cubes, edges and components.  Components are numbered
  *   by their smallest cube (networkx's connected_components order).
+ * rdcu_lines_edges / rdcu_lines_cubes write arrays sized by the counts of the handle's
+ *   last frame (rdcu_lines_find's outputs; rdcu_lines_profile finds the same frame).
  * rdcu_lines_edges: xyz[n_edges][2][3] (host or device) -- edge (u, v), u < v, of every
  *   component as cube coordinates c scaled (c * L) / (N - 1), components in order, each
  *   component's edges in ascending (u, v) order -- and comp_offsets[n_components + 1]
@@ -300,6 +302,10 @@ int rdcu_rhs_noalloc(const rdcu_spec *spec, const double *y, double *f, void *st
  *   does (rounded for prev, truncated toward zero for cur).
  * rdcu_lines_correlate_sets: the same matrix for explicit cube sets (C-order indices
  *   grouped by component, offsets n + 1 starting at 0, host or device), on l's grid.
+ * rdcu_lines_profile: one rdcu_lines_find on src, then `reps` runs of its launches with
+ *   CUDA events between the pass groups (phase, faces, mark, compact, components, sort,
+ *   edges; phase only for RDCU_LINES_STATE): mean ms and algorithmic bytes of each, as
+ *   rdcu_profile_passes reports them.  The handle keeps that frame's results.
  * rdcu_lines_info: the handle's stream (cudaStream_t), device bytes and the number of
  *   kernels it has launched. */
 #define RDCU_LINES_STATE 0
@@ -315,6 +321,8 @@ int rdcu_lines_correlate(rdcu_lines_t *prev, rdcu_lines_t *cur, long long *diffs
 int rdcu_lines_correlate_sets(rdcu_lines_t *l, const long long *prev_cubes, const long long *prev_offsets,
                               long long n_prev, const long long *cur_cubes, const long long *cur_offsets,
                               long long n_cur, long long *diffs);
+int rdcu_lines_profile(rdcu_lines_t *l, const double *src, int kind, int reps, rdcu_pass_timing *out, int max_passes,
+                       int *npass);
 int rdcu_lines_info(rdcu_lines_t *l, void **stream, long long *device_bytes, long long *launches);
 /* Last error message of the handle (or of the last failed rdcu_lines_create when l is
  * NULL). */

@@ -47,7 +47,7 @@ EXPORTS = [
     "rdcu_ensemble_create", "rdcu_ensemble_destroy", "rdcu_ensemble_set_state", "rdcu_ensemble_get_state",
     "rdcu_ensemble_solve", "rdcu_ensemble_counters", "rdcu_ensemble_tune", "rdcu_ensemble_info",
     "rdcu_ensemble_last_error", "rdcu_lines_create", "rdcu_lines_destroy", "rdcu_lines_find", "rdcu_lines_edges",
-    "rdcu_lines_cubes", "rdcu_lines_correlate", "rdcu_lines_correlate_sets", "rdcu_lines_info",
+    "rdcu_lines_cubes", "rdcu_lines_correlate", "rdcu_lines_correlate_sets", "rdcu_lines_profile", "rdcu_lines_info",
     "rdcu_lines_last_error", "rdcu_error_string", "rdcu_last_error",
 ]
 _STRING_RESULTS = ("rdcu_error_string", "rdcu_last_error", "rdcu_ensemble_last_error", "rdcu_lines_last_error")
@@ -144,6 +144,7 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
     lib.rdcu_lines_cubes.argtypes = [vp, vp, vp]
     lib.rdcu_lines_correlate.argtypes = [vp, vp, vp]
     lib.rdcu_lines_correlate_sets.argtypes = [vp, vp, vp, ll, vp, vp, ll, vp]
+    lib.rdcu_lines_profile.argtypes = [vp, vp, i, i, ctypes.POINTER(rdcu_pass_timing), i, pi]
     lib.rdcu_lines_info.argtypes = [vp, ctypes.POINTER(vp), pll, pll]
     lib.rdcu_lines_last_error.argtypes = [vp]
     lib.rdcu_lines_last_error.restype = ctypes.c_char_p

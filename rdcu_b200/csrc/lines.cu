@@ -289,6 +289,99 @@ __global__ void __launch_bounds__(kT) k_roots(const int* __restrict__ label, con
   }
 }
 
+// The components of a frame with few line cubes in one CTA: the forest, its roots and
+// their numbering in shared memory (atomics and root walks at shared-memory latency), the
+// same union-find rules as k_hook / k_flatten / k_roots / k_label, so the labels and the
+// component numbers are identical.  Writes deg, comp, key, order and the component count
+// to *n_comp.
+constexpr int kSmallThreads = 1024;
+constexpr int kSmallNodes = 12288;  // 2 x 4 B per node of shared memory (96 KB)
+
+__device__ int uf_find_s(int* parent, int x, int* err) {
+  volatile int* P = parent;
+  for (int it = 0; it < kUfLimit; ++it) {
+    const int p = P[x];
+    if (p == x) return x;
+    const int gp = P[p];
+    if (gp != p) P[x] = gp;
+    x = gp;
+  }
+  atomicExch(err, 1);
+  return -1;
+}
+
+__global__ void __launch_bounds__(kSmallThreads) k_components_small(const int* __restrict__ cubes,
+                                                                     const int* __restrict__ node_of,
+                                                                     int* __restrict__ deg, int* __restrict__ comp,
+                                                                     int* __restrict__ key, int* __restrict__ order,
+                                                                     int n, Grid g, int* err, int* n_comp) {
+  extern __shared__ int sm_int[];
+  int* parent = sm_int;          // [n]
+  int* croot = sm_int + n;       // [n]: label, then component of each root
+  __shared__ int red[kSmallThreads / 32];
+  __shared__ int run;
+  for (int v = threadIdx.x; v < n; v += kSmallThreads) parent[v] = v;
+  __syncthreads();
+  for (int v = threadIdx.x; v < n; v += kSmallThreads) {
+    int nb[6];
+    const int cnt = face_neighbours(g, cubes[v], nb);
+    int d = 0;
+    for (int q = 0; q < cnt; ++q) {
+      const int u = node_of[nb[q]];
+      if (u <= v) continue;
+      ++d;
+      int a = v, b = u;
+      for (int it = 0; it < kUfRetries; ++it) {
+        a = uf_find_s(parent, a, err);
+        b = uf_find_s(parent, b, err);
+        if (a < 0 || b < 0 || a == b) break;
+        if (a < b) {
+          const int t = a;
+          a = b;
+          b = t;
+        }
+        if (atomicCAS(parent + a, a, b) == a) break;
+        if (it == kUfRetries - 1) atomicExch(err, 1);
+      }
+    }
+    deg[v] = d;
+  }
+  __syncthreads();
+  for (int v = threadIdx.x; v < n; v += kSmallThreads) {
+    int r = uf_find_s(parent, v, err);
+    croot[v] = r < 0 ? v : r;
+  }
+  __syncthreads();
+  for (int v = threadIdx.x; v < n; v += kSmallThreads) parent[v] = croot[v];  // labels
+  if (threadIdx.x == 0) run = 0;
+  __syncthreads();
+  // roots numbered in node order: ordered block scan over rounds of kSmallThreads
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int base = 0; base < n; base += kSmallThreads) {
+    const int v = base + threadIdx.x;
+    const bool f = v < n && parent[v] == v;
+    const unsigned b = __ballot_sync(0xffffffffu, f);
+    if (lane == 0) red[w] = __popc(b);
+    __syncthreads();
+    int off = 0, tot = 0;
+    for (int q = 0; q < kSmallThreads / 32; ++q) {
+      off += (q < w) ? red[q] : 0;
+      tot += red[q];
+    }
+    if (f) croot[v] = run + off + __popc(b & ((1u << lane) - 1u));
+    __syncthreads();
+    if (threadIdx.x == 0) run += tot;
+    __syncthreads();
+  }
+  for (int v = threadIdx.x; v < n; v += kSmallThreads) {
+    const int c = croot[parent[v]];
+    comp[v] = c;
+    key[v] = c;
+    order[v] = v;
+  }
+  if (threadIdx.x == 0) *n_comp = run;
+}
+
 __global__ void __launch_bounds__(kT) k_label(const int* __restrict__ label, const int* __restrict__ comp_of_root,
                                               int* __restrict__ comp, int* __restrict__ key, int* __restrict__ order,
                                               int n) {
@@ -661,6 +754,11 @@ class LinesEngine {
       cudaGetLastError();
       return fail(msg, "cannot create a stream on the device");
     }
+    if (cudaFuncSetAttribute(k_components_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kSmallNodes * 2 * (int)sizeof(int)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(msg, "cannot configure shared memory");
+    }
     const long long N = g.total;
     if (!th_.ensure(N, &device_bytes, st) || !src_.ensure(2 * N, &device_bytes, st) ||
         !face_.ensure(N, &device_bytes, st) || !mark_.ensure(N, &device_bytes, st) ||
@@ -725,11 +823,7 @@ class LinesEngine {
     if (n > 0) {
       const int nn = (int)n;
       const int nbn = nblocks(n, kChunk);
-      launch(k_hook, nblocks(n, kT), kT, cubes_.p, node_of_.p, parent_.p, deg_.p, nn, g, flags_.p);
-      launch(k_flatten, nbn, kT, parent_.p, label_.p, nn, counts_.p, flags_.p);
-      if ((rc = scan(counts_.p, nbn, msg))) return rc;
-      launch(k_roots, nbn, kT, label_.p, counts_.p, root_comp_.p, nn);
-      launch(k_label, nblocks(n, kT), kT, label_.p, root_comp_.p, comp_.p, key_a_.p, order_.p, nn);
+      if ((rc = components(nn, msg))) return rc;
       const long long nc = read_total(msg);
       if (nc < 0) return RDCU_ERR_CUDA;
       n_comp = nc;
@@ -760,6 +854,78 @@ class LinesEngine {
     }
     if (!ck(cudaGetLastError(), msg)) return RDCU_ERR_CUDA;
     have = true;
+    return RDCU_OK;
+  }
+
+  // Times the passes of find on src: one find for the sizes, then `reps` runs of the same
+  // launches (no host reads; the sizes are known) with CUDA events between the groups.
+  // Each entry: name, mean ms, algorithmic bytes (grid passes: bytes per point x N; the
+  // graph groups: the arrays they must read and write once per node or edge).
+  struct PassTime {
+    const char* name;
+    double ms, bytes;
+  };
+  int profile(const double* src, int kind, bool on_device, int reps, std::vector<PassTime>* out, std::string* msg) {
+    int rc = find(src, kind, on_device, msg);
+    if (rc) return rc;
+    const int N = g.total, nb = nblocks(N, kChunk);
+    const int nn = (int)n_cubes, nbn = nblocks(n_cubes, kChunk), nc = (int)n_comp, ne = (int)n_edges;
+    const double* d = on_device ? src : src_.p;
+    const double* th = kind == RDCU_LINES_STATE ? th_.p : d;
+    const char* names[7] = {"phase", "faces", "mark", "compact", "components", "sort", "edges"};
+    int passes = 0;
+    for (int shift = 0; nc > 1 && ((nc - 1) >> shift) > 0; shift += 8) ++passes;
+    const double bytes[7] = {kind == RDCU_LINES_STATE ? 24.0 * N : 0.0, 9.0 * N, 2.0 * N,
+                             5.0 * N + 12.0 * nn, 48.0 * nn, 16.0 * passes * nn, 28.0 * nn + 48.0 * ne};
+    cudaEvent_t ev[8];
+    for (auto& e : ev)
+      if (!ck(cudaEventCreate(&e), msg)) return RDCU_ERR_CUDA;
+    std::vector<double> acc(7, 0.0);
+    for (int r = 0; r < reps && rc == RDCU_OK; ++r) {
+      cudaEventRecord(ev[0], st);
+      if (kind == RDCU_LINES_STATE) launch(k_phase, nblocks(N, kT), kT, d, th_.p, N);
+      cudaEventRecord(ev[1], st);
+      launch(k_faces, nblocks(N, kT), kT, th, face_.p, g);
+      cudaEventRecord(ev[2], st);
+      launch(k_mark, nb, kT, face_.p, mark_.p, counts_.p, g);
+      rc = scan(counts_.p, nb, msg);
+      cudaEventRecord(ev[3], st);
+      launch(k_compact, nb, kT, mark_.p, counts_.p, cubes_.p, node_of_.p, parent_.p, N);
+      cudaEventRecord(ev[4], st);
+      if (nn > 0 && rc == RDCU_OK) {
+        cudaMemsetAsync(flags_.p, 0, sizeof(int), st);
+        rc = components(nn, msg);
+      }
+      cudaEventRecord(ev[5], st);
+      int *k0 = key_a_.p, *v0 = order_.p, *k1 = key_b_.p, *v1 = val_tmp_.p;
+      for (int shift = 0; nn > 0 && rc == RDCU_OK && ((nc - 1) >> shift) > 0; shift += 8) {
+        launch(k_rs_hist, nbn, kT, k0, nn, shift, hist_.p, nbn);
+        rc = scan(hist_.p, 256 * nbn, msg);
+        launch(k_rs_scatter, nbn, kT, k0, v0, k1, v1, nn, shift, hist_.p, nbn);
+        std::swap(k0, k1);
+        std::swap(v0, v1);
+      }
+      cudaEventRecord(ev[6], st);
+      if (nn > 0 && rc == RDCU_OK) {
+        launch(k_edge_counts, nblocks(nn, kT), kT, v0, deg_.p, eoff_.p, nn);
+        rc = scan(eoff_.p, nn, msg);
+        launch(k_edges, nblocks(nn, kT), kT, v0, eoff_.p, cubes_.p, node_of_.p, comp_.p, g, xyz_.p, comp_noff_.p,
+               comp_eoff_.p, nn, nc, ne);
+      }
+      cudaEventRecord(ev[7], st);
+      if (!ck(cudaEventSynchronize(ev[7]), msg)) rc = RDCU_ERR_CUDA;
+      for (int i = 0; i < 7 && rc == RDCU_OK; ++i) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
+        acc[i] += ms;
+      }
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    if (rc) return rc;
+    if (!ck(cudaGetLastError(), msg)) return RDCU_ERR_CUDA;
+    out->clear();
+    for (int i = 0; i < 7; ++i)
+      if (i > 0 || kind == RDCU_LINES_STATE) out->push_back({names[i], acc[i] / reps, bytes[i]});
     return RDCU_OK;
   }
 
@@ -881,6 +1047,11 @@ class LinesEngine {
     k<<<grid, block, 0, st>>>(args...);
     ++launches;
   }
+  template <typename... KA, typename... A>
+  void launch_smem(void (*k)(KA...), dim3 grid, int block, size_t smem, A... args) {
+    k<<<grid, block, smem, st>>>(args...);
+    ++launches;
+  }
   static bool fail(std::string* msg, const char* m) {
     *msg = m;
     return false;
@@ -905,10 +1076,26 @@ class LinesEngine {
       if (!b->ensure(n, &device_bytes, st)) return false;
     return hist_.ensure(256ll * (nblocks(n, kChunk) + 1), &device_bytes, st);
   }
+  // components of the n >= 1 line cubes (after k_compact): deg, comp, key_a_ and order_,
+  // the component count in flags_[1].  One CTA in shared memory for small frames.
+  int components(int n, std::string* msg) {
+    if (n <= kSmallNodes) {
+      launch_smem(k_components_small, 1, kSmallThreads, (size_t)n * 2 * sizeof(int), (const int*)cubes_.p,
+                  (const int*)node_of_.p, deg_.p, comp_.p, key_a_.p, order_.p, n, g, flags_.p, flags_.p + 1);
+      return ck(cudaGetLastError(), msg) ? RDCU_OK : RDCU_ERR_CUDA;
+    }
+    const int nbn = nblocks(n, kChunk);
+    launch(k_hook, nblocks(n, kT), kT, cubes_.p, node_of_.p, parent_.p, deg_.p, n, g, flags_.p);
+    launch(k_flatten, nbn, kT, parent_.p, label_.p, n, counts_.p, flags_.p);
+    if (int rc = scan(counts_.p, nbn, msg)) return rc;
+    launch(k_roots, nbn, kT, label_.p, counts_.p, root_comp_.p, n);
+    launch(k_label, nblocks(n, kT), kT, label_.p, root_comp_.p, comp_.p, key_a_.p, order_.p, n);
+    return RDCU_OK;
+  }
   // exclusive scan of a[0..n) in place; the total goes to flags_[1]
   int scan(int* a, int n, std::string* msg) {
     const int nb = nblocks(n, kChunk);
-    if (nb <= 1) {
+    if (n <= 8 * 1024) {  // a few rounds of one block beat three launches
       launch(k_scan_one, 1, 1024, a, n, flags_.p + 1);
     } else {
       if (!sums_.ensure(nb, &device_bytes, st)) return fail_code(msg, "device memory", RDCU_ERR_NOMEM);
@@ -1042,6 +1229,25 @@ int rdcu_lines_correlate_sets(rdcu_lines_t* l, const long long* prev_cubes, cons
   std::string msg;
   const int rc = l->eng.correlate_sets(prev_cubes, prev_offsets, n_prev, cur_cubes, cur_offsets, n_cur, diffs, &msg);
   return rc ? lines_err(l, rc, "rdcu_lines_correlate_sets: " + msg) : RDCU_OK;
+}
+
+int rdcu_lines_profile(rdcu_lines_t* l, const double* src, int kind, int reps, rdcu_pass_timing* out, int max_passes,
+                       int* npass) {
+  if (!l || !src || !out || !npass || reps < 1) return lines_err(l, RDCU_ERR_INVALID, "bad argument");
+  if (kind != RDCU_LINES_STATE && kind != RDCU_LINES_PHASE) return lines_err(l, RDCU_ERR_INVALID, "unknown source kind");
+  if (int rc = lines_activate(l)) return rc;
+  std::string msg;
+  std::vector<rdcu::LinesEngine::PassTime> pt;
+  const int rc = l->eng.profile(src, kind, on_device(src), reps, &pt, &msg);
+  if (rc) return lines_err(l, rc, "rdcu_lines_profile: " + msg);
+  const int m = std::min((int)pt.size(), max_passes);
+  for (int i = 0; i < m; ++i) {
+    out[i].name = pt[i].name;
+    out[i].ms = pt[i].ms;
+    out[i].bytes = pt[i].bytes;
+  }
+  *npass = m;
+  return RDCU_OK;
 }
 
 int rdcu_lines_info(rdcu_lines_t* l, void** stream, long long* device_bytes, long long* launches) {

@@ -158,6 +158,20 @@ class Lines:
             ctypes.c_void_p(out.ctypes.data if out.size else 0)))
         return out
 
+    def profile(self, src, kind: int = STATE, reps: int = 5) -> List[Tuple[str, float, float]]:
+        """(pass, mean ms, algorithmic bytes) of each pass group of one find on ``src``.
+        The handle keeps that frame (its counts are refreshed here, since ``edges`` and
+        ``cubes`` size their arrays from them)."""
+        from . import rdcu_pass_timing
+
+        self.find(src, kind)
+        p, keep = _ptr(src)
+        arr = (rdcu_pass_timing * 16)()
+        n = ctypes.c_int()
+        self._check(self.lib.rdcu_lines_profile(self.h, ctypes.c_void_p(p), kind, reps, arr, 16, ctypes.byref(n)))
+        del keep
+        return [(arr[i].name.decode(), arr[i].ms, arr[i].bytes) for i in range(n.value)]
+
     def info(self) -> Tuple[int, int, int]:
         """(stream address, device bytes, kernels launched so far)."""
         st, b, k = ctypes.c_void_p(), ctypes.c_longlong(), ctypes.c_longlong()

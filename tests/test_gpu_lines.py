@@ -192,3 +192,16 @@ def test_driver_end_to_end(cuda, tmp_path):
         assert np.array_equal(diffs[n - 1], ol.correlate(lines[n - 1], lines[n], Ns, Ls)), n
     i2, c2, e2 = ancestry(lines, diffs, a.thr)
     assert all(np.array_equal(x, y) for x, y in zip(ids, i2)) and edges == e2
+
+
+def test_profile_passes(cuda):
+    """rdcu_lines_profile times the pass groups of one find and leaves that frame's results."""
+    Ns, Ls = (32, 24, 40), (20.0, 15.0, 25.0)
+    y = defect_state(Ns, 21, 0, 3, 0.1)
+    h = _lines(Ns, Ls)
+    p = h.profile(y, 0, reps=3)
+    assert [x[0] for x in p] == ["phase", "faces", "mark", "compact", "components", "sort", "edges"]
+    assert all(ms > 0 for _, ms, _ in p) and p[1][2] == 9.0 * np.prod(Ns)
+    assert same_components(h.lines(), ol.findlines(ol.phase(y, Ns), Ns, Ls), Ns, Ls)
+    assert [x[0] for x in h.profile(ol.phase(y, Ns), 1, reps=2)][0] == "faces"
+    h.close()
