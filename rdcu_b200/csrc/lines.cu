@@ -241,20 +241,24 @@ __device__ void uf_union(int* parent, int a, int b, int* err) {
 }
 
 __global__ void __launch_bounds__(kT) k_hook(const int* __restrict__ cubes, const int* __restrict__ node_of,
-                                             int* parent, int* __restrict__ deg, int n, Grid g, int* err) {
+                                             int* parent, int* __restrict__ deg, int n, Grid g, int* err,
+                                             int* n_edges) {
   const int v = blockIdx.x * kT + threadIdx.x;
-  if (v >= n) return;
-  int nb[6];
-  const int cnt = face_neighbours(g, cubes[v], nb);
   int d = 0;
-  for (int q = 0; q < cnt; ++q) {
-    const int u = node_of[nb[q]];
-    if (u > v) {
-      ++d;
-      uf_union(parent, v, u, err);
+  if (v < n) {
+    int nb[6];
+    const int cnt = face_neighbours(g, cubes[v], nb);
+    for (int q = 0; q < cnt; ++q) {
+      const int u = node_of[nb[q]];
+      if (u > v) {
+        ++d;
+        uf_union(parent, v, u, err);
+      }
     }
+    deg[v] = d;
   }
-  deg[v] = d;
+  for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+  if ((threadIdx.x & 31) == 0 && d) atomicAdd(n_edges, d);
 }
 
 __global__ void __launch_bounds__(kT) k_flatten(int* parent, int* __restrict__ label, int n, int* counts, int* err) {
@@ -314,7 +318,8 @@ __global__ void __launch_bounds__(kSmallThreads) k_components_small(const int* _
                                                                      const int* __restrict__ node_of,
                                                                      int* __restrict__ deg, int* __restrict__ comp,
                                                                      int* __restrict__ key, int* __restrict__ order,
-                                                                     int n, Grid g, int* err, int* n_comp) {
+                                                                     int n, Grid g, int* err, int* n_comp,
+                                                                     int* n_edges) {
   extern __shared__ int sm_int[];
   int* parent = sm_int;          // [n]
   int* croot = sm_int + n;       // [n]: label, then component of each root
@@ -322,6 +327,7 @@ __global__ void __launch_bounds__(kSmallThreads) k_components_small(const int* _
   __shared__ int run;
   for (int v = threadIdx.x; v < n; v += kSmallThreads) parent[v] = v;
   __syncthreads();
+  int dsum = 0;
   for (int v = threadIdx.x; v < n; v += kSmallThreads) {
     int nb[6];
     const int cnt = face_neighbours(g, cubes[v], nb);
@@ -345,7 +351,10 @@ __global__ void __launch_bounds__(kSmallThreads) k_components_small(const int* _
       }
     }
     deg[v] = d;
+    dsum += d;
   }
+  for (int o = 16; o > 0; o >>= 1) dsum += __shfl_xor_sync(0xffffffffu, dsum, o);
+  if ((threadIdx.x & 31) == 0 && dsum) atomicAdd(n_edges, dsum);
   __syncthreads();
   for (int v = threadIdx.x; v < n; v += kSmallThreads) {
     int r = uf_find_s(parent, v, err);
@@ -818,18 +827,26 @@ class LinesEngine {
     n_cubes = n;
     n_edges = n_comp = 0;
     if (!ensure_nodes(n)) return fail_code(msg, "device memory", RDCU_ERR_NOMEM);
-    if (!ck(cudaMemsetAsync(flags_.p, 0, sizeof(int), st), msg)) return RDCU_ERR_CUDA;
+    if (!ck(cudaMemsetAsync(flags_.p, 0, 3 * sizeof(int), st), msg)) return RDCU_ERR_CUDA;
     launch(k_compact, nb, kT, mark_.p, counts_.p, cubes_.p, node_of_.p, parent_.p, N);
     if (n > 0) {
       const int nn = (int)n;
       const int nbn = nblocks(n, kChunk);
       if ((rc = components(nn, msg))) return rc;
-      const long long nc = read_total(msg);
-      if (nc < 0) return RDCU_ERR_CUDA;
+      // one read: union-find error flag, component count, edge count
+      int* hf = reinterpret_cast<int*>(h_small_);
+      if (!ck(cudaMemcpyAsync(hf, flags_.p, 3 * sizeof(int), cudaMemcpyDeviceToHost, st), msg) ||
+          !ck(cudaStreamSynchronize(st), msg))
+        return RDCU_ERR_CUDA;
+      if (hf[0] != 0) return fail_code(msg, "union-find iteration bound reached", RDCU_ERR_TIMEOUT);
+      const long long nc = hf[1], ne = hf[2];
       n_comp = nc;
-      if (!comp_noff_.ensure(nc + 1, &device_bytes, st) || !comp_eoff_.ensure(nc + 1, &device_bytes, st))
+      n_edges = ne;
+      if (!comp_noff_.ensure(nc + 1, &device_bytes, st) || !comp_eoff_.ensure(nc + 1, &device_bytes, st) ||
+          !xyz_.ensure(ne * 6, &device_bytes, st))
         return fail_code(msg, "device memory", RDCU_ERR_NOMEM);
-      // nodes stably sorted by component, 8 bits a pass
+      // nodes stably sorted by component, 8 bits a pass; then the edges (no further host
+      // reads: edges(), cubes() and correlate() synchronise before using the results)
       int *k0 = key_a_.p, *v0 = order_.p, *k1 = key_b_.p, *v1 = val_tmp_.p;
       for (int shift = 0; ((nc - 1) >> shift) > 0; shift += 8) {
         launch(k_rs_hist, nbn, kT, k0, nn, shift, hist_.p, nbn);
@@ -841,16 +858,8 @@ class LinesEngine {
       sorted_ = v0;
       launch(k_edge_counts, nblocks(n, kT), kT, sorted_, deg_.p, eoff_.p, nn);
       if ((rc = scan(eoff_.p, nn, msg))) return rc;
-      const long long ne = read_total(msg);
-      if (ne < 0) return RDCU_ERR_CUDA;
-      n_edges = ne;
-      if (!xyz_.ensure(ne * 6, &device_bytes, st)) return fail_code(msg, "device memory", RDCU_ERR_NOMEM);
       launch(k_edges, nblocks(n, kT), kT, sorted_, eoff_.p, cubes_.p, node_of_.p, comp_.p, g, xyz_.p, comp_noff_.p,
              comp_eoff_.p, nn, (int)nc, (int)ne);
-      if (!ck(cudaMemcpyAsync(h_small_, flags_.p, sizeof(int), cudaMemcpyDeviceToHost, st), msg) ||
-          !ck(cudaStreamSynchronize(st), msg))
-        return RDCU_ERR_CUDA;
-      if (*(int*)h_small_ != 0) return fail_code(msg, "union-find iteration bound reached", RDCU_ERR_TIMEOUT);
     }
     if (!ck(cudaGetLastError(), msg)) return RDCU_ERR_CUDA;
     have = true;
@@ -893,7 +902,7 @@ class LinesEngine {
       launch(k_compact, nb, kT, mark_.p, counts_.p, cubes_.p, node_of_.p, parent_.p, N);
       cudaEventRecord(ev[4], st);
       if (nn > 0 && rc == RDCU_OK) {
-        cudaMemsetAsync(flags_.p, 0, sizeof(int), st);
+        cudaMemsetAsync(flags_.p, 0, 3 * sizeof(int), st);
         rc = components(nn, msg);
       }
       cudaEventRecord(ev[5], st);
@@ -1077,15 +1086,17 @@ class LinesEngine {
     return hist_.ensure(256ll * (nblocks(n, kChunk) + 1), &device_bytes, st);
   }
   // components of the n >= 1 line cubes (after k_compact): deg, comp, key_a_ and order_,
-  // the component count in flags_[1].  One CTA in shared memory for small frames.
+  // the component count in flags_[1], the edge count added to flags_[2] (zeroed by the
+  // caller).  One CTA in shared memory for small frames.
   int components(int n, std::string* msg) {
     if (n <= kSmallNodes) {
       launch_smem(k_components_small, 1, kSmallThreads, (size_t)n * 2 * sizeof(int), (const int*)cubes_.p,
-                  (const int*)node_of_.p, deg_.p, comp_.p, key_a_.p, order_.p, n, g, flags_.p, flags_.p + 1);
+                  (const int*)node_of_.p, deg_.p, comp_.p, key_a_.p, order_.p, n, g, flags_.p, flags_.p + 1,
+                  flags_.p + 2);
       return ck(cudaGetLastError(), msg) ? RDCU_OK : RDCU_ERR_CUDA;
     }
     const int nbn = nblocks(n, kChunk);
-    launch(k_hook, nblocks(n, kT), kT, cubes_.p, node_of_.p, parent_.p, deg_.p, n, g, flags_.p);
+    launch(k_hook, nblocks(n, kT), kT, cubes_.p, node_of_.p, parent_.p, deg_.p, n, g, flags_.p, flags_.p + 2);
     launch(k_flatten, nbn, kT, parent_.p, label_.p, n, counts_.p, flags_.p);
     if (int rc = scan(counts_.p, nbn, msg)) return rc;
     launch(k_roots, nbn, kT, label_.p, counts_.p, root_comp_.p, n);
