@@ -26,9 +26,11 @@ the 126 MB L2 (every stage moves ~0.27 GB arrays), so no L2 flush is needed.
 * ``cpu_baseline``: the oracle's numpy/scipy restatement (scipy.fft, all host cores) on
   one DP45 attempt of the same workload from the warm state.
 * ``--impl reference``: the reference's own nvcc sm_100a build (cuFFT/cuBLAS; the
-  reference has no CPU path) run twice, to W*TAU and to (W+K)*TAU; value = grid points
-  x (difference of accepted steps) / (difference of runtimes), so set-up and file output
-  cancel.
+  reference has no CPU path).  Its clock starts at program start, so set-up must stay out
+  of the window: 3D runs twice, to W*TAU and to (W+K)*TAU (grids up to 2M points: a
+  window ten times as long), value = grid points x (difference of accepted steps) /
+  (difference of runtimes); 2D runs once with outputs every W*TAU and takes the rate
+  between the progress lines at W*TAU and at the end.
 
 Multi-GPU (torchrun, N > 1): replicas.  The problem does not shard; every rank
 integrates its own copy, timing is the max over ranks, value is the sum of all ranks'
@@ -936,35 +938,61 @@ def run_reference(args):
     wl = WORKLOADS[args.workload]
     Ns, Ls = wl["Ns"], wl["Ls"]
     N = int(np.prod(Ns))
-    T_A, T_B = args.warmup * TAU, (args.warmup + args.steps) * TAU
+    T_A = args.warmup * TAU
+    # The reference times from program start (CUDA and cuFFT set-up included), so the
+    # window must not contain set-up, nor let its run-to-run variance dominate:
+    # 2D: one run with outputs every T_A, rate between the progress lines at T_A and at
+    #     the end (the outputs of these small grids cost nothing noticeable);
+    # 3D: two runs, to T_A and to T_B, differenced; grids up to 2M points use a window
+    #     ten times the bench's (the reference then integrates ~15 s in it).
+    mult = 10 if (len(Ns) == 3 and N <= (1 << 21)) else 1
+    T_B = (args.warmup + mult * args.steps) * TAU
 
-    def one(T):
+    def one(T, dt):
         with tempfile.TemporaryDirectory() as wd:
             fb = os.path.join(wd, "bench")
             open(fb + "coupling.dat", "w").write("\n".join(cgle_lines(len(Ns))) + "\n")
             # -D1 (the reference writes times.dat unconditionally at outputs, so -D0
-            # crashes it); one output at T; first step h0 as in our arm
+            # crashes it); first step h0 as in our arm
             cmd = [exe, "-n", "2", "-N", ",".join(map(str, Ns)), "-L", ",".join("%g" % l for l in Ls),
-                   "-A", "2", "-s", str(wl["seed"]), "-t", repr(T), "-d", "%r,%r" % (T, wl["h0"]), "-D1", fb]
+                   "-A", "2", "-s", str(wl["seed"]), "-t", repr(T), "-d", "%r,%r" % (dt, wl["h0"]), "-D1", fb]
             r = subprocess.run(cmd, capture_output=True, text=True, timeout=3600)
-            out = open(fb + ".out").read()
-            steps = int(re.search(r"steps: (\d+)", out).group(1))
-            runtime = float(re.search(r"runtime: ([0-9.]+)", out).group(1))
-            return steps, runtime, r.returncode, " ".join(shlex.quote(c) for c in cmd)
+            out = open(fb + ".out").read() if os.path.exists(fb + ".out") else ""
+            m = re.search(r"steps: (\d+)", out)
+            rt = re.search(r"runtime: ([0-9.]+)", out)
+            prog = []
+            for line in out.splitlines():
+                f = line.split("\t")
+                if len(f) >= 5 and re.fullmatch(r"[0-9.]+", f[0]):
+                    prog.append((float(f[1]), int(f[4])))
+            return (int(m.group(1)) if m else -1, float(rt.group(1)) if rt else -1.0, prog, r.returncode,
+                    " ".join(shlex.quote(c) for c in cmd))
 
-    sA, rA, cA, cmdA = one(T_A)
-    sB, rB, cB, cmdB = one(T_B)
-    if cA != 0 or cB != 0:
-        return {"impl": "reference", "unavailable": "reference run failed (rc %d/%d)" % (cA, cB)}
-    value = N * (sB - sA) / (rB - rA)
-    sample = ("reference nvcc sm_100a build (cuFFT/cuBLAS), runs to t=%g (%d steps, %.2f s) and t=%g "
-              "(%d steps, %.2f s); difference = the window" % (T_A, sA, rA, T_B, sB, rB))
+    if len(Ns) == 2:
+        sB, rB, prog, cB, cmdB = one(T_B, T_A)
+        if cB != 0 or len(prog) < 2:
+            return {"impl": "reference", "unavailable": "reference run failed (rc %d, %d outputs)" % (cB, len(prog))}
+        (e0, s0), (e1, s1) = prog[0], prog[-1]
+        value = N * (s1 - s0) / (e1 - e0)
+        window_steps, window_s = s1 - s0, e1 - e0
+        sample = ("reference nvcc sm_100a build (cuFFT/cuBLAS), one run to t=%g with outputs every %g; rate "
+                  "between the progress lines at t=%g and t=%g (%d steps, %.3f s), set-up excluded"
+                  % (T_B, T_A, T_A, T_B, window_steps, window_s))
+    else:
+        sA, rA, _, cA, cmdA = one(T_A, T_A)
+        sB, rB, _, cB, cmdB = one(T_B, T_B)
+        if cA != 0 or cB != 0:
+            return {"impl": "reference", "unavailable": "reference run failed (rc %d/%d)" % (cA, cB)}
+        value = N * (sB - sA) / (rB - rA)
+        window_steps, window_s = sB - sA, rB - rA
+        sample = ("reference nvcc sm_100a build (cuFFT/cuBLAS), runs to t=%g (%d steps, %.2f s) and t=%g "
+                  "(%d steps, %.2f s); difference = the window" % (T_A, sA, rA, T_B, sB, rB))
     return {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "grid-pt·steps/s", "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": (rB - rA) * 1e3 / args.steps,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": window_s * 1e3 / (mult * args.steps),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": args.workload, "grid": list(Ns), "L": list(Ls), "window_sim_time": [T_A, T_B],
-                   "accepted_steps": sB - sA, "command": cmdB},
+                   "accepted_steps": window_steps, "window_s": window_s, "command": cmdB},
         "cpu_baseline": {"value": value, "unit": "grid-pt·steps/s", "cores": 1, "kind": "reference",
                          "sample": sample},
         "e2e": {"value": value, "unit": "grid-pt·steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
