@@ -31,7 +31,7 @@ constexpr double kPi = 3.141592653589793;  // the double nearest pi (numpy's np.
 constexpr double kTwoPi = 2.0 * kPi;
 constexpr int kT = 256;                     // threads per block
 constexpr int kChunk = 1024;                // items per block in counting, compaction, sorting
-constexpr int kRounds = kChunk / kT;
+constexpr int kRounds = kChunk / kT;          // slices of kT items per chunk
 constexpr int kUfLimit = 1 << 26;           // bound of a root walk (a path is shorter than the nodes)
 constexpr int kUfRetries = 1 << 20;         // bound of the CAS retries of one union
 
@@ -145,8 +145,8 @@ __global__ void __launch_bounds__(kT) k_mark(const unsigned char* __restrict__ f
   if (threadIdx.x == 0) counts[blockIdx.x] = s;
 }
 
-// Exclusive prefix of this round's flags over the block, in index order; returns the
-// block's total for the round.
+// Exclusive prefix of one slice's flags over the block, in index order; returns the
+// block's total for the slice.
 __device__ __forceinline__ int block_rank(bool f, int* wcnt, int* pre) {
   const unsigned b = __ballot_sync(0xffffffffu, f);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -364,7 +364,7 @@ __global__ void __launch_bounds__(kSmallThreads) k_components_small(const int* _
   for (int v = threadIdx.x; v < n; v += kSmallThreads) parent[v] = croot[v];  // labels
   if (threadIdx.x == 0) run = 0;
   __syncthreads();
-  // roots numbered in node order: ordered block scan over rounds of kSmallThreads
+  // roots numbered in node order: ordered block scan over slices of kSmallThreads
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (int base = 0; base < n; base += kSmallThreads) {
     const int v = base + threadIdx.x;
@@ -480,9 +480,9 @@ __global__ void __launch_bounds__(kT) k_rs_hist(const int* __restrict__ key, int
   hist[threadIdx.x * nblk + blockIdx.x] = h[threadIdx.x];
 }
 
-// Items of a chunk keep their order within a digit: each round's lanes are ranked among
-// equal digits of their warp (match_any), warps among the warps before them, rounds after
-// the rounds before them.
+// Items of a chunk keep their order within a digit: each slice's lanes are ranked among
+// equal digits of their warp (match_any), warps among the warps before them, slices after
+// the slices before them.
 __global__ void __launch_bounds__(kT) k_rs_scatter(const int* __restrict__ kin, const int* __restrict__ vin,
                                                    int* __restrict__ kout, int* __restrict__ vout, int n, int shift,
                                                    const int* __restrict__ hist, int nblk) {
