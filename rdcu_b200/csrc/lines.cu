@@ -31,7 +31,7 @@ constexpr double kPi = 3.141592653589793;  // the double nearest pi (numpy's np.
 constexpr double kTwoPi = 2.0 * kPi;
 constexpr int kT = 256;                     // threads per block
 constexpr int kChunk = 1024;                // items per block in counting, compaction, sorting
-constexpr int kRounds = kChunk / kT;          // slices of kT items per chunk
+constexpr int kSlices = kChunk / kT;          // slices of kT items per chunk
 constexpr int kUfLimit = 1 << 26;           // bound of a root walk (a path is shorter than the nodes)
 constexpr int kUfRetries = 1 << 20;         // bound of the CAS retries of one union
 
@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(kT) k_mark(const unsigned char* __restrict__ f
                                              int* __restrict__ counts, Grid g) {
   __shared__ int red[kT / 32];
   int cnt = 0;
-  for (int r = 0; r < kRounds; ++r) {
+  for (int r = 0; r < kSlices; ++r) {
     const int c = blockIdx.x * kChunk + r * kT + threadIdx.x;
     if (c < g.total) {
       int i, j, k;
@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(kT) k_compact(const unsigned char* __restrict_
                                                 int* __restrict__ parent, int total) {
   __shared__ int wcnt[kT / 32];
   int run = offs[blockIdx.x];
-  for (int r = 0; r < kRounds; ++r) {
+  for (int r = 0; r < kSlices; ++r) {
     const int c = blockIdx.x * kChunk + r * kT + threadIdx.x;
     const bool m = c < total && mark[c];
     int pre;
@@ -264,7 +264,7 @@ __global__ void __launch_bounds__(kT) k_hook(const int* __restrict__ cubes, cons
 __global__ void __launch_bounds__(kT) k_flatten(int* parent, int* __restrict__ label, int n, int* counts, int* err) {
   __shared__ int red[kT / 32];
   int cnt = 0;
-  for (int r = 0; r < kRounds; ++r) {
+  for (int r = 0; r < kSlices; ++r) {
     const int v = blockIdx.x * kChunk + r * kT + threadIdx.x;
     if (v < n) {
       int root = uf_find(parent, v, err);
@@ -283,7 +283,7 @@ __global__ void __launch_bounds__(kT) k_roots(const int* __restrict__ label, con
                                               int* __restrict__ comp_of_root, int n) {
   __shared__ int wcnt[kT / 32];
   int run = offs[blockIdx.x];
-  for (int r = 0; r < kRounds; ++r) {
+  for (int r = 0; r < kSlices; ++r) {
     const int v = blockIdx.x * kChunk + r * kT + threadIdx.x;
     const bool f = v < n && label[v] == v;
     int pre;
@@ -426,7 +426,7 @@ __device__ __forceinline__ int block_excl_scan(int v, int* red, int* total) {
 __global__ void __launch_bounds__(kT) k_chunk_sums(const int* __restrict__ a, int n, int* __restrict__ sums) {
   __shared__ int red[kT / 32];
   int s = 0;
-  for (int r = 0; r < kRounds; ++r) {
+  for (int r = 0; r < kSlices; ++r) {
     const int i = blockIdx.x * kChunk + r * kT + threadIdx.x;
     if (i < n) s += a[i];
   }
@@ -456,7 +456,7 @@ __global__ void __launch_bounds__(1024) k_scan_one(int* a, int n, int* total) {
 __global__ void __launch_bounds__(kT) k_chunk_scan(int* a, int n, const int* __restrict__ sums) {
   __shared__ int red[kT / 32];
   int run = sums[blockIdx.x];
-  for (int r = 0; r < kRounds; ++r) {
+  for (int r = 0; r < kSlices; ++r) {
     const int i = blockIdx.x * kChunk + r * kT + threadIdx.x;
     const int v = i < n ? a[i] : 0;
     int tot;
@@ -472,7 +472,7 @@ __global__ void __launch_bounds__(kT) k_rs_hist(const int* __restrict__ key, int
   __shared__ int h[256];
   h[threadIdx.x] = 0;
   __syncthreads();
-  for (int r = 0; r < kRounds; ++r) {
+  for (int r = 0; r < kSlices; ++r) {
     const int i = blockIdx.x * kChunk + r * kT + threadIdx.x;
     if (i < n) atomicAdd(&h[(key[i] >> shift) & 255], 1);
   }
@@ -492,7 +492,7 @@ __global__ void __launch_bounds__(kT) k_rs_scatter(const int* __restrict__ kin, 
   base[threadIdx.x] = hist[threadIdx.x * nblk + blockIdx.x];
   for (int q = 0; q < kT / 32; ++q) wc[q][threadIdx.x] = 0;
   __syncthreads();
-  for (int r = 0; r < kRounds; ++r) {
+  for (int r = 0; r < kSlices; ++r) {
     const int i = blockIdx.x * kChunk + r * kT + threadIdx.x;
     const bool ok = i < n;
     const int key = ok ? kin[i] : 0;
