@@ -681,7 +681,7 @@ def run_lines(args, rank=0, world=1, local_rank=0):
     frames/s.  ``value`` runs on frames resident in HBM (edge lists stay on the device,
     the small distance matrix comes back); ``e2e`` starts from pinned host frames and
     brings every frame's edge list and distance matrix to the host through the public
-    API.  On N GPUs each rank processes its own frame sequence (independent frames: no
+    API, each frame's copy staged (rdcu_lines_prefetch) while the previous one is found.  On N GPUs each rank processes its own frame sequence (independent frames: no
     exchange)."""
     import torch
 
@@ -741,11 +741,16 @@ def run_lines(args, rank=0, world=1, local_rank=0):
     host = frames.cpu().pin_memory()
     torch.cuda.synchronize()
     hs[(k0 - 1) % 2].find(host[(k0 - 1) % R], STATE)
+    hs[k0 % 2].prefetch(host[k0 % R], STATE)
     w0 = time.perf_counter()
     out_bytes = 0
     for k in range(k0, k1):
-        d = step(k, host)
-        xyz, off = hs[k % 2].edges()
+        cur, prev = hs[k % 2], hs[(k - 1) % 2]
+        if k + 1 < k1:  # frame k+1 copies into the previous frame's handle while k is found
+            prev.prefetch(host[(k + 1) % R], STATE)
+        cur.find(None, STATE)
+        d = cur.correlate(prev)
+        xyz, off = cur.edges()
         out_bytes += xyz.nbytes + off.nbytes + d.nbytes
     e2e_s = time.perf_counter() - w0
     e2e_work = float(K * F)

@@ -284,7 +284,13 @@ int rdcu_rhs_noalloc(const rdcu_spec *spec, const double *y, double *f, void *st
  *   `device`; the handle owns a stream and keeps the results of its last frame.
  * rdcu_lines_find: one frame.  src (host or device) is the state -- u block then v block,
  *   2*N doubles, C order, as one frame of states.dat (makelines.py:60-65) -- when kind is
- *   RDCU_LINES_STATE, or the phase field theta (N doubles) when RDCU_LINES_PHASE.
+ *   RDCU_LINES_STATE, or the phase field theta (N doubles) when RDCU_LINES_PHASE.  src
+ *   NULL takes the frame staged by rdcu_lines_prefetch (same kind).
+ * rdcu_lines_prefetch: starts copying a host frame (pinned memory, for the copy to
+ *   overlap other work) into the handle's staging buffer on a copy stream and returns;
+ *   the handle's current results stay valid (a two-handle sequence stages frame k+1 in
+ *   the previous frame's handle while frame k is found in the other).  The host array
+ *   must stay unchanged until the rdcu_lines_find that uses it.
  *   Outputs the number of line cubes, edges and components.  Components are numbered
  *   by their smallest cube (networkx's connected_components order).
  * rdcu_lines_edges / rdcu_lines_cubes write arrays sized by the counts of the handle's
@@ -315,6 +321,7 @@ int rdcu_lines_create(rdcu_lines_t **out, const int Ns[3], const double Ls[3], i
 int rdcu_lines_destroy(rdcu_lines_t *l);
 int rdcu_lines_find(rdcu_lines_t *l, const double *src, int kind, long long *n_cubes, long long *n_edges,
                     long long *n_components);
+int rdcu_lines_prefetch(rdcu_lines_t *l, const double *src, int kind);
 int rdcu_lines_edges(rdcu_lines_t *l, double *xyz, long long *comp_offsets);
 int rdcu_lines_cubes(rdcu_lines_t *l, long long *cubes, long long *comp_offsets);
 int rdcu_lines_correlate(rdcu_lines_t *prev, rdcu_lines_t *cur, long long *diffs);

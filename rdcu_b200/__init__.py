@@ -46,7 +46,7 @@ EXPORTS = [
     "rdcu_set_coefficients", "rdcu_adjoint_forward", "rdcu_adjoint_backward",
     "rdcu_ensemble_create", "rdcu_ensemble_destroy", "rdcu_ensemble_set_state", "rdcu_ensemble_get_state",
     "rdcu_ensemble_solve", "rdcu_ensemble_counters", "rdcu_ensemble_tune", "rdcu_ensemble_info",
-    "rdcu_ensemble_last_error", "rdcu_lines_create", "rdcu_lines_destroy", "rdcu_lines_find", "rdcu_lines_edges",
+    "rdcu_ensemble_last_error", "rdcu_lines_create", "rdcu_lines_destroy", "rdcu_lines_find", "rdcu_lines_prefetch", "rdcu_lines_edges",
     "rdcu_lines_cubes", "rdcu_lines_correlate", "rdcu_lines_correlate_sets", "rdcu_lines_profile", "rdcu_lines_info",
     "rdcu_lines_last_error", "rdcu_error_string", "rdcu_last_error",
 ]
@@ -140,6 +140,7 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
     lib.rdcu_lines_create.argtypes = [ctypes.POINTER(vp), pi, pd, i]
     lib.rdcu_lines_destroy.argtypes = [vp]
     lib.rdcu_lines_find.argtypes = [vp, vp, i, pll, pll, pll]
+    lib.rdcu_lines_prefetch.argtypes = [vp, vp, i]
     lib.rdcu_lines_edges.argtypes = [vp, vp, vp]
     lib.rdcu_lines_cubes.argtypes = [vp, vp, vp]
     lib.rdcu_lines_correlate.argtypes = [vp, vp, vp]

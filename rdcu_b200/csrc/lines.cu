@@ -759,7 +759,10 @@ class LinesEngine {
     g.s0 = Ns[1] * Ns[2];
     g.d2 = make_fastdiv((unsigned)Ns[2]);
     g.d1 = make_fastdiv((unsigned)Ns[1]);
-    if (cudaSetDevice(dev) != cudaSuccess || cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaSetDevice(dev) != cudaSuccess || cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&cst_, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev_main_, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev_staged_, cudaEventDisableTiming) != cudaSuccess) {
       cudaGetLastError();
       return fail(msg, "cannot create a stream on the device");
     }
@@ -795,20 +798,47 @@ class LinesEngine {
     packed_b_.release();
     if (h_small_) cudaFreeHost(h_small_);
     h_small_ = nullptr;
+    if (cst_) cudaStreamSynchronize(cst_);
+    if (ev_main_) cudaEventDestroy(ev_main_);
+    if (ev_staged_) cudaEventDestroy(ev_staged_);
+    if (cst_) cudaStreamDestroy(cst_);
     if (st) cudaStreamDestroy(st);
-    st = nullptr;
+    st = cst_ = nullptr;
+    ev_main_ = ev_staged_ = nullptr;
   }
   ~LinesEngine() { release(); }
 
   // One frame from src: the 2-field state (RDCU_LINES_STATE, u block then v block) or the
   // phase field (RDCU_LINES_PHASE), on the device or the host.
+  // Starts copying the next frame (host memory; pinned for the copy to overlap) into the
+  // staging buffer on the copy stream, after this handle's queued work; find(nullptr)
+  // then uses it.  The handle's current results are not touched.
+  int prefetch(const double* src, int kind, std::string* msg) {
+    const long long len = kind == RDCU_LINES_STATE ? 2ll * g.total : g.total;
+    if (!ck(cudaEventRecord(ev_main_, st), msg) || !ck(cudaStreamWaitEvent(cst_, ev_main_, 0), msg) ||
+        !ck(cudaMemcpyAsync(src_.p, src, len * sizeof(double), cudaMemcpyDefault, cst_), msg) ||
+        !ck(cudaEventRecord(ev_staged_, cst_), msg))
+      return RDCU_ERR_CUDA;
+    staged_kind_ = kind;
+    return RDCU_OK;
+  }
+
   int find(const double* src, int kind, bool on_device, std::string* msg) {
     have = false;
     packed_mode_ = -1;
     const int N = g.total;
     const long long len = kind == RDCU_LINES_STATE ? 2ll * N : N;
     const double* d = src;
-    if (!on_device) {
+    if (src && staged_kind_ >= 0) {  // a prefetch still copying into the staging buffer
+      if (!ck(cudaStreamWaitEvent(st, ev_staged_, 0), msg)) return RDCU_ERR_CUDA;
+      staged_kind_ = -1;
+    }
+    if (!src) {  // the prefetched frame
+      if (staged_kind_ != kind) return fail_code(msg, "no prefetched frame of this kind", RDCU_ERR_STATE);
+      staged_kind_ = -1;
+      if (!ck(cudaStreamWaitEvent(st, ev_staged_, 0), msg)) return RDCU_ERR_CUDA;
+      d = src_.p;
+    } else if (!on_device) {
       if (!ck(cudaMemcpyAsync(src_.p, src, len * sizeof(double), cudaMemcpyDefault, st), msg)) return RDCU_ERR_CUDA;
       d = src_.p;
     }
@@ -1048,6 +1078,9 @@ class LinesEngine {
   Buf<long long> wide_, comp_noff_, comp_eoff_, diff64_, sets_;
   Buf<int4> packed_, packed_b_;
   long long* h_small_ = nullptr;  // pinned
+  cudaStream_t cst_ = nullptr;    // copy stream of prefetch
+  cudaEvent_t ev_main_ = nullptr, ev_staged_ = nullptr;
+  int staged_kind_ = -1;          // kind of the prefetched frame, -1: none
   int* sorted_ = nullptr;         // node order by component (order_ or val_tmp_)
   int packed_mode_ = -1;
 
@@ -1180,13 +1213,22 @@ int rdcu_lines_destroy(rdcu_lines_t* l) {
   return RDCU_OK;
 }
 
-int rdcu_lines_find(rdcu_lines_t* l, const double* src, int kind, long long* n_cubes, long long* n_edges,
-                    long long* n_components) {
+int rdcu_lines_prefetch(rdcu_lines_t* l, const double* src, int kind) {
   if (!l || !src) return lines_err(l, RDCU_ERR_INVALID, "null argument");
   if (kind != RDCU_LINES_STATE && kind != RDCU_LINES_PHASE) return lines_err(l, RDCU_ERR_INVALID, "unknown source kind");
   if (int rc = lines_activate(l)) return rc;
   std::string msg;
-  const int rc = l->eng.find(src, kind, on_device(src), &msg);
+  const int rc = l->eng.prefetch(src, kind, &msg);
+  return rc ? lines_err(l, rc, "rdcu_lines_prefetch: " + msg) : RDCU_OK;
+}
+
+int rdcu_lines_find(rdcu_lines_t* l, const double* src, int kind, long long* n_cubes, long long* n_edges,
+                    long long* n_components) {
+  if (!l) return lines_err(l, RDCU_ERR_INVALID, "null argument");
+  if (kind != RDCU_LINES_STATE && kind != RDCU_LINES_PHASE) return lines_err(l, RDCU_ERR_INVALID, "unknown source kind");
+  if (int rc = lines_activate(l)) return rc;
+  std::string msg;
+  const int rc = l->eng.find(src, kind, src && on_device(src), &msg);
   if (rc) return lines_err(l, rc, "rdcu_lines_find: " + msg);
   if (n_cubes) *n_cubes = l->eng.n_cubes;
   if (n_edges) *n_edges = l->eng.n_edges;

@@ -80,6 +80,7 @@ class Lines:
         self.h = h
         self.N = int(np.prod(self.Ns))
         self.counts = (0, 0, 0)
+        self._staged = None
 
     def _check(self, rc):
         if rc != RDCU_OK:
@@ -96,18 +97,35 @@ class Lines:
         except Exception:
             pass
 
-    def find(self, src, kind: int = STATE) -> Tuple[int, int, int]:
-        """One frame: ``src`` is a state (2*N doubles, ``kind=STATE``) or a phase field
-        (N doubles, ``kind=PHASE``) -- a numpy array, a torch tensor (CUDA or host) or a
-        raw address.  Returns (line cubes, edges, components)."""
+    def _check_len(self, src, kind):
         need = (2 if kind == STATE else 1) * self.N
         if not isinstance(src, int) and int(np.prod(getattr(src, "shape", (len(src),)))) != need:
             raise ValueError("source must hold %d values" % need)
+
+    def prefetch(self, src, kind: int = STATE) -> None:
+        """Starts copying a host frame (pinned, e.g. a pinned torch tensor, for the copy to
+        overlap) into the staging buffer; ``find(None, kind)`` uses it.  The last frame's
+        results stay valid meanwhile."""
+        self._check_len(src, kind)
         p, keep = _ptr(src)
+        self._check(self.lib.rdcu_lines_prefetch(self.h, ctypes.c_void_p(p), kind))
+        self._staged = keep  # the source must outlive the asynchronous copy
+
+    def find(self, src, kind: int = STATE) -> Tuple[int, int, int]:
+        """One frame: ``src`` is a state (2*N doubles, ``kind=STATE``) or a phase field
+        (N doubles, ``kind=PHASE``) -- a numpy array, a torch tensor (CUDA or host) or a
+        raw address -- or None for the frame staged by ``prefetch``.  Returns (line
+        cubes, edges, components)."""
+        if src is None:  # the frame staged by prefetch
+            p, keep = 0, None
+        else:
+            self._check_len(src, kind)
+            p, keep = _ptr(src)
         a, b, c = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
         self._check(self.lib.rdcu_lines_find(self.h, ctypes.c_void_p(p), kind, ctypes.byref(a), ctypes.byref(b),
                                              ctypes.byref(c)))
         del keep
+        self._staged = None
         self.counts = (a.value, b.value, c.value)
         return self.counts
 

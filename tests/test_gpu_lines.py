@@ -205,3 +205,38 @@ def test_profile_passes(cuda):
     assert same_components(h.lines(), ol.findlines(ol.phase(y, Ns), Ns, Ls), Ns, Ls)
     assert [x[0] for x in h.profile(ol.phase(y, Ns), 1, reps=2)][0] == "faces"
     h.close()
+
+
+def test_prefetched_frames(cuda):
+    """A two-handle sequence with each next frame staged by rdcu_lines_prefetch while the
+    current one is found gives the same lines and distance matrices as direct finds."""
+    import rdcu_b200 as R
+
+    Ns, Ls = (32, 24, 40), (20.0, 15.0, 25.0)
+    frames = [cuda.tensor(defect_state(Ns, 41, k, 3, 0.1, 1.0)).pin_memory() for k in range(5)]
+    ref = _lines(Ns, Ls)
+    want_lines = []
+    for k in range(5):
+        ref.find(frames[k].numpy(), 0)
+        want_lines.append(ref.lines())
+    hs = [_lines(Ns, Ls), _lines(Ns, Ls)]
+    hs[0].find(frames[0], 0)
+    hs[1].prefetch(frames[1], 0)
+    for k in range(1, 5):
+        c, p = hs[k % 2], hs[(k - 1) % 2]
+        if k + 1 < 5:
+            p.prefetch(frames[k + 1], 0)
+        c.find(None, 0)
+        assert same_components(c.lines(), want_lines[k], Ns, Ls), k
+        assert np.array_equal(c.correlate(p), ol.correlate(want_lines[k - 1], want_lines[k], Ns, Ls)), k
+    with pytest.raises(R.RdcuError) as e:
+        hs[0].find(None, 0)  # nothing staged
+    assert e.value.code == R.RDCU_ERR_STATE
+    hs[0].prefetch(frames[0], 0)
+    with pytest.raises(R.RdcuError) as e:
+        hs[0].find(None, 1)  # staged frame is a state, not a phase field
+    assert e.value.code == R.RDCU_ERR_STATE
+    hs[0].find(frames[2], 0)  # an explicit frame after a pending prefetch
+    assert same_components(hs[0].lines(), want_lines[2], Ns, Ls)
+    for h in hs + [ref]:
+        h.close()
