@@ -31,6 +31,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <type_traits>
 
 #include "fft_line.cuh"
@@ -1151,76 +1152,69 @@ __device__ __forceinline__ void load_args(A* dst, const A* src) {
   for (int w = threadIdx.x; w < (int)(sizeof(A) / 8); w += blockDim.x) d[w] = s[w];
 }
 
-// Runs f(radix set, length) for a work item: the body specialised to the member's line
-// length L when it is one of the specialised lengths (the switch is uniform across the
-// CTA), the general body otherwise.
-template <int RS, typename F>
-__device__ __forceinline__ void by_member_length(int L, F&& f) {
-  using RP = std::integral_constant<int, kRadixPow2>;
-  switch (L) {
-    case 64: f(RP{}, std::integral_constant<int, 64>{}); break;
-    case 128: f(RP{}, std::integral_constant<int, 128>{}); break;
-    case 256: f(RP{}, std::integral_constant<int, 256>{}); break;
-    case 512: f(RP{}, std::integral_constant<int, 512>{}); break;
-    case 96: f(std::integral_constant<int, kRadixAll>{}, std::integral_constant<int, 96>{}); break;
-    case 192: f(std::integral_constant<int, kRadixAll>{}, std::integral_constant<int, 192>{}); break;
-    default: f(std::integral_constant<int, RS>{}, std::integral_constant<int, 0>{}); break;
-  }
-}
-
-// Work-item bodies as called functions: each length variant keeps its own register
-// allocation (inlined into one kernel, the union of the variants spills).
+// Batched passes: persistent CTAs over (problem, tile) work items whose problems share one
+// line length, with that length's specialised body inlined (LX = 0: the plan's stages) and
+// the launch bounds of the single-problem kernels.  The groups of one pass run as
+// concurrent branches (SpectralBatch::launch_stage).
 template <int RS, int LX>
-__device__ __noinline__ void fwd_x_item(const FwdXArgs& a, int bx) {
-  fwd_x_body<RS, LX>(a, bx);
-}
-template <int RS, int LX>
-__device__ __noinline__ void mid_item(const MidArgs& a, int bx) {
-  mid_body<RS, LX>(a, bx);
-}
-template <int RS, int LX>
-__device__ __noinline__ void inv_x_item(const InvXArgs& a, int bx) {
-  inv_x_body<RS, LX>(a, bx);
-}
-
-template <int RS>
-__global__ void __launch_bounds__(kMaxBlock, 1)
-    k_fwd_x_batch(const FwdXArgs* __restrict__ args, const int2* __restrict__ items, int nitems) {
+__global__ void __launch_bounds__(LX > 0 ? kSpecBlock : kMaxBlock, LX > 0 ? 2 : 1)
+    k_fwd_x_group(const FwdXArgs* __restrict__ args, const int2* __restrict__ items, int nitems) {
   __shared__ __align__(16) FwdXArgs sa;
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const int2 w = items[it];
     load_args(&sa, args + w.x);
     __syncthreads();
-    by_member_length<RS>(sa.M, [&](auto rs, auto lx) { fwd_x_item<decltype(rs)::value, decltype(lx)::value>(sa, w.y); });
+    fwd_x_body<RS, LX>(sa, w.y);
     __syncthreads();
   }
 }
 
-template <int RS>
-__global__ void __launch_bounds__(kMaxBlock, 1)
-    k_mid_batch(const MidArgs* __restrict__ args, const int2* __restrict__ items, int nitems) {
+template <int RS, int LX>
+__global__ void __launch_bounds__(LX > 0 ? kSpecBlock : kMaxBlock, LX > 0 ? 3 : 1)
+    k_mid_group(const MidArgs* __restrict__ args, const int2* __restrict__ items, int nitems) {
   __shared__ __align__(16) MidArgs sa;
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const int2 w = items[it];
     load_args(&sa, args + w.x);
     __syncthreads();
-    by_member_length<RS>(sa.L0, [&](auto rs, auto lx) { mid_item<decltype(rs)::value, decltype(lx)::value>(sa, w.y); });
+    mid_body<RS, LX>(sa, w.y);
     __syncthreads();
   }
 }
 
-template <int RS>
-__global__ void __launch_bounds__(kMaxBlock, 1)
-    k_inv_x_batch(const InvXArgs* __restrict__ args, const int2* __restrict__ items, int nitems) {
+template <int RS, int LX>
+__global__ void __launch_bounds__(LX > 0 ? kSpecBlock : kMaxBlock, LX > 0 ? 3 : 1)
+    k_inv_x_group(const InvXArgs* __restrict__ args, const int2* __restrict__ items, int nitems) {
   __shared__ __align__(16) InvXArgs sa;
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const int2 w = items[it];
     load_args(&sa, args + w.x);
     __syncthreads();
-    by_member_length<RS>(sa.M, [&](auto rs, auto lx) { inv_x_item<decltype(rs)::value, decltype(lx)::value>(sa, w.y); });
+    inv_x_body<RS, LX>(sa, w.y);
     __syncthreads();
   }
 }
+
+// Kernel of pass k (0 fwd_x, 1 mid, 2 inv_x) for a group of line length L: the
+// specialised lengths, else the plan's stages with radix set rs.
+template <int RS, int LX>
+const void* group_kernel(int k) {
+  if (k == 0) return (const void*)k_fwd_x_group<RS, LX>;
+  if (k == 1) return (const void*)k_mid_group<RS, LX>;
+  return (const void*)k_inv_x_group<RS, LX>;
+}
+const void* group_kernel_for(int k, int L, int rs) {
+  switch (L) {
+    case 64: return group_kernel<kRadixPow2, 64>(k);
+    case 128: return group_kernel<kRadixPow2, 128>(k);
+    case 256: return group_kernel<kRadixPow2, 256>(k);
+    case 512: return group_kernel<kRadixPow2, 512>(k);
+    case 96: return group_kernel<kRadixAll, 96>(k);
+    case 192: return group_kernel<kRadixAll, 192>(k);
+    default: return rs == kRadixPow2 ? group_kernel<kRadixPow2, 0>(k) : group_kernel<kRadixAll, 0>(k);
+  }
+}
+bool length_specialised(int L) { return L == 64 || L == 96 || L == 128 || L == 192 || L == 256 || L == 512; }
 
 inline int round_up(int v, int m) { return (v + m - 1) / m * m; }
 
@@ -2385,14 +2379,21 @@ cudaError_t SpectralPlan::run_linear(const double* in, double* out, cudaStream_t
 // ----------------------------------------------------------------------------- batch
 struct SpectralBatch::Impl {
   int nm = 0;
-  bool pow2 = true;
   FwdXArgs* fwd[8] = {};
   MidArgs* mid[8] = {};
   InvXArgs* inv[8] = {};
   int2* items[3] = {};
   int nitems[3] = {0, 0, 0};
-  int grid[3] = {0, 0, 0}, block[3] = {0, 0, 0};
-  size_t smem[3] = {0, 0, 0};
+  // work items of one pass whose problems share a line length: [off, off + count) of items
+  struct Group {
+    int L = 0, rs = 0, off = 0, count = 0, grid = 0, block = 0;
+    size_t smem = 0;
+    const void* kern = nullptr;
+  };
+  std::vector<Group> groups[3];
+  static constexpr int kMaxSide = 8;  // side streams of concurrent groups
+  cudaStream_t side[kMaxSide] = {};
+  cudaEvent_t fork = nullptr, join[kMaxSide] = {};
 };
 
 void SpectralBatch::release() {
@@ -2404,6 +2405,11 @@ void SpectralBatch::release() {
   }
   for (auto* p : impl_->items)
     if (p) cudaFree(p);
+  for (int g = 0; g < Impl::kMaxSide; ++g) {
+    if (impl_->side[g]) cudaStreamDestroy(impl_->side[g]);
+    if (impl_->join[g]) cudaEventDestroy(impl_->join[g]);
+  }
+  if (impl_->fork) cudaEventDestroy(impl_->fork);
   delete impl_;
   impl_ = nullptr;
   device_bytes = 0;
@@ -2422,30 +2428,42 @@ bool SpectralBatch::init(const std::vector<BatchMember>& members, int elems_, st
   std::vector<std::vector<FwdXArgs>> hf(8);
   std::vector<std::vector<MidArgs>> hmid(8);
   std::vector<std::vector<InvXArgs>> hi(8);
-  std::vector<int2> it[3];
+  // per pass: group key (line length, radix set) -> its items and largest block / smem
+  struct Acc {
+    std::vector<int2> items;
+    int block = 0;
+    size_t smem = 0;
+  };
+  std::map<std::pair<int, int>, Acc> acc[3];
+  auto add = [&](int k, int L, const LinePlan& plan, int block, size_t smem, int m, int ntiles) {
+    Acc& g = acc[k][{L, plan_is_pow2(plan) ? kRadixPow2 : kRadixAll}];
+    g.block = std::max(g.block, block);
+    g.smem = std::max(g.smem, smem);
+    for (int j = 0; j < ntiles; ++j) g.items.push_back(make_int2(m, j));
+  };
+  // a specialised length keeps its blocks within the specialised kernels' 256 threads
+  auto elems_for = [&](int L) { return length_specialised(L) ? std::min(elems, kSpecBlock * kStageElems) : elems; };
   for (int m = 0; m < B.nm; ++m) {
     const SpectralPlan& p = *members[m].plan;
     if (p.ndim != 2) {
       *msg = "batched problems must be two-dimensional";
       return false;
     }
-    B.pow2 = B.pow2 && plan_is_pow2(p.plan_x_) && plan_is_pow2(p.plan_ax_[0]);
     const int M = p.M, Mh = p.Mh, R = p.R, n = p.n, nch = p.nch;
     const bool spectral = nch > 0;
     // fwd_x tiles: P line pairs per item
     const int pairs = (n * R + 1) / 2;
-    const int Pf = std::max(1, std::min(elems / M, pairs));
+    const int Pf = std::max(1, std::min(elems_for(M) / M, pairs));
     const bool ftws = (size_t)(M + Pf * M) * 16 <= kSmemBudget;
     const int gf = (pairs + Pf - 1) / Pf;
-    B.block[0] = std::max(B.block[0], std::min(kMaxBlock, std::max(128, round_up(stage_threads(p.plan_x_, Pf * M), 32))));
-    B.smem[0] = std::max(B.smem[0], spectral ? (size_t)((ftws ? M : 0) + Pf * M) * 16 : 0);
-    for (int j = 0; j < gf; ++j) it[0].push_back(make_int2(m, j));
+    add(0, M, p.plan_x_, std::min(kMaxBlock, std::max(128, round_up(stage_threads(p.plan_x_, Pf * M), 32))),
+        spectral ? (size_t)((ftws ? M : 0) + Pf * M) * 16 : 0, m, gf);
     // mid tiles: TW columns per item, every channel at once when the plan does so
     const int L0 = p.Ns[0], I = Mh;
     const int GBp = p.mid_[0].per_cta >> 16;
     const bool sorted = p.ch_sorted_ && nch <= GBp;
     int GB = sorted ? nch : std::min(std::max(nch, 1), 4);
-    int TW = std::max(1, std::min(elems / (std::max(n, GB) * L0), I));
+    int TW = std::max(1, std::min(elems_for(L0) / (std::max(n, GB) * L0), I));
     const size_t extra = (size_t)p.h_ch_off_[nch] * sizeof(ChanEntry) + (size_t)p.kv_total_ * 8 + (size_t)(nch + 2) * 4 +
                          16 + (size_t)p.h_ch_off_[nch] * (sizeof(ChanEntry) + 16 * 8);
     auto smem_of = [&](int tw_, int gb) { return (size_t)(L0 + (n + gb) * tw_ * tile_stride(L0, tw_)) * 16 + extra; };
@@ -2456,19 +2474,15 @@ bool SpectralBatch::init(const std::vector<BatchMember>& members, int elems_, st
       return false;
     }
     const int gm = (I + TW - 1) / TW;
-    if (spectral) {
-      B.block[1] = std::max(B.block[1], std::min(kMaxBlock, std::max(128, round_up(stage_threads(p.plan_ax_[0], std::max(n, GB) * TW * L0), 32))));
-      B.smem[1] = std::max(B.smem[1], sorted && nch <= n ? (size_t)(L0 + n * TW * tile_stride(L0, TW)) * 16 + extra
-                                                         : smem_of(TW, GB));
-      for (int j = 0; j < gm; ++j) it[1].push_back(make_int2(m, j));
-    }
+    if (spectral)
+      add(1, L0, p.plan_ax_[0],
+          std::min(kMaxBlock, std::max(128, round_up(stage_threads(p.plan_ax_[0], std::max(n, GB) * TW * L0), 32))),
+          sorted && nch <= n ? (size_t)(L0 + n * TW * tile_stride(L0, TW)) * 16 + extra : smem_of(TW, GB), m, gm);
     // inv_x tiles
     PassCfg gi;
     int itws = 0;
-    inv_geometry(M, R, n, nch, false, p.plan_x_, &gi, &itws, p.dict_smem_bytes(), elems);
-    B.smem[2] = std::max(B.smem[2], gi.smem);
-    B.block[2] = std::max(B.block[2], gi.block);
-    for (int j = 0; j < gi.grid; ++j) it[2].push_back(make_int2(m, j));
+    inv_geometry(M, R, n, nch, false, p.plan_x_, &gi, &itws, p.dict_smem_bytes(), elems_for(M));
+    add(2, M, p.plan_x_, gi.block, gi.smem, m, gi.grid);
     for (int st = 1; st <= 7; ++st) {
       RhsIO io{};
       io.mode = 1;
@@ -2543,56 +2557,82 @@ bool SpectralBatch::init(const std::vector<BatchMember>& members, int elems_, st
   };
   bool ok = true;
   for (int st = 1; st <= 7; ++st) ok = ok && put(&B.fwd[st], hf[st]) && put(&B.mid[st], hmid[st]) && put(&B.inv[st], hi[st]);
-  for (int k = 0; k < 3; ++k) {
-    ok = ok && put(&B.items[k], it[k]);
-    B.nitems[k] = nitems[k] = (int)it[k].size();
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  for (int k = 0; k < 3 && ok; ++k) {
+    std::vector<int2> all;
+    for (auto& kv : acc[k]) {
+      Impl::Group g;
+      g.L = kv.first.first;
+      g.rs = kv.first.second;
+      g.off = (int)all.size();
+      g.count = (int)kv.second.items.size();
+      g.block = std::max(kv.second.block, 128);
+      g.smem = kv.second.smem;
+      // a block wider than the specialised kernels allow takes the plan's stages
+      g.kern = group_kernel_for(k, g.block <= kSpecBlock ? g.L : 0, g.rs);
+      if (!opt_in_smem(g.kern)) {
+        *msg = "cannot enable large shared memory for the batched passes";
+        return false;
+      }
+      int per_sm = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, g.kern, g.block, g.smem) != cudaSuccess ||
+          per_sm < 1) {
+        cudaGetLastError();
+        *msg = "batched pass does not fit on an SM";
+        return false;
+      }
+      g.grid = std::max(1, std::min(g.count, per_sm * nsm));
+      all.insert(all.end(), kv.second.items.begin(), kv.second.items.end());
+      B.groups[k].push_back(g);
+    }
+    ok = put(&B.items[k], all);
+    B.nitems[k] = nitems[k] = (int)all.size();
   }
   if (!ok) {
     *msg = "out of device memory (batch tables)";
     return false;
   }
-  // persistent grids: as many CTAs as stay resident
-  int dev = 0, nsm = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  const void* kern[3] = {B.pow2 ? (const void*)k_fwd_x_batch<kRadixPow2> : (const void*)k_fwd_x_batch<kRadixAll>,
-                         B.pow2 ? (const void*)k_mid_batch<kRadixPow2> : (const void*)k_mid_batch<kRadixAll>,
-                         B.pow2 ? (const void*)k_inv_x_batch<kRadixPow2> : (const void*)k_inv_x_batch<kRadixAll>};
-  for (int k = 0; k < 3; ++k) {
-    if (!opt_in_smem(kern[k])) {
-      *msg = "cannot enable large shared memory for the batched passes";
-      return false;
-    }
-    B.block[k] = std::max(B.block[k], 128);
-    int per_sm = 1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern[k], B.block[k], B.smem[k]) != cudaSuccess || per_sm < 1) {
-      *msg = "batched pass does not fit on an SM";
-      return false;
-    }
-    B.grid[k] = std::max(1, std::min(B.nitems[k], per_sm * nsm));
+  // side streams and events of the concurrent groups
+  if (cudaEventCreateWithFlags(&B.fork, cudaEventDisableTiming) != cudaSuccess) {
+    *msg = "cannot create events";
+    return false;
   }
+  for (int g = 0; g < Impl::kMaxSide; ++g)
+    if (cudaStreamCreateWithFlags(&B.side[g], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&B.join[g], cudaEventDisableTiming) != cudaSuccess) {
+      *msg = "cannot create streams";
+      return false;
+    }
   return true;
 }
 
 cudaError_t SpectralBatch::launch_stage(int stage, cudaStream_t st) {
   Impl& B = *impl_;
   if (stage < 1 || stage > 7) return cudaErrorInvalidValue;
-  if (B.pow2)
-    k_fwd_x_batch<kRadixPow2><<<B.grid[0], B.block[0], B.smem[0], st>>>(B.fwd[stage], B.items[0], B.nitems[0]);
-  else
-    k_fwd_x_batch<kRadixAll><<<B.grid[0], B.block[0], B.smem[0], st>>>(B.fwd[stage], B.items[0], B.nitems[0]);
-  RDCU_TRY(cudaGetLastError());
-  if (B.nitems[1] > 0) {
-    if (B.pow2)
-      k_mid_batch<kRadixPow2><<<B.grid[1], B.block[1], B.smem[1], st>>>(B.mid[stage], B.items[1], B.nitems[1]);
-    else
-      k_mid_batch<kRadixAll><<<B.grid[1], B.block[1], B.smem[1], st>>>(B.mid[stage], B.items[1], B.nitems[1]);
-    RDCU_TRY(cudaGetLastError());
+  const void* args[3] = {B.fwd[stage], B.mid[stage], B.inv[stage]};
+  for (int k = 0; k < 3; ++k) {
+    const std::vector<Impl::Group>& G = B.groups[k];
+    if (G.empty()) continue;
+    auto launch = [&](const Impl::Group& g, cudaStream_t s) {
+      const void* a = args[k];
+      const int2* items = B.items[k] + g.off;
+      int cnt = g.count;
+      void* params[3] = {(void*)&a, (void*)&items, (void*)&cnt};
+      return cudaLaunchKernel(g.kern, dim3(g.grid), dim3(g.block), params, g.smem, s);
+    };
+    // group 0 on the stream, the others on side streams forked from it and joined back
+    const int nside = std::min((int)G.size() - 1, (int)Impl::kMaxSide);
+    if (nside > 0) RDCU_TRY(cudaEventRecord(B.fork, st));
+    for (int i = 0; i < nside; ++i) RDCU_TRY(cudaStreamWaitEvent(B.side[i], B.fork, 0));
+    for (size_t gi = 1; gi < G.size(); ++gi) RDCU_TRY(launch(G[gi], B.side[(gi - 1) % Impl::kMaxSide]));
+    RDCU_TRY(launch(G[0], st));
+    for (int i = 0; i < nside; ++i) {
+      RDCU_TRY(cudaEventRecord(B.join[i], B.side[i]));
+      RDCU_TRY(cudaStreamWaitEvent(st, B.join[i], 0));
+    }
   }
-  if (B.pow2)
-    k_inv_x_batch<kRadixPow2><<<B.grid[2], B.block[2], B.smem[2], st>>>(B.inv[stage], B.items[2], B.nitems[2]);
-  else
-    k_inv_x_batch<kRadixAll><<<B.grid[2], B.block[2], B.smem[2], st>>>(B.inv[stage], B.items[2], B.nitems[2]);
   return cudaGetLastError();
 }
 
