@@ -611,7 +611,10 @@ def run_ensemble(args, rank=0, world=1, local_rank=0):
         "baseline_sequential": {"value": seq_rate, "unit": "grid-pt·steps/s", "sample_members": sample,
                                 "seconds": seq_s, "note": "single handles one after another, same window"},
         "speedup_vs_sequential": (work / sec) / seq_rate,
-        "gpu_launches": int(attempts_batched) * 19,
+        # per batched attempt: stages 2..7, each one kernel per line-length group of each
+        # pass (fwd_x and inv_x by N[1], mid by N[0]), and the controller
+        "gpu_launches": int(attempts_batched) * (6 * (2 * len({x["Ns"][1] for x in mem}) +
+                                                      len({x["Ns"][0] for x in mem})) + 1),
         "clocks": clk.summary(),
         "e2e": {"value": e2e_work / e2e_s, "unit": "grid-pt·steps/s",
                 "h2d_bytes_per_step": 16.0 * float(np.sum(npts)) / args.steps,
