@@ -456,15 +456,16 @@ __global__ void __launch_bounds__(LX > 0 ? kSpecBlock : kMaxBlock, LX > 0 ? 2 : 
   const long long i0 = (long long)blockIdx.x * TW;
   double2* base = a.S + (long long)blockIdx.y * La * a.I;
   const int nel = La * TW;
+  // the last tile of a plane may hold fewer columns (e.g. 1 of 16 when I = 129): only
+  // its valid lines are loaded and transformed (lines are independent)
+  const int nl = (int)min((long long)TW, a.I - i0);
   for (int e = tid; e < nel; e += T) {
     const int z = fdiv(e, a.dTW), c = e - z * TW;
-    const long long ii = i0 + c;
-    const bool in = ii < a.I;
-    cp_async16(&buf[c * LS + z], in ? (const void*)&base[(long long)z * a.I + ii] : (const void*)base, in);
+    if (c < nl) cp_async16(&buf[c * LS + z], &base[(long long)z * a.I + i0 + c], true);
   }
   cp_async_wait_all();
   __syncthreads();
-  fft_lines_x<RS, LX, INV>(buf, LS, TW, a.plan, tw, twz);
+  fft_lines_x<RS, LX, INV>(buf, LS, nl, a.plan, tw, twz);
   for (int e = tid; e < nel; e += T) {
     const int z = fdiv(e, a.dTW), c = e - z * TW;
     const long long ii = i0 + c;
