@@ -17,9 +17,12 @@
 // the reference's stencils are circulant, so the FFT diagonalises J_lin and each
 // Fourier mode is an n x n solve (spectral.cu k_mid_solve).  GMRES runs to a relative
 // residual of 1e-12, far below the Newton tolerance, so Newton and step decisions are
-// those of an exact solve.
+// those of an exact solve.  Each restart cycle (up to 40 Arnoldi iterations) is one
+// CUDA graph whose WHILE node loops on the device: the host reads back one small
+// state record per cycle instead of the Gram-Schmidt coefficients per iteration.
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <vector>
 
@@ -113,24 +116,6 @@ __global__ void k_sum_rows(const double* part, int nrow, int ncol, double* out) 
   if (threadIdx.x == 0) out[r] = s;
 }
 
-// w -= sum_i h_i V_i   (h on the device)
-__global__ void k_vsub(const double* V, int nvec, const double* h, double* w, long long nN) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nN) return;
-  double acc = w[i];
-  for (int k = 0; k < nvec; ++k) acc -= h[k] * V[(long long)k * nN + i];
-  w[i] = acc;
-}
-
-// u = sum_i y_i V_i
-__global__ void k_vcomb(const double* V, int nvec, const double* y, double* u, long long nN) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nN) return;
-  double acc = 0.0;
-  for (int k = 0; k < nvec; ++k) acc += y[k] * V[(long long)k * nN + i];
-  u[i] = acc;
-}
-
 __global__ void k_scale(const double* x, double s, double* y, long long nN) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < nN) y[i] = s * x[i];
@@ -141,16 +126,6 @@ __global__ void k_axpy(double a, const double* x, double* y, long long nN) {
   if (i < nN) y[i] += a * x[i];
 }
 
-// y = x + alpha * (J x): the action of A = I + alpha J (csrgeam2 of bdf.cu:153)
-__global__ void k_apply_A(const int* rows, const int* cols, const double* vals, double alpha, const double* x,
-                          double* y, long long nN) {
-  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= nN) return;
-  double acc = 0.0;
-  for (int p = rows[r]; p < rows[r + 1]; ++p) acc += vals[p] * x[cols[p]];
-  y[r] = x[r] + alpha * acc;
-}
-
 // r = b - A x
 __global__ void k_residual(const int* rows, const int* cols, const double* vals, double alpha, const double* x,
                            const double* b, double* r, long long nN) {
@@ -159,6 +134,167 @@ __global__ void k_residual(const int* rows, const int* cols, const double* vals,
   double acc = 0.0;
   for (int p = rows[i]; p < rows[i + 1]; ++p) acc += vals[p] * x[cols[p]];
   r[i] = b[i] - (x[i] + alpha * acc);
+}
+
+// ---------------------------------------------------------------- device-resident GMRES
+// One restart cycle of GMRES(m) runs as a CUDA graph with a WHILE node (see
+// build_cycle_graph).  What changes between iterations and calls lives here, on the
+// device: the column j, alpha, the Givens factors, g and the Hessenberg matrix.  The
+// scalar update uses round-to-nearest intrinsics without contraction, so every value
+// is the one the same recurrence gives on the host.
+constexpr int kGmresM = 40;  // restart length m
+
+struct GmresState {
+  double alpha;   // A = I + alpha J
+  double tol;     // absolute residual target
+  double inv_hn;  // 1 / ||w|| of the last column: scale of the next basis vector
+  int j;          // column being built
+  int jdone;      // columns done
+  int total;      // iterations over all cycles of this solve
+  int max_total;
+  int cont;       // the loop goes on (the next basis vector was formed)
+  int conv;
+  int guard;      // iterations of this cycle: bounds the loop whatever j does
+  int pad;
+  double cs[kGmresM], sn[kGmresM], g[kGmresM + 1];
+  double H[kGmresM * kGmresM];  // H[k * m + j], k <= j
+  double y[kGmresM];            // least-squares solution (back-substitution)
+};
+
+__global__ void k_gm_init(GmresState* s, double alpha, double tol, double beta, int total, int max_total) {
+  for (int k = threadIdx.x; k <= kGmresM; k += blockDim.x) s->g[k] = k == 0 ? beta : 0.0;
+  if (threadIdx.x == 0) {
+    s->alpha = alpha;
+    s->tol = tol;
+    s->inv_hn = 0.0;
+    s->j = 0;
+    s->jdone = 0;
+    s->total = total;
+    s->max_total = max_total;
+    s->cont = 0;
+    s->conv = 0;
+    s->guard = 0;
+  }
+}
+
+// out = V_j
+__global__ void k_gm_take(const double* V, const GmresState* s, double* out, long long nN) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nN) out[i] = V[(long long)s->j * nN + i];
+}
+
+// y = x + alpha * (J x), alpha read on the device: the action of A = I + alpha J
+// (csrgeam2 of bdf.cu:153)
+__global__ void k_apply_A_dev(const int* rows, const int* cols, const double* vals, const double* alpha,
+                              const double* x, double* y, long long nN) {
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nN) return;
+  const double al = *alpha;
+  double acc = 0.0;
+  for (int p = rows[r]; p < rows[r + 1]; ++p) acc += vals[p] * x[cols[p]];
+  y[r] = x[r] + al * acc;
+}
+
+// k_dots, k_sum_rows and k_vsub over the j + 1 basis vectors (j read on the device;
+// rows past it return).  The same partial sums in the same order as the fixed forms.
+__global__ void k_dots_j(const double* V, const GmresState* s, const double* w, long long nN, double* part) {
+  const int nvec = s->j + 1;
+  const int row = blockIdx.y;
+  if (row > nvec) return;
+  const double* a = row < nvec ? V + (long long)row * nN : w;
+  double sum = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nN; i += (long long)gridDim.x * blockDim.x)
+    sum += a[i] * w[i];
+  sum = block_reduce(sum);
+  if (threadIdx.x == 0) part[(long long)row * gridDim.x + blockIdx.x] = sum;
+}
+
+__global__ void k_sum_rows_j(const double* part, const GmresState* s, int ncol, double* out) {
+  const int r = blockIdx.x;
+  if (r >= s->j + 2) return;
+  double sum = 0.0;
+  for (int c = threadIdx.x; c < ncol; c += blockDim.x) sum += part[(long long)r * ncol + c];
+  sum = block_reduce(sum);
+  if (threadIdx.x == 0) out[r] = sum;
+}
+
+__global__ void k_vsub_j(const double* V, const GmresState* s, const double* h, double* w, long long nN) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nN) return;
+  const int nvec = s->j + 1;
+  double acc = w[i];
+  for (int k = 0; k < nvec; ++k) acc -= h[k] * V[(long long)k * nN + i];
+  w[i] = acc;
+}
+
+// Column j of the Hessenberg matrix from the two Gram-Schmidt passes (dots rows 0 and
+// 1, stride `row`) and the norm of w (row 2); Givens rotations; stop test; the loop
+// condition.  One thread.
+__global__ void k_gm_update(GmresState* s, const double* dots, int row, cudaGraphConditionalHandle cond) {
+  if (threadIdx.x != 0) return;
+  const int j = s->j;
+  double hcol[kGmresM + 1];
+  for (int k = 0; k <= j; ++k) hcol[k] = __dadd_rn(__dadd_rn(0.0, dots[k]), dots[row + k]);
+  const double hn = sqrt(dots[2 * row]);
+  const int total = s->total + 1;
+  s->total = total;
+  for (int k = 0; k < j; ++k) {
+    const double a = __dadd_rn(__dmul_rn(s->cs[k], hcol[k]), __dmul_rn(s->sn[k], hcol[k + 1]));
+    hcol[k + 1] = __dadd_rn(__dmul_rn(-s->sn[k], hcol[k]), __dmul_rn(s->cs[k], hcol[k + 1]));
+    hcol[k] = a;
+  }
+  const double den = sqrt(__dadd_rn(__dmul_rn(hcol[j], hcol[j]), __dmul_rn(hn, hn)));
+  const double c = den > 0 ? hcol[j] / den : 1.0;
+  const double sj = den > 0 ? hn / den : 0.0;
+  s->cs[j] = c;
+  s->sn[j] = sj;
+  hcol[j] = den;
+  const double gj = s->g[j];
+  s->g[j + 1] = __dmul_rn(-sj, gj);
+  s->g[j] = __dmul_rn(c, gj);
+  for (int k = 0; k <= j; ++k) s->H[k * kGmresM + j] = hcol[k];
+  s->jdone = j + 1;
+  const bool met = fabs(s->g[j + 1]) <= s->tol || !(hn > 0);
+  const bool stop = met || total >= s->max_total;
+  s->conv = met ? 1 : 0;
+  const int guard = s->guard + 1;
+  s->guard = guard;
+  const int cont = (!stop && j + 1 < kGmresM && guard < kGmresM) ? 1 : 0;
+  s->cont = cont;
+  if (cont) {
+    s->inv_hn = 1.0 / hn;
+    s->j = j + 1;
+  }
+  cudaGraphSetConditional(cond, (unsigned int)cont);
+}
+
+// V_{j+1} = w / ||w|| when the loop goes on
+__global__ void k_gm_scale(const GmresState* s, const double* w, double* V, long long nN) {
+  if (!s->cont) return;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nN) V[(long long)s->j * nN + i] = s->inv_hn * w[i];
+}
+
+// back-substitution H y = g over the columns done (one thread)
+__global__ void k_gm_backsub(GmresState* s) {
+  if (threadIdx.x != 0) return;
+  const int jd = s->jdone;
+  for (int k = jd - 1; k >= 0; --k) {
+    double acc = s->g[k];
+    for (int q = k + 1; q < jd; ++q) acc = __dsub_rn(acc, __dmul_rn(s->H[k * kGmresM + q], s->y[q]));
+    const double d = s->H[k * kGmresM + k];
+    s->y[k] = d != 0 ? acc / d : 0.0;
+  }
+}
+
+// u = sum_{k < jdone} y_k V_k
+__global__ void k_vcomb_j(const double* V, const GmresState* s, double* u, long long nN) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nN) return;
+  const int nvec = s->jdone;
+  double acc = 0.0;
+  for (int k = 0; k < nvec; ++k) acc += s->y[k] * V[(long long)k * nN + i];
+  u[i] = acc;
 }
 
 // ytemp += dd; d += dd (the two Daxpy of bdf.cu:187-188)
@@ -243,14 +379,19 @@ struct BDFEngine::Impl {
   long long nN = 0;
   int blocks = 0;
   double *ytemp = nullptr, *yscale = nullptr, *f = nullptr, *d = nullptr, *dd = nullptr, *b = nullptr;
-  double *y_eval = nullptr, *w = nullptr, *z = nullptr, *xacc = nullptr, *r = nullptr;
+  double *y_eval = nullptr, *w = nullptr, *z = nullptr, *vj = nullptr, *r = nullptr;
   double* V = nullptr;
-  int m = 40;
+  int m = kGmresM;
   double* part = nullptr;   // [(m+2)][kRedBlocks]
-  double* dots = nullptr;   // [m+2] device
+  double* dots = nullptr;   // 3 rows of [m+2] (device)
   double* hdots = nullptr;  // pinned
-  double* hvec = nullptr;   // device coefficients for k_vsub / k_vcomb
-  double* hvec_host = nullptr;  // pinned
+  // the restart cycle as a graph (build_cycle_graph), its device state and a pinned
+  // copy of the state's header
+  GmresState* gm = nullptr;
+  GmresState* gm_host = nullptr;
+  cudaGraph_t cycle_graph = nullptr;
+  cudaGraphExec_t cycle_exec = nullptr;
+  double* cycle_x = nullptr;  // the solution vector the graph updates
   int refactor = 1, rejac = 1;
   double nconststeps = 0;
   double ntol = 0;
@@ -321,16 +462,16 @@ bool BDFEngine::init(FDProblem* fd, double atol, double rtol, int fixed, cudaStr
     return false;
   };
   if (cudaMalloc((void**)&D_, sb * 8) != cudaSuccess) return fail("BDF differences");
-  double** vecs[] = {&I.ytemp, &I.yscale, &I.f, &I.d, &I.dd, &I.b, &I.y_eval, &I.w, &I.z, &I.xacc, &I.r};
+  double** vecs[] = {&I.ytemp, &I.yscale, &I.f, &I.d, &I.dd, &I.b, &I.y_eval, &I.w, &I.z, &I.vj, &I.r};
   for (double** p : vecs)
     if (cudaMalloc((void**)p, sb) != cudaSuccess) return fail("BDF vectors");
   if (cudaMalloc((void**)&I.V, sb * (I.m + 1)) != cudaSuccess) return fail("GMRES basis");
   if (cudaMalloc((void**)&I.part, sizeof(double) * (I.m + 2) * kRedBlocks) != cudaSuccess) return fail("reductions");
   // three rows of m+2: the two Gram-Schmidt passes and the new vector's norm
   if (cudaMalloc((void**)&I.dots, sizeof(double) * 3 * (I.m + 2)) != cudaSuccess) return fail("reductions");
-  if (cudaMalloc((void**)&I.hvec, sizeof(double) * (I.m + 2)) != cudaSuccess) return fail("reductions");
+  if (cudaMalloc((void**)&I.gm, sizeof(GmresState)) != cudaSuccess) return fail("GMRES state");
   if (cudaMallocHost((void**)&I.hdots, sizeof(double) * 3 * (I.m + 2)) != cudaSuccess) return fail("pinned");
-  if (cudaMallocHost((void**)&I.hvec_host, sizeof(double) * (I.m + 2)) != cudaSuccess) return fail("pinned");
+  if (cudaMallocHost((void**)&I.gm_host, sizeof(GmresState)) != cudaSuccess) return fail("pinned");
   device_bytes = sb * (8 + 11 + I.m + 1) + fd->device_bytes;
   std::vector<LinEntry> lin = linear_part(*fd);
   if (!lin.empty() && fd->n <= kMaxPrecFields) {
@@ -346,11 +487,14 @@ bool BDFEngine::init(FDProblem* fd, double atol, double rtol, int fixed, cudaStr
 void BDFEngine::release() {
   if (impl_) {
     Impl& I = *impl_;
-    double* vecs[] = {I.ytemp, I.yscale, I.f, I.d, I.dd, I.b, I.y_eval, I.w, I.z, I.xacc, I.r, I.V, I.part, I.dots, I.hvec};
+    if (I.cycle_exec) cudaGraphExecDestroy(I.cycle_exec);
+    if (I.cycle_graph) cudaGraphDestroy(I.cycle_graph);
+    double* vecs[] = {I.ytemp, I.yscale, I.f, I.d, I.dd, I.b, I.y_eval, I.w, I.z, I.vj, I.r, I.V, I.part, I.dots};
     for (double* p : vecs)
       if (p) cudaFree(p);
+    if (I.gm) cudaFree(I.gm);
     if (I.hdots) cudaFreeHost(I.hdots);
-    if (I.hvec_host) cudaFreeHost(I.hvec_host);
+    if (I.gm_host) cudaFreeHost(I.gm_host);
     delete impl_;
     impl_ = nullptr;
   }
@@ -406,29 +550,103 @@ cudaError_t vdots(BDFEngine::Impl& I, int nvec, const double* w, cudaStream_t st
   return cudaGetLastError();
 }
 
-// vdots without the host copy: out[0..nvec) = V^T w, out[nvec] = w.w on the device
-cudaError_t vdots_dev(BDFEngine::Impl& I, int nvec, const double* w, cudaStream_t st, double* out) {
-  dim3 grid(kRedBlocks, nvec + 1);
-  k_dots<<<grid, kRedThreads, 0, st>>>(I.V, nvec, w, I.nN, I.part);
-  k_sum_rows<<<nvec + 1, kRedThreads, 0, st>>>(I.part, nvec + 1, kRedBlocks, out);
-  return cudaGetLastError();
-}
-
 }  // namespace
 
-// Solves (I + alpha J) x = b; x in I.dd.  Returns the number of GMRES iterations.
+// The GMRES(m) restart cycle as one CUDA graph: a WHILE node whose body is one Arnoldi
+// iteration -- z = P^-1 V_j, w = A z, two classical Gram-Schmidt passes, ||w||, the
+// Givens update (which clears the loop condition on convergence, after m columns or on
+// the iteration limit) and V_{j+1} = w/||w|| -- then the back-substitution and
+// x += P^-1 (V y).  The same kernels and arithmetic as one host-driven iteration at a
+// time, without a host round trip per iteration.
+static cudaError_t build_cycle_graph(BDFEngine::Impl& I, const FDProblem& fd, double* x, cudaStream_t st) {
+  if (I.cycle_exec) cudaGraphExecDestroy(I.cycle_exec);
+  if (I.cycle_graph) cudaGraphDestroy(I.cycle_graph);
+  I.cycle_exec = nullptr;
+  I.cycle_graph = nullptr;
+  const long long nN = I.nN;
+  const int nb = I.blocks;
+  const int m = I.m;
+  const int row = m + 2;
+  const double* alpha_dev = &I.gm->alpha;
+  cudaGraph_t graph = nullptr;
+  RDCU_TRY(cudaGraphCreate(&graph, 0));
+  cudaGraphConditionalHandle cond;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&cond, graph, 1, cudaGraphCondAssignDefault);
+  cudaGraphNode_t loop = nullptr;
+  cudaGraph_t body = nullptr;
+  if (e == cudaSuccess) {
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    e = cudaGraphAddNode(&loop, graph, nullptr, 0, &cp);
+    if (e == cudaSuccess) body = cp.conditional.phGraph_out[0];
+  }
+  // one Arnoldi iteration
+  if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    cudaError_t el = cudaSuccess;
+    const double* zin = I.have_prec ? I.z : I.vj;
+    k_gm_take<<<nb, 256, 0, st>>>(I.V, I.gm, I.vj, nN);
+    if (I.have_prec) el = I.prec.precond(I.vj, I.z, 0.0, alpha_dev, st);
+    k_apply_A_dev<<<nb, 256, 0, st>>>(fd.rows_, fd.cols_, fd.vals_, alpha_dev, zin, I.w, nN);
+    for (int pass = 0; pass < 2; ++pass) {
+      k_dots_j<<<dim3(kRedBlocks, m + 1), kRedThreads, 0, st>>>(I.V, I.gm, I.w, nN, I.part);
+      k_sum_rows_j<<<m + 1, kRedThreads, 0, st>>>(I.part, I.gm, kRedBlocks, I.dots + pass * row);
+      k_vsub_j<<<nb, 256, 0, st>>>(I.V, I.gm, I.dots + pass * row, I.w, nN);
+    }
+    k_dots<<<dim3(kRedBlocks, 1), kRedThreads, 0, st>>>(I.V, 0, I.w, nN, I.part);
+    k_sum_rows<<<1, kRedThreads, 0, st>>>(I.part, 1, kRedBlocks, I.dots + 2 * row);
+    k_gm_update<<<1, 32, 0, st>>>(I.gm, I.dots, row, cond);
+    k_gm_scale<<<nb, 256, 0, st>>>(I.gm, I.w, I.V, nN);
+    if (el == cudaSuccess) el = cudaGetLastError();
+    cudaGraph_t captured = nullptr;
+    e = cudaStreamEndCapture(st, &captured);
+    if (e == cudaSuccess) e = el;
+  }
+  // after the loop: x += P^-1 (V y)
+  if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(st, graph, &loop, nullptr, 1, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    cudaError_t el = cudaSuccess;
+    k_gm_backsub<<<1, 32, 0, st>>>(I.gm);
+    k_vcomb_j<<<nb, 256, 0, st>>>(I.V, I.gm, I.w, nN);
+    if (I.have_prec) {
+      el = I.prec.precond(I.w, I.z, 0.0, alpha_dev, st);
+      k_axpy<<<nb, 256, 0, st>>>(1.0, I.z, x, nN);
+    } else {
+      k_axpy<<<nb, 256, 0, st>>>(1.0, I.w, x, nN);
+    }
+    if (el == cudaSuccess) el = cudaGetLastError();
+    cudaGraph_t captured = nullptr;
+    e = cudaStreamEndCapture(st, &captured);
+    if (e == cudaSuccess) e = el;
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&I.cycle_exec, graph, 0);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    I.cycle_exec = nullptr;
+    return e;
+  }
+  I.cycle_graph = graph;
+  I.cycle_x = x;
+  return cudaSuccess;
+}
+
+// Solves (I + alpha J) x = b.  Returns the number of GMRES iterations.  The residual
+// norm of each restart is taken on the host; each restart cycle is one launch of the
+// cycle graph and one read of its state.
 static cudaError_t gmres(BDFEngine::Impl& I, const FDProblem& fd, double alpha, const double* b, double* x,
                          cudaStream_t st, int* iters) {
   const long long nN = I.nN;
   const int nb = I.blocks;
-  const int m = I.m;
   *iters = 0;
   RDCU_TRY(vdots(I, 0, b, st));
   const double beta0 = std::sqrt(I.hdots[0]);
   RDCU_TRY(cudaMemsetAsync(x, 0, sizeof(double) * nN, st));
   if (!(beta0 > 0)) return cudaStreamSynchronize(st);
+  if (!I.cycle_exec || I.cycle_x != x) RDCU_TRY(build_cycle_graph(I, fd, x, st));
   const double tol = I.lin_tol * beta0;
-  std::vector<double> H((m + 1) * m), cs(m), sn(m), g(m + 1), y(m);
   const double* r = b;
   double beta = beta0;
   int total = 0;
@@ -441,69 +659,13 @@ static cudaError_t gmres(BDFEngine::Impl& I, const FDProblem& fd, double alpha, 
       r = I.r;
     }
     k_scale<<<nb, 256, 0, st>>>(r, 1.0 / beta, I.V, nN);
-    std::fill(g.begin(), g.end(), 0.0);
-    g[0] = beta;
-    int jdone = 0;
-    bool conv = false;
-    for (int j = 0; j < m; ++j) {
-      const double* vj = I.V + (long long)j * nN;
-      const double* zin = vj;
-      if (I.have_prec) {
-        RDCU_TRY(I.prec.precond(vj, I.z, alpha, st));
-        zin = I.z;
-      }
-      k_apply_A<<<nb, 256, 0, st>>>(fd.rows_, fd.cols_, fd.vals_, alpha, zin, I.w, nN);
-      // classical Gram-Schmidt, twice, with the projections applied on the device; one
-      // host round trip per iteration brings back both passes' coefficients and the norm
-      double hcol[64];
-      const int row = m + 2;
-      for (int pass = 0; pass < 2; ++pass) {
-        RDCU_TRY(vdots_dev(I, j + 1, I.w, st, I.dots + pass * row));
-        k_vsub<<<nb, 256, 0, st>>>(I.V, j + 1, I.dots + pass * row, I.w, nN);
-      }
-      RDCU_TRY(vdots_dev(I, 0, I.w, st, I.dots + 2 * row));
-      RDCU_TRY(cudaMemcpyAsync(I.hdots, I.dots, sizeof(double) * 3 * row, cudaMemcpyDeviceToHost, st));
-      RDCU_TRY(cudaStreamSynchronize(st));
-      for (int k = 0; k <= j; ++k) hcol[k] = (0.0 + I.hdots[k]) + I.hdots[row + k];
-      const double hn = std::sqrt(I.hdots[2 * row]);
-      ++total;
-      // Givens rotations on column j
-      for (int k = 0; k < j; ++k) {
-        const double a = cs[k] * hcol[k] + sn[k] * hcol[k + 1];
-        hcol[k + 1] = -sn[k] * hcol[k] + cs[k] * hcol[k + 1];
-        hcol[k] = a;
-      }
-      const double den = std::sqrt(hcol[j] * hcol[j] + hn * hn);
-      cs[j] = den > 0 ? hcol[j] / den : 1.0;
-      sn[j] = den > 0 ? hn / den : 0.0;
-      hcol[j] = den;
-      g[j + 1] = -sn[j] * g[j];
-      g[j] = cs[j] * g[j];
-      for (int k = 0; k <= j; ++k) H[k * m + j] = hcol[k];
-      jdone = j + 1;
-      if (std::fabs(g[j + 1]) <= tol || !(hn > 0) || total >= I.lin_max_iters) {
-        conv = std::fabs(g[j + 1]) <= tol || !(hn > 0);
-        break;
-      }
-      k_scale<<<nb, 256, 0, st>>>(I.w, 1.0 / hn, I.V + (long long)(j + 1) * nN, nN);
-    }
-    // back substitution, then x += P^-1 (V y)
-    for (int k = jdone - 1; k >= 0; --k) {
-      double acc = g[k];
-      for (int q = k + 1; q < jdone; ++q) acc -= H[k * m + q] * y[q];
-      y[k] = H[k * m + k] != 0 ? acc / H[k * m + k] : 0.0;
-    }
-    for (int k = 0; k < jdone; ++k) I.hvec_host[k] = y[k];
-    RDCU_TRY(cudaMemcpyAsync(I.hvec, I.hvec_host, sizeof(double) * jdone, cudaMemcpyHostToDevice, st));
-    k_vcomb<<<nb, 256, 0, st>>>(I.V, jdone, I.hvec, I.w, nN);
-    if (I.have_prec) {
-      RDCU_TRY(I.prec.precond(I.w, I.z, alpha, st));
-      k_axpy<<<nb, 256, 0, st>>>(1.0, I.z, x, nN);
-    } else {
-      k_axpy<<<nb, 256, 0, st>>>(1.0, I.w, x, nN);
-    }
+    k_gm_init<<<1, 64, 0, st>>>(I.gm, alpha, tol, beta, total, I.lin_max_iters);
     RDCU_TRY(cudaGetLastError());
-    if (conv) break;
+    RDCU_TRY(cudaGraphLaunch(I.cycle_exec, st));
+    RDCU_TRY(cudaMemcpyAsync(I.gm_host, I.gm, offsetof(GmresState, cs), cudaMemcpyDeviceToHost, st));
+    RDCU_TRY(cudaStreamSynchronize(st));
+    total = I.gm_host->total;
+    if (I.gm_host->conv) break;
   }
   *iters = total;
   return cudaGetLastError();

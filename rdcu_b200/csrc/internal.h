@@ -159,6 +159,7 @@ struct LinTable {
   int Ns[3];
   double dx[3];
   double alpha;        // preconditioner of I + alpha * J_lin
+  const double* alpha_dev;  // when set, alpha is read from here (device-resident solves)
 };
 
 // ----------------------------------------------------------------------------- DP45

@@ -737,10 +737,11 @@ __device__ __forceinline__ void mode_solve(const LinTable& t, const int* nidx, d
     for (int j = 0; j < kMaxPrecFields; ++j) A[i][j] = make_double2(i == j ? 1.0 : 0.0, 0.0);
     b[i] = i < n ? v[i] : make_double2(0.0, 0.0);
   }
+  const double alpha = t.alpha_dev ? *t.alpha_dev : t.alpha;
   for (int q = 0; q < t.nent; ++q) {
     const LinEntry e = t.ent[q];
     const double2 sy = lin_symbol(e, nidx, t);
-    const double cf = t.alpha * e.coef;
+    const double cf = alpha * e.coef;
 #pragma unroll
     for (int i = 0; i < kMaxPrecFields; ++i)
 #pragma unroll
@@ -2130,6 +2131,11 @@ cudaError_t SpectralPlan::launch_forward(const double* y, cudaStream_t st) {
 }
 
 cudaError_t SpectralPlan::precond(const double* r, double* z, double alpha, cudaStream_t st) {
+  return precond(r, z, alpha, nullptr, st);
+}
+
+cudaError_t SpectralPlan::precond(const double* r, double* z, double alpha, const double* alpha_dev,
+                                  cudaStream_t st) {
   RDCU_TRY(launch_forward(r, st));
   LinTable lt{};
   lt.n = n;
@@ -2139,6 +2145,7 @@ cudaError_t SpectralPlan::precond(const double* r, double* z, double alpha, cuda
   lt.sinv = sinv_;
   lt.cosv = cosv_;
   lt.alpha = alpha;
+  lt.alpha_dev = alpha_dev;
   for (int a = 0; a < 3; ++a) {
     lt.off[a] = sc_off_[a];
     lt.Ns[a] = Ns[a];

@@ -83,6 +83,8 @@ class SpectralPlan {
   bool init_precond(int n, int ndim, const int* Ns, const double* Ls, const std::vector<LinEntry>& lin,
                     std::string* msg);
   cudaError_t precond(const double* r, double* z, double alpha, cudaStream_t stream);
+  // the same with alpha read on the device from alpha_dev (captured solves)
+  cudaError_t precond(const double* r, double* z, double alpha, const double* alpha_dev, cudaStream_t stream);
 
   int n = 0, ndim = 0, Ns[3] = {1, 1, 1};
   double Ls[3] = {1, 1, 1};
