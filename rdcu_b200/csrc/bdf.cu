@@ -177,10 +177,20 @@ __global__ void k_gm_init(GmresState* s, double alpha, double tol, double beta, 
   }
 }
 
-// out = V_j
-__global__ void k_gm_take(const double* V, const GmresState* s, double* out, long long nN) {
+// Start of iteration j: for j > 0, V_j = w / ||w|| from the previous iteration (the
+// scaling k_scale did); out = V_j, the preconditioner's input.
+__global__ void k_gm_take(double* V, const GmresState* s, const double* w, double* out, long long nN) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < nN) out[i] = V[(long long)s->j * nN + i];
+  if (i >= nN) return;
+  const int j = s->j;
+  double v;
+  if (j > 0) {
+    v = s->inv_hn * w[i];
+    V[(long long)j * nN + i] = v;
+  } else {
+    v = V[i];
+  }
+  out[i] = v;
 }
 
 // y = x + alpha * (J x), alpha read on the device: the action of A = I + alpha J
@@ -195,10 +205,13 @@ __global__ void k_apply_A_dev(const int* rows, const int* cols, const double* va
   y[r] = x[r] + al * acc;
 }
 
-// k_dots, k_sum_rows and k_vsub over the j + 1 basis vectors (j read on the device;
-// rows past it return).  The same partial sums in the same order as the fixed forms.
-__global__ void k_dots_j(const double* V, const GmresState* s, const double* w, long long nN, double* part) {
-  const int nvec = s->j + 1;
+// k_dots then k_sum_rows over the j + 1 basis vectors (nvec < 0: j + 1 read on the
+// device; rows past it return) in one launch: the last block of each row to finish
+// sums that row's partials with the threads and order of k_sum_rows (bitwise the
+// same), then clears the row's arrival count.
+__global__ void k_dots_sum(const double* V, const GmresState* s, int nvec, const double* w, long long nN,
+                           double* part, unsigned int* count, double* out) {
+  if (nvec < 0) nvec = s->j + 1;
   const int row = blockIdx.y;
   if (row > nvec) return;
   const double* a = row < nvec ? V + (long long)row * nN : w;
@@ -206,16 +219,22 @@ __global__ void k_dots_j(const double* V, const GmresState* s, const double* w, 
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nN; i += (long long)gridDim.x * blockDim.x)
     sum += a[i] * w[i];
   sum = block_reduce(sum);
-  if (threadIdx.x == 0) part[(long long)row * gridDim.x + blockIdx.x] = sum;
-}
-
-__global__ void k_sum_rows_j(const double* part, const GmresState* s, int ncol, double* out) {
-  const int r = blockIdx.x;
-  if (r >= s->j + 2) return;
-  double sum = 0.0;
-  for (int c = threadIdx.x; c < ncol; c += blockDim.x) sum += part[(long long)r * ncol + c];
-  sum = block_reduce(sum);
-  if (threadIdx.x == 0) out[r] = sum;
+  __shared__ int last;
+  if (threadIdx.x == 0) {
+    part[(long long)row * gridDim.x + blockIdx.x] = sum;
+    __threadfence();
+    last = atomicAdd(&count[row], 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double t = 0.0;
+  for (int c = threadIdx.x; c < (int)gridDim.x; c += blockDim.x) t += __ldcg(&part[(long long)row * gridDim.x + c]);
+  t = block_reduce(t);
+  if (threadIdx.x == 0) {
+    out[row] = t;
+    count[row] = 0u;
+  }
 }
 
 __global__ void k_vsub_j(const double* V, const GmresState* s, const double* h, double* w, long long nN) {
@@ -266,13 +285,6 @@ __global__ void k_gm_update(GmresState* s, const double* dots, int row, cudaGrap
     s->j = j + 1;
   }
   cudaGraphSetConditional(cond, (unsigned int)cont);
-}
-
-// V_{j+1} = w / ||w|| when the loop goes on
-__global__ void k_gm_scale(const GmresState* s, const double* w, double* V, long long nN) {
-  if (!s->cont) return;
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < nN) V[(long long)s->j * nN + i] = s->inv_hn * w[i];
 }
 
 // back-substitution H y = g over the columns done (one thread)
@@ -389,6 +401,7 @@ struct BDFEngine::Impl {
   // copy of the state's header
   GmresState* gm = nullptr;
   GmresState* gm_host = nullptr;
+  unsigned int* arrivals = nullptr;  // per-row block counts of k_dots_sum (zero between launches)
   cudaGraph_t cycle_graph = nullptr;
   cudaGraphExec_t cycle_exec = nullptr;
   double* cycle_x = nullptr;  // the solution vector the graph updates
@@ -470,6 +483,9 @@ bool BDFEngine::init(FDProblem* fd, double atol, double rtol, int fixed, cudaStr
   // three rows of m+2: the two Gram-Schmidt passes and the new vector's norm
   if (cudaMalloc((void**)&I.dots, sizeof(double) * 3 * (I.m + 2)) != cudaSuccess) return fail("reductions");
   if (cudaMalloc((void**)&I.gm, sizeof(GmresState)) != cudaSuccess) return fail("GMRES state");
+  if (cudaMalloc((void**)&I.arrivals, sizeof(unsigned int) * (I.m + 2)) != cudaSuccess ||
+      cudaMemset(I.arrivals, 0, sizeof(unsigned int) * (I.m + 2)) != cudaSuccess)
+    return fail("GMRES state");
   if (cudaMallocHost((void**)&I.hdots, sizeof(double) * 3 * (I.m + 2)) != cudaSuccess) return fail("pinned");
   if (cudaMallocHost((void**)&I.gm_host, sizeof(GmresState)) != cudaSuccess) return fail("pinned");
   device_bytes = sb * (8 + 11 + I.m + 1) + fd->device_bytes;
@@ -493,6 +509,7 @@ void BDFEngine::release() {
     for (double* p : vecs)
       if (p) cudaFree(p);
     if (I.gm) cudaFree(I.gm);
+    if (I.arrivals) cudaFree(I.arrivals);
     if (I.hdots) cudaFreeHost(I.hdots);
     if (I.gm_host) cudaFreeHost(I.gm_host);
     delete impl_;
@@ -553,10 +570,10 @@ cudaError_t vdots(BDFEngine::Impl& I, int nvec, const double* w, cudaStream_t st
 }  // namespace
 
 // The GMRES(m) restart cycle as one CUDA graph: a WHILE node whose body is one Arnoldi
-// iteration -- z = P^-1 V_j, w = A z, two classical Gram-Schmidt passes, ||w||, the
-// Givens update (which clears the loop condition on convergence, after m columns or on
-// the iteration limit) and V_{j+1} = w/||w|| -- then the back-substitution and
-// x += P^-1 (V y).  The same kernels and arithmetic as one host-driven iteration at a
+// iteration -- V_j = w/||w|| of the previous iteration, z = P^-1 V_j, w = A z, two
+// classical Gram-Schmidt passes, ||w||, the Givens update (which clears the loop
+// condition on convergence, after m columns or on the iteration limit) -- then the
+// back-substitution and x += P^-1 (V y).  The same kernels and arithmetic as one host-driven iteration at a
 // time, without a host round trip per iteration.
 static cudaError_t build_cycle_graph(BDFEngine::Impl& I, const FDProblem& fd, double* x, cudaStream_t st) {
   if (I.cycle_exec) cudaGraphExecDestroy(I.cycle_exec);
@@ -588,18 +605,17 @@ static cudaError_t build_cycle_graph(BDFEngine::Impl& I, const FDProblem& fd, do
   if (e == cudaSuccess) {
     cudaError_t el = cudaSuccess;
     const double* zin = I.have_prec ? I.z : I.vj;
-    k_gm_take<<<nb, 256, 0, st>>>(I.V, I.gm, I.vj, nN);
+    k_gm_take<<<nb, 256, 0, st>>>(I.V, I.gm, I.w, I.vj, nN);
     if (I.have_prec) el = I.prec.precond(I.vj, I.z, 0.0, alpha_dev, st);
     k_apply_A_dev<<<nb, 256, 0, st>>>(fd.rows_, fd.cols_, fd.vals_, alpha_dev, zin, I.w, nN);
     for (int pass = 0; pass < 2; ++pass) {
-      k_dots_j<<<dim3(kRedBlocks, m + 1), kRedThreads, 0, st>>>(I.V, I.gm, I.w, nN, I.part);
-      k_sum_rows_j<<<m + 1, kRedThreads, 0, st>>>(I.part, I.gm, kRedBlocks, I.dots + pass * row);
+      k_dots_sum<<<dim3(kRedBlocks, m + 1), kRedThreads, 0, st>>>(I.V, I.gm, -1, I.w, nN, I.part, I.arrivals,
+                                                                  I.dots + pass * row);
       k_vsub_j<<<nb, 256, 0, st>>>(I.V, I.gm, I.dots + pass * row, I.w, nN);
     }
-    k_dots<<<dim3(kRedBlocks, 1), kRedThreads, 0, st>>>(I.V, 0, I.w, nN, I.part);
-    k_sum_rows<<<1, kRedThreads, 0, st>>>(I.part, 1, kRedBlocks, I.dots + 2 * row);
+    k_dots_sum<<<dim3(kRedBlocks, 1), kRedThreads, 0, st>>>(I.V, I.gm, 0, I.w, nN, I.part, I.arrivals,
+                                                            I.dots + 2 * row);
     k_gm_update<<<1, 32, 0, st>>>(I.gm, I.dots, row, cond);
-    k_gm_scale<<<nb, 256, 0, st>>>(I.gm, I.w, I.V, nN);
     if (el == cudaSuccess) el = cudaGetLastError();
     cudaGraph_t captured = nullptr;
     e = cudaStreamEndCapture(st, &captured);
