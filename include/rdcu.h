@@ -175,6 +175,12 @@ int rdcu_profile_passes(rdcu_t *h, int reps, rdcu_pass_timing *out, int max_pass
 /* Accepted steps and attempts counted by the last rdcu_solve. */
 int rdcu_get_counters(rdcu_t *h, long long *accepted, long long *attempts);
 
+/* Linear-solver statistics of a BDF handle since its creation: GMRES iterations, linear
+ * solves (one per Newton iteration, where the reference calls cudssExecute SOLVE,
+ * bdf.cu:176-180) and GMRES(40) restart cycles.  Zeros for DP45 handles.  Any output
+ * pointer may be NULL. */
+int rdcu_get_linear_stats(rdcu_t *h, long long *iterations, long long *solves, long long *cycles);
+
 /* Uniform random initial condition of the reference CLI (rdcu.cu:898,991-1001):
  * srand(seed); y[N*i+j] = A0 + A/2*(2.0/RAND_MAX*rand()-1), field loop outer, with the
  * C library's own rand().  y: host array of n*N doubles.  No handle needed. */

@@ -41,7 +41,7 @@ EV_CHECKPOINT = 2
 # exported entry points of include/rdcu.h
 EXPORTS = [
     "rdcu_create", "rdcu_destroy", "rdcu_set_state", "rdcu_get_state", "rdcu_get_info",
-    "rdcu_rhs", "rdcu_jac", "rdcu_step", "rdcu_eval", "rdcu_solve", "rdcu_get_counters",
+    "rdcu_rhs", "rdcu_jac", "rdcu_step", "rdcu_eval", "rdcu_solve", "rdcu_get_counters", "rdcu_get_linear_stats",
     "rdcu_memcpy", "rdcu_advance", "rdcu_random_ic", "rdcu_profile_passes", "rdcu_rhs_noalloc",
     "rdcu_set_coefficients", "rdcu_adjoint_forward", "rdcu_adjoint_backward",
     "rdcu_ensemble_create", "rdcu_ensemble_destroy", "rdcu_ensemble_set_state", "rdcu_ensemble_get_state",
@@ -117,6 +117,8 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
     lib.rdcu_eval.argtypes = [vp, d, vp]
     lib.rdcu_solve.argtypes = [vp, d, d, d, pd, i, OUT_CB, vp]
     lib.rdcu_get_counters.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]
+    lib.rdcu_get_linear_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
+                                          ctypes.POINTER(ctypes.c_longlong)]
     lib.rdcu_memcpy.argtypes = [vp, vp, vp, ctypes.c_ulonglong]
     lib.rdcu_advance.argtypes = [vp, i, d, d, ctypes.POINTER(ctypes.c_longlong)]
     lib.rdcu_random_ic.argtypes = [pd, i, ctypes.c_longlong, d, d, i]
@@ -354,6 +356,13 @@ class Solver:
         a, b = ctypes.c_longlong(), ctypes.c_longlong()
         self._check(self.lib.rdcu_get_counters(self.h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
+
+    def linear_stats(self):
+        """BDF linear-solver statistics since creation: (GMRES iterations, linear solves,
+        restart cycles); zeros for DP45 handles."""
+        it, so, cy = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        self._check(self.lib.rdcu_get_linear_stats(self.h, ctypes.byref(it), ctypes.byref(so), ctypes.byref(cy)))
+        return it.value, so.value, cy.value
 
     @property
     def nterms(self) -> int:

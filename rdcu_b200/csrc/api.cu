@@ -475,6 +475,15 @@ int rdcu_get_counters(rdcu_t* h, long long* accepted, long long* attempts) {
   return RDCU_OK;
 }
 
+int rdcu_get_linear_stats(rdcu_t* h, long long* iterations, long long* solves, long long* cycles) {
+  if (!h) return set_err(h, RDCU_ERR_INVALID, "null argument");
+  const BDFEngine* b = h->bdf.get();
+  if (iterations) *iterations = b ? b->lin_iters : 0;
+  if (solves) *solves = b ? b->lin_solves : 0;
+  if (cycles) *cycles = b ? b->lin_cycles : 0;
+  return RDCU_OK;
+}
+
 int rdcu_set_coefficients(rdcu_t* h, const double* C) {
   if (!h || (!C && !h->terms.empty())) return set_err(h, RDCU_ERR_INVALID, "null argument");
   if (!h->sp) return set_err(h, RDCU_ERR_UNSUPPORTED, "coefficients can be replaced on pseudospectral handles");

@@ -649,14 +649,15 @@ static cudaError_t build_cycle_graph(BDFEngine::Impl& I, const FDProblem& fd, do
   return cudaSuccess;
 }
 
-// Solves (I + alpha J) x = b.  Returns the number of GMRES iterations.  The residual
-// norm of each restart is taken on the host; each restart cycle is one launch of the
-// cycle graph and one read of its state.
+// Solves (I + alpha J) x = b.  Returns the number of GMRES iterations and restart
+// cycles.  The residual norm of each restart is taken on the host; each restart cycle
+// is one launch of the cycle graph and one read of its state.
 static cudaError_t gmres(BDFEngine::Impl& I, const FDProblem& fd, double alpha, const double* b, double* x,
-                         cudaStream_t st, int* iters) {
+                         cudaStream_t st, int* iters, int* cycles) {
   const long long nN = I.nN;
   const int nb = I.blocks;
   *iters = 0;
+  *cycles = 0;
   RDCU_TRY(vdots(I, 0, b, st));
   const double beta0 = std::sqrt(I.hdots[0]);
   RDCU_TRY(cudaMemsetAsync(x, 0, sizeof(double) * nN, st));
@@ -678,6 +679,7 @@ static cudaError_t gmres(BDFEngine::Impl& I, const FDProblem& fd, double alpha, 
     k_gm_init<<<1, 64, 0, st>>>(I.gm, alpha, tol, beta, total, I.lin_max_iters);
     RDCU_TRY(cudaGetLastError());
     RDCU_TRY(cudaGraphLaunch(I.cycle_exec, st));
+    ++*cycles;
     RDCU_TRY(cudaMemcpyAsync(I.gm_host, I.gm, offsetof(GmresState, cs), cudaMemcpyDeviceToHost, st));
     RDCU_TRY(cudaStreamSynchronize(st));
     total = I.gm_host->total;
@@ -729,9 +731,10 @@ cudaError_t BDFEngine::step(double* t, double* h, double hmin, double hmax, int*
       I.refactor = 0;
     }
     k_newton_rhs<<<nb, 256, 0, st_>>>(I.b, I.f, I.d, D_, nN, order, hh, (1 - kKappa[order]) * kGamma[order], gam);
-    int iters = 0;
-    RDCU_TRY(gmres(I, *fd_, I.alpha, I.b, I.dd, st_, &iters));
+    int iters = 0, cycles = 0;
+    RDCU_TRY(gmres(I, *fd_, I.alpha, I.b, I.dd, st_, &iters, &cycles));
     lin_iters += iters;
+    lin_cycles += cycles;
     ++lin_solves;
     RDCU_TRY(wnorm(I, I.dd, st_, &dnorm));
     dnorm /= sqN;

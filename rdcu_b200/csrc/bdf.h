@@ -37,7 +37,7 @@ class BDFEngine {
   size_t device_bytes = 0;
   std::string last_msg;
   // linear-solver statistics
-  long long lin_iters = 0, lin_solves = 0;
+  long long lin_iters = 0, lin_solves = 0, lin_cycles = 0;
 
   struct Impl;
 
