@@ -448,6 +448,7 @@ def run_bdf(args):
     stream = torch.cuda.ExternalStream(s.stream)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
+    lin0 = s.linear_stats()
     with ClockSampler(0) as clk:
         e0.record(stream)
         s.solve(T_B, [])
@@ -455,6 +456,7 @@ def run_bdf(args):
         e1.synchronize()
     sec = e0.elapsed_time(e1) / 1e3
     acc, att = s.counters()
+    lin = [b - a for a, b in zip(lin0, s.linear_stats())]
     # e2e: the same window from host arrays through the C ABI, final state to the host
     w0 = time.perf_counter()
     s.set_state(tA, hA, yA.ctypes.data, oA, D.ctypes.data)
@@ -471,6 +473,7 @@ def run_bdf(args):
         "config": {"workload": args.workload, "grid": list(Ns), "L": list(Ls), "method": "BDF (NDF orders 1-5), FD",
                    "rtol": 1e-6, "atol": 1e-6, "window_sim_time": [T_A, T_B], "accepted_steps": acc,
                    "attempts": att, "linear_solver": "GMRES(40), FFT preconditioner",
+                   "gmres": {"iterations": lin[0], "solves": lin[1], "restart_cycles": lin[2]},
                    "l2": "state 1 MB: L2-resident (latency-bound regime)"},
         "clocks": clk.summary(),
         "e2e": {"value": N * acc2 / e2e_s, "unit": "grid-pt·steps/s", "h2d_bytes_per_step": 9 * nN * 8 / args.steps,
