@@ -573,8 +573,8 @@ cudaError_t vdots(BDFEngine::Impl& I, int nvec, const double* w, cudaStream_t st
 // iteration -- V_j = w/||w|| of the previous iteration, z = P^-1 V_j, w = A z, two
 // classical Gram-Schmidt passes, ||w||, the Givens update (which clears the loop
 // condition on convergence, after m columns or on the iteration limit) -- then the
-// back-substitution and x += P^-1 (V y).  The same kernels and arithmetic as one host-driven iteration at a
-// time, without a host round trip per iteration.
+// back-substitution and x += P^-1 (V y).  No host round trip per iteration: the host
+// launches the graph once per cycle and reads back the state's header.
 static cudaError_t build_cycle_graph(BDFEngine::Impl& I, const FDProblem& fd, double* x, cudaStream_t st) {
   if (I.cycle_exec) cudaGraphExecDestroy(I.cycle_exec);
   if (I.cycle_graph) cudaGraphDestroy(I.cycle_graph);
