@@ -7,15 +7,20 @@ reference makelines.py:260-268); the same CLI is built here as ``rdcu_b200/bin/r
 This module exposes the library itself to Python: problem handles, RHS and Jacobian
 evaluation, stepping, dense output and whole integrations with an output callback.
 
-Device memory is passed as raw CUDA pointers (for example ``torch.Tensor.data_ptr()``
-of a float64 CUDA tensor).  There is no CPU fallback: loading fails loudly when the
-library is missing.
+Buffers are passed as integer addresses (host or device, for example
+``torch.Tensor.data_ptr()`` of a float64 CUDA tensor) or as the array or tensor itself,
+which keeps it alive for the call (see ``_addr``).  There is no CPU fallback: loading
+fails loudly when the library is missing.
 """
 from __future__ import annotations
 
 import ctypes
+import numbers
 import os
-from typing import Callable, List, Optional, Sequence
+from typing import Callable, List, Optional, Sequence, Union
+
+# a buffer argument: an integer address, a numpy array or a tensor (see _addr)
+Buffer = Union[int, "numpy.ndarray", "torch.Tensor"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "librdcu.so")
@@ -93,6 +98,27 @@ class rdcu_pass_timing(ctypes.Structure):
 OUT_CB = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(rdcu_event))
 
 _lib = None
+
+
+def _addr(x) -> Optional[ctypes.c_void_p]:
+    """A buffer argument as a C pointer.  Accepts an integer address (0 or None: NULL), a
+    C-contiguous numpy array or a contiguous tensor (its ``data_ptr()``).  An array or
+    tensor passed this way stays referenced for the whole call.  An address taken from
+    a temporary (``np.array(y).ctypes.data``) does not: the library may read freed
+    memory."""
+    if x is None:
+        return None
+    if isinstance(x, numbers.Integral) and not isinstance(x, bool):
+        return ctypes.c_void_p(int(x)) if int(x) else None
+    if hasattr(x, "data_ptr"):
+        if hasattr(x, "is_contiguous") and not x.is_contiguous():
+            raise ValueError("tensor arguments must be contiguous")
+        return ctypes.c_void_p(x.data_ptr())
+    if hasattr(x, "__array_interface__") and hasattr(x, "flags"):
+        if not x.flags["C_CONTIGUOUS"]:
+            raise ValueError("array arguments must be C-contiguous")
+        return ctypes.c_void_p(x.ctypes.data)
+    raise TypeError("expected an address, a numpy array or a tensor, got %s" % type(x).__name__)
 
 
 def load_library(path: Optional[str] = None) -> ctypes.CDLL:
@@ -189,7 +215,7 @@ def random_ic(n: int, N: int, A: float, A0: float, seed: int):
 NOALLOC_SCRATCH_BYTES = 64 << 20
 
 
-def rhs_noalloc(n: int, Ns: Sequence[int], Ls: Sequence[float], terms, y_ptr: int, f_ptr: int,
+def rhs_noalloc(n: int, Ns: Sequence[int], Ls: Sequence[float], terms, y_ptr: Buffer, f_ptr: Buffer,
                 stream: int = 0, device: int = 0) -> None:
     """f = RHS(y) of a pseudospectral problem through rdcu_rhs_noalloc, the entry point
     that allocates no device memory (for callers that cannot allocate: its scratch is a
@@ -214,7 +240,7 @@ def rhs_noalloc(n: int, Ns: Sequence[int], Ls: Sequence[float], terms, y_ptr: in
     spec.c = ctypes.cast(cps, ctypes.POINTER(ctypes.POINTER(ctypes.c_int)))
     spec.method = METHOD_DP45
     spec.device = device
-    rc = lib.rdcu_rhs_noalloc(ctypes.byref(spec), ctypes.c_void_p(y_ptr), ctypes.c_void_p(f_ptr),
+    rc = lib.rdcu_rhs_noalloc(ctypes.byref(spec), _addr(y_ptr), _addr(f_ptr),
                               ctypes.c_void_p(stream) if stream else None)
     if rc != RDCU_OK:
         raise RdcuError(rc, lib.rdcu_last_error(None).decode())
@@ -280,26 +306,22 @@ class Solver:
     def stream(self) -> int:
         return self.info().stream
 
-    def set_state(self, t: float, h: float, y_ptr: int, order: int = 0, D_ptr: int = 0):
-        self._check(self.lib.rdcu_set_state(self.h, t, h, ctypes.c_void_p(y_ptr), order,
-                                            ctypes.c_void_p(D_ptr) if D_ptr else None))
+    def set_state(self, t: float, h: float, y_ptr: Buffer, order: int = 0, D_ptr: Buffer = 0):
+        self._check(self.lib.rdcu_set_state(self.h, t, h, _addr(y_ptr), order, _addr(D_ptr)))
 
-    def get_state(self, y_ptr: int = 0, D_ptr: int = 0):
+    def get_state(self, y_ptr: Buffer = 0, D_ptr: Buffer = 0):
         t, h, o = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
         self._check(self.lib.rdcu_get_state(self.h, ctypes.byref(t), ctypes.byref(h), ctypes.byref(o),
-                                            ctypes.c_void_p(y_ptr) if y_ptr else None,
-                                            ctypes.c_void_p(D_ptr) if D_ptr else None))
+                                            _addr(y_ptr), _addr(D_ptr)))
         return t.value, h.value, o.value
 
-    def rhs(self, y_ptr: int, f_ptr: int, Y_ptr: int = 0, t: float = 0.0):
-        self._check(self.lib.rdcu_rhs(self.h, t, ctypes.c_void_p(y_ptr), ctypes.c_void_p(f_ptr),
-                                      ctypes.c_void_p(Y_ptr) if Y_ptr else None))
+    def rhs(self, y_ptr: Buffer, f_ptr: Buffer, Y_ptr: Buffer = 0, t: float = 0.0):
+        self._check(self.lib.rdcu_rhs(self.h, t, _addr(y_ptr), _addr(f_ptr), _addr(Y_ptr)))
 
-    def jac(self, y_ptr: int, rows_ptr: int, cols_ptr: int, vals_ptr: int, t: float = 0.0) -> int:
+    def jac(self, y_ptr: Buffer, rows_ptr: Buffer, cols_ptr: Buffer, vals_ptr: Buffer, t: float = 0.0) -> int:
         nnz = ctypes.c_int()
-        self._check(self.lib.rdcu_jac(self.h, t, ctypes.c_void_p(y_ptr), ctypes.byref(nnz),
-                                      ctypes.c_void_p(rows_ptr), ctypes.c_void_p(cols_ptr),
-                                      ctypes.c_void_p(vals_ptr)))
+        self._check(self.lib.rdcu_jac(self.h, t, _addr(y_ptr), ctypes.byref(nnz), _addr(rows_ptr),
+                                      _addr(cols_ptr), _addr(vals_ptr)))
         return nnz.value
 
     def step(self, t: float, h: float, hmin: float = 0.0, hmax: float = float("inf")):
@@ -308,8 +330,8 @@ class Solver:
                                        ctypes.byref(acc)))
         return bool(acc.value), tt.value, hh.value
 
-    def eval(self, t_eval: float, y_ptr: int):
-        self._check(self.lib.rdcu_eval(self.h, t_eval, ctypes.c_void_p(y_ptr)))
+    def eval(self, t_eval: float, y_ptr: Buffer):
+        self._check(self.lib.rdcu_eval(self.h, t_eval, _addr(y_ptr)))
 
     def solve(self, t1: float, t_eval: Sequence[float] = (), hmin: float = 0.0, hmax: float = float("inf"),
               callback: Optional[Callable[[rdcu_event], int]] = None):
@@ -327,9 +349,9 @@ class Solver:
         self._check(self.lib.rdcu_solve(self.h, t1, hmin, hmax, ctypes.cast(te, ctypes.POINTER(ctypes.c_double)),
                                         len(t_eval), cb, None))
 
-    def memcpy(self, dst: int, src: int, nbytes: int):
+    def memcpy(self, dst: Buffer, src: Buffer, nbytes: int):
         """Synchronous copy between host/device addresses."""
-        self._check(self.lib.rdcu_memcpy(self.h, ctypes.c_void_p(dst), ctypes.c_void_p(src), nbytes))
+        self._check(self.lib.rdcu_memcpy(self.h, _addr(dst), _addr(src), nbytes))
 
     def copy_to_numpy(self, src: int, count: int):
         """float64 array of `count` values copied from a device address."""
@@ -377,18 +399,16 @@ class Solver:
         for k, c in enumerate(C):
             self._C[k] = float(c)
 
-    def adjoint_forward(self, y0_ptr: int, hs: Sequence[float], K: int = 50, yT_ptr: int = 0):
+    def adjoint_forward(self, y0_ptr: Buffer, hs: Sequence[float], K: int = 50, yT_ptr: Buffer = 0):
         """DP45 over the step sizes hs from y0 (fixed steps), checkpointing every K steps."""
         arr = (ctypes.c_double * max(1, len(hs)))(*[float(h) for h in hs])
-        self._check(self.lib.rdcu_adjoint_forward(self.h, ctypes.c_void_p(y0_ptr), arr, len(hs), int(K),
-                                                  ctypes.c_void_p(yT_ptr) if yT_ptr else None))
+        self._check(self.lib.rdcu_adjoint_forward(self.h, _addr(y0_ptr), arr, len(hs), int(K), _addr(yT_ptr)))
 
-    def adjoint_backward(self, lamT_ptr: int, grad_y0_ptr: int = 0):
+    def adjoint_backward(self, lamT_ptr: Buffer, grad_y0_ptr: Buffer = 0):
         """dL/dy0 (written to grad_y0_ptr) and dL/dC (returned, one per term) of the last
         adjoint_forward, given dL/dyT at lamT_ptr."""
         g = (ctypes.c_double * max(1, self.nterms))()
-        self._check(self.lib.rdcu_adjoint_backward(self.h, ctypes.c_void_p(lamT_ptr),
-                                                   ctypes.c_void_p(grad_y0_ptr) if grad_y0_ptr else None, g))
+        self._check(self.lib.rdcu_adjoint_backward(self.h, _addr(lamT_ptr), _addr(grad_y0_ptr), g))
         return [g[k] for k in range(self.nterms)]
 
 
@@ -457,13 +477,13 @@ class Ensemble:
     def __len__(self):
         return len(self.sizes)
 
-    def set_state(self, i: int, t: float, h: float, y_ptr: int):
-        self._check(self.lib.rdcu_ensemble_set_state(self.e, i, t, h, ctypes.c_void_p(y_ptr)))
+    def set_state(self, i: int, t: float, h: float, y_ptr: Buffer):
+        self._check(self.lib.rdcu_ensemble_set_state(self.e, i, t, h, _addr(y_ptr)))
 
-    def get_state(self, i: int, y_ptr: int = 0):
+    def get_state(self, i: int, y_ptr: Buffer = 0):
         t, h = ctypes.c_double(), ctypes.c_double()
         self._check(self.lib.rdcu_ensemble_get_state(self.e, i, ctypes.byref(t), ctypes.byref(h),
-                                                     ctypes.c_void_p(y_ptr) if y_ptr else None))
+                                                     _addr(y_ptr)))
         return t.value, h.value
 
     def solve(self, t1: float, hmin: float = 0.0, hmax: float = float("inf")):

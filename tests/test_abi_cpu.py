@@ -96,3 +96,27 @@ def test_problem_coupling_lists_match_the_oracle():
             parsed = [op.parse_term(s) for s in pp.cgle_coupling_lines(ndim, b, c)]
             assert any(abs(t.C - c) < 1e-6 for t in parsed) and any(abs(t.C + b) < 1e-6 for t in parsed)
     assert pp.brusselator_coupling_lines() == op.brusselator_coupling_lines()
+
+
+def test_buffer_arguments():
+    """Buffers go to the C ABI as addresses, arrays or tensors; arrays and tensors must
+    be contiguous; 0 and None are NULL."""
+    import numpy as np
+    import torch
+
+    import rdcu_b200 as R
+
+    a = np.zeros(4)
+    assert R._addr(a).value == a.ctypes.data
+    assert R._addr(0) is None and R._addr(None) is None
+    assert R._addr(np.int64(16)).value == 16
+    t = torch.zeros(3, dtype=torch.float64)
+    assert R._addr(t).value == t.data_ptr()
+    with pytest.raises(ValueError):
+        R._addr(np.zeros((4, 4))[:, 1])
+    with pytest.raises(ValueError):
+        R._addr(torch.zeros(4, 4)[:, 1])
+    with pytest.raises(TypeError):
+        R._addr(True)
+    with pytest.raises(TypeError):
+        R._addr("0x10")

@@ -163,3 +163,29 @@ def test_dictionary_forms(cuda, case):
     y = rng.uniform(-1, 1, prob.n * prob.N)
     f, _ = gpu_rhs(cuda, prob, y)
     assert rel_err(f, osp.rhs(y, prob)) < TOL
+
+
+def test_array_and_tensor_arguments(cuda):
+    """Host arrays and CUDA tensors passed as buffers give the same results as integer
+    addresses. A temporary passed itself is safe, because the call holds it."""
+    import torch
+
+    import rdcu_b200 as R
+
+    prob = Problem(2, (16, 16), (20.0, 20.0), cgle_terms(2))
+    y = np.random.default_rng(9).uniform(-1, 1, 2 * prob.N)
+    s = R.Solver(prob.n, prob.Ns, prob.Ls, spec_terms(prob))
+    f1 = np.empty_like(y)
+    s.rhs(y.ctypes.data, f1.ctypes.data)
+    f2 = np.empty_like(y)
+    s.rhs(y, f2)
+    yd = torch.tensor(y, device="cuda")
+    fd = torch.empty_like(yd)
+    s.rhs(yd, fd)
+    torch.cuda.synchronize()
+    assert np.array_equal(f1, f2) and np.array_equal(f1, fd.cpu().numpy())
+    s.set_state(0.0, 1e-3, np.array(y))
+    out = np.empty_like(y)
+    s.get_state(out)
+    assert np.array_equal(out, y)
+    s.close()
