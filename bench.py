@@ -918,15 +918,12 @@ def cpu_baseline(Ns, Ls, y, t, h):
 
 # ----------------------------------------------------------------------------- reference arm
 def reference_binary():
+    """The reference's own build, compiled beforehand from its sources by
+    oracle/build_ref.sh (the build step does it where the sources are present)."""
     p = os.path.join(ROOT, "oracle", "_ref", "rdcu_ref")
     if os.path.exists(p):
         return p, None
-    if os.path.exists("/root/reference/rdcu.cu"):
-        r = subprocess.run(["bash", os.path.join(ROOT, "oracle", "build_ref.sh")], capture_output=True, text=True)
-        if r.returncode == 0 and os.path.exists(p):
-            return p, None
-        return None, "reference build failed: " + r.stderr.strip().splitlines()[-1] if r.stderr else "build failed"
-    return None, "reference binary oracle/_ref/rdcu_ref not built and reference sources absent"
+    return None, "reference binary oracle/_ref/rdcu_ref not built (oracle/build_ref.sh builds it from the sources)"
 
 
 def run_reference(args):

@@ -122,7 +122,7 @@ def read_coupling_file(path: str) -> List[Term]:
 
 def y_names(n: int, ndim: int) -> List[str]:
     """Y-index table printed by ``-h`` (rdcu.cu:769-785) and used in the verbose
-    equation print (rdcu.cu:789-805).  Index k = Yind*n + field (survey of rdcu.cu)."""
+    equation print (rdcu.cu:789-805).  Index k = Yind*n + field."""
     names = [f"u{i}" for i in range(n)]
     for j in range(ndim):
         for i in range(n):
