@@ -5,7 +5,9 @@ constants (bdf.cu:8-9,23), ``makeRU`` (bdf.cu:35-69), kernels ``updateD``, ``err
 ``step0``, ``rhs``, ``interpolate``, ``scale_err`` (bdf.cu:72-132), ``bdf_step``
 (bdf.cu:135-323), ``bdf_eval`` (bdf.cu:325-328), ``bdf_run`` (bdf.cu:330-389) and the
 tolerance set-up of ``bdf_init`` (bdf.cu:391-401).  The cuDSS LU of A = I + alpha*J is
-replaced by scipy's SuperLU on the same CSR matrix (a direct solve, like cuDSS).
+replaced by scipy's SuperLU on the same CSR matrix (a direct solve, like cuDSS), or,
+with ``linear="gmres"``, by the restarted GMRES(40) of ``oracle.gmres`` (the library's
+solver in its unpreconditioned form).
 """
 from __future__ import annotations
 
@@ -69,7 +71,7 @@ class BDF:
 
     def __init__(self, D0: np.ndarray, order: int, atol: float, rtol: float, fixed: bool,
                  dydt: Callable[[float, np.ndarray], np.ndarray],
-                 jac: Callable[[float, np.ndarray], tuple]):
+                 jac: Callable[[float, np.ndarray], tuple], linear: str = "lu"):
         # D has 8 slots (bdf.cu:416); slots 0..order come from the caller (bdf.cu:449)
         self.N = D0[0].size
         self.D = [np.zeros(self.N) for _ in range(8)]
@@ -83,6 +85,10 @@ class BDF:
         self.nconststeps = 0.0
         self.J = None
         self.lu = None
+        if linear not in ("lu", "gmres"):
+            raise ValueError("linear solver: 'lu' or 'gmres'")
+        self.linear = linear
+        self.lin_stats = {"iterations": 0, "solves": 0, "cycles": 0}
 
     def _set_jac(self, t, y):
         rows, cols, vals = self.jacf(t, y)
@@ -90,7 +96,12 @@ class BDF:
 
     def _refactor(self, alpha):
         A = sp.identity(self.N, format="csr") + alpha * self.J
-        self.lu = spla.splu(A.tocsc())
+        if self.linear == "gmres":
+            from oracle.gmres import Gmres
+
+            self.lu = Gmres(A, self.lin_stats)
+        else:
+            self.lu = spla.splu(A.tocsc())
 
     def _update_D(self, factor):
         RU = make_RU(self.order, factor)

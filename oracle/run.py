@@ -45,6 +45,7 @@ class RunConfig:
     rtol: float = 1e-8
     atol: float = 1e-8
     max_attempts: int | None = None
+    linear: str = "lu"  # BDF linear solver: "lu" (direct, as cuDSS) or "gmres" (oracle.gmres)
 
 
 def run(filebase: str, cfg: RunConfig) -> dict:
@@ -132,7 +133,7 @@ def run(filebase: str, cfg: RunConfig) -> dict:
     state = {"steps": 0, "eval_i": 0, "attempts": 0}
     if cfg.stiff:
         D0 = [y] + list(D_re)
-        stepper = obdf.BDF(D0, order, cfg.atol, cfg.rtol, cfg.fixed, dydt, jac)
+        stepper = obdf.BDF(D0, order, cfg.atol, cfg.rtol, cfg.fixed, dydt, jac, linear=cfg.linear)
     else:
         stepper = odp.DP45(y, cfg.atol, cfg.rtol, cfg.fixed, dydt)
 
@@ -177,7 +178,7 @@ def run(filebase: str, cfg: RunConfig) -> dict:
     for fh in files.values():
         fh.close()
     return {"steps": state["steps"], "attempts": state["attempts"], "t": t, "h": h,
-            "order": getattr(stepper, "order", None)}
+            "order": getattr(stepper, "order", None), "linear": getattr(stepper, "lin_stats", None)}
 
 
 def config_from_argv(argv: List[str]):

@@ -73,3 +73,19 @@ def defect_state(Ns, seed: int, frame: int = 0, nterms: int = 3, noise: float = 
     th += noise * np.random.default_rng([seed, frame]).normal(size=Ns)
     r = 1.0 + 0.2 * np.random.default_rng([seed, frame, 1]).uniform(size=Ns)
     return np.concatenate([(r * np.cos(th)).ravel(), (r * np.sin(th)).ravel()])
+
+
+def five_field_stiff_problem():
+    """A stiff system of five coupled diffusing fields on an 8 x 8 periodic grid, L = 8:
+    u_f' = D_f (d00 + d11) u_f - u_f + 0.5 u_{f+1} - 0.2 u_f^3, D = 10, 20, 40, 80, 5
+    (d00 u_f = Y[15+f], d11 u_f = Y[30+f] for n = 5).  Five fields are beyond the BDF
+    preconditioner, and at rtol = 1e-4 the late steps (h ~ 0.15) make GMRES(40) restart.
+    Returns the problem and the initial state, U[0.5, 1.5] with numpy seed 6."""
+    n = 5
+    D = [10.0, 20.0, 40.0, 80.0, 5.0]
+    lines = []
+    for f in range(n):
+        lines += ["%g,%d,%d,1" % (D[f], f, 15 + f), "%g,%d,%d,1" % (D[f], f, 30 + f), "-1.0,%d,%d,1" % (f, f),
+                  "0.5,%d,%d,1" % (f, (f + 1) % n), "-0.2,%d,%d,3" % (f, f)]
+    prob = Problem(n, (8, 8), (8.0, 8.0), [parse_term(s) for s in lines])
+    return prob, np.random.default_rng(6).uniform(0.5, 1.5, n * prob.N)

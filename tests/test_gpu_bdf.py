@@ -14,7 +14,7 @@ import pytest
 from oracle import fd as ofd
 from oracle import run as orun
 from oracle.problem import Problem, brusselator_coupling_lines, cgle_terms, parse_term
-from tests.helpers import rel_err, random_terms, spec_terms
+from tests.helpers import five_field_stiff_problem, rel_err, random_terms, spec_terms
 
 pytestmark = pytest.mark.gpu
 
@@ -119,19 +119,12 @@ def test_unpreconditioned_gmres_with_restarts(cuda):
     """Five fields, one more than the preconditioner's n x n mode solves take, so the
     linear solves run plain GMRES(40); on this stiff diffusion system (condition ~100)
     most solves need several restart cycles to reach the 1e-12 relative residual.  The
-    run must match the direct-solve oracle step for step, as the preconditioned runs do."""
+    run must match the direct-solve oracle step for step, as the preconditioned runs do,
+    and its solver counts must match the oracle's restatement of the same GMRES."""
     import rdcu_b200 as R
 
-    n = 5
-    # stiff enough that a solve at the run's later steps (h up to ~0.15) takes ~100 iterations
-    D = [10.0, 20.0, 40.0, 80.0, 5.0]
-    lines = []
-    for f in range(n):
-        # D_f (d00 + d11) u_f - u_f + 0.5 u_{f+1} - 0.2 u_f^3; d00 u_f = Y[15+f], d11 u_f = Y[30+f]
-        lines += ["%g,%d,%d,1" % (D[f], f, 15 + f), "%g,%d,%d,1" % (D[f], f, 30 + f), "-1.0,%d,%d,1" % (f, f),
-                  "0.5,%d,%d,1" % (f, (f + 1) % n), "-0.2,%d,%d,3" % (f, f)]
-    prob = Problem(n, (8, 8), (8.0, 8.0), [parse_term(s) for s in lines])
-    y0 = np.random.default_rng(6).uniform(0.5, 1.5, n * prob.N)
+    prob, y0 = five_field_stiff_problem()
+    n = prob.n
     t1, dt, rtol = 1.0, 0.5, 1e-4
     s = _solver(prob, rtol=rtol, atol=rtol)
     y = np.array(y0)  # the library reads the state from this buffer
@@ -150,20 +143,27 @@ def test_unpreconditioned_gmres_with_restarts(cuda):
     iters, solves, cycles = s.linear_stats()
     s.close()
     assert solves > 0 and cycles > solves and iters > 40 * (cycles - solves)
-    with tempfile.TemporaryDirectory() as wd:
-        fb = wd + "/o"
-        y0.tofile(fb + "ic.dat")
-        cfg = orun.RunConfig(n=n, Ns=prob.Ns, Ls=prob.Ls, terms=prob.terms, t1=t1, dt=dt, rtol=rtol, atol=rtol,
-                             stiff=True)
-        summ = orun.run(fb, cfg)
-        oh = np.fromfile(fb + "steps.dat")
-        ost = np.fromfile(fb + "states.dat").reshape(-1, n * prob.N)[1:]
+    out = {}
+    for linear in ("lu", "gmres"):
+        with tempfile.TemporaryDirectory() as wd:
+            fb = wd + "/o"
+            y0.tofile(fb + "ic.dat")
+            cfg = orun.RunConfig(n=n, Ns=prob.Ns, Ls=prob.Ls, terms=prob.terms, t1=t1, dt=dt, rtol=rtol,
+                                 atol=rtol, stiff=True, linear=linear)
+            summ = orun.run(fb, cfg)
+            out[linear] = (summ, np.fromfile(fb + "steps.dat"),
+                           np.fromfile(fb + "states.dat").reshape(-1, n * prob.N)[1:])
+    summ, oh, ost = out["lu"]
     assert sum(ev["acc"]) == summ["steps"]
     assert len(ev["h"]) == len(oh)
     assert np.max(np.abs(np.array(ev["h"]) - oh) / np.abs(oh)) < 1e-8
     assert len(ev["states"]) == len(ost)
     for a, b in zip(ev["states"], ost):
         assert rel_err(a, b) < 1e-8
+    st = out["gmres"][0]["linear"]
+    assert solves == st["solves"]
+    assert abs(iters - st["iterations"]) <= 0.02 * st["iterations"]
+    assert abs(cycles - st["cycles"]) <= 0.02 * st["cycles"]
 
 
 def test_linear_stats_of_a_dp45_handle_are_zero(cuda):

@@ -1,6 +1,9 @@
 """Self-consistency of the oracle (CPU): analytic derivatives, the Hermitian form of
 the reference's multipliers, the FD Jacobian against finite differences of the FD RHS,
-the convergence orders of the DP45 and BDF restatements, and the CPU port."""
+the convergence orders of the DP45 and BDF restatements, the CPU port, and the BDF with
+the library's GMRES solver against the direct solve."""
+import tempfile
+
 import numpy as np
 import pytest
 
@@ -8,9 +11,10 @@ from oracle import bdf as obdf
 from oracle import cpu_port
 from oracle import dp45 as odp
 from oracle import fd as ofd
+from oracle import run as orun
 from oracle import spectral as osp
 from oracle.problem import Problem, cgle_terms, parse_term
-from tests.helpers import random_terms, rel_err
+from tests.helpers import five_field_stiff_problem, random_terms, rel_err
 
 
 def _grid(prob):
@@ -96,3 +100,26 @@ def test_cpu_port_equals_oracle_rhs():
         prob = Problem(2, Ns, tuple(10.0 + i for i in range(len(Ns))), cgle_terms(len(Ns)))
         y = rng.uniform(-1, 1, 2 * prob.N)
         assert rel_err(cpu_port.PortRHS(prob, 2)(0, y), osp.rhs(y, prob)) < 1e-14
+
+
+def test_gmres_solves_keep_the_direct_solve_decisions():
+    """The library replaces the reference's direct LU by restarted GMRES(40) to a 1e-12
+    relative residual.  On a stiff five-field system whose solves restart, the oracle BDF
+    with that GMRES (oracle.gmres) takes the same steps as with the direct solve, with
+    step sizes and states equal to 1e-8."""
+    prob, y0 = five_field_stiff_problem()
+    res = {}
+    for linear in ("lu", "gmres"):
+        with tempfile.TemporaryDirectory() as wd:
+            fb = wd + "/o"
+            y0.tofile(fb + "ic.dat")
+            cfg = orun.RunConfig(n=prob.n, Ns=prob.Ns, Ls=prob.Ls, terms=prob.terms, t1=1.0, dt=0.5, rtol=1e-4,
+                                 atol=1e-4, stiff=True, linear=linear)
+            summ = orun.run(fb, cfg)
+            res[linear] = (summ, np.fromfile(fb + "steps.dat"), np.fromfile(fb + "states.dat"))
+    (lu, lu_h, lu_y), (gm, gm_h, gm_y) = res["lu"], res["gmres"]
+    assert gm["steps"] == lu["steps"] and gm["attempts"] == lu["attempts"]
+    st = gm["linear"]
+    assert st["solves"] > 0 and st["cycles"] > st["solves"]
+    assert np.max(np.abs(gm_h - lu_h) / np.abs(lu_h)) < 1e-8
+    assert rel_err(gm_y, lu_y) < 1e-8
