@@ -12,6 +12,8 @@ in numpy/scipy, what the reference's CUDA C++ does on the hot path:
 * ``dp45``     -- the Dormand-Prince 4(5) stepper (reference ``dp45.cu``).
 * ``bdf``      -- the variable-order NDF/BDF stepper (reference ``bdf.cu``), with a
   scipy sparse LU in place of cuDSS.
+* ``gmres``    -- the restarted GMRES(40) that replaces cuDSS in the library, used to
+  check on the CPU that its solves keep the stepper's decisions.
 * ``run``      -- an emulation of the reference ``main``/``step_eval`` that writes the
   same output files (reference ``rdcu.cu:252-341,599-1273``).
 
