@@ -16,6 +16,12 @@ in numpy/scipy, what the reference's CUDA C++ does on the hot path:
   check on the CPU that its solves keep the stepper's decisions.
 * ``run``      -- an emulation of the reference ``main``/``step_eval`` that writes the
   same output files (reference ``rdcu.cu:252-341,599-1273``).
+* ``tangent``  -- the tangent-linear derivative of fixed-step DP45 on the oracle RHS,
+  used to check the library's discrete adjoint by duality.
+* ``lines``    -- defect-line extraction and frame correlation of 3D CGLE states
+  (reference ``makelines.py``).
+* ``cpu_port`` -- a faster host restatement of the pseudospectral RHS and DP45, timed
+  as the CPU baseline of ``bench.py``.
 
 Parity pinning: the oracle is checked against fixtures produced by the reference's
 own nvcc build (``oracle/build_ref.sh``) under ``tests/golden``; see the generating
