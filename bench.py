@@ -169,7 +169,7 @@ class ClockSampler:
 
 # ----------------------------------------------------------------------------- our arm
 # DRAM bytes (read + write) per launch of each pass of DP45 stage 4 on the 3D CGLE, from
-# one ncu capture (`ncu --set full ... python -m rdcu_b200.profile_case 256,256,128`,
+# one ncu capture (`ncu --set full ... python -m tests.profile_case 256,256,128`,
 # 8.39 M grid points); traffic grows with the grid points, so the full-size workload's
 # figure is this one scaled by its points.
 NCU_POINTS = 256 * 256 * 128

@@ -261,10 +261,13 @@ const char *rdcu_ensemble_last_error(rdcu_ensemble_t *e);
  * no handle and no allocation: no cudaMalloc, cudaFree or allocating library call.
  * Its working memory (FFT tables, dictionary tables, spectra) lives in one file-scope
  * __device__ array of RDCU_NOALLOC_SCRATCH_BYTES (64 MiB) that every GPU which loads
- * librdcu holds until the process exits.  Problems that need more scratch than that
- * (about n_fields * N * 16 bytes for the spectra plus a few KB of tables; a 2-field
- * grid of up to ~1M points fits) are rejected with RDCU_ERR_UNSUPPORTED.
- *   - y and f are device pointers of n*N doubles; spec->device selects the GPU.
+ * librdcu holds until the process exits.  A problem needs about
+ * (n_fields + n_channels) * N * 8 bytes of it for the half spectra, n_channels being the
+ * dictionary's inverse transforms (one per field for the CGLE, up to one per distinct
+ * derivative factor), plus a few KB of tables: the 2-field CGLE fits up to ~2M grid
+ * points.  Larger problems are rejected with RDCU_ERR_UNSUPPORTED.
+ *   - y and f are device pointers of n*N doubles; spec->device selects the GPU, which is
+ *     made current for the call; the caller's current device is restored on return.
  *   - The work is queued on `stream` (a cudaStream_t; NULL for the default stream) and
  *     the call returns after that stream has finished it.
  *   - The first call on a device looks up the array's device address

@@ -7,6 +7,7 @@
 # bench.py; librdcu never links or calls it.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+# RDCU_REFERENCE_DIR: the reference checkout (default: the read-only copy on the build machine)
 REF="${RDCU_REFERENCE_DIR:-/root/reference}"
 OUT="$HERE/_ref"
 NVCC="${NVCC:-/usr/local/cuda/bin/nvcc}"

@@ -86,7 +86,7 @@ class Gmres:
                 if met or total >= MAX_ITERS:
                     conv = met
                     break
-                V.append(w / hn)
+                V.append(w * (1.0 / hn))  # the library scales by the reciprocal (bdf.cu k_gm_update)
             y = np.zeros(jdone)
             for k in range(jdone - 1, -1, -1):
                 acc = g[k]

@@ -41,6 +41,19 @@ cudaError_t scratch_address(int dev, void** out) {
   return cudaSuccess;
 }
 
+// Makes `dev` current for the call and puts the caller's current device back on every
+// return path (callers embedded in another framework keep their device selection).
+struct DeviceGuard {
+  int prev = -1;
+  cudaError_t set(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    return cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
 bool on_device(const void* p) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
@@ -77,7 +90,8 @@ extern "C" int rdcu_rhs_noalloc(const rdcu_spec* spec, const double* y, double* 
       if (t.ints[j] < 0 || t.ints[j] >= nY * spec->n) return fail(RDCU_ERR_INVALID, "coupling term Y index out of range");
     terms.push_back(std::move(t));
   }
-  cudaError_t e = cudaSetDevice(spec->device);
+  DeviceGuard dg;
+  cudaError_t e = dg.set(spec->device);
   if (e != cudaSuccess) return fail(RDCU_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
   if (!on_device(y) || !on_device(f)) return fail(RDCU_ERR_INVALID, "y and f must be device pointers");
   void* base = nullptr;

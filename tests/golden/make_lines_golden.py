@@ -1,7 +1,7 @@
 """Golden vectors for the defect-line path, produced by the reference's own Python
 (makelines.py: findlines_np, correlate_np, and its __main__ driver and ancestry block).
 
-    python tests/golden/make_lines_golden.py --reference /root/reference --out tests/golden
+    python tests/golden/make_lines_golden.py --reference "$RDCU_REFERENCE_DIR" --out tests/golden
 
 Needs the reference sources (and networkx, as the reference does); runs on the CPU.
 Writes lines_<case>.npz (the phase field and the per-component edges), lines_frames.npz
@@ -44,7 +44,7 @@ def _pack(lines):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", required=True)
+    ap.add_argument("--reference", default=os.environ.get("RDCU_REFERENCE_DIR"), required="RDCU_REFERENCE_DIR" not in os.environ)
     ap.add_argument("--out", required=True)
     a = ap.parse_args()
     sys.path.insert(0, a.reference)

@@ -2,15 +2,18 @@
 RHS stage (rdcu_profile_passes); prints one JSON line.  Intended as a small, fixed
 workload for profilers such as Nsight Compute:
 
-    python -m rdcu_b200.profile_case 256,256,128 [--attempts 3] [--reps 2]
+    python -m tests.profile_case 256,256,128 [--attempts 3] [--reps 2]
 """
 import argparse
 import json
+import os
+import sys
 
 import numpy as np
 
-from . import Solver, random_ic
-from .problems import cgle_coupling_lines
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+from rdcu_b200 import Solver, random_ic  # noqa: E402
+from rdcu_b200.problems import cgle_coupling_lines  # noqa: E402
 
 
 def cgle_terms(ndim, b=2.0, c=0.8):

@@ -1,0 +1,102 @@
+"""GPU: this library's rdcu CLI against the reference's own build, side by side on the same
+GPU, at the benchmark problem sizes.
+
+The reference binary (oracle/_ref/rdcu_ref, the unmodified reference sources built for
+sm_100a by oracle/build_ref.sh) and rdcu_b200/bin/rdcu run the same argv and coupling
+file in separate directories; the outputs are compared file by file:
+
+* the RHS at t = 0 (-t 0 -D2, f.dat) within 1e-12 relative in max-norm (rdcu.cu:167-184);
+* short adaptive DP45 runs (dp45.cu:87-169): the same accepted-step count, steps.dat (the
+  step size after every attempt) and the dense-output states within 1e-8.
+
+Sizes: the 2D CGLE 128^2 problem (L = 100, 18 terms, seed 1, rtol = atol = 1e-8), the 3D
+CGLE 128^3 and 256^3 problems (L = 200, 22 terms, seed 2).  The reference binary must
+be present: on a GPU machine its absence is a failure, not a skip.
+"""
+import os
+import shlex
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle.problem import cgle_coupling_lines
+from tests.helpers import rel_err
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLI = os.path.join(ROOT, "rdcu_b200", "bin", "rdcu")
+REF = os.path.join(ROOT, "oracle", "_ref", "rdcu_ref")
+
+C1 = "-n 2 -N 128,128 -L 100,100 -A 2 -s 1 -r 1e-8 -a 1e-8"
+C3D128 = "-n 2 -N 128,128,128 -L 200,200,200 -A 2 -s 2 -r 1e-8 -a 1e-8"
+C3D256 = "-n 2 -N 256,256,256 -L 200,200,200 -A 2 -s 2 -r 1e-8 -a 1e-8"
+
+
+def run(binary, args, coupling, wd, name="c"):
+    """Runs one rdcu command in wd; returns (filebase, .out text)."""
+    assert os.path.exists(binary), "missing %s (build it with oracle/build_ref.sh / rdcu_b200.build)" % binary
+    os.makedirs(wd, exist_ok=True)
+    fb = os.path.join(wd, name)
+    if not os.path.exists(fb + "coupling.dat"):
+        with open(fb + "coupling.dat", "w") as fh:
+            fh.write("\n".join(coupling) + "\n")
+    r = subprocess.run([binary] + shlex.split(args) + [fb], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, (binary, args, r.stdout[-2000:], r.stderr[-2000:])
+    return fb, open(fb + ".out").read()
+
+
+def steps_of(out_text):
+    for line in out_text.splitlines():
+        if line.startswith("steps:"):
+            return int(line.split()[1])
+    raise AssertionError("no steps: line in\n" + out_text[-1000:])
+
+
+def both(tmp_path, args, coupling):
+    ours = run(CLI, args, coupling, str(tmp_path / "ours"))
+    ref = run(REF, args, coupling, str(tmp_path / "ref"))
+    return ours, ref
+
+
+def check_rhs(tmp_path, base, ndim):
+    (fo, _), (fr, _) = both(tmp_path, base + " -t 0 -D2", cgle_coupling_lines(ndim))
+    np.testing.assert_array_equal(np.fromfile(fo + "states.dat"), np.fromfile(fr + "states.dat"))
+    f, g = np.fromfile(fo + "f.dat"), np.fromfile(fr + "f.dat")
+    assert f.size == g.size
+    assert rel_err(f, g) < 1e-12, rel_err(f, g)
+
+
+def check_adaptive(tmp_path, args, ndim, stride=1):
+    (fo, oo), (fr, orf) = both(tmp_path, args, cgle_coupling_lines(ndim))
+    assert steps_of(oo) == steps_of(orf)
+    s, sr = np.fromfile(fo + "steps.dat"), np.fromfile(fr + "steps.dat")
+    assert s.size == sr.size
+    assert np.max(np.abs(s - sr) / np.abs(sr)) < 1e-8
+    np.testing.assert_array_equal(np.fromfile(fo + "times.dat"), np.fromfile(fr + "times.dat"))
+    y = np.memmap(fo + "states.dat", np.float64, "r")
+    yr = np.memmap(fr + "states.dat", np.float64, "r")
+    assert y.size == yr.size
+    assert rel_err(np.asarray(y[::stride]), np.asarray(yr[::stride])) < 1e-8
+
+
+def test_rhs_cgle2d_128(tmp_path):
+    check_rhs(tmp_path, C1, 2)
+
+
+def test_adaptive_cgle2d_128(tmp_path):
+    check_adaptive(tmp_path, C1 + " -t 1 -d 0.25 -D1", 2)
+
+
+def test_rhs_cgle3d_128(tmp_path):
+    check_rhs(tmp_path, C3D128, 3)
+
+
+def test_adaptive_cgle3d_128(tmp_path):
+    check_adaptive(tmp_path, C3D128 + " -t 0.25 -d 0.25 -D1", 3)
+
+
+def test_adaptive_cgle3d_256(tmp_path):
+    # two outputs of 268 MB per build: compared on every 97th value
+    check_adaptive(tmp_path, C3D256 + " -t 0.25 -d 0.25 -D1", 3, stride=97)
