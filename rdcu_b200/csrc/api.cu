@@ -280,6 +280,8 @@ int rdcu_rhs(rdcu_t* h, double t, const double* y, double* f, double* Y) {
   if (f_host) CHECK_CUDA(h, cudaMemcpyAsync(f, fd, sb, cudaMemcpyDeviceToHost, h->stream), "rdcu_rhs");
   if (Y_host) CHECK_CUDA(h, cudaMemcpyAsync(Y, Yd, Yb, cudaMemcpyDeviceToHost, h->stream), "rdcu_rhs");
   CHECK_CUDA(h, cudaStreamSynchronize(h->stream), "rdcu_rhs");
+  if (h->sp && h->sp->take_pipe_error())
+    return set_err(h, RDCU_ERR_CUDA, "rdcu_rhs: a tile pass gave up waiting for its copies");
   return RDCU_OK;
 }
 

@@ -186,6 +186,7 @@ cudaError_t DP45Engine::sync_ctl() {
   RDCU_TRY(cudaMemcpyAsync(h_ctl_pinned_, d_ctl_, sizeof(DP45Ctl), cudaMemcpyDeviceToHost, st_));
   RDCU_TRY(cudaStreamSynchronize(st_));
   host_ctl = *h_ctl_pinned_;
+  if (host_ctl.pipe_err) return cudaErrorLaunchTimeout;  // a tile pass gave up waiting
   return cudaSuccess;
 }
 
@@ -278,7 +279,16 @@ cudaError_t DP45Engine::launch_attempt_capture(double* const* ytemp_out) {
 }
 
 cudaError_t DP45Engine::ensure_graph() {
+  if (graph_exec_ && sp_ && graph_gen_ != sp_->buffers_gen) {
+    // the plan replaced a spectral buffer (Y output grows the channel spectra): the
+    // captured kernels hold the old address
+    cudaGraphExecDestroy(graph_exec_);
+    cudaGraphDestroy(graph_);
+    graph_exec_ = nullptr;
+    graph_ = nullptr;
+  }
   if (graph_exec_ || !use_graph) return cudaSuccess;
+  graph_gen_ = sp_ ? sp_->buffers_gen : 0;
   cudaStream_t cap = st_;
   RDCU_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
   cudaError_t e = launch_attempt();

@@ -94,6 +94,7 @@ class DP45Engine {
   double atol_ = 0, rtol_ = 0;
   cudaGraphExec_t graph_exec_ = nullptr;
   cudaGraph_t graph_ = nullptr;
+  int graph_gen_ = -1;  // the plan's buffers_gen when the attempt graph was captured
   cudaError_t ensure_graph();
 };
 

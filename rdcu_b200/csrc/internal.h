@@ -187,7 +187,7 @@ struct DP45Ctl {
   int max_attempts;     // per launch sequence
   int attempts_this_launch;
   int nparts;           // error partial sums written by the stage-7 epilogue
-  int pad;
+  int pipe_err;         // nonzero: a pass on TMA tiles gave up waiting for its copies
 };
 
 struct DP45Bufs {

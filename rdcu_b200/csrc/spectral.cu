@@ -29,12 +29,14 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <cudaTypedefs.h>
 #include <cstdlib>
 #include <cstring>
 #include <map>
 #include <type_traits>
 
 #include "fft_line.cuh"
+#include "pencil.cuh"
 #include "spectral.h"
 
 namespace rdcu {
@@ -685,6 +687,271 @@ __global__ void __launch_bounds__(LX > 0 ? kSpecBlock : kMaxBlock, LX > 0 ? 3 : 
   mid_body<RS, LX>(a, blockIdx.x);
 }
 
+// ---- axis-0 pass of 3D grids on TMA tiles (pencil.cuh): 128- or 256-point lines, at
+// most two fields, channels written over their sources (the operator-grouped form of
+// k_mid's multipliers, groups built at plan time).  Persistent CTAs of kPipeThreads:
+// warp w transforms column (w & 7) of the tile (two half-warp columns for 128-point
+// lines) for source / channel w >> 3.  Per tile: TMA loads of every source's boxes, the
+// forward FFTs, the multipliers (each warp forms its channel at its points from all
+// sources), the inverse FFTs in place, TMA stores of the channels.
+struct MidPipeArgs {
+  int I, nsrc, G, ntiles, ngrp, Mh;
+  const double2* tw;      // axis-0 twiddle table (global)
+  const ChanEntry* grp;   // one entry per operator group (its operator)
+  const double* A;        // [ngrp][16]: A[g][channel * 4 + source]
+  const double* kv;       // wavenumbers of every axis (ChanTable layout)
+  int kv_off[3];
+  int Ns[3];
+  int kv_total;
+  RhsIO io;
+  int* err;
+};
+
+constexpr int kPipeThreads = 512;
+constexpr int kPipeSrcBytes = 32768;  // one source's tile: 8 columns x 256 rows or 16 x 128
+
+__host__ __device__ constexpr size_t mid_pipe_smem(int ngrp, int kv_total) {
+  return 1024 + 4 * (size_t)kPipeSrcBytes + 16 + (size_t)ngrp * sizeof(ChanEntry) + (size_t)ngrp * 16 * 8 +
+         (size_t)kv_total * 8;
+}
+
+template <int L>
+__global__ void __launch_bounds__(kPipeThreads, 1)
+    k_mid_pipe(const __grid_constant__ CUtensorMap tmF, const __grid_constant__ CUtensorMap tmC, MidPipeArgs a) {
+  extern __shared__ char smraw[];
+  if (a.io.mode == 1 && !a.io.ctl->running) return;
+  constexpr int NB = 256 / L;  // boxes per source tile
+  constexpr int LPL = L / 8;
+  constexpr int BOXB = L * 128;
+  char* sm = smraw + ((1024 - (smem_u32(smraw) & 1023)) & 1023);
+  char* buf[2] = {sm, sm + 2 * kPipeSrcBytes};
+  uint64_t* full = reinterpret_cast<uint64_t*>(sm + 4 * kPipeSrcBytes);
+  ChanEntry* sgrp = reinterpret_cast<ChanEntry*>(full + 2);
+  double* sA = reinterpret_cast<double*>(sgrp + a.ngrp);
+  double* skv = sA + 16 * a.ngrp;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int t = tid; t < a.ngrp; t += kPipeThreads) sgrp[t] = a.grp[t];
+  for (int t = tid; t < 16 * a.ngrp; t += kPipeThreads) sA[t] = a.A[t];
+  for (int t = tid; t < a.kv_total; t += kPipeThreads) skv[t] = a.kv[t];
+  if (tid == 0) {
+    mbar_init(&full[0], 1);
+    mbar_init(&full[1], 1);
+    mbar_fence_init();
+    tma_prefetch(&tmF);
+    tma_prefetch(&tmC);
+  }
+  __syncthreads();
+  const int h = warp >> 3;                              // source (forward) / channel (inverse)
+  const int cc = (warp & 7) * (32 / LPL) + lane / LPL;  // column of the tile
+  const int coff = (cc >> 3) * BOXB;                    // offset of the column's box in a source tile
+  const int c = cc & 7;
+  WarpLine<L> wl;
+  wl.init(a.tw, lane % LPL);
+  auto issue = [&](int tile, int b) {
+    mbar_expect_tx(&full[b], (unsigned)(a.nsrc * kPipeSrcBytes));
+    const int P0 = tile * 8 * NB;
+    for (int s = 0; s < a.nsrc; ++s)
+      for (int bx = 0; bx < NB; ++bx)
+        tma_load_2d(buf[b] + s * kPipeSrcBytes + bx * BOXB, &tmF, 2 * (P0 + 8 * bx), s * L, &full[b]);
+  };
+  if (tid == 0) {
+    if ((int)blockIdx.x < a.ntiles) issue(blockIdx.x, 0);
+    if ((int)(blockIdx.x + gridDim.x) < a.ntiles) issue(blockIdx.x + gridDim.x, 1);
+  }
+  int it = 0;
+  for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, ++it) {
+    const int b = it & 1;
+    const bool ok = mbar_wait(&full[b], (unsigned)((it >> 1) & 1));
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        atomicExch(a.io.mode == 1 ? &a.io.ctl->pipe_err : a.err, kPipeErrTimeout);
+        mbar_wait(&full[b ^ 1], (unsigned)(((it + 1) >> 1) & 1));  // bounded: the other buffer's loads
+        bulk_wait_all();
+      }
+      return;
+    }
+    char* tb = buf[b];
+    const long long P = (long long)tile * 8 * NB + cc;
+    double2 v[8];
+    if (h < a.nsrc) {
+      char* bx = tb + h * kPipeSrcBytes + coff;
+      wl.load(v, bx, c);
+      wl.template transform<false>(v, bx, c);
+      wl.store(v, bx, c);
+    }
+    __syncthreads();
+    if (h < a.G) {
+      // channel h at this lane's points z = ml + LPL p of column P (k_mid's arithmetic)
+      const bool inP = P < a.I;
+      const int k1 = inP ? (int)(P / a.Mh) : 0, kx = inP ? (int)(P - (long long)k1 * a.Mh) : 0;
+      const int m1 = k1 == 0 ? 0 : a.Ns[1] - k1, m2 = kx == 0 ? 0 : a.Ns[2] - kx;
+      const double kp1 = skv[a.kv_off[1] + k1], km1 = skv[a.kv_off[1] + m1];
+      const double kp2 = skv[a.kv_off[2] + kx], km2 = skv[a.kv_off[2] + m2];
+#pragma unroll
+      for (int p = 0; p < 8; ++p) {
+        const int z = wl.ml + LPL * p;
+        double2 acc = make_double2(0.0, 0.0);
+        if (inP) {
+          const int m0 = z == 0 ? 0 : a.Ns[0] - z;
+          const double kp[3] = {skv[a.kv_off[0] + z], kp1, kp2};
+          const double km[3] = {skv[a.kv_off[0] + m0], km1, km2};
+          double2 u[2];
+          u[0] = *swz_col(tb + coff, c, z);
+          u[1] = a.nsrc > 1 ? *swz_col(tb + kPipeSrcBytes + coff, c, z) : make_double2(0.0, 0.0);
+          for (int g = 0; g < a.ngrp; ++g) {
+            const ChanEntry en = sgrp[g];
+            double ap = 1.0, am = 1.0;
+            if (en.nax >= 1) {
+              ap *= sel3(kp[0], kp[1], kp[2], en.ax0);
+              am *= sel3(km[0], km[1], km[2], en.ax0);
+            }
+            if (en.nax >= 2) {
+              ap *= sel3(kp[0], kp[1], kp[2], en.ax1);
+              am *= sel3(km[0], km[1], km[2], en.ax1);
+            }
+            const double sgn = (en.nax & 1) ? -1.0 : 1.0;
+            int q;
+            double beta;
+            if (en.part == 0) {
+              q = en.nax;
+              beta = 0.5 * (ap + sgn * am);
+            } else {
+              q = en.nax + 3;
+              beta = 0.5 * (ap - sgn * am);
+            }
+            const double* Ag = sA + g * 16 + h * 4;
+            double2 sum = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int s4 = 0; s4 < 2; ++s4) {
+              if (s4 >= a.nsrc) break;
+              const double w = Ag[s4];
+              sum.x += w * u[s4].x;
+              sum.y += w * u[s4].y;
+            }
+            double2 vv = make_double2(beta * sum.x, beta * sum.y);
+            switch (q & 3) {
+              case 1: vv = make_double2(-vv.y, vv.x); break;
+              case 2: vv = make_double2(-vv.x, -vv.y); break;
+              case 3: vv = make_double2(vv.y, -vv.x); break;
+              default: break;
+            }
+            acc.x += vv.x;
+            acc.y += vv.y;
+          }
+        }
+        v[p] = acc;
+      }
+    }
+    __syncthreads();  // every source read before the channels overwrite them
+    if (h < a.G) {
+      char* bx = tb + h * kPipeSrcBytes + coff;
+      wl.template transform<true>(v, bx, c);
+      wl.store(v, bx, c);
+    }
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      const int P0 = tile * 8 * NB;
+      for (int ch = 0; ch < a.G; ++ch)
+        for (int bx = 0; bx < NB; ++bx) tma_store_2d(&tmC, 2 * (P0 + 8 * bx), ch * L, tb + ch * kPipeSrcBytes + bx * BOXB);
+      bulk_commit();
+      const int nt = tile + 2 * (int)gridDim.x;
+      if (nt < a.ntiles) {
+        bulk_wait_read_all();  // the stores have read this buffer
+        issue(nt, b);
+      }
+    }
+  }
+  if (tid == 0) bulk_wait_all();
+}
+
+// ---- middle-axis pass of 3D grids on TMA tiles: FFT (forward or inverse) of every
+// line along axis 1, in place.  A box is 8 consecutive x-wavenumber columns by the whole
+// axis-1 line of one plane (field or channel, axis-0 index); a tile is c2c_boxes(L)
+// consecutive boxes, one line per warp (256 points) or half warp (128 points).
+struct C2CPipeArgs {
+  int nbox, nchunk, ntiles;
+  const double2* tw;
+  RhsIO io;
+  int* err;
+};
+
+__host__ __device__ constexpr int c2c_boxes(int L) { return 2 * (256 / L); }
+constexpr size_t kC2cPipeSmem = 1024 + 4 * (size_t)kPipeSrcBytes + 16;
+
+template <int L, bool INV>
+__global__ void __launch_bounds__(kPipeThreads, 1)
+    k_c2c_pipe(const __grid_constant__ CUtensorMap tm, C2CPipeArgs a) {
+  extern __shared__ char smraw[];
+  if (a.io.mode == 1 && !a.io.ctl->running) return;
+  constexpr int BPT = c2c_boxes(L);
+  constexpr int LPL = L / 8;
+  constexpr int BOXB = L * 128;
+  char* sm = smraw + ((1024 - (smem_u32(smraw) & 1023)) & 1023);
+  char* buf[2] = {sm, sm + 2 * kPipeSrcBytes};
+  uint64_t* full = reinterpret_cast<uint64_t*>(sm + 4 * kPipeSrcBytes);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (tid == 0) {
+    mbar_init(&full[0], 1);
+    mbar_init(&full[1], 1);
+    mbar_fence_init();
+    tma_prefetch(&tm);
+  }
+  __syncthreads();
+  const int li = warp * (32 / LPL) + lane / LPL;  // line of the tile
+  const int coff = (li >> 3) * BOXB, c = li & 7;
+  WarpLine<L> wl;
+  wl.init(a.tw, lane % LPL);
+  auto issue = [&](int tile, int b) {
+    const int b0 = tile * BPT, nb = min(BPT, a.nbox - b0);
+    mbar_expect_tx(&full[b], (unsigned)(nb * BOXB));
+    for (int k = 0; k < nb; ++k) {
+      const int plane = (b0 + k) / a.nchunk, chunk = (b0 + k) - plane * a.nchunk;
+      tma_load_3d(buf[b] + k * BOXB, &tm, 16 * chunk, 0, plane, &full[b]);
+    }
+  };
+  if (tid == 0) {
+    if ((int)blockIdx.x < a.ntiles) issue(blockIdx.x, 0);
+    if ((int)(blockIdx.x + gridDim.x) < a.ntiles) issue(blockIdx.x + gridDim.x, 1);
+  }
+  int it = 0;
+  for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, ++it) {
+    const int b = it & 1;
+    const bool ok = mbar_wait(&full[b], (unsigned)((it >> 1) & 1));
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        atomicExch(a.io.mode == 1 ? &a.io.ctl->pipe_err : a.err, kPipeErrTimeout);
+        mbar_wait(&full[b ^ 1], (unsigned)(((it + 1) >> 1) & 1));
+        bulk_wait_all();
+      }
+      return;
+    }
+    char* bx = buf[b] + coff;
+    if (tile * BPT + (li >> 3) < a.nbox) {
+      double2 v[8];
+      wl.load(v, bx, c);
+      wl.template transform<INV>(v, bx, c);
+      wl.store(v, bx, c);
+    }
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      const int b0 = tile * BPT, nb = min(BPT, a.nbox - b0);
+      for (int k = 0; k < nb; ++k) {
+        const int plane = (b0 + k) / a.nchunk, chunk = (b0 + k) - plane * a.nchunk;
+        tma_store_3d(&tm, 16 * chunk, 0, plane, buf[b] + k * BOXB);
+      }
+      bulk_commit();
+      const int nt = tile + 2 * (int)gridDim.x;
+      if (nt < a.ntiles) {
+        bulk_wait_read_all();
+        issue(nt, b);
+      }
+    }
+  }
+  if (tid == 0) bulk_wait_all();
+}
+
 struct Mult1DArgs {
   int Mh, nch, ch0;
   const double2* Sf;
@@ -1145,6 +1412,123 @@ __global__ void __launch_bounds__(LX > 0 ? kSpecBlock : kMaxBlock, LX > 0 ? 3 : 
   inv_x_body<RS, LX>(a, blockIdx.x);
 }
 
+// ---- x pass of 3D grids with 128- or 256-point rows and a dense-polynomial dictionary
+// of at most two inverse channels: one row per warp (two per warp for 128 points).  The
+// channels' half spectra go from global memory straight into registers (k_inv_x's
+// Hermitian extension and two-channel packing), the inverse transform runs in registers
+// with its exchanges in a per-warp line buffer (WarpLine), then the dictionary and the
+// stage-7 error terms are formed for the lane's points.  Same arithmetic as k_inv_x, per
+// point and per row partial (x = lane, lane + 32, ... then the butterfly over the lanes);
+// no block barriers after the table staging.
+struct InvRowArgs {
+  int R, n, nch, Mh;
+  const double2* tw;
+  const double2* Sc;
+  DictTable dict;
+  RhsIO io;
+};
+constexpr int kRowThreads = 256;
+
+__host__ __device__ constexpr size_t inv_row_smem(int n, int count) {
+  return (size_t)(kRowThreads / 32) * 256 * 16 + (size_t)n * count * 8 + 64;
+}
+
+template <int L, int NF>
+__global__ void __launch_bounds__(kRowThreads, 2) k_inv_row(InvRowArgs a) {
+  extern __shared__ double2 sm[];
+  if (a.io.mode == 1 && !a.io.ctl->running) return;
+  using MN = Mono<NF>;
+  constexpr int LPL = L / 8, RPW = 32 / LPL;  // lanes per row, rows per warp
+  const Resolved r = resolve(a.io);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  double* spoly = reinterpret_cast<double*>(sm + (kRowThreads / 32) * 256);
+  int* sfold = reinterpret_cast<int*>(spoly + NF * MN::count);
+  for (int t = tid; t < NF * MN::count; t += kRowThreads) spoly[t] = a.dict.poly[t];
+  for (int t = tid; t < NF; t += kRowThreads) sfold[t] = a.dict.fold[t];
+  __syncthreads();
+  const int sub = lane / LPL, ml = lane % LPL;
+  double2* line = sm + warp * 256 + sub * L;
+  WarpLine<L> wl;
+  wl.init(a.tw, ml);
+  const bool err = (a.io.mode == 1 && r.stage == 7 && a.io.err_part != nullptr);
+  const long long RL = (long long)a.R * L;
+  const long long wstride = (long long)gridDim.x * (kRowThreads / 32) * RPW;
+  for (long long row0 = ((long long)blockIdx.x * (kRowThreads / 32) + warp) * RPW; row0 < a.R; row0 += wstride) {
+    const long long row = row0 + sub;
+    const bool live = row < a.R;
+    double2 v[8];
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+      const int kx = ml + LPL * p;
+      const int kk = kx >= a.Mh ? L - kx : kx;
+      double2 Av = make_double2(0.0, 0.0), Bv = make_double2(0.0, 0.0);
+      if (live) {
+        Av = a.Sc[row * a.Mh + kk];
+        if (a.nch > 1) Bv = a.Sc[((long long)a.R + row) * a.Mh + kk];
+      }
+      if (kx == 0 || 2 * kx == L) {
+        Av.y = 0.0;
+        Bv.y = 0.0;
+      }
+      if (kx >= a.Mh) {
+        Av.y = -Av.y;
+        Bv.y = -Bv.y;
+      }
+      v[p] = make_double2(Av.x - Bv.y, Av.y + Bv.x);
+    }
+    wl.template transform<true>(v, [line](int e) { return line + e; });
+    // the lane's values back to its own line positions (the transform's last barrier has
+    // passed; nothing else reads them), so the point loop holds no spectral registers
+#pragma unroll
+    for (int p = 0; p < 8; ++p) line[ml + LPL * p] = v[p];
+    double es_even = 0.0, es_odd = 0.0;  // 128 points: the partials of lanes ml and ml + 16
+#pragma unroll 1
+    for (int p = 0; p < 8; ++p) {
+      const double2 z = line[ml + LPL * p];
+      const long long gx = row * L + ml + LPL * p;
+      double u[NF];
+#pragma unroll
+      for (int f = 0; f < NF; ++f) u[f] = live ? r.u[f * RL + gx] : 0.0;
+      double mono[MN::count];
+      mono[0] = 1.0;
+#pragma unroll
+      for (int m = 1; m < MN::count; ++m) mono[m] = mono[MN::parent(m)] * u[MN::var(m)];
+      double err2 = 0.0;
+#pragma unroll
+      for (int i = 0; i < NF; ++i) {
+        const int fc = sfold[i];
+        double acc = fc >= 0 ? ((fc & 1) ? z.y : z.x) : 0.0;
+        const double* ci = spoly + i * MN::count;
+#pragma unroll
+        for (int m = 0; m < MN::count; ++m) acc += ci[m] * mono[m];
+        if (live) {
+          const long long gi = i * RL + gx;
+          r.f[gi] = acc;
+          if (err) {
+            const double yold = r.y[gi];
+            const double es = c_e[0] * r.k[0][gi] + c_e[2] * r.k[2][gi] + c_e[3] * r.k[3][gi] +
+                              c_e[4] * r.k[4][gi] + c_e[5] * r.k[5][gi] + c_e[6] * acc;
+            const double ev = r.h * es / (r.atol + r.rtol * fmax(fabs(yold), fabs(u[i])));
+            err2 += ev * ev;
+          }
+        }
+      }
+      if (L == 256 || (p & 1) == 0)
+        es_even += err2;
+      else
+        es_odd += err2;
+    }
+    __syncwarp();  // the next row's transform rewrites the line
+    if (err) {
+      double sacc = es_even;
+      if (L == 128) sacc = es_even + es_odd;  // k_inv_x's first butterfly step (lane ^ 16)
+#pragma unroll
+      for (int o = LPL / 2; o > 0; o >>= 1) sacc += __shfl_xor_sync(0xffffffffu, sacc, o);
+      if (ml == 0 && live) a.io.err_part[row] = sacc;
+    }
+  }
+}
+
 // ---- batched passes: persistent CTAs over (problem, tile) work items
 template <typename A>
 __device__ __forceinline__ void load_args(A* dst, const A* src) {
@@ -1433,6 +1817,68 @@ static std::vector<ChanEntry> sorted_entries(const std::vector<ChanEntry>& ent, 
     return kx < ky;
   });
   return srt;
+}
+
+// Operator groups of the operator-sorted hot entries, as k_mid forms them in each CTA:
+// one group per distinct operator (its first entry), and A[g][channel * 4 + source] the
+// sum of the group's coefficients in entry order.
+static void operator_groups(const std::vector<ChanEntry>& srt, std::vector<ChanEntry>* grp, std::vector<double>* A) {
+  grp->clear();
+  A->clear();
+  int last = -1;
+  for (const ChanEntry& en : srt) {
+    const int key = en.nax | (en.ax0 << 2) | (en.ax1 << 4) | (en.part << 6);
+    if (key != last) {
+      last = key;
+      grp->push_back(en);
+      A->resize(A->size() + 16, 0.0);
+    }
+    (*A)[(grp->size() - 1) * 16 + en.pad * 4 + en.src] += en.coef;
+  }
+}
+
+// cuTensorMapEncodeTiled from the driver (no link-time dependency on libcuda).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = []() -> PFN_cuTensorMapEncodeTiled_v12000 {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+// A 2D view of `rows` rows of `row_doubles` doubles (rows contiguous), moved in boxes of
+// 16 doubles (8 complex values, 128 bytes) by box_rows rows with the 128-byte swizzle.
+static bool encode_rows(CUtensorMap* m, void* base, long long row_doubles, long long rows, int box_rows) {
+  const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc || !base) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)row_doubles, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)row_doubles * 8};
+  const cuuint32_t box[2] = {16, (cuuint32_t)box_rows};
+  const cuuint32_t es[2] = {1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+
+// A 3D view of `planes` planes of `rows` rows of `row_c` complex values (the half spectra
+// [plane][axis 1][x]), moved in boxes of 8 complex values by `rows` rows of one plane
+// with the 128-byte swizzle.
+static bool encode_planes(CUtensorMap* m, void* base, long long row_c, long long rows, long long planes) {
+  const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc || !base || rows > 256) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)(2 * row_c), (cuuint64_t)rows, (cuuint64_t)planes};
+  const cuuint64_t strides[2] = {(cuuint64_t)(2 * row_c * 8), (cuuint64_t)(2 * row_c * 8 * rows)};
+  const cuuint32_t box[3] = {16, (cuuint32_t)rows, 1};
+  const cuuint32_t es[3] = {1, 1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
 }
 
 // Device memory of the plan: cudaMalloc, or the next 256-byte-aligned piece of the arena.
@@ -1817,8 +2263,172 @@ bool SpectralPlan::init(int n_, int ndim_, const int* Ns_, const double* Ls_,
     *msg = "grid too large for the shared-memory x pass";
     return false;
   }
+  setup_pipes();
   built_ = true;
   return true;
+}
+
+// Which 3D passes run as the specialised kernels: k_inv_row for 128- or 256-point rows
+// with a dense-polynomial dictionary of at most two channels; k_mid_pipe for 128- or
+// 256-point axis-0 lines with at most two fields and no more channels than fields
+// (written over their sources); k_c2c_pipe with it for 128- or 256-point axis-1 lines.
+// Every other plan keeps the general kernels.
+void SpectralPlan::setup_pipes() {
+  pipe_mid_ = pipe_c2c_ = inv_row_ = false;
+  if (ndim != 3) return;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  sms_ = std::max(1, sms);
+  if ((M == 128 || M == 256) && poly_nf_ == n && n >= 1 && n <= 3 && nch >= 1 && nch <= 2) {
+    const size_t smem = inv_row_smem(n, poly_count_);
+    bool ok = true;
+    auto attr = [&](const void* fn) {
+      ok &= cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess;
+    };
+    if (M == 128) {
+      attr((const void*)k_inv_row<128, 1>);
+      attr((const void*)k_inv_row<128, 2>);
+      attr((const void*)k_inv_row<128, 3>);
+    } else {
+      attr((const void*)k_inv_row<256, 1>);
+      attr((const void*)k_inv_row<256, 2>);
+      attr((const void*)k_inv_row<256, 3>);
+    }
+    cudaGetLastError();
+    inv_row_ = ok;
+  }
+  if (!(Ns[0] == 128 || Ns[0] == 256) || !ch_sorted_ || nch < 1 || nch > n || n > 2) return;
+  const long long I = (long long)Ns[1] * Mh;
+  if (2 * I > 0x7fffffffLL) return;
+  std::vector<ChanEntry> grp;
+  std::vector<double> A;
+  operator_groups(sorted_entries(h_ch_ent_, h_ch_off_, nch), &grp, &A);
+  const size_t smem = mid_pipe_smem((int)grp.size(), kv_total_);
+  if (smem > 227 * 1024) return;
+  if (!encode_rows(&tm_sf_, Sf_, 2 * I, (long long)n * Ns[0], Ns[0]) || !encode_sc_map()) return;
+  const void* fn = Ns[0] == 128 ? (const void*)k_mid_pipe<128> : (const void*)k_mid_pipe<256>;
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  if (upload_vec(&mid_grp_, grp) != cudaSuccess || upload_vec(&mid_A_, A) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  if (!pipe_err_ && (dev_alloc(&pipe_err_, sizeof(int)) != cudaSuccess ||
+                     cudaMemsetAsync(pipe_err_, 0, sizeof(int), arena_ ? arena_->stream : 0) != cudaSuccess)) {
+    cudaGetLastError();
+    pipe_err_ = nullptr;
+    return;
+  }
+  const int cols = 8 * (256 / Ns[0]);  // columns per tile
+  const int ntiles = (int)((I + cols - 1) / cols);
+  pipe_grid_ = std::max(1, std::min(ntiles, sms_));
+  mid_ngrp_ = (int)grp.size();
+  pipe_mid_ = true;
+  if (Ns[1] == 128 || Ns[1] == 256) {
+    const void* ff = Ns[1] == 128 ? (const void*)k_c2c_pipe<128, false> : (const void*)k_c2c_pipe<256, false>;
+    const void* fi = Ns[1] == 128 ? (const void*)k_c2c_pipe<128, true> : (const void*)k_c2c_pipe<256, true>;
+    if (encode_planes(&tm_sf_c2c_, Sf_, Mh, Ns[1], (long long)n * Ns[0]) &&
+        cudaFuncSetAttribute(ff, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kC2cPipeSmem) == cudaSuccess &&
+        cudaFuncSetAttribute(fi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kC2cPipeSmem) == cudaSuccess)
+      pipe_c2c_ = true;
+    cudaGetLastError();
+  }
+}
+
+bool SpectralPlan::encode_sc_map() {
+  const long long I = (long long)Ns[1] * Mh;
+  return encode_rows(&tm_sc_, Sc_, 2 * I, (long long)sc_rows_ * Ns[0], Ns[0]) &&
+         (Ns[1] > 256 || encode_planes(&tm_sc_c2c_, Sc_, Mh, Ns[1], (long long)sc_rows_ * Ns[0]));
+}
+
+int SpectralPlan::take_pipe_error() {
+  if (!pipe_err_) return 0;
+  int e = 0;
+  if (cudaMemcpy(&e, pipe_err_, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+  if (e) cudaMemset(pipe_err_, 0, sizeof(int));
+  return e;
+}
+
+cudaError_t SpectralPlan::launch_inv_row(const RhsIO& io, cudaStream_t st) {
+  InvRowArgs a{};
+  a.R = R;
+  a.n = n;
+  a.nch = nch;
+  a.Mh = Mh;
+  a.tw = tw_x_;
+  a.Sc = Sc_;
+  a.dict = dict_table();
+  a.io = io;
+  const size_t smem = inv_row_smem(n, poly_count_);
+  const int rows_per_cta = (kRowThreads / 32) * (32 / (M / 8));
+  const int grid = std::max(1, std::min((R + rows_per_cta - 1) / rows_per_cta, 4 * sms_));
+  auto go = [&](auto lx) {
+    constexpr int LX = decltype(lx)::value;
+    switch (n) {
+      case 1: k_inv_row<LX, 1><<<grid, kRowThreads, smem, st>>>(a); break;
+      case 2: k_inv_row<LX, 2><<<grid, kRowThreads, smem, st>>>(a); break;
+      default: k_inv_row<LX, 3><<<grid, kRowThreads, smem, st>>>(a); break;
+    }
+  };
+  if (M == 128)
+    go(std::integral_constant<int, 128>{});
+  else
+    go(std::integral_constant<int, 256>{});
+  return cudaGetLastError();
+}
+
+cudaError_t SpectralPlan::launch_mid_pipe(const RhsIO& io, cudaStream_t st) {
+  MidPipeArgs a{};
+  a.I = Ns[1] * Mh;
+  a.nsrc = n;
+  a.G = nch;
+  a.ntiles = (a.I + 8 * (256 / Ns[0]) - 1) / (8 * (256 / Ns[0]));
+  a.ngrp = mid_ngrp_;
+  a.Mh = Mh;
+  a.tw = tw_ax_[0];
+  a.grp = mid_grp_;
+  a.A = mid_A_;
+  a.kv = kv_;
+  for (int ax = 0; ax < 3; ++ax) {
+    a.kv_off[ax] = kv_off_[ax];
+    a.Ns[ax] = Ns[ax];
+  }
+  a.kv_total = kv_total_;
+  a.io = io;
+  a.err = pipe_err_;
+  const size_t smem = mid_pipe_smem(mid_ngrp_, kv_total_);
+  if (Ns[0] == 128)
+    k_mid_pipe<128><<<pipe_grid_, kPipeThreads, smem, st>>>(tm_sf_, tm_sc_, a);
+  else
+    k_mid_pipe<256><<<pipe_grid_, kPipeThreads, smem, st>>>(tm_sf_, tm_sc_, a);
+  return cudaGetLastError();
+}
+
+cudaError_t SpectralPlan::launch_c2c_pipe(bool inv, int nplanes, cudaStream_t st, const RhsIO& io) {
+  C2CPipeArgs a{};
+  a.nchunk = (Mh + 7) / 8;
+  a.nbox = nplanes * a.nchunk;
+  const int bpt = c2c_boxes(Ns[1]);
+  a.ntiles = (a.nbox + bpt - 1) / bpt;
+  a.tw = tw_ax_[1];
+  a.io = io;
+  a.err = pipe_err_;
+  const int grid = std::max(1, std::min(a.ntiles, sms_));
+  if (!inv) {
+    if (Ns[1] == 128)
+      k_c2c_pipe<128, false><<<grid, kPipeThreads, kC2cPipeSmem, st>>>(tm_sf_c2c_, a);
+    else
+      k_c2c_pipe<256, false><<<grid, kPipeThreads, kC2cPipeSmem, st>>>(tm_sf_c2c_, a);
+  } else {
+    if (Ns[1] == 128)
+      k_c2c_pipe<128, true><<<grid, kPipeThreads, kC2cPipeSmem, st>>>(tm_sc_c2c_, a);
+    else
+      k_c2c_pipe<256, true><<<grid, kPipeThreads, kC2cPipeSmem, st>>>(tm_sc_c2c_, a);
+  }
+  return cudaGetLastError();
 }
 
 cudaError_t SpectralPlan::ensure_channel_capacity(int rows) {
@@ -1830,6 +2440,8 @@ cudaError_t SpectralPlan::ensure_channel_capacity(int rows) {
   device_bytes += (size_t)(rows - sc_rows_) * srow;
   Sc_ = p;
   sc_rows_ = rows;
+  ++buffers_gen;
+  if ((pipe_mid_ || pipe_c2c_) && !encode_sc_map()) pipe_mid_ = pipe_c2c_ = false;
   return cudaSuccess;
 }
 
@@ -1837,7 +2449,8 @@ void SpectralPlan::release() {
   if (ch_sorted_ && !arena_) cudaFree(ch_sorted_);
   ch_sorted_ = nullptr;
   void* ptrs[] = {tw_x_, tw_ax_[0], tw_ax_[1], tw_ax_[2], kv_, ch_off_, ch_ent_, d_terms_, d_fac_, d_poly_,
-                  d_field_begin_, d_fold_, ych_off_, ych_ent_, ych_dst_, Sf_, Sc_, lin_ent_, sinv_, cosv_};
+                  d_field_begin_, d_fold_, ych_off_, ych_ent_, ych_dst_, Sf_, Sc_, lin_ent_, sinv_, cosv_,
+                  mid_grp_, mid_A_, pipe_err_};
   if (!arena_)  // arena memory belongs to the caller
     for (void* p : ptrs)
       if (p) cudaFree(p);
@@ -1859,6 +2472,10 @@ void SpectralPlan::release() {
   lin_ent_ = nullptr;
   sinv_ = nullptr;
   cosv_ = nullptr;
+  mid_grp_ = nullptr;
+  mid_A_ = nullptr;
+  pipe_err_ = nullptr;
+  pipe_mid_ = pipe_c2c_ = inv_row_ = false;
   nlin_ = 0;
   built_ = false;
 }
@@ -1896,9 +2513,13 @@ cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, co
       m.chan.ent = ch_sorted_;  // staged into shared memory in operator order
     }
     const size_t smem = c.smem;  // includes the staged tables
-    prep(m);
-    by_length(plan_ax_[0], c.block, [&](auto rs, auto lx) { k_mid<decltype(rs)::value, decltype(lx)::value><<<c.grid, c.block, smem, st>>>(m); });
-    RDCU_TRY(cudaGetLastError());
+    if (which == 0 && pipe_mid_ && g_first == 0 && nch_run == nch) {
+      RDCU_TRY(launch_mid_pipe(io, st));
+    } else {
+      prep(m);
+      by_length(plan_ax_[0], c.block, [&](auto rs, auto lx) { k_mid<decltype(rs)::value, decltype(lx)::value><<<c.grid, c.block, smem, st>>>(m); });
+      RDCU_TRY(cudaGetLastError());
+    }
     if (ndim == 3) {
       C2CArgs a{};
       a.La = Ns[1];
@@ -1909,9 +2530,13 @@ cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, co
       a.S = Sc_;
       a.io = io;
       dim3 grid(c2c_i_.grid, nch_run * Ns[0]);
-      prep(a);
-      by_length(plan_ax_[1], c2c_i_.block, [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, true, decltype(lx)::value><<<grid, c2c_i_.block, c2c_i_.smem, st>>>(a); });
-      RDCU_TRY(cudaGetLastError());
+      if (pipe_c2c_) {
+        RDCU_TRY(launch_c2c_pipe(true, nch_run * Ns[0], st, io));
+      } else {
+        prep(a);
+        by_length(plan_ax_[1], c2c_i_.block, [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, true, decltype(lx)::value><<<grid, c2c_i_.block, c2c_i_.smem, st>>>(a); });
+        RDCU_TRY(cudaGetLastError());
+      }
     }
   } else if (spectral) {
     Mult1DArgs m{};
@@ -1929,6 +2554,7 @@ cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, co
   // inverse x pass: the dictionary needs every channel of a row in one CTA; the Y.dat
   // output is launched one channel pair at a time
   const int step = Yout ? 2 : std::max(1, nch_run);
+  if (!Yout && inv_row_ && ct.ent == ch_ent_ && g_first == 0 && nch_run == nch) return launch_inv_row(io, st);
   for (int c0 = 0; c0 < std::max(1, nch_run); c0 += step) {
     const int cnt = spectral ? std::min(step, nch_run - c0) : 0;
     InvXArgs a{};
@@ -1992,9 +2618,13 @@ cudaError_t SpectralPlan::run(const RhsIO& io, cudaStream_t st) {
     a.S = Sf_;
     a.io = io;
     dim3 grid(c2c_f_.grid, n * Ns[0]);
-    prep(a);
-    by_length(plan_ax_[1], c2c_f_.block, [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, false, decltype(lx)::value><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(a); });
-    RDCU_TRY(cudaGetLastError());
+    if (pipe_c2c_) {
+      RDCU_TRY(launch_c2c_pipe(false, n * Ns[0], st, io));
+    } else {
+      prep(a);
+      by_length(plan_ax_[1], c2c_f_.block, [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, false, decltype(lx)::value><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(a); });
+      RDCU_TRY(cudaGetLastError());
+    }
   }
   return launch_passes(io, chan_table(ch_off_, ch_ent_, nch), h_ch_off_, nch, 0, nullptr, nullptr, st);
 }
@@ -2265,6 +2895,7 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
     c.io = io;
     dim3 grid(c2c_f_.grid, n * Ns[0]);
     RDCU_TRY(timed("c2c_axis1_fwd", 2.0 * n * spec_row, [&]() {
+      if (pipe_c2c_) return launch_c2c_pipe(false, n * Ns[0], st, io);
       prep(c);
       by_length(plan_ax_[1], c2c_f_.block, [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, false, decltype(lx)::value><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(c); });
       return cudaGetLastError();
@@ -2297,6 +2928,7 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
     }
     const size_t msmem = c.smem;
     RDCU_TRY(timed("mid_axis0", (double)(n + nch) * spec_row, [&]() {
+      if (pipe_mid_) return launch_mid_pipe(io, st);
       prep(m);
       by_length(plan_ax_[0], c.block, [&](auto rs, auto lx) { k_mid<decltype(rs)::value, decltype(lx)::value><<<c.grid, c.block, msmem, st>>>(m); });
       return cudaGetLastError();
@@ -2312,6 +2944,7 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
       a.io = io;
       dim3 grid(c2c_i_.grid, nch * Ns[0]);
       RDCU_TRY(timed("c2c_axis1_inv", 2.0 * nch * spec_row, [&]() {
+        if (pipe_c2c_) return launch_c2c_pipe(true, nch * Ns[0], st, io);
         prep(a);
         by_length(plan_ax_[1], c2c_i_.block, [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, true, decltype(lx)::value><<<grid, c2c_i_.block, c2c_i_.smem, st>>>(a); });
         return cudaGetLastError();
@@ -2338,6 +2971,7 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
   a.P = g.per_cta;
   a.tw_smem = tws;
   RDCU_TRY(timed("inv_x_dictionary", nch * spec_row + 2.0 * n * arr, [&]() {
+    if (inv_row_) return launch_inv_row(io, st);
     prep(a);
     by_length(plan_x_, g.block, [&](auto rs, auto lx) { k_inv_x<decltype(rs)::value, decltype(lx)::value><<<g.grid, g.block, g.smem, st>>>(a); });
     return cudaGetLastError();
@@ -2365,6 +2999,14 @@ cudaError_t SpectralPlan::set_coefficients(const std::vector<double>& C) {
   if (ch_sorted_ && nch >= 1 && nch <= 4) {
     const std::vector<ChanEntry> srt = sorted_entries(ent, h_ch_off_, nch);
     RDCU_TRY(cudaMemcpy(ch_sorted_, srt.data(), srt.size() * sizeof(ChanEntry), cudaMemcpyHostToDevice));
+    if (pipe_mid_) {
+      std::vector<ChanEntry> grp;
+      std::vector<double> A;
+      operator_groups(srt, &grp, &A);
+      if ((int)grp.size() != mid_ngrp_) return cudaErrorInvalidValue;
+      RDCU_TRY(cudaMemcpy(mid_grp_, grp.data(), grp.size() * sizeof(ChanEntry), cudaMemcpyHostToDevice));
+      RDCU_TRY(cudaMemcpy(mid_A_, A.data(), A.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
   }
   if (!dt.empty()) RDCU_TRY(cudaMemcpy(d_terms_, dt.data(), dt.size() * sizeof(DictTerm), cudaMemcpyHostToDevice));
   h_ch_ent_ = ent;

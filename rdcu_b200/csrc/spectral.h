@@ -1,5 +1,6 @@
 // Fused pseudospectral RHS of the dictionary: plan and launchers.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <string>
@@ -93,6 +94,11 @@ class SpectralPlan {
   int nch = 0;                // channels of the hot RHS
   int nparts_max = 0;         // error partials buffer size needed (stage-7 epilogue)
   size_t device_bytes = 0;
+  // Nonzero when a pass on TMA tiles gave up waiting for its copies (read and cleared).
+  int take_pipe_error();
+  // Incremented whenever a device buffer that launches capture is replaced (work
+  // captured in a CUDA graph before that must be captured again).
+  int buffers_gen = 0;
 
  private:
   bool built_ = false;
@@ -146,6 +152,20 @@ class SpectralPlan {
   cudaError_t upload_vec(T** dst, const std::vector<T>& v);
   // launch configurations
   PassCfg fwd_, inv_, mid_[2], c2c_f_, c2c_i_, mult_;
+  // 3D passes on TMA tiles (k_mid_pipe, k_c2c_pipe) and the warp-per-row x pass
+  // (k_inv_row): tensor maps of the field and channel spectra, operator groups and
+  // their coefficient matrices, error word
+  bool pipe_mid_ = false, pipe_c2c_ = false, inv_row_ = false;
+  int pipe_grid_ = 0, mid_ngrp_ = 0, sms_ = 1;
+  CUtensorMap tm_sf_{}, tm_sc_{}, tm_sf_c2c_{}, tm_sc_c2c_{};
+  ChanEntry* mid_grp_ = nullptr;
+  double* mid_A_ = nullptr;
+  int* pipe_err_ = nullptr;
+  void setup_pipes();
+  bool encode_sc_map();
+  cudaError_t launch_mid_pipe(const RhsIO& io, cudaStream_t stream);
+  cudaError_t launch_c2c_pipe(bool inv, int nplanes, cudaStream_t stream, const RhsIO& io);
+  cudaError_t launch_inv_row(const RhsIO& io, cudaStream_t stream);
 
   ChanTable chan_table(const int* off, const ChanEntry* ent, int nch) const;
   DictTable dict_table() const;

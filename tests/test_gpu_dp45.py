@@ -53,7 +53,10 @@ def test_fixed_step_trajectory(cuda):
 
 
 @pytest.mark.parametrize("Ns,Ls,rtol", [((32, 32), (40.0, 40.0), 1e-8), ((64,), (30.0,), 1e-6),
-                                        ((8, 8, 16), (12.0, 12.0, 20.0), 1e-7)])
+                                        ((8, 8, 16), (12.0, 12.0, 20.0), 1e-7),
+                                        ((256, 4, 8), (200.0, 4.0, 8.0), 1e-8),
+                                        ((128, 8, 6), (100.0, 6.0, 5.0), 1e-8),
+                                        ((8, 128, 128), (6.0, 100.0, 100.0), 1e-8)])
 def test_adaptive_sequence(cuda, Ns, Ls, rtol):
     rng = np.random.default_rng(len(Ns))
     prob = Problem(2, Ns, Ls, cgle_terms(len(Ns)))

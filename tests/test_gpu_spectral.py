@@ -189,3 +189,37 @@ def test_array_and_tensor_arguments(cuda):
     s.get_state(out)
     assert np.array_equal(out, y)
     s.close()
+
+
+# 3D grids whose lines have 128 or 256 points run the specialised passes: the axis-0
+# and axis-1 passes on TMA tiles (at most two fields, no more inverse channels than
+# fields) and the x pass one row per warp (dense-polynomial dictionaries); the other axes
+# stay small so the oracle finishes in seconds.  Odd sizes leave a partial last tile
+# (columns beyond the spectrum are zero-filled on load and clipped on store).
+def _tile_terms(kind):
+    if kind == "cgle":
+        return 2, cgle_terms(3)
+    if kind == "one_field":  # n = 1: one folded linear channel
+        return 1, [parse_term(s) for s in ["1.0,0,0,1", "0.5,0,4,1", "0.7,0,8,1", "0.3,0,12,1", "-1.0,0,0,3"]]
+    # n = 2: a folded channel for field 0 and the derivative d_1 u0 inside a product
+    # (two channels), constant and power-0 factors
+    return 2, [parse_term(s) for s in ["1.0,0,0,1", "0.4,0,14,1", "-0.6,0,22,1", "0.8,1,4,1,1,1", "-0.3,1,1,3",
+                                       "0.2,1", "0.5,0,1,2,0,0"]]
+
+
+@pytest.mark.parametrize("Ns,kind", [((256, 6, 10), "cgle"), ((128, 12, 8), "cgle"), ((256, 4, 6), "one_field"),
+                                     ((128, 7, 9), "mixed"), ((128, 3, 5), "cgle"), ((256, 5, 7), "mixed"),
+                                     ((6, 256, 10), "cgle"), ((5, 128, 7), "cgle"), ((4, 6, 256), "cgle"),
+                                     ((6, 5, 128), "one_field"), ((128, 128, 8), "cgle"), ((8, 128, 256), "cgle")])
+def test_tiled_passes_3d(cuda, Ns, kind):
+    rng = np.random.default_rng(sum(Ns))
+    n, terms = _tile_terms(kind)
+    Ls = tuple(float(rng.uniform(5, 50)) for _ in Ns)
+    prob = Problem(n, Ns, Ls, terms)
+    for y in (rng.uniform(-1, 1, n * prob.N), smooth_field(rng, prob)):
+        f, Y = gpu_rhs(cuda, prob, y, want_Y=True)
+        fo, Yo = osp.rhs(y, prob, return_Y=True)
+        assert rel_err(f, fo) < TOL
+        for k in range(prob.nY * n):
+            scale = max(np.max(np.abs(Yo[k])), 1e-300)
+            assert np.max(np.abs(Y[k] - Yo[k])) / scale < TOL, k
