@@ -53,6 +53,30 @@ CASES = [
 ]
 
 
+# Runs in sequence in one directory: -R restarts from FILEBASEfs.dat (rdcu.cu:944-990)
+# and append-mode outputs whenever an IC was loaded (rdcu.cu:1013-1016).  The
+# fixtures hold every output file after the last run and each run's .out text.
+_C2 = "-n 2 -N 32,32 -L 40,40 -A 2 -s 1"
+SEQ_CASES = [
+    # DP45 to t = 0.5, then -R to t = 1: the restart appends states/times/steps and
+    # rewrites fs.dat; no initial state is written on reload
+    dict(name="restart_dp45_2d", coupling=cgle_coupling_lines(2),
+         runs=[_C2 + " -t 0.5 -d 0.25 -D1", _C2 + " -t 1 -d 0.25 -D1 -R"]),
+    # fixed steps, restarted
+    dict(name="restart_fixed_2d", coupling=cgle_coupling_lines(2),
+         runs=[_C2 + " -F -t 0.05 -d 0.01 -D1", _C2 + " -F -t 0.1 -d 0.01 -D1 -R"]),
+    # a DP45 fs.dat reloaded by a stiff run: "Couldn't read order!" (rdcu.cu:968-975);
+    # the reference's BDF then stops at its cuDSS set-up, so only the .out lines up to
+    # the restart message are compared
+    dict(name="restart_dp45_to_bdf_2d", coupling=cgle_coupling_lines(2),
+         runs=[_C2 + " -t 0.5 -d 0.25 -D1", "-S " + _C2 + " -t 1 -d 0.25 -D1 -R"], out_only=True),
+    # ic.dat present: both runs start from it and append every output
+    dict(name="append_ic_2d", coupling=cgle_coupling_lines(2),
+         runs=["-n 2 -N 16,16 -L 20,20 -t 0.5 -d 0.25 -D2", "-n 2 -N 16,16 -L 20,20 -t 0.5 -d 0.25 -D2"],
+         ic=dict(n=2, N=256, seed=9, amp=1.0)),
+]
+
+
 def case_ic(case):
     spec = case.get("ic")
     if not spec:
@@ -81,6 +105,34 @@ def oracle_run_case(case, workdir):
     out = {"summary": summary}
     kinds = {"states": np.float64, "times": np.float64, "steps": np.float64, "f": np.float64,
              "Y": np.complex128, "rows": np.int32, "cols": np.int32, "vals": np.float64, "fs": np.uint8}
+    for k, dt in kinds.items():
+        p = fb + k + ".dat"
+        if os.path.exists(p):
+            out[k] = np.fromfile(p, dt)
+    return out
+
+
+def oracle_run_seq(case, workdir):
+    """The runs of a sequence case through the oracle's driver emulation, in one
+    directory; returns the output files after the last run."""
+    import os
+    import shlex
+
+    from oracle import run as orun
+    from oracle.problem import parse_term
+
+    fb = os.path.join(workdir, case["name"])
+    with open(fb + "coupling.dat", "w") as fh:
+        fh.write("\n".join(case["coupling"]) + "\n")
+    ic = case_ic(case)
+    if ic is not None:
+        ic.tofile(fb + "ic.dat")
+    out = {}
+    for i, args in enumerate(case["runs"]):
+        cfg, _, _, _ = orun.config_from_argv(shlex.split(args) + [fb])
+        cfg.terms = cfg.terms + [parse_term(s) for s in case["coupling"]]
+        out["summary_%d" % i] = orun.run(fb, cfg)
+    kinds = {"states": np.float64, "times": np.float64, "steps": np.float64, "f": np.float64, "fs": np.uint8}
     for k, dt in kinds.items():
         p = fb + k + ".dat"
         if os.path.exists(p):

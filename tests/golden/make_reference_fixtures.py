@@ -16,7 +16,7 @@ import tempfile
 import numpy as np
 
 sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))))
-from tests.golden.cases import CASES, case_ic  # noqa: E402
+from tests.golden.cases import CASES, SEQ_CASES, case_ic  # noqa: E402
 
 FILES = {"states": np.float64, "times": np.float64, "steps": np.float64, "f": np.float64,
          "Y": np.complex128, "rows": np.int32, "cols": np.int32, "vals": np.float64, "fs": np.uint8}
@@ -42,6 +42,29 @@ def run_case(ref, case, workdir):
     return out
 
 
+def run_seq_case(ref, case, workdir):
+    """The runs of a sequence case in one directory; files after the last run, and each
+    run's return code, stdout and .out text."""
+    fb = os.path.join(workdir, case["name"])
+    with open(fb + "coupling.dat", "w") as fh:
+        fh.write("\n".join(case["coupling"]) + "\n")
+    ic = case_ic(case)
+    if ic is not None:
+        ic.tofile(fb + "ic.dat")
+    out = {"runs": np.array(case["runs"])}
+    for i, args in enumerate(case["runs"]):
+        r = subprocess.run([ref] + shlex.split(args) + [fb], capture_output=True, text=True, timeout=600)
+        out["returncode_%d" % i] = np.array(r.returncode)
+        out["stdout_%d" % i] = np.array(r.stdout)
+        if os.path.exists(fb + ".out"):
+            out["out_%d" % i] = np.array(open(fb + ".out").read())
+    for k, dt in FILES.items():
+        p = fb + k + ".dat"
+        if os.path.exists(p):
+            out[k] = np.fromfile(p, dt)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", required=True)
@@ -56,6 +79,12 @@ def main():
             res = run_case(a.ref, case, wd)
             np.savez_compressed(os.path.join(a.out, case["name"] + ".npz"), **res)
             print(case["name"], "rc", int(res["returncode"]), sorted(k for k in res if k not in ("argv", "stdout")))
+        for case in SEQ_CASES:
+            if a.only and a.only not in case["name"]:
+                continue
+            res = run_seq_case(a.ref, case, wd)
+            np.savez_compressed(os.path.join(a.out, case["name"] + ".npz"), **res)
+            print(case["name"], sorted(k for k in res if not k.startswith("stdout")))
 
 
 if __name__ == "__main__":
