@@ -216,13 +216,17 @@ def test_tiled_passes_3d(cuda, Ns, kind):
     n, terms = _tile_terms(kind)
     Ls = tuple(float(rng.uniform(5, 50)) for _ in Ns)
     prob = Problem(n, Ns, Ls, terms)
-    for y in (rng.uniform(-1, 1, n * prob.N), smooth_field(rng, prob)):
-        f, Y = gpu_rhs(cuda, prob, y, want_Y=True)
-        fo, Yo = osp.rhs(y, prob, return_Y=True)
-        assert rel_err(f, fo) < TOL
-        # Y.dat blocks: the oracle's full complex transforms of these 10^4-point grids
-        # leave roundoff of ~2e-12 of the block's scale in imaginary parts that are
-        # exactly zero here (even-order blocks), hence 1e-11 for the blocks
-        for k in range(prob.nY * n):
-            scale = max(np.max(np.abs(Yo[k])), 1e-300)
-            assert np.max(np.abs(Y[k] - Yo[k])) / scale < 1e-11, k
+    # white noise: the RHS and every Y.dat block.  The oracle's full complex transforms
+    # of these 10^4-point grids leave roundoff of ~2e-12 of a block's scale in imaginary
+    # parts that are exactly zero here (even-order blocks), hence 1e-11 for the blocks.
+    y = rng.uniform(-1, 1, n * prob.N)
+    f, Y = gpu_rhs(cuda, prob, y, want_Y=True)
+    fo, Yo = osp.rhs(y, prob, return_Y=True)
+    assert rel_err(f, fo) < TOL
+    for k in range(prob.nY * n):
+        scale = max(np.max(np.abs(Yo[k])), 1e-300)
+        assert np.max(np.abs(Y[k] - Yo[k])) / scale < 1e-11, k
+    # a smooth field (some of its blocks are pure roundoff): the RHS
+    y = smooth_field(rng, prob)
+    f, _ = gpu_rhs(cuda, prob, y)
+    assert rel_err(f, osp.rhs(y, prob)) < TOL
