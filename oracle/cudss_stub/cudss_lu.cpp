@@ -16,7 +16,10 @@
 #include <cusolverSp_LOWLEVEL_PREVIEW.h>
 #include <cusparse.h>
 
+#include <algorithm>
+#include <cmath>
 #include <cstdio>
+#include <utility>
 #include <vector>
 
 #include "cudss.h"
@@ -40,7 +43,8 @@ struct cudss_stub_data {
   std::vector<int> p;          // reordering: row/column i of A(p,p) is p[i] of A
   std::vector<int> brow, bcol;  // pattern of A(p,p)
   std::vector<int> map;        // valB = valA[map]
-  std::vector<double> aval, bval, rhs, xp, x;
+  std::vector<double> aval, bval, rhs, xp, x, bsave;
+  std::vector<int> arow, acol;  // A's own pattern (residual check)
   cusparseMatDescr_t descr = nullptr;
   csrluInfoHost_t info = nullptr;
   std::vector<char> buffer;
@@ -136,25 +140,49 @@ cudssStatus_t cudssExecute(cudssHandle_t h, cudssPhase_t phase, cudssConfig_t, c
       cusparseSetMatType(d->descr, CUSPARSE_MATRIX_TYPE_GENERAL);
       cusparseSetMatIndexBase(d->descr, CUSPARSE_INDEX_BASE_ZERO);
     }
+    d->arow = row;
+    d->acol = col;
     d->p.assign(n, 0);
     cusolverStatus_t s = cusolverSpXcsrmetisndHost(h->sp, n, A->nnz, d->descr, row.data(), col.data(), nullptr,
                                                    d->p.data());
-    if (s != CUSOLVER_STATUS_SUCCESS) return fail(d, "reordering", (int)s);
-    d->brow = row;
-    d->bcol = col;
-    d->map.resize(A->nnz);
-    for (int i = 0; i < A->nnz; ++i) d->map[i] = i;
-    size_t bytes = 0;
-    s = cusolverSpXcsrperm_bufferSizeHost(h->sp, n, n, A->nnz, d->descr, d->brow.data(), d->bcol.data(), d->p.data(),
-                                          d->p.data(), &bytes);
-    if (s != CUSOLVER_STATUS_SUCCESS) return fail(d, "permutation size", (int)s);
-    std::vector<char> pbuf(bytes + 1);
-    s = cusolverSpXcsrpermHost(h->sp, n, n, A->nnz, d->descr, d->brow.data(), d->bcol.data(), d->p.data(),
-                               d->p.data(), d->map.data(), pbuf.data());
-    if (s != CUSOLVER_STATUS_SUCCESS) return fail(d, "permutation", (int)s);
+    if (s != CUSOLVER_STATUS_SUCCESS) {
+      std::fprintf(stderr, "cudss stand-in: nested dissection failed (%d), trying AMD\n", (int)s);
+      s = cusolverSpXcsrsymamdHost(h->sp, n, A->nnz, d->descr, row.data(), col.data(), d->p.data());
+    }
+    if (s != CUSOLVER_STATUS_SUCCESS) {
+      std::fprintf(stderr, "cudss stand-in: AMD failed (%d), natural order\n", (int)s);
+      for (int i = 0; i < n; ++i) d->p[i] = i;
+    }
+    {
+      std::vector<char> seen(n, 0);
+      for (int i = 0; i < n; ++i) {
+        if (d->p[i] < 0 || d->p[i] >= n || seen[d->p[i]]) return fail(d, "reordering (not a permutation)", -6);
+        seen[d->p[i]] = 1;
+      }
+    }
+    // B = A(p, p) built explicitly (row i of B is row p[i] of A, columns renumbered by
+    // the inverse permutation and sorted), with valB = valA[map]
+    std::vector<int> pinv(n);
+    for (int i = 0; i < n; ++i) pinv[d->p[i]] = i;
+    d->brow.assign(n + 1, 0);
+    d->bcol.clear();
+    d->map.clear();
+    std::vector<std::pair<int, int>> ent;
+    for (int i = 0; i < n; ++i) {
+      const int r = d->p[i];
+      ent.clear();
+      for (int q = row[r]; q < row[r + 1]; ++q) ent.push_back({pinv[col[q]], q});
+      std::sort(ent.begin(), ent.end());
+      for (const auto& e : ent) {
+        d->bcol.push_back(e.first);
+        d->map.push_back(e.second);
+      }
+      d->brow[i + 1] = (int)d->bcol.size();
+    }
     if (d->info) cusolverSpDestroyCsrluInfoHost(d->info);
     cusolverSpCreateCsrluInfoHost(&d->info);
-    s = cusolverSpXcsrluAnalysisHost(h->sp, n, A->nnz, d->descr, d->brow.data(), d->bcol.data(), d->info);
+    cusolverStatus_t s2 = cusolverSpXcsrluAnalysisHost(h->sp, n, A->nnz, d->descr, d->brow.data(), d->bcol.data(), d->info);
+    s = s2;
     if (s != CUSOLVER_STATUS_SUCCESS) return fail(d, "symbolic LU", (int)s);
     d->aval.resize(A->nnz);
     d->bval.assign(A->nnz, 0.0);
@@ -192,7 +220,21 @@ cudssStatus_t cudssExecute(cudssHandle_t h, cudssPhase_t phase, cudssConfig_t, c
     for (int i = 0; i < n; ++i) d->rhs[i] = d->x[d->p[i]];
     cusolverStatus_t s = cusolverSpDcsrluSolveHost(h->sp, n, d->rhs.data(), d->xp.data(), d->info, d->buffer.data());
     if (s != CUSOLVER_STATUS_SUCCESS) return fail(d, "LU solve", (int)s);
+    d->bsave = d->x;
     for (int i = 0; i < n; ++i) d->x[d->p[i]] = d->xp[i];
+    // max-norm residual of A x = b (a wrong solve would otherwise only show as failed
+    // Newton iterations)
+    double rn = 0.0, bn = 0.0;
+    for (int i = 0; i < n; ++i) {
+      double acc = -d->bsave[i];
+      for (int q = d->arow[i]; q < d->arow[i + 1]; ++q) acc += d->aval[q] * d->x[d->acol[q]];
+      rn = std::fmax(rn, std::fabs(acc));
+      bn = std::fmax(bn, std::fabs(d->bsave[i]));
+    }
+    if (rn > 1e-8 * (bn > 0 ? bn : 1.0)) {
+      std::fprintf(stderr, "cudss stand-in: solve residual %.3e (max |b| %.3e)\n", rn, bn);
+      return fail(d, "LU solve (residual)", -5);
+    }
     if (cudaMemcpy(x->dn, d->x.data(), sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess)
       return fail(d, "solution copy", -2);
     return CUDSS_STATUS_SUCCESS;

@@ -710,9 +710,11 @@ struct MidPipeArgs {
 constexpr int kPipeThreads = 512;
 constexpr int kPipeSrcBytes = 32768;  // one source's tile: 8 columns x 256 rows or 16 x 128
 
+constexpr int kPipeCols = 16;  // most columns of a tile (16 for 128-point lines, 8 for 256)
+
 __host__ __device__ constexpr size_t mid_pipe_smem(int ngrp, int kv_total) {
   return 1024 + 4 * (size_t)kPipeSrcBytes + 16 + (size_t)ngrp * sizeof(ChanEntry) + (size_t)ngrp * 16 * 8 +
-         (size_t)kv_total * 8;
+         (size_t)kv_total * 8 + (size_t)ngrp * kPipeCols * 3 * 8 + (size_t)ngrp * 4 + 16;
 }
 
 template <int L>
@@ -729,8 +731,18 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
   ChanEntry* sgrp = reinterpret_cast<ChanEntry*>(full + 2);
   double* sA = reinterpret_cast<double*>(sgrp + a.ngrp);
   double* skv = sA + 16 * a.ngrp;
+  // per tile: each group's column factors (kp and km products over the factors not on
+  // axis 0) and, for groups without an axis-0 factor, its whole multiplier beta
+  double* sgt = skv + a.kv_total;
+  int* sgc = reinterpret_cast<int*>(sgt + a.ngrp * kPipeCols * 3);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   for (int t = tid; t < a.ngrp; t += kPipeThreads) sgrp[t] = a.grp[t];
+  for (int t = tid; t < a.ngrp; t += kPipeThreads) {
+    const ChanEntry en = a.grp[t];
+    const int na0 = (en.nax >= 1 && en.ax0 == 0) + (en.nax >= 2 && en.ax1 == 0);
+    const int q = en.part == 0 ? en.nax : en.nax + 3;
+    sgc[t] = na0 | (en.nax << 2) | (en.part << 4) | ((q & 3) << 5);
+  }
   for (int t = tid; t < 16 * a.ngrp; t += kPipeThreads) sA[t] = a.A[t];
   for (int t = tid; t < a.kv_total; t += kPipeThreads) skv[t] = a.kv[t];
   if (tid == 0) {
@@ -772,6 +784,30 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
     }
     char* tb = buf[b];
     const long long P = (long long)tile * 8 * NB + cc;
+    // the tile's column factors (read after the barrier that ends the forward FFTs)
+    for (int t = tid; t < a.ngrp * 8 * NB; t += kPipeThreads) {
+      const int g = t / (8 * NB), col = t - g * (8 * NB);
+      const long long Pc = (long long)tile * 8 * NB + col;
+      const int k1 = Pc < a.I ? (int)(Pc / a.Mh) : 0, kx = Pc < a.I ? (int)(Pc - (long long)k1 * a.Mh) : 0;
+      const int m1 = k1 == 0 ? 0 : a.Ns[1] - k1, m2 = kx == 0 ? 0 : a.Ns[2] - kx;
+      const double kpc[3] = {1.0, skv[a.kv_off[1] + k1], skv[a.kv_off[2] + kx]};
+      const double kmc[3] = {1.0, skv[a.kv_off[1] + m1], skv[a.kv_off[2] + m2]};
+      const ChanEntry en = sgrp[g];
+      double cp = 1.0, cm = 1.0;  // k_mid's products, axis-0 factors left out
+      if (en.nax >= 1 && en.ax0 != 0) {
+        cp *= kpc[en.ax0];
+        cm *= kmc[en.ax0];
+      }
+      if (en.nax >= 2 && en.ax1 != 0) {
+        cp *= kpc[en.ax1];
+        cm *= kmc[en.ax1];
+      }
+      const double sgn = (en.nax & 1) ? -1.0 : 1.0;
+      double* gt = sgt + (g * kPipeCols + col) * 3;
+      gt[0] = cp;
+      gt[1] = cm;
+      gt[2] = en.part == 0 ? 0.5 * (cp + sgn * cm) : 0.5 * (cp - sgn * cm);
+    }
     double2 v[8];
     if (h < a.nsrc) {
       char* bx = tb + h * kPipeSrcBytes + coff;
@@ -781,43 +817,40 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
     }
     __syncthreads();
     if (h < a.G) {
-      // channel h at this lane's points z = ml + LPL p of column P (k_mid's arithmetic)
+      // channel h at this lane's points z = ml + LPL p of column P: k_mid's arithmetic,
+      // the factors off axis 0 taken from the tile's column table
       const bool inP = P < a.I;
-      const int k1 = inP ? (int)(P / a.Mh) : 0, kx = inP ? (int)(P - (long long)k1 * a.Mh) : 0;
-      const int m1 = k1 == 0 ? 0 : a.Ns[1] - k1, m2 = kx == 0 ? 0 : a.Ns[2] - kx;
-      const double kp1 = skv[a.kv_off[1] + k1], km1 = skv[a.kv_off[1] + m1];
-      const double kp2 = skv[a.kv_off[2] + kx], km2 = skv[a.kv_off[2] + m2];
 #pragma unroll
       for (int p = 0; p < 8; ++p) {
         const int z = wl.ml + LPL * p;
         double2 acc = make_double2(0.0, 0.0);
         if (inP) {
           const int m0 = z == 0 ? 0 : a.Ns[0] - z;
-          const double kp[3] = {skv[a.kv_off[0] + z], kp1, kp2};
-          const double km[3] = {skv[a.kv_off[0] + m0], km1, km2};
+          const double kp0 = skv[a.kv_off[0] + z], km0 = skv[a.kv_off[0] + m0];
           double2 u[2];
           u[0] = *swz_col(tb + coff, c, z);
           u[1] = a.nsrc > 1 ? *swz_col(tb + kPipeSrcBytes + coff, c, z) : make_double2(0.0, 0.0);
           for (int g = 0; g < a.ngrp; ++g) {
-            const ChanEntry en = sgrp[g];
-            double ap = 1.0, am = 1.0;
-            if (en.nax >= 1) {
-              ap *= sel3(kp[0], kp[1], kp[2], en.ax0);
-              am *= sel3(km[0], km[1], km[2], en.ax0);
-            }
-            if (en.nax >= 2) {
-              ap *= sel3(kp[0], kp[1], kp[2], en.ax1);
-              am *= sel3(km[0], km[1], km[2], en.ax1);
-            }
-            const double sgn = (en.nax & 1) ? -1.0 : 1.0;
-            int q;
+            const int code = sgc[g];
+            const int na0 = code & 3, nax = (code >> 2) & 3, part = (code >> 4) & 1, q = code >> 5;
+            const double* gt = sgt + (g * kPipeCols + cc) * 3;
             double beta;
-            if (en.part == 0) {
-              q = en.nax;
-              beta = 0.5 * (ap + sgn * am);
+            if (na0 == 0) {
+              beta = gt[2];
             } else {
-              q = en.nax + 3;
-              beta = 0.5 * (ap - sgn * am);
+              double ap, am;
+              if (na0 == 2) {
+                ap = kp0 * kp0;
+                am = km0 * km0;
+              } else if (nax == 1) {
+                ap = kp0;
+                am = km0;
+              } else {
+                ap = kp0 * gt[0];
+                am = km0 * gt[1];
+              }
+              const double sgn = (nax & 1) ? -1.0 : 1.0;
+              beta = part == 0 ? 0.5 * (ap + sgn * am) : 0.5 * (ap - sgn * am);
             }
             const double* Ag = sA + g * 16 + h * 4;
             double2 sum = make_double2(0.0, 0.0);
@@ -829,7 +862,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
               sum.y += w * u[s4].y;
             }
             double2 vv = make_double2(beta * sum.x, beta * sum.y);
-            switch (q & 3) {
+            switch (q) {
               case 1: vv = make_double2(-vv.y, vv.x); break;
               case 2: vv = make_double2(-vv.x, -vv.y); break;
               case 3: vv = make_double2(vv.y, -vv.x); break;
