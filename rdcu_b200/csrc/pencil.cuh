@@ -4,9 +4,10 @@
 // of the transformed axis, moved between global and shared memory by the tensor memory
 // accelerator (cp.async.bulk.tensor) with the 128-byte swizzle: row z of the box is 128
 // bytes, and column c of it sits at byte z*128 + ((c ^ (z & 7)) << 4) from the box base
-// (1024-byte aligned).  Each CTA is persistent and double-buffers its tiles: the loads
-// of the next tile complete on an mbarrier while the current one is transformed, and
-// results leave by TMA stores from the same buffer.
+// (1024-byte aligned).  Each CTA is persistent and keeps a ring of three tile buffers:
+// while one tile is transformed, the stores of the one before leave from its buffer and
+// the loads of the one after complete on an mbarrier; results leave by TMA stores from
+// the buffer they were computed in.
 //
 // Each line is transformed by one warp (256 points) or one half warp (128 points), its
 // eight values per lane held in registers; the Stockham stages of the plan (8, 8, then
@@ -102,6 +103,8 @@ __device__ __forceinline__ void tma_store_3d(const CUtensorMap* m, int x, int y,
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 // the stores issued so far have finished reading shared memory
 __device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// every store group but the most recent one has finished reading shared memory
+__device__ __forceinline__ void bulk_wait_read_1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
 // ... and have completed
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 

@@ -709,12 +709,13 @@ struct MidPipeArgs {
 
 constexpr int kPipeThreads = 512;
 constexpr int kPipeSrcBytes = 32768;  // one source's tile: 8 columns x 256 rows or 16 x 128
-
+constexpr int kPipeBufBytes = 2 * kPipeSrcBytes;  // one tile buffer (two sources, or two boxes)
+constexpr int kPipeBufs = 3;  // tile ring: computing on one, storing from the one before, loading the next
 constexpr int kPipeCols = 16;  // most columns of a tile (16 for 128-point lines, 8 for 256)
 
 __host__ __device__ constexpr size_t mid_pipe_smem(int ngrp, int kv_total) {
-  return 1024 + 4 * (size_t)kPipeSrcBytes + 16 + (size_t)ngrp * sizeof(ChanEntry) + (size_t)ngrp * 16 * 8 +
-         (size_t)kv_total * 8 + (size_t)ngrp * kPipeCols * 3 * 8 + (size_t)ngrp * 4 + 16;
+  return 1024 + kPipeBufs * (size_t)kPipeBufBytes + 8 * kPipeBufs + 8 + (size_t)ngrp * sizeof(ChanEntry) +
+         (size_t)ngrp * 16 * 8 + (size_t)kv_total * 8 + (size_t)ngrp * kPipeCols * 3 * 8 + (size_t)ngrp * 4 + 16;
 }
 
 template <int L>
@@ -726,9 +727,8 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
   constexpr int LPL = L / 8;
   constexpr int BOXB = L * 128;
   char* sm = smraw + ((1024 - (smem_u32(smraw) & 1023)) & 1023);
-  char* buf[2] = {sm, sm + 2 * kPipeSrcBytes};
-  uint64_t* full = reinterpret_cast<uint64_t*>(sm + 4 * kPipeSrcBytes);
-  ChanEntry* sgrp = reinterpret_cast<ChanEntry*>(full + 2);
+  uint64_t* full = reinterpret_cast<uint64_t*>(sm + kPipeBufs * kPipeBufBytes);
+  ChanEntry* sgrp = reinterpret_cast<ChanEntry*>(full + kPipeBufs + 1);
   double* sA = reinterpret_cast<double*>(sgrp + a.ngrp);
   double* skv = sA + 16 * a.ngrp;
   // per tile: each group's column factors (kp and km products over the factors not on
@@ -746,8 +746,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
   for (int t = tid; t < 16 * a.ngrp; t += kPipeThreads) sA[t] = a.A[t];
   for (int t = tid; t < a.kv_total; t += kPipeThreads) skv[t] = a.kv[t];
   if (tid == 0) {
-    mbar_init(&full[0], 1);
-    mbar_init(&full[1], 1);
+    for (int k = 0; k < kPipeBufs; ++k) mbar_init(&full[k], 1);
     mbar_fence_init();
     tma_prefetch(&tmF);
     tma_prefetch(&tmC);
@@ -762,27 +761,28 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
   auto issue = [&](int tile, int b) {
     mbar_expect_tx(&full[b], (unsigned)(a.nsrc * kPipeSrcBytes));
     const int P0 = tile * 8 * NB;
+    char* dst = sm + b * kPipeBufBytes;
     for (int s = 0; s < a.nsrc; ++s)
       for (int bx = 0; bx < NB; ++bx)
-        tma_load_2d(buf[b] + s * kPipeSrcBytes + bx * BOXB, &tmF, 2 * (P0 + 8 * bx), s * L, &full[b]);
+        tma_load_2d(dst + s * kPipeSrcBytes + bx * BOXB, &tmF, 2 * (P0 + 8 * bx), s * L, &full[b]);
   };
   if (tid == 0) {
     if ((int)blockIdx.x < a.ntiles) issue(blockIdx.x, 0);
     if ((int)(blockIdx.x + gridDim.x) < a.ntiles) issue(blockIdx.x + gridDim.x, 1);
   }
-  int it = 0;
-  for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, ++it) {
-    const int b = it & 1;
-    const bool ok = mbar_wait(&full[b], (unsigned)((it >> 1) & 1));
+  int it = 0, b = 0;
+  for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, ++it, b = (b + 1 == kPipeBufs) ? 0 : b + 1) {
+    const bool ok = mbar_wait(&full[b], (unsigned)((it / kPipeBufs) & 1));
     if (__syncthreads_or(!ok)) {
       if (tid == 0) {
         atomicExch(a.io.mode == 1 ? &a.io.ctl->pipe_err : a.err, kPipeErrTimeout);
-        mbar_wait(&full[b ^ 1], (unsigned)(((it + 1) >> 1) & 1));  // bounded: the other buffer's loads
+        const int b1 = (b + 1) % kPipeBufs;  // bounded: the next buffer's loads
+        if (tile + (int)gridDim.x < a.ntiles) mbar_wait(&full[b1], (unsigned)(((it + 1) / kPipeBufs) & 1));
         bulk_wait_all();
       }
       return;
     }
-    char* tb = buf[b];
+    char* tb = sm + b * kPipeBufBytes;
     const long long P = (long long)tile * 8 * NB + cc;
     // the tile's column factors (read after the barrier that ends the forward FFTs)
     for (int t = tid; t < a.ngrp * 8 * NB; t += kPipeThreads) {
@@ -890,8 +890,8 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
       bulk_commit();
       const int nt = tile + 2 * (int)gridDim.x;
       if (nt < a.ntiles) {
-        bulk_wait_read_all();  // the stores have read this buffer
-        issue(nt, b);
+        bulk_wait_read_1();  // the previous tile's stores have read the buffer the next load fills
+        issue(nt, (b + 2) % kPipeBufs);
       }
     }
   }
@@ -910,7 +910,7 @@ struct C2CPipeArgs {
 };
 
 __host__ __device__ constexpr int c2c_boxes(int L) { return 2 * (256 / L); }
-constexpr size_t kC2cPipeSmem = 1024 + 4 * (size_t)kPipeSrcBytes + 16;
+constexpr size_t kC2cPipeSmem = 1024 + kPipeBufs * (size_t)kPipeBufBytes + 8 * kPipeBufs + 8;
 
 template <int L, bool INV>
 __global__ void __launch_bounds__(kPipeThreads, 1)
@@ -921,12 +921,10 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
   constexpr int LPL = L / 8;
   constexpr int BOXB = L * 128;
   char* sm = smraw + ((1024 - (smem_u32(smraw) & 1023)) & 1023);
-  char* buf[2] = {sm, sm + 2 * kPipeSrcBytes};
-  uint64_t* full = reinterpret_cast<uint64_t*>(sm + 4 * kPipeSrcBytes);
+  uint64_t* full = reinterpret_cast<uint64_t*>(sm + kPipeBufs * kPipeBufBytes);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0) {
-    mbar_init(&full[0], 1);
-    mbar_init(&full[1], 1);
+    for (int k = 0; k < kPipeBufs; ++k) mbar_init(&full[k], 1);
     mbar_fence_init();
     tma_prefetch(&tm);
   }
@@ -938,28 +936,30 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
   auto issue = [&](int tile, int b) {
     const int b0 = tile * BPT, nb = min(BPT, a.nbox - b0);
     mbar_expect_tx(&full[b], (unsigned)(nb * BOXB));
+    char* dst = sm + b * kPipeBufBytes;
     for (int k = 0; k < nb; ++k) {
       const int plane = (b0 + k) / a.nchunk, chunk = (b0 + k) - plane * a.nchunk;
-      tma_load_3d(buf[b] + k * BOXB, &tm, 16 * chunk, 0, plane, &full[b]);
+      tma_load_3d(dst + k * BOXB, &tm, 16 * chunk, 0, plane, &full[b]);
     }
   };
   if (tid == 0) {
     if ((int)blockIdx.x < a.ntiles) issue(blockIdx.x, 0);
     if ((int)(blockIdx.x + gridDim.x) < a.ntiles) issue(blockIdx.x + gridDim.x, 1);
   }
-  int it = 0;
-  for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, ++it) {
-    const int b = it & 1;
-    const bool ok = mbar_wait(&full[b], (unsigned)((it >> 1) & 1));
+  int it = 0, b = 0;
+  for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, ++it, b = (b + 1 == kPipeBufs) ? 0 : b + 1) {
+    const bool ok = mbar_wait(&full[b], (unsigned)((it / kPipeBufs) & 1));
     if (__syncthreads_or(!ok)) {
       if (tid == 0) {
         atomicExch(a.io.mode == 1 ? &a.io.ctl->pipe_err : a.err, kPipeErrTimeout);
-        mbar_wait(&full[b ^ 1], (unsigned)(((it + 1) >> 1) & 1));
+        const int b1 = (b + 1) % kPipeBufs;
+        if (tile + (int)gridDim.x < a.ntiles) mbar_wait(&full[b1], (unsigned)(((it + 1) / kPipeBufs) & 1));
         bulk_wait_all();
       }
       return;
     }
-    char* bx = buf[b] + coff;
+    char* tb = sm + b * kPipeBufBytes;
+    char* bx = tb + coff;
     if (tile * BPT + (li >> 3) < a.nbox) {
       double2 v[8];
       wl.load(v, bx, c);
@@ -972,13 +972,13 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
       const int b0 = tile * BPT, nb = min(BPT, a.nbox - b0);
       for (int k = 0; k < nb; ++k) {
         const int plane = (b0 + k) / a.nchunk, chunk = (b0 + k) - plane * a.nchunk;
-        tma_store_3d(&tm, 16 * chunk, 0, plane, buf[b] + k * BOXB);
+        tma_store_3d(&tm, 16 * chunk, 0, plane, tb + k * BOXB);
       }
       bulk_commit();
       const int nt = tile + 2 * (int)gridDim.x;
       if (nt < a.ntiles) {
-        bulk_wait_read_all();
-        issue(nt, b);
+        bulk_wait_read_1();
+        issue(nt, (b + 2) % kPipeBufs);
       }
     }
   }
@@ -1446,13 +1446,14 @@ __global__ void __launch_bounds__(LX > 0 ? kSpecBlock : kMaxBlock, LX > 0 ? 3 : 
 }
 
 // ---- x pass of 3D grids with 128- or 256-point rows and a dense-polynomial dictionary
-// of at most two inverse channels: one row per warp (two per warp for 128 points).  The
+// of at most two inverse channels (DP45 stages without the error epilogue, and plain
+// RHS evaluations): one row per warp (two per warp for 128 points).  Per row, the
+// physical fields start copying into the warp's shared staging area (cp.async), the
 // channels' half spectra go from global memory straight into registers (k_inv_x's
 // Hermitian extension and two-channel packing), the inverse transform runs in registers
-// with its exchanges in a per-warp line buffer (WarpLine), then the dictionary and the
-// stage-7 error terms are formed for the lane's points.  Same arithmetic as k_inv_x, per
-// point and per row partial (x = lane, lane + 32, ... then the butterfly over the lanes);
-// no block barriers after the table staging.
+// with its exchanges in the warp's line buffer (WarpLine), then the dictionary is formed
+// at the lane's points -- k_inv_x's arithmetic per point.  No block barriers after the
+// table staging.
 struct InvRowArgs {
   int R, n, nch, Mh;
   const double2* tw;
@@ -1461,9 +1462,11 @@ struct InvRowArgs {
   RhsIO io;
 };
 constexpr int kRowThreads = 256;
+constexpr int kRowWarps = kRowThreads / 32;
 
+// per warp: one 256-point complex line and up to three 256-point real field rows
 __host__ __device__ constexpr size_t inv_row_smem(int n, int count) {
-  return (size_t)(kRowThreads / 32) * 256 * 16 + (size_t)n * count * 8 + 64;
+  return (size_t)kRowWarps * (256 * 16 + 3 * 256 * 8) + (size_t)n * count * 8 + 64;
 }
 
 template <int L, int NF>
@@ -1474,21 +1477,40 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_inv_row(InvRowArgs a) {
   constexpr int LPL = L / 8, RPW = 32 / LPL;  // lanes per row, rows per warp
   const Resolved r = resolve(a.io);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  double* spoly = reinterpret_cast<double*>(sm + (kRowThreads / 32) * 256);
+  double* ubase = reinterpret_cast<double*>(sm + kRowWarps * 256);
+  double* spoly = ubase + kRowWarps * 3 * 256;
   int* sfold = reinterpret_cast<int*>(spoly + NF * MN::count);
   for (int t = tid; t < NF * MN::count; t += kRowThreads) spoly[t] = a.dict.poly[t];
   for (int t = tid; t < NF; t += kRowThreads) sfold[t] = a.dict.fold[t];
   __syncthreads();
   const int sub = lane / LPL, ml = lane % LPL;
   double2* line = sm + warp * 256 + sub * L;
+  double* ub = ubase + warp * 3 * 256 + sub * NF * L;  // this row's fields: ub[f * L + x]
   WarpLine<L> wl;
   wl.init(a.tw, ml);
-  const bool err = (a.io.mode == 1 && r.stage == 7 && a.io.err_part != nullptr);
   const long long RL = (long long)a.R * L;
-  const long long wstride = (long long)gridDim.x * (kRowThreads / 32) * RPW;
-  for (long long row0 = ((long long)blockIdx.x * (kRowThreads / 32) + warp) * RPW; row0 < a.R; row0 += wstride) {
+  const bool u16 = (reinterpret_cast<unsigned long long>(r.u) & 15) == 0;
+  const long long wstride = (long long)gridDim.x * kRowWarps * RPW;
+  for (long long row0 = ((long long)blockIdx.x * kRowWarps + warp) * RPW; row0 < a.R; row0 += wstride) {
     const long long row = row0 + sub;
     const bool live = row < a.R;
+    // the row's physical fields into the staging area, overlapped with what follows
+    if (live) {
+      if (u16) {
+#pragma unroll
+        for (int f = 0; f < NF; ++f)
+#pragma unroll
+          for (int k = 0; k < L / 2 / LPL; ++k) {
+            const int x2 = 2 * (ml + LPL * k);
+            cp_async16(ub + f * L + x2, r.u + f * RL + row * L + x2, true);
+          }
+      } else {
+#pragma unroll
+        for (int f = 0; f < NF; ++f)
+#pragma unroll
+          for (int k = 0; k < 8; ++k) ub[f * L + ml + LPL * k] = r.u[f * RL + row * L + ml + LPL * k];
+      }
+    }
     double2 v[8];
 #pragma unroll
     for (int p = 0; p < 8; ++p) {
@@ -1511,22 +1533,22 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_inv_row(InvRowArgs a) {
     }
     wl.template transform<true>(v, [line](int e) { return line + e; });
     // the lane's values back to its own line positions (the transform's last barrier has
-    // passed; nothing else reads them), so the point loop holds no spectral registers
+    // passed), so the point loop holds no spectral registers
 #pragma unroll
     for (int p = 0; p < 8; ++p) line[ml + LPL * p] = v[p];
-    double es_even = 0.0, es_odd = 0.0;  // 128 points: the partials of lanes ml and ml + 16
-#pragma unroll 1
+    cp_async_wait_all();
+    __syncwarp();  // every lane's field copies landed
+#pragma unroll 2
     for (int p = 0; p < 8; ++p) {
-      const double2 z = line[ml + LPL * p];
-      const long long gx = row * L + ml + LPL * p;
+      const int x = ml + LPL * p;
+      const double2 z = line[x];
       double u[NF];
 #pragma unroll
-      for (int f = 0; f < NF; ++f) u[f] = live ? r.u[f * RL + gx] : 0.0;
+      for (int f = 0; f < NF; ++f) u[f] = ub[f * L + x];
       double mono[MN::count];
       mono[0] = 1.0;
 #pragma unroll
       for (int m = 1; m < MN::count; ++m) mono[m] = mono[MN::parent(m)] * u[MN::var(m)];
-      double err2 = 0.0;
 #pragma unroll
       for (int i = 0; i < NF; ++i) {
         const int fc = sfold[i];
@@ -1534,31 +1556,10 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_inv_row(InvRowArgs a) {
         const double* ci = spoly + i * MN::count;
 #pragma unroll
         for (int m = 0; m < MN::count; ++m) acc += ci[m] * mono[m];
-        if (live) {
-          const long long gi = i * RL + gx;
-          r.f[gi] = acc;
-          if (err) {
-            const double yold = r.y[gi];
-            const double es = c_e[0] * r.k[0][gi] + c_e[2] * r.k[2][gi] + c_e[3] * r.k[3][gi] +
-                              c_e[4] * r.k[4][gi] + c_e[5] * r.k[5][gi] + c_e[6] * acc;
-            const double ev = r.h * es / (r.atol + r.rtol * fmax(fabs(yold), fabs(u[i])));
-            err2 += ev * ev;
-          }
-        }
+        if (live) r.f[i * RL + row * L + x] = acc;
       }
-      if (L == 256 || (p & 1) == 0)
-        es_even += err2;
-      else
-        es_odd += err2;
     }
-    __syncwarp();  // the next row's transform rewrites the line
-    if (err) {
-      double sacc = es_even;
-      if (L == 128) sacc = es_even + es_odd;  // k_inv_x's first butterfly step (lane ^ 16)
-#pragma unroll
-      for (int o = LPL / 2; o > 0; o >>= 1) sacc += __shfl_xor_sync(0xffffffffu, sacc, o);
-      if (ml == 0 && live) a.io.err_part[row] = sacc;
-    }
+    __syncwarp();  // the next row's copies and transform rewrite the staging area and line
   }
 }
 
@@ -2396,7 +2397,7 @@ cudaError_t SpectralPlan::launch_inv_row(const RhsIO& io, cudaStream_t st) {
   a.dict = dict_table();
   a.io = io;
   const size_t smem = inv_row_smem(n, poly_count_);
-  const int rows_per_cta = (kRowThreads / 32) * (32 / (M / 8));
+  const int rows_per_cta = kRowWarps * (32 / (M / 8));
   const int grid = std::max(1, std::min((R + rows_per_cta - 1) / rows_per_cta, 4 * sms_));
   auto go = [&](auto lx) {
     constexpr int LX = decltype(lx)::value;
@@ -2587,7 +2588,10 @@ cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, co
   // inverse x pass: the dictionary needs every channel of a row in one CTA; the Y.dat
   // output is launched one channel pair at a time
   const int step = Yout ? 2 : std::max(1, nch_run);
-  if (!Yout && inv_row_ && ct.ent == ch_ent_ && g_first == 0 && nch_run == nch) return launch_inv_row(io, st);
+  // the row kernel has no error epilogue: stage 7 of an adaptive step keeps k_inv_x
+  const bool err_epilogue = io.mode == 1 && io.stage == 7 && io.err_part != nullptr;
+  if (!Yout && inv_row_ && !err_epilogue && ct.ent == ch_ent_ && g_first == 0 && nch_run == nch)
+    return launch_inv_row(io, st);
   for (int c0 = 0; c0 < std::max(1, nch_run); c0 += step) {
     const int cnt = spectral ? std::min(step, nch_run - c0) : 0;
     InvXArgs a{};
@@ -3004,7 +3008,7 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
   a.P = g.per_cta;
   a.tw_smem = tws;
   RDCU_TRY(timed("inv_x_dictionary", nch * spec_row + 2.0 * n * arr, [&]() {
-    if (inv_row_) return launch_inv_row(io, st);
+    if (inv_row_ && !(io.mode == 1 && io.stage == 7 && io.err_part != nullptr)) return launch_inv_row(io, st);
     prep(a);
     by_length(plan_x_, g.block, [&](auto rs, auto lx) { k_inv_x<decltype(rs)::value, decltype(lx)::value><<<g.grid, g.block, g.smem, st>>>(a); });
     return cudaGetLastError();

@@ -13,7 +13,7 @@ import tempfile
 import numpy as np
 import pytest
 
-from tests.golden.cases import CASES, case_ic, fixture, fixture_steps
+from tests.golden.cases import CASES, SEQ_CASES, case_ic, fixture, fixture_steps
 from tests.helpers import rel_err
 
 pytestmark = pytest.mark.gpu
@@ -76,3 +76,67 @@ def test_cli_matches_reference(case):
         assert o["steps"].size == fx["steps"].size
         assert np.max(np.abs(o["steps"] - fx["steps"]) / np.abs(fx["steps"])) < 1e-8
         assert rel_err(o["states"], fx["states"]) < 1e-8
+
+
+def run_seq_cli(case, wd):
+    fb = os.path.join(wd, case["name"])
+    with open(fb + "coupling.dat", "w") as fh:
+        fh.write("\n".join(case["coupling"]) + "\n")
+    ic = case_ic(case)
+    if ic is not None:
+        ic.tofile(fb + "ic.dat")
+    out = {}
+    for i, args in enumerate(case["runs"]):
+        r = subprocess.run([CLI] + shlex.split(args) + [fb], capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stdout + r.stderr
+        out["out_%d" % i] = open(fb + ".out").read()
+    for k, dt in list(KINDS.items()) + [("fs", np.uint8)]:
+        if os.path.exists(fb + k + ".dat"):
+            out[k] = np.fromfile(fb + k + ".dat", dt)
+    return out
+
+
+def message_lines(text):
+    """The .out lines after the argv line: status messages as they are, progress lines as
+    (fraction of the run, h, accepted steps) -- their elapsed-time columns differ -- and
+    no runtime line."""
+    res = []
+    for line in str(text).splitlines()[1:]:
+        if not line.strip() or line.startswith("runtime:"):
+            continue
+        if line[0].isdigit():
+            c = line.split("\t")
+            res.append((c[0], c[3], c[4]))
+        else:
+            res.append(line)
+    return res
+
+
+@pytest.mark.parametrize("case", SEQ_CASES, ids=[c["name"] for c in SEQ_CASES])
+def test_cli_sequence_matches_reference(case):
+    """-R restarts and ic.dat append runs: each run's .out messages, and every output file
+    after the last run, against the reference's."""
+    fx = fixture(case["name"])
+    with tempfile.TemporaryDirectory() as wd:
+        o = run_seq_cli(case, wd)
+    for i in range(len(case["runs"])):
+        ours, ref = message_lines(o["out_%d" % i]), message_lines(fx["out_%d" % i])
+        if case.get("out_only") and i == len(case["runs"]) - 1:
+            # the reference's BDF stops at its cuDSS set-up: messages up to the restart
+            k = next(j for j, l in enumerate(ref) if isinstance(l, str) and l.startswith("Restarting at"))
+            assert ours[: k + 1] == ref[: k + 1], (ours[: k + 1], ref[: k + 1])
+        else:
+            assert ours == ref, (i, ours, ref)
+    if case.get("out_only"):
+        return
+    np.testing.assert_array_equal(o["times"], fx["times"])
+    assert o["states"].size == fx["states"].size
+    assert rel_err(o["states"], fx["states"]) < 1e-8
+    assert o["steps"].size == fx["steps"].size
+    assert np.max(np.abs(o["steps"] - fx["steps"]) / np.abs(fx["steps"])) < 1e-8
+    if "f" in fx:
+        assert rel_err(o["f"], fx["f"]) < 1e-7
+    a, b = o["fs"].view(np.float64), fx["fs"].view(np.float64)
+    assert a.size == b.size
+    assert rel_err(a[:-2], b[:-2]) < 1e-8
+    assert np.max(np.abs(a[-2:] - b[-2:]) / np.abs(b[-2:])) < 1e-10
