@@ -77,6 +77,27 @@ SEQ_CASES = [
 ]
 
 
+# The reference's BDF path (bdf.cu) run by oracle/_ref/rdcu_ref_lu: the unmodified
+# reference sources with a solving stand-in for cuDSS (oracle/cudss_stub/cudss_lu.cpp,
+# cuSOLVER's host sparse LU).  "ref": "lu" marks the cases that need it.
+_B2 = "-S -n 2 -N 32,32 -L 40,40 -A 2 -s 1"
+BDF_SEQ_CASES = [
+    # a stiff run of the 2D CGLE (finite differences, variable-order BDF)
+    dict(name="bdf_cgle_2d", coupling=cgle_coupling_lines(2), runs=[_B2 + " -t 2 -d 0.5 -D1"], ref="lu"),
+    # the Brusselator from an ic.dat (offsets (1, 3) plus noise)
+    dict(name="bdf_brusselator_2d", coupling=brusselator_coupling_lines(),
+         runs=["-S -n 2 -N 32,32 -L 16,16 -t 3 -d 1 -D1"], ic=dict(n=2, N=1024, seed=3, base=(1.0, 3.0), amp=0.1),
+         ref="lu"),
+    # BDF to t = 1, then -R to t = 2: fs.dat carries the order and the D blocks
+    # (rdcu.cu:322-339, reloaded at :977-983)
+    dict(name="restart_bdf_2d", coupling=cgle_coupling_lines(2),
+         runs=[_B2 + " -t 1 -d 0.5 -D1", _B2 + " -t 2 -d 0.5 -D1 -R"], ref="lu"),
+    # a DP45 fs.dat reloaded by a stiff run ("Couldn't read order!"), the whole run
+    dict(name="restart_dp45_to_bdf_lu_2d", coupling=cgle_coupling_lines(2),
+         runs=[_C2 + " -t 0.5 -d 0.25 -D1", "-S " + _C2 + " -t 1 -d 0.25 -D1 -R"], ref="lu"),
+]
+
+
 def case_ic(case):
     spec = case.get("ic")
     if not spec:
@@ -152,3 +173,39 @@ def fixture_steps(fx):
         if line.startswith("steps:"):
             return int(line.split()[1])
     return None
+
+
+def fs_parts(raw, nN):
+    """fs.dat as written by the reference (rdcu.cu:322-339): y (nN doubles), t, h, and
+    for stiff runs the int32 order and order*nN doubles D_1..D_order."""
+    raw = np.asarray(raw, np.uint8)
+    out = {"y": raw[: 8 * nN].view(np.float64), "th": raw[8 * nN: 8 * nN + 16].view(np.float64)}
+    rest = raw[8 * nN + 16:]
+    if rest.size >= 4:
+        out["order"] = int(rest[:4].view(np.int32)[0])
+        out["D"] = rest[4:].view(np.float64)
+    return out
+
+
+def compare_sequence_outputs(o, fx, nN, states_tol=1e-8):
+    """Every output file of a sequence case against the reference's fixture: times
+    exactly, states and step sizes to states_tol, f.dat to 1e-7, fs.dat's state, t, h,
+    order and D blocks."""
+    def rel(a, b):
+        return float(np.max(np.abs(a - b))) / max(float(np.max(np.abs(b))), 1e-300)
+
+    np.testing.assert_array_equal(o["times"], fx["times"])
+    assert o["states"].size == fx["states"].size
+    assert rel(o["states"], fx["states"]) < states_tol
+    assert o["steps"].size == fx["steps"].size
+    assert np.max(np.abs(o["steps"] - fx["steps"]) / np.abs(fx["steps"])) < states_tol
+    if "f" in fx:
+        assert rel(o["f"], fx["f"]) < 1e-7
+    a, b = fs_parts(o["fs"], nN), fs_parts(fx["fs"], nN)
+    assert rel(a["y"], b["y"]) < states_tol
+    assert np.max(np.abs(a["th"] - b["th"]) / np.abs(b["th"])) < 1e-10
+    assert ("order" in a) == ("order" in b)
+    if "order" in b:
+        assert a["order"] == b["order"]
+        assert a["D"].size == b["D"].size
+        assert rel(a["D"], b["D"]) < 1e3 * states_tol  # differences: D_k of h^k scale

@@ -1,7 +1,7 @@
 """Runs the golden cases (cases.py) through the reference's own build and stores every
 output file as a compressed .npz fixture.
 
-    python tests/golden/make_reference_fixtures.py --ref oracle/_ref/rdcu_ref --out DIR
+    python tests/golden/make_reference_fixtures.py --ref oracle/_ref/rdcu_ref --ref-lu oracle/_ref/rdcu_ref_lu --out DIR
 
 Needs a GPU (the reference is CUDA-only).  The committed fixtures in tests/golden were
 made with this script from the reference sources built by oracle/build_ref.sh.
@@ -16,7 +16,7 @@ import tempfile
 import numpy as np
 
 sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))))
-from tests.golden.cases import CASES, SEQ_CASES, case_ic  # noqa: E402
+from tests.golden.cases import BDF_SEQ_CASES, CASES, SEQ_CASES, case_ic  # noqa: E402
 
 FILES = {"states": np.float64, "times": np.float64, "steps": np.float64, "f": np.float64,
          "Y": np.complex128, "rows": np.int32, "cols": np.int32, "vals": np.float64, "fs": np.uint8}
@@ -68,6 +68,7 @@ def run_seq_case(ref, case, workdir):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", required=True)
+    ap.add_argument("--ref-lu", default=None, help="the reference built with the solving cuDSS stand-in")
     ap.add_argument("--out", required=True)
     ap.add_argument("--only", default=None)
     a = ap.parse_args()
@@ -79,10 +80,10 @@ def main():
             res = run_case(a.ref, case, wd)
             np.savez_compressed(os.path.join(a.out, case["name"] + ".npz"), **res)
             print(case["name"], "rc", int(res["returncode"]), sorted(k for k in res if k not in ("argv", "stdout")))
-        for case in SEQ_CASES:
+        for case in SEQ_CASES + (BDF_SEQ_CASES if a.ref_lu else []):
             if a.only and a.only not in case["name"]:
                 continue
-            res = run_seq_case(a.ref, case, wd)
+            res = run_seq_case(a.ref_lu if case.get("ref") == "lu" else a.ref, case, wd)
             np.savez_compressed(os.path.join(a.out, case["name"] + ".npz"), **res)
             print(case["name"], sorted(k for k in res if not k.startswith("stdout")))
 
