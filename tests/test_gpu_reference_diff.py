@@ -35,7 +35,8 @@ C3D256 = "-n 2 -N 256,256,256 -L 200,200,200 -A 2 -s 2 -r 1e-8 -a 1e-8"
 
 
 def run(binary, args, coupling, wd, name="c"):
-    """Runs one rdcu command in wd; returns (filebase, .out text)."""
+    """Runs one rdcu command in wd (FILEBASE wd/name, coupling file written unless there
+    is one); returns (filebase, .out text)."""
     assert os.path.exists(binary), "missing %s (build it with oracle/build_ref.sh / rdcu_b200.build)" % binary
     os.makedirs(wd, exist_ok=True)
     fb = os.path.join(wd, name)
@@ -100,3 +101,48 @@ def test_adaptive_cgle3d_128(tmp_path):
 def test_adaptive_cgle3d_256(tmp_path):
     # two outputs of 268 MB per build: compared on every 97th value
     check_adaptive(tmp_path, C3D256 + " -t 0.25 -d 0.25 -D1", 3, stride=97)
+
+
+REF_LU = os.path.join(ROOT, "oracle", "_ref", "rdcu_ref_lu")
+
+
+def test_bdf_brusselator_64_vs_reference_bdf(tmp_path):
+    """The reference's BDF path (bdf.cu:135-389, its own sources built with a solving
+    stand-in for the missing cuDSS, oracle/cudss_stub/cudss_lu.cpp) and this library's
+    on the Brusselator 64^2 from an ic.dat: the same accepted steps, step sizes, states,
+    final order and backward differences."""
+    from oracle.problem import brusselator_coupling_lines
+    from tests.golden.cases import fs_parts
+
+    rng = np.random.default_rng(3)
+    N = 64 * 64
+    ic = np.concatenate([1.0 + rng.uniform(-0.1, 0.1, N), 3.0 + rng.uniform(-0.1, 0.1, N)])
+    args = "-S -n 2 -N 64,64 -L 16,16 -t 5 -d 1 -D1"
+    outs = []
+    for binary, wd in ((CLI, tmp_path / "ours"), (REF_LU, tmp_path / "ref")):
+        os.makedirs(wd, exist_ok=True)
+        ic.tofile(str(wd / "cic.dat"))  # FILEBASE wd/c
+        fb, out = run(binary, args, brusselator_coupling_lines(), str(wd))
+        outs.append((fb, out))
+    (fo, oo), (fr, orf) = outs
+    assert steps_of(oo) == steps_of(orf)
+    s, sr = np.fromfile(fo + "steps.dat"), np.fromfile(fr + "steps.dat")
+    assert s.size == sr.size and np.max(np.abs(s - sr) / np.abs(sr)) < 1e-8
+    assert rel_err(np.fromfile(fo + "states.dat"), np.fromfile(fr + "states.dat")) < 1e-8
+    a, b = fs_parts(np.fromfile(fo + "fs.dat", np.uint8), 2 * N), fs_parts(np.fromfile(fr + "fs.dat", np.uint8), 2 * N)
+    assert a["order"] == b["order"]
+    assert np.max(np.abs(a["th"] - b["th"]) / np.abs(b["th"])) < 1e-10
+    assert rel_err(a["D"], b["D"]) < 1e-6
+
+
+def test_dp45_notebook_case_vs_reference(tmp_path):
+    """The reference notebook's first run (2D CGLE 256^2, L = 100, T = 10, outputs every
+    0.1, default amplitude 1e-3 and seed 1; cgle.ipynb cell 5).  The noise grows by e^10
+    before the chaotic phase, so rounding decides the last few steps: this library and
+    the reference binary on the same GPU agree to within 1% of the accepted steps (the
+    notebook's own 924 steps came from an earlier version of the reference; the
+    reference binary built from the current sources takes 857 on a B200)."""
+    args = "-t 10 -d 0.1 -N 256,256 -L 100,100 -n 2 -D1"
+    (_, oo), (_, orf) = both(tmp_path, args, cgle_coupling_lines(2))
+    so, sr = steps_of(oo), steps_of(orf)
+    assert abs(so - sr) <= 0.01 * sr, (so, sr)
