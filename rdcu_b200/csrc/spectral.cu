@@ -705,6 +705,10 @@ struct MidPipeArgs {
   int kv_total;
   RhsIO io;
   int* err;
+  // multiplier tables (TAB kernels): channel c at (z, column P) = sum_s (Mz[z][c][s] +
+  // Mc[P][c][s]) U_s, the operator groups summed at plan time
+  const double2* Mz;  // [L0][G][nsrc]
+  const double2* Mc;  // [I][G][nsrc]
 };
 
 constexpr int kPipeThreads = 512;
@@ -713,12 +717,15 @@ constexpr int kPipeBufBytes = 2 * kPipeSrcBytes;  // one tile buffer (two source
 constexpr int kPipeBufs = 3;  // tile ring: computing on one, storing from the one before, loading the next
 constexpr int kPipeCols = 16;  // most columns of a tile (16 for 128-point lines, 8 for 256)
 
-__host__ __device__ constexpr size_t mid_pipe_smem(int ngrp, int kv_total) {
+__host__ __device__ constexpr size_t mid_pipe_smem(int ngrp, int kv_total, int ztab) {
   return 1024 + kPipeBufs * (size_t)kPipeBufBytes + 8 * kPipeBufs + 8 + (size_t)ngrp * sizeof(ChanEntry) +
-         (size_t)ngrp * 16 * 8 + (size_t)kv_total * 8 + (size_t)ngrp * kPipeCols * 3 * 8 + (size_t)ngrp * 4 + 16;
+         (size_t)ngrp * 16 * 8 + (size_t)kv_total * 8 + (size_t)ngrp * kPipeCols * 3 * 8 + (size_t)ngrp * 4 + 16 +
+         (size_t)ztab * 16 + 16;
 }
 
-template <int L>
+// TAB: the multipliers from the plan's tables (no operator group mixes axis 0 with
+// another axis); otherwise k_mid's group arithmetic with per-tile column factors.
+template <int L, bool TAB>
 __global__ void __launch_bounds__(kPipeThreads, 1)
     k_mid_pipe(const __grid_constant__ CUtensorMap tmF, const __grid_constant__ CUtensorMap tmC, MidPipeArgs a) {
   extern __shared__ char smraw[];
@@ -735,7 +742,11 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
   // axis 0) and, for groups without an axis-0 factor, its whole multiplier beta
   double* sgt = skv + a.kv_total;
   int* sgc = reinterpret_cast<int*>(sgt + a.ngrp * kPipeCols * 3);
+  double2* smz = reinterpret_cast<double2*>(
+      (reinterpret_cast<uintptr_t>(sgc + a.ngrp) + 15) & ~static_cast<uintptr_t>(15));  // TAB: Mz
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (TAB)
+    for (int t = tid; t < L * a.G * a.nsrc; t += kPipeThreads) smz[t] = a.Mz[t];
   for (int t = tid; t < a.ngrp; t += kPipeThreads) sgrp[t] = a.grp[t];
   for (int t = tid; t < a.ngrp; t += kPipeThreads) {
     const ChanEntry en = a.grp[t];
@@ -785,7 +796,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
     char* tb = sm + b * kPipeBufBytes;
     const long long P = (long long)tile * 8 * NB + cc;
     // the tile's column factors (read after the barrier that ends the forward FFTs)
-    for (int t = tid; t < a.ngrp * 8 * NB; t += kPipeThreads) {
+    for (int t = tid; !TAB && t < a.ngrp * 8 * NB; t += kPipeThreads) {
       const int g = t / (8 * NB), col = t - g * (8 * NB);
       const long long Pc = (long long)tile * 8 * NB + col;
       const int k1 = Pc < a.I ? (int)(Pc / a.Mh) : 0, kx = Pc < a.I ? (int)(Pc - (long long)k1 * a.Mh) : 0;
@@ -816,7 +827,30 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
       wl.store(v, bx, c);
     }
     __syncthreads();
-    if (h < a.G) {
+    if (TAB && h < a.G) {
+      // channel h at this lane's points: (Mz[z] + Mc[P]) . U
+      const bool inP = P < a.I;
+      double2 mc[2] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
+      if (inP)
+        for (int s2 = 0; s2 < a.nsrc; ++s2) mc[s2] = a.Mc[(P * a.G + h) * a.nsrc + s2];
+#pragma unroll
+      for (int p = 0; p < 8; ++p) {
+        const int z = wl.ml + LPL * p;
+        double2 acc = make_double2(0.0, 0.0);
+        if (inP) {
+          const double2 u0 = *swz_col(tb + coff, c, z);
+          const double2* mz = smz + (z * a.G + h) * a.nsrc;
+          const double2 m0 = c_add(mz[0], mc[0]);
+          acc = c_mul(m0, u0);
+          if (a.nsrc > 1) {
+            const double2 u1 = *swz_col(tb + kPipeSrcBytes + coff, c, z);
+            const double2 m1 = c_add(mz[1], mc[1]);
+            acc = c_add(acc, c_mul(m1, u1));
+          }
+        }
+        v[p] = acc;
+      }
+    } else if (!TAB && h < a.G) {
       // channel h at this lane's points z = ml + LPL p of column P: k_mid's arithmetic,
       // the factors off axis 0 taken from the tile's column table
       const bool inP = P < a.I;
@@ -2153,6 +2187,7 @@ bool SpectralPlan::init(int n_, int ndim_, const int* Ns_, const double* Ls_,
     }
   }
   kv_total_ = (int)kv.size();
+  h_kv_ = kv;
 
   // ---- device tables
   device_bytes = 0;
@@ -2338,11 +2373,22 @@ void SpectralPlan::setup_pipes() {
   std::vector<ChanEntry> grp;
   std::vector<double> A;
   operator_groups(sorted_entries(h_ch_ent_, h_ch_off_, nch), &grp, &A);
-  const size_t smem = mid_pipe_smem((int)grp.size(), kv_total_);
+  // multiplier tables unless an operator group mixes axis 0 with another axis
+  mid_tab_ = true;
+  for (const ChanEntry& en : grp) {
+    const int na0 = (en.nax >= 1 && en.ax0 == 0) + (en.nax >= 2 && en.ax1 == 0);
+    if (na0 > 0 && na0 < en.nax) mid_tab_ = false;
+  }
+  const size_t smem = mid_pipe_smem((int)grp.size(), kv_total_, mid_tab_ ? Ns[0] * nch * n : 0);
   if (smem > 227 * 1024) return;
   if (!encode_rows(&tm_sf_, Sf_, 2 * I, (long long)n * Ns[0], Ns[0]) || !encode_sc_map()) return;
-  const void* fn = Ns[0] == 128 ? (const void*)k_mid_pipe<128> : (const void*)k_mid_pipe<256>;
+  const void* fn = Ns[0] == 128 ? (mid_tab_ ? (const void*)k_mid_pipe<128, true> : (const void*)k_mid_pipe<128, false>)
+                                : (mid_tab_ ? (const void*)k_mid_pipe<256, true> : (const void*)k_mid_pipe<256, false>);
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  if (mid_tab_ && build_mid_tables(grp, A) != cudaSuccess) {
     cudaGetLastError();
     return;
   }
@@ -2370,6 +2416,64 @@ void SpectralPlan::setup_pipes() {
       pipe_c2c_ = true;
     cudaGetLastError();
   }
+}
+
+// The multiplier of each channel and source summed over the operator groups, split by
+// the axes the groups depend on: Mz[z][c][s] (groups on axis 0 only) and Mc[P][c][s]
+// (the others; P = axis-1 index * Mh + x wavenumber).  Each group contributes
+// i^q beta_g A_g[c][s], beta_g as k_mid forms it.
+cudaError_t SpectralPlan::build_mid_tables(const std::vector<ChanEntry>& grp, const std::vector<double>& A) {
+  const int G = nch, L0 = Ns[0];
+  const long long I = (long long)Ns[1] * Mh;
+  std::vector<double2> mz((size_t)L0 * G * n, make_double2(0.0, 0.0)), mc((size_t)I * G * n, make_double2(0.0, 0.0));
+  auto kp = [&](int ax, int na) { return h_kv_[kv_off_[ax] + na]; };
+  auto km = [&](int ax, int na) { return h_kv_[kv_off_[ax] + (na == 0 ? 0 : Ns[ax] - na)]; };
+  auto add = [&](double2* m, const ChanEntry& en, const double* Ag, const int* nidx) {
+    double ap = 1.0, am = 1.0;
+    if (en.nax >= 1) {
+      ap *= kp(en.ax0, nidx[en.ax0]);
+      am *= km(en.ax0, nidx[en.ax0]);
+    }
+    if (en.nax >= 2) {
+      ap *= kp(en.ax1, nidx[en.ax1]);
+      am *= km(en.ax1, nidx[en.ax1]);
+    }
+    const double sgn = (en.nax & 1) ? -1.0 : 1.0;
+    const double beta = en.part == 0 ? 0.5 * (ap + sgn * am) : 0.5 * (ap - sgn * am);
+    const int q = (en.part == 0 ? en.nax : en.nax + 3) & 3;
+    for (int c = 0; c < G; ++c)
+      for (int s2 = 0; s2 < n; ++s2) {
+        const double v = beta * Ag[c * 4 + s2];
+        double2& d = m[c * n + s2];
+        switch (q) {
+          case 0: d.x += v; break;
+          case 1: d.y += v; break;
+          case 2: d.x -= v; break;
+          default: d.y -= v; break;
+        }
+      }
+  };
+  for (size_t g = 0; g < grp.size(); ++g) {
+    const ChanEntry& en = grp[g];
+    const int na0 = (en.nax >= 1 && en.ax0 == 0) + (en.nax >= 2 && en.ax1 == 0);
+    if (na0 > 0) {
+      for (int z = 0; z < L0; ++z) {
+        const int nidx[3] = {z, 0, 0};
+        add(&mz[(size_t)z * G * n], en, &A[g * 16], nidx);
+      }
+    } else {
+      for (long long P = 0; P < I; ++P) {
+        const int k1 = (int)(P / Mh), kx = (int)(P - (long long)k1 * Mh);
+        const int nidx[3] = {0, k1, kx};
+        add(&mc[(size_t)P * G * n], en, &A[g * 16], nidx);
+      }
+    }
+  }
+  if (!mid_mz_) RDCU_TRY(dev_alloc(&mid_mz_, mz.size() * sizeof(double2)));
+  if (!mid_mc_) RDCU_TRY(dev_alloc(&mid_mc_, mc.size() * sizeof(double2)));
+  RDCU_TRY(cudaMemcpy(mid_mz_, mz.data(), mz.size() * sizeof(double2), cudaMemcpyHostToDevice));
+  RDCU_TRY(cudaMemcpy(mid_mc_, mc.data(), mc.size() * sizeof(double2), cudaMemcpyHostToDevice));
+  return cudaSuccess;
 }
 
 bool SpectralPlan::encode_sc_map() {
@@ -2433,11 +2537,20 @@ cudaError_t SpectralPlan::launch_mid_pipe(const RhsIO& io, cudaStream_t st) {
   a.kv_total = kv_total_;
   a.io = io;
   a.err = pipe_err_;
-  const size_t smem = mid_pipe_smem(mid_ngrp_, kv_total_);
-  if (Ns[0] == 128)
-    k_mid_pipe<128><<<pipe_grid_, kPipeThreads, smem, st>>>(tm_sf_, tm_sc_, a);
-  else
-    k_mid_pipe<256><<<pipe_grid_, kPipeThreads, smem, st>>>(tm_sf_, tm_sc_, a);
+  a.Mz = mid_mz_;
+  a.Mc = mid_mc_;
+  const size_t smem = mid_pipe_smem(mid_ngrp_, kv_total_, mid_tab_ ? Ns[0] * nch * n : 0);
+  if (Ns[0] == 128) {
+    if (mid_tab_)
+      k_mid_pipe<128, true><<<pipe_grid_, kPipeThreads, smem, st>>>(tm_sf_, tm_sc_, a);
+    else
+      k_mid_pipe<128, false><<<pipe_grid_, kPipeThreads, smem, st>>>(tm_sf_, tm_sc_, a);
+  } else {
+    if (mid_tab_)
+      k_mid_pipe<256, true><<<pipe_grid_, kPipeThreads, smem, st>>>(tm_sf_, tm_sc_, a);
+    else
+      k_mid_pipe<256, false><<<pipe_grid_, kPipeThreads, smem, st>>>(tm_sf_, tm_sc_, a);
+  }
   return cudaGetLastError();
 }
 
@@ -2484,7 +2597,7 @@ void SpectralPlan::release() {
   ch_sorted_ = nullptr;
   void* ptrs[] = {tw_x_, tw_ax_[0], tw_ax_[1], tw_ax_[2], kv_, ch_off_, ch_ent_, d_terms_, d_fac_, d_poly_,
                   d_field_begin_, d_fold_, ych_off_, ych_ent_, ych_dst_, Sf_, Sc_, lin_ent_, sinv_, cosv_,
-                  mid_grp_, mid_A_, pipe_err_};
+                  mid_grp_, mid_A_, pipe_err_, mid_mz_, mid_mc_};
   if (!arena_)  // arena memory belongs to the caller
     for (void* p : ptrs)
       if (p) cudaFree(p);
@@ -2508,6 +2621,8 @@ void SpectralPlan::release() {
   cosv_ = nullptr;
   mid_grp_ = nullptr;
   mid_A_ = nullptr;
+  mid_mz_ = nullptr;
+  mid_mc_ = nullptr;
   pipe_err_ = nullptr;
   pipe_mid_ = pipe_c2c_ = inv_row_ = false;
   nlin_ = 0;
@@ -3043,6 +3158,7 @@ cudaError_t SpectralPlan::set_coefficients(const std::vector<double>& C) {
       if ((int)grp.size() != mid_ngrp_) return cudaErrorInvalidValue;
       RDCU_TRY(cudaMemcpy(mid_grp_, grp.data(), grp.size() * sizeof(ChanEntry), cudaMemcpyHostToDevice));
       RDCU_TRY(cudaMemcpy(mid_A_, A.data(), A.size() * sizeof(double), cudaMemcpyHostToDevice));
+      if (mid_tab_) RDCU_TRY(build_mid_tables(grp, A));
     }
   }
   if (!dt.empty()) RDCU_TRY(cudaMemcpy(d_terms_, dt.data(), dt.size() * sizeof(DictTerm), cudaMemcpyHostToDevice));

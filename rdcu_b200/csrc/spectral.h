@@ -160,6 +160,11 @@ class SpectralPlan {
   CUtensorMap tm_sf_{}, tm_sc_{}, tm_sf_c2c_{}, tm_sc_c2c_{};
   ChanEntry* mid_grp_ = nullptr;
   double* mid_A_ = nullptr;
+  bool mid_tab_ = false;           // multiplier tables (no group mixes axis 0 with another axis)
+  double2* mid_mz_ = nullptr;      // [L0][nch][n]
+  double2* mid_mc_ = nullptr;      // [N1 * Mh][nch][n]
+  std::vector<double> h_kv_;       // host copy of the wavenumbers
+  cudaError_t build_mid_tables(const std::vector<ChanEntry>& grp, const std::vector<double>& A);
   int* pipe_err_ = nullptr;
   void setup_pipes();
   bool encode_sc_map();
