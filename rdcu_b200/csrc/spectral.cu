@@ -707,7 +707,7 @@ struct MidPipeArgs {
   int* err;
   // multiplier tables (TAB kernels): channel c at (z, column P) = sum_s (Mz[z][c][s] +
   // Mc[P][c][s]) U_s, the operator groups summed at plan time
-  const double2* Mz;  // [L0][G][nsrc]
+  const double2* Mz;  // [G][nsrc][L0]
   const double2* Mc;  // [I][G][nsrc]
 };
 
@@ -819,6 +819,10 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
       gt[1] = cm;
       gt[2] = en.part == 0 ? 0.5 * (cp + sgn * cm) : 0.5 * (cp - sgn * cm);
     }
+    // TAB: this lane's column multipliers, loaded before the transform needs them
+    double2 mc[2] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
+    if (TAB && h < a.G && P < a.I)
+      for (int s2 = 0; s2 < a.nsrc; ++s2) mc[s2] = a.Mc[(P * a.G + h) * a.nsrc + s2];
     double2 v[8];
     if (h < a.nsrc) {
       char* bx = tb + h * kPipeSrcBytes + coff;
@@ -830,21 +834,18 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
     if (TAB && h < a.G) {
       // channel h at this lane's points: (Mz[z] + Mc[P]) . U
       const bool inP = P < a.I;
-      double2 mc[2] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
-      if (inP)
-        for (int s2 = 0; s2 < a.nsrc; ++s2) mc[s2] = a.Mc[(P * a.G + h) * a.nsrc + s2];
 #pragma unroll
       for (int p = 0; p < 8; ++p) {
         const int z = wl.ml + LPL * p;
         double2 acc = make_double2(0.0, 0.0);
         if (inP) {
           const double2 u0 = *swz_col(tb + coff, c, z);
-          const double2* mz = smz + (z * a.G + h) * a.nsrc;
+          const double2* mz = smz + h * a.nsrc * L + z;  // [h][s][z]: consecutive lanes, consecutive z
           const double2 m0 = c_add(mz[0], mc[0]);
           acc = c_mul(m0, u0);
           if (a.nsrc > 1) {
             const double2 u1 = *swz_col(tb + kPipeSrcBytes + coff, c, z);
-            const double2 m1 = c_add(mz[1], mc[1]);
+            const double2 m1 = c_add(mz[L], mc[1]);
             acc = c_add(acc, c_mul(m1, u1));
           }
         }
@@ -1481,13 +1482,13 @@ __global__ void __launch_bounds__(LX > 0 ? kSpecBlock : kMaxBlock, LX > 0 ? 3 : 
 
 // ---- x pass of 3D grids with 128- or 256-point rows and a dense-polynomial dictionary
 // of at most two inverse channels (DP45 stages without the error epilogue, and plain
-// RHS evaluations): one row per warp (two per warp for 128 points).  Per row, the
-// physical fields start copying into the warp's shared staging area (cp.async), the
-// channels' half spectra go from global memory straight into registers (k_inv_x's
-// Hermitian extension and two-channel packing), the inverse transform runs in registers
-// with its exchanges in the warp's line buffer (WarpLine), then the dictionary is formed
-// at the lane's points -- k_inv_x's arithmetic per point.  No block barriers after the
-// table staging.
+// RHS evaluations): one row per warp (two per warp for 128 points).  Each warp streams
+// its rows through two staging slots in shared memory: while one row is transformed and
+// evaluated, asynchronous copies (cp.async) bring the next row's channel half spectra
+// and physical fields.  Per row: k_inv_x's Hermitian extension and two-channel packing
+// from the staged spectra, the inverse transform in registers with its exchanges in the
+// warp's line buffer (WarpLine), then the dictionary at the lane's points -- k_inv_x's
+// arithmetic per point.  No block barriers after the table staging.
 struct InvRowArgs {
   int R, n, nch, Mh;
   const double2* tw;
@@ -1497,69 +1498,93 @@ struct InvRowArgs {
 };
 constexpr int kRowThreads = 256;
 constexpr int kRowWarps = kRowThreads / 32;
+// one staging slot of a warp: 2 channels x (at most 129 + padding) spectral values and
+// NF x 256 field values (two rows of 128 points take the same room)
+constexpr int kRowSpec = 2 * 136;  // double2 per slot
+__host__ __device__ constexpr int row_slot_doubles(int nf) { return 2 * kRowSpec + nf * 256; }
 
-// per warp: one 256-point complex line and up to three 256-point real field rows
 __host__ __device__ constexpr size_t inv_row_smem(int n, int count) {
-  return (size_t)kRowWarps * (256 * 16 + 3 * 256 * 8) + (size_t)n * count * 8 + 64;
+  return (size_t)kRowWarps * (256 * 16 + 2 * (size_t)row_slot_doubles(n) * 8) + (size_t)n * count * 8 + 64;
 }
 
 template <int L, int NF>
-__global__ void __launch_bounds__(kRowThreads, 2) k_inv_row(InvRowArgs a) {
+__global__ void __launch_bounds__(kRowThreads, 1) k_inv_row(InvRowArgs a) {
   extern __shared__ double2 sm[];
   if (a.io.mode == 1 && !a.io.ctl->running) return;
   using MN = Mono<NF>;
   constexpr int LPL = L / 8, RPW = 32 / LPL;  // lanes per row, rows per warp
+  constexpr int SLOT = row_slot_doubles(NF);
   const Resolved r = resolve(a.io);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  double* ubase = reinterpret_cast<double*>(sm + kRowWarps * 256);
-  double* spoly = ubase + kRowWarps * 3 * 256;
+  double* stage = reinterpret_cast<double*>(sm + kRowWarps * 256);
+  double* spoly = stage + kRowWarps * 2 * SLOT;
   int* sfold = reinterpret_cast<int*>(spoly + NF * MN::count);
   for (int t = tid; t < NF * MN::count; t += kRowThreads) spoly[t] = a.dict.poly[t];
   for (int t = tid; t < NF; t += kRowThreads) sfold[t] = a.dict.fold[t];
   __syncthreads();
   const int sub = lane / LPL, ml = lane % LPL;
   double2* line = sm + warp * 256 + sub * L;
-  double* ub = ubase + warp * 3 * 256 + sub * NF * L;  // this row's fields: ub[f * L + x]
   WarpLine<L> wl;
   wl.init(a.tw, ml);
   const long long RL = (long long)a.R * L;
-  const bool u16 = (reinterpret_cast<unsigned long long>(r.u) & 15) == 0;
+  // the row's spectra (both channels) and fields as 16-byte pieces, when aligned
+  const bool a16 = ((reinterpret_cast<unsigned long long>(r.u) | reinterpret_cast<unsigned long long>(a.Sc)) & 15) == 0;
+  const int Mh = a.Mh, nch = a.nch;
   const long long wstride = (long long)gridDim.x * kRowWarps * RPW;
-  for (long long row0 = ((long long)blockIdx.x * kRowWarps + warp) * RPW; row0 < a.R; row0 += wstride) {
+  // slot k of this warp; the sub-row's part of it
+  auto slot_spec = [&](int k) { return reinterpret_cast<double2*>(stage + (warp * 2 + k) * SLOT) + sub * (kRowSpec / RPW); };
+  auto slot_u = [&](int k) { return stage + (warp * 2 + k) * SLOT + 2 * kRowSpec + sub * NF * L; };
+  auto fetch = [&](long long row, int k) {
+    if (row >= a.R) return;
+    double2* sp = slot_spec(k);
+    double* su = slot_u(k);
+    if (a16) {
+      for (int c = 0; c < nch; ++c)
+        for (int e = ml; e < Mh; e += LPL) cp_async16(sp + c * Mh + e, a.Sc + ((long long)c * a.R + row) * Mh + e, true);
+#pragma unroll
+      for (int f = 0; f < NF; ++f)
+#pragma unroll
+        for (int k2 = 0; k2 < L / 2 / LPL; ++k2) {
+          const int x2 = 2 * (ml + LPL * k2);
+          cp_async16(su + f * L + x2, r.u + f * RL + row * L + x2, true);
+        }
+    } else {
+      for (int c = 0; c < nch; ++c)
+        for (int e = ml; e < Mh; e += LPL) sp[c * Mh + e] = a.Sc[((long long)c * a.R + row) * Mh + e];
+      for (int f = 0; f < NF; ++f)
+        for (int k2 = 0; k2 < 8; ++k2) su[f * L + ml + LPL * k2] = r.u[f * RL + row * L + ml + LPL * k2];
+    }
+  };
+  long long row0 = ((long long)blockIdx.x * kRowWarps + warp) * RPW;
+  fetch(row0 + sub, 0);
+  cp_async_commit();
+  int k = 0;
+  for (; row0 < a.R; row0 += wstride, k ^= 1) {
     const long long row = row0 + sub;
     const bool live = row < a.R;
-    // the row's physical fields into the staging area, overlapped with what follows
-    if (live) {
-      if (u16) {
-#pragma unroll
-        for (int f = 0; f < NF; ++f)
-#pragma unroll
-          for (int k = 0; k < L / 2 / LPL; ++k) {
-            const int x2 = 2 * (ml + LPL * k);
-            cp_async16(ub + f * L + x2, r.u + f * RL + row * L + x2, true);
-          }
-      } else {
-#pragma unroll
-        for (int f = 0; f < NF; ++f)
-#pragma unroll
-          for (int k = 0; k < 8; ++k) ub[f * L + ml + LPL * k] = r.u[f * RL + row * L + ml + LPL * k];
-      }
-    }
+    // the next row's copies go to the other slot (its last reads ended at the previous
+    // row's final barrier)
+    fetch(row0 + wstride + sub, k ^ 1);
+    cp_async_commit();
+    cp_async_wait_1();
+    __syncwarp();  // this row's copies (every lane's) landed
+    const double2* sp = slot_spec(k);
+    const double* su = slot_u(k);
     double2 v[8];
 #pragma unroll
     for (int p = 0; p < 8; ++p) {
       const int kx = ml + LPL * p;
-      const int kk = kx >= a.Mh ? L - kx : kx;
+      const int kk = kx >= Mh ? L - kx : kx;
       double2 Av = make_double2(0.0, 0.0), Bv = make_double2(0.0, 0.0);
       if (live) {
-        Av = a.Sc[row * a.Mh + kk];
-        if (a.nch > 1) Bv = a.Sc[((long long)a.R + row) * a.Mh + kk];
+        Av = sp[kk];
+        if (nch > 1) Bv = sp[Mh + kk];
       }
       if (kx == 0 || 2 * kx == L) {
         Av.y = 0.0;
         Bv.y = 0.0;
       }
-      if (kx >= a.Mh) {
+      if (kx >= Mh) {
         Av.y = -Av.y;
         Bv.y = -Bv.y;
       }
@@ -1570,15 +1595,13 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_inv_row(InvRowArgs a) {
     // passed), so the point loop holds no spectral registers
 #pragma unroll
     for (int p = 0; p < 8; ++p) line[ml + LPL * p] = v[p];
-    cp_async_wait_all();
-    __syncwarp();  // every lane's field copies landed
 #pragma unroll 2
     for (int p = 0; p < 8; ++p) {
       const int x = ml + LPL * p;
       const double2 z = line[x];
       double u[NF];
 #pragma unroll
-      for (int f = 0; f < NF; ++f) u[f] = ub[f * L + x];
+      for (int f = 0; f < NF; ++f) u[f] = su[f * L + x];
       double mono[MN::count];
       mono[0] = 1.0;
 #pragma unroll
@@ -1593,8 +1616,9 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_inv_row(InvRowArgs a) {
         if (live) r.f[i * RL + row * L + x] = acc;
       }
     }
-    __syncwarp();  // the next row's copies and transform rewrite the staging area and line
+    __syncwarp();  // the next row's transform and the copies after it rewrite the line and this slot
   }
+  cp_async_wait_all();
 }
 
 // ---- batched passes: persistent CTAs over (problem, tile) work items
@@ -2419,7 +2443,7 @@ void SpectralPlan::setup_pipes() {
 }
 
 // The multiplier of each channel and source summed over the operator groups, split by
-// the axes the groups depend on: Mz[z][c][s] (groups on axis 0 only) and Mc[P][c][s]
+// the axes the groups depend on: Mz[c][s][z] (groups on axis 0 only) and Mc[P][c][s]
 // (the others; P = axis-1 index * Mh + x wavenumber).  Each group contributes
 // i^q beta_g A_g[c][s], beta_g as k_mid forms it.
 cudaError_t SpectralPlan::build_mid_tables(const std::vector<ChanEntry>& grp, const std::vector<double>& A) {
@@ -2428,7 +2452,8 @@ cudaError_t SpectralPlan::build_mid_tables(const std::vector<ChanEntry>& grp, co
   std::vector<double2> mz((size_t)L0 * G * n, make_double2(0.0, 0.0)), mc((size_t)I * G * n, make_double2(0.0, 0.0));
   auto kp = [&](int ax, int na) { return h_kv_[kv_off_[ax] + na]; };
   auto km = [&](int ax, int na) { return h_kv_[kv_off_[ax] + (na == 0 ? 0 : Ns[ax] - na)]; };
-  auto add = [&](double2* m, const ChanEntry& en, const double* Ag, const int* nidx) {
+  // m[(c * n + s) * stride]: the (c, s) entry of the point's multiplier
+  auto add = [&](double2* m, long long stride, const ChanEntry& en, const double* Ag, const int* nidx) {
     double ap = 1.0, am = 1.0;
     if (en.nax >= 1) {
       ap *= kp(en.ax0, nidx[en.ax0]);
@@ -2444,7 +2469,7 @@ cudaError_t SpectralPlan::build_mid_tables(const std::vector<ChanEntry>& grp, co
     for (int c = 0; c < G; ++c)
       for (int s2 = 0; s2 < n; ++s2) {
         const double v = beta * Ag[c * 4 + s2];
-        double2& d = m[c * n + s2];
+        double2& d = m[(c * n + s2) * stride];
         switch (q) {
           case 0: d.x += v; break;
           case 1: d.y += v; break;
@@ -2459,13 +2484,13 @@ cudaError_t SpectralPlan::build_mid_tables(const std::vector<ChanEntry>& grp, co
     if (na0 > 0) {
       for (int z = 0; z < L0; ++z) {
         const int nidx[3] = {z, 0, 0};
-        add(&mz[(size_t)z * G * n], en, &A[g * 16], nidx);
+        add(&mz[z], L0, en, &A[g * 16], nidx);
       }
     } else {
       for (long long P = 0; P < I; ++P) {
         const int k1 = (int)(P / Mh), kx = (int)(P - (long long)k1 * Mh);
         const int nidx[3] = {0, k1, kx};
-        add(&mc[(size_t)P * G * n], en, &A[g * 16], nidx);
+        add(&mc[(size_t)P * G * n], 1, en, &A[g * 16], nidx);
       }
     }
   }
@@ -2502,7 +2527,7 @@ cudaError_t SpectralPlan::launch_inv_row(const RhsIO& io, cudaStream_t st) {
   a.io = io;
   const size_t smem = inv_row_smem(n, poly_count_);
   const int rows_per_cta = kRowWarps * (32 / (M / 8));
-  const int grid = std::max(1, std::min((R + rows_per_cta - 1) / rows_per_cta, 4 * sms_));
+  const int grid = std::max(1, std::min((R + rows_per_cta - 1) / rows_per_cta, sms_));  // one resident CTA per SM
   auto go = [&](auto lx) {
     constexpr int LX = decltype(lx)::value;
     switch (n) {
