@@ -720,7 +720,7 @@ constexpr int kPipeCols = 16;  // most columns of a tile (16 for 128-point lines
 __host__ __device__ constexpr size_t mid_pipe_smem(int ngrp, int kv_total, int ztab) {
   return 1024 + kPipeBufs * (size_t)kPipeBufBytes + 8 * kPipeBufs + 8 + (size_t)ngrp * sizeof(ChanEntry) +
          (size_t)ngrp * 16 * 8 + (size_t)kv_total * 8 + (size_t)ngrp * kPipeCols * 3 * 8 + (size_t)ngrp * 4 + 16 +
-         (size_t)ztab * 16 + 16;
+         (size_t)ztab * 16 + 16 + (ztab ? kPipeBufs * kPipeCols * 4 * 16 : 0);
 }
 
 // TAB: the multipliers from the plan's tables (no operator group mixes axis 0 with
@@ -744,6 +744,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
   int* sgc = reinterpret_cast<int*>(sgt + a.ngrp * kPipeCols * 3);
   double2* smz = reinterpret_cast<double2*>(
       (reinterpret_cast<uintptr_t>(sgc + a.ngrp) + 15) & ~static_cast<uintptr_t>(15));  // TAB: Mz
+  double2* smc = smz + L * a.G * a.nsrc;  // TAB: each buffer's column multipliers (Mc rows of its tile)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (TAB)
     for (int t = tid; t < L * a.G * a.nsrc; t += kPipeThreads) smz[t] = a.Mz[t];
@@ -770,12 +771,15 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
   WarpLine<L> wl;
   wl.init(a.tw, lane % LPL);
   auto issue = [&](int tile, int b) {
-    mbar_expect_tx(&full[b], (unsigned)(a.nsrc * kPipeSrcBytes));
     const int P0 = tile * 8 * NB;
+    const int ncol = min(8 * NB, a.I - P0);
+    const unsigned mcb = TAB ? (unsigned)(ncol * a.G * a.nsrc * 16) : 0u;
+    mbar_expect_tx(&full[b], (unsigned)(a.nsrc * kPipeSrcBytes) + mcb);
     char* dst = sm + b * kPipeBufBytes;
     for (int s = 0; s < a.nsrc; ++s)
       for (int bx = 0; bx < NB; ++bx)
         tma_load_2d(dst + s * kPipeSrcBytes + bx * BOXB, &tmF, 2 * (P0 + 8 * bx), s * L, &full[b]);
+    if (TAB) bulk_load(smc + b * kPipeCols * 4, a.Mc + (long long)P0 * a.G * a.nsrc, mcb, &full[b]);
   };
   if (tid == 0) {
     if ((int)blockIdx.x < a.ntiles) issue(blockIdx.x, 0);
@@ -819,10 +823,6 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
       gt[1] = cm;
       gt[2] = en.part == 0 ? 0.5 * (cp + sgn * cm) : 0.5 * (cp - sgn * cm);
     }
-    // TAB: this lane's column multipliers, loaded before the transform needs them
-    double2 mc[2] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
-    if (TAB && h < a.G && P < a.I)
-      for (int s2 = 0; s2 < a.nsrc; ++s2) mc[s2] = a.Mc[(P * a.G + h) * a.nsrc + s2];
     double2 v[8];
     if (h < a.nsrc) {
       char* bx = tb + h * kPipeSrcBytes + coff;
@@ -834,6 +834,9 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
     if (TAB && h < a.G) {
       // channel h at this lane's points: (Mz[z] + Mc[P]) . U
       const bool inP = P < a.I;
+      double2 mc[2] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
+      if (inP)
+        for (int s2 = 0; s2 < a.nsrc; ++s2) mc[s2] = smc[b * kPipeCols * 4 + (cc * a.G + h) * a.nsrc + s2];
 #pragma unroll
       for (int p = 0; p < 8; ++p) {
         const int z = wl.ml + LPL * p;
