@@ -162,9 +162,11 @@ int rdcu_advance(rdcu_t *h, int n_attempts, double hmin, double hmax, long long 
 /* Per-kernel timing of one fused RHS stage for roofline reporting: each pass kernel of
  * DP45 stage 4 (forward x transform with the stage combination, strided transforms,
  * axis-0 pass with the derivative multipliers, inverse x transform with the dictionary)
- * is launched `reps` times between CUDA events on the handle's stream.  Fills up to
- * max_passes entries with the pass name, its average time in ms and the bytes the pass
- * must read and write per launch.  Leaves y and k1 untouched.  DP45 handles only. */
+ * is launched `reps` times between CUDA events on the handle's stream, then stage 7's
+ * forward pass ("fwd_x_stage7", six slopes) and inverse pass ("inv_x_stage7", with the
+ * error estimate's reads on adaptive handles).  Fills up to max_passes entries with the
+ * pass name, its average time in ms and the bytes the pass must read and write per
+ * launch.  Leaves y and k1 untouched.  DP45 handles only. */
 typedef struct rdcu_pass_timing {
   const char *name;
   double ms;

@@ -368,7 +368,8 @@ class Solver:
         return acc.value
 
     def profile_passes(self, reps: int = 20):
-        """[(name, ms per launch, bytes per launch)] for each pass of one fused RHS stage."""
+        """[(name, ms per launch, bytes per launch)] for each pass of DP45 stage 4, then
+        stage 7's forward and inverse passes (rdcu_profile_passes)."""
         arr = (rdcu_pass_timing * 16)()
         npass = ctypes.c_int()
         self._check(self.lib.rdcu_profile_passes(self.h, reps, arr, 16, ctypes.byref(npass)))

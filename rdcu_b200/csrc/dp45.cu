@@ -10,6 +10,7 @@
 // so the host only wakes up at output times.
 #include <algorithm>
 #include <cmath>
+#include <string>
 #include <cstring>
 
 #include "dp45.h"
@@ -367,6 +368,16 @@ cudaError_t DP45Engine::profile(int reps, std::vector<SpectralPlan::PassTime>* o
   io.bufs = bufs;
   io.ctl = d_ctl_;
   RDCU_TRY(sp_->profile(io, reps, st_, out));
+  // stage 7: the stage combination over six slopes, and (adaptive steps) the inverse
+  // pass with the error epilogue
+  std::vector<SpectralPlan::PassTime> p7;
+  io.stage = 7;
+  io.err_part = fixed_ ? nullptr : err_part_;
+  RDCU_TRY(sp_->profile(io, reps, st_, &p7));
+  for (const auto& p : p7) {
+    if (std::string(p.name) == "fwd_x") out->push_back({"fwd_x_stage7", p.ms, p.bytes});
+    if (std::string(p.name) == "inv_x_dictionary") out->push_back({"inv_x_stage7", p.ms, p.bytes});
+  }
   // leave the controller idle, as after a completed attempt
   k_dp45_arm<<<1, 1, 0, st_>>>(d_ctl_, 0, INFINITY, 0.0, INFINITY, 0, 0, 1);
   RDCU_TRY(cudaGetLastError());

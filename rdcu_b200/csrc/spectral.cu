@@ -3150,7 +3150,9 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
   inv_geometry(M, R, n, nch, false, plan_x_, &g, &tws, dict_smem_bytes());
   a.P = g.per_cta;
   a.tw_smem = tws;
-  RDCU_TRY(timed("inv_x_dictionary", nch * spec_row + 2.0 * n * arr, [&]() {
+  // stage 7 of an adaptive step also reads y and five slopes for the error estimate
+  const bool err_epilogue = io.mode == 1 && io.stage == 7 && io.err_part != nullptr;
+  RDCU_TRY(timed("inv_x_dictionary", nch * spec_row + 2.0 * n * arr + (err_epilogue ? 6.0 * n * arr : 0.0), [&]() {
     if (inv_row_ && !(io.mode == 1 && io.stage == 7 && io.err_part != nullptr)) return launch_inv_row(io, st);
     prep(a);
     by_length(plan_x_, g.block, [&](auto rs, auto lx) { k_inv_x<decltype(rs)::value, decltype(lx)::value><<<g.grid, g.block, g.smem, st>>>(a); });
