@@ -177,8 +177,8 @@ NCU_POINTS = 256 * 256 * 128
 # one ncu capture (`ncu --set full -k regex:"k_(faces|hook|corr)" ... bench.py --workload
 # lines_cgle3d_128 --steps 1 --warmup 3`): k_faces reads the 16.8 MB phase field once.
 NCU_TRAFFIC_LINES = {"faces": 16.8e6}
-NCU_TRAFFIC_3D = {"fwd_x": 772.5e6, "c2c_axis1_fwd": 218.7e6, "mid_axis0": 234.5e6, "c2c_axis1_inv": 218.7e6,
-                  "inv_x_dictionary": 374.7e6}
+NCU_TRAFFIC_3D = {"fwd_x": 772.5e6, "c2c_axis1_fwd": 219.3e6, "mid_axis0": 226.4e6, "c2c_axis1_inv": 219.6e6,
+                  "inv_x_dictionary": 373.3e6}
 
 
 def combine_ranks(seconds, work, device):
@@ -297,7 +297,8 @@ def run_ours(args, rank, world, local_rank):
                 "d2h_bytes_per_step": 2 * nN * 8 / args.steps, "accepted_steps": acc2, "seconds": e2e_s},
         "roofline": {"bound": "hbm", "kernel": top[0], "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
-                     "traffic": (NCU_TRAFFIC_3D[top[0]] * N / NCU_POINTS) if len(Ns) == 3 else None,
+                     "traffic": (NCU_TRAFFIC_3D[top[0]] * N / NCU_POINTS)
+                     if len(Ns) == 3 and top[0] in NCU_TRAFFIC_3D else None,
                      "traffic_note": "ncu DRAM bytes of the 256x256x128 capture scaled by grid points"
                                      if len(Ns) == 3 else "no capture for 1D/2D",
                      "algorithmic_bytes_per_launch": top[2], "launch_ms": top[1],
