@@ -709,6 +709,9 @@ struct MidPipeArgs {
   // Mc[P][c][s]) U_s, the operator groups summed at plan time
   const double2* Mz;  // [G][nsrc][L0]
   const double2* Mc;  // [I][G][nsrc]
+  // k_mid_pipe2: the groups on axis 0 alone as beta_g(z) and rotated matrices R_g
+  const double* Bz;   // [NZ][L0]
+  const double2* Rz;  // [NZ][G][nsrc]
 };
 
 constexpr int kPipeThreads = 512;
@@ -924,6 +927,150 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
     if (tid == 0) {
       const int P0 = tile * 8 * NB;
       for (int ch = 0; ch < a.G; ++ch)
+        for (int bx = 0; bx < NB; ++bx) tma_store_2d(&tmC, 2 * (P0 + 8 * bx), ch * L, tb + ch * kPipeSrcBytes + bx * BOXB);
+      bulk_commit();
+      const int nt = tile + 2 * (int)gridDim.x;
+      if (nt < a.ntiles) {
+        bulk_wait_read_1();  // the previous tile's stores have read the buffer the next load fills
+        issue(nt, (b + 2) % kPipeBufs);
+      }
+    }
+  }
+  if (tid == 0) bulk_wait_all();
+}
+
+// ---- axis-0 pass, one column per warp (two per warp for 128-point lines): the lanes of a
+// column transform every source, form every channel in registers and transform the
+// channels back, so a tile needs no block barrier between its phases.  For
+// multipliers that split into at most two groups on axis 0 alone (NZ) and groups off
+// axis 0: channel c at (z, P) = sum_s (Mc[P][c][s] + sum_g beta_g(z) R_g[c][s]) U_s, with
+// the lane's beta_g at its eight points and the R_g in registers and the tile's Mc rows
+// bulk-copied with the tile.  kMid2Threads: one warp per column pair or column.
+constexpr int kMid2Threads = 256;
+
+__host__ __device__ constexpr size_t mid2_smem(int L0) {
+  return 1024 + kPipeBufs * (size_t)kPipeBufBytes + 8 * kPipeBufs + 8 + kPipeBufs * kPipeCols * 4 * 16 +
+         2 * (size_t)L0 * 8 + 2 * 4 * 16;
+}
+
+template <int L, int NZ>
+__global__ void __launch_bounds__(kMid2Threads, 1)
+    k_mid_pipe2(const __grid_constant__ CUtensorMap tmF, const __grid_constant__ CUtensorMap tmC, MidPipeArgs a) {
+  extern __shared__ char smraw[];
+  if (a.io.mode == 1 && !a.io.ctl->running) return;
+  constexpr int NB = 256 / L;  // boxes per source tile
+  constexpr int LPL = L / 8;
+  constexpr int BOXB = L * 128;
+  char* sm = smraw + ((1024 - (smem_u32(smraw) & 1023)) & 1023);
+  uint64_t* full = reinterpret_cast<uint64_t*>(sm + kPipeBufs * kPipeBufBytes);
+  double2* smc = reinterpret_cast<double2*>(full + kPipeBufs + 1);  // each buffer's Mc rows
+  double2* srz = smc + kPipeBufs * kPipeCols * 4;                     // R_g[c][s], zero-padded to 2 x 2
+  double* sbz = reinterpret_cast<double*>(srz + NZ * 4);              // beta_g(z)
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int G = a.G, nsrc = a.nsrc;
+  for (int t = tid; t < NZ * L; t += kMid2Threads) sbz[t] = a.Bz[t];
+  for (int t = tid; t < NZ * 4; t += kMid2Threads) {
+    const int g = t >> 2, ch = (t >> 1) & 1, s2 = t & 1;
+    srz[t] = (ch < G && s2 < nsrc) ? a.Rz[(g * G + ch) * nsrc + s2] : make_double2(0.0, 0.0);
+  }
+  if (tid == 0) {
+    for (int k = 0; k < kPipeBufs; ++k) mbar_init(&full[k], 1);
+    mbar_fence_init();
+    tma_prefetch(&tmF);
+    tma_prefetch(&tmC);
+  }
+  __syncthreads();
+  const int cc = warp * (32 / LPL) + lane / LPL;  // column of the tile
+  const int coff = (cc >> 3) * BOXB;              // offset of the column's box in a source tile
+  const int c = cc & 7;
+  WarpLine<L> wl;
+  wl.init(a.tw, lane % LPL);
+  auto issue = [&](int tile, int b) {
+    const int P0 = tile * 8 * NB;
+    const int ncol = min(8 * NB, a.I - P0);
+    const unsigned mcb = (unsigned)(ncol * G * nsrc * 16);
+    mbar_expect_tx(&full[b], (unsigned)(nsrc * kPipeSrcBytes) + mcb);
+    char* dst = sm + b * kPipeBufBytes;
+    for (int s2 = 0; s2 < nsrc; ++s2)
+      for (int bx = 0; bx < NB; ++bx)
+        tma_load_2d(dst + s2 * kPipeSrcBytes + bx * BOXB, &tmF, 2 * (P0 + 8 * bx), s2 * L, &full[b]);
+    bulk_load(smc + b * kPipeCols * 4, a.Mc + (long long)P0 * G * nsrc, mcb, &full[b]);
+  };
+  if (tid == 0) {
+    if ((int)blockIdx.x < a.ntiles) issue(blockIdx.x, 0);
+    if ((int)(blockIdx.x + gridDim.x) < a.ntiles) issue(blockIdx.x + gridDim.x, 1);
+  }
+  int it = 0, b = 0;
+  for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, ++it, b = (b + 1 == kPipeBufs) ? 0 : b + 1) {
+    const bool ok = mbar_wait(&full[b], (unsigned)((it / kPipeBufs) & 1));
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        atomicExch(a.io.mode == 1 ? &a.io.ctl->pipe_err : a.err, kPipeErrTimeout);
+        const int b1 = (b + 1) % kPipeBufs;  // bounded: the next buffer's loads
+        if (tile + (int)gridDim.x < a.ntiles) mbar_wait(&full[b1], (unsigned)(((it + 1) / kPipeBufs) & 1));
+        bulk_wait_all();
+      }
+      return;
+    }
+    char* tb = sm + b * kPipeBufBytes;
+    const long long P = (long long)tile * 8 * NB + cc;
+    const bool inP = P < a.I;
+    double2 x[2][8];
+#pragma unroll
+    for (int s2 = 0; s2 < 2; ++s2) {
+      if (s2 < nsrc) {
+        char* bx = tb + s2 * kPipeSrcBytes + coff;
+        wl.load(x[s2], bx, c);
+        wl.template transform<false>(x[s2], bx, c);
+      } else {
+#pragma unroll
+        for (int p = 0; p < 8; ++p) x[s2][p] = make_double2(0.0, 0.0);
+      }
+    }
+    double2 mc[2][2];
+#pragma unroll
+    for (int ch = 0; ch < 2; ++ch)
+#pragma unroll
+      for (int s2 = 0; s2 < 2; ++s2)
+        mc[ch][s2] = (inP && ch < G && s2 < nsrc) ? smc[b * kPipeCols * 4 + (cc * G + ch) * nsrc + s2]
+                                                   : make_double2(0.0, 0.0);
+    // every channel at the lane's points, over the sources in place
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+      double2 out[2];
+#pragma unroll
+      for (int ch = 0; ch < 2; ++ch) {
+        double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int s2 = 0; s2 < 2; ++s2) {
+          double2 m = mc[ch][s2];
+#pragma unroll
+          for (int g = 0; g < NZ; ++g) {
+            const double bg = sbz[g * L + wl.ml + LPL * p];
+            const double2 r = srz[g * 4 + ch * 2 + s2];
+            m.x += bg * r.x;
+            m.y += bg * r.y;
+          }
+          acc = c_add(acc, c_mul(m, x[s2][p]));
+        }
+        out[ch] = inP ? acc : make_double2(0.0, 0.0);
+      }
+      x[0][p] = out[0];
+      x[1][p] = out[1];
+    }
+#pragma unroll
+    for (int ch = 0; ch < 2; ++ch) {
+      if (ch < G) {
+        char* bx = tb + ch * kPipeSrcBytes + coff;
+        wl.template transform<true>(x[ch], bx, c);
+        wl.store(x[ch], bx, c);
+      }
+    }
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      const int P0 = tile * 8 * NB;
+      for (int ch = 0; ch < G; ++ch)
         for (int bx = 0; bx < NB; ++bx) tma_store_2d(&tmC, 2 * (P0 + 8 * bx), ch * L, tb + ch * kPipeSrcBytes + bx * BOXB);
       bulk_commit();
       const int nt = tile + 2 * (int)gridDim.x;
@@ -2406,6 +2553,21 @@ void SpectralPlan::setup_pipes() {
     const int na0 = (en.nax >= 1 && en.ax0 == 0) + (en.nax >= 2 && en.ax1 == 0);
     if (na0 > 0 && na0 < en.nax) mid_tab_ = false;
   }
+  // one column per warp with register multipliers: at most two groups on axis 0 alone
+  mid_nz_ = 0;
+  for (const ChanEntry& en : grp) {
+    const int na0 = (en.nax >= 1 && en.ax0 == 0) + (en.nax >= 2 && en.ax1 == 0);
+    if (na0 > 0 && na0 == en.nax) ++mid_nz_;
+  }
+  mid2_ = mid_tab_ && mid_nz_ <= 2;
+  if (mid2_) {
+    const void* f2 = Ns[0] == 128 ? (mid_nz_ == 2 ? (const void*)k_mid_pipe2<128, 2> : (const void*)k_mid_pipe2<128, 1>)
+                                  : (mid_nz_ == 2 ? (const void*)k_mid_pipe2<256, 2> : (const void*)k_mid_pipe2<256, 1>);
+    if (cudaFuncSetAttribute(f2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mid2_smem(Ns[0])) != cudaSuccess) {
+      cudaGetLastError();
+      mid2_ = false;
+    }
+  }
   const size_t smem = mid_pipe_smem((int)grp.size(), kv_total_, mid_tab_ ? Ns[0] * nch * n : 0);
   if (smem > 227 * 1024) return;
   if (!encode_rows(&tm_sf_, Sf_, 2 * I, (long long)n * Ns[0], Ns[0]) || !encode_sc_map()) return;
@@ -2497,6 +2659,34 @@ cudaError_t SpectralPlan::build_mid_tables(const std::vector<ChanEntry>& grp, co
       }
     }
   }
+  // the groups on axis 0 alone, for k_mid_pipe2: beta_g(z) and i^q A_g[c][s]
+  const int NZ = std::max(1, mid_nz_);
+  std::vector<double> bz((size_t)NZ * L0, 0.0);
+  std::vector<double2> rz((size_t)NZ * G * n, make_double2(0.0, 0.0));
+  int gz = 0;
+  for (size_t g = 0; g < grp.size() && gz < NZ; ++g) {
+    const ChanEntry& en = grp[g];
+    const int na0 = (en.nax >= 1 && en.ax0 == 0) + (en.nax >= 2 && en.ax1 == 0);
+    if (!(na0 > 0 && na0 == en.nax)) continue;
+    for (int z = 0; z < L0; ++z) {
+      const double ap = en.nax == 1 ? kp(0, z) : kp(0, z) * kp(0, z);
+      const double am = en.nax == 1 ? km(0, z) : km(0, z) * km(0, z);
+      const double sgn = (en.nax & 1) ? -1.0 : 1.0;
+      bz[(size_t)gz * L0 + z] = en.part == 0 ? 0.5 * (ap + sgn * am) : 0.5 * (ap - sgn * am);
+    }
+    const int q = (en.part == 0 ? en.nax : en.nax + 3) & 3;
+    for (int c = 0; c < G; ++c)
+      for (int s2 = 0; s2 < n; ++s2) {
+        const double v = A[g * 16 + c * 4 + s2];
+        rz[((size_t)gz * G + c) * n + s2] = q == 0 ? make_double2(v, 0.0) : q == 1 ? make_double2(0.0, v)
+                                           : q == 2 ? make_double2(-v, 0.0) : make_double2(0.0, -v);
+      }
+    ++gz;
+  }
+  if (!mid_bz_) RDCU_TRY(dev_alloc(&mid_bz_, bz.size() * sizeof(double)));
+  if (!mid_rz_) RDCU_TRY(dev_alloc(&mid_rz_, rz.size() * sizeof(double2)));
+  RDCU_TRY(cudaMemcpy(mid_bz_, bz.data(), bz.size() * sizeof(double), cudaMemcpyHostToDevice));
+  RDCU_TRY(cudaMemcpy(mid_rz_, rz.data(), rz.size() * sizeof(double2), cudaMemcpyHostToDevice));
   if (!mid_mz_) RDCU_TRY(dev_alloc(&mid_mz_, mz.size() * sizeof(double2)));
   if (!mid_mc_) RDCU_TRY(dev_alloc(&mid_mc_, mc.size() * sizeof(double2)));
   RDCU_TRY(cudaMemcpy(mid_mz_, mz.data(), mz.size() * sizeof(double2), cudaMemcpyHostToDevice));
@@ -2567,6 +2757,24 @@ cudaError_t SpectralPlan::launch_mid_pipe(const RhsIO& io, cudaStream_t st) {
   a.err = pipe_err_;
   a.Mz = mid_mz_;
   a.Mc = mid_mc_;
+  a.Bz = mid_bz_;
+  a.Rz = mid_rz_;
+  if (mid2_) {
+    const size_t sm2 = mid2_smem(Ns[0]);
+    const int grid2 = std::max(1, std::min(a.ntiles, sms_));
+    if (Ns[0] == 128) {
+      if (mid_nz_ == 2)
+        k_mid_pipe2<128, 2><<<grid2, kMid2Threads, sm2, st>>>(tm_sf_, tm_sc_, a);
+      else
+        k_mid_pipe2<128, 1><<<grid2, kMid2Threads, sm2, st>>>(tm_sf_, tm_sc_, a);
+    } else {
+      if (mid_nz_ == 2)
+        k_mid_pipe2<256, 2><<<grid2, kMid2Threads, sm2, st>>>(tm_sf_, tm_sc_, a);
+      else
+        k_mid_pipe2<256, 1><<<grid2, kMid2Threads, sm2, st>>>(tm_sf_, tm_sc_, a);
+    }
+    return cudaGetLastError();
+  }
   const size_t smem = mid_pipe_smem(mid_ngrp_, kv_total_, mid_tab_ ? Ns[0] * nch * n : 0);
   if (Ns[0] == 128) {
     if (mid_tab_)
@@ -2625,7 +2833,7 @@ void SpectralPlan::release() {
   ch_sorted_ = nullptr;
   void* ptrs[] = {tw_x_, tw_ax_[0], tw_ax_[1], tw_ax_[2], kv_, ch_off_, ch_ent_, d_terms_, d_fac_, d_poly_,
                   d_field_begin_, d_fold_, ych_off_, ych_ent_, ych_dst_, Sf_, Sc_, lin_ent_, sinv_, cosv_,
-                  mid_grp_, mid_A_, pipe_err_, mid_mz_, mid_mc_};
+                  mid_grp_, mid_A_, pipe_err_, mid_mz_, mid_mc_, mid_bz_, mid_rz_};
   if (!arena_)  // arena memory belongs to the caller
     for (void* p : ptrs)
       if (p) cudaFree(p);
@@ -2651,6 +2859,9 @@ void SpectralPlan::release() {
   mid_A_ = nullptr;
   mid_mz_ = nullptr;
   mid_mc_ = nullptr;
+  mid_bz_ = nullptr;
+  mid_rz_ = nullptr;
+  mid2_ = false;
   pipe_err_ = nullptr;
   pipe_mid_ = pipe_c2c_ = inv_row_ = false;
   nlin_ = 0;

@@ -163,6 +163,10 @@ class SpectralPlan {
   bool mid_tab_ = false;           // multiplier tables (no group mixes axis 0 with another axis)
   double2* mid_mz_ = nullptr;      // [L0][nch][n]
   double2* mid_mc_ = nullptr;      // [N1 * Mh][nch][n]
+  bool mid2_ = false;              // k_mid_pipe2: at most two groups on axis 0 alone
+  int mid_nz_ = 0;                 // their number
+  double* mid_bz_ = nullptr;       // [max(1, mid_nz_)][L0] beta_g(z)
+  double2* mid_rz_ = nullptr;      // [max(1, mid_nz_)][nch][n] i^q A_g
   std::vector<double> h_kv_;       // host copy of the wavenumbers
   cudaError_t build_mid_tables(const std::vector<ChanEntry>& grp, const std::vector<double>& A);
   int* pipe_err_ = nullptr;

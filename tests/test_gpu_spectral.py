@@ -201,6 +201,9 @@ def _tile_terms(kind):
         return 2, cgle_terms(3)
     if kind == "one_field":  # n = 1: one folded linear channel
         return 1, [parse_term(s) for s in ["1.0,0,0,1", "0.5,0,4,1", "0.7,0,8,1", "0.3,0,12,1", "-1.0,0,0,3"]]
+    if kind == "axis0_pair":  # n = 2: d_0 and d_0 d_0 both in the channels (two axis-0 groups)
+        return 2, [parse_term(s) for s in ["1.0,0,0,1", "0.4,0,2,1", "0.6,0,8,1", "-0.5,1,3,1", "0.3,1,9,1",
+                                           "0.2,1,16,1", "-1.0,0,0,3", "0.5,1,0,1,1,2"]]
     # n = 2: a folded channel for field 0 and the derivative d_1 u0 inside a product
     # (two channels), constant and power-0 factors
     return 2, [parse_term(s) for s in ["1.0,0,0,1", "0.4,0,14,1", "-0.6,0,22,1", "0.8,1,4,1,1,1", "-0.3,1,1,3",
@@ -210,7 +213,8 @@ def _tile_terms(kind):
 @pytest.mark.parametrize("Ns,kind", [((256, 6, 10), "cgle"), ((128, 12, 8), "cgle"), ((256, 4, 6), "one_field"),
                                      ((128, 7, 9), "mixed"), ((128, 3, 5), "cgle"), ((256, 5, 7), "mixed"),
                                      ((6, 256, 10), "cgle"), ((5, 128, 7), "cgle"), ((4, 6, 256), "cgle"),
-                                     ((6, 5, 128), "one_field"), ((128, 128, 8), "cgle"), ((8, 128, 256), "cgle")])
+                                     ((6, 5, 128), "one_field"), ((128, 128, 8), "cgle"), ((8, 128, 256), "cgle"),
+                                     ((256, 6, 8), "axis0_pair"), ((128, 5, 6), "axis0_pair")])
 def test_tiled_passes_3d(cuda, Ns, kind):
     rng = np.random.default_rng(sum(Ns))
     n, terms = _tile_terms(kind)
