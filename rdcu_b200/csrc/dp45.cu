@@ -121,6 +121,10 @@ bool DP45Engine::init(SpectralPlan* sp, double atol, double rtol, int fixed, cud
   device_bytes += sb;
   const int np = std::max(1, sp->nparts_max);
   if (cudaMalloc((void**)&err_part_, np * sizeof(double)) != cudaSuccess) return fail("error partials");
+  if (!fixed && sp->wants_err_aux()) {
+    if (cudaMalloc((void**)&err_aux_, 2 * sb) != cudaSuccess) return fail("error terms");
+    device_bytes += 2 * sb;
+  }
   if (cudaMalloc((void**)&d_ctl_, sizeof(DP45Ctl)) != cudaSuccess) return fail("controller");
   if (cudaMalloc((void**)&log_h_, log_cap_ * sizeof(double)) != cudaSuccess) return fail("log");
   if (cudaMalloc((void**)&log_acc_, log_cap_ * sizeof(int)) != cudaSuccess) return fail("log");
@@ -163,7 +167,7 @@ void DP45Engine::release() {
     if (p) cudaFree(p);
     p = nullptr;
   }
-  void* d[] = {y_eval, err_part_, d_ctl_, log_h_, log_acc_, log_t_, d_teval_};
+  void* d[] = {y_eval, err_part_, d_ctl_, log_h_, log_acc_, log_t_, d_teval_, err_aux_};
   for (void* p : d)
     if (p) cudaFree(p);
   void* hp[] = {h_ctl_pinned_, h_log_h_, h_log_acc_, h_log_t_};
@@ -171,6 +175,7 @@ void DP45Engine::release() {
     if (p) cudaFreeHost(p);
   y_eval = nullptr;
   err_part_ = nullptr;
+  err_aux_ = nullptr;
   d_ctl_ = nullptr;
   log_h_ = nullptr;
   log_acc_ = nullptr;
@@ -271,6 +276,7 @@ cudaError_t DP45Engine::launch_attempt_capture(double* const* ytemp_out) {
     io.bufs = bufs;
     io.ctl = d_ctl_;
     io.err_part = (s == 7 && !fixed_) ? err_part_ : nullptr;
+    io.err_aux = (s == 7 && !fixed_) ? err_aux_ : nullptr;
     if (ytemp_out && s <= 6) io.ytemp_out = ytemp_out[s];
     RDCU_TRY(sp_->run(io, st_));
   }
@@ -373,6 +379,7 @@ cudaError_t DP45Engine::profile(int reps, std::vector<SpectralPlan::PassTime>* o
   std::vector<SpectralPlan::PassTime> p7;
   io.stage = 7;
   io.err_part = fixed_ ? nullptr : err_part_;
+  io.err_aux = fixed_ ? nullptr : err_aux_;
   RDCU_TRY(sp_->profile(io, reps, st_, &p7));
   for (const auto& p : p7) {
     if (std::string(p.name) == "fwd_x") out->push_back({"fwd_x_stage7", p.ms, p.bytes});

@@ -95,6 +95,7 @@ class DP45Engine {
   cudaGraphExec_t graph_exec_ = nullptr;
   cudaGraph_t graph_ = nullptr;
   int graph_gen_ = -1;  // the plan's buffers_gen when the attempt graph was captured
+  double* err_aux_ = nullptr;  // stage-7 error terms (2 * nN doubles) when the plan wants them
   cudaError_t ensure_graph();
 };
 

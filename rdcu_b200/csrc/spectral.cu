@@ -65,6 +65,8 @@ struct Resolved {
   const double* k[7] = {};
   double h = 0, atol = 0, rtol = 0;
   int stage = 0;
+  double* aux = nullptr;       // stage 7: the error terms fwd_x writes (RhsIO::err_aux)
+  long long nN = 0;            // its half length (set by the pass that uses it)
 };
 
 __device__ __forceinline__ Resolved resolve(const RhsIO& io) {
@@ -91,8 +93,17 @@ __device__ __forceinline__ Resolved resolve(const RhsIO& io) {
     r.ytemp = io.ytemp_out ? io.ytemp_out : io.bufs.ybuf[c->yn_slot];
     r.u = r.ytemp;
     r.f = (io.stage == 7) ? io.bufs.kbuf[c->k7_buf] : io.bufs.kbuf[io.stage - 1];
+    if (io.stage == 7) r.aux = io.err_aux;
   }
   return r;
+}
+
+// Stage 7's error terms at point i from y, the slopes and the new state ynew, in
+// k_inv_x's operation order: the slope sum without e_7 k_7 (e_2 = 0) and the scale.
+__device__ __forceinline__ void stage7_error_terms(long long i, double ynew, const Resolved& r, double* es_p,
+                                                   double* den) {
+  *es_p = c_e[0] * r.k[0][i] + c_e[2] * r.k[2][i] + c_e[3] * r.k[3][i] + c_e[4] * r.k[4][i] + c_e[5] * r.k[5][i];
+  *den = r.atol + r.rtol * fmax(fabs(r.y[i]), fabs(ynew));
 }
 
 // Stage states follow the reference kernels' arithmetic order (dp45.cu:34-69): stage 2
@@ -285,6 +296,12 @@ __device__ __forceinline__ void fwd_load(const FwdXArgs& a, const Resolved& r, d
       const int e = e0 + u * T;
       if (e >= nel) break;
       if (r.ytemp && gi[u] >= 0) r.ytemp[gi[u]] = v[u];
+      if (S == 7 && r.aux && gi[u] >= 0) {
+        double es_p, den;
+        stage7_error_terms(gi[u], v[u], r, &es_p, &den);
+        r.aux[gi[u]] = es_p;
+        r.aux[r.nN + gi[u]] = den;
+      }
       if (a.do_fft) {
         const int pl = fdivc<2 * LX>(e, a.d2M);
         const int w = e - pl * 2 * M;
@@ -356,6 +373,13 @@ __device__ __forceinline__ void fwd_load2(const FwdXArgs& a, const Resolved& r, 
       const int e = e0 + u * T;
       if (e >= npair) break;
       if (r.ytemp && gi[u] >= 0) *reinterpret_cast<double2*>(r.ytemp + gi[u]) = v[u];
+      if (S == 7 && r.aux && gi[u] >= 0) {
+        double2 es_p, den;
+        stage7_error_terms(gi[u], v[u].x, r, &es_p.x, &den.x);
+        stage7_error_terms(gi[u] + 1, v[u].y, r, &es_p.y, &den.y);
+        *reinterpret_cast<double2*>(r.aux + gi[u]) = es_p;
+        *reinterpret_cast<double2*>(r.aux + r.nN + gi[u]) = den;
+      }
       if (a.do_fft) {
         const int pl = (unsigned)e / LX;
         const int w = e - pl * LX;
@@ -375,7 +399,8 @@ template <int RS, int LX>
 __device__ __forceinline__ void fwd_x_body(const FwdXArgs& a, int bx) {
   extern __shared__ double2 sm[];
   if (a.io.mode == 1 && !a.io.ctl->running) return;
-  const Resolved r = resolve(a.io);
+  Resolved r = resolve(a.io);
+  r.nN = (long long)a.nrows * (LX ? LX : a.M);
   const int M = LX ? LX : a.M, T = blockDim.x, tid = threadIdx.x;
   const double2* tw = a.tw;
   double2* buf = sm;
@@ -1646,24 +1671,27 @@ struct InvRowArgs {
   DictTable dict;
   RhsIO io;
 };
-constexpr int kRowThreads = 256;
-constexpr int kRowWarps = kRowThreads / 32;
-// one staging slot of a warp: 2 channels x (at most 129 + padding) spectral values and
-// NF x 256 field values (two rows of 128 points take the same room)
+// Warps per CTA: 8, or 5 with the stage-7 error epilogue (its staging slots also hold
+// the row's error terms).
+__host__ __device__ constexpr int row_warps(bool err) { return err ? 5 : 8; }
+// one staging slot of a warp: 2 channels x (at most 129 + padding) spectral values,
+// NF x 256 field values and, with the error epilogue, 2 x NF x 256 error terms (two
+// rows of 128 points take the same room)
 constexpr int kRowSpec = 2 * 136;  // double2 per slot
-__host__ __device__ constexpr int row_slot_doubles(int nf) { return 2 * kRowSpec + nf * 256; }
+__host__ __device__ constexpr int row_slot_doubles(int nf, bool err) { return 2 * kRowSpec + nf * 256 * (err ? 3 : 1); }
 
-__host__ __device__ constexpr size_t inv_row_smem(int n, int count) {
-  return (size_t)kRowWarps * (256 * 16 + 2 * (size_t)row_slot_doubles(n) * 8) + (size_t)n * count * 8 + 64;
+__host__ __device__ constexpr size_t inv_row_smem(int n, int count, bool err) {
+  return (size_t)row_warps(err) * (256 * 16 + 2 * (size_t)row_slot_doubles(n, err) * 8) + (size_t)n * count * 8 + 64;
 }
 
-template <int L, int NF>
-__global__ void __launch_bounds__(kRowThreads, 1) k_inv_row(InvRowArgs a) {
+template <int L, int NF, bool ERR>
+__global__ void __launch_bounds__(row_warps(ERR) * 32, 1) k_inv_row(InvRowArgs a) {
   extern __shared__ double2 sm[];
   if (a.io.mode == 1 && !a.io.ctl->running) return;
   using MN = Mono<NF>;
+  constexpr int kRowWarps = row_warps(ERR), kRowThreads = kRowWarps * 32;
   constexpr int LPL = L / 8, RPW = 32 / LPL;  // lanes per row, rows per warp
-  constexpr int SLOT = row_slot_doubles(NF);
+  constexpr int SLOT = row_slot_doubles(NF, ERR);
   const Resolved r = resolve(a.io);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   double* stage = reinterpret_cast<double*>(sm + kRowWarps * 256);
@@ -1678,12 +1706,16 @@ __global__ void __launch_bounds__(kRowThreads, 1) k_inv_row(InvRowArgs a) {
   wl.init(a.tw, ml);
   const long long RL = (long long)a.R * L;
   // the row's spectra (both channels) and fields as 16-byte pieces, when aligned
-  const bool a16 = ((reinterpret_cast<unsigned long long>(r.u) | reinterpret_cast<unsigned long long>(a.Sc)) & 15) == 0;
+  const bool a16 = ((reinterpret_cast<unsigned long long>(r.u) | reinterpret_cast<unsigned long long>(a.Sc) |
+                     (ERR ? reinterpret_cast<unsigned long long>(r.aux) : 0ull)) & 15) == 0;
   const int Mh = a.Mh, nch = a.nch;
   const long long wstride = (long long)gridDim.x * kRowWarps * RPW;
   // slot k of this warp; the sub-row's part of it
   auto slot_spec = [&](int k) { return reinterpret_cast<double2*>(stage + (warp * 2 + k) * SLOT) + sub * (kRowSpec / RPW); };
   auto slot_u = [&](int k) { return stage + (warp * 2 + k) * SLOT + 2 * kRowSpec + sub * NF * L; };
+  // ERR: the row's error terms (slope part, then scale) after the fields of both rows
+  auto slot_e = [&](int k) { return stage + (warp * 2 + k) * SLOT + 2 * kRowSpec + NF * 256 + sub * 2 * NF * L; };
+  const long long nN = (long long)NF * RL;
   auto fetch = [&](long long row, int k) {
     if (row >= a.R) return;
     double2* sp = slot_spec(k);
@@ -1698,11 +1730,27 @@ __global__ void __launch_bounds__(kRowThreads, 1) k_inv_row(InvRowArgs a) {
           const int x2 = 2 * (ml + LPL * k2);
           cp_async16(su + f * L + x2, r.u + f * RL + row * L + x2, true);
         }
+      if (ERR) {
+        double* se = slot_e(k);
+#pragma unroll
+        for (int q = 0; q < 2 * NF; ++q)
+#pragma unroll
+          for (int k2 = 0; k2 < L / 2 / LPL; ++k2) {
+            const int x2 = 2 * (ml + LPL * k2);
+            cp_async16(se + q * L + x2, r.aux + (q >= NF ? nN : 0) + (q % NF) * RL + row * L + x2, true);
+          }
+      }
     } else {
       for (int c = 0; c < nch; ++c)
         for (int e = ml; e < Mh; e += LPL) sp[c * Mh + e] = a.Sc[((long long)c * a.R + row) * Mh + e];
       for (int f = 0; f < NF; ++f)
         for (int k2 = 0; k2 < 8; ++k2) su[f * L + ml + LPL * k2] = r.u[f * RL + row * L + ml + LPL * k2];
+      if (ERR) {
+        double* se = slot_e(k);
+        for (int q = 0; q < 2 * NF; ++q)
+          for (int k2 = 0; k2 < 8; ++k2)
+            se[q * L + ml + LPL * k2] = r.aux[(q >= NF ? nN : 0) + (q % NF) * RL + row * L + ml + LPL * k2];
+      }
     }
   };
   long long row0 = ((long long)blockIdx.x * kRowWarps + warp) * RPW;
@@ -1720,6 +1768,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) k_inv_row(InvRowArgs a) {
     __syncwarp();  // this row's copies (every lane's) landed
     const double2* sp = slot_spec(k);
     const double* su = slot_u(k);
+    const double* se = slot_e(k);
     double2 v[8];
 #pragma unroll
     for (int p = 0; p < 8; ++p) {
@@ -1745,6 +1794,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) k_inv_row(InvRowArgs a) {
     // passed), so the point loop holds no spectral registers
 #pragma unroll
     for (int p = 0; p < 8; ++p) line[ml + LPL * p] = v[p];
+    double es_even = 0.0, es_odd = 0.0;  // ERR, 128 points: the partials of lanes ml and ml + 16
 #pragma unroll 2
     for (int p = 0; p < 8; ++p) {
       const int x = ml + LPL * p;
@@ -1756,6 +1806,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) k_inv_row(InvRowArgs a) {
       mono[0] = 1.0;
 #pragma unroll
       for (int m = 1; m < MN::count; ++m) mono[m] = mono[MN::parent(m)] * u[MN::var(m)];
+      double err2 = 0.0;
 #pragma unroll
       for (int i = 0; i < NF; ++i) {
         const int fc = sfold[i];
@@ -1764,7 +1815,26 @@ __global__ void __launch_bounds__(kRowThreads, 1) k_inv_row(InvRowArgs a) {
 #pragma unroll
         for (int m = 0; m < MN::count; ++m) acc += ci[m] * mono[m];
         if (live) r.f[i * RL + row * L + x] = acc;
+        if (ERR) {
+          // k_inv_x's error kernel (dp45.cu:79-84) from the forward pass's terms
+          const double es = se[i * L + x] + c_e[6] * acc;
+          const double ev = r.h * es / se[(NF + i) * L + x];
+          err2 += ev * ev;
+        }
       }
+      if (L == 256 || (p & 1) == 0)
+        es_even += err2;
+      else
+        es_odd += err2;
+    }
+    if (ERR) {
+      // one partial per row in k_inv_x's order: x = lane, lane + 32, ..., then the
+      // butterfly over the lanes (for 128 points its first step pairs lanes ml, ml + 16)
+      double sacc = es_even;
+      if (L == 128) sacc = es_even + es_odd;
+#pragma unroll
+      for (int o = LPL / 2; o > 0; o >>= 1) sacc += __shfl_xor_sync(0xffffffffu, sacc, o);
+      if (ml == 0 && live) a.io.err_part[row] = sacc;
     }
     __syncwarp();  // the next row's transform and the copies after it rewrite the line and this slot
   }
@@ -2523,20 +2593,27 @@ void SpectralPlan::setup_pipes() {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   sms_ = std::max(1, sms);
-  if ((M == 128 || M == 256) && poly_nf_ == n && n >= 1 && n <= 3 && nch >= 1 && nch <= 2) {
-    const size_t smem = inv_row_smem(n, poly_count_);
+  if ((M == 128 || M == 256) && poly_nf_ == n && n >= 1 && n <= 3 && nch >= 1 && nch <= 2 &&
+      inv_row_smem(n, poly_count_, true) <= 227 * 1024) {
     bool ok = true;
-    auto attr = [&](const void* fn) {
-      ok &= cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess;
+    auto attr = [&](const void* fn, bool err) {
+      ok &= cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)inv_row_smem(n, poly_count_, err)) == cudaSuccess;
     };
+    auto both = [&](auto lx, auto nf) {
+      constexpr int LX = decltype(lx)::value, NF = decltype(nf)::value;
+      attr((const void*)k_inv_row<LX, NF, false>, false);
+      attr((const void*)k_inv_row<LX, NF, true>, true);
+    };
+    using I1 = std::integral_constant<int, 1>;
+    using I2 = std::integral_constant<int, 2>;
+    using I3 = std::integral_constant<int, 3>;
     if (M == 128) {
-      attr((const void*)k_inv_row<128, 1>);
-      attr((const void*)k_inv_row<128, 2>);
-      attr((const void*)k_inv_row<128, 3>);
+      using L = std::integral_constant<int, 128>;
+      n == 1 ? both(L{}, I1{}) : n == 2 ? both(L{}, I2{}) : both(L{}, I3{});
     } else {
-      attr((const void*)k_inv_row<256, 1>);
-      attr((const void*)k_inv_row<256, 2>);
-      attr((const void*)k_inv_row<256, 3>);
+      using L = std::integral_constant<int, 256>;
+      n == 1 ? both(L{}, I1{}) : n == 2 ? both(L{}, I2{}) : both(L{}, I3{});
     }
     cudaGetLastError();
     inv_row_ = ok;
@@ -2718,15 +2795,25 @@ cudaError_t SpectralPlan::launch_inv_row(const RhsIO& io, cudaStream_t st) {
   a.Sc = Sc_;
   a.dict = dict_table();
   a.io = io;
-  const size_t smem = inv_row_smem(n, poly_count_);
-  const int rows_per_cta = kRowWarps * (32 / (M / 8));
+  const bool err = io.mode == 1 && io.stage == 7 && io.err_part != nullptr && io.err_aux != nullptr;
+  const size_t smem = inv_row_smem(n, poly_count_, err);
+  const int rows_per_cta = row_warps(err) * (32 / (M / 8));
   const int grid = std::max(1, std::min((R + rows_per_cta - 1) / rows_per_cta, sms_));  // one resident CTA per SM
+  const int threads = row_warps(err) * 32;
   auto go = [&](auto lx) {
     constexpr int LX = decltype(lx)::value;
-    switch (n) {
-      case 1: k_inv_row<LX, 1><<<grid, kRowThreads, smem, st>>>(a); break;
-      case 2: k_inv_row<LX, 2><<<grid, kRowThreads, smem, st>>>(a); break;
-      default: k_inv_row<LX, 3><<<grid, kRowThreads, smem, st>>>(a); break;
+    if (err) {
+      switch (n) {
+        case 1: k_inv_row<LX, 1, true><<<grid, threads, smem, st>>>(a); break;
+        case 2: k_inv_row<LX, 2, true><<<grid, threads, smem, st>>>(a); break;
+        default: k_inv_row<LX, 3, true><<<grid, threads, smem, st>>>(a); break;
+      }
+    } else {
+      switch (n) {
+        case 1: k_inv_row<LX, 1, false><<<grid, threads, smem, st>>>(a); break;
+        case 2: k_inv_row<LX, 2, false><<<grid, threads, smem, st>>>(a); break;
+        default: k_inv_row<LX, 3, false><<<grid, threads, smem, st>>>(a); break;
+      }
     }
   };
   if (M == 128)
@@ -2942,9 +3029,10 @@ cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, co
   // inverse x pass: the dictionary needs every channel of a row in one CTA; the Y.dat
   // output is launched one channel pair at a time
   const int step = Yout ? 2 : std::max(1, nch_run);
-  // the row kernel has no error epilogue: stage 7 of an adaptive step keeps k_inv_x
+  // stage 7 of an adaptive step: the row kernel's error epilogue reads the terms the
+  // forward pass left in err_aux; without them k_inv_x forms the error from y and slopes
   const bool err_epilogue = io.mode == 1 && io.stage == 7 && io.err_part != nullptr;
-  if (!Yout && inv_row_ && !err_epilogue && ct.ent == ch_ent_ && g_first == 0 && nch_run == nch)
+  if (!Yout && inv_row_ && (!err_epilogue || io.err_aux) && ct.ent == ch_ent_ && g_first == 0 && nch_run == nch)
     return launch_inv_row(io, st);
   for (int c0 = 0; c0 < std::max(1, nch_run); c0 += step) {
     const int cnt = spectral ? std::min(step, nch_run - c0) : 0;
@@ -3270,7 +3358,9 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
   fa.tw = tw_x_;
   fa.S = Sf_;
   fa.io = io;
-  RDCU_TRY(timed("fwd_x", n * ((1 + nk) * arr + (s >= 2 ? arr : 0) + spec_row), [&]() {
+  // stage 7 with err_aux also writes the two error terms
+  const double aux_w = (io.mode == 1 && io.stage == 7 && io.err_part && io.err_aux) ? 2.0 : 0.0;
+  RDCU_TRY(timed("fwd_x", n * ((1 + nk) * arr + (s >= 2 ? arr : 0) + spec_row + aux_w * arr), [&]() {
     prep(fa);
     by_length(plan_x_, fwd_.block, [&](auto rs, auto lx) { k_fwd_x<decltype(rs)::value, decltype(lx)::value><<<fwd_.grid, fwd_.block, fwd_.smem, st>>>(fa); });
     return cudaGetLastError();
@@ -3361,10 +3451,13 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
   inv_geometry(M, R, n, nch, false, plan_x_, &g, &tws, dict_smem_bytes());
   a.P = g.per_cta;
   a.tw_smem = tws;
-  // stage 7 of an adaptive step also reads y and five slopes for the error estimate
+  // stage 7 of an adaptive step also reads y and five slopes for the error estimate, or
+  // the two error terms the forward pass wrote (err_aux)
   const bool err_epilogue = io.mode == 1 && io.stage == 7 && io.err_part != nullptr;
-  RDCU_TRY(timed("inv_x_dictionary", nch * spec_row + 2.0 * n * arr + (err_epilogue ? 6.0 * n * arr : 0.0), [&]() {
-    if (inv_row_ && !(io.mode == 1 && io.stage == 7 && io.err_part != nullptr)) return launch_inv_row(io, st);
+  const double err_arrays = err_epilogue ? (io.err_aux ? 2.0 : 6.0) : 0.0;
+  RDCU_TRY(timed("inv_x_dictionary", nch * spec_row + 2.0 * n * arr + err_arrays * n * arr, [&]() {
+    if (inv_row_ && !(io.mode == 1 && io.stage == 7 && io.err_part != nullptr && !io.err_aux))
+      return launch_inv_row(io, st);
     prep(a);
     by_length(plan_x_, g.block, [&](auto rs, auto lx) { k_inv_x<decltype(rs)::value, decltype(lx)::value><<<g.grid, g.block, g.smem, st>>>(a); });
     return cudaGetLastError();

@@ -27,6 +27,11 @@ struct RhsIO {
   DP45Ctl* ctl = nullptr;     // mode 1
   double* err_part = nullptr; // mode 1, stage 7: per-CTA partial sums of err^2
   double* ytemp_out = nullptr;// mode 1, stages >= 2: write the stage state here instead of its slot
+  // mode 1, stage 7 of an adaptive step (plans with wants_err_aux()): 2 * nN doubles
+  // the forward pass fills with each point's error terms -- the slope part
+  // sum_{j != 2, 7} e_j k_j and the scale atol + rtol max(|y|, |y_new|) -- which the
+  // inverse pass completes with e_7 k_7 instead of reading y and five slopes again
+  double* err_aux = nullptr;
 };
 
 struct PassCfg {
@@ -94,6 +99,9 @@ class SpectralPlan {
   int nch = 0;                // channels of the hot RHS
   int nparts_max = 0;         // error partials buffer size needed (stage-7 epilogue)
   size_t device_bytes = 0;
+  // Whether stage 7 of an adaptive step should carry RhsIO::err_aux (the x pass one row
+  // per warp evaluates the error from it).
+  bool wants_err_aux() const { return inv_row_; }
   // Nonzero when a pass on TMA tiles gave up waiting for its copies (read and cleared).
   int take_pipe_error();
   // Incremented whenever a device buffer that launches capture is replaced (work
