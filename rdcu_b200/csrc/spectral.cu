@@ -339,6 +339,32 @@ __device__ __forceinline__ double2 stage_value_t2(long long i, const Resolved& r
   return make_double2(yi.x + r.h * ax, yi.y + r.h * ay);
 }
 
+// Stage 7 at the two points i, i+1 with the error terms from the same loads: the new
+// state (stage_value_t2<7>'s arithmetic) and stage7_error_terms' slope sum and scale.
+__device__ __forceinline__ double2 stage7_value_terms2(long long i, const Resolved& r, double2* es_p, double2* den) {
+  const double2 yi = *reinterpret_cast<const double2*>(r.y + i);
+  const double2 k0 = *reinterpret_cast<const double2*>(r.k[0] + i);
+  const double2 k2 = *reinterpret_cast<const double2*>(r.k[2] + i);
+  const double2 k3 = *reinterpret_cast<const double2*>(r.k[3] + i);
+  const double2 k4 = *reinterpret_cast<const double2*>(r.k[4] + i);
+  const double2 k5 = *reinterpret_cast<const double2*>(r.k[5] + i);
+  double ax = c_a[7][0] * k0.x, ay = c_a[7][0] * k0.y;
+  ax += c_a[7][2] * k2.x;
+  ay += c_a[7][2] * k2.y;
+  ax += c_a[7][3] * k3.x;
+  ay += c_a[7][3] * k3.y;
+  ax += c_a[7][4] * k4.x;
+  ay += c_a[7][4] * k4.y;
+  ax += c_a[7][5] * k5.x;
+  ay += c_a[7][5] * k5.y;
+  const double2 v = make_double2(yi.x + r.h * ax, yi.y + r.h * ay);
+  es_p->x = c_e[0] * k0.x + c_e[2] * k2.x + c_e[3] * k3.x + c_e[4] * k4.x + c_e[5] * k5.x;
+  es_p->y = c_e[0] * k0.y + c_e[2] * k2.y + c_e[3] * k3.y + c_e[4] * k4.y + c_e[5] * k5.y;
+  den->x = r.atol + r.rtol * fmax(fabs(yi.x), fabs(v.x));
+  den->y = r.atol + r.rtol * fmax(fabs(yi.y), fabs(v.y));
+  return v;
+}
+
 // fwd_load for a compile-time power-of-two row length: each thread moves pairs of
 // consecutive points (16-byte loads and stores of the state arrays).
 template <int S, int LX>
@@ -348,8 +374,9 @@ __device__ __forceinline__ void fwd_load2(const FwdXArgs& a, const Resolved& r, 
   constexpr int kUnroll = 4, H = LX / 2;
   const int T = blockDim.x, tid = threadIdx.x;
   const int npair = a.P * LX;  // P line pairs of two rows, LX/2 point pairs per row
+  const bool terms = S == 7 && r.aux != nullptr;
   for (int e0 = tid; e0 < npair; e0 += T * kUnroll) {
-    double2 v[kUnroll];
+    double2 v[kUnroll], tes[kUnroll], tden[kUnroll];
     long long gi[kUnroll];
 #pragma unroll
     for (int u = 0; u < kUnroll; ++u) {
@@ -364,7 +391,10 @@ __device__ __forceinline__ void fwd_load2(const FwdXArgs& a, const Resolved& r, 
         const long long g = row0 + 2 * pl + half;
         if (g < a.nrows) {
           gi[u] = g * LX + x;
-          v[u] = stage_value_t2<S>(gi[u], r);
+          if (terms)
+            v[u] = stage7_value_terms2(gi[u], r, &tes[u], &tden[u]);
+          else
+            v[u] = stage_value_t2<S>(gi[u], r);
         }
       }
     }
@@ -373,12 +403,9 @@ __device__ __forceinline__ void fwd_load2(const FwdXArgs& a, const Resolved& r, 
       const int e = e0 + u * T;
       if (e >= npair) break;
       if (r.ytemp && gi[u] >= 0) *reinterpret_cast<double2*>(r.ytemp + gi[u]) = v[u];
-      if (S == 7 && r.aux && gi[u] >= 0) {
-        double2 es_p, den;
-        stage7_error_terms(gi[u], v[u].x, r, &es_p.x, &den.x);
-        stage7_error_terms(gi[u] + 1, v[u].y, r, &es_p.y, &den.y);
-        *reinterpret_cast<double2*>(r.aux + gi[u]) = es_p;
-        *reinterpret_cast<double2*>(r.aux + r.nN + gi[u]) = den;
+      if (terms && gi[u] >= 0) {
+        *reinterpret_cast<double2*>(r.aux + gi[u]) = tes[u];
+        *reinterpret_cast<double2*>(r.aux + r.nN + gi[u]) = tden[u];
       }
       if (a.do_fft) {
         const int pl = (unsigned)e / LX;
