@@ -376,7 +376,7 @@ __device__ __forceinline__ void fwd_load2(const FwdXArgs& a, const Resolved& r, 
   const int npair = a.P * LX;  // P line pairs of two rows, LX/2 point pairs per row
   const bool terms = S == 7 && r.aux != nullptr;
   for (int e0 = tid; e0 < npair; e0 += T * kUnroll) {
-    double2 v[kUnroll], tes[kUnroll], tden[kUnroll];
+    double2 v[kUnroll];
     long long gi[kUnroll];
 #pragma unroll
     for (int u = 0; u < kUnroll; ++u) {
@@ -391,10 +391,15 @@ __device__ __forceinline__ void fwd_load2(const FwdXArgs& a, const Resolved& r, 
         const long long g = row0 + 2 * pl + half;
         if (g < a.nrows) {
           gi[u] = g * LX + x;
-          if (terms)
-            v[u] = stage7_value_terms2(gi[u], r, &tes[u], &tden[u]);
-          else
+          if (terms) {
+            // the error terms leave at once (no registers held across the unrolled loads)
+            double2 es_p, den;
+            v[u] = stage7_value_terms2(gi[u], r, &es_p, &den);
+            *reinterpret_cast<double2*>(r.aux + gi[u]) = es_p;
+            *reinterpret_cast<double2*>(r.aux + r.nN + gi[u]) = den;
+          } else {
             v[u] = stage_value_t2<S>(gi[u], r);
+          }
         }
       }
     }
@@ -403,10 +408,7 @@ __device__ __forceinline__ void fwd_load2(const FwdXArgs& a, const Resolved& r, 
       const int e = e0 + u * T;
       if (e >= npair) break;
       if (r.ytemp && gi[u] >= 0) *reinterpret_cast<double2*>(r.ytemp + gi[u]) = v[u];
-      if (terms && gi[u] >= 0) {
-        *reinterpret_cast<double2*>(r.aux + gi[u]) = tes[u];
-        *reinterpret_cast<double2*>(r.aux + r.nN + gi[u]) = tden[u];
-      }
+
       if (a.do_fft) {
         const int pl = (unsigned)e / LX;
         const int w = e - pl * LX;
