@@ -294,7 +294,8 @@ def run_ours(args, rank, world, local_rank):
                    "window_sim_time": [T_A, T_B], "tau_per_step": TAU,
                    "accepted_steps": acc, "attempts": att, "parallelism": "replicas" if world > 1 else "single",
                    "l2": "inputs > L2 (no flush needed)"},
-        "gpu_launches": launches_per_attempt(len(Ns)) * att * world,
+        # the passes of six stages and the controller, per attempt
+        "gpu_launches": (sum(weights) + 1) * att * world,
         "clocks": clk.summary(),
         "e2e": {"value": e2e_value, "unit": "grid-pt·steps/s", "h2d_bytes_per_step": nN * 8 / args.steps,
                 "d2h_bytes_per_step": 2 * nN * 8 / args.steps, "accepted_steps": acc2, "seconds": e2e_s},
@@ -904,18 +905,13 @@ def run_lines_reference(args):
 
 def launches_per_attempt_of(name):
     """Launches of a pass in one DP45 attempt (stages 2-7): the forward and inverse
-    row passes of stages 2-6 five times and their stage-7 forms once; the passes
-    between them (c2c, mid) six times."""
+    x passes of stages 2-6 five times and their stage-7 forms once; the passes between
+    them (axis 0, and axis 1 unless the x passes do it) six times."""
     if name.endswith("_stage7"):
         return 1
-    if name.startswith("fwd_x") or name.startswith("inv_x"):
+    if name.startswith("fwd_") or name.startswith("inv_"):
         return 5
     return 6
-
-
-def launches_per_attempt(ndim):
-    per_stage = {1: 3, 2: 3, 3: 5}[ndim]
-    return 6 * per_stage + 1
 
 
 def cpu_baseline(Ns, Ls, y, t, h):

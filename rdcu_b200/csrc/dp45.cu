@@ -382,8 +382,11 @@ cudaError_t DP45Engine::profile(int reps, std::vector<SpectralPlan::PassTime>* o
   io.err_aux = fixed_ ? nullptr : err_aux_;
   RDCU_TRY(sp_->profile(io, reps, st_, &p7));
   for (const auto& p : p7) {
-    if (std::string(p.name) == "fwd_x") out->push_back({"fwd_x_stage7", p.ms, p.bytes});
-    if (std::string(p.name) == "inv_x_dictionary") out->push_back({"inv_x_stage7", p.ms, p.bytes});
+    const std::string nm = p.name;
+    if (nm == "fwd_x") out->push_back({"fwd_x_stage7", p.ms, p.bytes});
+    if (nm == "inv_x_dictionary") out->push_back({"inv_x_stage7", p.ms, p.bytes});
+    if (nm == "fwd_plane") out->push_back({"fwd_plane_stage7", p.ms, p.bytes});
+    if (nm == "inv_plane") out->push_back({"inv_plane_stage7", p.ms, p.bytes});
   }
   // leave the controller idle, as after a completed attempt
   k_dp45_arm<<<1, 1, 0, st_>>>(d_ctl_, 0, INFINITY, 0.0, INFINITY, 0, 0, 1);

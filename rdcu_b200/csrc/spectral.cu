@@ -1870,6 +1870,359 @@ __global__ void __launch_bounds__(row_warps(ERR) * 32, 1) k_inv_row(InvRowArgs a
   cp_async_wait_all();
 }
 
+// ---- 3D x passes that also transform along axis 1, one thread-block cluster per plane
+// (an alternative to the axis-1 passes on TMA tiles, enabled by SpectralPlan::setup_planes
+// on request).  For 3D grids whose x rows and axis-1 lines have 128 or 256 points, the
+// forward x pass also does the forward axis-1 transform and the inverse x pass the
+// inverse one, so the
+// spectra of a stage cross HBM once each way between the x and axis-0 passes (the axis-1
+// passes on TMA tiles read and write them once more each).  A cluster of C = N1/32 CTAs
+// takes one axis-0 plane at a time (with one field, in the forward pass); CTA r of the
+// cluster holds the 32 rows y = r + C q (q < 32) of the plane.  The axis-1 DFT of length
+// N1 = 32 C splits as
+//     X[a + 32 b] = sum_r W_C^(r b) W_N1^(r a) sum_q W_32^(q a) x[r + C q]   (a < 32, b < C):
+// each CTA transforms its own rows over q -- a 32-point DFT per x wavenumber, as 8-point
+// DFTs over q2, the twiddles W_32^(q1 k2), then 4-point DFTs over q1 (q = q1 + 4 q2,
+// a = k2 + 8 k1) -- and applies W_N1^(r a); after a cluster barrier CTA j reads the
+// values of its a-range (a = j 32/C + i) from every CTA of the cluster through
+// distributed shared memory and finishes the C-point DFTs over r, writing the spectra
+// in the layout the axis-0 pass reads.  The inverse pass takes the same steps backwards.
+// The x transforms are the warp-per-line transforms of the row kernels (WarpLine),
+// bitwise those of the other x passes; the axis-1 transform uses the line kernels'
+// twiddle table in another factorisation, so it agrees with the tiled axis-1 pass to
+// rounding.  Control flow is uniform over a cluster: every CTA takes the same planes and
+// passes the same cluster barriers, and none leaves while another may read its shared
+// memory.
+
+__device__ __forceinline__ unsigned cl_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ unsigned cl_id() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ unsigned cl_count() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%nclusterid.x;" : "=r"(r));
+  return r;
+}
+// every thread of every CTA of the cluster arrives (release) and waits (acquire)
+__device__ __forceinline__ void cl_sync() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// the shared-memory address of p in CTA `rank` of the cluster
+__device__ __forceinline__ unsigned cl_map(const void* p, unsigned rank) {
+  unsigned d;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(d) : "r"(smem_u32(p)), "r"(rank));
+  return d;
+}
+__device__ __forceinline__ double2 cl_load(unsigned addr) {
+  double2 v;
+  asm volatile("ld.shared::cluster.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(addr) : "memory");
+  return v;
+}
+
+struct PlaneArgs {
+  int N0, n, nch;       // axis-0 planes, fields, inverse channels
+  const double2* twx;   // x twiddles (LX-point table)
+  const double2* twy;   // axis-1 twiddles (N1-point table)
+  double2* S;           // forward: field half spectra [field][z][ky][kx] (written)
+  const double2* Sc;    // inverse: channel half spectra [channel][z][ky][kx] (read)
+  DictTable dict;
+  RhsIO io;
+};
+
+constexpr int kPlaneFwdThreads = 512;
+constexpr int kPlaneInvThreads = 256;
+// forward: 16 complex lines of LX points, then 32 half-spectrum rows
+__host__ __device__ constexpr size_t plane_fwd_smem(int LX) { return (size_t)(16 * LX + 32 * (LX / 2 + 1)) * 16; }
+// inverse: the exchange block (32 half rows, later the warps' line buffers), two
+// channels' 32 half rows, the dictionary's polynomial and fold tables
+__host__ __device__ constexpr size_t plane_inv_smem(int LX, int nf, int count) {
+  return (size_t)(3 * 32 * (LX / 2 + 1)) * 16 + (size_t)nf * count * 8 + 64;
+}
+
+// Stage values of the CTA's 32 rows of one (plane, field): row q of the CTA is global
+// row grow0 + C q; rows 2l and 2l + 1 become the real and imaginary parts of line l.
+// The stage state (and stage 7's error terms) leave as fwd_load2 writes them.
+template <int S, int LX, int C>
+__device__ __forceinline__ void plane_load(const Resolved& r, double2* lines, long long grow0) {
+  constexpr int kUnroll = 4, H = LX / 2, NP = 32 * H;
+  static_assert(NP % (kPlaneFwdThreads * kUnroll) == 0, "whole unrolled rounds");
+  const bool terms = S == 7 && r.aux != nullptr;
+  for (int e0 = threadIdx.x; e0 < NP; e0 += kPlaneFwdThreads * kUnroll) {
+    double2 v[kUnroll];
+    long long gi[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const int e = e0 + u * kPlaneFwdThreads;
+      const int q = e / H, x = 2 * (e - q * H);
+      gi[u] = (grow0 + (long long)C * q) * LX + x;
+      if (terms) {
+        double2 es_p, den;
+        v[u] = stage7_value_terms2(gi[u], r, &es_p, &den);
+        *reinterpret_cast<double2*>(r.aux + gi[u]) = es_p;
+        *reinterpret_cast<double2*>(r.aux + r.nN + gi[u]) = den;
+      } else {
+        v[u] = stage_value_t2<S>(gi[u], r);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const int e = e0 + u * kPlaneFwdThreads;
+      const int q = e / H, x = 2 * (e - q * H);
+      if (r.ytemp) *reinterpret_cast<double2*>(r.ytemp + gi[u]) = v[u];
+      double* b = reinterpret_cast<double*>(lines) + 2 * ((q >> 1) * LX + x) + (q & 1);
+      b[0] = v[u].x;
+      b[2] = v[u].y;
+    }
+  }
+}
+
+template <int LX, int C>
+__global__ void __launch_bounds__(kPlaneFwdThreads, 1) k_fwd_plane(PlaneArgs a) {
+  extern __shared__ double2 smp[];
+  if (a.io.mode == 1 && !a.io.ctl->running) return;  // the same for every CTA
+  constexpr int Mh = LX / 2 + 1, N1 = 32 * C, LPL = LX / 8, AC = 32 / C, T = kPlaneFwdThreads;
+  double2* lines = smp;          // 16 lines of LX points
+  double2* rows = smp + 16 * LX;  // 32 half rows of Mh points; the axis-1 stages in place
+  Resolved r = resolve(a.io);
+  r.nN = (long long)a.n * a.N0 * N1 * LX;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const unsigned rank = cl_rank();
+  const int li = warp * (32 / LPL) + lane / LPL;  // the warp's line (two per warp for 128 points)
+  WarpLine<LX> wl;
+  wl.init(a.twx, lane % LPL);
+  const int nitems = a.N0 * a.n;
+  for (int it = (int)cl_id(); it < nitems; it += (int)cl_count()) {
+    const int f = it / a.N0, z = it - f * a.N0;
+    const long long grow0 = ((long long)f * a.N0 + z) * N1 + rank;
+    switch (r.stage) {
+      case 2: plane_load<2, LX, C>(r, lines, grow0); break;
+      case 3: plane_load<3, LX, C>(r, lines, grow0); break;
+      case 4: plane_load<4, LX, C>(r, lines, grow0); break;
+      case 5: plane_load<5, LX, C>(r, lines, grow0); break;
+      case 6: plane_load<6, LX, C>(r, lines, grow0); break;
+      case 7: plane_load<7, LX, C>(r, lines, grow0); break;
+      default: plane_load<1, LX, C>(r, lines, grow0); break;
+    }
+    __syncthreads();
+    if (li < 16) {
+      double2* line = lines + li * LX;
+      double2 v[8];
+#pragma unroll
+      for (int p = 0; p < 8; ++p) v[p] = line[wl.ml + LPL * p];
+      __syncwarp();
+      wl.template transform<false>(v, [line](int e) { return line + e; });
+#pragma unroll
+      for (int p = 0; p < 8; ++p) line[wl.ml + LPL * p] = v[p];
+    }
+    // the cluster has read the previous item's rows; this CTA's lines are complete
+    cl_sync();
+    // the two real rows of each line (fwd_x_body's separation)
+    for (int i = tid; i < 16 * Mh; i += T) {
+      const int l = i / Mh, kx = i - l * Mh;
+      const double2 zz = lines[l * LX + kx];
+      const double2 zm = lines[l * LX + (kx == 0 ? 0 : LX - kx)];
+      rows[(2 * l) * Mh + kx] = make_double2(0.5 * (zz.x + zm.x), 0.5 * (zz.y - zm.y));
+      rows[(2 * l + 1) * Mh + kx] = make_double2(0.5 * (zz.y + zm.y), -0.5 * (zz.x - zm.x));
+    }
+    __syncthreads();
+    // 8-point DFTs over q2, times W_32^(q1 k2), back to rows q1 + 4 k2
+    for (int i = tid; i < 4 * Mh; i += T) {
+      const int q1 = i / Mh, kx = i - q1 * Mh;
+      double2 v[8];
+#pragma unroll
+      for (int q2 = 0; q2 < 8; ++q2) v[q2] = rows[(q1 + 4 * q2) * Mh + kx];
+      Dft<8, false>::run(v, nullptr, 0);
+      if (q1 > 0) {
+#pragma unroll
+        for (int k2 = 1; k2 < 8; ++k2) v[k2] = c_mul(v[k2], a.twy[C * q1 * k2]);
+      }
+#pragma unroll
+      for (int k2 = 0; k2 < 8; ++k2) rows[(q1 + 4 * k2) * Mh + kx] = v[k2];
+    }
+    __syncthreads();
+    // 4-point DFTs over q1: Y[k2 + 8 k1] times W_N1^(r a), at row 4 k2 + k1
+    for (int i = tid; i < 8 * Mh; i += T) {
+      const int k2 = i / Mh, kx = i - k2 * Mh;
+      double2 w[4];
+#pragma unroll
+      for (int q1 = 0; q1 < 4; ++q1) w[q1] = rows[(q1 + 4 * k2) * Mh + kx];
+      Dft<4, false>::run(w, nullptr, 0);
+#pragma unroll
+      for (int k1 = 0; k1 < 4; ++k1) {
+        const int t = (int)rank * (k2 + 8 * k1);
+        rows[(4 * k2 + k1) * Mh + kx] = t ? c_mul(w[k1], a.twy[t]) : w[k1];
+      }
+    }
+    cl_sync();  // every CTA's values are visible to the cluster
+    // C-point DFTs over r for this CTA's a-range, to the spectra
+    for (int i = tid; i < AC * Mh; i += T) {
+      const int al = i / Mh, kx = i - al * Mh;
+      const int aa = (int)rank * AC + al;
+      const double2* src = rows + (4 * (aa & 7) + (aa >> 3)) * Mh + kx;
+      double2 v[C];
+#pragma unroll
+      for (int rr = 0; rr < C; ++rr) v[rr] = cl_load(cl_map(src, rr));
+      Dft<C, false>::run(v, nullptr, 0);
+      double2* dst = a.S + (((long long)f * a.N0 + z) * N1 + aa) * Mh + kx;
+#pragma unroll
+      for (int b = 0; b < C; ++b) dst[(long long)32 * b * Mh] = v[b];
+    }
+  }
+  cl_sync();
+}
+
+template <int LX, int C, int NF, bool ERR>
+__global__ void __launch_bounds__(kPlaneInvThreads, 1) k_inv_plane(PlaneArgs a) {
+  extern __shared__ double2 smp[];
+  if (a.io.mode == 1 && !a.io.ctl->running) return;  // the same for every CTA
+  using MN = Mono<NF>;
+  constexpr int Mh = LX / 2 + 1, N1 = 32 * C, LPL = LX / 8, RPW = 32 / LPL, AC = 32 / C, T = kPlaneInvThreads;
+  constexpr int NW = T / 32;
+  double2* zo = smp;              // [r][al] blocks of Mh values; later the warps' line buffers
+  double2* rows = smp + 32 * Mh;  // two channels' 32 half rows
+  double* spoly = reinterpret_cast<double*>(rows + 2 * 32 * Mh);
+  int* sfold = reinterpret_cast<int*>(spoly + NF * MN::count);
+  const Resolved r = resolve(a.io);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int t = tid; t < NF * MN::count; t += T) spoly[t] = a.dict.poly[t];
+  for (int t = tid; t < NF; t += T) sfold[t] = a.dict.fold[t];
+  const unsigned rank = cl_rank();
+  const int sub = lane / LPL, ml = lane % LPL;
+  WarpLine<LX> wl;
+  wl.init(a.twx, ml);
+  const long long RL = (long long)a.N0 * N1 * LX, nN = (long long)NF * RL;
+  const int nch = a.nch;
+  for (int z = (int)cl_id(); z < a.N0; z += (int)cl_count()) {
+    for (int c = 0; c < nch; ++c) {
+      // the cluster has read zo (previous channel); this CTA's line buffers are free
+      cl_sync();
+      // C-point inverse DFTs over b of this CTA's a-range, times conj W_N1^(r a), to zo[r][al]
+      for (int i = tid; i < AC * Mh; i += T) {
+        const int al = i / Mh, kx = i - al * Mh;
+        const int aa = (int)rank * AC + al;
+        const double2* src = a.Sc + (((long long)c * a.N0 + z) * N1 + aa) * Mh + kx;
+        double2 v[C];
+#pragma unroll
+        for (int b = 0; b < C; ++b) v[b] = src[(long long)32 * b * Mh];
+        Dft<C, true>::run(v, nullptr, 0);
+#pragma unroll
+        for (int rr = 0; rr < C; ++rr) {
+          const int t = rr * aa;
+          zo[(rr * AC + al) * Mh + kx] = t ? c_mul(v[rr], tw_get<true>(a.twy, t)) : v[rr];
+        }
+      }
+      cl_sync();  // every CTA's values are visible to the cluster
+      double2* rc = rows + c * 32 * Mh;
+      // 4-point inverse DFTs over k1 (a = k2 + 8 k1) of this CTA's values, times
+      // conj W_32^(k2 q1), at rows q1 + 4 k2
+      for (int i = tid; i < 8 * Mh; i += T) {
+        const int k2 = i / Mh, kx = i - k2 * Mh;
+        double2 w[4];
+#pragma unroll
+        for (int k1 = 0; k1 < 4; ++k1) {
+          const int aa = k2 + 8 * k1;
+          w[k1] = cl_load(cl_map(zo + ((int)rank * AC + aa % AC) * Mh + kx, aa / AC));
+        }
+        Dft<4, true>::run(w, nullptr, 0);
+#pragma unroll
+        for (int q1 = 0; q1 < 4; ++q1) {
+          const int t = C * k2 * q1;
+          rc[(q1 + 4 * k2) * Mh + kx] = t ? c_mul(w[q1], tw_get<true>(a.twy, t)) : w[q1];
+        }
+      }
+      __syncthreads();
+      // 8-point inverse DFTs over k2: row q1 + 4 q2
+      for (int i = tid; i < 4 * Mh; i += T) {
+        const int q1 = i / Mh, kx = i - q1 * Mh;
+        double2 v[8];
+#pragma unroll
+        for (int k2 = 0; k2 < 8; ++k2) v[k2] = rc[(q1 + 4 * k2) * Mh + kx];
+        Dft<8, true>::run(v, nullptr, 0);
+#pragma unroll
+        for (int q2 = 0; q2 < 8; ++q2) rc[(q1 + 4 * q2) * Mh + kx] = v[q2];
+      }
+    }
+    cl_sync();  // the cluster has read zo: it becomes the line buffers; every channel's rows are complete
+    // k_inv_row's per-row work on this CTA's rows
+    for (int q0 = warp * RPW; q0 < 32; q0 += NW * RPW) {
+      const int q = q0 + sub;
+      const long long row = (long long)z * N1 + rank + (long long)C * q;
+      double2* line = zo + (warp * RPW + sub) * LX;
+      double uu[8][NF];
+#pragma unroll
+      for (int p = 0; p < 8; ++p)
+#pragma unroll
+        for (int f = 0; f < NF; ++f) uu[p][f] = r.u[f * RL + row * LX + ml + LPL * p];
+      const double2* sa = rows + q * Mh;
+      const double2* sb = rows + 32 * Mh + q * Mh;
+      double2 v[8];
+#pragma unroll
+      for (int p = 0; p < 8; ++p) {
+        const int kx = ml + LPL * p;
+        const int kk = kx >= Mh ? LX - kx : kx;
+        double2 Av = sa[kk], Bv = nch > 1 ? sb[kk] : make_double2(0.0, 0.0);
+        if (kx == 0 || 2 * kx == LX) {
+          Av.y = 0.0;
+          Bv.y = 0.0;
+        }
+        if (kx >= Mh) {
+          Av.y = -Av.y;
+          Bv.y = -Bv.y;
+        }
+        v[p] = make_double2(Av.x - Bv.y, Av.y + Bv.x);
+      }
+      wl.template transform<true>(v, [line](int e) { return line + e; });
+      double es_even = 0.0, es_odd = 0.0;
+#pragma unroll
+      for (int p = 0; p < 8; ++p) {
+        const int x = ml + LPL * p;
+        const double2 zz = v[p];
+        double mono[MN::count];
+        mono[0] = 1.0;
+#pragma unroll
+        for (int m = 1; m < MN::count; ++m) mono[m] = mono[MN::parent(m)] * uu[p][MN::var(m)];
+        double err2 = 0.0;
+#pragma unroll
+        for (int i = 0; i < NF; ++i) {
+          const int fc = sfold[i];
+          double acc = fc >= 0 ? ((fc & 1) ? zz.y : zz.x) : 0.0;
+          const double* ci = spoly + i * MN::count;
+#pragma unroll
+          for (int m = 0; m < MN::count; ++m) acc += ci[m] * mono[m];
+          const long long gi = i * RL + row * LX + x;
+          r.f[gi] = acc;
+          if (ERR) {
+            // k_inv_x's error kernel (dp45.cu:79-84) from the forward pass's terms
+            const double es = r.aux[gi] + c_e[6] * acc;
+            const double ev = r.h * es / r.aux[nN + gi];
+            err2 += ev * ev;
+          }
+        }
+        if (LX == 256 || (p & 1) == 0)
+          es_even += err2;
+        else
+          es_odd += err2;
+      }
+      if (ERR) {
+        // one partial per row in k_inv_x's order (k_inv_row's butterfly)
+        double sacc = es_even;
+        if (LX == 128) sacc = es_even + es_odd;
+#pragma unroll
+        for (int o = LPL / 2; o > 0; o >>= 1) sacc += __shfl_xor_sync(0xffffffffu, sacc, o);
+        if (ml == 0) a.io.err_part[row] = sacc;
+      }
+      __syncwarp();  // the next row's transform rewrites the line
+    }
+  }
+  cl_sync();
+}
+
 // ---- batched passes: persistent CTAs over (problem, tile) work items
 template <typename A>
 __device__ __forceinline__ void load_args(A* dst, const A* src) {
@@ -2606,6 +2959,7 @@ bool SpectralPlan::init(int n_, int ndim_, const int* Ns_, const double* Ls_,
     return false;
   }
   setup_pipes();
+  setup_planes();
   built_ = true;
   return true;
 }
@@ -2930,6 +3284,142 @@ cudaError_t SpectralPlan::launch_c2c_pipe(bool inv, int nplanes, cudaStream_t st
   return cudaGetLastError();
 }
 
+// ---- 3D x passes that also transform along axis 1 (k_fwd_plane, k_inv_plane)
+namespace {
+
+using PlaneKernel = void (*)(PlaneArgs);
+
+PlaneKernel plane_fwd_kernel(int M, int C) {
+  if (M == 128) return C == 4 ? k_fwd_plane<128, 4> : k_fwd_plane<128, 8>;
+  return C == 4 ? k_fwd_plane<256, 4> : k_fwd_plane<256, 8>;
+}
+
+template <int LX, int C>
+PlaneKernel plane_inv_kernel_lc(int nf, bool err) {
+  if (nf == 1) return err ? k_inv_plane<LX, C, 1, true> : k_inv_plane<LX, C, 1, false>;
+  return err ? k_inv_plane<LX, C, 2, true> : k_inv_plane<LX, C, 2, false>;
+}
+
+PlaneKernel plane_inv_kernel(int M, int C, int nf, bool err) {
+  if (M == 128) return C == 4 ? plane_inv_kernel_lc<128, 4>(nf, err) : plane_inv_kernel_lc<128, 8>(nf, err);
+  return C == 4 ? plane_inv_kernel_lc<256, 4>(nf, err) : plane_inv_kernel_lc<256, 8>(nf, err);
+}
+
+cudaLaunchConfig_t cluster_config(int grid, int block, size_t smem, int C, cudaStream_t st, cudaLaunchAttribute* at) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid, 1, 1);
+  cfg.blockDim = dim3((unsigned)block, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = (unsigned)C;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cfg;
+}
+
+// Clusters of C CTAs of `kernel` that fit the GPU at once (0 when none does).
+int plane_clusters(PlaneKernel kernel, int block, size_t smem, int C) {
+  if (cudaFuncSetAttribute((const void*)kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  cudaLaunchAttribute at[1];
+  cudaLaunchConfig_t cfg = cluster_config(C, block, smem, C, nullptr, at);
+  int ncl = 0;
+  if (cudaOccupancyMaxActiveClusters(&ncl, (const void*)kernel, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return ncl;
+}
+
+}  // namespace
+
+// The fused axis-1 passes need 3D grids with 128- or 256-point x rows and axis-1 lines
+// (clusters of N1/32 CTAs), the tiled axis-0 pass between them, and for the inverse the
+// row kernel's dictionary form (a dense polynomial of at most two fields and two
+// inverse channels).  They are used only when RDCU_PLANE_PASSES=1 is set in the
+// environment at plan creation: on a B200 they are slower than the separate passes
+// (3D CGLE 256^3: 7.4 vs 5.4 ms per DP45 attempt) -- at most 15 clusters of 8 CTAs are
+// resident (120 of 148 SMs), and within a CTA the loads, the transforms and the
+// cluster exchanges of a plane follow one another (DRAM 26% busy in the forward pass,
+// 18% in the inverse), where the row and tile kernels overlap them.
+void SpectralPlan::setup_planes() {
+  plane_fwd_ = plane_inv_ = false;
+  if (ndim != 3 || !pipe_mid_ || nch < 1 || n > 3) return;
+  if (!(M == 128 || M == 256) || !(Ns[1] == 128 || Ns[1] == 256)) return;
+  const char* env = std::getenv("RDCU_PLANE_PASSES");
+  if (!env || std::strcmp(env, "1") != 0) return;
+  const int C = Ns[1] / 32;
+  const int nf = plane_clusters(plane_fwd_kernel(M, C), kPlaneFwdThreads, plane_fwd_smem(M), C);
+  if (nf > 0) {
+    plane_fwd_grid_ = C * std::min(nf, Ns[0] * n);
+    plane_fwd_ = true;
+  }
+  if (!inv_row_ || nch > 2 || n > 2) return;
+  const size_t ism = plane_inv_smem(M, n, poly_count_);
+  if (ism > 227 * 1024) return;
+  const int ni0 = plane_clusters(plane_inv_kernel(M, C, n, false), kPlaneInvThreads, ism, C);
+  const int ni1 = plane_clusters(plane_inv_kernel(M, C, n, true), kPlaneInvThreads, ism, C);
+  if (ni0 > 0 && ni1 > 0) {
+    plane_inv_grid_ = C * std::min(std::min(ni0, ni1), Ns[0]);
+    plane_inv_ = true;
+  }
+}
+
+// the forward pass reads the state with 16-byte loads: its arrays must be 16-byte aligned
+bool SpectralPlan::plane_fwd_ok(const RhsIO& io) const {
+  if (!plane_fwd_ || nch < 1) return false;
+  unsigned long long m = reinterpret_cast<unsigned long long>(io.ytemp_out);
+  if (io.mode == 0) m |= reinterpret_cast<unsigned long long>(io.y);
+  return (m & 15) == 0;
+}
+
+// the hot channel table in one launch; at stage 7 of an adaptive step with the forward
+// pass's error terms
+bool SpectralPlan::plane_inv_ok(const RhsIO& io) const {
+  if (!plane_inv_) return false;
+  const bool err_epilogue = io.mode == 1 && io.stage == 7 && io.err_part != nullptr;
+  return !err_epilogue || io.err_aux != nullptr;
+}
+
+cudaError_t SpectralPlan::launch_plane_fwd(const RhsIO& io, cudaStream_t st) {
+  PlaneArgs a{};
+  a.N0 = Ns[0];
+  a.n = n;
+  a.nch = nch;
+  a.twx = tw_x_;
+  a.twy = tw_ax_[1];
+  a.S = Sf_;
+  a.io = io;
+  const int C = Ns[1] / 32;
+  cudaLaunchAttribute at[1];
+  cudaLaunchConfig_t cfg = cluster_config(plane_fwd_grid_, kPlaneFwdThreads, plane_fwd_smem(M), C, st, at);
+  return cudaLaunchKernelEx(&cfg, plane_fwd_kernel(M, C), a);
+}
+
+cudaError_t SpectralPlan::launch_plane_inv(const RhsIO& io, cudaStream_t st) {
+  PlaneArgs a{};
+  a.N0 = Ns[0];
+  a.n = n;
+  a.nch = nch;
+  a.twx = tw_x_;
+  a.twy = tw_ax_[1];
+  a.Sc = Sc_;
+  a.dict = dict_table();
+  a.io = io;
+  const bool err = io.mode == 1 && io.stage == 7 && io.err_part != nullptr && io.err_aux != nullptr;
+  const int C = Ns[1] / 32;
+  cudaLaunchAttribute at[1];
+  cudaLaunchConfig_t cfg =
+      cluster_config(plane_inv_grid_, kPlaneInvThreads, plane_inv_smem(M, n, poly_count_), C, st, at);
+  return cudaLaunchKernelEx(&cfg, plane_inv_kernel(M, C, n, err), a);
+}
+
 cudaError_t SpectralPlan::ensure_channel_capacity(int rows) {
   if (rows <= sc_rows_) return cudaSuccess;
   const size_t srow = (size_t)R * Mh * sizeof(double2);
@@ -2990,6 +3480,8 @@ cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, co
                                         int nch_run, int g_first, double* Yout, const int* ydst, cudaStream_t st,
                                         int yplain) {
   const bool spectral = nch_run > 0;
+  // the inverse x pass with the axis-1 transform: the hot table, every channel, no Y.dat
+  const bool plane_inv = spectral && !Yout && ct.ent == ch_ent_ && g_first == 0 && nch_run == nch && plane_inv_ok(io);
   if (spectral && ndim >= 2) {
     const int which = (ct.ent == ch_ent_) ? 0 : 1;  // hot table or the Y-block table
     const PassCfg& c = mid_[which];
@@ -3024,7 +3516,7 @@ cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, co
       by_length(plan_ax_[0], c.block, [&](auto rs, auto lx) { k_mid<decltype(rs)::value, decltype(lx)::value><<<c.grid, c.block, smem, st>>>(m); });
       RDCU_TRY(cudaGetLastError());
     }
-    if (ndim == 3) {
+    if (ndim == 3 && !plane_inv) {
       C2CArgs a{};
       a.La = Ns[1];
       a.I = Mh;
@@ -3061,6 +3553,7 @@ cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, co
   // stage 7 of an adaptive step: the row kernel's error epilogue reads the terms the
   // forward pass left in err_aux; without them k_inv_x forms the error from y and slopes
   const bool err_epilogue = io.mode == 1 && io.stage == 7 && io.err_part != nullptr;
+  if (plane_inv) return launch_plane_inv(io, st);
   if (!Yout && inv_row_ && (!err_epilogue || io.err_aux) && ct.ent == ch_ent_ && g_first == 0 && nch_run == nch)
     return launch_inv_row(io, st);
   for (int c0 = 0; c0 < std::max(1, nch_run); c0 += step) {
@@ -3099,6 +3592,10 @@ cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, co
 cudaError_t SpectralPlan::run(const RhsIO& io, cudaStream_t st) {
   const bool spectral = nch > 0;
   const bool need_fwd = spectral || (io.mode == 1 && io.stage >= 2);
+  if (spectral && plane_fwd_ok(io)) {
+    RDCU_TRY(launch_plane_fwd(io, st));
+    return launch_passes(io, chan_table(ch_off_, ch_ent_, nch), h_ch_off_, nch, 0, nullptr, nullptr, st);
+  }
   if (need_fwd) {
     FwdXArgs a{};
     a.M = M;
@@ -3389,12 +3886,19 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
   fa.io = io;
   // stage 7 with err_aux also writes the two error terms
   const double aux_w = (io.mode == 1 && io.stage == 7 && io.err_part && io.err_aux) ? 2.0 : 0.0;
-  RDCU_TRY(timed("fwd_x", n * ((1 + nk) * arr + (s >= 2 ? arr : 0) + spec_row + aux_w * arr), [&]() {
-    prep(fa);
-    by_length(plan_x_, fwd_.block, [&](auto rs, auto lx) { k_fwd_x<decltype(rs)::value, decltype(lx)::value><<<fwd_.grid, fwd_.block, fwd_.smem, st>>>(fa); });
-    return cudaGetLastError();
-  }));
-  if (spectral && ndim == 3) {
+  const double fwd_bytes = n * ((1 + nk) * arr + (s >= 2 ? arr : 0) + spec_row + aux_w * arr);
+  const bool plane_fwd = spectral && plane_fwd_ok(io);
+  const bool plane_inv = spectral && plane_inv_ok(io);
+  if (plane_fwd) {
+    RDCU_TRY(timed("fwd_plane", fwd_bytes, [&]() { return launch_plane_fwd(io, st); }));
+  } else {
+    RDCU_TRY(timed("fwd_x", fwd_bytes, [&]() {
+      prep(fa);
+      by_length(plan_x_, fwd_.block, [&](auto rs, auto lx) { k_fwd_x<decltype(rs)::value, decltype(lx)::value><<<fwd_.grid, fwd_.block, fwd_.smem, st>>>(fa); });
+      return cudaGetLastError();
+    }));
+  }
+  if (spectral && ndim == 3 && !plane_fwd) {
     C2CArgs c{};
     c.La = Ns[1];
     c.I = Mh;
@@ -3443,7 +3947,7 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
       by_length(plan_ax_[0], c.block, [&](auto rs, auto lx) { k_mid<decltype(rs)::value, decltype(lx)::value><<<c.grid, c.block, msmem, st>>>(m); });
       return cudaGetLastError();
     }));
-    if (ndim == 3) {
+    if (ndim == 3 && !plane_inv) {
       C2CArgs a{};
       a.La = Ns[1];
       a.I = Mh;
@@ -3484,7 +3988,14 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
   // the two error terms the forward pass wrote (err_aux)
   const bool err_epilogue = io.mode == 1 && io.stage == 7 && io.err_part != nullptr;
   const double err_arrays = err_epilogue ? (io.err_aux ? 2.0 : 6.0) : 0.0;
-  RDCU_TRY(timed("inv_x_dictionary", nch * spec_row + 2.0 * n * arr + err_arrays * n * arr, [&]() {
+  const double inv_bytes = nch * spec_row + 2.0 * n * arr + err_arrays * n * arr;
+  if (plane_inv) {
+    RDCU_TRY(timed("inv_plane", inv_bytes, [&]() { return launch_plane_inv(io, st); }));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return cudaSuccess;
+  }
+  RDCU_TRY(timed("inv_x_dictionary", inv_bytes, [&]() {
     if (inv_row_ && !(io.mode == 1 && io.stage == 7 && io.err_part != nullptr && !io.err_aux))
       return launch_inv_row(io, st);
     prep(a);

@@ -183,6 +183,15 @@ class SpectralPlan {
   cudaError_t launch_mid_pipe(const RhsIO& io, cudaStream_t stream);
   cudaError_t launch_c2c_pipe(bool inv, int nplanes, cudaStream_t stream, const RhsIO& io);
   cudaError_t launch_inv_row(const RhsIO& io, cudaStream_t stream);
+  // 3D x passes that also transform along axis 1, one thread-block cluster per plane
+  // (k_fwd_plane, k_inv_plane): enabled flags and persistent grid sizes
+  bool plane_fwd_ = false, plane_inv_ = false;
+  int plane_fwd_grid_ = 0, plane_inv_grid_ = 0;
+  void setup_planes();
+  bool plane_fwd_ok(const RhsIO& io) const;
+  bool plane_inv_ok(const RhsIO& io) const;
+  cudaError_t launch_plane_fwd(const RhsIO& io, cudaStream_t stream);
+  cudaError_t launch_plane_inv(const RhsIO& io, cudaStream_t stream);
 
   ChanTable chan_table(const int* off, const ChanEntry* ent, int nch) const;
   DictTable dict_table() const;

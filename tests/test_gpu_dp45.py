@@ -80,6 +80,42 @@ def test_adaptive_sequence(cuda, Ns, Ls, rtol):
     assert rel_err(out.cpu().numpy(), o.y) < 1e-9
 
 
+def test_plane_passes_dp45_3d(cuda, monkeypatch):
+    """3D CGLE 128^3 with RDCU_PLANE_PASSES=1 (x rows and axis-1 lines of 128 points:
+    the x passes that also transform along axis 1, one cluster per plane): ten adaptive
+    attempts against the default axis-1 passes on TMA tiles -- the same accept/reject
+    sequence, step sizes and states within 1e-9 (the axis-1 transforms round
+    differently; the error norm's cancellation amplifies that) -- and the passes
+    profiled are the plane passes, stage 7 with its error epilogue included."""
+    rng = np.random.default_rng(5)
+    prob = Problem(2, (128, 128, 128), (200.0, 200.0, 200.0), cgle_terms(3))
+    y0 = rng.uniform(-1, 1, 2 * prob.N)
+    runs = []
+    for plane in (True, False):
+        if plane:
+            monkeypatch.setenv("RDCU_PLANE_PASSES", "1")
+        else:
+            monkeypatch.delenv("RDCU_PLANE_PASSES", raising=False)
+        s, yd = _setup(cuda, prob, y0)
+        s.set_state(0.0, 1e-3, yd.data_ptr())
+        names = [p[0] for p in s.profile_passes(reps=1)]
+        assert ("fwd_plane" in names and "inv_plane_stage7" in names) == plane, names
+        s.set_state(0.0, 1e-3, yd.data_ptr())
+        t, h, seq = 0.0, 1e-3, []
+        for _ in range(10):
+            acc, t, h = s.step(t, h)
+            seq.append((acc, t, h))
+        out = cuda.empty_like(yd)
+        s.get_state(out.data_ptr())
+        runs.append((seq, out.cpu().numpy()))
+        s.close()
+    (sa, ya), (sb, yb) = runs
+    for i, ((a1, t1, h1), (a2, t2, h2)) in enumerate(zip(sa, sb)):
+        assert a1 == a2, i
+        assert abs(h1 - h2) <= 1e-9 * abs(h2) and abs(t1 - t2) <= 1e-9 * max(1.0, abs(t2)), (i, h1, h2)
+    assert rel_err(ya, yb) < 1e-9
+
+
 def test_dense_output(cuda):
     rng = np.random.default_rng(21)
     prob = Problem(2, (16, 16), (20.0, 20.0), cgle_terms(2))

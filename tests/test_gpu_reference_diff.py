@@ -98,6 +98,14 @@ def test_adaptive_cgle3d_128(tmp_path):
     check_adaptive(tmp_path, C3D128 + " -t 0.25 -d 0.25 -D1", 3)
 
 
+def test_cgle3d_128_plane_passes(tmp_path, monkeypatch):
+    """The same 128^3 RHS and adaptive run with the x passes that also transform along
+    axis 1 (RDCU_PLANE_PASSES=1, one thread-block cluster per plane)."""
+    monkeypatch.setenv("RDCU_PLANE_PASSES", "1")
+    check_rhs(tmp_path / "rhs", C3D128, 3)
+    check_adaptive(tmp_path / "run", C3D128 + " -t 0.25 -d 0.25 -D1", 3)
+
+
 def test_adaptive_cgle3d_256(tmp_path):
     # two outputs of 268 MB per build: compared on every 97th value
     check_adaptive(tmp_path, C3D256 + " -t 0.25 -d 0.25 -D1", 3, stride=97)

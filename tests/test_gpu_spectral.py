@@ -234,3 +234,25 @@ def test_tiled_passes_3d(cuda, Ns, kind):
     y = smooth_field(rng, prob)
     f, _ = gpu_rhs(cuda, prob, y)
     assert rel_err(f, osp.rhs(y, prob)) < TOL
+
+
+# With RDCU_PLANE_PASSES=1, 3D grids whose x rows and axis-1 lines both have 128 or 256
+# points (axis-0 lines of 128 or 256 points too) take the x passes that also transform
+# along axis 1, one thread-block cluster per plane; by default the axis-1 passes on TMA
+# tiles run.  Both against the oracle, and against each other to rounding ("mixed" has
+# a derivative inside a product: the forward plane pass with the general inverse x pass).
+@pytest.mark.parametrize("Ns,kind", [((128, 128, 128), "cgle"), ((128, 256, 128), "cgle"),
+                                     ((128, 128, 256), "one_field"), ((128, 128, 128), "mixed"),
+                                     ((128, 128, 128), "axis0_pair"), ((256, 128, 128), "cgle")])
+def test_plane_passes_3d(cuda, monkeypatch, Ns, kind):
+    rng = np.random.default_rng(sum(Ns) + len(kind))
+    n, terms = _tile_terms(kind)
+    Ls = tuple(float(rng.uniform(20, 80)) for _ in Ns)
+    prob = Problem(n, Ns, Ls, terms)
+    for y in (rng.uniform(-1, 1, n * prob.N), smooth_field(rng, prob)):
+        monkeypatch.setenv("RDCU_PLANE_PASSES", "1")
+        f, _ = gpu_rhs(cuda, prob, y)
+        assert rel_err(f, osp.rhs(y, prob)) < TOL
+        monkeypatch.delenv("RDCU_PLANE_PASSES")
+        g, _ = gpu_rhs(cuda, prob, y)
+        assert rel_err(f, g) < 1e-13
