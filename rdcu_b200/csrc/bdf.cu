@@ -354,6 +354,218 @@ __global__ void k_interp(const double* D, long long nN, int order, Small fac, do
   y[i] = v;
 }
 
+// ---------------------------------------------------------------- device-resident Newton loop
+// The Newton iteration of one attempt (bdf.cu:147-190) runs as one CUDA graph (see
+// build_newton_graph): WHILE nodes for the Newton iterations, for the GMRES restarts of
+// each linear solve and for the Arnoldi iterations of each restart, with the scalar
+// logic -- norms, the rate tests, the restart tests -- in one-thread kernels on this
+// record.  After the loop the graph forms the squared error norm of the correction d
+// (bdf.cu:231-239).  The host writes the attempt's inputs with k_newton_arm and reads
+// the record back once per attempt.
+struct NewtonCtl {
+  // inputs of the attempt
+  double hh;         // step size
+  double coef;       // (1 - kappa_k) gamma_k of the order
+  double alpha_new;  // -hh / coef: alpha after a refactorisation
+  double gam[6];     // gamma_j
+  int order;
+  int refactor;      // a refactorisation is due (cleared when done)
+  // persistent
+  double alpha;      // alpha of the current "factorisation"
+  // loop state
+  double dnorm, dnormold, rate, beta, tol;
+  int it, converged, update, restart, proceed, total;
+  // results
+  double errsq;  // sum of (d / yscale)^2 after the loop
+  long long lin_iters, lin_cycles, lin_solves;
+};
+
+__global__ void k_newton_arm(NewtonCtl* c, double hh, double coef, double alpha_new, int order, int refactor,
+                             Small gam) {
+  c->hh = hh;
+  c->coef = coef;
+  c->alpha_new = alpha_new;
+  for (int j = 0; j < 6; ++j) c->gam[j] = gam.v[j];
+  c->order = order;
+  if (refactor) c->refactor = 1;
+  c->lin_iters = 0;
+  c->lin_cycles = 0;
+  c->lin_solves = 0;
+}
+
+// start of the Newton loop (the loop variables of bdf.cu:147-150)
+__global__ void k_newton_start(NewtonCtl* c, cudaGraphConditionalHandle cond) {
+  c->it = 0;
+  c->dnorm = 0.0;
+  c->dnormold = 0.0;
+  c->rate = 0.0;
+  c->converged = 0;
+  c->update = 0;
+  cudaGraphSetConditional(cond, 1u);
+}
+
+// start of an iteration: the refactorisation's alpha (bdf.cu:152-156)
+__global__ void k_newton_begin(NewtonCtl* c) {
+  if (c->refactor) {
+    c->alpha = c->alpha_new;
+    c->refactor = 0;
+  }
+}
+
+// k_newton_rhs with the order, h and coefficients of the record
+__global__ void k_newton_rhs_dev(double* b, const double* f, const double* d, const double* D, long long nN,
+                                 const NewtonCtl* c) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nN) return;
+  const int order = c->order;
+  const double h = c->hh, alpha = c->coef;
+  double v = h / alpha * f[i];
+  for (int j = 1; j <= order; ++j) v -= D[nN * j + i] * c->gam[j] / alpha;
+  v -= d[i];
+  b[i] = v;
+}
+
+// k_wsq then k_sum_rows in one launch (k_dots_sum's last-block pattern, bitwise the
+// same sums): out[0] = sum of (x / yscale)^2
+__global__ void k_wsq_sum(const double* x, const double* yscale, long long nN, double* part, unsigned int* count,
+                          double* out) {
+  double sum = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nN; i += (long long)gridDim.x * blockDim.x) {
+    const double v = x[i] / yscale[i];
+    sum += v * v;
+  }
+  sum = block_reduce(sum);
+  __shared__ int last;
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = sum;
+    __threadfence();
+    last = atomicAdd(count, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double t = 0.0;
+  for (int q = threadIdx.x; q < (int)gridDim.x; q += blockDim.x) t += __ldcg(&part[q]);
+  t = block_reduce(t);
+  if (threadIdx.x == 0) {
+    out[0] = t;
+    *count = 0u;
+  }
+}
+
+// start of a linear solve (gmres): beta0 = ||b||, the tolerance, the restart loop's
+// condition (no restart when b = 0: x stays 0)
+__global__ void k_solve_begin(NewtonCtl* c, const double* bb, double lin_tol, cudaGraphConditionalHandle cond) {
+  const double beta0 = sqrt(bb[0]);
+  c->beta = beta0;
+  c->tol = lin_tol * beta0;
+  c->total = 0;
+  c->restart = 0;
+  c->proceed = 0;
+  c->lin_solves += 1;
+  cudaGraphSetConditional(cond, beta0 > 0 ? 1u : 0u);
+}
+
+// r = b - A x from the second restart on
+__global__ void k_residual_dev(const int* rows, const int* cols, const double* vals, const NewtonCtl* c,
+                               const double* x, const double* b, double* r, long long nN) {
+  if (c->restart == 0) return;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nN) return;
+  const double alpha = c->alpha;
+  double acc = 0.0;
+  for (int p = rows[i]; p < rows[i + 1]; ++p) acc += vals[p] * x[cols[p]];
+  r[i] = b[i] - (x[i] + alpha * acc);
+}
+
+// restart test (beta = ||r|| > tol from the second restart on), V_0 = r / beta and the
+// cycle's GMRES state (k_gm_init); the Arnoldi loop runs only when the cycle goes on
+__global__ void k_restart_begin(NewtonCtl* c, GmresState* s, const double* rr, int max_total,
+                                cudaGraphConditionalHandle cond) {
+  if (c->restart > 0) c->beta = sqrt(rr[0]);
+  const int proceed = (c->restart == 0 || c->beta > c->tol) ? 1 : 0;
+  c->proceed = proceed;
+  for (int k = 0; k <= kGmresM; ++k) s->g[k] = k == 0 ? c->beta : 0.0;
+  s->alpha = c->alpha;
+  s->tol = c->tol;
+  s->inv_hn = 0.0;
+  s->j = 0;
+  s->jdone = 0;
+  s->total = c->total;
+  s->max_total = max_total;
+  s->cont = 0;
+  s->conv = 0;
+  s->guard = 0;
+  if (proceed) c->lin_cycles += 1;
+  cudaGraphSetConditional(cond, (unsigned)proceed);
+}
+
+// V_0 = (1 / beta) * (b on the first restart, else r)
+__global__ void k_scale_dev(const NewtonCtl* c, const double* b, const double* r, double* V, long long nN) {
+  if (!c->proceed) return;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nN) return;
+  const double s = 1.0 / c->beta;
+  V[i] = s * (c->restart == 0 ? b[i] : r[i]);
+}
+
+// end of a restart: iterations so far, convergence, the restart loop's condition
+__global__ void k_restart_end(NewtonCtl* c, const GmresState* s, int max_total, cudaGraphConditionalHandle cond) {
+  int cont = 0;
+  if (c->proceed) {
+    c->total = s->total;
+    c->restart += 1;
+    cont = (!s->conv && c->restart < 50 && c->total < max_total) ? 1 : 0;
+  }
+  cudaGraphSetConditional(cond, (unsigned)cont);
+}
+
+__global__ void k_solve_end(NewtonCtl* c) { c->lin_iters += c->total; }
+
+// Newton convergence tests (bdf.cu:168-183) on ||dd|| (weighted RMS): stop, converge,
+// or apply the correction and go on
+__global__ void k_newton_ctl(NewtonCtl* c, const double* ss, double sqN, double ntol, int nwit,
+                             cudaGraphConditionalHandle cond) {
+  const double dnorm = sqrt(ss[0]) / sqN;
+  c->dnorm = dnorm;
+  const double dnormold = c->dnormold;
+  double rate = c->rate;
+  if (dnormold > 0) rate = dnorm / dnormold;
+  c->rate = rate;
+  const int it = c->it;
+  bool stop = false;
+  if (rate >= 1)
+    stop = true;
+  else if (pow(rate, (double)(nwit - it)) / (1 - rate) * dnorm > ntol)
+    stop = true;
+  else if (dnormold > 0 && rate / (1 - rate) * dnorm < ntol) {
+    c->converged = 1;
+    stop = true;
+  }
+  int cont = 0;
+  c->update = stop ? 0 : 1;
+  if (!stop) {
+    c->dnormold = dnorm;
+    c->it = it + 1;
+    cont = it + 1 < nwit ? 1 : 0;
+  }
+  cudaGraphSetConditional(cond, (unsigned)cont);
+}
+
+// ytemp += dd; d += dd when the iteration goes on
+__global__ void k_newton_update_dev(const NewtonCtl* c, const double* dd, double* ytemp, double* d, long long nN) {
+  if (!c->update) return;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nN) return;
+  ytemp[i] += dd[i];
+  d[i] += dd[i];
+}
+
+__global__ void k_zero(double* x, long long nN) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nN) x[i] = 0.0;
+}
+
 // makeRU (bdf.cu:35-69)
 void make_RU(int order, double factor, double* RU) {
   double R[36], U[36];
@@ -405,6 +617,14 @@ struct BDFEngine::Impl {
   cudaGraph_t cycle_graph = nullptr;
   cudaGraphExec_t cycle_exec = nullptr;
   double* cycle_x = nullptr;  // the solution vector the graph updates
+  // the Newton loop of an attempt as a graph (build_newton_graph), its record and a
+  // pinned copy; newton_failed: the graph could not be built (host loop instead)
+  NewtonCtl* nctl = nullptr;
+  NewtonCtl* nctl_host = nullptr;
+  double* ndots = nullptr;  // ||b||^2, ||r||^2, ||dd||^2 (weighted) of the graph
+  cudaGraph_t newton_graph = nullptr;
+  cudaGraphExec_t newton_exec = nullptr;
+  bool newton_failed = false;
   int refactor = 1, rejac = 1;
   double nconststeps = 0;
   double ntol = 0;
@@ -488,6 +708,11 @@ bool BDFEngine::init(FDProblem* fd, double atol, double rtol, int fixed, cudaStr
     return fail("GMRES state");
   if (cudaMallocHost((void**)&I.hdots, sizeof(double) * 3 * (I.m + 2)) != cudaSuccess) return fail("pinned");
   if (cudaMallocHost((void**)&I.gm_host, sizeof(GmresState)) != cudaSuccess) return fail("pinned");
+  if (cudaMalloc((void**)&I.nctl, sizeof(NewtonCtl)) != cudaSuccess ||
+      cudaMemset(I.nctl, 0, sizeof(NewtonCtl)) != cudaSuccess ||
+      cudaMalloc((void**)&I.ndots, sizeof(double) * 4) != cudaSuccess)
+    return fail("Newton state");
+  if (cudaMallocHost((void**)&I.nctl_host, sizeof(NewtonCtl)) != cudaSuccess) return fail("pinned");
   device_bytes = sb * (8 + 11 + I.m + 1) + fd->device_bytes;
   std::vector<LinEntry> lin = linear_part(*fd);
   if (!lin.empty() && fd->n <= kMaxPrecFields) {
@@ -505,6 +730,11 @@ void BDFEngine::release() {
     Impl& I = *impl_;
     if (I.cycle_exec) cudaGraphExecDestroy(I.cycle_exec);
     if (I.cycle_graph) cudaGraphDestroy(I.cycle_graph);
+    if (I.newton_exec) cudaGraphExecDestroy(I.newton_exec);
+    if (I.newton_graph) cudaGraphDestroy(I.newton_graph);
+    if (I.nctl) cudaFree(I.nctl);
+    if (I.ndots) cudaFree(I.ndots);
+    if (I.nctl_host) cudaFreeHost(I.nctl_host);
     double* vecs[] = {I.ytemp, I.yscale, I.f, I.d, I.dd, I.b, I.y_eval, I.w, I.z, I.vj, I.r, I.V, I.part, I.dots};
     for (double* p : vecs)
       if (p) cudaFree(p);
@@ -689,6 +919,122 @@ static cudaError_t gmres(BDFEngine::Impl& I, const FDProblem& fd, double alpha, 
   return cudaGetLastError();
 }
 
+// A WHILE node on handle h after the capture's current frontier in graph g (being
+// captured on st); the capture continues after it.  *body receives its body graph.
+static cudaError_t add_while_node(cudaGraph_t g, cudaStream_t st, cudaGraphConditionalHandle h, cudaGraph_t* body) {
+  cudaStreamCaptureStatus cs;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  RDCU_TRY(cudaStreamGetCaptureInfo(st, &cs, nullptr, nullptr, &deps, &nd));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node = nullptr;
+  RDCU_TRY(cudaGraphAddNode(&node, g, deps, nd, &cp));
+  *body = cp.conditional.phGraph_out[0];
+  return cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies);
+}
+
+// Captures `fill` into graph g on st.
+template <typename F>
+static cudaError_t capture_into(cudaGraph_t g, cudaStream_t st, F&& fill) {
+  RDCU_TRY(cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = fill();
+  if (e == cudaSuccess) e = cudaGetLastError();
+  cudaGraph_t captured = nullptr;
+  const cudaError_t e2 = cudaStreamEndCapture(st, &captured);
+  return e != cudaSuccess ? e : e2;
+}
+
+// The Newton loop of one attempt (bdf.cu:147-190) with its linear solves (gmres above)
+// as one graph: Newton WHILE { f = F(ytemp); alpha on refactorisation; b; ||b||; x = 0;
+// restart WHILE { r = b - A x and ||r|| (from the second restart); test; V_0; Arnoldi
+// WHILE { one iteration, as in build_cycle_graph }; x += P^-1 V y }; ||dd||; tests;
+// update }, then yscale at ytemp and ||d||^2 for the error test (bdf.cu:231-239).
+static cudaError_t build_newton_graph(BDFEngine::Impl& I, FDProblem& fd, const double* D, cudaStream_t st) {
+  const long long nN = I.nN;
+  const int nb = I.blocks, m = I.m, row = m + 2;
+  const double* alpha_dev = &I.gm->alpha;
+  const double sqN = std::pow((double)nN, 0.5);
+  double* x = I.dd;
+  cudaGraph_t G = nullptr;
+  RDCU_TRY(cudaGraphCreate(&G, 0));
+  cudaGraphConditionalHandle hn, hr, ha;
+  cudaGraph_t Bn = nullptr, Br = nullptr, Ba = nullptr;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&hn, G, 0, cudaGraphCondAssignDefault);
+  if (e == cudaSuccess)
+    e = capture_into(G, st, [&]() -> cudaError_t {
+      k_newton_start<<<1, 1, 0, st>>>(I.nctl, hn);
+      RDCU_TRY(add_while_node(G, st, hn, &Bn));
+      k_errscale<<<nb, 256, 0, st>>>(I.ytemp, nN, I.atl, I.rtl, I.yscale);
+      k_wsq_sum<<<kRedBlocks, kRedThreads, 0, st>>>(I.d, I.yscale, nN, I.part, I.arrivals, &I.nctl->errsq);
+      return cudaSuccess;
+    });
+  if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&hr, Bn, 0, cudaGraphCondAssignDefault);
+  if (e == cudaSuccess)
+    e = capture_into(Bn, st, [&]() -> cudaError_t {
+      RDCU_TRY(fd.rhs(I.ytemp, I.f, nullptr));
+      k_newton_begin<<<1, 1, 0, st>>>(I.nctl);
+      k_newton_rhs_dev<<<nb, 256, 0, st>>>(I.b, I.f, I.d, D, nN, I.nctl);
+      k_dots_sum<<<dim3(kRedBlocks, 1), kRedThreads, 0, st>>>(I.V, I.gm, 0, I.b, nN, I.part, I.arrivals, I.ndots);
+      k_solve_begin<<<1, 1, 0, st>>>(I.nctl, I.ndots, I.lin_tol, hr);
+      k_zero<<<nb, 256, 0, st>>>(x, nN);
+      RDCU_TRY(add_while_node(Bn, st, hr, &Br));
+      k_solve_end<<<1, 1, 0, st>>>(I.nctl);
+      k_wsq_sum<<<kRedBlocks, kRedThreads, 0, st>>>(x, I.yscale, nN, I.part, I.arrivals, I.ndots + 2);
+      k_newton_ctl<<<1, 1, 0, st>>>(I.nctl, I.ndots + 2, sqN, I.ntol, kNwit, hn);
+      k_newton_update_dev<<<nb, 256, 0, st>>>(I.nctl, x, I.ytemp, I.d, nN);
+      return cudaSuccess;
+    });
+  if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&ha, Br, 0, cudaGraphCondAssignDefault);
+  if (e == cudaSuccess)
+    e = capture_into(Br, st, [&]() -> cudaError_t {
+      k_residual_dev<<<nb, 256, 0, st>>>(fd.rows_, fd.cols_, fd.vals_, I.nctl, x, I.b, I.r, nN);
+      k_dots_sum<<<dim3(kRedBlocks, 1), kRedThreads, 0, st>>>(I.V, I.gm, 0, I.r, nN, I.part, I.arrivals,
+                                                              I.ndots + 1);
+      k_restart_begin<<<1, 1, 0, st>>>(I.nctl, I.gm, I.ndots + 1, I.lin_max_iters, ha);
+      k_scale_dev<<<nb, 256, 0, st>>>(I.nctl, I.b, I.r, I.V, nN);
+      RDCU_TRY(add_while_node(Br, st, ha, &Ba));
+      k_gm_backsub<<<1, 32, 0, st>>>(I.gm);
+      k_vcomb_j<<<nb, 256, 0, st>>>(I.V, I.gm, I.w, nN);
+      if (I.have_prec) {
+        RDCU_TRY(I.prec.precond(I.w, I.z, 0.0, alpha_dev, st));
+        k_axpy<<<nb, 256, 0, st>>>(1.0, I.z, x, nN);
+      } else {
+        k_axpy<<<nb, 256, 0, st>>>(1.0, I.w, x, nN);
+      }
+      k_restart_end<<<1, 1, 0, st>>>(I.nctl, I.gm, I.lin_max_iters, hr);
+      return cudaSuccess;
+    });
+  if (e == cudaSuccess)
+    e = capture_into(Ba, st, [&]() -> cudaError_t {
+      const double* zin = I.have_prec ? I.z : I.vj;
+      k_gm_take<<<nb, 256, 0, st>>>(I.V, I.gm, I.w, I.vj, nN);
+      if (I.have_prec) RDCU_TRY(I.prec.precond(I.vj, I.z, 0.0, alpha_dev, st));
+      k_apply_A_dev<<<nb, 256, 0, st>>>(fd.rows_, fd.cols_, fd.vals_, alpha_dev, zin, I.w, nN);
+      for (int pass = 0; pass < 2; ++pass) {
+        k_dots_sum<<<dim3(kRedBlocks, m + 1), kRedThreads, 0, st>>>(I.V, I.gm, -1, I.w, nN, I.part, I.arrivals,
+                                                                    I.dots + pass * row);
+        k_vsub_j<<<nb, 256, 0, st>>>(I.V, I.gm, I.dots + pass * row, I.w, nN);
+      }
+      k_dots_sum<<<dim3(kRedBlocks, 1), kRedThreads, 0, st>>>(I.V, I.gm, 0, I.w, nN, I.part, I.arrivals,
+                                                              I.dots + 2 * row);
+      k_gm_update<<<1, 32, 0, st>>>(I.gm, I.dots, row, ha);
+      return cudaSuccess;
+    });
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&I.newton_exec, G, 0);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(G);
+    I.newton_exec = nullptr;
+    cudaGetLastError();
+    return e;
+  }
+  I.newton_graph = G;
+  return cudaSuccess;
+}
+
 // bdf_run set-up (bdf.cu:333-374): f and J at D_0; order 0 -> D_1 = h f
 static cudaError_t bdf_setup(BDFEngine::Impl& I, FDProblem& fd, double* D, int* order, double h,
                              cudaStream_t st) {
@@ -724,7 +1070,31 @@ cudaError_t BDFEngine::step(double* t, double* h, double hmin, double hmax, int*
   RDCU_TRY(cudaMemsetAsync(I.d, 0, sizeof(double) * nN, st_));
   Small gam{};
   for (int j = 0; j < 6; ++j) gam.v[j] = kGamma[j];
-  for (it = 0; it < kNwit; it++) {
+  if (!I.newton_exec && !I.newton_failed && build_newton_graph(I, *fd_, D_, st_) != cudaSuccess)
+    I.newton_failed = true;
+  // the graph also leaves yscale at ytemp and ||d||^2 for the error test
+  bool errsq_ready = false;
+  double errsq = 0.0;
+  if (I.newton_exec) {
+    // the Newton loop on the device: one launch, one record read back
+    const double coef = (1 - kKappa[order]) * kGamma[order];
+    k_newton_arm<<<1, 1, 0, st_>>>(I.nctl, hh, coef, -hh / coef, order, I.refactor, gam);
+    RDCU_TRY(cudaGetLastError());
+    RDCU_TRY(cudaGraphLaunch(I.newton_exec, st_));
+    RDCU_TRY(cudaMemcpyAsync(I.nctl_host, I.nctl, sizeof(NewtonCtl), cudaMemcpyDeviceToHost, st_));
+    RDCU_TRY(cudaStreamSynchronize(st_));
+    const NewtonCtl& c = *I.nctl_host;
+    converged = c.converged;
+    it = c.it;
+    I.alpha = c.alpha;
+    I.refactor = c.refactor;
+    lin_iters += c.lin_iters;
+    lin_cycles += c.lin_cycles;
+    lin_solves += c.lin_solves;
+    errsq = c.errsq;
+    errsq_ready = true;
+  }
+  for (it = I.newton_exec ? it : 0; !I.newton_exec && it < kNwit; it++) {
     RDCU_TRY(fd_->rhs(I.ytemp, I.f, nullptr));
     if (I.refactor) {
       I.alpha = -hh / ((1 - kKappa[order]) * kGamma[order]);
@@ -788,8 +1158,12 @@ cudaError_t BDFEngine::step(double* t, double* h, double hmin, double hmax, int*
   // error test (bdf.cu:231-259)
   const double safety = (2 * kNwit + 1) * 0.9 / (2 * kNwit + it + 1);
   double errnorm;
-  k_errscale<<<nb, 256, 0, st_>>>(I.ytemp, nN, I.atl, I.rtl, I.yscale);
-  RDCU_TRY(wnorm(I, I.d, st_, &errnorm));
+  if (errsq_ready) {
+    errnorm = std::sqrt(errsq);
+  } else {
+    k_errscale<<<nb, 256, 0, st_>>>(I.ytemp, nN, I.atl, I.rtl, I.yscale);
+    RDCU_TRY(wnorm(I, I.d, st_, &errnorm));
+  }
   errnorm *= (kKappa[order] * kGamma[order] + 1.0 / (order + 1)) / sqN;
   factor = safety * std::pow(errnorm, (-1.0 / (order + 1)));
   if (errnorm > 1) {
