@@ -17,9 +17,11 @@
 // the reference's stencils are circulant, so the FFT diagonalises J_lin and each
 // Fourier mode is an n x n solve (spectral.cu k_mid_solve).  GMRES runs to a relative
 // residual of 1e-12, far below the Newton tolerance, so Newton and step decisions are
-// those of an exact solve.  Each restart cycle (up to 40 Arnoldi iterations) is one
-// CUDA graph whose WHILE node loops on the device: the host reads back one small
-// state record per cycle instead of the Gram-Schmidt coefficients per iteration.
+// those of an exact solve.  The Newton loop of an attempt, with its linear solves (GMRES
+// restarts of up to 40 Arnoldi iterations), is one CUDA graph of nested WHILE nodes
+// whose tests run on the device: the host reads back one small record per attempt.  If
+// that graph cannot be built, each restart cycle alone is a graph and the host runs
+// the Newton and restart loops.
 #include <algorithm>
 #include <cmath>
 #include <cstddef>
