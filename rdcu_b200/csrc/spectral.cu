@@ -423,8 +423,10 @@ __device__ __forceinline__ void fwd_load2(const FwdXArgs& a, const Resolved& r, 
   }
 }
 
-// bx: the CTA's index within this plan's grid (blockIdx.x, or a work item of a batch)
-template <int RS, int LX>
+// bx: the CTA's index within this plan's grid (blockIdx.x, or a work item of a batch).
+// SF > 0: the stage is SF, known at compile time (a kernel per stage has the registers
+// of its own stage combination, not those of the largest); SF = 0: the stage of a.io.
+template <int RS, int LX, int SF = 0>
 __device__ __forceinline__ void fwd_x_body(const FwdXArgs& a, int bx) {
   extern __shared__ double2 sm[];
   if (a.io.mode == 1 && !a.io.ctl->running) return;
@@ -444,7 +446,7 @@ __device__ __forceinline__ void fwd_x_body(const FwdXArgs& a, int bx) {
   unsigned long long align = reinterpret_cast<unsigned long long>(r.y) | reinterpret_cast<unsigned long long>(r.ytemp);
   for (int j = 0; j < 7; ++j) align |= reinterpret_cast<unsigned long long>(r.k[j]);
   if (LX > 0 && (align & 15) == 0) {
-    switch (r.stage) {
+    switch (SF > 0 ? SF : r.stage) {
       case 2: fwd_load2<2, LX>(a, r, buf, row0); break;
       case 3: fwd_load2<3, LX>(a, r, buf, row0); break;
       case 4: fwd_load2<4, LX>(a, r, buf, row0); break;
@@ -454,7 +456,7 @@ __device__ __forceinline__ void fwd_x_body(const FwdXArgs& a, int bx) {
       default: fwd_load2<1, LX>(a, r, buf, row0); break;
     }
   } else {
-    switch (r.stage) {
+    switch (SF > 0 ? SF : r.stage) {
       case 2: fwd_load<2, LX>(a, r, buf, row0); break;
       case 3: fwd_load<3, LX>(a, r, buf, row0); break;
       case 4: fwd_load<4, LX>(a, r, buf, row0); break;
@@ -487,9 +489,9 @@ __device__ __forceinline__ void fwd_x_body(const FwdXArgs& a, int bx) {
   }
 }
 
-template <int RS, int LX>
-__global__ void __launch_bounds__(LX > 0 ? kSpecBlock : kMaxBlock, LX > 0 ? 2 : 1) k_fwd_x(FwdXArgs a) {
-  fwd_x_body<RS, LX>(a, blockIdx.x);
+template <int RS, int LX, int SF = 0>
+__global__ void __launch_bounds__(LX > 0 ? kSpecBlock : kMaxBlock, LX > 0 ? (SF > 0 ? 4 : 2) : 1) k_fwd_x(FwdXArgs a) {
+  fwd_x_body<RS, LX, SF>(a, blockIdx.x);
 }
 
 struct C2CArgs {
@@ -2425,6 +2427,30 @@ static void by_length(const LinePlan& p, int block, F&& f) {
     f(RA{}, std::integral_constant<int, 0>{});
 }
 
+// k_fwd_x on the plan's x lines: a kernel per stage (1..7; the stage of a DP45 launch, 1
+// for a plain evaluation) for 128- and 256-point rows, the runtime-stage kernel
+// otherwise.
+static void launch_fwd_x(const LinePlan& plan, int block, int grid, size_t smem, cudaStream_t st,
+                         const FwdXArgs& a) {
+  const int stage = a.io.mode == 1 ? std::max(1, a.io.stage) : 1;
+  by_length(plan, block, [&](auto rs, auto lx) {
+    constexpr int RS = decltype(rs)::value, LX = decltype(lx)::value;
+    if constexpr (LX == 128 || LX == 256) {
+      switch (stage) {
+        case 2: k_fwd_x<RS, LX, 2><<<grid, block, smem, st>>>(a); break;
+        case 3: k_fwd_x<RS, LX, 3><<<grid, block, smem, st>>>(a); break;
+        case 4: k_fwd_x<RS, LX, 4><<<grid, block, smem, st>>>(a); break;
+        case 5: k_fwd_x<RS, LX, 5><<<grid, block, smem, st>>>(a); break;
+        case 6: k_fwd_x<RS, LX, 6><<<grid, block, smem, st>>>(a); break;
+        case 7: k_fwd_x<RS, LX, 7><<<grid, block, smem, st>>>(a); break;
+        default: k_fwd_x<RS, LX, 1><<<grid, block, smem, st>>>(a); break;
+      }
+    } else {
+      k_fwd_x<RS, LX><<<grid, block, smem, st>>>(a);
+    }
+  });
+}
+
 // ----------------------------------------------------------------------------- plan
 ChanTable SpectralPlan::chan_table(const int* off, const ChanEntry* ent, int nchan) const {
   ChanTable t{};
@@ -2941,6 +2967,15 @@ bool SpectralPlan::init(int n_, int ndim_, const int* Ns_, const double* Ls_,
       by_length(pl, blk, [&](auto rs, auto lx) {
         constexpr int RS = decltype(rs)::value, LX = decltype(lx)::value;
         optin_ok &= opt_in_smem((const void*)k_fwd_x<RS, LX>);
+        if constexpr (LX == 128 || LX == 256) {
+          optin_ok &= opt_in_smem((const void*)k_fwd_x<RS, LX, 1>);
+          optin_ok &= opt_in_smem((const void*)k_fwd_x<RS, LX, 2>);
+          optin_ok &= opt_in_smem((const void*)k_fwd_x<RS, LX, 3>);
+          optin_ok &= opt_in_smem((const void*)k_fwd_x<RS, LX, 4>);
+          optin_ok &= opt_in_smem((const void*)k_fwd_x<RS, LX, 5>);
+          optin_ok &= opt_in_smem((const void*)k_fwd_x<RS, LX, 6>);
+          optin_ok &= opt_in_smem((const void*)k_fwd_x<RS, LX, 7>);
+        }
         optin_ok &= opt_in_smem((const void*)k_inv_x<RS, LX>);
         optin_ok &= opt_in_smem((const void*)k_mid<RS, LX>);
         optin_ok &= opt_in_smem((const void*)k_c2c<RS, false, LX>);
@@ -3610,7 +3645,7 @@ cudaError_t SpectralPlan::run(const RhsIO& io, cudaStream_t st) {
     a.io = io;
     const size_t smem = spectral ? fwd_.smem : 0;
     prep(a);
-    by_length(plan_x_, fwd_.block, [&](auto rs, auto lx) { k_fwd_x<decltype(rs)::value, decltype(lx)::value><<<fwd_.grid, fwd_.block, smem, st>>>(a); });
+    launch_fwd_x(plan_x_, fwd_.block, fwd_.grid, smem, st, a);
     RDCU_TRY(cudaGetLastError());
   }
   if (spectral && ndim == 3) {
@@ -3652,7 +3687,7 @@ cudaError_t SpectralPlan::run_Y(const double* y, double* Yout, cudaStream_t st) 
   a.S = Sf_;
   a.io = io;
   prep(a);
-  by_length(plan_x_, fwd_.block, [&](auto rs, auto lx) { k_fwd_x<decltype(rs)::value, decltype(lx)::value><<<fwd_.grid, fwd_.block, fwd_.smem, st>>>(a); });
+  launch_fwd_x(plan_x_, fwd_.block, fwd_.grid, fwd_.smem, st, a);
   RDCU_TRY(cudaGetLastError());
   if (ndim == 3) {
     C2CArgs c{};
@@ -3746,7 +3781,7 @@ cudaError_t SpectralPlan::launch_forward(const double* y, cudaStream_t st) {
   a.S = Sf_;
   a.io = io;
   prep(a);
-  by_length(plan_x_, fwd_.block, [&](auto rs, auto lx) { k_fwd_x<decltype(rs)::value, decltype(lx)::value><<<fwd_.grid, fwd_.block, fwd_.smem, st>>>(a); });
+  launch_fwd_x(plan_x_, fwd_.block, fwd_.grid, fwd_.smem, st, a);
   RDCU_TRY(cudaGetLastError());
   if (ndim == 3) {
     C2CArgs c{};
@@ -3894,7 +3929,7 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
   } else {
     RDCU_TRY(timed("fwd_x", fwd_bytes, [&]() {
       prep(fa);
-      by_length(plan_x_, fwd_.block, [&](auto rs, auto lx) { k_fwd_x<decltype(rs)::value, decltype(lx)::value><<<fwd_.grid, fwd_.block, fwd_.smem, st>>>(fa); });
+      launch_fwd_x(plan_x_, fwd_.block, fwd_.grid, fwd_.smem, st, fa);
       return cudaGetLastError();
     }));
   }
