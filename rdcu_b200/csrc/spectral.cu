@@ -1702,14 +1702,13 @@ struct InvRowArgs {
   DictTable dict;
   RhsIO io;
 };
-// Warps per CTA: 8, or 5 with the stage-7 error epilogue (its staging slots also hold
-// the row's error terms).
-__host__ __device__ constexpr int row_warps(bool err) { return err ? 5 : 8; }
-// one staging slot of a warp: 2 channels x (at most 129 + padding) spectral values,
-// NF x 256 field values and, with the error epilogue, 2 x NF x 256 error terms (two
-// rows of 128 points take the same room)
+// Warps per CTA (the stage-7 error epilogue reads each row's error terms straight into
+// registers, before the row's transform).
+__host__ __device__ constexpr int row_warps(bool) { return 8; }
+// one staging slot of a warp: 2 channels x (at most 129 + padding) spectral values and
+// NF x 256 field values (two rows of 128 points take the same room)
 constexpr int kRowSpec = 2 * 136;  // double2 per slot
-__host__ __device__ constexpr int row_slot_doubles(int nf, bool err) { return 2 * kRowSpec + nf * 256 * (err ? 3 : 1); }
+__host__ __device__ constexpr int row_slot_doubles(int nf, bool) { return 2 * kRowSpec + nf * 256; }
 
 __host__ __device__ constexpr size_t inv_row_smem(int n, int count, bool err) {
   return (size_t)row_warps(err) * (256 * 16 + 2 * (size_t)row_slot_doubles(n, err) * 8) + (size_t)n * count * 8 + 64;
@@ -1737,15 +1736,12 @@ __global__ void __launch_bounds__(row_warps(ERR) * 32, 1) k_inv_row(InvRowArgs a
   wl.init(a.tw, ml);
   const long long RL = (long long)a.R * L;
   // the row's spectra (both channels) and fields as 16-byte pieces, when aligned
-  const bool a16 = ((reinterpret_cast<unsigned long long>(r.u) | reinterpret_cast<unsigned long long>(a.Sc) |
-                     (ERR ? reinterpret_cast<unsigned long long>(r.aux) : 0ull)) & 15) == 0;
+  const bool a16 = ((reinterpret_cast<unsigned long long>(r.u) | reinterpret_cast<unsigned long long>(a.Sc)) & 15) == 0;
   const int Mh = a.Mh, nch = a.nch;
   const long long wstride = (long long)gridDim.x * kRowWarps * RPW;
   // slot k of this warp; the sub-row's part of it
   auto slot_spec = [&](int k) { return reinterpret_cast<double2*>(stage + (warp * 2 + k) * SLOT) + sub * (kRowSpec / RPW); };
   auto slot_u = [&](int k) { return stage + (warp * 2 + k) * SLOT + 2 * kRowSpec + sub * NF * L; };
-  // ERR: the row's error terms (slope part, then scale) after the fields of both rows
-  auto slot_e = [&](int k) { return stage + (warp * 2 + k) * SLOT + 2 * kRowSpec + NF * 256 + sub * 2 * NF * L; };
   const long long nN = (long long)NF * RL;
   auto fetch = [&](long long row, int k) {
     if (row >= a.R) return;
@@ -1761,27 +1757,11 @@ __global__ void __launch_bounds__(row_warps(ERR) * 32, 1) k_inv_row(InvRowArgs a
           const int x2 = 2 * (ml + LPL * k2);
           cp_async16(su + f * L + x2, r.u + f * RL + row * L + x2, true);
         }
-      if (ERR) {
-        double* se = slot_e(k);
-#pragma unroll
-        for (int q = 0; q < 2 * NF; ++q)
-#pragma unroll
-          for (int k2 = 0; k2 < L / 2 / LPL; ++k2) {
-            const int x2 = 2 * (ml + LPL * k2);
-            cp_async16(se + q * L + x2, r.aux + (q >= NF ? nN : 0) + (q % NF) * RL + row * L + x2, true);
-          }
-      }
     } else {
       for (int c = 0; c < nch; ++c)
         for (int e = ml; e < Mh; e += LPL) sp[c * Mh + e] = a.Sc[((long long)c * a.R + row) * Mh + e];
       for (int f = 0; f < NF; ++f)
         for (int k2 = 0; k2 < 8; ++k2) su[f * L + ml + LPL * k2] = r.u[f * RL + row * L + ml + LPL * k2];
-      if (ERR) {
-        double* se = slot_e(k);
-        for (int q = 0; q < 2 * NF; ++q)
-          for (int k2 = 0; k2 < 8; ++k2)
-            se[q * L + ml + LPL * k2] = r.aux[(q >= NF ? nN : 0) + (q % NF) * RL + row * L + ml + LPL * k2];
-      }
     }
   };
   long long row0 = ((long long)blockIdx.x * kRowWarps + warp) * RPW;
@@ -1799,7 +1779,19 @@ __global__ void __launch_bounds__(row_warps(ERR) * 32, 1) k_inv_row(InvRowArgs a
     __syncwarp();  // this row's copies (every lane's) landed
     const double2* sp = slot_spec(k);
     const double* su = slot_u(k);
-    const double* se = slot_e(k);
+    // ERR: the row's error terms at the lane's points (slope part, then scale), loaded
+    // before the transform so that it covers their latency
+    double es_t[ERR ? 8 : 1][NF], den_t[ERR ? 8 : 1][NF];
+    if (ERR && live) {
+#pragma unroll
+      for (int p = 0; p < 8; ++p)
+#pragma unroll
+        for (int i = 0; i < NF; ++i) {
+          const long long gi = i * RL + row * L + ml + LPL * p;
+          es_t[ERR ? p : 0][i] = r.aux[gi];
+          den_t[ERR ? p : 0][i] = r.aux[nN + gi];
+        }
+    }
     double2 v[8];
 #pragma unroll
     for (int p = 0; p < 8; ++p) {
@@ -1826,7 +1818,8 @@ __global__ void __launch_bounds__(row_warps(ERR) * 32, 1) k_inv_row(InvRowArgs a
 #pragma unroll
     for (int p = 0; p < 8; ++p) line[ml + LPL * p] = v[p];
     double es_even = 0.0, es_odd = 0.0;  // ERR, 128 points: the partials of lanes ml and ml + 16
-#pragma unroll 2
+    // (unrolled fully with the error epilogue: its terms stay in registers)
+#pragma unroll(ERR ? 8 : 2)
     for (int p = 0; p < 8; ++p) {
       const int x = ml + LPL * p;
       const double2 z = line[x];
@@ -1848,8 +1841,8 @@ __global__ void __launch_bounds__(row_warps(ERR) * 32, 1) k_inv_row(InvRowArgs a
         if (live) r.f[i * RL + row * L + x] = acc;
         if (ERR) {
           // k_inv_x's error kernel (dp45.cu:79-84) from the forward pass's terms
-          const double es = se[i * L + x] + c_e[6] * acc;
-          const double ev = r.h * es / se[(NF + i) * L + x];
+          const double es = es_t[ERR ? p : 0][i] + c_e[6] * acc;
+          const double ev = r.h * es / den_t[ERR ? p : 0][i];
           err2 += ev * ev;
         }
       }
