@@ -169,17 +169,18 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------------------- our arm
-# DRAM bytes (read + write) per launch of each pass of DP45 stage 4 on the 3D CGLE, from
-# one ncu capture (`ncu --set full ... python -m tests.profile_case 256,256,128`,
-# 8.39 M grid points); traffic grows with the grid points, so the full-size workload's
-# figure is this one scaled by its points.
+# DRAM bytes (read + write) per launch of each pass of DP45 stages 4 and 7 on the 3D
+# CGLE, from one ncu capture per kernel (`ncu --set full ... python -m tests.profile_case
+# 256,256,128 --attempts 2 --reps 1`, 8.39 M grid points; the axis-1 inverse pass is
+# the forward one's kernel on the same bytes); traffic grows with the grid points, so
+# the full-size workload's figure is this one scaled by its points.
 NCU_POINTS = 256 * 256 * 128
 # DRAM bytes per launch of the defect-line grid passes on the 128^3 workload frames, from
 # one ncu capture (`ncu --set full -k regex:"k_(faces|hook|corr)" ... bench.py --workload
 # lines_cgle3d_128 --steps 1 --warmup 3`): k_faces reads the 16.8 MB phase field once.
 NCU_TRAFFIC_LINES = {"faces": 16.8e6}
-NCU_TRAFFIC_3D = {"fwd_x": 772.5e6, "c2c_axis1_fwd": 219.3e6, "mid_axis0": 226.4e6, "c2c_axis1_inv": 219.6e6,
-                  "inv_x_dictionary": 373.3e6}
+NCU_TRAFFIC_3D = {"fwd_x": 772.4e6, "c2c_axis1_fwd": 218.2e6, "mid_axis0": 225.0e6, "c2c_axis1_inv": 218.2e6,
+                  "inv_x_dictionary": 373.6e6, "fwd_x_stage7": 1296.7e6, "inv_x_stage7": 656.5e6}
 
 
 def combine_ranks(seconds, work, device):
