@@ -961,11 +961,11 @@ def run_reference(args):
     N = int(np.prod(Ns))
     T_A = args.warmup * TAU
     # The reference times from program start (CUDA and cuFFT set-up included), so the
-    # window must not contain set-up, nor let its run-to-run variance dominate:
-    # 2D: one run with outputs every T_A, rate between the progress lines at T_A and at
-    #     the end (the outputs of these small grids cost nothing noticeable);
-    # 3D: two runs, to T_A and to T_B, differenced; grids up to 2M points use a window
-    #     ten times the bench's (the reference then integrates ~15 s in it).
+    # rate comes from the progress lines of one run, set-up outside the window:
+    # 2D: outputs every T_A, rate between the progress lines at T_A and at the end (the
+    #     outputs of these small grids cost nothing noticeable);
+    # 3D: outputs only at the window's two ends (below); grids up to 2M points use a
+    #     window ten times the bench's (the reference then integrates ~15 s in it).
     mult = 10 if (len(Ns) == 3 and N <= (1 << 21)) else 1
     T_B = (args.warmup + mult * args.steps) * TAU
 
