@@ -489,9 +489,12 @@ __device__ __forceinline__ void fwd_x_body(const FwdXArgs& a, int bx) {
   }
 }
 
+// The CTAs take the rows from the last to the first: the previous stage's row kernel
+// ended on the last rows of the slope this stage reads (still in L2), and the axis-1
+// pass after it starts on the first planes, written last here.
 template <int RS, int LX, int SF = 0>
 __global__ void __launch_bounds__(LX > 0 ? kSpecBlock : kMaxBlock, LX > 0 ? (SF > 0 ? 4 : 2) : 1) k_fwd_x(FwdXArgs a) {
-  fwd_x_body<RS, LX, SF>(a, blockIdx.x);
+  fwd_x_body<RS, LX, SF>(a, gridDim.x - 1 - blockIdx.x);
 }
 
 struct C2CArgs {
@@ -1174,8 +1177,11 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
   const int coff = (li >> 3) * BOXB, c = li & 7;
   WarpLine<L> wl;
   wl.init(a.tw, lane % LPL);
+  // the inverse pass takes its tiles in reverse order: it ends on the planes the row
+  // kernel after it starts with, which are then still in L2
+  auto order = [&](int tile) { return INV ? a.ntiles - 1 - tile : tile; };
   auto issue = [&](int tile, int b) {
-    const int b0 = tile * BPT, nb = min(BPT, a.nbox - b0);
+    const int b0 = order(tile) * BPT, nb = min(BPT, a.nbox - b0);
     mbar_expect_tx(&full[b], (unsigned)(nb * BOXB));
     char* dst = sm + b * kPipeBufBytes;
     for (int k = 0; k < nb; ++k) {
@@ -1201,7 +1207,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
     }
     char* tb = sm + b * kPipeBufBytes;
     char* bx = tb + coff;
-    if (tile * BPT + (li >> 3) < a.nbox) {
+    if (order(tile) * BPT + (li >> 3) < a.nbox) {
       double2 v[8];
       wl.load(v, bx, c);
       wl.template transform<INV>(v, bx, c);
@@ -1210,7 +1216,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
     fence_proxy_async_smem();
     __syncthreads();
     if (tid == 0) {
-      const int b0 = tile * BPT, nb = min(BPT, a.nbox - b0);
+      const int b0 = order(tile) * BPT, nb = min(BPT, a.nbox - b0);
       for (int k = 0; k < nb; ++k) {
         const int plane = (b0 + k) / a.nchunk, chunk = (b0 + k) - plane * a.nchunk;
         tma_store_3d(&tm, 16 * chunk, 0, plane, tb + k * BOXB);
