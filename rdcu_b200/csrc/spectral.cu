@@ -1708,24 +1708,25 @@ struct InvRowArgs {
   DictTable dict;
   RhsIO io;
 };
-// Warps per CTA (the stage-7 error epilogue reads each row's error terms straight into
-// registers, before the row's transform).
-__host__ __device__ constexpr int row_warps(bool) { return 8; }
+// Warps per CTA: ten for at most two fields (168 registers each; their staging fits),
+// else eight; eight with the stage-7 error epilogue, which reads each row's error terms
+// straight into registers before the row's transform (255 registers).
+__host__ __device__ constexpr int row_warps(bool err, int nf) { return err || nf > 2 ? 8 : 10; }
 // one staging slot of a warp: 2 channels x (at most 129 + padding) spectral values and
 // NF x 256 field values (two rows of 128 points take the same room)
 constexpr int kRowSpec = 2 * 136;  // double2 per slot
 __host__ __device__ constexpr int row_slot_doubles(int nf, bool) { return 2 * kRowSpec + nf * 256; }
 
 __host__ __device__ constexpr size_t inv_row_smem(int n, int count, bool err) {
-  return (size_t)row_warps(err) * (256 * 16 + 2 * (size_t)row_slot_doubles(n, err) * 8) + (size_t)n * count * 8 + 64;
+  return (size_t)row_warps(err, n) * (256 * 16 + 2 * (size_t)row_slot_doubles(n, err) * 8) + (size_t)n * count * 8 + 64;
 }
 
 template <int L, int NF, bool ERR>
-__global__ void __launch_bounds__(row_warps(ERR) * 32, 1) k_inv_row(InvRowArgs a) {
+__global__ void __launch_bounds__(row_warps(ERR, NF) * 32, 1) k_inv_row(InvRowArgs a) {
   extern __shared__ double2 sm[];
   if (a.io.mode == 1 && !a.io.ctl->running) return;
   using MN = Mono<NF>;
-  constexpr int kRowWarps = row_warps(ERR), kRowThreads = kRowWarps * 32;
+  constexpr int kRowWarps = row_warps(ERR, NF), kRowThreads = kRowWarps * 32;
   constexpr int LPL = L / 8, RPW = 32 / LPL;  // lanes per row, rows per warp
   constexpr int SLOT = row_slot_doubles(NF, ERR);
   const Resolved r = resolve(a.io);
@@ -3011,7 +3012,7 @@ void SpectralPlan::setup_pipes() {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   sms_ = std::max(1, sms);
   if ((M == 128 || M == 256) && poly_nf_ == n && n >= 1 && n <= 3 && nch >= 1 && nch <= 2 &&
-      inv_row_smem(n, poly_count_, true) <= 227 * 1024) {
+      std::max(inv_row_smem(n, poly_count_, true), inv_row_smem(n, poly_count_, false)) <= 227 * 1024) {
     bool ok = true;
     auto attr = [&](const void* fn, bool err) {
       ok &= cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -3214,9 +3215,9 @@ cudaError_t SpectralPlan::launch_inv_row(const RhsIO& io, cudaStream_t st) {
   a.io = io;
   const bool err = io.mode == 1 && io.stage == 7 && io.err_part != nullptr && io.err_aux != nullptr;
   const size_t smem = inv_row_smem(n, poly_count_, err);
-  const int rows_per_cta = row_warps(err) * (32 / (M / 8));
+  const int rows_per_cta = row_warps(err, n) * (32 / (M / 8));
   const int grid = std::max(1, std::min((R + rows_per_cta - 1) / rows_per_cta, sms_));  // one resident CTA per SM
-  const int threads = row_warps(err) * 32;
+  const int threads = row_warps(err, n) * 32;
   auto go = [&](auto lx) {
     constexpr int LX = decltype(lx)::value;
     if (err) {
