@@ -1012,7 +1012,10 @@ __host__ __device__ constexpr size_t mid2_smem(int L0) {
          2 * (size_t)L0 * 8 + 2 * 4 * 16;
 }
 
-template <int L, int NZ>
+// REALM: every multiplier is real (the operator groups' i^q rotations are all even, as
+// for the CGLE's second derivatives): each channel term is two products instead of a
+// complex product, in the complex product's rounding (no contraction).
+template <int L, int NZ, bool REALM>
 __global__ void __launch_bounds__(kMid2Threads, 1)
     k_mid_pipe2(const __grid_constant__ CUtensorMap tmF, const __grid_constant__ CUtensorMap tmC, MidPipeArgs a) {
   extern __shared__ char smraw[];
@@ -1102,15 +1105,26 @@ __global__ void __launch_bounds__(kMid2Threads, 1)
         double2 acc = make_double2(0.0, 0.0);
 #pragma unroll
         for (int s2 = 0; s2 < 2; ++s2) {
-          double2 m = mc[ch][s2];
+          if (REALM) {
+            double m = mc[ch][s2].x;
 #pragma unroll
-          for (int g = 0; g < NZ; ++g) {
-            const double bg = sbz[g * L + wl.ml + LPL * p];
-            const double2 r = srz[g * 4 + ch * 2 + s2];
-            m.x += bg * r.x;
-            m.y += bg * r.y;
+            for (int g = 0; g < NZ; ++g) {
+              const double bg = sbz[g * L + wl.ml + LPL * p];
+              m += bg * srz[g * 4 + ch * 2 + s2].x;
+            }
+            acc.x = __dadd_rn(acc.x, __dmul_rn(m, x[s2][p].x));
+            acc.y = __dadd_rn(acc.y, __dmul_rn(m, x[s2][p].y));
+          } else {
+            double2 m = mc[ch][s2];
+#pragma unroll
+            for (int g = 0; g < NZ; ++g) {
+              const double bg = sbz[g * L + wl.ml + LPL * p];
+              const double2 r = srz[g * 4 + ch * 2 + s2];
+              m.x += bg * r.x;
+              m.y += bg * r.y;
+            }
+            acc = c_add(acc, c_mul(m, x[s2][p]));
           }
-          acc = c_add(acc, c_mul(m, x[s2][p]));
         }
         out[ch] = inP ? acc : make_double2(0.0, 0.0);
       }
@@ -3004,6 +3018,17 @@ bool SpectralPlan::init(int n_, int ndim_, const int* Ns_, const double* Ls_,
 // 256-point axis-0 lines with at most two fields and no more channels than fields
 // (written over their sources); k_c2c_pipe with it for 128- or 256-point axis-1 lines.
 // Every other plan keeps the general kernels.
+using MidKernel = void (*)(const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, MidPipeArgs);
+
+static MidKernel mid2_kernel(int L0, int nz, bool real) {
+  if (L0 == 128) {
+    if (nz == 2) return real ? k_mid_pipe2<128, 2, true> : k_mid_pipe2<128, 2, false>;
+    return real ? k_mid_pipe2<128, 1, true> : k_mid_pipe2<128, 1, false>;
+  }
+  if (nz == 2) return real ? k_mid_pipe2<256, 2, true> : k_mid_pipe2<256, 2, false>;
+  return real ? k_mid_pipe2<256, 1, true> : k_mid_pipe2<256, 1, false>;
+}
+
 void SpectralPlan::setup_pipes() {
   pipe_mid_ = pipe_c2c_ = inv_row_ = false;
   if (ndim != 3) return;
@@ -3056,12 +3081,12 @@ void SpectralPlan::setup_pipes() {
   }
   mid2_ = mid_tab_ && mid_nz_ <= 2;
   if (mid2_) {
-    const void* f2 = Ns[0] == 128 ? (mid_nz_ == 2 ? (const void*)k_mid_pipe2<128, 2> : (const void*)k_mid_pipe2<128, 1>)
-                                  : (mid_nz_ == 2 ? (const void*)k_mid_pipe2<256, 2> : (const void*)k_mid_pipe2<256, 1>);
-    if (cudaFuncSetAttribute(f2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mid2_smem(Ns[0])) != cudaSuccess) {
-      cudaGetLastError();
-      mid2_ = false;
-    }
+    for (bool real : {false, true})
+      if (cudaFuncSetAttribute(mid2_kernel(Ns[0], mid_nz_, real), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)mid2_smem(Ns[0])) != cudaSuccess) {
+        cudaGetLastError();
+        mid2_ = false;
+      }
   }
   const size_t smem = mid_pipe_smem((int)grp.size(), kv_total_, mid_tab_ ? Ns[0] * nch * n : 0);
   if (smem > 227 * 1024) return;
@@ -3178,6 +3203,17 @@ cudaError_t SpectralPlan::build_mid_tables(const std::vector<ChanEntry>& grp, co
       }
     ++gz;
   }
+  // every multiplier real: the axis-0 pass's real form (the i^q rotations are fixed by the
+  // operators, so later coefficients keep the form)
+  bool real = true;
+  for (const double2& v : rz) real &= v.y == 0.0;
+  for (const double2& v : mc) real &= v.y == 0.0;
+  if (!mid_tables_built_) {
+    mid_real_ = real;
+    mid_tables_built_ = true;
+  } else if (mid_real_ && !real) {
+    return cudaErrorInvalidValue;
+  }
   if (!mid_bz_) RDCU_TRY(dev_alloc(&mid_bz_, bz.size() * sizeof(double)));
   if (!mid_rz_) RDCU_TRY(dev_alloc(&mid_rz_, rz.size() * sizeof(double2)));
   RDCU_TRY(cudaMemcpy(mid_bz_, bz.data(), bz.size() * sizeof(double), cudaMemcpyHostToDevice));
@@ -3267,17 +3303,7 @@ cudaError_t SpectralPlan::launch_mid_pipe(const RhsIO& io, cudaStream_t st) {
   if (mid2_) {
     const size_t sm2 = mid2_smem(Ns[0]);
     const int grid2 = std::max(1, std::min(a.ntiles, sms_));
-    if (Ns[0] == 128) {
-      if (mid_nz_ == 2)
-        k_mid_pipe2<128, 2><<<grid2, kMid2Threads, sm2, st>>>(tm_sf_, tm_sc_, a);
-      else
-        k_mid_pipe2<128, 1><<<grid2, kMid2Threads, sm2, st>>>(tm_sf_, tm_sc_, a);
-    } else {
-      if (mid_nz_ == 2)
-        k_mid_pipe2<256, 2><<<grid2, kMid2Threads, sm2, st>>>(tm_sf_, tm_sc_, a);
-      else
-        k_mid_pipe2<256, 1><<<grid2, kMid2Threads, sm2, st>>>(tm_sf_, tm_sc_, a);
-    }
+    mid2_kernel(Ns[0], mid_nz_, mid_real_)<<<grid2, kMid2Threads, sm2, st>>>(tm_sf_, tm_sc_, a);
     return cudaGetLastError();
   }
   const size_t smem = mid_pipe_smem(mid_ngrp_, kv_total_, mid_tab_ ? Ns[0] * nch * n : 0);

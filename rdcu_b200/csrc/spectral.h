@@ -172,6 +172,8 @@ class SpectralPlan {
   double2* mid_mz_ = nullptr;      // [L0][nch][n]
   double2* mid_mc_ = nullptr;      // [N1 * Mh][nch][n]
   bool mid2_ = false;              // k_mid_pipe2: at most two groups on axis 0 alone
+  bool mid_real_ = false;          // every multiplier of the tables is real
+  bool mid_tables_built_ = false;
   int mid_nz_ = 0;                 // their number
   double* mid_bz_ = nullptr;       // [max(1, mid_nz_)][L0] beta_g(z)
   double2* mid_rz_ = nullptr;      // [max(1, mid_nz_)][nch][n] i^q A_g
