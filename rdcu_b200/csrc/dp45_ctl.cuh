@@ -35,8 +35,12 @@ __device__ __forceinline__ void dp45_control(DP45Ctl* c, const double* part, dou
   __shared__ double red[kCtlThreads];
   const int tid = threadIdx.x;
   double s = 0.0;
-  if (!c->fixed)
-    for (int i = tid; i < c->nparts; i += kCtlThreads) s += part[i];
+  if (!c->fixed) {
+    // unrolled so that a thread's loads are in flight together; the sum keeps its order
+    const int np = c->nparts;
+#pragma unroll 16
+    for (int i = tid; i < np; i += kCtlThreads) s += part[i];
+  }
   red[tid] = s;
   __syncthreads();
   for (int w = kCtlThreads / 2; w > 0; w >>= 1) {
