@@ -246,7 +246,7 @@ def run_ours(args, rank, world, local_rank):
     passes = s.profile_passes(reps=10)
     peak, peak_kind = load_peaks()
     # the dominant pass is the one with the most device time per attempt
-    weights = [launches_per_attempt_of(p[0]) for p in passes]
+    weights = [launches_per_attempt_of(p[0], [q[0] for q in passes]) for p in passes]
     top = max(zip(passes, weights), key=lambda pw: pw[0][1] * pw[1])[0]
     achieved = top[2] / (top[1] / 1e3) / 1e9
     total_ms = sum(p[1] * w for p, w in zip(passes, weights))
@@ -904,10 +904,20 @@ def run_lines_reference(args):
     }
 
 
-def launches_per_attempt_of(name):
+def launches_per_attempt_of(name, names=()):
     """Launches of a pass in one DP45 attempt (stages 2-7): the forward and inverse
     x passes of stages 2-6 five times and their stage-7 forms once; the passes between
-    them (axis 0, and axis 1 unless the x passes do it) six times."""
+    them (axis 0, and axis 1 unless the x passes do it) six times.  With fused x passes
+    (`inv_fwd_row` among `names`: the inverse pass of stages 2-5 also does the next
+    stage's forward pass) the attempt runs stage 2's forward pass, the fused pass four
+    times, stage 6's inverse pass and stage 7's two x passes; the forward pass of stage 4
+    (`fwd_x`) is listed but does not run."""
+    if "inv_fwd_row" in names:
+        fused = {"fwd_x_stage2": 1, "inv_fwd_row": 4, "inv_x_dictionary": 1, "fwd_x_stage7": 1,
+                 "inv_x_stage7": 1, "fwd_x": 0}
+        if name in fused:
+            return fused[name]
+        return 6
     if name.endswith("_stage7"):
         return 1
     if name.startswith("fwd_") or name.startswith("inv_"):

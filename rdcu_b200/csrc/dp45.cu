@@ -122,8 +122,8 @@ bool DP45Engine::init(SpectralPlan* sp, double atol, double rtol, int fixed, cud
   const int np = std::max(1, sp->nparts_max);
   if (cudaMalloc((void**)&err_part_, np * sizeof(double)) != cudaSuccess) return fail("error partials");
   if (!fixed && sp->wants_err_aux()) {
-    if (cudaMalloc((void**)&err_aux_, 2 * sb) != cudaSuccess) return fail("error terms");
-    device_bytes += 2 * sb;
+    if (cudaMalloc((void**)&err_aux_, sb) != cudaSuccess) return fail("error terms");
+    device_bytes += sb;
   }
   if (cudaMalloc((void**)&d_ctl_, sizeof(DP45Ctl)) != cudaSuccess) return fail("controller");
   if (cudaMalloc((void**)&log_h_, log_cap_ * sizeof(double)) != cudaSuccess) return fail("log");
@@ -239,6 +239,17 @@ cudaError_t DP45Engine::arm(int check, double t1, double hmin, double hmax, int 
   return cudaGetLastError();
 }
 
+RhsIO DP45Engine::stage_io(int s) const {
+  RhsIO io{};
+  io.mode = 1;
+  io.stage = s;
+  io.bufs = bufs;
+  io.ctl = d_ctl_;
+  io.err_part = (s == 7 && !fixed_) ? err_part_ : nullptr;
+  io.err_aux = (s == 7 && !fixed_) ? err_aux_ : nullptr;
+  return io;
+}
+
 cudaError_t DP45Engine::launch_k1() {
   RhsIO io{};
   io.mode = 1;
@@ -269,16 +280,16 @@ cudaError_t DP45Engine::set_h_async(double h) {
 }
 
 cudaError_t DP45Engine::launch_attempt_capture(double* const* ytemp_out) {
+  RhsIO io[8];
+  for (int s = 2; s <= 7; ++s) io[s] = stage_io(s);
+  for (int s = 2; s <= 6; ++s)
+    if (ytemp_out) io[s].ytemp_out = ytemp_out[s];
+  // a stage's inverse x pass may also do the next stage's forward x pass
+  bool fwd_done = false;
   for (int s = 2; s <= 7; ++s) {
-    RhsIO io{};
-    io.mode = 1;
-    io.stage = s;
-    io.bufs = bufs;
-    io.ctl = d_ctl_;
-    io.err_part = (s == 7 && !fixed_) ? err_part_ : nullptr;
-    io.err_aux = (s == 7 && !fixed_) ? err_aux_ : nullptr;
-    if (ytemp_out && s <= 6) io.ytemp_out = ytemp_out[s];
-    RDCU_TRY(sp_->run(io, st_));
+    bool fused = false;
+    RDCU_TRY(sp_->run(io[s], st_, s < 7 ? &io[s + 1] : nullptr, fwd_done, &fused));
+    fwd_done = fused;
   }
   k_dp45_ctl<<<1, kCtlThreads, 0, st_>>>(d_ctl_, err_part_, log_h_, log_t_, log_acc_, (double)nN_,
                                          d_teval_);
@@ -368,25 +379,28 @@ cudaError_t DP45Engine::profile(int reps, std::vector<SpectralPlan::PassTime>* o
     RDCU_TRY(launch_k1());
     k1_valid_ = true;
   }
-  RhsIO io{};
-  io.mode = 1;
-  io.stage = 4;
-  io.bufs = bufs;
-  io.ctl = d_ctl_;
-  RDCU_TRY(sp_->profile(io, reps, st_, out));
+  RhsIO io4 = stage_io(4), io5 = stage_io(5);
+  RDCU_TRY(sp_->profile(io4, reps, st_, out, &io5));
   // stage 7: the stage combination over six slopes, and (adaptive steps) the inverse
   // pass with the error epilogue
   std::vector<SpectralPlan::PassTime> p7;
-  io.stage = 7;
-  io.err_part = fixed_ ? nullptr : err_part_;
-  io.err_aux = fixed_ ? nullptr : err_aux_;
-  RDCU_TRY(sp_->profile(io, reps, st_, &p7));
+  RDCU_TRY(sp_->profile(stage_io(7), reps, st_, &p7));
   for (const auto& p : p7) {
     const std::string nm = p.name;
     if (nm == "fwd_x") out->push_back({"fwd_x_stage7", p.ms, p.bytes});
     if (nm == "inv_x_dictionary") out->push_back({"inv_x_stage7", p.ms, p.bytes});
     if (nm == "fwd_plane") out->push_back({"fwd_plane_stage7", p.ms, p.bytes});
     if (nm == "inv_plane") out->push_back({"inv_plane_stage7", p.ms, p.bytes});
+  }
+  bool fused = false;
+  for (const auto& p : *out) fused |= std::string(p.name) == "inv_fwd_row";
+  if (fused) {
+    // with fused x passes stage 2's forward pass runs alone (stages 3..6 get theirs from
+    // the inverse pass before them)
+    std::vector<SpectralPlan::PassTime> p2;
+    RDCU_TRY(sp_->profile(stage_io(2), reps, st_, &p2));
+    for (const auto& p : p2)
+      if (std::string(p.name) == "fwd_x") out->push_back({"fwd_x_stage2", p.ms, p.bytes});
   }
   // leave the controller idle, as after a completed attempt
   k_dp45_arm<<<1, 1, 0, st_>>>(d_ctl_, 0, INFINITY, 0.0, INFINITY, 0, 0, 1);

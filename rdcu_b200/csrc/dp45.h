@@ -48,6 +48,8 @@ class DP45Engine {
   // (entries may be null) instead of the scratch state slot
   cudaError_t launch_attempt_capture(double* const* ytemp_out);
   cudaError_t launch_k1();
+  // the RhsIO of DP45 stage s (2..7) of this engine's attempt
+  RhsIO stage_io(int s) const;
   // device copy of the current state y (slot chosen on the device); no sync
   cudaError_t copy_current_y(double* dst);
   // sets the step size of the next attempt on the device; no sync
@@ -95,7 +97,7 @@ class DP45Engine {
   cudaGraphExec_t graph_exec_ = nullptr;
   cudaGraph_t graph_ = nullptr;
   int graph_gen_ = -1;  // the plan's buffers_gen when the attempt graph was captured
-  double* err_aux_ = nullptr;  // stage-7 error terms (2 * nN doubles) when the plan wants them
+  double* err_aux_ = nullptr;  // stage-7 slope sums (nN doubles) when the plan wants them
   cudaError_t ensure_graph();
 };
 

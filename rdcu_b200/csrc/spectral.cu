@@ -65,8 +65,8 @@ struct Resolved {
   const double* k[7] = {};
   double h = 0, atol = 0, rtol = 0;
   int stage = 0;
-  double* aux = nullptr;       // stage 7: the error terms fwd_x writes (RhsIO::err_aux)
-  long long nN = 0;            // its half length (set by the pass that uses it)
+  double* aux = nullptr;       // stage 7: the slope sums fwd_x writes (RhsIO::err_aux)
+  long long nN = 0;            // n * N (set by the pass that uses it)
 };
 
 __device__ __forceinline__ Resolved resolve(const RhsIO& io) {
@@ -98,12 +98,15 @@ __device__ __forceinline__ Resolved resolve(const RhsIO& io) {
   return r;
 }
 
-// Stage 7's error terms at point i from y, the slopes and the new state ynew, in
-// k_inv_x's operation order: the slope sum without e_7 k_7 (e_2 = 0) and the scale.
-__device__ __forceinline__ void stage7_error_terms(long long i, double ynew, const Resolved& r, double* es_p,
-                                                   double* den) {
-  *es_p = c_e[0] * r.k[0][i] + c_e[2] * r.k[2][i] + c_e[3] * r.k[3][i] + c_e[4] * r.k[4][i] + c_e[5] * r.k[5][i];
-  *den = r.atol + r.rtol * fmax(fabs(r.y[i]), fabs(ynew));
+// Stage 7's error term at point i from the slopes, in k_inv_x's operation order: the
+// slope sum without e_7 k_7 (e_2 = 0).
+__device__ __forceinline__ double stage7_slope_sum(long long i, const Resolved& r) {
+  return c_e[0] * r.k[0][i] + c_e[2] * r.k[2][i] + c_e[3] * r.k[3][i] + c_e[4] * r.k[4][i] + c_e[5] * r.k[5][i];
+}
+// the error scale atol + rtol max(|y|, |y_new|) (dp45.cu:79-84); the inverse pass forms
+// it from y and the stage-7 state it reads anyway, bitwise the value of the forward pass
+__device__ __forceinline__ double stage7_scale(const Resolved& r, double y, double ynew) {
+  return r.atol + r.rtol * fmax(fabs(y), fabs(ynew));
 }
 
 // Stage states follow the reference kernels' arithmetic order (dp45.cu:34-69): stage 2
@@ -296,12 +299,7 @@ __device__ __forceinline__ void fwd_load(const FwdXArgs& a, const Resolved& r, d
       const int e = e0 + u * T;
       if (e >= nel) break;
       if (r.ytemp && gi[u] >= 0) r.ytemp[gi[u]] = v[u];
-      if (S == 7 && r.aux && gi[u] >= 0) {
-        double es_p, den;
-        stage7_error_terms(gi[u], v[u], r, &es_p, &den);
-        r.aux[gi[u]] = es_p;
-        r.aux[r.nN + gi[u]] = den;
-      }
+      if (S == 7 && r.aux && gi[u] >= 0) r.aux[gi[u]] = stage7_slope_sum(gi[u], r);
       if (a.do_fft) {
         const int pl = fdivc<2 * LX>(e, a.d2M);
         const int w = e - pl * 2 * M;
@@ -339,9 +337,9 @@ __device__ __forceinline__ double2 stage_value_t2(long long i, const Resolved& r
   return make_double2(yi.x + r.h * ax, yi.y + r.h * ay);
 }
 
-// Stage 7 at the two points i, i+1 with the error terms from the same loads: the new
-// state (stage_value_t2<7>'s arithmetic) and stage7_error_terms' slope sum and scale.
-__device__ __forceinline__ double2 stage7_value_terms2(long long i, const Resolved& r, double2* es_p, double2* den) {
+// Stage 7 at the two points i, i+1 with the error term from the same loads: the new
+// state (stage_value_t2<7>'s arithmetic) and stage7_slope_sum's slope sum.
+__device__ __forceinline__ double2 stage7_value_terms2(long long i, const Resolved& r, double2* es_p) {
   const double2 yi = *reinterpret_cast<const double2*>(r.y + i);
   const double2 k0 = *reinterpret_cast<const double2*>(r.k[0] + i);
   const double2 k2 = *reinterpret_cast<const double2*>(r.k[2] + i);
@@ -360,8 +358,6 @@ __device__ __forceinline__ double2 stage7_value_terms2(long long i, const Resolv
   const double2 v = make_double2(yi.x + r.h * ax, yi.y + r.h * ay);
   es_p->x = c_e[0] * k0.x + c_e[2] * k2.x + c_e[3] * k3.x + c_e[4] * k4.x + c_e[5] * k5.x;
   es_p->y = c_e[0] * k0.y + c_e[2] * k2.y + c_e[3] * k3.y + c_e[4] * k4.y + c_e[5] * k5.y;
-  den->x = r.atol + r.rtol * fmax(fabs(yi.x), fabs(v.x));
-  den->y = r.atol + r.rtol * fmax(fabs(yi.y), fabs(v.y));
   return v;
 }
 
@@ -392,11 +388,10 @@ __device__ __forceinline__ void fwd_load2(const FwdXArgs& a, const Resolved& r, 
         if (g < a.nrows) {
           gi[u] = g * LX + x;
           if (terms) {
-            // the error terms leave at once (no registers held across the unrolled loads)
-            double2 es_p, den;
-            v[u] = stage7_value_terms2(gi[u], r, &es_p, &den);
+            // the error term leaves at once (no registers held across the unrolled loads)
+            double2 es_p;
+            v[u] = stage7_value_terms2(gi[u], r, &es_p);
             *reinterpret_cast<double2*>(r.aux + gi[u]) = es_p;
-            *reinterpret_cast<double2*>(r.aux + r.nN + gi[u]) = den;
           } else {
             v[u] = stage_value_t2<S>(gi[u], r);
           }
@@ -1162,6 +1157,7 @@ __global__ void __launch_bounds__(kMid2Threads, 1)
 // consecutive boxes, one line per warp (256 points) or half warp (128 points).
 struct C2CPipeArgs {
   int nbox, nchunk, ntiles;
+  int rev;  // take the tiles from the last to the first
   const double2* tw;
   RhsIO io;
   int* err;
@@ -1191,9 +1187,10 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
   const int coff = (li >> 3) * BOXB, c = li & 7;
   WarpLine<L> wl;
   wl.init(a.tw, lane % LPL);
-  // the inverse pass takes its tiles in reverse order: it ends on the planes the row
-  // kernel after it starts with, which are then still in L2
-  auto order = [&](int tile) { return INV ? a.ntiles - 1 - tile : tile; };
+  // the inverse pass takes its tiles in reverse order before a row kernel (it ends on
+  // the planes the row kernel starts with, which are then still in L2) and in order
+  // before a fused row kernel, which takes its rows from the last to the first
+  auto order = [&](int tile) { return a.rev ? a.ntiles - 1 - tile : tile; };
   auto issue = [&](int tile, int b) {
     const int b0 = order(tile) * BPT, nb = min(BPT, a.nbox - b0);
     mbar_expect_tx(&full[b], (unsigned)(nb * BOXB));
@@ -1723,8 +1720,8 @@ struct InvRowArgs {
   RhsIO io;
 };
 // Warps per CTA: ten for at most two fields (168 registers each; their staging fits),
-// else eight; eight with the stage-7 error epilogue, which reads each row's error terms
-// straight into registers before the row's transform (255 registers).
+// else eight; eight with the stage-7 error epilogue, which reads each row's slope sums
+// and y straight into registers before the row's transform (255 registers).
 __host__ __device__ constexpr int row_warps(bool err, int nf) { return err || nf > 2 ? 8 : 10; }
 // one staging slot of a warp: 2 channels x (at most 129 + padding) spectral values and
 // NF x 256 field values (two rows of 128 points take the same room)
@@ -1800,9 +1797,10 @@ __global__ void __launch_bounds__(row_warps(ERR, NF) * 32, 1) k_inv_row(InvRowAr
     __syncwarp();  // this row's copies (every lane's) landed
     const double2* sp = slot_spec(k);
     const double* su = slot_u(k);
-    // ERR: the row's error terms at the lane's points (slope part, then scale), loaded
-    // before the transform so that it covers their latency
-    double es_t[ERR ? 8 : 1][NF], den_t[ERR ? 8 : 1][NF];
+    // ERR: the row's slope sums and y at the lane's points (y gives the error scale with
+    // the staged stage-7 state), loaded before the transform so that it covers their
+    // latency
+    double es_t[ERR ? 8 : 1][NF], y_t[ERR ? 8 : 1][NF];
     if (ERR && live) {
 #pragma unroll
       for (int p = 0; p < 8; ++p)
@@ -1810,7 +1808,7 @@ __global__ void __launch_bounds__(row_warps(ERR, NF) * 32, 1) k_inv_row(InvRowAr
         for (int i = 0; i < NF; ++i) {
           const long long gi = i * RL + row * L + ml + LPL * p;
           es_t[ERR ? p : 0][i] = r.aux[gi];
-          den_t[ERR ? p : 0][i] = r.aux[nN + gi];
+          y_t[ERR ? p : 0][i] = r.y[gi];
         }
     }
     double2 v[8];
@@ -1861,9 +1859,9 @@ __global__ void __launch_bounds__(row_warps(ERR, NF) * 32, 1) k_inv_row(InvRowAr
         for (int m = 0; m < MN::count; ++m) acc += ci[m] * mono[m];
         if (live) r.f[i * RL + row * L + x] = acc;
         if (ERR) {
-          // k_inv_x's error kernel (dp45.cu:79-84) from the forward pass's terms
+          // k_inv_x's error kernel (dp45.cu:79-84) from the forward pass's slope sum
           const double es = es_t[ERR ? p : 0][i] + c_e[6] * acc;
-          const double ev = r.h * es / den_t[ERR ? p : 0][i];
+          const double ev = r.h * es / stage7_scale(r, y_t[ERR ? p : 0][i], u[i]);
           err2 += ev * ev;
         }
       }
@@ -1880,6 +1878,192 @@ __global__ void __launch_bounds__(row_warps(ERR, NF) * 32, 1) k_inv_row(InvRowAr
 #pragma unroll
       for (int o = LPL / 2; o > 0; o >>= 1) sacc += __shfl_xor_sync(0xffffffffu, sacc, o);
       if (ml == 0 && live) a.io.err_part[row] = sacc;
+    }
+    __syncwarp();  // the next row's transform and the copies after it rewrite the line and this slot
+  }
+  cp_async_wait_all();
+}
+
+// ---- the inverse x pass of DP45 stage s fused with the forward x pass of stage s + 1
+// (s = 2..5; 3D grids with 128- or 256-point rows, two fields, a dense-polynomial
+// dictionary of at most two channels).  Per row, k_inv_row's steps (staged channel spectra
+// and fields, inverse transform, dictionary, slope k_s written), then stage s + 1 at the
+// lane's points: its state from y, the slopes before k_s (read while the inverse
+// transform runs) and k_s still in registers -- stage_value_t2's terms in its order --
+// written out, then transformed forward as one complex line (field 0 real part, field 1
+// imaginary part) and split into the two fields' half spectra with k_fwd_x's formulas.
+// Against separate launches this saves reading k_s back and one launch per stage.
+// k_fwd_x pairs two rows of one field in a line instead, so the spectra agree with its
+// spectra to rounding; the stage states are the same arithmetic.  Stage 7's forward pass
+// stays separate: with its error terms the fused kernel ran out of registers (spills;
+// 256^3: 0.75 ms against 0.57 ms for the two kernels).
+struct InvFwdRowArgs {
+  InvRowArgs inv;  // stage s: channel spectra in, slope k_s out
+  RhsIO io2;       // stage s + 1: its state out
+  double2* Sf;     // stage s + 1's field half spectra [field][row][Mh]
+};
+constexpr int kFuseWarps = 8;
+__host__ __device__ constexpr size_t inv_fwd_row_smem(int count) {
+  return (size_t)kFuseWarps * (256 * 16 + 2 * (size_t)row_slot_doubles(2, false) * 8) + (size_t)2 * count * 8 + 64;
+}
+
+template <int L, int S2>
+__global__ void __launch_bounds__(kFuseWarps * 32, 1) k_inv_fwd_row(const __grid_constant__ InvFwdRowArgs fa) {
+  static_assert(S2 >= 3 && S2 <= 6, "the stage after an inverse pass of stages 2..5");
+  extern __shared__ double2 sm[];
+  const InvRowArgs& a = fa.inv;
+  if (!a.io.ctl->running) return;
+  constexpr int NF = 2;
+  using MN = Mono<NF>;
+  constexpr int LPL = L / 8, RPW = 32 / LPL;  // lanes per row, rows per warp
+  constexpr int SLOT = row_slot_doubles(NF, false);
+  constexpr int NEW = S2 - 2;  // slot of k_s among stage S2's slopes
+  const Resolved r = resolve(a.io);
+  const Resolved r2 = resolve(fa.io2);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  double* stage = reinterpret_cast<double*>(sm + kFuseWarps * 256);
+  double* spoly = stage + kFuseWarps * 2 * SLOT;
+  int* sfold = reinterpret_cast<int*>(spoly + NF * MN::count);
+  for (int t = tid; t < NF * MN::count; t += kFuseWarps * 32) spoly[t] = a.dict.poly[t];
+  for (int t = tid; t < NF; t += kFuseWarps * 32) sfold[t] = a.dict.fold[t];
+  __syncthreads();
+  const int sub = lane / LPL, ml = lane % LPL;
+  double2* line = sm + warp * 256 + sub * L;
+  WarpLine<L> wl;
+  wl.init(a.tw, ml);
+  const long long RL = (long long)a.R * L;
+  const bool a16 = ((reinterpret_cast<unsigned long long>(r.u) | reinterpret_cast<unsigned long long>(a.Sc)) & 15) == 0;
+  const int Mh = a.Mh, nch = a.nch;
+  const long long wstride = (long long)gridDim.x * kFuseWarps * RPW;
+  auto slot_spec = [&](int k) { return reinterpret_cast<double2*>(stage + (warp * 2 + k) * SLOT) + sub * (kRowSpec / RPW); };
+  auto slot_u = [&](int k) { return stage + (warp * 2 + k) * SLOT + 2 * kRowSpec + sub * NF * L; };
+  // the rows go from the last to the first (q counts them): the axis-1 pass after this
+  // one starts on the first planes, which are then still in L2
+  auto fetch = [&](long long q, int k) {
+    if (q >= a.R) return;
+    const long long row = a.R - 1 - q;
+    double2* sp = slot_spec(k);
+    double* su = slot_u(k);
+    if (a16) {
+      for (int c = 0; c < nch; ++c)
+        for (int e = ml; e < Mh; e += LPL) cp_async16(sp + c * Mh + e, a.Sc + ((long long)c * a.R + row) * Mh + e, true);
+#pragma unroll
+      for (int f = 0; f < NF; ++f)
+#pragma unroll
+        for (int k2 = 0; k2 < L / 2 / LPL; ++k2) {
+          const int x2 = 2 * (ml + LPL * k2);
+          cp_async16(su + f * L + x2, r.u + f * RL + row * L + x2, true);
+        }
+    } else {
+      for (int c = 0; c < nch; ++c)
+        for (int e = ml; e < Mh; e += LPL) sp[c * Mh + e] = a.Sc[((long long)c * a.R + row) * Mh + e];
+      for (int f = 0; f < NF; ++f)
+        for (int k2 = 0; k2 < 8; ++k2) su[f * L + ml + LPL * k2] = r.u[f * RL + row * L + ml + LPL * k2];
+    }
+  };
+  long long row0 = ((long long)blockIdx.x * kFuseWarps + warp) * RPW;
+  fetch(row0 + sub, 0);
+  cp_async_commit();
+  int k = 0;
+  for (; row0 < a.R; row0 += wstride, k ^= 1) {
+    const bool live = row0 + sub < a.R;
+    const long long row = live ? a.R - 1 - (row0 + sub) : 0;
+    fetch(row0 + wstride + sub, k ^ 1);
+    cp_async_commit();
+    // stage S2's sums over the slopes before k_s at the lane's points, issued before the
+    // inverse transform so that it covers their latency
+    double yv[8][NF], ax[8][NF];
+#pragma unroll
+    for (int p = 0; p < 8; ++p)
+#pragma unroll
+      for (int i = 0; i < NF; ++i) {
+        double yy = 0.0, s = 0.0;
+        if (live) {
+          const long long gi = i * RL + row * L + ml + LPL * p;
+          yy = r2.y[gi];
+          s = c_a[S2][0] * r2.k[0][gi];
+          if (S2 >= 4) s += c_a[S2][1] * r2.k[1][gi];
+#pragma unroll
+          for (int j = 2; j < NEW; ++j) s += c_a[S2][j] * r2.k[j][gi];
+        }
+        yv[p][i] = yy;
+        ax[p][i] = s;
+      }
+    cp_async_wait_1();
+    __syncwarp();  // this row's copies (every lane's) landed
+    const double2* sp = slot_spec(k);
+    const double* su = slot_u(k);
+    double2 v[8];
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+      const int kx = ml + LPL * p;
+      const int kk = kx >= Mh ? L - kx : kx;
+      double2 Av = make_double2(0.0, 0.0), Bv = make_double2(0.0, 0.0);
+      if (live) {
+        Av = sp[kk];
+        if (nch > 1) Bv = sp[Mh + kk];
+      }
+      if (kx == 0 || 2 * kx == L) {
+        Av.y = 0.0;
+        Bv.y = 0.0;
+      }
+      if (kx >= Mh) {
+        Av.y = -Av.y;
+        Bv.y = -Bv.y;
+      }
+      v[p] = make_double2(Av.x - Bv.y, Av.y + Bv.x);
+    }
+    wl.template transform<true>(v, [line](int e) { return line + e; });
+#pragma unroll
+    for (int p = 0; p < 8; ++p) line[ml + LPL * p] = v[p];
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+      const int x = ml + LPL * p;
+      const double2 z = line[x];
+      double u[NF];
+#pragma unroll
+      for (int f = 0; f < NF; ++f) u[f] = su[f * L + x];
+      double mono[MN::count];
+      mono[0] = 1.0;
+#pragma unroll
+      for (int m = 1; m < MN::count; ++m) mono[m] = mono[MN::parent(m)] * u[MN::var(m)];
+#pragma unroll
+      for (int i = 0; i < NF; ++i) {
+        const int fc = sfold[i];
+        double acc = fc >= 0 ? ((fc & 1) ? z.y : z.x) : 0.0;
+        const double* ci = spoly + i * MN::count;
+#pragma unroll
+        for (int m = 0; m < MN::count; ++m) acc += ci[m] * mono[m];
+        const long long gi = i * RL + row * L + x;
+        // stage S2 at this point: k_s is its last slope term
+        double s = ax[p][i];
+        s += c_a[S2][NEW] * acc;
+        const double yn = yv[p][i] + r2.h * s;
+        if (live) {
+          r.f[gi] = acc;
+          if (r2.ytemp) r2.ytemp[gi] = yn;
+        }
+        yv[p][i] = yn;
+      }
+    }
+    __syncwarp();  // every lane's reads of the line are done before the forward transform
+#pragma unroll
+    for (int p = 0; p < 8; ++p) v[p] = make_double2(yv[p][0], yv[p][1]);
+    wl.template transform<false>(v, [line](int e) { return line + e; });
+#pragma unroll
+    for (int p = 0; p < 8; ++p) line[ml + LPL * p] = v[p];
+    __syncwarp();
+    if (live) {
+#pragma unroll
+      for (int p = 0; p < (L / 2 + LPL) / LPL; ++p) {
+        const int kx = ml + LPL * p;
+        if (kx < Mh) {
+          const double2 z = line[kx];
+          const double2 zm = line[kx == 0 ? 0 : L - kx];
+          fa.Sf[row * Mh + kx] = make_double2(0.5 * (z.x + zm.x), 0.5 * (z.y - zm.y));
+          fa.Sf[((long long)a.R + row) * Mh + kx] = make_double2(0.5 * (z.y + zm.y), -0.5 * (z.x - zm.x));
+        }
+      }
     }
     __syncwarp();  // the next row's transform and the copies after it rewrite the line and this slot
   }
@@ -1963,7 +2147,7 @@ __host__ __device__ constexpr size_t plane_inv_smem(int LX, int nf, int count) {
 
 // Stage values of the CTA's 32 rows of one (plane, field): row q of the CTA is global
 // row grow0 + C q; rows 2l and 2l + 1 become the real and imaginary parts of line l.
-// The stage state (and stage 7's error terms) leave as fwd_load2 writes them.
+// The stage state (and stage 7's slope sums) leave as fwd_load2 writes them.
 template <int S, int LX, int C>
 __device__ __forceinline__ void plane_load(const Resolved& r, double2* lines, long long grow0) {
   constexpr int kUnroll = 4, H = LX / 2, NP = 32 * H;
@@ -1978,10 +2162,9 @@ __device__ __forceinline__ void plane_load(const Resolved& r, double2* lines, lo
       const int q = e / H, x = 2 * (e - q * H);
       gi[u] = (grow0 + (long long)C * q) * LX + x;
       if (terms) {
-        double2 es_p, den;
-        v[u] = stage7_value_terms2(gi[u], r, &es_p, &den);
+        double2 es_p;
+        v[u] = stage7_value_terms2(gi[u], r, &es_p);
         *reinterpret_cast<double2*>(r.aux + gi[u]) = es_p;
-        *reinterpret_cast<double2*>(r.aux + r.nN + gi[u]) = den;
       } else {
         v[u] = stage_value_t2<S>(gi[u], r);
       }
@@ -2214,9 +2397,9 @@ __global__ void __launch_bounds__(kPlaneInvThreads, 1) k_inv_plane(PlaneArgs a) 
           const long long gi = i * RL + row * LX + x;
           r.f[gi] = acc;
           if (ERR) {
-            // k_inv_x's error kernel (dp45.cu:79-84) from the forward pass's terms
+            // k_inv_x's error kernel (dp45.cu:79-84) from the forward pass's slope sum
             const double es = r.aux[gi] + c_e[6] * acc;
-            const double ev = r.h * es / r.aux[nN + gi];
+            const double ev = r.h * es / stage7_scale(r, r.y[gi], uu[p][i]);
             err2 += ev * ev;
           }
         }
@@ -3030,7 +3213,7 @@ static MidKernel mid2_kernel(int L0, int nz, bool real) {
 }
 
 void SpectralPlan::setup_pipes() {
-  pipe_mid_ = pipe_c2c_ = inv_row_ = false;
+  pipe_mid_ = pipe_c2c_ = inv_row_ = fuse_rows_ = false;
   if (ndim != 3) return;
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
@@ -3060,6 +3243,25 @@ void SpectralPlan::setup_pipes() {
     }
     cudaGetLastError();
     inv_row_ = ok;
+    // the inverse x pass of a stage fused with the next stage's forward x pass (two
+    // fields); RDCU_FUSED_ROWS=0 keeps them separate
+    const char* fz = getenv("RDCU_FUSED_ROWS");
+    fuse_rows_ = inv_row_ && n == 2 && !(fz && fz[0] == '0') && inv_fwd_row_smem(poly_count_) <= 227 * 1024;
+    if (fuse_rows_) {
+      auto fattr = [&](auto lx) {
+        constexpr int LX = decltype(lx)::value;
+        const void* fns[] = {(const void*)k_inv_fwd_row<LX, 3>, (const void*)k_inv_fwd_row<LX, 4>,
+                             (const void*)k_inv_fwd_row<LX, 5>, (const void*)k_inv_fwd_row<LX, 6>};
+        for (const void* fn : fns)
+          fuse_rows_ &= cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)inv_fwd_row_smem(poly_count_)) == cudaSuccess;
+      };
+      if (M == 128)
+        fattr(std::integral_constant<int, 128>{});
+      else
+        fattr(std::integral_constant<int, 256>{});
+      cudaGetLastError();
+    }
   }
   if (!(Ns[0] == 128 || Ns[0] == 256) || !ch_sorted_ || nch < 1 || nch > n || n > 2) return;
   const long long I = (long long)Ns[1] * Mh;
@@ -3277,6 +3479,42 @@ cudaError_t SpectralPlan::launch_inv_row(const RhsIO& io, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+bool SpectralPlan::fuse_ok(const RhsIO& io, const RhsIO& next) const {
+  return fuse_rows_ && inv_row_ && io.mode == 1 && next.mode == 1 && io.ctl == next.ctl && io.stage >= 2 && io.stage <= 5 &&
+         next.stage == io.stage + 1 && !plane_inv_ok(io) && !plane_fwd_ok(next);
+}
+
+cudaError_t SpectralPlan::launch_inv_fwd_row(const RhsIO& io, const RhsIO& next, cudaStream_t st) {
+  InvFwdRowArgs f{};
+  f.inv.R = R;
+  f.inv.n = n;
+  f.inv.nch = nch;
+  f.inv.Mh = Mh;
+  f.inv.tw = tw_x_;
+  f.inv.Sc = Sc_;
+  f.inv.dict = dict_table();
+  f.inv.io = io;
+  f.io2 = next;
+  f.Sf = Sf_;
+  const size_t smem = inv_fwd_row_smem(poly_count_);
+  const int rows_per_cta = kFuseWarps * (32 / (M / 8));
+  const int grid = std::max(1, std::min((R + rows_per_cta - 1) / rows_per_cta, sms_));  // one resident CTA per SM
+  auto go = [&](auto lx) {
+    constexpr int LX = decltype(lx)::value;
+    switch (next.stage) {
+      case 3: k_inv_fwd_row<LX, 3><<<grid, kFuseWarps * 32, smem, st>>>(f); break;
+      case 4: k_inv_fwd_row<LX, 4><<<grid, kFuseWarps * 32, smem, st>>>(f); break;
+      case 5: k_inv_fwd_row<LX, 5><<<grid, kFuseWarps * 32, smem, st>>>(f); break;
+      default: k_inv_fwd_row<LX, 6><<<grid, kFuseWarps * 32, smem, st>>>(f); break;
+    }
+  };
+  if (M == 128)
+    go(std::integral_constant<int, 128>{});
+  else
+    go(std::integral_constant<int, 256>{});
+  return cudaGetLastError();
+}
+
 cudaError_t SpectralPlan::launch_mid_pipe(const RhsIO& io, cudaStream_t st) {
   MidPipeArgs a{};
   a.I = Ns[1] * Mh;
@@ -3321,8 +3559,9 @@ cudaError_t SpectralPlan::launch_mid_pipe(const RhsIO& io, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-cudaError_t SpectralPlan::launch_c2c_pipe(bool inv, int nplanes, cudaStream_t st, const RhsIO& io) {
+cudaError_t SpectralPlan::launch_c2c_pipe(bool inv, int nplanes, cudaStream_t st, const RhsIO& io, int rev) {
   C2CPipeArgs a{};
+  a.rev = rev < 0 ? (inv ? 1 : 0) : rev;
   a.nchunk = (Mh + 7) / 8;
   a.nbox = nplanes * a.nchunk;
   const int bpt = c2c_boxes(Ns[1]);
@@ -3441,7 +3680,7 @@ bool SpectralPlan::plane_fwd_ok(const RhsIO& io) const {
 }
 
 // the hot channel table in one launch; at stage 7 of an adaptive step with the forward
-// pass's error terms
+// pass's slope sums
 bool SpectralPlan::plane_inv_ok(const RhsIO& io) const {
   if (!plane_inv_) return false;
   const bool err_epilogue = io.mode == 1 && io.stage == 7 && io.err_part != nullptr;
@@ -3539,7 +3778,7 @@ void SpectralPlan::release() {
 // set the inverse x pass writes channels to Y.dat layout instead of the dictionary.
 cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, const std::vector<int>& hoff,
                                         int nch_run, int g_first, double* Yout, const int* ydst, cudaStream_t st,
-                                        int yplain) {
+                                        int yplain, const RhsIO* next, bool* fused) {
   const bool spectral = nch_run > 0;
   // the inverse x pass with the axis-1 transform: the hot table, every channel, no Y.dat
   const bool plane_inv = spectral && !Yout && ct.ent == ch_ent_ && g_first == 0 && nch_run == nch && plane_inv_ok(io);
@@ -3588,7 +3827,9 @@ cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, co
       a.io = io;
       dim3 grid(c2c_i_.grid, nch_run * Ns[0]);
       if (pipe_c2c_) {
-        RDCU_TRY(launch_c2c_pipe(true, nch_run * Ns[0], st, io));
+        // before a fused row kernel (rows from the last to the first) the tiles go in order
+        const bool to_fused = next && fused && fuse_ok(io, *next);
+        RDCU_TRY(launch_c2c_pipe(true, nch_run * Ns[0], st, io, to_fused ? 0 : 1));
       } else {
         prep(a);
         by_length(plan_ax_[1], c2c_i_.block, [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, true, decltype(lx)::value><<<grid, c2c_i_.block, c2c_i_.smem, st>>>(a); });
@@ -3615,8 +3856,13 @@ cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, co
   // forward pass left in err_aux; without them k_inv_x forms the error from y and slopes
   const bool err_epilogue = io.mode == 1 && io.stage == 7 && io.err_part != nullptr;
   if (plane_inv) return launch_plane_inv(io, st);
-  if (!Yout && inv_row_ && (!err_epilogue || io.err_aux) && ct.ent == ch_ent_ && g_first == 0 && nch_run == nch)
+  if (!Yout && inv_row_ && (!err_epilogue || io.err_aux) && ct.ent == ch_ent_ && g_first == 0 && nch_run == nch) {
+    if (next && fused && fuse_ok(io, *next)) {
+      *fused = true;
+      return launch_inv_fwd_row(io, *next, st);
+    }
     return launch_inv_row(io, st);
+  }
   for (int c0 = 0; c0 < std::max(1, nch_run); c0 += step) {
     const int cnt = spectral ? std::min(step, nch_run - c0) : 0;
     InvXArgs a{};
@@ -3650,14 +3896,16 @@ cudaError_t SpectralPlan::launch_passes(const RhsIO& io, const ChanTable& ct, co
   return cudaSuccess;
 }
 
-cudaError_t SpectralPlan::run(const RhsIO& io, cudaStream_t st) {
+cudaError_t SpectralPlan::run(const RhsIO& io, cudaStream_t st, const RhsIO* next, bool fwd_done, bool* fused) {
   const bool spectral = nch > 0;
   const bool need_fwd = spectral || (io.mode == 1 && io.stage >= 2);
+  if (fused) *fused = false;
+  if (!fused) next = nullptr;
   if (spectral && plane_fwd_ok(io)) {
     RDCU_TRY(launch_plane_fwd(io, st));
     return launch_passes(io, chan_table(ch_off_, ch_ent_, nch), h_ch_off_, nch, 0, nullptr, nullptr, st);
   }
-  if (need_fwd) {
+  if (need_fwd && !fwd_done) {
     FwdXArgs a{};
     a.M = M;
     a.Mh = Mh;
@@ -3692,7 +3940,7 @@ cudaError_t SpectralPlan::run(const RhsIO& io, cudaStream_t st) {
       RDCU_TRY(cudaGetLastError());
     }
   }
-  return launch_passes(io, chan_table(ch_off_, ch_ent_, nch), h_ch_off_, nch, 0, nullptr, nullptr, st);
+  return launch_passes(io, chan_table(ch_off_, ch_ent_, nch), h_ch_off_, nch, 0, nullptr, nullptr, st, 0, next, fused);
 }
 
 cudaError_t SpectralPlan::run_Y(const double* y, double* Yout, cudaStream_t st) {
@@ -3913,27 +4161,23 @@ cudaError_t SpectralPlan::precond(const double* r, double* z, double alpha, cons
   return cudaGetLastError();
 }
 
-cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, std::vector<PassTime>* out) {
+cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, std::vector<PassTime>* out,
+                                  const RhsIO* next) {
+  // Each round runs the stage's passes once in an attempt's order (forward x, axis 1,
+  // axis 0, axis 1, inverse x), so that every pass reads what the pass before it wrote
+  // from the stage's own inputs (the axis passes and the fused row pass work in place:
+  // repeating one of them alone would feed it its own output); one untimed round, then
+  // `reps` rounds with a pair of events around each launch.  With next, each round also
+  // runs the passes again up to the axis-1 pass and then the fused inverse/forward pass.
   out->clear();
-  cudaEvent_t e0, e1;
-  RDCU_TRY(cudaEventCreate(&e0));
-  RDCU_TRY(cudaEventCreate(&e1));
   const double spec_row = (double)R * Mh * 16.0;  // one field's half spectrum
   const double arr = (double)N * 8.0;             // one field's physical array
   const int s = io.stage >= 2 ? io.stage : 1;
   const int nk = s >= 2 ? (s == 7 ? s - 2 : s - 1) : 0;  // slopes the stage combination reads
-  auto timed = [&](const char* name, double bytes, auto&& launch) -> cudaError_t {
-    RDCU_TRY(launch());  // warm-up
-    RDCU_TRY(cudaEventRecord(e0, st));
-    for (int r = 0; r < reps; ++r) RDCU_TRY(launch());
-    RDCU_TRY(cudaEventRecord(e1, st));
-    RDCU_TRY(cudaEventSynchronize(e1));
-    float ms = 0;
-    RDCU_TRY(cudaEventElapsedTime(&ms, e0, e1));
-    out->push_back({name, ms / reps, bytes});
-    return cudaSuccess;
-  };
   const bool spectral = nch > 0;
+  const bool plane_fwd = spectral && plane_fwd_ok(io);
+  const bool plane_inv = spectral && plane_inv_ok(io);
+  const bool fused = next && fuse_ok(io, *next);
   FwdXArgs fa{};
   fa.M = M;
   fa.Mh = Mh;
@@ -3945,87 +4189,52 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
   fa.tw = tw_x_;
   fa.S = Sf_;
   fa.io = io;
-  // stage 7 with err_aux also writes the two error terms
-  const double aux_w = (io.mode == 1 && io.stage == 7 && io.err_part && io.err_aux) ? 2.0 : 0.0;
-  const double fwd_bytes = n * ((1 + nk) * arr + (s >= 2 ? arr : 0) + spec_row + aux_w * arr);
-  const bool plane_fwd = spectral && plane_fwd_ok(io);
-  const bool plane_inv = spectral && plane_inv_ok(io);
-  if (plane_fwd) {
-    RDCU_TRY(timed("fwd_plane", fwd_bytes, [&]() { return launch_plane_fwd(io, st); }));
-  } else {
-    RDCU_TRY(timed("fwd_x", fwd_bytes, [&]() {
-      prep(fa);
-      launch_fwd_x(plan_x_, fwd_.block, fwd_.grid, fwd_.smem, st, fa);
-      return cudaGetLastError();
-    }));
+  prep(fa);
+  C2CArgs cf{};
+  cf.La = Ns[1];
+  cf.I = Mh;
+  cf.TW = c2c_f_.per_cta;
+  cf.plan = plan_ax_[1];
+  cf.tw = tw_ax_[1];
+  cf.S = Sf_;
+  cf.io = io;
+  prep(cf);
+  const dim3 gcf(c2c_f_.grid, n * Ns[0]);
+  C2CArgs ci{};
+  ci.La = Ns[1];
+  ci.I = Mh;
+  ci.TW = c2c_i_.per_cta;
+  ci.plan = plan_ax_[1];
+  ci.tw = tw_ax_[1];
+  ci.S = Sc_;
+  ci.io = io;
+  prep(ci);
+  const dim3 gci(c2c_i_.grid, nch * Ns[0]);
+  const PassCfg& mc = mid_[0];
+  MidArgs m{};
+  m.L0 = Ns[0];
+  m.I = (ndim == 3) ? Ns[1] * Mh : Mh;
+  m.TW = mc.per_cta & 0xffff;
+  m.GB = mc.per_cta >> 16;
+  m.nsrc = n;
+  m.G = nch;
+  m.ch0 = 0;
+  m.ndim = ndim;
+  m.D1 = Ns[1];
+  m.Mh = Mh;
+  m.plan = plan_ax_[0];
+  m.tw = tw_ax_[0];
+  m.Sf = Sf_;
+  m.Sc = Sc_;
+  m.chan = chan_table(ch_off_, ch_ent_, nch);
+  m.io = io;
+  m.ent0 = 0;
+  m.nent = h_ch_off_[nch];
+  if (ch_sorted_ && nch <= m.GB) {
+    m.sorted = 1;
+    m.chan.ent = ch_sorted_;
   }
-  if (spectral && ndim == 3 && !plane_fwd) {
-    C2CArgs c{};
-    c.La = Ns[1];
-    c.I = Mh;
-    c.TW = c2c_f_.per_cta;
-    c.plan = plan_ax_[1];
-    c.tw = tw_ax_[1];
-    c.S = Sf_;
-    c.io = io;
-    dim3 grid(c2c_f_.grid, n * Ns[0]);
-    RDCU_TRY(timed("c2c_axis1_fwd", 2.0 * n * spec_row, [&]() {
-      if (pipe_c2c_) return launch_c2c_pipe(false, n * Ns[0], st, io);
-      prep(c);
-      by_length(plan_ax_[1], c2c_f_.block, [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, false, decltype(lx)::value><<<grid, c2c_f_.block, c2c_f_.smem, st>>>(c); });
-      return cudaGetLastError();
-    }));
-  }
-  if (spectral && ndim >= 2) {
-    const PassCfg& c = mid_[0];
-    MidArgs m{};
-    m.L0 = Ns[0];
-    m.I = (ndim == 3) ? Ns[1] * Mh : Mh;
-    m.TW = c.per_cta & 0xffff;
-    m.GB = c.per_cta >> 16;
-    m.nsrc = n;
-    m.G = nch;
-    m.ch0 = 0;
-    m.ndim = ndim;
-    m.D1 = Ns[1];
-    m.Mh = Mh;
-    m.plan = plan_ax_[0];
-    m.tw = tw_ax_[0];
-    m.Sf = Sf_;
-    m.Sc = Sc_;
-    m.chan = chan_table(ch_off_, ch_ent_, nch);
-    m.io = io;
-    m.ent0 = 0;
-    m.nent = h_ch_off_[nch];
-    if (ch_sorted_ && nch <= m.GB) {
-      m.sorted = 1;
-      m.chan.ent = ch_sorted_;
-    }
-    const size_t msmem = c.smem;
-    RDCU_TRY(timed("mid_axis0", (double)(n + nch) * spec_row, [&]() {
-      if (pipe_mid_) return launch_mid_pipe(io, st);
-      prep(m);
-      by_length(plan_ax_[0], c.block, [&](auto rs, auto lx) { k_mid<decltype(rs)::value, decltype(lx)::value><<<c.grid, c.block, msmem, st>>>(m); });
-      return cudaGetLastError();
-    }));
-    if (ndim == 3 && !plane_inv) {
-      C2CArgs a{};
-      a.La = Ns[1];
-      a.I = Mh;
-      a.TW = c2c_i_.per_cta;
-      a.plan = plan_ax_[1];
-      a.tw = tw_ax_[1];
-      a.S = Sc_;
-      a.io = io;
-      dim3 grid(c2c_i_.grid, nch * Ns[0]);
-      RDCU_TRY(timed("c2c_axis1_inv", 2.0 * nch * spec_row, [&]() {
-        if (pipe_c2c_) return launch_c2c_pipe(true, nch * Ns[0], st, io);
-        prep(a);
-        by_length(plan_ax_[1], c2c_i_.block, [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, true, decltype(lx)::value><<<grid, c2c_i_.block, c2c_i_.smem, st>>>(a); });
-        return cudaGetLastError();
-      }));
-    }
-  }
+  prep(m);
   InvXArgs a{};
   a.M = M;
   a.Mh = Mh;
@@ -4045,26 +4254,106 @@ cudaError_t SpectralPlan::profile(const RhsIO& io, int reps, cudaStream_t st, st
   inv_geometry(M, R, n, nch, false, plan_x_, &g, &tws, dict_smem_bytes());
   a.P = g.per_cta;
   a.tw_smem = tws;
+  prep(a);
+
+  // stage 7 with err_aux also writes each point's slope sum
+  const double aux_w = (io.mode == 1 && io.stage == 7 && io.err_part && io.err_aux) ? 1.0 : 0.0;
+  const double fwd_bytes = n * ((1 + nk) * arr + (s >= 2 ? arr : 0) + spec_row + aux_w * arr);
   // stage 7 of an adaptive step also reads y and five slopes for the error estimate, or
-  // the two error terms the forward pass wrote (err_aux)
+  // y and the slope sums the forward pass wrote (err_aux)
   const bool err_epilogue = io.mode == 1 && io.stage == 7 && io.err_part != nullptr;
   const double err_arrays = err_epilogue ? (io.err_aux ? 2.0 : 6.0) : 0.0;
   const double inv_bytes = nch * spec_row + 2.0 * n * arr + err_arrays * n * arr;
-  if (plane_inv) {
-    RDCU_TRY(timed("inv_plane", inv_bytes, [&]() { return launch_plane_inv(io, st); }));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    return cudaSuccess;
-  }
-  RDCU_TRY(timed("inv_x_dictionary", inv_bytes, [&]() {
+  // the fused pass: the inverse part's bytes, then the next stage's combination without
+  // the slope k_s (in registers)
+  const double fused_bytes =
+      fused ? nch * spec_row + 2.0 * n * arr + n * ((next->stage - 1) * arr + arr + spec_row) : 0.0;
+
+  auto go_fwd = [&]() -> cudaError_t {
+    if (plane_fwd) return launch_plane_fwd(io, st);
+    launch_fwd_x(plan_x_, fwd_.block, fwd_.grid, fwd_.smem, st, fa);
+    return cudaGetLastError();
+  };
+  auto go_c2c_f = [&]() -> cudaError_t {
+    if (pipe_c2c_) return launch_c2c_pipe(false, n * Ns[0], st, io);
+    by_length(plan_ax_[1], c2c_f_.block, [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, false, decltype(lx)::value><<<gcf, c2c_f_.block, c2c_f_.smem, st>>>(cf); });
+    return cudaGetLastError();
+  };
+  auto go_mid = [&]() -> cudaError_t {
+    if (pipe_mid_) return launch_mid_pipe(io, st);
+    by_length(plan_ax_[0], mc.block, [&](auto rs, auto lx) { k_mid<decltype(rs)::value, decltype(lx)::value><<<mc.grid, mc.block, mc.smem, st>>>(m); });
+    return cudaGetLastError();
+  };
+  // rev: the axis-1 inverse pass's tile order (in order before the fused row pass)
+  auto go_c2c_i = [&](int rev) -> cudaError_t {
+    if (pipe_c2c_) return launch_c2c_pipe(true, nch * Ns[0], st, io, rev);
+    by_length(plan_ax_[1], c2c_i_.block, [&](auto rs, auto lx) { k_c2c<decltype(rs)::value, true, decltype(lx)::value><<<gci, c2c_i_.block, c2c_i_.smem, st>>>(ci); });
+    return cudaGetLastError();
+  };
+  auto go_inv = [&]() -> cudaError_t {
+    if (plane_inv) return launch_plane_inv(io, st);
     if (inv_row_ && !(io.mode == 1 && io.stage == 7 && io.err_part != nullptr && !io.err_aux))
       return launch_inv_row(io, st);
-    prep(a);
     by_length(plan_x_, g.block, [&](auto rs, auto lx) { k_inv_x<decltype(rs)::value, decltype(lx)::value><<<g.grid, g.block, g.smem, st>>>(a); });
     return cudaGetLastError();
-  }));
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  };
+
+  // the passes reported, in order
+  std::vector<PassTime> tab;
+  tab.push_back({plane_fwd ? "fwd_plane" : "fwd_x", 0.0, fwd_bytes});
+  const int i_c2c_f = (spectral && ndim == 3 && !plane_fwd) ? (int)tab.size() : -1;
+  if (i_c2c_f >= 0) tab.push_back({"c2c_axis1_fwd", 0.0, 2.0 * n * spec_row});
+  const int i_mid = (spectral && ndim >= 2) ? (int)tab.size() : -1;
+  if (i_mid >= 0) tab.push_back({"mid_axis0", 0.0, (double)(n + nch) * spec_row});
+  const int i_c2c_i = (spectral && ndim == 3 && !plane_inv) ? (int)tab.size() : -1;
+  if (i_c2c_i >= 0) tab.push_back({"c2c_axis1_inv", 0.0, 2.0 * nch * spec_row});
+  const int i_inv = (int)tab.size();
+  tab.push_back({plane_inv ? "inv_plane" : "inv_x_dictionary", 0.0, inv_bytes});
+  const int i_fused = fused ? (int)tab.size() : -1;
+  if (fused) tab.push_back({"inv_fwd_row", 0.0, fused_bytes});
+
+  std::vector<cudaEvent_t> ev;
+  std::vector<int> which;
+  cudaError_t err = cudaSuccess;
+  // one launch: untimed (idx < 0 or a warm-up round) or between two new events
+  auto one = [&](bool rec, int idx, auto&& go) -> cudaError_t {
+    if (!rec || idx < 0) return go();
+    cudaEvent_t e0, e1;
+    RDCU_TRY(cudaEventCreate(&e0));
+    ev.push_back(e0);
+    RDCU_TRY(cudaEventCreate(&e1));
+    ev.push_back(e1);
+    which.push_back(idx);
+    RDCU_TRY(cudaEventRecord(e0, st));
+    RDCU_TRY(go());
+    return cudaEventRecord(e1, st);
+  };
+  auto round = [&](bool rec) -> cudaError_t {
+    RDCU_TRY(one(rec, 0, go_fwd));
+    if (i_c2c_f >= 0) RDCU_TRY(one(rec, i_c2c_f, go_c2c_f));
+    if (i_mid >= 0) RDCU_TRY(one(rec, i_mid, go_mid));
+    if (i_c2c_i >= 0) RDCU_TRY(one(rec, i_c2c_i, [&]() { return go_c2c_i(-1); }));
+    RDCU_TRY(one(rec, i_inv, go_inv));
+    if (fused) {
+      RDCU_TRY(go_fwd());
+      if (i_c2c_f >= 0) RDCU_TRY(go_c2c_f());
+      if (i_mid >= 0) RDCU_TRY(go_mid());
+      if (i_c2c_i >= 0) RDCU_TRY(go_c2c_i(0));
+      RDCU_TRY(one(rec, i_fused, [&]() { return launch_inv_fwd_row(io, *next, st); }));
+    }
+    return cudaSuccess;
+  };
+  err = round(false);
+  for (int r = 0; r < reps && err == cudaSuccess; ++r) err = round(true);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+  for (size_t k = 0; k < which.size() && err == cudaSuccess; ++k) {
+    float ms = 0;
+    err = cudaEventElapsedTime(&ms, ev[2 * k], ev[2 * k + 1]);
+    tab[which[k]].ms += ms / reps;
+  }
+  for (cudaEvent_t e : ev) cudaEventDestroy(e);
+  if (err != cudaSuccess) return err;
+  *out = tab;
   return cudaSuccess;
 }
 

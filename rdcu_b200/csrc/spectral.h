@@ -27,10 +27,11 @@ struct RhsIO {
   DP45Ctl* ctl = nullptr;     // mode 1
   double* err_part = nullptr; // mode 1, stage 7: per-CTA partial sums of err^2
   double* ytemp_out = nullptr;// mode 1, stages >= 2: write the stage state here instead of its slot
-  // mode 1, stage 7 of an adaptive step (plans with wants_err_aux()): 2 * nN doubles
-  // the forward pass fills with each point's error terms -- the slope part
-  // sum_{j != 2, 7} e_j k_j and the scale atol + rtol max(|y|, |y_new|) -- which the
-  // inverse pass completes with e_7 k_7 instead of reading y and five slopes again
+  // mode 1, stage 7 of an adaptive step (plans with wants_err_aux()): nN doubles the
+  // forward pass fills with each point's slope sum sum_{j != 2, 7} e_j k_j, which the
+  // inverse pass completes with e_7 k_7 (and divides by the scale atol + rtol
+  // max(|y|, |y_new|), from y and the stage state it reads) instead of reading five
+  // slopes again
   double* err_aux = nullptr;
 };
 
@@ -71,8 +72,11 @@ class SpectralPlan {
   void release();
   ~SpectralPlan() { release(); }
 
-  // f = RHS(y) on `stream` (mode 0) or one DP45 stage (mode 1).
-  cudaError_t run(const RhsIO& io, cudaStream_t stream);
+  // f = RHS(y) on `stream` (mode 0) or one DP45 stage (mode 1).  A DP45 stage may also
+  // do the forward x pass of the stage after it (next, when fused is given): *fused
+  // tells whether it did; the run of that next stage then passes fwd_done = true.
+  cudaError_t run(const RhsIO& io, cudaStream_t stream, const RhsIO* next = nullptr, bool fwd_done = false,
+                  bool* fused = nullptr);
   // All complex Y blocks (Y.dat layout) of y, written to Yout (device).
   cudaError_t run_Y(const double* y, double* Yout, cudaStream_t stream);
 
@@ -82,7 +86,9 @@ class SpectralPlan {
     double bytes;
   };
   // Times every pass of one RHS evaluation (io) `reps` times each.
-  cudaError_t profile(const RhsIO& io, int reps, cudaStream_t stream, std::vector<PassTime>* out);
+  // With next (the stage after io), also the fused inverse/forward pass of the two.
+  cudaError_t profile(const RhsIO& io, int reps, cudaStream_t stream, std::vector<PassTime>* out,
+                      const RhsIO* next = nullptr);
 
   // FFT-only plan for the BDF preconditioner: z = (I + alpha*J_lin)^-1 r with J_lin
   // the constant-coefficient linear FD operator of `lin` (solved mode by mode).
@@ -183,8 +189,13 @@ class SpectralPlan {
   void setup_pipes();
   bool encode_sc_map();
   cudaError_t launch_mid_pipe(const RhsIO& io, cudaStream_t stream);
-  cudaError_t launch_c2c_pipe(bool inv, int nplanes, cudaStream_t stream, const RhsIO& io);
+  // rev: tiles from the last to the first (-1: the inverse pass does, the forward pass not)
+  cudaError_t launch_c2c_pipe(bool inv, int nplanes, cudaStream_t stream, const RhsIO& io, int rev = -1);
   cudaError_t launch_inv_row(const RhsIO& io, cudaStream_t stream);
+  // stage io's inverse x pass fused with stage next's forward x pass (k_inv_fwd_row)
+  bool fuse_rows_ = false;
+  bool fuse_ok(const RhsIO& io, const RhsIO& next) const;
+  cudaError_t launch_inv_fwd_row(const RhsIO& io, const RhsIO& next, cudaStream_t stream);
   // 3D x passes that also transform along axis 1, one thread-block cluster per plane
   // (k_fwd_plane, k_inv_plane): enabled flags and persistent grid sizes
   bool plane_fwd_ = false, plane_inv_ = false;
@@ -198,7 +209,8 @@ class SpectralPlan {
   ChanTable chan_table(const int* off, const ChanEntry* ent, int nch) const;
   DictTable dict_table() const;
   cudaError_t launch_passes(const RhsIO& io, const ChanTable& ct, const std::vector<int>& hoff, int nch_run,
-                            int g_first, double* Yout, const int* ydst, cudaStream_t stream, int yplain = 0);
+                            int g_first, double* Yout, const int* ydst, cudaStream_t stream, int yplain = 0,
+                            const RhsIO* next = nullptr, bool* fused = nullptr);
   size_t dict_smem_bytes() const;
   cudaError_t launch_forward(const double* y, cudaStream_t stream);
   bool geometry(std::string* msg);

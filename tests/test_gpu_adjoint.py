@@ -59,6 +59,8 @@ CASES = {
     "cgle2d": lambda rng: Problem(2, (32, 24), (40.0, 30.0), cgle_terms(2)),
     "cgle1d_odd": lambda rng: Problem(2, (45,), (30.0,), cgle_terms(1)),
     "cgle3d": lambda rng: Problem(2, (8, 6, 10), (10.0, 8.0, 12.0), cgle_terms(3)),
+    # 128-point x rows: the forward stages run the fused inverse/forward x passes
+    "cgle3d_rows": lambda rng: Problem(2, (4, 6, 128), (5.0, 6.0, 100.0), cgle_terms(3)),
     # 2D, n=2: Y index = Yind*2 + field; u0_x = 2, u1_y = 5, u0_xy = 8
     "random2d": lambda rng: Problem(2, (16, 15), (50.0, 45.0), _random_dictionary(
         rng, 2, 2, 7, [(0.7, [0, 2, 1]), (-0.4, [1, 2, 1, 0, 1]), (0.3, [0, 5, 1]), (0.2, [1, 8, 1, 1, 2]),
@@ -67,7 +69,7 @@ CASES = {
     "random3d": lambda rng: Problem(1, (6, 4, 8), (12.0, 9.0, 15.0), _random_dictionary(
         rng, 1, 3, 6, [(0.6, [0, 3, 1]), (-0.5, [0, 1, 1, 0, 2]), (0.25, [0, 6, 1, 0, 1])])),
 }
-SEEDS = {"cgle2d": 1, "cgle1d_odd": 2, "cgle3d": 3, "random2d": 4, "random3d": 5}
+SEEDS = {"cgle2d": 1, "cgle1d_odd": 2, "cgle3d": 3, "random2d": 4, "random3d": 5, "cgle3d_rows": 6}
 
 
 @pytest.mark.parametrize("case", sorted(CASES))

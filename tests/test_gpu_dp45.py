@@ -116,6 +116,54 @@ def test_plane_passes_dp45_3d(cuda, monkeypatch):
     assert rel_err(ya, yb) < 1e-9
 
 
+@pytest.mark.parametrize("Ns,Ls", [((6, 10, 256), (5.0, 8.0, 200.0)), ((128, 128, 128), (200.0, 200.0, 200.0))])
+def test_fused_row_passes_dp45_3d(cuda, monkeypatch, Ns, Ls):
+    """3D CGLE with 256- and 128-point x rows: by default a stage's inverse x pass and
+    the next stage's forward x pass run as one kernel (k_inv_fwd_row, stages 2..5);
+    RDCU_FUSED_ROWS=0 runs them as separate kernels.  Ten adaptive attempts each: the
+    same accept/reject sequence, step sizes and states within 1e-9 (the fused forward
+    transform packs the two fields of a row into one complex line where k_fwd_x packs
+    two rows of a field, so the spectra round differently), the fused passes are the
+    ones profiled, and on the small grid the fused run follows the oracle's attempts."""
+    rng = np.random.default_rng(9)
+    prob = Problem(2, Ns, Ls, cgle_terms(3))
+    y0 = rng.uniform(-1, 1, 2 * prob.N)
+    runs = []
+    for fused in (True, False):
+        if fused:
+            monkeypatch.delenv("RDCU_FUSED_ROWS", raising=False)
+        else:
+            monkeypatch.setenv("RDCU_FUSED_ROWS", "0")
+        s, yd = _setup(cuda, prob, y0)
+        s.set_state(0.0, 1e-3, yd.data_ptr())
+        names = [p[0] for p in s.profile_passes(reps=1)]
+        assert ("inv_fwd_row" in names and "fwd_x_stage2" in names) == fused, names
+        s.set_state(0.0, 1e-3, yd.data_ptr())
+        t, h, seq = 0.0, 1e-3, []
+        for _ in range(10):
+            acc, t, h = s.step(t, h)
+            seq.append((acc, t, h))
+        out = cuda.empty_like(yd)
+        s.get_state(out.data_ptr())
+        runs.append((seq, out.cpu().numpy()))
+        s.close()
+    (sa, ya), (sb, yb) = runs
+    for i, ((a1, t1, h1), (a2, t2, h2)) in enumerate(zip(sa, sb)):
+        assert a1 == a2, i
+        assert abs(h1 - h2) <= 1e-9 * abs(h2) and abs(t1 - t2) <= 1e-9 * max(1.0, abs(t2)), (i, h1, h2)
+    assert rel_err(ya, yb) < 1e-9
+    if prob.N <= 20000:
+        o = _oracle(prob, y0, False)
+        to, ho = 0.0, 1e-3
+        for i, (acc, t, h) in enumerate(sa):
+            ok, to, ho = o.step(to, ho, 0.0, np.inf)
+            if ok:
+                o.k[0] = o.k[6]
+            assert acc == ok, i
+            assert abs(h - ho) <= 1e-9 * abs(ho), (i, h, ho)
+        assert rel_err(ya, o.y) < 1e-9
+
+
 def test_dense_output(cuda):
     rng = np.random.default_rng(21)
     prob = Problem(2, (16, 16), (20.0, 20.0), cgle_terms(2))
