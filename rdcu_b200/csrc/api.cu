@@ -183,6 +183,14 @@ int rdcu_create(rdcu_t** out, const rdcu_spec* spec) {
       return set_err(nullptr, msg.find("memory") != std::string::npos ? RDCU_ERR_NOMEM : RDCU_ERR_UNSUPPORTED, msg);
     }
   }
+  // The set-up uploads its tables with cudaMemcpy from pageable host memory, which can
+  // return before the copy has landed; the handle's stream is non-blocking, so nothing
+  // orders its first launches after those copies.  Wait for the device here.
+  e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    cudaStreamDestroy(h->stream);
+    return set_err(nullptr, RDCU_ERR_CUDA, std::string("set-up: ") + cudaGetErrorString(e));
+  }
   *out = h.release();
   return RDCU_OK;
 }
@@ -498,6 +506,8 @@ int rdcu_set_coefficients(rdcu_t* h, const double* C) {
   CHECK_CUDA(h, cudaStreamSynchronize(h->stream), "rdcu_set_coefficients");
   CHECK_CUDA(h, h->sp->set_coefficients(c), "rdcu_set_coefficients");
   if (h->adj) CHECK_CUDA(h, h->adj->set_coefficients(c), "rdcu_set_coefficients");
+  // the new tables went up with cudaMemcpy (see rdcu_create)
+  CHECK_CUDA(h, cudaDeviceSynchronize(), "rdcu_set_coefficients");
   h->dp->invalidate_k1();
   return RDCU_OK;
 }
@@ -516,6 +526,8 @@ int rdcu_adjoint_forward(rdcu_t* h, const double* y0, const double* hs, int nste
                  &msg))
       return set_err(h, msg.find("memory") != std::string::npos ? RDCU_ERR_NOMEM : RDCU_ERR_UNSUPPORTED, msg);
     h->adj = std::move(a);
+    // its tables were uploaded with cudaMemcpy (see rdcu_create)
+    CHECK_CUDA(h, cudaDeviceSynchronize(), "rdcu_adjoint_forward set-up");
   }
   CHECK_CUDA(h, h->adj->forward(y0, hs, nsteps, K, yT), "rdcu_adjoint_forward");
   return RDCU_OK;
@@ -613,6 +625,13 @@ int rdcu_ensemble_create(rdcu_ensemble_t** out, const rdcu_spec* specs, int coun
       cudaStreamDestroy(e->stream);
       return ens_err(nullptr, RDCU_ERR_CUDA, std::string("ensemble tolerances: ") + cudaGetErrorString(c));
     }
+  }
+  // set-up copies made with cudaMemcpy may still be in flight (see rdcu_create)
+  c = cudaDeviceSynchronize();
+  if (c != cudaSuccess) {
+    e->eng.release();
+    cudaStreamDestroy(e->stream);
+    return ens_err(nullptr, RDCU_ERR_CUDA, std::string("ensemble set-up: ") + cudaGetErrorString(c));
   }
   *out = e.release();
   return RDCU_OK;

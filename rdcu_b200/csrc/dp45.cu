@@ -150,7 +150,12 @@ bool DP45Engine::init(SpectralPlan* sp, double atol, double rtol, int fixed, cud
   c.nparts = sp->nparts_max;
   c.hmax = INFINITY;
   host_ctl = c;
-  if (cudaMemcpy(d_ctl_, &c, sizeof(c), cudaMemcpyHostToDevice) != cudaSuccess) return fail("controller");
+  // ordered on the engine's stream (a plain cudaMemcpy from pageable memory can return
+  // before the copy lands, and the stream does not wait for the legacy default stream)
+  *h_ctl_pinned_ = c;
+  if (cudaMemcpyAsync(d_ctl_, h_ctl_pinned_, sizeof(c), cudaMemcpyHostToDevice, st_) != cudaSuccess ||
+      cudaStreamSynchronize(st_) != cudaSuccess)
+    return fail("controller");
   return true;
 }
 

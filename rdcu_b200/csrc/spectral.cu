@@ -1154,7 +1154,9 @@ __global__ void __launch_bounds__(kMid2Threads, 1)
 // ---- middle-axis pass of 3D grids on TMA tiles: FFT (forward or inverse) of every
 // line along axis 1, in place.  A box is 8 consecutive x-wavenumber columns by the whole
 // axis-1 line of one plane (field or channel, axis-0 index); a tile is c2c_boxes(L)
-// consecutive boxes, one line per warp (256 points) or half warp (128 points).
+// consecutive boxes (32 KB), one line per warp (256 points) or half warp (128 points).
+// Two CTAs of eight warps per SM, each with its own ring of three tiles, so that one
+// CTA's barrier and store waits overlap the other's transforms.
 struct C2CPipeArgs {
   int nbox, nchunk, ntiles;
   int rev;  // take the tiles from the last to the first
@@ -1163,11 +1165,19 @@ struct C2CPipeArgs {
   int* err;
 };
 
-__host__ __device__ constexpr int c2c_boxes(int L) { return 2 * (256 / L); }
-constexpr size_t kC2cPipeSmem = 1024 + kPipeBufs * (size_t)kPipeBufBytes + 8 * kPipeBufs + 8;
+constexpr int kC2cThreads = 256;
+constexpr int kC2cBufBytes = 32 * 1024;
+constexpr int kC2cBufs = 3;
+__host__ __device__ constexpr int c2c_boxes(int L) { return 256 / L; }
+static_assert(c2c_boxes(256) * 256 * 128 == kC2cBufBytes && c2c_boxes(128) * 128 * 128 == kC2cBufBytes,
+              "a tile fills one buffer");
+static_assert((kC2cThreads / 32) * (32 / (256 / 8)) == 8 * c2c_boxes(256) &&
+                  (kC2cThreads / 32) * (32 / (128 / 8)) == 8 * c2c_boxes(128),
+              "one line of a tile per warp (256 points) or half warp (128 points)");
+constexpr size_t kC2cPipeSmem = 1024 + kC2cBufs * (size_t)kC2cBufBytes + 8 * kC2cBufs + 8;
 
 template <int L, bool INV>
-__global__ void __launch_bounds__(kPipeThreads, 1)
+__global__ void __launch_bounds__(kC2cThreads, 2)
     k_c2c_pipe(const __grid_constant__ CUtensorMap tm, C2CPipeArgs a) {
   extern __shared__ char smraw[];
   if (a.io.mode == 1 && !a.io.ctl->running) return;
@@ -1175,10 +1185,10 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
   constexpr int LPL = L / 8;
   constexpr int BOXB = L * 128;
   char* sm = smraw + ((1024 - (smem_u32(smraw) & 1023)) & 1023);
-  uint64_t* full = reinterpret_cast<uint64_t*>(sm + kPipeBufs * kPipeBufBytes);
+  uint64_t* full = reinterpret_cast<uint64_t*>(sm + kC2cBufs * kC2cBufBytes);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0) {
-    for (int k = 0; k < kPipeBufs; ++k) mbar_init(&full[k], 1);
+    for (int k = 0; k < kC2cBufs; ++k) mbar_init(&full[k], 1);
     mbar_fence_init();
     tma_prefetch(&tm);
   }
@@ -1194,7 +1204,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
   auto issue = [&](int tile, int b) {
     const int b0 = order(tile) * BPT, nb = min(BPT, a.nbox - b0);
     mbar_expect_tx(&full[b], (unsigned)(nb * BOXB));
-    char* dst = sm + b * kPipeBufBytes;
+    char* dst = sm + b * kC2cBufBytes;
     for (int k = 0; k < nb; ++k) {
       const int plane = (b0 + k) / a.nchunk, chunk = (b0 + k) - plane * a.nchunk;
       tma_load_3d(dst + k * BOXB, &tm, 16 * chunk, 0, plane, &full[b]);
@@ -1205,18 +1215,18 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
     if ((int)(blockIdx.x + gridDim.x) < a.ntiles) issue(blockIdx.x + gridDim.x, 1);
   }
   int it = 0, b = 0;
-  for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, ++it, b = (b + 1 == kPipeBufs) ? 0 : b + 1) {
-    const bool ok = mbar_wait(&full[b], (unsigned)((it / kPipeBufs) & 1));
+  for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, ++it, b = (b + 1 == kC2cBufs) ? 0 : b + 1) {
+    const bool ok = mbar_wait(&full[b], (unsigned)((it / kC2cBufs) & 1));
     if (__syncthreads_or(!ok)) {
       if (tid == 0) {
         atomicExch(a.io.mode == 1 ? &a.io.ctl->pipe_err : a.err, kPipeErrTimeout);
-        const int b1 = (b + 1) % kPipeBufs;
-        if (tile + (int)gridDim.x < a.ntiles) mbar_wait(&full[b1], (unsigned)(((it + 1) / kPipeBufs) & 1));
+        const int b1 = (b + 1) % kC2cBufs;
+        if (tile + (int)gridDim.x < a.ntiles) mbar_wait(&full[b1], (unsigned)(((it + 1) / kC2cBufs) & 1));
         bulk_wait_all();
       }
       return;
     }
-    char* tb = sm + b * kPipeBufBytes;
+    char* tb = sm + b * kC2cBufBytes;
     char* bx = tb + coff;
     if (order(tile) * BPT + (li >> 3) < a.nbox) {
       double2 v[8];
@@ -1236,7 +1246,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
       const int nt = tile + 2 * (int)gridDim.x;
       if (nt < a.ntiles) {
         bulk_wait_read_1();
-        issue(nt, (b + 2) % kPipeBufs);
+        issue(nt, (b + 2) % kC2cBufs);
       }
     }
   }
@@ -1797,9 +1807,9 @@ __global__ void __launch_bounds__(row_warps(ERR, NF) * 32, 1) k_inv_row(InvRowAr
     __syncwarp();  // this row's copies (every lane's) landed
     const double2* sp = slot_spec(k);
     const double* su = slot_u(k);
-    // ERR: the row's slope sums and y at the lane's points (y gives the error scale with
-    // the staged stage-7 state), loaded before the transform so that it covers their
-    // latency
+    // ERR: the row's slope sums and y at the lane's points, loaded before the transform
+    // so that it covers their latency (y and the staged stage-7 state give the error
+    // scale)
     double es_t[ERR ? 8 : 1][NF], y_t[ERR ? 8 : 1][NF];
     if (ERR && live) {
 #pragma unroll
@@ -1861,7 +1871,7 @@ __global__ void __launch_bounds__(row_warps(ERR, NF) * 32, 1) k_inv_row(InvRowAr
         if (ERR) {
           // k_inv_x's error kernel (dp45.cu:79-84) from the forward pass's slope sum
           const double es = es_t[ERR ? p : 0][i] + c_e[6] * acc;
-          const double ev = r.h * es / stage7_scale(r, y_t[ERR ? p : 0][i], u[i]);
+          const double ev = r.h * es / stage7_scale(r, y_t[ERR ? p : 0][i], su[i * L + x]);
           err2 += ev * ev;
         }
       }
@@ -3569,17 +3579,17 @@ cudaError_t SpectralPlan::launch_c2c_pipe(bool inv, int nplanes, cudaStream_t st
   a.tw = tw_ax_[1];
   a.io = io;
   a.err = pipe_err_;
-  const int grid = std::max(1, std::min(a.ntiles, sms_));
+  const int grid = std::max(1, std::min(a.ntiles, 2 * sms_));  // two resident CTAs per SM
   if (!inv) {
     if (Ns[1] == 128)
-      k_c2c_pipe<128, false><<<grid, kPipeThreads, kC2cPipeSmem, st>>>(tm_sf_c2c_, a);
+      k_c2c_pipe<128, false><<<grid, kC2cThreads, kC2cPipeSmem, st>>>(tm_sf_c2c_, a);
     else
-      k_c2c_pipe<256, false><<<grid, kPipeThreads, kC2cPipeSmem, st>>>(tm_sf_c2c_, a);
+      k_c2c_pipe<256, false><<<grid, kC2cThreads, kC2cPipeSmem, st>>>(tm_sf_c2c_, a);
   } else {
     if (Ns[1] == 128)
-      k_c2c_pipe<128, true><<<grid, kPipeThreads, kC2cPipeSmem, st>>>(tm_sc_c2c_, a);
+      k_c2c_pipe<128, true><<<grid, kC2cThreads, kC2cPipeSmem, st>>>(tm_sc_c2c_, a);
     else
-      k_c2c_pipe<256, true><<<grid, kPipeThreads, kC2cPipeSmem, st>>>(tm_sc_c2c_, a);
+      k_c2c_pipe<256, true><<<grid, kC2cThreads, kC2cPipeSmem, st>>>(tm_sc_c2c_, a);
   }
   return cudaGetLastError();
 }
