@@ -35,3 +35,20 @@ def test_failed_run_is_reported(tmp_path):
     exe = _fake_cli(tmp_path, ["rdcu initialization failed: x"], rc=1)
     res, err = bench.cli_run(exe, dict(cli="-n 2", Ns=(8, 8), outputs=2))
     assert res is None and "rc 1" in err
+
+
+def test_launches_per_attempt_separate_and_fused():
+    """Per-attempt launch counts of the profiled passes: five forward and inverse x
+    passes without fusion; with the fused row pass (stages 2-5) stage 2's forward pass,
+    four fused launches, stage 6's inverse pass and stage 7's two x passes.  Either way
+    the 3D attempt's spectral passes run six times each, and the fused attempt is the 27
+    launches (with the controller) of its launch list."""
+    sep = ["fwd_x", "c2c_axis1_fwd", "mid_axis0", "c2c_axis1_inv", "inv_x_dictionary", "fwd_x_stage7", "inv_x_stage7"]
+    w = [bench.launches_per_attempt_of(p, sep) for p in sep]
+    assert w == [5, 6, 6, 6, 5, 1, 1]
+    assert sum(w) + 1 == 31
+    fused = sep + ["inv_fwd_row", "fwd_x_stage2"]
+    w = dict((p, bench.launches_per_attempt_of(p, fused)) for p in fused)
+    assert w == {"fwd_x": 0, "c2c_axis1_fwd": 6, "mid_axis0": 6, "c2c_axis1_inv": 6, "inv_x_dictionary": 1,
+                 "fwd_x_stage7": 1, "inv_x_stage7": 1, "inv_fwd_row": 4, "fwd_x_stage2": 1}
+    assert sum(w.values()) + 1 == 27
