@@ -173,14 +173,18 @@ class ClockSampler:
 # CGLE, from one ncu capture per kernel (`ncu --set full ... python -m tests.profile_case
 # 256,256,128 --attempts 2 --reps 1`, 8.39 M grid points; the axis-1 inverse pass is
 # the forward one's kernel on the same bytes); traffic grows with the grid points, so
-# the full-size workload's figure is this one scaled by its points.
+# the full-size workload's figure is this one scaled by its points.  inv_fwd_row (the
+# fused stage 4 -> 5 pass) and the axis-1 passes are captures of the current kernels;
+# the stage-7 entries predate the forward pass writing only the slope sums (its capture
+# includes the scale array, 134 MB at this size, which it no longer writes).
 NCU_POINTS = 256 * 256 * 128
 # DRAM bytes per launch of the defect-line grid passes on the 128^3 workload frames, from
 # one ncu capture (`ncu --set full -k regex:"k_(faces|hook|corr)" ... bench.py --workload
 # lines_cgle3d_128 --steps 1 --warmup 3`): k_faces reads the 16.8 MB phase field once.
 NCU_TRAFFIC_LINES = {"faces": 16.8e6}
-NCU_TRAFFIC_3D = {"fwd_x": 772.4e6, "c2c_axis1_fwd": 218.2e6, "mid_axis0": 225.0e6, "c2c_axis1_inv": 218.2e6,
-                  "inv_x_dictionary": 373.6e6, "fwd_x_stage7": 1296.7e6, "inv_x_stage7": 656.5e6}
+NCU_TRAFFIC_3D = {"fwd_x": 772.4e6, "c2c_axis1_fwd": 218.8e6, "mid_axis0": 225.0e6, "c2c_axis1_inv": 218.8e6,
+                  "inv_x_dictionary": 373.6e6, "fwd_x_stage7": 1296.7e6, "inv_x_stage7": 656.5e6,
+                  "inv_fwd_row": 1171.4e6}
 
 
 def combine_ranks(seconds, work, device):
