@@ -1899,7 +1899,8 @@ __global__ void __launch_bounds__(row_warps(ERR, NF) * 32, 1) k_inv_row(InvRowAr
 // dictionary of at most two channels).  Per row, k_inv_row's steps (staged channel spectra
 // and fields, inverse transform, dictionary, slope k_s written), then stage s + 1 at the
 // lane's points: its state from y, the slopes before k_s (read while the inverse
-// transform runs) and k_s still in registers -- stage_value_t2's terms in its order --
+// transform runs) and k_s still in registers -- the stage combination of dp45.cu:34-69
+// with stage_value_t2's terms in its order --
 // written out, then transformed forward as one complex line (field 0 real part, field 1
 // imaginary part) and split into the two fields' half spectra with k_fwd_x's formulas.
 // Against separate launches this saves reading k_s back and one launch per stage.
